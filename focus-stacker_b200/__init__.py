@@ -1,0 +1,14 @@
+"""B200 (sm_100a) implementation of the focus-stacker remap + pyramid-contrast
+fusion hot path: a C-ABI shared library (libfocuscuda.so, csrc/) and its
+host-side mirror of the reference's operator interface (api.py).
+
+The directory name carries a hyphen, so load it with load_package() (or
+importlib) under the module name `focus_stacker_b200`.
+"""
+from . import _lib  # noqa: F401
+from .api import (  # noqa: F401
+    Context, FocusCudaError, ImagePose, Method, PyramidContrastStack, Rect, SCENE_PRODUCTION, SCENE_SMALL,
+    compute_common_overlap_roi, exact_expand_divisor, fuse_aligned_images, fuse_remapped_images,
+    inverse_map_points, parse_method, parse_window_size, remap_rigid_image, remap_rigid_image_device,
+    synth_frame_device, synth_pose,
+)

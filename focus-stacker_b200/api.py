@@ -1,0 +1,394 @@
+"""Host-side mirror of the reference's operator interface for the remap +
+pyramid-contrast fusion path, over libfocuscuda.so.
+
+Names and argument meanings follow the reference (asingleoat/focus-stacker):
+  * ImagePose / Rect                 src/optimize.zig:32-48, src/remap.zig:573-578
+  * compute_common_overlap_roi       src/remap.zig:585-633 (None = no overlap)
+  * remap_rigid_image                src/remap.zig:166-204 (RGB/gray u8 -> +alpha)
+  * Method / parse_method            src/fuse/config.zig:10-24, 281-287, plus
+                                     the drop-in "cuda-pyramid-contrast"
+  * fuse_remapped_images             stack path, src/stack/pipeline.zig:314-605
+  * fuse_aligned_images              fuse-only path, src/fuse/pipeline.zig:148-445
+Errors are raised as FocusCudaError carrying the C status (the reference's
+Zig error unions map onto the same categories: InvalidValue, OutOfMemory,
+MismatchedImageSizes, ...).  Host arrays are numpy; device buffers are any
+object with data_ptr() (e.g. a torch CUDA tensor) or a raw integer pointer.
+"""
+from __future__ import annotations
+
+import ctypes
+import enum
+from dataclasses import dataclass, fields
+from typing import Optional, Sequence
+
+import numpy as np
+
+from . import _lib
+
+L = _lib.lib
+
+
+class FocusCudaError(RuntimeError):
+    def __init__(self, status: int, message: str = ""):
+        self.status = status
+        self.code = _lib.STATUS_NAMES.get(status, str(status))
+        super().__init__(f"{self.code}: {message}" if message else self.code)
+
+
+@dataclass
+class ImagePose:
+    yaw: float = 0.0
+    pitch: float = 0.0
+    roll: float = 0.0
+    hfov_delta: float = 0.0
+    trans_x: float = 0.0
+    trans_y: float = 0.0
+    trans_z: float = 0.0
+    translation_plane_yaw: float = 0.0
+    translation_plane_pitch: float = 0.0
+    radial_a: float = 0.0
+    radial_b: float = 0.0
+    radial_c: float = 0.0
+    center_shift_x: float = 0.0
+    center_shift_y: float = 0.0
+    base_hfov_degrees: float = 50.0
+
+    def to_c(self) -> _lib.FsPose:
+        return _lib.FsPose(*[float(getattr(self, f.name)) for f in fields(self)])
+
+    @staticmethod
+    def from_c(p: _lib.FsPose) -> "ImagePose":
+        return ImagePose(*[getattr(p, f.name) for f in fields(ImagePose)])
+
+    def as_dict(self) -> dict:
+        return {f.name: float(getattr(self, f.name)) for f in fields(self)}
+
+
+@dataclass(frozen=True)
+class Rect:
+    left: int
+    top: int
+    right: int
+    bottom: int
+
+    @property
+    def width(self) -> int:
+        return self.right - self.left
+
+    @property
+    def height(self) -> int:
+        return self.bottom - self.top
+
+    def to_c(self) -> _lib.FsRect:
+        return _lib.FsRect(self.left, self.top, self.right, self.bottom)
+
+    def as_tuple(self):
+        return (self.left, self.top, self.right, self.bottom)
+
+
+def _pose(p) -> ImagePose:
+    if p is None:
+        return ImagePose()
+    if isinstance(p, ImagePose):
+        return p
+    if isinstance(p, dict):
+        return ImagePose(**p)
+    return ImagePose(**{f.name: getattr(p, f.name) for f in fields(ImagePose)})
+
+
+class Method(enum.Enum):
+    """Fusion methods of the reference CLIs plus the CUDA drop-in."""
+    HARDMASK_CONTRAST = "hardmask-contrast"
+    SOFTMASK_CONTRAST = "softmask-contrast"
+    PYRAMID_CONTRAST = "pyramid-contrast"
+    HYBRID_PYRAMID_CONTRAST = "hybrid-pyramid-contrast"
+    CUDA_PYRAMID_CONTRAST = "cuda-pyramid-contrast"
+
+    def cli_name(self) -> str:
+        return self.value
+
+
+def parse_method(value: str) -> Method:
+    """src/fuse/config.zig:281-287; unknown names raise ValueError (InvalidValue)."""
+    for m in Method:
+        if m.value == value:
+            return m
+    raise ValueError("InvalidValue")
+
+
+def parse_window_size(value: str) -> int:
+    """src/fuse/config.zig:295-299: odd and >= 3."""
+    try:
+        v = int(value, 10)
+    except ValueError:
+        raise ValueError("InvalidValue") from None
+    if v <= 0 or v < 3 or (v & 1) == 0:
+        raise ValueError("InvalidValue")
+    return v
+
+
+def _check(rc: int, ctx_handle=None):
+    if rc != _lib.FS_OK:
+        msg = ""
+        if ctx_handle:
+            raw = L().fs_last_error(ctx_handle)
+            msg = raw.decode() if raw else ""
+        raise FocusCudaError(rc, msg)
+
+
+def _ptr(buf) -> int:
+    if isinstance(buf, int):
+        return buf
+    if hasattr(buf, "data_ptr"):
+        return int(buf.data_ptr())
+    raise TypeError("expected a device buffer with data_ptr() or an integer pointer")
+
+
+class Context:
+    """One CUDA device context (fs_ctx): stream, HBM budget, kernel accounting."""
+
+    def __init__(self, device: int = 0, hbm_budget_bytes: int = 0):
+        h = ctypes.c_void_p()
+        rc = L().fs_create(device, hbm_budget_bytes, ctypes.byref(h))
+        if rc != _lib.FS_OK:
+            raise FocusCudaError(rc, "fs_create")
+        self.handle = h
+        self.device = device
+
+    def close(self):
+        if self.handle:
+            L().fs_destroy(self.handle)
+            self.handle = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def last_error(self) -> str:
+        raw = L().fs_last_error(self.handle)
+        return raw.decode() if raw else ""
+
+    def synchronize(self):
+        _check(L().fs_ctx_synchronize(self.handle), self.handle)
+
+    def device_bytes(self) -> int:
+        return int(L().fs_ctx_device_bytes(self.handle))
+
+    def launch_count(self) -> int:
+        return int(L().fs_ctx_launch_count(self.handle))
+
+    def set_kernel_timing(self, enable: bool):
+        _check(L().fs_ctx_set_kernel_timing(self.handle, 1 if enable else 0), self.handle)
+
+    def kernel_stats(self, kernel: str):
+        n = ctypes.c_uint64()
+        ms = ctypes.c_double()
+        _check(L().fs_ctx_kernel_stats(self.handle, kernel.encode(), ctypes.byref(n), ctypes.byref(ms)), self.handle)
+        return int(n.value), float(ms.value)
+
+
+# ------------------------------------------------------------ pose utilities
+def compute_common_overlap_roi(remap_active: Sequence[bool], widths: Sequence[int], heights: Sequence[int],
+                               poses: Sequence) -> Optional[Rect]:
+    n = len(poses)
+    parr = (_lib.FsPose * max(1, n))(*[_pose(p).to_c() for p in poses])
+    w = (ctypes.c_uint32 * max(1, n))(*widths)
+    h = (ctypes.c_uint32 * max(1, n))(*heights)
+    a = (ctypes.c_uint8 * max(1, n))(*[1 if x else 0 for x in remap_active])
+    out = _lib.FsRect()
+    has = ctypes.c_int()
+    _check(L().fs_compute_roi(parr, w, h, a, n, ctypes.byref(out), ctypes.byref(has)))
+    return Rect(out.left, out.top, out.right, out.bottom) if has.value else None
+
+
+def inverse_map_points(pose, width: int, height: int, xy: np.ndarray) -> np.ndarray:
+    xy = np.ascontiguousarray(xy, dtype=np.float64).reshape(-1, 2)
+    out = np.zeros_like(xy)
+    p = _pose(pose).to_c()
+    _check(L().fs_inverse_map_points(ctypes.byref(p), width, height, xy.shape[0],
+                                     xy.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                     out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
+    return out
+
+
+def exact_expand_divisor(x: int, y: int, src_w: int, src_h: int) -> float:
+    return float(L().fs_exact_expand_divisor(x, y, src_w, src_h))
+
+
+# ---------------------------------------------------------------------- remap
+def remap_rigid_image(ctx: Context, src: np.ndarray, pose, roi: Optional[Rect] = None) -> np.ndarray:
+    """src: HxW (gray) or HxWx3 uint8.  Returns the ROI-sized image with an extra alpha channel."""
+    src = np.ascontiguousarray(src)
+    if src.dtype != np.uint8:
+        raise FocusCudaError(8, "only 8-bit samples are implemented")
+    h, w = src.shape[:2]
+    ch = 1 if src.ndim == 2 else src.shape[2]
+    r = roi or Rect(0, 0, w, h)
+    out = np.zeros((r.height, r.width, ch + 1), np.uint8)
+    p = _pose(pose).to_c()
+    rc = L().fs_remap_frame(ctx.handle, src.ctypes.data, w * ch, w, h, ch, ctypes.byref(p),
+                            ctypes.byref(r.to_c()), out.ctypes.data, r.width * (ch + 1))
+    _check(rc, ctx.handle)
+    return out
+
+
+def remap_rigid_image_device(ctx: Context, src, src_stride: int, width: int, height: int, channels: int, pose,
+                             roi: Optional[Rect], dst, dst_stride: int):
+    p = _pose(pose).to_c()
+    r = roi.to_c() if roi else None
+    rc = L().fs_remap_frame_device(ctx.handle, _ptr(src), src_stride, width, height, channels, ctypes.byref(p),
+                                   ctypes.byref(r) if r else None, _ptr(dst), dst_stride)
+    _check(rc, ctx.handle)
+
+
+# --------------------------------------------------------------------- fusion
+class PyramidContrastStack:
+    """Streaming two-pass pyramid-contrast fusion on the device (fs_stack).
+
+    add_frame / add_frame_device run pass 1 as frames arrive (in the
+    reference's active-frame order); finish runs pass 2 and the collapse."""
+
+    def __init__(self, ctx: Context, src_width: int, src_height: int, frame_count: int, roi: Optional[Rect] = None,
+                 channels: int = 3, contrast_window: int = 5, aligned: bool = False, frames_per_batch: int = 0,
+                 level_storage: int = 0):
+        self.ctx = ctx
+        d = _lib.FsStackDesc()
+        d.src_width, d.src_height = src_width, src_height
+        d.has_roi = 1 if roi is not None else 0
+        if roi is not None:
+            d.roi = roi.to_c()
+        d.channels = channels
+        d.sample_bits = 8
+        d.frame_count = frame_count
+        d.contrast_window = contrast_window
+        d.input_is_aligned = 1 if aligned else 0
+        d.level_storage = level_storage
+        d.frames_per_batch = frames_per_batch
+        self.desc = d
+        h = ctypes.c_void_p()
+        _check(L().fs_stack_begin(ctx.handle, ctypes.byref(d), ctypes.byref(h)), ctx.handle)
+        self.handle = h
+        w, hh = ctypes.c_uint32(), ctypes.c_uint32()
+        L().fs_stack_output_size(h, ctypes.byref(w), ctypes.byref(hh))
+        self.out_width, self.out_height = w.value, hh.value
+        self._keep = []
+
+    def set_base_output(self, dst, row_stride_elems: int):
+        """Also write the collapsed FP32 base (RGB, device buffer) during finish."""
+        self._keep.append(dst)
+        _check(L().fs_stack_set_base_output(self.handle, _ptr(dst), row_stride_elems), self.ctx.handle)
+
+    def add_frame(self, pixels: np.ndarray, pose=None):
+        pixels = np.ascontiguousarray(pixels)
+        p = _pose(pose).to_c() if pose is not None else None
+        rc = L().fs_stack_add_frame(self.handle, pixels.ctypes.data, pixels.shape[1] * pixels.shape[2],
+                                    ctypes.byref(p) if p is not None else None)
+        _check(rc, self.ctx.handle)
+
+    def add_frame_device(self, buf, row_stride: int, pose=None):
+        p = _pose(pose).to_c() if pose is not None else None
+        self._keep.append(buf)
+        rc = L().fs_stack_add_frame_device(self.handle, _ptr(buf), row_stride, ctypes.byref(p) if p is not None else None)
+        _check(rc, self.ctx.handle)
+
+    def finish(self, refetch=None) -> np.ndarray:
+        out = np.zeros((self.out_height, self.out_width, 3), np.uint8)
+        self.finish_into(out, refetch)
+        return out
+
+    def finish_into(self, out: np.ndarray, refetch=None):
+        cb = self._make_cb(refetch)
+        rc = L().fs_stack_finish(self.handle, cb, None, out.ctypes.data, out.strides[0])
+        _check(rc, self.ctx.handle)
+
+    def finish_device(self, dst, dst_stride: int, refetch=None):
+        cb = self._make_cb(refetch)
+        _check(L().fs_stack_finish_device(self.handle, cb, None, _ptr(dst), dst_stride), self.ctx.handle)
+
+    def _make_cb(self, refetch):
+        held = []
+
+        def cb(user, index, pixels, stride):
+            try:
+                arr = np.ascontiguousarray(refetch(int(index)))
+                held.append(arr)
+                pixels[0] = arr.ctypes.data
+                stride[0] = arr.shape[1] * arr.shape[2]
+                return 0
+            except Exception:
+                return 1
+
+        self._cb_hold = (_lib.FETCH_CB(cb) if refetch else _lib.FETCH_CB(0), held)
+        return self._cb_hold[0]
+
+    def close(self):
+        if self.handle:
+            L().fs_stack_destroy(self.handle)
+            self.handle = None
+            self._keep = []
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def fuse_remapped_images(ctx: Context, sources: Sequence[np.ndarray], poses: Sequence, roi: Optional[Rect],
+                         contrast_window: int = 5, frames_per_batch: int = 0) -> np.ndarray:
+    """Stack path: remap every active frame through its pose into the ROI and
+    fuse with pyramid-contrast (runCollapsedPyramidStackPass)."""
+    h, w = sources[0].shape[:2]
+    with PyramidContrastStack(ctx, w, h, len(sources), roi=roi, channels=3, contrast_window=contrast_window,
+                              frames_per_batch=frames_per_batch) as st:
+        for src, pose in zip(sources, poses):
+            if src.shape[:2] != (h, w):
+                raise FocusCudaError(7, "MismatchedImageSizes")
+            st.add_frame(src, pose)
+        return st.finish()
+
+
+def fuse_aligned_images(ctx: Context, images: Sequence[np.ndarray], contrast_window: int = 5,
+                        frames_per_batch: int = 0) -> np.ndarray:
+    """Fuse-only path (focus_fuse_zig): pre-aligned RGB or RGBA frames."""
+    h, w, c = images[0].shape
+    with PyramidContrastStack(ctx, w, h, len(images), channels=c, contrast_window=contrast_window, aligned=True,
+                              frames_per_batch=frames_per_batch) as st:
+        for im in images:
+            if im.shape != (h, w, c):
+                raise FocusCudaError(7, "MismatchedImageSizes" if im.shape[:2] != (h, w) else "MismatchedImageFormats")
+            st.add_frame(im)
+        return st.finish()
+
+
+# ------------------------------------------------------------------ synthetic
+SCENE_SMALL = 0       # blur <= 3 px, shifts +-20 px, roll +-0.2 deg (1024x768-class stacks)
+SCENE_PRODUCTION = 1  # blur <= 8 px, shifts +-60 px, roll +-0.3 deg (7952x5304-class stacks)
+
+
+def synth_pose(seed: int, scene: int, width: int, height: int, frame: int, frame_count: int) -> ImagePose:
+    p = _lib.FsPose()
+    _check(L().fs_synth_pose(seed, scene, width, height, frame, frame_count, ctypes.byref(p)))
+    return ImagePose.from_c(p)
+
+
+def synth_frame_device(ctx: Context, seed: int, scene: int, width: int, height: int, frame: int, frame_count: int,
+                       dst, dst_stride: int) -> ImagePose:
+    p = _lib.FsPose()
+    _check(L().fs_synth_frame_device(ctx.handle, seed, scene, width, height, frame, frame_count, _ptr(dst), dst_stride,
+                                     ctypes.byref(p)), ctx.handle)
+    return ImagePose.from_c(p)

@@ -1,0 +1,762 @@
+// C ABI of libfocuscuda.so: contexts, stacks (two-pass pyramid-contrast
+// fusion), remap-only and synthetic-input entry points.
+//
+// A stack holds on the device: the weight sums and union support of pass 1
+// (level-0 planes), the mask-support pyramid, the FP32 accumulator pyramid,
+// K per-frame level slots for pass 2, and (when the HBM budget allows) the
+// frames themselves, so pass 2 does not need them again from the host.  The
+// host side only composes per-frame transforms (FP64) and sequences launches
+// on one stream.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/focuscuda.h"
+#include "fs_common.h"
+#include "fs_host.h"
+#include "fusion_kernels.cuh"
+
+using namespace fs;
+
+namespace {
+
+struct KernelTiming {
+  const char* name;
+  cudaEvent_t start, stop;
+};
+
+}  // namespace
+
+struct fs_ctx {
+  int device = 0;
+  uint64_t budget = 0;
+  uint64_t held = 0;
+  cudaStream_t stream = nullptr;
+  cudaStream_t copy = nullptr;
+  std::string err;
+  mutable std::mutex mu;
+  bool timing = false;
+  std::vector<KernelTiming> timings;
+  uint64_t launches = 0;
+};
+
+namespace {
+
+struct Alloc {
+  void* p = nullptr;
+  size_t bytes = 0;
+};
+
+int set_err(fs_ctx* ctx, int code, const std::string& msg) {
+  if (ctx) {
+    std::lock_guard<std::mutex> g(ctx->mu);
+    ctx->err = msg;
+  }
+  return code;
+}
+
+int cuda_err(fs_ctx* ctx, cudaError_t e, const char* what) {
+  return set_err(ctx, FS_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+int dev_alloc(fs_ctx* ctx, size_t bytes, void** out) {
+  if (bytes == 0) bytes = 16;
+  if (ctx->held + bytes > ctx->budget)
+    return set_err(ctx, FS_ERR_BUDGET, "device memory budget exceeded (" + std::to_string(ctx->held + bytes) +
+                                           " > " + std::to_string(ctx->budget) + " bytes)");
+  cudaError_t e = cudaMalloc(out, bytes);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return set_err(ctx, FS_ERR_OOM, std::string("cudaMalloc failed: ") + cudaGetErrorString(e));
+  }
+  ctx->held += bytes;
+  return FS_OK;
+}
+
+void dev_free(fs_ctx* ctx, void* p, size_t bytes) {
+  if (!p) return;
+  cudaFree(p);
+  if (bytes == 0) bytes = 16;
+  ctx->held -= std::min<uint64_t>(ctx->held, bytes);
+}
+
+// Launch wrapper: counts launches and optionally brackets them with events
+// on the launching stream.
+template <typename F>
+cudaError_t timed(fs_ctx* ctx, const char* name, F&& launch) {
+  KernelTiming t = {name, nullptr, nullptr};
+  if (ctx->timing) {
+    cudaEventCreate(&t.start);
+    cudaEventCreate(&t.stop);
+    cudaEventRecord(t.start, ctx->stream);
+  }
+  cudaError_t e = launch();
+  ctx->launches += 1;
+  if (ctx->timing) {
+    cudaEventRecord(t.stop, ctx->stream);
+    ctx->timings.push_back(t);
+  }
+  return e;
+}
+
+int64_t round_up(int64_t v, int64_t m) { return (v + m - 1) / m * m; }
+
+}  // namespace
+
+// ===================================================================== stack
+struct fs_stack {
+  fs_ctx* ctx = nullptr;
+  fs_stack_desc d;
+  fs_rect roi;
+  uint32_t W = 0, H = 0, L = 0, K = 1, border = 2;
+  bool aligned = false;
+  std::vector<uint32_t> lw, lh;
+  std::vector<int64_t> pitch;  // per level, elements (f32) == bytes (u8)
+  float* norm = nullptr;
+  uint8_t* uni = nullptr;
+  std::vector<uint8_t*> sm;    // mask support, level l (sm[0] == uni)
+  std::vector<float*> acc;     // per level, 3 planes
+  std::vector<std::vector<LevelPlanes>> slot;  // [k][l], l = 1 .. L-2
+  uint8_t* out_dev = nullptr;
+  std::vector<Alloc> allocs;
+  struct Frame {
+    const uint8_t* px = nullptr;  // device pointer (owned or borrowed)
+    int64_t pitch = 0;
+    bool owned = false;
+    bool resident = true;         // false: transient staging copy, pass 2 refetches it
+    fs_pose pose;
+  };
+  std::vector<Frame> frames;
+  std::vector<uint8_t*> staging;  // refetch buffers for pass 2 (K), when frames are not resident
+  int64_t frame_pitch = 0;        // pitch of owned frame copies
+  size_t frame_bytes = 0;
+  bool keep_frames = true;
+  size_t pass1_done = 0;          // frames whose pass 1 has been launched
+  bool finished = false;
+  cudaEvent_t copy_done = nullptr;
+  float* base_out = nullptr;      // optional device buffer for the collapsed base (RGB f32)
+  int64_t base_pitch = 0;         // elements
+};
+
+namespace {
+
+uint32_t in_channels(const fs_stack* s) { return s->d.channels; }
+
+int stack_alloc(fs_stack* s, size_t bytes, void** out) {
+  int rc = dev_alloc(s->ctx, bytes, out);
+  if (rc == FS_OK) s->allocs.push_back({*out, bytes == 0 ? 16 : bytes});
+  return rc;
+}
+
+bool build_frame_in(fs_stack* s, const fs_stack::Frame& fr, FrameIn* fi, std::string* why) {
+  std::memset(fi, 0, sizeof(*fi));
+  fi->src.px = fr.px;
+  fi->src.pitch = fr.pitch;
+  fi->src.w = (int32_t)s->d.src_width;
+  fi->src.h = (int32_t)s->d.src_height;
+  fi->src.ch = (int32_t)in_channels(s);
+  if (s->aligned) {
+    fi->warp.kind = WARP_ALIGNED;
+    return true;
+  }
+  const char* w = nullptr;
+  if (!compose_warp(fr.pose, s->d.src_width, s->d.src_height, s->roi, &fi->warp, &w)) {
+    *why = w ? w : "invalid pose";
+    return false;
+  }
+  return true;
+}
+
+int launch_pass1_batch(fs_stack* s, size_t begin, size_t end) {
+  Pass1Args a;
+  std::memset(&a, 0, sizeof(a));
+  a.W = (int32_t)s->W;
+  a.H = (int32_t)s->H;
+  a.border = (int32_t)s->border;
+  a.window_ok = (s->W >= s->d.contrast_window && s->H >= s->d.contrast_window) ? 1 : 0;
+  a.K = (int32_t)(end - begin);
+  a.first = begin == 0 ? 1 : 0;
+  a.norm = s->norm;
+  a.norm_pitch = s->pitch[0];
+  a.uni = s->uni;
+  a.uni_pitch = s->pitch[0];
+  for (size_t k = begin; k < end; ++k) {
+    std::string why;
+    if (!build_frame_in(s, s->frames[k], &a.f[k - begin], &why)) return set_err(s->ctx, FS_ERR_INVALID, why);
+  }
+  cudaError_t e = timed(s->ctx, "pass1", [&] { return launch_pass1(a, s->ctx->stream); });
+  if (e != cudaSuccess) return cuda_err(s->ctx, e, "pass1 launch");
+  return FS_OK;
+}
+
+int run_pending_pass1(fs_stack* s, bool flush) {
+  while (s->frames.size() - s->pass1_done >= s->K || (flush && s->frames.size() > s->pass1_done)) {
+    size_t begin = s->pass1_done, end = std::min(s->frames.size(), begin + s->K);
+    int rc = launch_pass1_batch(s, begin, end);
+    if (rc != FS_OK) return rc;
+    s->pass1_done = end;
+  }
+  return FS_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int fs_api_version(void) { return FS_API_VERSION; }
+
+const char* fs_status_string(int status) {
+  switch (status) {
+    case FS_OK: return "ok";
+    case FS_ERR_INVALID: return "invalid argument";
+    case FS_ERR_OOM: return "out of memory";
+    case FS_ERR_BUDGET: return "device memory budget exceeded";
+    case FS_ERR_CUDA: return "CUDA error";
+    case FS_ERR_TIMEOUT: return "device wait timed out";
+    case FS_ERR_STATE: return "call out of order";
+    case FS_ERR_MISMATCH: return "frame does not match the stack";
+    case FS_ERR_UNSUPPORTED: return "unsupported";
+    case FS_ERR_NO_DEVICE: return "no usable CUDA device";
+    default: return "unknown status";
+  }
+}
+
+void fs_pose_default(fs_pose* p) {
+  std::memset(p, 0, sizeof(*p));
+  p->base_hfov_degrees = 50.0;
+}
+
+int fs_create(int device, uint64_t hbm_budget_bytes, fs_ctx** out) {
+  if (!out) return FS_ERR_INVALID;
+  *out = nullptr;
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n <= device || device < 0) {
+    cudaGetLastError();
+    return FS_ERR_NO_DEVICE;
+  }
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, device) != cudaSuccess || prop.major < 10) {
+    cudaGetLastError();
+    return FS_ERR_NO_DEVICE;
+  }
+  if (cudaSetDevice(device) != cudaSuccess) return FS_ERR_NO_DEVICE;
+  fs_ctx* c = new fs_ctx();
+  c->device = device;
+  size_t free_b = 0, total_b = 0;
+  cudaMemGetInfo(&free_b, &total_b);
+  c->budget = hbm_budget_bytes ? hbm_budget_bytes : (uint64_t)(free_b / 2);
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&c->copy, cudaStreamNonBlocking) != cudaSuccess) {
+    delete c;
+    return FS_ERR_CUDA;
+  }
+  *out = c;
+  return FS_OK;
+}
+
+void fs_destroy(fs_ctx* ctx) {
+  if (!ctx) return;
+  cudaSetDevice(ctx->device);
+  for (auto& t : ctx->timings) {
+    cudaEventDestroy(t.start);
+    cudaEventDestroy(t.stop);
+  }
+  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  if (ctx->copy) cudaStreamDestroy(ctx->copy);
+  delete ctx;
+}
+
+const char* fs_last_error(const fs_ctx* ctx) {
+  if (!ctx) return "no context";
+  return ctx->err.c_str();
+}
+
+uint64_t fs_ctx_device_bytes(const fs_ctx* ctx) { return ctx ? ctx->held : 0; }
+
+int fs_ctx_set_kernel_timing(fs_ctx* ctx, int enable) {
+  if (!ctx) return FS_ERR_INVALID;
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
+  for (auto& t : ctx->timings) {
+    cudaEventDestroy(t.start);
+    cudaEventDestroy(t.stop);
+  }
+  ctx->timings.clear();
+  ctx->timing = enable != 0;
+  return FS_OK;
+}
+
+int fs_ctx_kernel_stats(fs_ctx* ctx, const char* kernel, uint64_t* launches, double* total_ms) {
+  if (!ctx || !kernel) return FS_ERR_INVALID;
+  cudaSetDevice(ctx->device);
+  cudaError_t e = cudaStreamSynchronize(ctx->stream);
+  if (e != cudaSuccess) return cuda_err(ctx, e, "synchronize");
+  uint64_t n = 0;
+  double ms = 0.0;
+  for (auto& t : ctx->timings) {
+    if (std::strcmp(t.name, kernel) != 0) continue;
+    float v = 0.f;
+    cudaEventElapsedTime(&v, t.start, t.stop);
+    ms += v;
+    ++n;
+  }
+  if (launches) *launches = n;
+  if (total_ms) *total_ms = ms;
+  return FS_OK;
+}
+
+uint64_t fs_ctx_launch_count(const fs_ctx* ctx) { return ctx ? ctx->launches : 0; }
+
+int fs_ctx_synchronize(fs_ctx* ctx) {
+  if (!ctx) return FS_ERR_INVALID;
+  cudaSetDevice(ctx->device);
+  cudaError_t e = cudaStreamSynchronize(ctx->stream);
+  if (e != cudaSuccess) return cuda_err(ctx, e, "synchronize");
+  return FS_OK;
+}
+
+// ---------------------------------------------------------------- pose utils
+int fs_compute_roi(const fs_pose* poses, const uint32_t* widths, const uint32_t* heights, const uint8_t* active,
+                   size_t n, fs_rect* out, int* has_roi) {
+  if (!poses || !widths || !heights || !out || !has_roi) return FS_ERR_INVALID;
+  fs_rect r = {0, 0, 0, 0};
+  bool ok = compute_roi(poses, widths, heights, active, n, &r);
+  *has_roi = ok ? 1 : 0;
+  *out = r;
+  return FS_OK;
+}
+
+int fs_inverse_map_points(const fs_pose* pose, uint32_t width, uint32_t height, size_t n, const double* xy,
+                          double* out_xy) {
+  if (!pose || (!xy && n) || (!out_xy && n)) return FS_ERR_INVALID;
+  for (size_t i = 0; i < n; ++i)
+    inverse_map_point_f64(*pose, width, height, xy[2 * i], xy[2 * i + 1], &out_xy[2 * i], &out_xy[2 * i + 1]);
+  return FS_OK;
+}
+
+// Host evaluation of the kernels' no-wrap expand normaliser (for checks of
+// the closed form against the reference's sequential SKIPSM expand).
+float fs_exact_expand_divisor(int x, int y, int src_w, int src_h) { return exact_expand_divisor(x, y, src_w, src_h); }
+
+// ------------------------------------------------------------------- remap
+static int remap_impl(fs_ctx* ctx, const void* src, size_t src_stride, uint32_t width, uint32_t height,
+                      uint32_t channels, const fs_pose* pose, const fs_rect* roi, void* dst, size_t dst_stride,
+                      bool device) {
+  if (!ctx || !src || !dst || !pose) return set_err(ctx, FS_ERR_INVALID, "null argument");
+  if (channels != 1 && channels != 3) return set_err(ctx, FS_ERR_UNSUPPORTED, "remap supports 1 or 3 channels");
+  if (width == 0 || height == 0) return set_err(ctx, FS_ERR_INVALID, "empty frame");
+  fs_rect r = roi ? *roi : fs_rect{0, 0, (int32_t)width, (int32_t)height};
+  if (r.right <= r.left || r.bottom <= r.top) return set_err(ctx, FS_ERR_INVALID, "empty roi");
+  uint32_t ow = (uint32_t)(r.right - r.left), oh = (uint32_t)(r.bottom - r.top);
+  if (src_stride < (size_t)width * channels || dst_stride < (size_t)ow * (channels + 1))
+    return set_err(ctx, FS_ERR_INVALID, "row stride too small");
+  cudaSetDevice(ctx->device);
+  RemapArgs a;
+  std::memset(&a, 0, sizeof(a));
+  const char* why = nullptr;
+  if (!compose_warp(*pose, width, height, r, &a.f.warp, &why)) return set_err(ctx, FS_ERR_INVALID, why);
+  a.W = (int32_t)ow;
+  a.H = (int32_t)oh;
+  a.dst_ch = (int32_t)channels + 1;
+  a.f.src.w = (int32_t)width;
+  a.f.src.h = (int32_t)height;
+  a.f.src.ch = (int32_t)channels;
+  void *dsrc = nullptr, *ddst = nullptr;
+  size_t sbytes = src_stride * height, dbytes = dst_stride * oh;
+  if (device) {
+    dsrc = const_cast<void*>(src);
+    ddst = dst;
+  } else {
+    int rc = dev_alloc(ctx, sbytes, &dsrc);
+    if (rc != FS_OK) return rc;
+    rc = dev_alloc(ctx, dbytes, &ddst);
+    if (rc != FS_OK) {
+      dev_free(ctx, dsrc, sbytes);
+      return rc;
+    }
+    cudaMemcpyAsync(dsrc, src, sbytes, cudaMemcpyHostToDevice, ctx->stream);
+  }
+  a.f.src.px = (const uint8_t*)dsrc;
+  a.f.src.pitch = (int64_t)src_stride;
+  a.dst = (uint8_t*)ddst;
+  a.dst_pitch = (int64_t)dst_stride;
+  cudaError_t e = timed(ctx, "remap", [&] { return launch_remap(a, ctx->stream); });
+  if (e == cudaSuccess && !device) e = cudaMemcpyAsync(dst, ddst, dbytes, cudaMemcpyDeviceToHost, ctx->stream);
+  cudaError_t e2 = cudaStreamSynchronize(ctx->stream);
+  if (!device) {
+    dev_free(ctx, dsrc, sbytes);
+    dev_free(ctx, ddst, dbytes);
+  }
+  if (e != cudaSuccess) return cuda_err(ctx, e, "remap");
+  if (e2 != cudaSuccess) return cuda_err(ctx, e2, "remap");
+  return FS_OK;
+}
+
+int fs_remap_frame(fs_ctx* ctx, const void* src, size_t src_stride, uint32_t width, uint32_t height,
+                   uint32_t channels, const fs_pose* pose, const fs_rect* roi, void* dst, size_t dst_stride) {
+  return remap_impl(ctx, src, src_stride, width, height, channels, pose, roi, dst, dst_stride, false);
+}
+
+int fs_remap_frame_device(fs_ctx* ctx, const void* src, size_t src_stride, uint32_t width, uint32_t height,
+                          uint32_t channels, const fs_pose* pose, const fs_rect* roi, void* dst, size_t dst_stride) {
+  return remap_impl(ctx, src, src_stride, width, height, channels, pose, roi, dst, dst_stride, true);
+}
+
+// ------------------------------------------------------------------- stacks
+int fs_stack_begin(fs_ctx* ctx, const fs_stack_desc* desc, fs_stack** out) {
+  if (!ctx || !desc || !out) return set_err(ctx, FS_ERR_INVALID, "null argument");
+  *out = nullptr;
+  const fs_stack_desc& d = *desc;
+  if (d.sample_bits != 8) return set_err(ctx, FS_ERR_UNSUPPORTED, "only 8-bit samples are implemented");
+  if (d.src_width == 0 || d.src_height == 0 || d.frame_count == 0) return set_err(ctx, FS_ERR_INVALID, "empty stack");
+  if (d.contrast_window < 3 || (d.contrast_window & 1) == 0)
+    return set_err(ctx, FS_ERR_INVALID, "contrast window must be odd and >= 3");
+  if (d.contrast_window > 31) return set_err(ctx, FS_ERR_UNSUPPORTED, "contrast window larger than 31");
+  if (d.level_storage != FS_STORAGE_F32) return set_err(ctx, FS_ERR_UNSUPPORTED, "level storage other than FP32");
+  bool aligned = d.input_is_aligned != 0;
+  if (aligned ? (d.channels != 3 && d.channels != 4) : d.channels != 3)
+    return set_err(ctx, FS_ERR_INVALID, "channels must be 3 (RGB source) or 3/4 (aligned RGB/RGBA)");
+  fs_rect roi = d.has_roi ? d.roi : fs_rect{0, 0, (int32_t)d.src_width, (int32_t)d.src_height};
+  if (aligned) roi = fs_rect{0, 0, (int32_t)d.src_width, (int32_t)d.src_height};
+  if (roi.right <= roi.left || roi.bottom <= roi.top) return set_err(ctx, FS_ERR_INVALID, "empty roi");
+  cudaSetDevice(ctx->device);
+  fs_stack* s = new fs_stack();
+  s->ctx = ctx;
+  s->d = d;
+  s->roi = roi;
+  s->aligned = aligned;
+  s->W = (uint32_t)(roi.right - roi.left);
+  s->H = (uint32_t)(roi.bottom - roi.top);
+  s->L = level_count(s->W, s->H);
+  s->border = d.contrast_window / 2;
+  uint32_t k = d.frames_per_batch ? d.frames_per_batch : 8;
+  s->K = std::max(1u, std::min<uint32_t>(std::min<uint32_t>(k, (uint32_t)kMaxBatch), d.frame_count));
+  uint32_t w = s->W, h = s->H;
+  for (uint32_t l = 0; l < s->L; ++l) {
+    s->lw.push_back(w);
+    s->lh.push_back(h);
+    s->pitch.push_back(round_up(w, 32));
+    w = next_level_size(w);
+    h = next_level_size(h);
+  }
+  auto fail = [&](int rc) {
+    fs_stack_destroy(s);
+    return rc;
+  };
+  int rc;
+  void* p;
+  size_t n0 = (size_t)s->pitch[0] * s->H;
+  if ((rc = stack_alloc(s, n0 * 4, &p)) != FS_OK) return fail(rc);
+  s->norm = (float*)p;
+  if ((rc = stack_alloc(s, n0, &p)) != FS_OK) return fail(rc);
+  s->uni = (uint8_t*)p;
+  s->sm.push_back(s->uni);
+  for (uint32_t l = 1; l < s->L; ++l) {
+    if ((rc = stack_alloc(s, (size_t)s->pitch[l] * s->lh[l], &p)) != FS_OK) return fail(rc);
+    s->sm.push_back((uint8_t*)p);
+  }
+  for (uint32_t l = 0; l < s->L; ++l) {
+    if ((rc = stack_alloc(s, (size_t)s->pitch[l] * s->lh[l] * 3 * 4, &p)) != FS_OK) return fail(rc);
+    s->acc.push_back((float*)p);
+  }
+  s->slot.assign(s->K, std::vector<LevelPlanes>(s->L));
+  for (uint32_t kk = 0; kk < s->K; ++kk) {
+    for (uint32_t l = 1; l + 1 < s->L; ++l) {
+      size_t plane = (size_t)s->pitch[l] * s->lh[l];
+      LevelPlanes lp;
+      if ((rc = stack_alloc(s, plane * 4 * 4 + plane, &p)) != FS_OK) return fail(rc);
+      lp.g = (float*)p;
+      lp.m = lp.g + 3 * plane;
+      lp.s = (uint8_t*)(lp.m + plane);
+      lp.plane = (int64_t)plane;
+      s->slot[kk][l] = lp;
+    }
+  }
+  if ((rc = stack_alloc(s, (size_t)s->W * s->H * 3, &p)) != FS_OK) return fail(rc);
+  s->out_dev = (uint8_t*)p;
+  // frame residency: keep every frame on the device when the budget allows
+  s->frame_pitch = round_up((int64_t)d.src_width * d.channels, 16);
+  s->frame_bytes = (size_t)s->frame_pitch * d.src_height;
+  s->keep_frames = ctx->held + s->frame_bytes * d.frame_count <= ctx->budget;
+  cudaEventCreateWithFlags(&s->copy_done, cudaEventDisableTiming);
+  *out = s;
+  return FS_OK;
+}
+
+static int add_frame_impl(fs_stack* s, const void* pixels, size_t row_stride, const fs_pose* pose, bool device) {
+  if (!s || !pixels) return FS_ERR_INVALID;
+  fs_ctx* ctx = s->ctx;
+  if (s->finished) return set_err(ctx, FS_ERR_STATE, "stack already finished");
+  if (s->frames.size() >= s->d.frame_count) return set_err(ctx, FS_ERR_STATE, "more frames than frame_count");
+  if (!s->aligned && !pose) return set_err(ctx, FS_ERR_INVALID, "pose required for source frames");
+  size_t row_bytes = (size_t)s->d.src_width * s->d.channels;
+  if (row_stride < row_bytes) return set_err(ctx, FS_ERR_MISMATCH, "row stride smaller than the stack's row");
+  cudaSetDevice(ctx->device);
+  fs_stack::Frame fr;
+  if (pose) fr.pose = *pose; else fs_pose_default(&fr.pose);
+  if (device) {
+    fr.px = (const uint8_t*)pixels;
+    fr.pitch = (int64_t)row_stride;
+  } else {
+    // copy into a device buffer (kept for pass 2 when the budget allows)
+    bool keep = s->keep_frames;
+    uint8_t* buf = nullptr;
+    if (keep) {
+      void* p;
+      int rc = stack_alloc(s, s->frame_bytes, &p);
+      if (rc != FS_OK) return rc;
+      buf = (uint8_t*)p;
+      fr.owned = true;
+    } else {
+      // transient: reuse a staging slot of the current pass-1 batch
+      size_t slot = s->frames.size() % s->K;
+      while (s->staging.size() <= slot) {
+        void* p;
+        int rc = stack_alloc(s, s->frame_bytes, &p);
+        if (rc != FS_OK) return rc;
+        s->staging.push_back((uint8_t*)p);
+      }
+      if (slot == 0 && s->frames.size() > 0) {
+        // the previous batch must have consumed the slots
+        cudaError_t e = cudaStreamSynchronize(ctx->stream);
+        if (e != cudaSuccess) return cuda_err(ctx, e, "synchronize");
+      }
+      buf = s->staging[slot];
+      fr.resident = false;
+    }
+    cudaError_t e = cudaMemcpy2DAsync(buf, (size_t)s->frame_pitch, pixels, row_stride, row_bytes, s->d.src_height,
+                                      cudaMemcpyHostToDevice, ctx->copy);
+    if (e != cudaSuccess) return cuda_err(ctx, e, "frame upload");
+    cudaEventRecord(s->copy_done, ctx->copy);
+    cudaStreamWaitEvent(ctx->stream, s->copy_done, 0);
+    // the caller may reuse its buffer once this returns
+    e = cudaEventSynchronize(s->copy_done);
+    if (e != cudaSuccess) return cuda_err(ctx, e, "frame upload");
+    fr.px = buf;
+    fr.pitch = s->frame_pitch;
+  }
+  s->frames.push_back(fr);
+  return run_pending_pass1(s, s->frames.size() == s->d.frame_count);
+}
+
+int fs_stack_add_frame(fs_stack* stack, const void* pixels, size_t row_stride, const fs_pose* pose) {
+  return add_frame_impl(stack, pixels, row_stride, pose, false);
+}
+
+int fs_stack_add_frame_device(fs_stack* stack, const void* dev_pixels, size_t row_stride, const fs_pose* pose) {
+  return add_frame_impl(stack, dev_pixels, row_stride, pose, true);
+}
+
+static int finish_impl(fs_stack* s, fs_frame_fetch_cb refetch, void* user, void* out, size_t out_stride,
+                       bool device_out) {
+  if (!s || !out) return FS_ERR_INVALID;
+  fs_ctx* ctx = s->ctx;
+  if (s->finished) return set_err(ctx, FS_ERR_STATE, "stack already finished");
+  if (s->frames.size() != s->d.frame_count)
+    return set_err(ctx, FS_ERR_STATE, "fewer frames added than frame_count");
+  if (out_stride < (size_t)s->W * 3) return set_err(ctx, FS_ERR_INVALID, "output stride too small");
+  cudaSetDevice(ctx->device);
+  int rc = run_pending_pass1(s, true);
+  if (rc != FS_OK) return rc;
+  cudaStream_t st = ctx->stream;
+  cudaError_t e;
+  // mask-support pyramid (frame independent)
+  for (uint32_t l = 0; l + 1 < s->L; ++l) {
+    MaskSupportArgs m = {s->sm[l], (int32_t)s->lw[l], (int32_t)s->lh[l], s->pitch[l],
+                         s->sm[l + 1], (int32_t)s->lw[l + 1], (int32_t)s->lh[l + 1], s->pitch[l + 1]};
+    e = timed(ctx, "mask_support", [&] { return launch_mask_support(m, st); });
+    if (e != cudaSuccess) return cuda_err(ctx, e, "mask support");
+  }
+  for (uint32_t l = 0; l < s->L; ++l) {
+    e = cudaMemsetAsync(s->acc[l], 0, (size_t)s->pitch[l] * s->lh[l] * 3 * 4, st);
+    if (e != cudaSuccess) return cuda_err(ctx, e, "accumulator clear");
+  }
+  // pass 2 in batches of K frames
+  const size_t N = s->frames.size();
+  std::vector<fs_stack::Frame> batch_frames;
+  for (size_t begin = 0; begin < N; begin += s->K) {
+    size_t end = std::min(N, begin + s->K);
+    batch_frames.assign(s->frames.begin() + begin, s->frames.begin() + end);
+    for (size_t k = begin; k < end; ++k) {
+      fs_stack::Frame& fr = batch_frames[k - begin];
+      if (fr.resident) continue;
+      // the frame was only staged for pass 1: fetch it again from the host
+      // (the reference re-decodes, src/stack/pipeline.zig:561-597)
+      if (!refetch) return set_err(ctx, FS_ERR_STATE, "frame not resident and no refetch callback");
+      const void* hp = nullptr;
+      size_t hs = 0;
+      if (refetch(user, (uint32_t)k, &hp, &hs) != 0 || !hp) return set_err(ctx, FS_ERR_INVALID, "refetch callback failed");
+      if (hs < (size_t)s->d.src_width * s->d.channels) return set_err(ctx, FS_ERR_MISMATCH, "refetched row stride too small");
+      uint8_t* buf = s->staging[(k - begin) % s->staging.size()];
+      e = cudaMemcpy2DAsync(buf, (size_t)s->frame_pitch, hp, hs, (size_t)s->d.src_width * s->d.channels,
+                            s->d.src_height, cudaMemcpyHostToDevice, st);
+      if (e != cudaSuccess) return cuda_err(ctx, e, "frame refetch upload");
+      e = cudaStreamSynchronize(st);  // the callback's buffer may be reused after it returns again
+      if (e != cudaSuccess) return cuda_err(ctx, e, "frame refetch upload");
+      fr.px = buf;
+      fr.pitch = s->frame_pitch;
+    }
+    LevelArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.levels = (int32_t)s->L;
+    a.K = (int32_t)(end - begin);
+    a.border = (int32_t)s->border;
+    a.window_ok = (s->W >= s->d.contrast_window && s->H >= s->d.contrast_window) ? 1 : 0;
+    a.inv_count = 1.0f / (float)N;
+    a.norm = s->norm;
+    a.uni = s->uni;
+    for (size_t k = begin; k < end; ++k) {
+      std::string why;
+      if (!build_frame_in(s, batch_frames[k - begin], &a.f[k - begin], &why))
+        return set_err(ctx, FS_ERR_INVALID, why);
+    }
+    for (uint32_t l = 0; l + 1 < s->L || (s->L == 1 && l == 0); ++l) {
+      a.level = (int32_t)l;
+      a.wl = (int32_t)s->lw[l];
+      a.hl = (int32_t)s->lh[l];
+      a.pitch_l = s->pitch[l];
+      a.exact_expand = std::max(s->lw[l], s->lh[l]) <= kExactExpandMaxDim ? 1 : 0;
+      a.sm_l = s->sm[l];
+      a.acc_l = s->acc[l];
+      a.acc_plane_l = s->pitch[l] * s->lh[l];
+      if (l + 1 < s->L) {
+        a.wn = (int32_t)s->lw[l + 1];
+        a.hn = (int32_t)s->lh[l + 1];
+        a.pitch_n = s->pitch[l + 1];
+        a.sm_n = s->sm[l + 1];
+        a.acc_n = s->acc[l + 1];
+        a.acc_plane_n = s->pitch[l + 1] * s->lh[l + 1];
+      } else {
+        a.wn = a.hn = 1;
+        a.pitch_n = 32;
+      }
+      for (size_t k = 0; k < (size_t)a.K; ++k) {
+        if (l >= 1) a.in[k] = s->slot[k][l];
+        if (l + 1 < s->L - 1) a.out[k] = s->slot[k][l + 1];
+      }
+      if (l == 0) e = timed(ctx, "level0", [&] { return launch_level0(a, st); });
+      else e = timed(ctx, "level", [&] { return launch_level(a, st); });
+      if (e != cudaSuccess) return cuda_err(ctx, e, "level launch");
+      if (s->L == 1) break;
+    }
+  }
+  // collapse + quantise (src/fuse/pyramid.zig:223-269)
+  if (s->L == 1) {
+    e = timed(ctx, "collapse", [&] {
+      return launch_quantize(s->acc[0], s->pitch[0] * s->lh[0], s->pitch[0], (int)s->W, (int)s->H, s->out_dev,
+                             (int64_t)s->W * 3, s->base_out, s->base_pitch, st);
+    });
+    if (e != cudaSuccess) return cuda_err(ctx, e, "quantise");
+  }
+  for (uint32_t l = s->L - 1; l >= 1 && s->L > 1; --l) {
+    CollapseArgs c;
+    std::memset(&c, 0, sizeof(c));
+    c.wp = (int32_t)s->lw[l - 1];
+    c.hp = (int32_t)s->lh[l - 1];
+    c.wc = (int32_t)s->lw[l];
+    c.hc = (int32_t)s->lh[l];
+    c.pitch_p = s->pitch[l - 1];
+    c.pitch_c = s->pitch[l];
+    c.exact_expand = std::max(s->lw[l - 1], s->lh[l - 1]) <= kExactExpandMaxDim ? 1 : 0;
+    c.acc_p = s->acc[l - 1];
+    c.plane_p = s->pitch[l - 1] * s->lh[l - 1];
+    c.acc_c = s->acc[l];
+    c.plane_c = s->pitch[l] * s->lh[l];
+    c.out = l == 1 ? s->out_dev : nullptr;
+    c.out_pitch = (int64_t)s->W * 3;
+    c.base = l == 1 ? s->base_out : nullptr;
+    c.base_pitch = s->base_pitch;
+    e = timed(ctx, "collapse", [&] { return launch_collapse(c, st); });
+    if (e != cudaSuccess) return cuda_err(ctx, e, "collapse");
+  }
+  if (device_out) {
+    e = cudaMemcpy2DAsync(out, out_stride, s->out_dev, (size_t)s->W * 3, (size_t)s->W * 3, s->H,
+                          cudaMemcpyDeviceToDevice, st);
+  } else {
+    e = cudaMemcpy2DAsync(out, out_stride, s->out_dev, (size_t)s->W * 3, (size_t)s->W * 3, s->H,
+                          cudaMemcpyDeviceToHost, st);
+  }
+  if (e != cudaSuccess) return cuda_err(ctx, e, "output copy");
+  e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return cuda_err(ctx, e, "fusion");
+  s->finished = true;
+  return FS_OK;
+}
+
+int fs_stack_finish(fs_stack* stack, fs_frame_fetch_cb refetch, void* user, void* out_pixels, size_t out_stride) {
+  return finish_impl(stack, refetch, user, out_pixels, out_stride, false);
+}
+
+int fs_stack_finish_device(fs_stack* stack, fs_frame_fetch_cb refetch, void* user, void* dev_out, size_t out_stride) {
+  return finish_impl(stack, refetch, user, dev_out, out_stride, true);
+}
+
+int fs_stack_set_base_output(fs_stack* s, float* dev_base, size_t row_stride_elems) {
+  if (!s) return FS_ERR_INVALID;
+  if (dev_base && row_stride_elems < (size_t)s->W * 3) return set_err(s->ctx, FS_ERR_INVALID, "base stride too small");
+  s->base_out = dev_base;
+  s->base_pitch = (int64_t)row_stride_elems;
+  return FS_OK;
+}
+
+int fs_stack_output_size(const fs_stack* s, uint32_t* width, uint32_t* height) {
+  if (!s) return FS_ERR_INVALID;
+  if (width) *width = s->W;
+  if (height) *height = s->H;
+  return FS_OK;
+}
+
+int fs_stack_destroy(fs_stack* s) {
+  if (!s) return FS_ERR_INVALID;
+  fs_ctx* ctx = s->ctx;
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
+  cudaStreamSynchronize(ctx->copy);
+  for (auto& a : s->allocs) dev_free(ctx, a.p, a.bytes);
+  if (s->copy_done) cudaEventDestroy(s->copy_done);
+  delete s;
+  return FS_OK;
+}
+
+int fs_fuse_stack(fs_ctx* ctx, const fs_stack_desc* desc, const void* const* frames, const size_t* row_strides,
+                  const fs_pose* poses, void* out_pixels, size_t out_stride) {
+  if (!ctx || !desc || !frames || !row_strides || !out_pixels) return set_err(ctx, FS_ERR_INVALID, "null argument");
+  fs_stack* s = nullptr;
+  int rc = fs_stack_begin(ctx, desc, &s);
+  if (rc != FS_OK) return rc;
+  for (uint32_t k = 0; k < desc->frame_count && rc == FS_OK; ++k)
+    rc = fs_stack_add_frame(s, frames[k], row_strides[k], poses ? &poses[k] : nullptr);
+  if (rc == FS_OK) rc = fs_stack_finish(s, nullptr, nullptr, out_pixels, out_stride);
+  fs_stack_destroy(s);
+  return rc;
+}
+
+// ---------------------------------------------------------------- synthetic
+int fs_synth_pose(uint64_t seed, int scene, uint32_t width, uint32_t height, uint32_t frame, uint32_t frame_count,
+                  fs_pose* pose_out) {
+  if (!pose_out) return FS_ERR_INVALID;
+  synth_pose(seed, scene, width, height, frame, frame_count, pose_out);
+  return FS_OK;
+}
+
+int fs_synth_frame_device(fs_ctx* ctx, uint64_t seed, int scene, uint32_t width, uint32_t height, uint32_t frame,
+                          uint32_t frame_count, void* dev_out, size_t out_stride, fs_pose* pose_out) {
+  if (!ctx || !dev_out) return set_err(ctx, FS_ERR_INVALID, "null argument");
+  if (out_stride < (size_t)width * 3) return set_err(ctx, FS_ERR_INVALID, "stride too small");
+  cudaSetDevice(ctx->device);
+  const char* why = nullptr;
+  int rc = synth_render(seed, scene, width, height, frame, frame_count, dev_out, out_stride, pose_out, ctx->stream,
+                        &why);
+  if (rc != FS_OK) return set_err(ctx, rc, why ? why : "synthetic render failed");
+  cudaError_t e = cudaStreamSynchronize(ctx->stream);
+  if (e != cudaSuccess) return cuda_err(ctx, e, "synthetic render");
+  return FS_OK;
+}
+
+}  // extern "C"

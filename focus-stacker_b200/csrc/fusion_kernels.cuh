@@ -1,0 +1,140 @@
+// Kernel argument records and launchers of the fusion path.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/focuscuda.h"
+#include "fs_common.h"
+#include "remap_device.cuh"
+
+namespace fs {
+
+static constexpr int kMaxBatch = 8;   // frames per pass over per-pixel state (K)
+static constexpr int kTileW = 64;     // level-l tile (output pixels) of the level kernels
+static constexpr int kTileH = 32;
+static constexpr int kThreads = 256;
+
+// One input frame of a batch.
+struct FrameIn {
+  SrcImage src;   // source frame (remap) or aligned frame (RGBA / RGB)
+  Warp warp;      // kind WARP_ALIGNED for aligned input
+};
+
+// Planes of one pyramid level (FP32 planar RGB, u8 support, FP32 mask).
+struct LevelPlanes {
+  float* g;        // 3 planes: g + c * plane
+  uint8_t* s;      // image support (0/1)
+  float* m;        // normalised mask
+  int64_t plane;   // elements per colour plane (h * pitch)
+};
+
+struct Pass1Args {
+  int32_t W, H;          // ROI (level 0) size
+  int32_t border;        // contrast window / 2
+  int32_t window_ok;     // W >= window && H >= window
+  int32_t K;             // frames in this batch
+  int32_t first;         // 1: weight sums / union start at zero
+  float* norm;
+  int64_t norm_pitch;    // elements
+  uint8_t* uni;
+  int64_t uni_pitch;     // bytes
+  FrameIn f[kMaxBatch];
+};
+
+struct LevelArgs {
+  int32_t level;         // l: this launch reads level l, writes level l + 1
+  int32_t levels;        // L
+  int32_t wl, hl;        // level l size
+  int32_t wn, hn;        // level l + 1 size
+  int64_t pitch_l, pitch_n;   // elements per row (f32 planes); u8 planes use the same pitch in bytes
+  int32_t exact_expand;  // max(wl, hl) <= 512: no-wrap expand back to level l
+  int32_t K;
+  // level-0 only (frame input)
+  int32_t border, window_ok;
+  float inv_count;       // 1 / N (f32), the reference's default weight
+  const float* norm;
+  const uint8_t* uni;
+  FrameIn f[kMaxBatch];
+  // level >= 1 inputs (per frame in batch)
+  LevelPlanes in[kMaxBatch];
+  // outputs at level l + 1 (per frame in batch)
+  LevelPlanes out[kMaxBatch];
+  const uint8_t* sm_l;   // mask support at level l (union at level 0)
+  const uint8_t* sm_n;   // mask support at level l + 1
+  float* acc_l;          // accumulator level l, 3 planes
+  int64_t acc_plane_l;
+  float* acc_n;          // accumulator level l + 1 (used when l + 1 is the top level)
+  int64_t acc_plane_n;
+};
+
+struct CollapseArgs {
+  int32_t wp, hp, wc, hc;     // parent / child sizes
+  int64_t pitch_p, pitch_c;
+  int32_t exact_expand;       // max(wp, hp) <= 512
+  float* acc_p;               // parent accumulator (updated in place)
+  int64_t plane_p;
+  const float* acc_c;
+  int64_t plane_c;
+  uint8_t* out;               // final level: interleaved RGB u8 output, else null
+  int64_t out_pitch;
+  float* base;                // final level, optional: collapsed base before quantisation (RGB f32)
+  int64_t base_pitch;         // elements per row
+};
+
+struct MaskSupportArgs {
+  const uint8_t* src;
+  int32_t sw, sh;
+  int64_t spitch;
+  uint8_t* dst;
+  int32_t dw, dh;
+  int64_t dpitch;
+};
+
+struct RemapArgs {
+  FrameIn f;
+  int32_t W, H;       // output size
+  uint8_t* dst;
+  int64_t dst_pitch;
+  int32_t dst_ch;     // channels + 1
+};
+
+size_t pass1_smem_bytes(int border);
+size_t level0_smem_bytes(int border);
+size_t level_smem_bytes();
+
+cudaError_t launch_pass1(const Pass1Args& a, cudaStream_t s);
+cudaError_t launch_level0(const LevelArgs& a, cudaStream_t s);
+cudaError_t launch_level(const LevelArgs& a, cudaStream_t s);
+cudaError_t launch_collapse(const CollapseArgs& a, cudaStream_t s);
+cudaError_t launch_mask_support(const MaskSupportArgs& a, cudaStream_t s);
+cudaError_t launch_remap(const RemapArgs& a, cudaStream_t s);
+cudaError_t launch_quantize(const float* acc, int64_t plane, int64_t pitch, int w, int h, uint8_t* out,
+                            int64_t out_pitch, float* base, int64_t base_pitch, cudaStream_t s);
+
+// Synthetic stacks (synth.cu).
+void synth_pose(uint64_t seed, int scene, uint32_t width, uint32_t height, uint32_t frame, uint32_t frame_count,
+                fs_pose* p);
+int synth_render(uint64_t seed, int scene, uint32_t width, uint32_t height, uint32_t frame, uint32_t frame_count,
+                 void* dev_out, size_t out_stride, fs_pose* pose_out, cudaStream_t stream, const char** why);
+
+// Host evaluation of the no-wrap expand divisor (shared with the kernels).
+FS_HD float exact_expand_divisor(int x, int y, int sw, int sh) {
+  const int j = x >> 1, q = y >> 1;
+  const bool xe = (x & 1) == 0, ye = (y & 1) == 0;
+  if (sh == 1) {
+    if (sw == 1) return ye ? (xe ? 36.f : 24.f) : (xe ? 6.f : 4.f);
+    if (j < sw - 1) return ye ? (xe ? (j == 0 ? 42.f : 48.f) : 48.f) : (xe ? (j == 0 ? 7.f : 8.f) : 8.f);
+    return ye ? (xe ? 49.f : 28.f) : (xe ? 7.f : 4.f);
+  }
+  if (q < sh - 1) {
+    if (sw == 1 || j == sw - 1) return ye ? (xe ? (q == 0 ? 49.f : 56.f) : (q == 0 ? 28.f : 32.f)) : (xe ? 14.f : 8.f);
+    if (ye) return xe ? (q == 0 ? (j == 0 ? 49.f : 56.f) : (j == 0 ? 56.f : 64.f)) : (q == 0 ? 56.f : 64.f);
+    return xe ? (j == 0 ? 14.f : 16.f) : 16.f;
+  }
+  if (sw == 1) return ye ? (xe ? 42.f : 28.f) : (xe ? 6.f : 4.f);
+  if (j < sw - 1) return ye ? (xe ? (j == 0 ? 49.f : 56.f) : 56.f) : (xe ? (j == 0 ? 7.f : 8.f) : 8.f);
+  return ye ? (xe ? 49.f : 28.f) : (xe ? 7.f : 4.f);
+}
+
+}  // namespace fs

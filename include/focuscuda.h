@@ -1,0 +1,203 @@
+/*
+ * focuscuda.h - C ABI of libfocuscuda.so, the sm_100a (B200) implementation
+ * of the focus-stacker remap + pyramid-contrast fusion hot path.
+ *
+ * Plain C types only: pointers, sizes, PODs.  Every call returns an fs_status
+ * (0 = FS_OK); fs_last_error() gives a message for the last failure on a
+ * context.  Pixel buffers are interleaved, row-major, u8 (8-bit samples),
+ * with an explicit row stride in bytes.
+ *
+ * Each entry point names the reference (asingleoat/focus-stacker, Zig)
+ * interface it replaces; paths are relative to the reference project root.
+ */
+#ifndef FOCUSCUDA_H
+#define FOCUSCUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FS_API_VERSION 1
+
+typedef enum fs_status {
+  FS_OK = 0,
+  FS_ERR_INVALID = 1,     /* bad argument (size, window, null pointer, ...)  */
+  FS_ERR_OOM = 2,         /* device or pinned host allocation failed         */
+  FS_ERR_BUDGET = 3,      /* request exceeds the context's HBM budget        */
+  FS_ERR_CUDA = 4,        /* CUDA runtime error                              */
+  FS_ERR_TIMEOUT = 5,     /* a bounded device wait gave up                   */
+  FS_ERR_STATE = 6,       /* call out of order (e.g. frame after finish)     */
+  FS_ERR_MISMATCH = 7,    /* frame size / format differs from the stack's    */
+  FS_ERR_UNSUPPORTED = 8, /* valid but not implemented (e.g. 16-bit fusion)  */
+  FS_ERR_NO_DEVICE = 9    /* no CUDA device / library built for another arch */
+} fs_status;
+
+/* == ImagePose (src/optimize.zig:32-48), same field order and defaults
+ * (base_hfov_degrees = 50).  Angles in radians, hfov in degrees. */
+typedef struct fs_pose {
+  double yaw, pitch, roll, hfov_delta;
+  double trans_x, trans_y, trans_z;
+  double translation_plane_yaw, translation_plane_pitch;
+  double radial_a, radial_b, radial_c;
+  double center_shift_x, center_shift_y;
+  double base_hfov_degrees;
+} fs_pose;
+
+/* == remap.Rect (src/remap.zig:573-578): [left, right) x [top, bottom). */
+typedef struct fs_rect {
+  int32_t left, top, right, bottom;
+} fs_rect;
+
+typedef struct fs_ctx fs_ctx;
+typedef struct fs_stack fs_stack;
+
+/* Pyramid level storage for the precision forms. */
+typedef enum fs_level_storage { FS_STORAGE_F32 = 0, FS_STORAGE_F16 = 1, FS_STORAGE_BF16 = 2 } fs_level_storage;
+
+/* ---------------------------------------------------------------- context */
+
+/* Open a context on CUDA device `device`.  hbm_budget_bytes caps the device
+ * memory the context may hold (0 = half of the device's free memory, the
+ * analogue of --memory-fraction 0.5, src/memory_budget.zig:3-53). */
+int fs_create(int device, uint64_t hbm_budget_bytes, fs_ctx** out);
+void fs_destroy(fs_ctx* ctx);
+const char* fs_last_error(const fs_ctx* ctx);
+const char* fs_status_string(int status);
+int fs_api_version(void);
+/* Bytes of device memory the context currently holds. */
+uint64_t fs_ctx_device_bytes(const fs_ctx* ctx);
+/* Wait for all work queued on the context's stream. */
+int fs_ctx_synchronize(fs_ctx* ctx);
+/* Kernel accounting: number of kernels this context launched so far, and
+ * (when timing is enabled) per-kernel launch counts and device time measured
+ * with CUDA events on the launching stream.  Kernel names: "pass1",
+ * "level0", "level", "collapse", "mask_support", "remap".  Enabling or
+ * disabling timing clears the recorded times.  Not part of the reference. */
+uint64_t fs_ctx_launch_count(const fs_ctx* ctx);
+int fs_ctx_set_kernel_timing(fs_ctx* ctx, int enable);
+int fs_ctx_kernel_stats(fs_ctx* ctx, const char* kernel, uint64_t* launches, double* total_ms);
+
+/* ------------------------------------------------- host pose utilities */
+
+/* Fill *pose with ImagePose defaults (all zero, base_hfov_degrees = 50). */
+void fs_pose_default(fs_pose* pose);
+
+/* Common-overlap ROI of the active frames (FP64, host):
+ * replaces remap.computeCommonOverlapRoi, src/remap.zig:585-633.
+ * *has_roi = 0 when the frames share no overlap (the reference's null). */
+int fs_compute_roi(const fs_pose* poses, const uint32_t* widths, const uint32_t* heights, const uint8_t* active,
+                   size_t n, fs_rect* out, int* has_roi);
+
+/* Map n aligned-frame points (x, y pairs) to source-frame coordinates with
+ * the per-frame transform this library composes on the host in FP64 (the
+ * map the kernels evaluate): replaces optimize.inverseTransformPointCached,
+ * src/optimize.zig:3593-3616. */
+int fs_inverse_map_points(const fs_pose* pose, uint32_t width, uint32_t height, size_t n, const double* xy,
+                          double* out_xy);
+
+/* Normaliser of the no-wrap EXPAND at output (x, y) for a src_w x src_h
+ * source level, as the kernels evaluate it: the position-dependent divisors
+ * of expandRgbExactNoWrap, src/fuse/pyramid.zig:1167-1354 (host only). */
+float fs_exact_expand_divisor(int x, int y, int src_w, int src_h);
+
+/* ------------------------------------------------------------- remap only */
+
+/* Remap one frame through its pose into the ROI with a support-alpha
+ * channel: replaces remap.remapRigidImage, src/remap.zig:166-204 (u8).
+ * src: width x height x channels (1 or 3) samples; dst: roi-sized,
+ * (channels + 1) samples per pixel.  roi == NULL means the full frame.
+ * Host buffers; the call copies in and out and returns when done. */
+int fs_remap_frame(fs_ctx* ctx, const void* src, size_t src_stride, uint32_t width, uint32_t height,
+                   uint32_t channels, const fs_pose* pose, const fs_rect* roi, void* dst, size_t dst_stride);
+
+/* Same, with device pointers (src and dst already in device memory). */
+int fs_remap_frame_device(fs_ctx* ctx, const void* src, size_t src_stride, uint32_t width, uint32_t height,
+                          uint32_t channels, const fs_pose* pose, const fs_rect* roi, void* dst, size_t dst_stride);
+
+/* ------------------------------------------------------- fusion (stacks) */
+
+typedef struct fs_stack_desc {
+  uint32_t src_width, src_height; /* input frame size                                 */
+  int32_t has_roi;                /* 0: output = full frame; 1: output = roi          */
+  fs_rect roi;                    /* output region in aligned-frame coordinates       */
+  uint32_t channels;              /* 3 = RGB source frames; aligned input: 3 or 4     */
+  uint32_t sample_bits;           /* 8                                                */
+  uint32_t frame_count;           /* active frames that will be added (N)             */
+  uint32_t contrast_window;       /* odd >= 3, default 5 (--contrast-window-size)     */
+  int32_t input_is_aligned;       /* 1: frames are pre-aligned (focus_fuse_zig path)  */
+  int32_t level_storage;          /* fs_level_storage                                 */
+  uint32_t frames_per_batch;      /* K frames per pass over per-pixel state; 0 = auto */
+} fs_stack_desc;
+
+/* Start a pyramid-contrast fusion of frame_count frames (device state:
+ * weight sums, union support, FP32 accumulator pyramid).  Replaces the
+ * pass-1 set-up of stack/pipeline.zig:412-459 / fuse/pipeline.zig:292-321. */
+int fs_stack_begin(fs_ctx* ctx, const fs_stack_desc* desc, fs_stack** out);
+
+/* Pass 1 for the next active frame, in the reference's frame order: remap
+ * (unless aligned) -> local-contrast weight -> alpha -> weight sum and
+ * union support.  Replaces the body of src/stack/pipeline.zig:412-477
+ * (src/fuse/pipeline.zig:292-334 for aligned input).  `pixels` is a host
+ * buffer copied before the call returns; `pose` is ignored for aligned input. */
+int fs_stack_add_frame(fs_stack* stack, const void* pixels, size_t row_stride, const fs_pose* pose);
+
+/* Same with a device pointer; the buffer must stay valid and unchanged until
+ * fs_stack_finish returns (pass 2 reads it again). */
+int fs_stack_add_frame_device(fs_stack* stack, const void* dev_pixels, size_t row_stride, const fs_pose* pose);
+
+/* Pass-2 source for frames the stack could not keep in device memory: set
+ * *pixels / *row_stride to host memory holding frame `frame_index` again
+ * (the reference re-decodes, src/stack/pipeline.zig:561-597).  Return 0 on
+ * success. */
+typedef int (*fs_frame_fetch_cb)(void* user, uint32_t frame_index, const void** pixels, size_t* row_stride);
+
+/* Pass 2 (normalise, mask + Laplacian pyramids, weighted blend) and the
+ * collapse + quantise, writing interleaved RGB u8 to host memory.  Replaces
+ * runPyramidStackFusion's pass 2 plus pyramid.collapseToImageWithJobsAndDebug
+ * (src/stack/pipeline.zig:515-597, src/fuse/pyramid.zig:223-269). */
+int fs_stack_finish(fs_stack* stack, fs_frame_fetch_cb refetch, void* user, void* out_pixels, size_t out_stride);
+
+/* Same with a device output buffer. */
+int fs_stack_finish_device(fs_stack* stack, fs_frame_fetch_cb refetch, void* user, void* dev_out, size_t out_stride);
+
+/* Optional: also write the collapsed level-0 base before quantisation
+ * (interleaved RGB FP32, device memory, row stride in elements) during
+ * finish.  Used to measure error against FP64 evaluations on the 16-bit
+ * grid.  Not part of the reference. */
+int fs_stack_set_base_output(fs_stack* stack, float* dev_base, size_t row_stride_elems);
+
+/* Output size of the stack (the ROI). */
+int fs_stack_output_size(const fs_stack* stack, uint32_t* width, uint32_t* height);
+
+int fs_stack_destroy(fs_stack* stack);
+
+/* One-shot form over host frames already in memory: begin, add every frame
+ * in order, finish.  Replaces runCollapsedPyramidStackPass
+ * (src/stack/pipeline.zig:314-359) / runCollapsedPyramidPass
+ * (src/fuse/pipeline.zig:148-180). */
+int fs_fuse_stack(fs_ctx* ctx, const fs_stack_desc* desc, const void* const* frames, const size_t* row_strides,
+                  const fs_pose* poses, void* out_pixels, size_t out_stride);
+
+/* ------------------------------------------------------ synthetic input */
+
+/* Render frame k of a synthetic focus stack (seeded; see the generator in
+ * the library source) directly into device memory as interleaved RGB u8,
+ * and return the pose that realigns it.  scene: 0 = small (blur <= 3 px,
+ * shifts +-20 px, roll +-0.2 deg), 1 = production (blur <= 8 px, shifts +-60
+ * px, roll +-0.3 deg).  Not part of the reference; used by tests and the
+ * benchmark. */
+int fs_synth_frame_device(fs_ctx* ctx, uint64_t seed, int scene, uint32_t width, uint32_t height, uint32_t frame,
+                          uint32_t frame_count, void* dev_out, size_t out_stride, fs_pose* pose_out);
+
+/* Pose of synthetic frame k (host only). */
+int fs_synth_pose(uint64_t seed, int scene, uint32_t width, uint32_t height, uint32_t frame, uint32_t frame_count,
+                  fs_pose* pose_out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FOCUSCUDA_H */

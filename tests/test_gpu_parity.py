@@ -1,0 +1,290 @@
+"""GPU parity: libfocuscuda (through its C ABI) against the CPU oracle.
+
+Bar: remap alpha bit-exact everywhere and RGB bit-exact wherever alpha > 0;
+fused output within 1 LSB of the 16-bit grid (|base_gpu - base_oracle| <=
+1/257 in 8-bit units) of the oracle's FP32 evaluation, and u8 output within
+1 LSB.
+
+RGB of alpha-0 pixels: a sample that lands within ~1e-13 px of the integer
+one pixel outside the frame (identity-like poses put it exactly there) gets
+RGB = the edge pixel when the reference's rounding residue is positive and 0
+when it is negative (src/remap.zig:736-752), with alpha 0 either way.  That
+residue comes from the last bit of the reference's trig chain, so those
+invisible samples are compared separately and only bounded in count.
+"""
+import math
+
+import numpy as np
+import pytest
+
+import oracle
+from __graft_entry__ import load_package
+
+fsb = load_package()
+pytestmark = pytest.mark.gpu
+
+LSB16 = 1.0 / 257.0
+
+
+@pytest.fixture(scope="module")
+def torch():
+    t = pytest.importorskip("torch")
+    if not t.cuda.is_available():
+        pytest.skip("no CUDA device")
+    return t
+
+
+@pytest.fixture(scope="module")
+def ctx(torch):
+    c = fsb.Context(0)
+    yield c
+    c.close()
+
+
+def synth_stack(torch, ctx, W, H, F, seed, scene=fsb.SCENE_SMALL):
+    frames, poses = [], []
+    for k in range(F):
+        buf = torch.empty((H, W, 3), dtype=torch.uint8, device="cuda:0")
+        poses.append(fsb.synth_frame_device(ctx, seed, scene, W, H, k, F, buf, W * 3))
+        frames.append(buf.cpu().numpy())
+    return frames, poses
+
+
+def gpu_fuse(ctx, torch, frames, poses, roi, window=5, k=0, aligned=False):
+    h, w = frames[0].shape[:2]
+    c = frames[0].shape[2]
+    st = fsb.PyramidContrastStack(ctx, w, h, len(frames), roi=None if aligned else roi, channels=c,
+                                  contrast_window=window, aligned=aligned, frames_per_batch=k)
+    base = torch.zeros((st.out_height, st.out_width, 3), dtype=torch.float32, device="cuda:0")
+    st.set_base_output(base, st.out_width * 3)
+    for f, p in zip(frames, poses):
+        st.add_frame(f, p)
+    out = st.finish()
+    st.close()
+    return out, base.cpu().numpy().astype(np.float64)
+
+
+def with_kind(pose, kind, rng):
+    p = fsb.ImagePose(**pose.as_dict())
+    if kind == "lens":
+        p.radial_a, p.radial_b, p.radial_c = rng.uniform(-0.01, 0.01, 3)
+        p.center_shift_x, p.center_shift_y = rng.uniform(-2, 2, 2)
+    elif kind == "shift":
+        p.center_shift_x, p.center_shift_y = rng.uniform(-2, 2, 2)
+    elif kind == "trans":
+        p.trans_x, p.trans_y, p.trans_z = rng.uniform(-2, 2), rng.uniform(-2, 2), rng.uniform(-0.01, 0.01)
+        p.translation_plane_yaw, p.translation_plane_pitch = rng.uniform(-0.01, 0.01, 2)
+    return p
+
+
+# ------------------------------------------------------------------ remap
+def test_identity_remap_preserves_interior_grayscale_pixels(ctx):
+    # src/remap.zig:1018-1057 through the GPU
+    src = np.arange(1, 26, dtype=np.uint8).reshape(5, 5)
+    out = fsb.remap_rigid_image(ctx, src, fsb.ImagePose())
+    assert out.shape == (5, 5, 2)
+    assert (out[2, 2, 0], out[2, 2, 1]) == (13, 255)
+    assert (out[3, 2, 0], out[3, 2, 1]) == (18, 255)
+    assert (out[2, 3, 0], out[2, 3, 1]) == (14, 255)
+    assert np.array_equal(out, oracle.remap(src, {}, None))
+
+
+def assert_remap_equal(got, ref, max_alpha0_rgb=None):
+    assert got.shape == ref.shape
+    ch = got.shape[2] - 1
+    assert np.array_equal(got[..., ch], ref[..., ch]), int((got[..., ch] != ref[..., ch]).sum())
+    vis = ref[..., ch] > 0
+    assert np.array_equal(got[vis], ref[vis]), int((got[vis] != ref[vis]).any(-1).sum())
+    hidden = int((got[~vis] != ref[~vis]).any(-1).sum())
+    if max_alpha0_rgb is not None:
+        assert hidden <= max_alpha0_rgb, hidden
+    return hidden
+
+
+def _full(band, rows, h):
+    full = np.zeros((h,) + band.shape[1:], band.dtype)
+    full[rows[0]:rows[1]] = band
+    return full
+
+
+def test_identity_remap_matches_reference_golden_tiff(ctx, golden):
+    h, w = int(golden["height"]), int(golden["width"])
+    rows = golden["ident_rows"]
+    src = _full(golden["ident_src"], rows, h)
+    out = fsb.remap_rigid_image(ctx, src, fsb.ImagePose(), fsb.Rect(0, int(rows[0]), w, int(rows[1])))
+    assert np.array_equal(out, golden["ident_golden"])
+
+
+def test_pair_pose_remap_matches_oracle_and_golden(ctx, golden):
+    h, w = int(golden["height"]), int(golden["width"])
+    yaw, pitch, roll, dv, base = golden["pose_values"]
+    pose = fsb.ImagePose(yaw=yaw, pitch=pitch, roll=roll, hfov_delta=dv, base_hfov_degrees=base)
+    src = _full(golden["pose_src"], golden["pose_src_rows"], h)
+    r0, r1 = (int(v) for v in golden["pose_out_rows"])
+    out = fsb.remap_rigid_image(ctx, src, pose, fsb.Rect(0, r0, w, r1))
+    assert np.array_equal(out, oracle.remap(src, pose.as_dict(), (0, r0, w, r1)))
+    ref = golden["pose_golden"]
+    m = (out[..., 3] == 255) & (ref[..., 3] == 255)
+    d = (out[..., :3].astype(np.float64) - ref[..., :3])[m]
+    assert math.sqrt((d ** 2).mean()) / 255.0 <= 0.005
+
+
+@pytest.mark.parametrize("kind", ["basic", "shift", "lens", "trans"])
+@pytest.mark.parametrize("size", [(320, 240), (97, 61)])
+def test_remap_bit_exact(torch, ctx, kind, size):
+    W, H = size
+    frames, poses = synth_stack(torch, ctx, W, H, 4, seed=11)
+    rng = np.random.default_rng(5)
+    for k in range(4):
+        pose = with_kind(poses[k], kind, rng)
+        for roi in (None, fsb.Rect(3, 2, W - 5, H - 1), fsb.Rect(-4, -3, W + 6, H + 2)):
+            got = fsb.remap_rigid_image(ctx, frames[k], pose, roi)
+            ref = oracle.remap(frames[k], pose.as_dict(), roi.as_tuple() if roi else None)
+            # alpha-0 RGB can differ only on the one-pixel ring just outside the frame
+            assert_remap_equal(got, ref, max_alpha0_rgb=2 * (W + H) + 8)
+
+
+def test_remap_bit_exact_production_frame(torch, ctx):
+    # a full 7952x5304 frame of the production scene (shifts up to 60 px, roll 0.3 deg)
+    W, H = 7952, 5304
+    buf = torch.empty((H, W, 3), dtype=torch.uint8, device="cuda:0")
+    pose = fsb.synth_frame_device(ctx, 3, fsb.SCENE_PRODUCTION, W, H, 5, 30, buf, W * 3)
+    src = buf.cpu().numpy()
+    roi = fsb.Rect(61, 57, W - 64, H - 70)
+    got = fsb.remap_rigid_image(ctx, src, pose, roi)
+    ref = oracle.remap(src, pose.as_dict(), roi.as_tuple(), jobs=8)
+    assert np.array_equal(got, ref), int((got != ref).any(-1).sum())
+    gray = np.ascontiguousarray(src[..., 1])
+    groi = fsb.Rect(-30, -20, W + 25, H + 40)
+    g = fsb.remap_rigid_image(ctx, gray, pose, groi)
+    assert_remap_equal(g, oracle.remap(gray, pose.as_dict(), groi.as_tuple(), jobs=8), max_alpha0_rgb=0)
+
+
+# ----------------------------------------------------------------- fusion
+def check_fused(out, base, ref_out, ref_base):
+    d = np.abs(base - ref_base)
+    assert d.max() <= LSB16, f"max |base diff| = {d.max()} > 1/257"
+    du = np.abs(out.astype(np.int32) - ref_out.astype(np.int32))
+    assert du.max() <= 1
+
+
+@pytest.mark.parametrize("W,H,F,window", [
+    (320, 240, 4, 5), (513, 511, 3, 5), (64, 48, 3, 3), (200, 150, 5, 7), (130, 70, 9, 5),
+    (7, 5, 2, 3), (2, 3, 2, 3), (1, 1, 2, 3), (4, 9, 3, 5),
+])
+def test_stack_fusion_matches_oracle(torch, ctx, W, H, F, window):
+    frames, poses = synth_stack(torch, ctx, W, H, F, seed=W * 100 + H)
+    roi = fsb.compute_common_overlap_roi([True] * F, [W] * F, [H] * F, poses) or fsb.Rect(0, 0, W, H)
+    out, base = gpu_fuse(ctx, torch, frames, poses, roi, window)
+    ref_out, ref_base = oracle.stack_fuse(frames, [p.as_dict() for p in poses], roi.as_tuple(), window=window,
+                                          want_base=True)
+    check_fused(out, base, ref_out, ref_base)
+
+
+def test_config0_stack_matches_oracle(torch, ctx):
+    # 8 RGB frames of 1024x768, small scene, default levels, FP32
+    W, H, F = 1024, 768, 8
+    frames, poses = synth_stack(torch, ctx, W, H, F, seed=0)
+    roi = fsb.compute_common_overlap_roi([True] * F, [W] * F, [H] * F, poses)
+    assert roi is not None and roi.as_tuple() == oracle.compute_roi([p.as_dict() for p in poses], [W] * F, [H] * F)
+    out, base = gpu_fuse(ctx, torch, frames, poses, roi)
+    ref_out, ref_base = oracle.stack_fuse(frames, [p.as_dict() for p in poses], roi.as_tuple(), jobs=8,
+                                          want_base=True)
+    check_fused(out, base, ref_out, ref_base)
+    _, ref64 = oracle.stack_fuse(frames, [p.as_dict() for p in poses], roi.as_tuple(), jobs=8, precision=64,
+                                 want_base=True)
+    assert np.abs(base - ref64).max() <= LSB16
+
+
+@pytest.mark.parametrize("channels", [3, 4])
+def test_aligned_fusion_matches_oracle(torch, ctx, channels):
+    W, H, F = 256, 192, 5
+    frames, poses = synth_stack(torch, ctx, W, H, F, seed=21)
+    roi = fsb.compute_common_overlap_roi([True] * F, [W] * F, [H] * F, poses)
+    aligned = [oracle.remap(f, p.as_dict(), roi.as_tuple()) for f, p in zip(frames, poses)]
+    if channels == 3:
+        aligned = [np.ascontiguousarray(a[..., :3]) for a in aligned]
+    out, base = gpu_fuse(ctx, torch, aligned, [None] * F, None, aligned=True)
+    ref_out, ref_base = oracle.fuse_aligned(aligned, want_base=True)
+    check_fused(out, base, ref_out, ref_base)
+
+
+def test_batch_size_does_not_change_results(torch, ctx):
+    W, H, F = 300, 200, 7
+    frames, poses = synth_stack(torch, ctx, W, H, F, seed=4)
+    roi = fsb.compute_common_overlap_roi([True] * F, [W] * F, [H] * F, poses)
+    outs = [gpu_fuse(ctx, torch, frames, poses, roi, k=k) for k in (1, 3, 8)]
+    for o, b in outs[1:]:
+        assert np.array_equal(o, outs[0][0])
+        assert np.array_equal(b, outs[0][1])
+
+
+def test_identical_frames_fuse_to_the_frame(torch, ctx):
+    # size-independent property: with identity poses, fusing copies of one
+    # frame reconstructs it (masks sum to one on every level)
+    W, H = 7952, 5304
+    buf = torch.empty((H, W, 3), dtype=torch.uint8, device="cuda:0")
+    fsb.synth_frame_device(ctx, 1, fsb.SCENE_PRODUCTION, W, H, 0, 30, buf, W * 3)
+    st = fsb.PyramidContrastStack(ctx, W, H, 3, roi=None, frames_per_batch=3)
+    for _ in range(3):
+        st.add_frame_device(buf, W * 3, fsb.ImagePose())
+    out = torch.empty((H, W, 3), dtype=torch.uint8, device="cuda:0")
+    st.finish_device(out, W * 3)
+    st.close()
+    d = (out.int() - buf.int()).abs()
+    assert int(d.max()) <= 1
+    assert float((d > 0).float().mean()) < 1e-4
+
+
+def test_refetch_path_matches_resident(torch, ctx):
+    W, H, F = 200, 120, 5
+    frames, poses = synth_stack(torch, ctx, W, H, F, seed=8)
+    roi = fsb.compute_common_overlap_roi([True] * F, [W] * F, [H] * F, poses)
+    ref, _ = gpu_fuse(ctx, torch, frames, poses, roi, k=2)
+    # a budget that fits the stack state but not every frame copy
+    probe = fsb.PyramidContrastStack(ctx, W, H, F, roi=roi, frames_per_batch=2)
+    state = ctx.device_bytes()
+    probe.close()
+    small = fsb.Context(0, hbm_budget_bytes=state + 3 * W * H * 3 + 4096)
+    st = fsb.PyramidContrastStack(small, W, H, F, roi=roi, frames_per_batch=2)
+    for f, p in zip(frames, poses):
+        st.add_frame(f, p)
+    calls = []
+
+    def refetch(i):
+        calls.append(i)
+        return frames[i]
+
+    out = st.finish(refetch=refetch)
+    st.close()
+    small.close()
+    assert calls == list(range(F))
+    assert np.array_equal(out, ref)
+
+
+def test_stack_errors(torch, ctx):
+    W, H = 64, 48
+    frames, poses = synth_stack(torch, ctx, W, H, 2, seed=2)
+    with pytest.raises(fsb.FocusCudaError) as e:
+        fsb.PyramidContrastStack(ctx, W, H, 2, contrast_window=4)
+    assert e.value.code == "FS_ERR_INVALID"
+    st = fsb.PyramidContrastStack(ctx, W, H, 2)
+    st.add_frame(frames[0], poses[0])
+    with pytest.raises(fsb.FocusCudaError) as e:
+        st.finish()
+    assert e.value.code == "FS_ERR_STATE"
+    with pytest.raises(fsb.FocusCudaError) as e:
+        st.add_frame(frames[1][:, :W // 2].copy(), poses[1])
+    assert e.value.code == "FS_ERR_MISMATCH"
+    st.add_frame(frames[1], poses[1])
+    with pytest.raises(fsb.FocusCudaError) as e:
+        st.add_frame(frames[1], poses[1])
+    assert e.value.code == "FS_ERR_STATE"
+    st.finish()
+    with pytest.raises(fsb.FocusCudaError) as e:
+        st.finish()
+    assert e.value.code == "FS_ERR_STATE"
+    st.close()
+    with pytest.raises(fsb.FocusCudaError) as e:
+        fsb.PyramidContrastStack(fsb.Context(0, hbm_budget_bytes=1024), 640, 480, 2)
+    assert e.value.code == "FS_ERR_BUDGET"

@@ -1,0 +1,184 @@
+"""CPU tests of the library's host logic and closed forms (no GPU needed)."""
+import math
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+from __graft_entry__ import load_package
+
+fsb = load_package()
+
+
+def test_library_exports_every_declared_symbol():
+    import re
+    hdr = open(os.path.join(os.path.dirname(__file__), "..", "include", "focuscuda.h")).read()
+    declared = set(re.findall(r"\b(fs_[a-z0-9_]+)\s*\(", hdr)) - {"fs_frame_fetch_cb"}
+    assert declared == set(fsb._lib.EXPORTED)
+    L = fsb._lib.lib()
+    for name in declared:
+        assert getattr(L, name) is not None
+
+
+def test_status_strings_and_version():
+    L = fsb._lib.lib()
+    assert L.fs_api_version() == 1
+    assert L.fs_status_string(0) == b"ok"
+    assert L.fs_status_string(3) == b"device memory budget exceeded"
+
+
+def test_context_without_gpu_reports_no_device():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    with pytest.raises(fsb.FocusCudaError) as e:
+        fsb.Context(0)
+    assert e.value.code == "FS_ERR_NO_DEVICE"
+
+
+def test_parse_method_and_window():
+    assert fsb.parse_method("cuda-pyramid-contrast") is fsb.Method.CUDA_PYRAMID_CONTRAST
+    assert fsb.parse_method("pyramid-contrast") is fsb.Method.PYRAMID_CONTRAST
+    with pytest.raises(ValueError):
+        fsb.parse_method("pyramid")
+    assert fsb.parse_window_size("7") == 7
+    for bad in ("4", "1", "0", "x"):
+        with pytest.raises(ValueError):
+            fsb.parse_window_size(bad)
+
+
+def _random_poses(rng, n, w, kinds=("basic",)):
+    poses = []
+    f = (w / 2) / math.tan(math.radians(25))
+    for i in range(n):
+        kind = kinds[i % len(kinds)]
+        p = fsb.ImagePose(yaw=math.atan(rng.uniform(-60, 60) / f), pitch=math.atan(rng.uniform(-60, 60) / f),
+                          roll=math.radians(rng.uniform(-0.3, 0.3)), hfov_delta=rng.uniform(-0.2, 0.2))
+        if kind == "lens":
+            p.radial_a, p.radial_b, p.radial_c = rng.uniform(-0.02, 0.02, 3)
+            p.center_shift_x, p.center_shift_y = rng.uniform(-3, 3, 2)
+        if kind == "shift":
+            p.center_shift_x, p.center_shift_y = rng.uniform(-3, 3, 2)
+        if kind == "trans":
+            p.trans_x, p.trans_y, p.trans_z = rng.uniform(-3, 3), rng.uniform(-3, 3), rng.uniform(-0.02, 0.02)
+            p.translation_plane_yaw, p.translation_plane_pitch = rng.uniform(-0.02, 0.02, 2)
+        poses.append(p)
+    return poses
+
+
+@pytest.mark.parametrize("size", [(10, 8), (768, 512), (1024, 768), (7952, 5304), (641, 479)])
+def test_roi_matches_oracle(size):
+    w, h = size
+    rng = np.random.default_rng(w * 7 + h)
+    for trial in range(20):
+        n = int(rng.integers(1, 6))
+        poses = _random_poses(rng, n, w, ("basic", "lens", "trans", "shift"))
+        if trial % 3 == 0:
+            poses[0] = fsb.ImagePose()
+        active = [bool(v) for v in rng.integers(0, 2, n)] if trial % 4 == 1 else [True] * n
+        got = fsb.compute_common_overlap_roi(active, [w] * n, [h] * n, poses)
+        ref = oracle.compute_roi([p.as_dict() for p in poses], [w] * n, [h] * n, active)
+        assert (got.as_tuple() if got else None) == ref
+
+
+def test_identity_roi_residues_match_reference_chain():
+    # the reference's forward chain leaves +-1e-13 residues at identity
+    # corners that ceil/floor turn into a one-row ROI change
+    for w, h in [(768, 512), (1024, 768), (7952, 5304), (10, 8)]:
+        got = fsb.compute_common_overlap_roi([True], [w], [h], [fsb.ImagePose()])
+        assert got.as_tuple() == oracle.compute_roi([{}], [w], [h])
+
+
+@pytest.mark.parametrize("kind", ["basic", "lens", "shift", "trans"])
+def test_composed_map_matches_reference_inverse_chain(kind):
+    w, h = 1024, 768
+    rng = np.random.default_rng({"basic": 1, "lens": 2, "shift": 3, "trans": 4}[kind])
+    poses = _random_poses(rng, 6, w, (kind,))
+    pts = np.stack([rng.uniform(-20, w + 20, 400), rng.uniform(-20, h + 20, 400)], 1)
+    worst = 0.0
+    for p in poses:
+        got = fsb.inverse_map_points(p, w, h, pts)
+        for (x, y), (gx, gy) in zip(pts, got):
+            rx, ry = oracle.inverse_point(p.as_dict(), w, h, x, y)
+            worst = max(worst, abs(gx - rx), abs(gy - ry))
+    assert worst < 1e-8, worst
+
+
+def test_composed_map_large_frame_and_angles():
+    w, h = 7952, 5304
+    rng = np.random.default_rng(9)
+    pts = np.stack([rng.uniform(0, w, 300), rng.uniform(0, h, 300)], 1)
+    for yaw_deg in (0.0, 0.4, 3.0, 15.0):
+        p = fsb.ImagePose(yaw=math.radians(yaw_deg), pitch=math.radians(-yaw_deg / 2), roll=math.radians(0.3),
+                          hfov_delta=0.1)
+        got = fsb.inverse_map_points(p, w, h, pts)
+        ref = np.array([oracle.inverse_point(p.as_dict(), w, h, x, y) for x, y in pts])
+        assert np.abs(got - ref).max() < 1e-7
+
+
+# ---- closed forms of the EXPAND used by the kernels, evaluated in numpy f32
+def _expand_closed_form(src, dw, dh):
+    """Per-output-pixel restatement of the kernels' expand (both modes)."""
+    sh, sw = src.shape[:2]
+    f32 = np.float32
+    exact = max(dw, dh) <= 512
+    out = np.zeros((dh, dw, 3), np.float32)
+
+    def s(j, r):
+        if exact:
+            if j < 0 or j >= sw or r < 0 or r >= sh:
+                return np.zeros(3, np.float32)
+            return src[r, j]
+        return src[min(max(r, 0), sh - 1), min(max(j, 0), sw - 1)]
+
+    def hval(x, r):
+        j = x >> 1
+        if exact:
+            if x % 2 == 0:
+                return (s(j - 1, r) + f32(6) * s(j, r)) + s(j + 1, r)
+            return f32(4) * (s(j, r) + s(j + 1, r))
+        if x % 2 == 0:
+            return ((s(j - 1, r) + f32(6) * s(j, r)) + s(j + 1, r)) * f32(0.125)
+        return (s(j, r) + s(j + 1, r)) * f32(0.5)
+
+    for y in range(dh):
+        q = y >> 1
+        for x in range(dw):
+            if exact:
+                if y % 2 == 0:
+                    v = (hval(x, q - 1) + f32(6) * hval(x, q)) + hval(x, q + 1)
+                else:
+                    v = hval(x, q) + hval(x, q + 1)
+                v = v / f32(fsb.exact_expand_divisor(x, y, sw, sh))
+            else:
+                cq = lambda r: min(max(r, 0), sh - 1)
+                if y % 2 == 0:
+                    v = ((hval(x, cq(q - 1)) + f32(6) * hval(x, cq(q))) + hval(x, cq(q + 1))) * f32(0.125)
+                else:
+                    r0 = hval(x, cq(q))
+                    v = (r0 + r0) * f32(0.5)
+            out[y, x] = v
+    return out
+
+
+@pytest.mark.parametrize("sw,sh", [(1, 1), (1, 3), (3, 1), (2, 2), (2, 5), (5, 2), (4, 4), (7, 5), (6, 9)])
+def test_exact_expand_closed_form_is_bitwise_the_reference_skipsm(sw, sh):
+    rng = np.random.default_rng(sw * 31 + sh)
+    src = rng.uniform(-50, 300, (sh, sw, 3)).astype(np.float32)
+    for dw in (2 * sw - 1, 2 * sw):
+        for dh in (2 * sh - 1, 2 * sh):
+            if dw < 1 or dh < 1:
+                continue
+            ref = oracle.expand_rgb(src, dw, dh)
+            got = _expand_closed_form(src, dw, dh)
+            assert np.array_equal(got.view(np.uint32), ref.view(np.uint32)), (dw, dh)
+
+
+@pytest.mark.parametrize("sw,sh,dw,dh", [(257, 3, 513, 5), (260, 4, 519, 8), (3, 300, 6, 599)])
+def test_clamped_expand_closed_form_is_bitwise_the_reference(sw, sh, dw, dh):
+    rng = np.random.default_rng(sw + sh)
+    src = rng.uniform(-50, 300, (sh, sw, 3)).astype(np.float32)
+    ref = oracle.expand_rgb(src, dw, dh)
+    got = _expand_closed_form(src, dw, dh)
+    assert np.array_equal(got.view(np.uint32), ref.view(np.uint32))
