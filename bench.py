@@ -1,0 +1,415 @@
+#!/usr/bin/env python
+"""Benchmark of the remap + pyramid-contrast fusion path (libfocuscuda, sm_100a).
+
+Workload (one step = one whole stack): 30 RGB u8 frames of 7952x5304 from the
+production synthetic scene (shifts up to 60 px, roll up to 0.3 deg, blur up to
+8 px), remapped through their poses into the common-overlap ROI and fused with
+pyramid-contrast at full pyramid depth, FP32 levels: pass 1 over all frames,
+pass 2, collapse and quantise.
+
+  value  fused MPix*frames/s = frames x ROI pixels / device time per step, all
+         ranks together, frames already resident in HBM (3.8 GB per stack,
+         larger than L2, so no flush is needed);
+  e2e    the same metric through the public API from pinned host frames: the
+         host->device copy of every frame and the device->host copy of the
+         fused output are inside the timed region.
+
+`--impl reference` times the CPU oracle (the C++ restatement of the
+reference's Zig path; the Zig reference cannot be built in this image) on
+the host cores for the same metric, on a bounded sample of the workload.
+
+Multi-GPU: one process per GPU (torchrun), each rank fuses its own stack
+(independent stacks, no data-path collective; weak scaling).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+from __graft_entry__ import load_package  # noqa: E402
+
+METRIC = "fused MPix*frames/s (plain FP32 pyramid-contrast, remap+fuse)"
+UNIT = "MPix*frames/s"
+
+FRAMES, WIDTH, HEIGHT = 30, 7952, 5304
+# CPU samples: frames x width x height of the same scene (bounded CPU work)
+CPU_SAMPLE = (3, 1988, 1326)
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--frames", type=int, default=FRAMES)
+    ap.add_argument("--width", type=int, default=WIDTH)
+    ap.add_argument("--height", type=int, default=HEIGHT)
+    ap.add_argument("--batch", type=int, default=0, help="frames per pass over per-pixel state (0 = library default)")
+    ap.add_argument("--seed", type=int, default=1)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-case", action="store_true",
+                    help="small case for ncu: 4 frames, no e2e / CPU legs, one timed step")
+    return ap.parse_args()
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    FIELDS = ("clocks.sm", "clocks.max.sm", "power.draw", "clocks_event_reasons.hw_slowdown",
+              "clocks_event_reasons.hw_thermal_slowdown", "clocks_event_reasons.sw_thermal_slowdown",
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), "--query-gpu=" + ",".join(self.FIELDS),
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+        time.sleep(0.3)
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.2)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm, smax, reasons = [], [], set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) != len(self.FIELDS):
+                continue
+            try:
+                sm.append(float(parts[0]))
+                smax.append(float(parts[1]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[3:]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------- algorithmic bytes
+def level_sizes(w, h):
+    sizes = [(w, h)]
+    while w > 1 or h > 1:
+        w = (w + 1) // 2 if w > 1 else 1
+        h = (h + 1) // 2 if h > 1 else 1
+        sizes.append((w, h))
+    return sizes
+
+
+def algorithmic_bytes(roi_w, roi_h, frames, k):
+    """Per-kernel algorithmic HBM bytes of one stack (the level-streaming model):
+    every tensor is read once per consumer and written once; the u8 frames are
+    read once per pass; per-pixel state is read/written once per batch of k
+    frames.  Returns {kernel: bytes per step} and the pipeline total."""
+    sz = level_sizes(roi_w, roi_h)
+    A = [w * h for w, h in sz]
+    L = len(sz)
+    batches = -(-frames // k)
+    b = {}
+    # pass 1: frame 3 B/px; weight sum f32 and union u8 read+write per batch (first batch writes only)
+    b["pass1"] = frames * 3 * A[0] + batches * 10 * A[0] - 5 * A[0]
+    # level 0: frame 3 B/px; level-1 Gaussian/support/mask written (17 B/px at 1/4 area);
+    # weight sum 4 + union 1 read and accumulator 24 read+write per batch
+    l1 = A[1] if L > 1 else 0
+    b["level0"] = frames * (3 * A[0] + 17 * l1) + batches * (29 * A[0])
+    # levels l >= 1: read G/S/M (17 B) and write the next level (17 B at 1/4 area);
+    # mask support 1 B and accumulator 24 B per batch
+    lv = 0
+    for l in range(1, L - 1):
+        nxt = A[l + 1] if l + 1 < L - 1 else 0
+        top = A[l + 1] * 24 * batches if l + 1 == L - 1 else 0
+        lv += frames * (17 * A[l] + 17 * nxt) + batches * 25 * A[l] + top
+    b["level"] = lv
+    # mask-support pyramid: read level l, write level l + 1
+    b["mask_support"] = sum(A[l] + A[l + 1] for l in range(L - 1))
+    # collapse: read child accumulator (12 B), read+write parent (24 B); last level writes u8 instead
+    col = 0
+    for l in range(L - 1, 0, -1):
+        col += 12 * A[l] + (24 * A[l - 1] if l - 1 > 0 else 12 * A[0] + 3 * A[0])
+    b["collapse"] = col
+    return b, sum(b.values())
+
+
+def profile_traffic(kernel: str):
+    """Per-launch DRAM traffic of `kernel` on this workload from a committed
+    ncu summary (profiles/<kernel>_*.md, line `traffic_bytes_per_launch: N`)."""
+    pdir = os.path.join(ROOT, "profiles")
+    if not os.path.isdir(pdir):
+        return None
+    for name in sorted(os.listdir(pdir)):
+        if not name.startswith(kernel + "_") or not name.endswith(".md"):
+            continue
+        with open(os.path.join(pdir, name)) as fh:
+            for line in fh:
+                if line.strip().startswith("traffic_bytes_per_launch:"):
+                    try:
+                        return float(line.split(":", 1)[1].strip().split()[0])
+                    except ValueError:
+                        return None
+    return None
+
+
+def measured_hbm_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as fh:
+            return float(json.load(fh)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+# ----------------------------------------------------------- CPU baseline
+def cpu_sample_frames(fsb, sample, seed, ctx=None, torch=None):
+    """Sample frames of the production scene: rendered on the GPU when a
+    context is given, else on the CPU (the reference arm touches no GPU)."""
+    F, W, H = sample
+    frames, poses = [], []
+    for k in range(F):
+        if ctx is not None:
+            buf = torch.empty((H, W, 3), dtype=torch.uint8, device=f"cuda:{ctx.device}")
+            poses.append(fsb.synth_frame_device(ctx, seed, fsb.SCENE_PRODUCTION, W, H, k, F, buf, W * 3))
+            frames.append(buf.cpu().numpy())
+        else:
+            from importlib import import_module
+            synth_cpu = import_module("focus_stacker_b200.synth_cpu")
+            img, pose = synth_cpu.synth_frame_cpu(seed, fsb.SCENE_PRODUCTION, W, H, k, F)
+            frames.append(img)
+            poses.append(pose)
+    return frames, poses
+
+
+def cpu_baseline(fsb, steps=1, warmup=0, sample=CPU_SAMPLE, seed=1, ctx=None, torch=None):
+    """Time the oracle (C++ restatement, all host threads) on a bounded sample."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    F, W, H = sample
+    frames, poses = cpu_sample_frames(fsb, sample, seed, ctx, torch)
+    roi = fsb.compute_common_overlap_roi([True] * F, [W] * F, [H] * F, poses)
+    cores = os.cpu_count() or 1
+    pd = [p.as_dict() for p in poses]
+    times = []
+    for i in range(warmup + steps):
+        t0 = time.perf_counter()
+        oracle.stack_fuse(frames, pd, roi.as_tuple(), jobs=cores)
+        dt = time.perf_counter() - t0
+        if i >= warmup:
+            times.append(dt)
+    t = statistics.median(times)
+    px = F * roi.width * roi.height
+    return {"value": px / t / 1e6, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"{F} frames of {W}x{H} (ROI {roi.width}x{roi.height}), same scene recipe, "
+                      f"oracle stack_fuse (remap + pyramid-contrast, FP32) with {cores} threads, "
+                      f"median of {len(times)} runs: {t:.2f} s"}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    fsb = load_package()
+    cb = cpu_baseline(fsb, steps=args.steps, warmup=args.warmup)
+    line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": workload_config(args, None, 0),
+            "cpu_baseline": cb,
+            "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def workload_config(args, roi, k):
+    return {"workload": f"{args.frames}x{args.width}x{args.height} RGB u8 synthetic focus stack "
+                        "(production scene), remap + pyramid-contrast, FP32 levels",
+            "frames": args.frames, "src": [args.width, args.height],
+            "roi": roi.as_tuple() if roi is not None else None,
+            "levels": len(level_sizes(roi.width, roi.height)) if roi is not None else None,
+            "frames_per_batch": k, "contrast_window": 5,
+            "l2": "inputs (frames x W x H x 3 B) larger than the 126 MB L2; no flush",
+            "parallelism": f"replicas x{args.gpus} (one stack per GPU)"}
+
+
+# ------------------------------------------------------------------- main
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    import torch
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", local))
+    if args.profile_case:
+        args.frames, args.steps, args.warmup = 4, 1, 1
+        args.no_e2e = args.no_cpu_baseline = True
+    fsb = load_package()
+    dev = local
+    F, W, H = args.frames, args.width, args.height
+    ctx = fsb.Context(dev)
+    frames, poses = [], []
+    for k in range(F):
+        buf = torch.empty((H, W, 3), dtype=torch.uint8, device=f"cuda:{dev}")
+        poses.append(fsb.synth_frame_device(ctx, args.seed + rank, fsb.SCENE_PRODUCTION, W, H, k, F, buf, W * 3))
+        frames.append(buf)
+    roi = fsb.compute_common_overlap_roi([True] * F, [W] * F, [H] * F, poses)
+    out = torch.empty((roi.height, roi.width, 3), dtype=torch.uint8, device=f"cuda:{dev}")
+
+    def step():
+        st = fsb.PyramidContrastStack(ctx, W, H, F, roi=roi, frames_per_batch=args.batch)
+        for f, p in zip(frames, poses):
+            st.add_frame_device(f, W * 3, p)
+        st.finish_device(out, roi.width * 3)
+        k_used = st.desc.frames_per_batch
+        st.close()
+        return k_used
+
+    for _ in range(args.warmup):
+        step()
+    ctx.synchronize()
+    stream = torch.cuda.ExternalStream(ctx.stream_handle(), device=f"cuda:{dev}")
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    clocks = ClockSampler(dev)
+    clocks.start()
+    n0 = ctx.launch_count()
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    e1.synchronize()
+    torch.cuda.synchronize(dev)
+    launches = (ctx.launch_count() - n0) // max(1, args.steps)
+    clock_info = clocks.stop()
+    ms = e0.elapsed_time(e1) / args.steps
+    if dist:
+        t = torch.tensor([ms], device=f"cuda:{dev}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    px = F * roi.width * roi.height
+    value = world * px / (ms / 1e3) / 1e6
+
+    # per-kernel device time (CUDA events on the library's stream), one extra step
+    ctx.set_kernel_timing(True)
+    step()
+    stats = {}
+    for name in ("pass1", "level0", "level", "collapse", "mask_support"):
+        n, tot = ctx.kernel_stats(name)
+        stats[name] = (n, tot)
+    ctx.set_kernel_timing(False)
+    k_default = 8 if args.batch == 0 else args.batch
+    k_eff = max(1, min(k_default, 8, F))
+    alg, alg_total = algorithmic_bytes(roi.width, roi.height, F, k_eff)
+    dom = max(stats, key=lambda n: stats[n][1])
+    n_dom, ms_dom = stats[dom]
+    peak, peak_kind = measured_hbm_peak()
+    per_launch = alg[dom] / max(1, n_dom)
+    achieved = per_launch / (ms_dom / max(1, n_dom) / 1e3) / 1e9
+    traffic = profile_traffic(dom)
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                "frac": round(achieved / peak, 4), "traffic": traffic, "peak_source": peak_kind,
+                "alg_bytes_per_launch": per_launch, "launches_per_step": n_dom,
+                "avg_launch_ms": ms_dom / max(1, n_dom)}
+    kernel_table = {n: {"launches": v[0], "total_ms": round(v[1], 4), "share": round(v[1] / max(1e-9, sum(
+        x[1] for x in stats.values())), 4), "alg_bytes": alg[n]} for n, v in stats.items()}
+    pipeline = {"alg_bytes_per_frame_pixel": alg_total / px,
+                "achieved_gbs": alg_total / (ms / 1e3) / 1e9,
+                "frac": (alg_total / (ms / 1e3) / 1e9) / peak}
+
+    # end to end through the public API from pinned host memory
+    e2e = None
+    if not args.no_e2e:
+        hframes = []
+        for f in frames:
+            h = torch.empty(f.shape, dtype=torch.uint8, pin_memory=True)
+            h.copy_(f)
+            hframes.append(h.numpy())
+        hout = torch.empty((roi.height, roi.width, 3), dtype=torch.uint8, pin_memory=True).numpy()
+
+        def step_e2e():
+            st = fsb.PyramidContrastStack(ctx, W, H, F, roi=roi, frames_per_batch=args.batch)
+            for f, p in zip(hframes, poses):
+                st.add_frame(f, p)
+            st.finish_into(hout)
+            st.close()
+
+        step_e2e()
+        if dist:
+            dist.barrier()
+        t0 = time.perf_counter()
+        n_e2e = max(1, min(args.steps, 5))
+        for _ in range(n_e2e):
+            step_e2e()
+        dt = (time.perf_counter() - t0) / n_e2e
+        if dist:
+            t = torch.tensor([dt], device=f"cuda:{dev}")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            dt = float(t.item())
+        e2e = {"value": world * px / dt / 1e6, "unit": UNIT, "h2d_bytes_per_step": F * W * H * 3,
+               "d2h_bytes_per_step": roi.width * roi.height * 3, "ms_per_step": dt * 1e3}
+        del hframes
+
+    cpu = None
+    if not args.no_cpu_baseline and rank == 0 and world == 1:
+        cpu = cpu_baseline(fsb, steps=1, warmup=1, sample=(4, 3976, 2652), ctx=ctx, torch=torch)
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": round(value, 2), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": round(ms, 4), "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": workload_config(args, roi, k_eff),
+                "e2e": e2e, "gpu_launches": launches, "clocks": clock_info, "roofline": roofline,
+                "cpu_baseline": cpu, "kernels": kernel_table, "pipeline_roofline": pipeline}
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -23,8 +23,8 @@ STATUS_NAMES = {
 # Every function the header declares (checked by the CPU tests).
 EXPORTED = (
     "fs_create", "fs_destroy", "fs_last_error", "fs_status_string", "fs_api_version", "fs_ctx_device_bytes",
-    "fs_ctx_synchronize", "fs_ctx_launch_count", "fs_ctx_set_kernel_timing", "fs_ctx_kernel_stats",
-    "fs_pose_default", "fs_compute_roi", "fs_inverse_map_points", "fs_exact_expand_divisor",
+    "fs_ctx_synchronize", "fs_ctx_trim", "fs_ctx_stream", "fs_ctx_launch_count", "fs_ctx_set_kernel_timing", "fs_ctx_kernel_stats",
+    "fs_pose_default", "fs_compute_roi", "fs_inverse_map_points", "fs_forward_map_points", "fs_exact_expand_divisor",
     "fs_remap_frame", "fs_remap_frame_device",
     "fs_stack_begin", "fs_stack_add_frame", "fs_stack_add_frame_device", "fs_stack_finish",
     "fs_stack_finish_device", "fs_stack_set_base_output", "fs_stack_output_size", "fs_stack_destroy", "fs_fuse_stack",
@@ -87,6 +87,8 @@ def _bind(L):
     L.fs_ctx_device_bytes.argtypes = [ctx]
     L.fs_ctx_device_bytes.restype = u64
     L.fs_ctx_synchronize.argtypes = [ctx]
+    L.fs_ctx_trim.argtypes = [ctx]
+    L.fs_ctx_stream.argtypes = [ctx, P(vp)]
     L.fs_ctx_launch_count.argtypes = [ctx]
     L.fs_ctx_launch_count.restype = u64
     L.fs_ctx_set_kernel_timing.argtypes = [ctx, i32]
@@ -95,6 +97,7 @@ def _bind(L):
     L.fs_pose_default.restype = None
     L.fs_compute_roi.argtypes = [P(FsPose), P(u32), P(u32), P(ctypes.c_uint8), sz, P(FsRect), P(i32)]
     L.fs_inverse_map_points.argtypes = [P(FsPose), u32, u32, sz, P(ctypes.c_double), P(ctypes.c_double)]
+    L.fs_forward_map_points.argtypes = [P(FsPose), u32, u32, sz, P(ctypes.c_double), P(ctypes.c_double)]
     L.fs_exact_expand_divisor.argtypes = [i32, i32, i32, i32]
     L.fs_exact_expand_divisor.restype = ctypes.c_float
     for f in (L.fs_remap_frame, L.fs_remap_frame_device):

@@ -182,6 +182,15 @@ class Context:
     def device_bytes(self) -> int:
         return int(L().fs_ctx_device_bytes(self.handle))
 
+    def trim(self):
+        _check(L().fs_ctx_trim(self.handle), self.handle)
+
+    def stream_handle(self) -> int:
+        """cudaStream_t of the context (e.g. for torch.cuda.ExternalStream)."""
+        v = ctypes.c_void_p()
+        _check(L().fs_ctx_stream(self.handle, ctypes.byref(v)), self.handle)
+        return int(v.value or 0)
+
     def launch_count(self) -> int:
         return int(L().fs_ctx_launch_count(self.handle))
 
@@ -214,6 +223,17 @@ def inverse_map_points(pose, width: int, height: int, xy: np.ndarray) -> np.ndar
     out = np.zeros_like(xy)
     p = _pose(pose).to_c()
     _check(L().fs_inverse_map_points(ctypes.byref(p), width, height, xy.shape[0],
+                                     xy.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                     out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
+    return out
+
+
+def forward_map_points(pose, width: int, height: int, xy: np.ndarray) -> np.ndarray:
+    """Source-frame points -> aligned-frame points (the reference's transformPoint)."""
+    xy = np.ascontiguousarray(xy, dtype=np.float64).reshape(-1, 2)
+    out = np.zeros_like(xy)
+    p = _pose(pose).to_c()
+    _check(L().fs_forward_map_points(ctypes.byref(p), width, height, xy.shape[0],
                                      xy.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
                                      out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
     return out

@@ -13,6 +13,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -44,6 +45,10 @@ struct fs_ctx {
   bool timing = false;
   std::vector<KernelTiming> timings;
   uint64_t launches = 0;
+  // Device buffers released by finished stacks, kept for reuse by the next
+  // stack of the same geometry (counted in `held`); fs_ctx_trim frees them.
+  std::multimap<size_t, void*> pool;
+  uint64_t pooled = 0;
 };
 
 namespace {
@@ -65,8 +70,25 @@ int cuda_err(fs_ctx* ctx, cudaError_t e, const char* what) {
   return set_err(ctx, FS_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
 }
 
+void pool_trim(fs_ctx* ctx) {
+  for (auto& kv : ctx->pool) {
+    cudaFree(kv.second);
+    ctx->held -= std::min<uint64_t>(ctx->held, kv.first);
+  }
+  ctx->pool.clear();
+  ctx->pooled = 0;
+}
+
 int dev_alloc(fs_ctx* ctx, size_t bytes, void** out) {
   if (bytes == 0) bytes = 16;
+  auto it = ctx->pool.find(bytes);
+  if (it != ctx->pool.end()) {
+    *out = it->second;
+    ctx->pool.erase(it);
+    ctx->pooled -= bytes;
+    return FS_OK;
+  }
+  if (ctx->held + bytes > ctx->budget && ctx->pooled > 0) pool_trim(ctx);
   if (ctx->held + bytes > ctx->budget)
     return set_err(ctx, FS_ERR_BUDGET, "device memory budget exceeded (" + std::to_string(ctx->held + bytes) +
                                            " > " + std::to_string(ctx->budget) + " bytes)");
@@ -84,6 +106,15 @@ void dev_free(fs_ctx* ctx, void* p, size_t bytes) {
   cudaFree(p);
   if (bytes == 0) bytes = 16;
   ctx->held -= std::min<uint64_t>(ctx->held, bytes);
+}
+
+// Return a buffer to the context's pool (stream-ordered: callers synchronize
+// the stream before releasing).
+void dev_release(fs_ctx* ctx, void* p, size_t bytes) {
+  if (!p) return;
+  if (bytes == 0) bytes = 16;
+  ctx->pool.emplace(bytes, p);
+  ctx->pooled += bytes;
 }
 
 // Launch wrapper: counts launches and optionally brackets them with events
@@ -263,6 +294,8 @@ int fs_create(int device, uint64_t hbm_budget_bytes, fs_ctx** out) {
 void fs_destroy(fs_ctx* ctx) {
   if (!ctx) return;
   cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
+  pool_trim(ctx);
   for (auto& t : ctx->timings) {
     cudaEventDestroy(t.start);
     cudaEventDestroy(t.stop);
@@ -278,6 +311,20 @@ const char* fs_last_error(const fs_ctx* ctx) {
 }
 
 uint64_t fs_ctx_device_bytes(const fs_ctx* ctx) { return ctx ? ctx->held : 0; }
+
+int fs_ctx_trim(fs_ctx* ctx) {
+  if (!ctx) return FS_ERR_INVALID;
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
+  pool_trim(ctx);
+  return FS_OK;
+}
+
+int fs_ctx_stream(const fs_ctx* ctx, void** stream) {
+  if (!ctx || !stream) return FS_ERR_INVALID;
+  *stream = (void*)ctx->stream;
+  return FS_OK;
+}
 
 int fs_ctx_set_kernel_timing(fs_ctx* ctx, int enable) {
   if (!ctx) return FS_ERR_INVALID;
@@ -337,6 +384,14 @@ int fs_inverse_map_points(const fs_pose* pose, uint32_t width, uint32_t height, 
   if (!pose || (!xy && n) || (!out_xy && n)) return FS_ERR_INVALID;
   for (size_t i = 0; i < n; ++i)
     inverse_map_point_f64(*pose, width, height, xy[2 * i], xy[2 * i + 1], &out_xy[2 * i], &out_xy[2 * i + 1]);
+  return FS_OK;
+}
+
+int fs_forward_map_points(const fs_pose* pose, uint32_t width, uint32_t height, size_t n, const double* xy,
+                          double* out_xy) {
+  if (!pose || (!xy && n) || (!out_xy && n)) return FS_ERR_INVALID;
+  for (size_t i = 0; i < n; ++i)
+    forward_map_point(*pose, width, height, xy[2 * i], xy[2 * i + 1], &out_xy[2 * i], &out_xy[2 * i + 1]);
   return FS_OK;
 }
 
@@ -718,7 +773,7 @@ int fs_stack_destroy(fs_stack* s) {
   cudaSetDevice(ctx->device);
   cudaStreamSynchronize(ctx->stream);
   cudaStreamSynchronize(ctx->copy);
-  for (auto& a : s->allocs) dev_free(ctx, a.p, a.bytes);
+  for (auto& a : s->allocs) dev_release(ctx, a.p, a.bytes);
   if (s->copy_done) cudaEventDestroy(s->copy_done);
   delete s;
   return FS_OK;

@@ -80,13 +80,20 @@ FS_DF dfl df_mul_f(dfl a, float b) {
   p.lo = FS_FMA(a.lo, b, p.lo);
   return df_fast_two_sum(p.hi, p.lo);
 }
-// a / b with two correction steps.
+#ifdef __CUDACC__
+#define FS_FDIV(a, b) __fdividef((a), (b))
+#else
+#define FS_FDIV(a, b) ((a) / (b))
+#endif
+// a / b: an approximate FP32 quotient (a few ulp) refined by two exact
+// remainder corrections, which is what carries the ~2^-46 accuracy.
 FS_DF dfl df_div(dfl a, dfl b) {
-  float q1 = a.hi / b.hi;
+  float rb = FS_FDIV(1.0f, b.hi);
+  float q1 = FS_MUL(a.hi, rb);
   dfl r = df_sub(a, df_mul_f(b, q1));
-  float q2 = r.hi / b.hi;
+  float q2 = FS_MUL(r.hi, rb);
   r = df_sub(r, df_mul_f(b, q2));
-  float q3 = r.hi / b.hi;
+  float q3 = FS_MUL(r.hi, rb);
   dfl q = df_fast_two_sum(q1, q2);
   return df_add_f(q, q3);
 }

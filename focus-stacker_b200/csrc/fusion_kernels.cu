@@ -45,29 +45,45 @@ __device__ void fill_region(const FrameIn& f, int W, int H, int rx0, int ry0, in
     }
     return;
   }
-  const int nbx = (rw + 7) >> 3, nby = (rh + 3) >> 2;
+  const int nbx = (rw + 7) >> 3, nby = (rh + 3) >> 2, nb = nbx * nby;
   const int du = lane & 7, dv = lane >> 3;
   const bool fast_ok = f.warp.kind == WARP_HOMOGRAPHY && !f.warp.guard;
-  for (int blk = warp; blk < nbx * nby; blk += nwarps) {
-    const int bx = blk % nbx, by = blk / nbx;
-    const int AX = rx0 + bx * 8, AY = ry0 + by * 4;
-    bool aok = false;
-    Anchor an;
-    if (fast_ok) an = make_anchor(f.warp, AX, AY, &aok);
-    const int rx = bx * 8 + du, ry = by * 4 + dv;
-    if (rx >= rw || ry >= rh) continue;
-    const int X = AX + du, Y = AY + dv;
-    uint32_t v = 0;
-    if (X >= 0 && Y >= 0 && X < W && Y < H) {
-      v = aok ? sample_fast(f.warp, f.src, an, du, dv, X, Y) : sample_exact(f.warp, f.src, X, Y);
+  // this warp handles blocks warp, warp + nwarps, ...; lane j forms the
+  // anchor of the j-th of up to 32 of them, then each block takes it by shuffle
+  for (int g0 = warp; g0 < nb; g0 += nwarps * 32) {
+    Anchor mine = {};
+    bool mine_ok = false;
+    {
+      const int bj = g0 + lane * nwarps;
+      if (fast_ok && bj < nb) mine = make_anchor(f.warp, rx0 + (bj % nbx) * 8, ry0 + (bj / nbx) * 4, &mine_ok);
     }
-    reg[ry * rw + rx] = v;
+    const int cnt = min(32, (nb - g0 + nwarps - 1) / nwarps);
+    for (int j = 0; j < cnt; ++j) {
+      const int blk = g0 + j * nwarps;
+      const int bx = blk % nbx, by = blk / nbx;
+      const int AX = rx0 + bx * 8, AY = ry0 + by * 4;
+      const bool aok = __shfl_sync(0xffffffffu, mine_ok ? 1 : 0, j) != 0;
+      const Anchor an = shfl_anchor(mine, j);
+      const int rx = bx * 8 + du, ry = by * 4 + dv;
+      if (rx >= rw || ry >= rh) continue;
+      const int X = AX + du, Y = AY + dv;
+      uint32_t v = 0;
+      if (X >= 0 && Y >= 0 && X < W && Y < H) {
+        v = aok ? sample_fast(f.warp, f.src, an, du, dv, X, Y) : sample_exact(f.warp, f.src, X, Y);
+      }
+      reg[ry * rw + rx] = v;
+    }
   }
 }
 
 __device__ __forceinline__ uint32_t px_alpha(uint32_t v) { return v >> 24; }
 __device__ __forceinline__ int px_gray(uint32_t v) { return (int)(v & 255u) + (int)((v >> 8) & 255u) + (int)((v >> 16) & 255u); }
 __device__ __forceinline__ float px_chan(uint32_t v, int c) { return (float)((v >> (8 * c)) & 255u); }
+
+// f32(alpha) / 255 as the reference computes it (src/fuse/masks.zig:18).
+__device__ __forceinline__ float alpha_support(uint32_t al) {
+  return al == 255u ? 1.0f : __fdiv_rn((float)al, 255.0f);
+}
 
 // Sample standard deviation of gray = k / 765 over the supported window
 // pixels, from exact integer sums of k and k^2 (src/fuse/contrast.zig:284-290):
@@ -77,7 +93,7 @@ __device__ __forceinline__ float window_stddev(int n, long long s1, long long s2
   long long num = (long long)n * s2 - s1 * s1;
   if (num <= 0) return 0.0f;
   float den = (float)((long long)n * (n - 1)) * 585225.0f;
-  return sqrtf((float)num / den);
+  return sqrtf(__fdividef((float)num, den));
 }
 
 }  // namespace
@@ -99,16 +115,15 @@ __global__ void __launch_bounds__(kThreads) pass1_kernel(const __grid_constant__
   const int x0 = blockIdx.x * kTileW, y0 = blockIdx.y * kTileH;
   constexpr int PPT = kTileW * kTileH / kThreads;  // output pixels per thread
   float nacc[PPT];
-  uint32_t uacc[PPT];
+  uint32_t umask = 0;  // union support of this thread's pixels, one bit each
 #pragma unroll
   for (int i = 0; i < PPT; ++i) {
     int p = threadIdx.x + i * kThreads;
     int X = x0 + (p % kTileW), Y = y0 + (p / kTileW);
     nacc[i] = 0.0f;
-    uacc[i] = 0;
     if (!a.first && X < a.W && Y < a.H) {
       nacc[i] = a.norm[(int64_t)Y * a.norm_pitch + X];
-      uacc[i] = a.uni[(int64_t)Y * a.uni_pitch + X];
+      if (a.uni[(int64_t)Y * a.uni_pitch + X]) umask |= 1u << i;
     }
   }
   for (int k = 0; k < a.K; ++k) {
@@ -142,7 +157,7 @@ __global__ void __launch_bounds__(kThreads) pass1_kernel(const __grid_constant__
       if (X >= a.W || Y >= a.H) continue;
       uint32_t own = reg[(r + b) * rw + (c + b)];
       uint32_t al = px_alpha(own);
-      if (al > 0) uacc[i] = 1;
+      if (al > 0) umask |= 1u << i;
       float w = 0.0f;
       if (a.window_ok && al > 0 && X >= b && Y >= b && X < a.W - b && Y < a.H - b) {
         int n = 0;
@@ -154,7 +169,7 @@ __global__ void __launch_bounds__(kThreads) pass1_kernel(const __grid_constant__
           s2 += hs2[j];
         }
         float sd = window_stddev(n, s1, s2);
-        w = __fmul_rn(sd, __fdiv_rn((float)al, 255.0f));
+        w = __fmul_rn(sd, alpha_support(al));
       }
       nacc[i] = __fadd_rn(nacc[i], w);
     }
@@ -166,7 +181,7 @@ __global__ void __launch_bounds__(kThreads) pass1_kernel(const __grid_constant__
     int X = x0 + (p % kTileW), Y = y0 + (p / kTileW);
     if (X < a.W && Y < a.H) {
       a.norm[(int64_t)Y * a.norm_pitch + X] = nacc[i];
-      a.uni[(int64_t)Y * a.uni_pitch + X] = (uint8_t)uacc[i];
+      a.uni[(int64_t)Y * a.uni_pitch + X] = (uint8_t)((umask >> i) & 1u);
     }
   }
 }
@@ -540,7 +555,7 @@ __global__ void __launch_bounds__(kThreads) level_kernel(const __grid_constant__
               s1 += cs.s1[j];
               s2 += cs.s2[j];
             }
-            w = __fmul_rn(window_stddev(n, s1, s2), __fdiv_rn((float)al, 255.0f));
+            w = __fmul_rn(window_stddev(n, s1, s2), alpha_support(al));
           }
           float nv = normr[i];
           mval = nv > 1e-12f ? __fdiv_rn(w, nv) : a.inv_count;
@@ -738,26 +753,35 @@ cudaError_t launch_mask_support(const MaskSupportArgs& a, cudaStream_t s) {
 __global__ void __launch_bounds__(kThreads) remap_kernel(const __grid_constant__ RemapArgs a) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
   const int x0 = blockIdx.x * kTileW, y0 = blockIdx.y * kTileH;
-  const int nbx = kTileW / 8, nby = kTileH / 4;
+  const int nbx = kTileW / 8, nby = kTileH / 4, nb = nbx * nby;
   const bool fast_ok = a.f.warp.kind == WARP_HOMOGRAPHY && !a.f.warp.guard;
-  for (int blk = warp; blk < nbx * nby; blk += nwarps) {
-    int AX = x0 + (blk % nbx) * 8, AY = y0 + (blk / nbx) * 4;
-    bool aok = false;
-    Anchor an;
-    if (fast_ok) an = make_anchor(a.f.warp, AX, AY, &aok);
-    int du = lane & 7, dv = lane >> 3;
-    int X = AX + du, Y = AY + dv;
-    if (X >= a.W || Y >= a.H) continue;
-    uint32_t v = aok ? sample_fast(a.f.warp, a.f.src, an, du, dv, X, Y) : sample_exact(a.f.warp, a.f.src, X, Y);
-    uint8_t* d = a.dst + (int64_t)Y * a.dst_pitch + (int64_t)X * a.dst_ch;
-    if (a.dst_ch == 4) {
-      d[0] = v & 255u;
-      d[1] = (v >> 8) & 255u;
-      d[2] = (v >> 16) & 255u;
-      d[3] = v >> 24;
-    } else {
-      d[0] = v & 255u;
-      d[1] = v >> 24;
+  const int du = lane & 7, dv = lane >> 3;
+  for (int g0 = warp; g0 < nb; g0 += nwarps * 32) {
+    Anchor mine = {};
+    bool mine_ok = false;
+    {
+      const int bj = g0 + lane * nwarps;
+      if (fast_ok && bj < nb) mine = make_anchor(a.f.warp, x0 + (bj % nbx) * 8, y0 + (bj / nbx) * 4, &mine_ok);
+    }
+    const int cnt = min(32, (nb - g0 + nwarps - 1) / nwarps);
+    for (int j = 0; j < cnt; ++j) {
+      const int blk = g0 + j * nwarps;
+      const int AX = x0 + (blk % nbx) * 8, AY = y0 + (blk / nbx) * 4;
+      const bool aok = __shfl_sync(0xffffffffu, mine_ok ? 1 : 0, j) != 0;
+      const Anchor an = shfl_anchor(mine, j);
+      const int X = AX + du, Y = AY + dv;
+      if (X >= a.W || Y >= a.H) continue;
+      uint32_t v = aok ? sample_fast(a.f.warp, a.f.src, an, du, dv, X, Y) : sample_exact(a.f.warp, a.f.src, X, Y);
+      uint8_t* d = a.dst + (int64_t)Y * a.dst_pitch + (int64_t)X * a.dst_ch;
+      if (a.dst_ch == 4) {
+        d[0] = v & 255u;
+        d[1] = (v >> 8) & 255u;
+        d[2] = (v >> 16) & 255u;
+        d[3] = v >> 24;
+      } else {
+        d[0] = v & 255u;
+        d[1] = v >> 24;
+      }
     }
   }
 }

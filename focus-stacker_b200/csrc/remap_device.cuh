@@ -79,6 +79,25 @@ __device__ __forceinline__ bool warp_disp(const Warp& w, float X, float Y, dfl* 
   return true;
 }
 
+// Block anchor broadcast from lane `src` of the warp.
+__device__ __forceinline__ Anchor shfl_anchor(const Anchor& a, int src) {
+  const unsigned full = 0xffffffffu;
+  Anchor o;
+  o.ix = __shfl_sync(full, a.ix, src);
+  o.iy = __shfl_sync(full, a.iy, src);
+  o.fxh = __shfl_sync(full, a.fxh, src);
+  o.fxl = __shfl_sync(full, a.fxl, src);
+  o.fyh = __shfl_sync(full, a.fyh, src);
+  o.fyl = __shfl_sync(full, a.fyl, src);
+  o.am1x = __shfl_sync(full, a.am1x, src);
+  o.bx = __shfl_sync(full, a.bx, src);
+  o.ay = __shfl_sync(full, a.ay, src);
+  o.bm1y = __shfl_sync(full, a.bm1y, src);
+  o.gam = __shfl_sync(full, a.gam, src);
+  o.eta = __shfl_sync(full, a.eta, src);
+  return o;
+}
+
 __device__ __forceinline__ Anchor make_anchor(const Warp& w, int X, int Y, bool* ok) {
   Anchor a = {};
   dfl dx, dy, D;
@@ -222,7 +241,7 @@ __device__ __forceinline__ uint32_t sample_fast(const Warp& w, const SrcImage& s
   float den = 1.0f + gd;
   float nx = fmaf(a.am1x, fdu, a.bx * fdv) - fdu * gd;
   float ny = fmaf(a.ay, fdu, a.bm1y * fdv) - fdv * gd;
-  float rd = __frcp_rn(den);
+  float rd = __fdividef(1.0f, den);
   float tx = a.fxh + fmaf(nx, rd, a.fxl);
   float ty = a.fyh + fmaf(ny, rd, a.fyl);
   float flx = floorf(tx), fly = floorf(ty);

@@ -363,6 +363,12 @@ std::vector<P2> clip(const std::vector<P2>& subject, const std::vector<P2>& clip
 
 }  // namespace
 
+void forward_map_point(const fs_pose& pose, uint32_t w, uint32_t h, double x, double y, double* ox, double* oy) {
+  P2 p = fwd_point(pose, x, y, w, h);
+  *ox = p.x;
+  *oy = p.y;
+}
+
 bool compute_roi(const fs_pose* poses, const uint32_t* widths, const uint32_t* heights, const uint8_t* active,
                  size_t n, fs_rect* out) {
   std::vector<P2> poly;

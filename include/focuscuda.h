@@ -71,6 +71,13 @@ int fs_api_version(void);
 uint64_t fs_ctx_device_bytes(const fs_ctx* ctx);
 /* Wait for all work queued on the context's stream. */
 int fs_ctx_synchronize(fs_ctx* ctx);
+/* Device buffers of destroyed stacks stay in a per-context pool (still
+ * counted against the budget) and are reused by later stacks of the same
+ * geometry; fs_ctx_trim frees them.  Not part of the reference. */
+int fs_ctx_trim(fs_ctx* ctx);
+/* The CUDA stream (cudaStream_t) all of the context's kernels run on, for
+ * callers that order their own work or record events against it. */
+int fs_ctx_stream(const fs_ctx* ctx, void** stream);
 /* Kernel accounting: number of kernels this context launched so far, and
  * (when timing is enabled) per-kernel launch counts and device time measured
  * with CUDA events on the launching stream.  Kernel names: "pass1",
@@ -96,6 +103,12 @@ int fs_compute_roi(const fs_pose* poses, const uint32_t* widths, const uint32_t*
  * map the kernels evaluate): replaces optimize.inverseTransformPointCached,
  * src/optimize.zig:3593-3616. */
 int fs_inverse_map_points(const fs_pose* pose, uint32_t width, uint32_t height, size_t n, const double* xy,
+                          double* out_xy);
+
+/* Forward map of n source-frame points to aligned-frame coordinates (FP64,
+ * host): replaces optimize.transformPoint, src/optimize.zig:3506-3525
+ * ((-1, -1) where the reference's chain rejects the point). */
+int fs_forward_map_points(const fs_pose* pose, uint32_t width, uint32_t height, size_t n, const double* xy,
                           double* out_xy);
 
 /* Normaliser of the no-wrap EXPAND at output (x, y) for a src_w x src_h

@@ -1076,8 +1076,10 @@ static void accumulateImage(const Frame& im, const Real* normalized_mask, const 
   // buildAndAccumulateImagePyramidInto: fillRgbBase + fillBinarySupport
   {
     size_t sc = im.stride();
-    for (size_t i = 0; i < n0; ++i)
-      for (int c = 0; c < 3; ++c) P.gauss[0].px[i * 3 + c] = (Real)im.at(i * sc + c);
+    parallelRows(im.height, n0 >= 262144 ? jobs : 1, [&](uint32_t r0, uint32_t r1) {  // fillRgbBase
+      for (size_t i = (size_t)r0 * im.width; i < (size_t)r1 * im.width; ++i)
+        for (int c = 0; c < 3; ++c) P.gauss[0].px[i * 3 + c] = (Real)im.at(i * sc + c);
+    });
     std::vector<float> sup(n0);
     fillBinarySupport(im, sup.data());
     for (size_t i = 0; i < n0; ++i) P.image_support[0].px[i] = (Real)sup[i];
@@ -1095,13 +1097,17 @@ static void accumulateImage(const Frame& im, const Real* normalized_mask, const 
     const Real* m = P.mask[l].px.data();
     Real* dst = P.acc[l].px.data();
     size_t n = (size_t)cur.w * cur.h;
-    for (size_t i = 0; i < n; ++i) {  // accumulateLapRowsSequential, src/fuse/pyramid.zig:1480-1504
-      Real wgt = m[i];
-      for (int c = 0; c < 3; ++c) {
-        Real lap = cur.px[i * 3 + c] - ex.px[i * 3 + c];
-        dst[i * 3 + c] += lap * wgt;
+    // accumulateLapRowsSequential, src/fuse/pyramid.zig:1480-1504 (row-parallel
+    // above 262144 pixels like src/fuse/pyramid.zig:1463-1467)
+    parallelRows(cur.h, n >= 262144 ? jobs : 1, [&](uint32_t r0, uint32_t r1) {
+      for (size_t i = (size_t)r0 * cur.w; i < (size_t)r1 * cur.w; ++i) {
+        Real wgt = m[i];
+        for (int c = 0; c < 3; ++c) {
+          Real lap = cur.px[i * 3 + c] - ex.px[i * 3 + c];
+          dst[i * 3 + c] += lap * wgt;
+        }
       }
-    }
+    });
   }
   {  // accumulateGaussianRowsSequential, src/fuse/pyramid.zig:1506-1529
     auto& g = P.gauss[L - 1];
@@ -1143,10 +1149,22 @@ static void weightMap(const Frame& im, uint32_t window, int jobs, std::vector<fl
                       std::vector<float>& w) {
   size_t n = (size_t)im.width * im.height;
   gray.resize(n); sup.resize(n); w.resize(n);
-  fillAverageFromLoaded(gray.data(), im);
-  fillBinarySupport(im, sup.data());
+  parallelRows(im.height, jobs, [&](uint32_t r0, uint32_t r1) {
+    Frame band = im;
+    size_t off = (size_t)r0 * im.width * im.stride() * (im.sample_bits == 8 ? 1 : 2);
+    band.pixels = (const uint8_t*)im.pixels + off;
+    band.height = r1 - r0;
+    fillAverageFromLoaded(gray.data() + (size_t)r0 * im.width, band);
+    fillBinarySupport(band, sup.data() + (size_t)r0 * im.width);
+  });
   computeLocalContrastWeights(gray.data(), im.width, im.height, sup.data(), window, jobs, w.data());
-  applySupportInto<float>(im, w.data());
+  parallelRows(im.height, jobs, [&](uint32_t r0, uint32_t r1) {
+    Frame band = im;
+    size_t off = (size_t)r0 * im.width * im.stride() * (im.sample_bits == 8 ? 1 : 2);
+    band.pixels = (const uint8_t*)im.pixels + off;
+    band.height = r1 - r0;
+    applySupportInto<float>(band, w.data() + (size_t)r0 * im.width);
+  });
 }
 
 }  // namespace oracle
@@ -1304,7 +1322,9 @@ int oracle_fuse_aligned(const void* const* frames, size_t count, uint32_t width,
     if (precision == 32) {
       weightMap(im, window, jobs, gray, sup, w);
       accumulateBinarySupportMax(im, uni.data());
-      for (size_t i = 0; i < n; ++i) norm32[i] += w[i];
+      parallelRows(height, jobs, [&](uint32_t r0, uint32_t r1) {
+        for (size_t i = (size_t)r0 * width; i < (size_t)r1 * width; ++i) norm32[i] += w[i];
+      });
     } else {
       gray.resize(n); sup.resize(n); w.resize(n);
       fillAverageFromLoaded(gray.data(), im);
@@ -1324,7 +1344,10 @@ int oracle_fuse_aligned(const void* const* frames, size_t count, uint32_t width,
     for (size_t k = 0; k < count; ++k) {  // pass 2 (src/fuse/pipeline.zig:389-420)
       Frame im = frame(k);
       weightMap(im, window, jobs, gray, sup, w);
-      normalizeWeightsInto<float>(w.data(), norm32.data(), count, m.data(), n);
+      parallelRows(height, jobs, [&](uint32_t r0, uint32_t r1) {
+        size_t b = (size_t)r0 * width, e = (size_t)r1 * width;
+        normalizeWeightsInto<float>(w.data() + b, norm32.data() + b, count, m.data() + b, e - b);
+      });
       accumulateImage<float>(im, m.data(), uni.data(), P, jobs);
     }
     std::vector<float> b(n * 3);

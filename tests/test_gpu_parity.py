@@ -242,9 +242,12 @@ def test_refetch_path_matches_resident(torch, ctx):
     roi = fsb.compute_common_overlap_roi([True] * F, [W] * F, [H] * F, poses)
     ref, _ = gpu_fuse(ctx, torch, frames, poses, roi, k=2)
     # a budget that fits the stack state but not every frame copy
+    ctx.trim()
+    before = ctx.device_bytes()
     probe = fsb.PyramidContrastStack(ctx, W, H, F, roi=roi, frames_per_batch=2)
-    state = ctx.device_bytes()
+    state = ctx.device_bytes() - before
     probe.close()
+    ctx.trim()
     small = fsb.Context(0, hbm_budget_bytes=state + 3 * W * H * 3 + 4096)
     st = fsb.PyramidContrastStack(small, W, H, F, roi=roi, frames_per_batch=2)
     for f, p in zip(frames, poses):
