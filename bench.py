@@ -134,36 +134,45 @@ def level_sizes(w, h):
     return sizes
 
 
-def algorithmic_bytes(roi_w, roi_h, frames, k):
-    """Per-kernel algorithmic HBM bytes of one stack (the level-streaming model):
-    every tensor is read once per consumer and written once; the u8 frames are
-    read once per pass; per-pixel state is read/written once per batch of k
-    frames.  Returns {kernel: bytes per step} and the pipeline total."""
+def algorithmic_bytes(roi_w, roi_h, frames, k, mode="cache", storage_bytes=4):
+    """Per-kernel algorithmic HBM bytes of one stack (level-streaming model):
+    every tensor is written once and read once per consumer, the u8 frames are
+    read once per remap, per-pixel state (weight sum, union, accumulators) is
+    read and written once per batch of k frames.  mode "cache": pass 1 keeps
+    the remapped frame (RGBA, 4 B) and its weight (4 B) for pass 2; "recompute":
+    pass 2 remaps again into per-batch slots.  Returns {kernel: bytes per step}
+    and the pipeline total."""
     sz = level_sizes(roi_w, roi_h)
     A = [w * h for w, h in sz]
     L = len(sz)
     batches = -(-frames // k)
+    s = storage_bytes
     b = {}
-    # pass 1: frame 3 B/px; weight sum f32 and union u8 read+write per batch (first batch writes only)
-    b["pass1"] = frames * 3 * A[0] + batches * 10 * A[0] - 5 * A[0]
-    # level 0: frame 3 B/px; level-1 Gaussian/support/mask written (17 B/px at 1/4 area);
-    # weight sum 4 + union 1 read and accumulator 24 read+write per batch
+    keep = 8 if mode == "cache" else 0
+    # pass 1: frame 3 B/px (+ kept planes 8 B/px); weight sum f32 and union u8
+    # read+write per batch (the first batch only writes)
+    b["pass1"] = frames * (3 + keep) * A[0] + batches * 10 * A[0] - 5 * A[0]
+    # pass-2 re-remap (recompute mode): frame 3 B/px read, planes 8 B/px written
+    b["remap_weights"] = 0 if mode == "cache" else frames * 11 * A[0]
+    # level 0: planes 8 B/px read; level-1 Gaussian/mask (4 s B) + support (1 B)
+    # written at 1/4 area; weight sum 4 + union 1 read and accumulator 24
+    # read+write per batch
     l1 = A[1] if L > 1 else 0
-    b["level0"] = frames * (3 * A[0] + 17 * l1) + batches * (29 * A[0])
-    # levels l >= 1: read G/S/M (17 B) and write the next level (17 B at 1/4 area);
+    b["level0"] = frames * (8 * A[0] + (4 * s + 1) * l1) + batches * 29 * A[0]
+    # levels l >= 1: read Gaussian/mask/support, write the next level;
     # mask support 1 B and accumulator 24 B per batch
     lv = 0
     for l in range(1, L - 1):
         nxt = A[l + 1] if l + 1 < L - 1 else 0
         top = A[l + 1] * 24 * batches if l + 1 == L - 1 else 0
-        lv += frames * (17 * A[l] + 17 * nxt) + batches * 25 * A[l] + top
+        lv += frames * ((4 * s + 1) * (A[l] + nxt)) + batches * 25 * A[l] + top
     b["level"] = lv
-    # mask-support pyramid: read level l, write level l + 1
     b["mask_support"] = sum(A[l] + A[l + 1] for l in range(L - 1))
-    # collapse: read child accumulator (12 B), read+write parent (24 B); last level writes u8 instead
+    # collapse: read child accumulator (12 B), read+write parent (24 B); the
+    # last step reads the base (12 B) and writes u8 RGB (3 B)
     col = 0
     for l in range(L - 1, 0, -1):
-        col += 12 * A[l] + (24 * A[l - 1] if l - 1 > 0 else 12 * A[0] + 3 * A[0])
+        col += 12 * A[l] + (24 * A[l - 1] if l - 1 > 0 else 15 * A[0])
     b["collapse"] = col
     return b, sum(b.values())
 
@@ -296,14 +305,15 @@ def main():
     roi = fsb.compute_common_overlap_roi([True] * F, [W] * F, [H] * F, poses)
     out = torch.empty((roi.height, roi.width, 3), dtype=torch.uint8, device=f"cuda:{dev}")
 
+    mode_used = {}
+
     def step():
         st = fsb.PyramidContrastStack(ctx, W, H, F, roi=roi, frames_per_batch=args.batch)
+        mode_used["mode"] = st.pass2_mode
         for f, p in zip(frames, poses):
             st.add_frame_device(f, W * 3, p)
         st.finish_device(out, roi.width * 3)
-        k_used = st.desc.frames_per_batch
         st.close()
-        return k_used
 
     for _ in range(args.warmup):
         step()
@@ -337,13 +347,14 @@ def main():
     ctx.set_kernel_timing(True)
     step()
     stats = {}
-    for name in ("pass1", "level0", "level", "collapse", "mask_support"):
+    for name in ("pass1", "remap_weights", "level0", "level", "collapse", "mask_support"):
         n, tot = ctx.kernel_stats(name)
         stats[name] = (n, tot)
     ctx.set_kernel_timing(False)
     k_default = 8 if args.batch == 0 else args.batch
     k_eff = max(1, min(k_default, 8, F))
-    alg, alg_total = algorithmic_bytes(roi.width, roi.height, F, k_eff)
+    alg, alg_total = algorithmic_bytes(roi.width, roi.height, F, k_eff,
+                                       "cache" if mode_used["mode"] == "cache" else "recompute")
     dom = max(stats, key=lambda n: stats[n][1])
     n_dom, ms_dom = stats[dom]
     peak, peak_kind = measured_hbm_peak()
@@ -355,7 +366,7 @@ def main():
                 "alg_bytes_per_launch": per_launch, "launches_per_step": n_dom,
                 "avg_launch_ms": ms_dom / max(1, n_dom)}
     kernel_table = {n: {"launches": v[0], "total_ms": round(v[1], 4), "share": round(v[1] / max(1e-9, sum(
-        x[1] for x in stats.values())), 4), "alg_bytes": alg[n]} for n, v in stats.items()}
+        x[1] for x in stats.values())), 4), "alg_bytes": alg[n]} for n, v in stats.items() if v[0] > 0}
     pipeline = {"alg_bytes_per_frame_pixel": alg_total / px,
                 "achieved_gbs": alg_total / (ms / 1e3) / 1e9,
                 "frac": (alg_total / (ms / 1e3) / 1e9) / peak}
@@ -401,7 +412,7 @@ def main():
         line = {"metric": METRIC, "value": round(value, 2), "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": round(ms, 4), "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-                "config": workload_config(args, roi, k_eff),
+                "config": dict(workload_config(args, roi, k_eff), pass2=mode_used["mode"]),
                 "e2e": e2e, "gpu_launches": launches, "clocks": clock_info, "roofline": roofline,
                 "cpu_baseline": cpu, "kernels": kernel_table, "pipeline_roofline": pipeline}
         print(json.dumps(line), flush=True)

@@ -27,7 +27,7 @@ EXPORTED = (
     "fs_pose_default", "fs_compute_roi", "fs_inverse_map_points", "fs_forward_map_points", "fs_exact_expand_divisor",
     "fs_remap_frame", "fs_remap_frame_device",
     "fs_stack_begin", "fs_stack_add_frame", "fs_stack_add_frame_device", "fs_stack_finish",
-    "fs_stack_finish_device", "fs_stack_set_base_output", "fs_stack_output_size", "fs_stack_destroy", "fs_fuse_stack",
+    "fs_stack_finish_device", "fs_stack_set_base_output", "fs_stack_pass2_mode", "fs_stack_output_size", "fs_stack_destroy", "fs_fuse_stack",
     "fs_synth_frame_device", "fs_synth_pose",
 )
 
@@ -109,6 +109,7 @@ def _bind(L):
     L.fs_stack_finish_device.argtypes = [vp, FETCH_CB, vp, vp, sz]
     L.fs_stack_output_size.argtypes = [vp, P(u32), P(u32)]
     L.fs_stack_set_base_output.argtypes = [vp, vp, sz]
+    L.fs_stack_pass2_mode.argtypes = [vp]
     L.fs_stack_destroy.argtypes = [vp]
     L.fs_fuse_stack.argtypes = [ctx, P(FsStackDesc), P(vp), P(sz), P(FsPose), vp, sz]
     L.fs_synth_frame_device.argtypes = [ctx, u64, i32, u32, u32, u32, u32, vp, sz, P(FsPose)]

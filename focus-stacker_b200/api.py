@@ -301,6 +301,13 @@ class PyramidContrastStack:
         self.out_width, self.out_height = w.value, hh.value
         self._keep = []
 
+    PASS2_MODES = ("cache", "resident", "refetch")
+
+    @property
+    def pass2_mode(self) -> str:
+        """Where pass 2 takes its frames from (chosen from the HBM budget)."""
+        return self.PASS2_MODES[L().fs_stack_pass2_mode(self.handle)]
+
     def set_base_output(self, dst, row_stride_elems: int):
         """Also write the collapsed FP32 base (RGB, device buffer) during finish."""
         self._keep.append(dst)

@@ -141,12 +141,23 @@ int64_t round_up(int64_t v, int64_t m) { return (v + m - 1) / m * m; }
 }  // namespace
 
 // ===================================================================== stack
+// Pass-2 source of a stack, chosen at fs_stack_begin from the HBM budget:
+//  CACHE     pass 1 keeps every remapped frame (RGBA u32) and its weight on
+//            the device; pass 2 reads them (the reference's cached path,
+//            src/stack/pipeline.zig:454-457, 515-560);
+//  RESIDENT  frames stay on the device and pass 2 remaps them again;
+//  REFETCH   frames are only staged; pass 2 asks the caller for them again
+//            and remaps them (src/stack/pipeline.zig:561-597).
+enum Pass2Mode { P2_CACHE = 0, P2_RESIDENT = 1, P2_REFETCH = 2 };
+
 struct fs_stack {
   fs_ctx* ctx = nullptr;
   fs_stack_desc d;
   fs_rect roi;
   uint32_t W = 0, H = 0, L = 0, K = 1, border = 2;
   bool aligned = false;
+  int storage = FS_STORAGE_F32;
+  Pass2Mode mode = P2_CACHE;
   std::vector<uint32_t> lw, lh;
   std::vector<int64_t> pitch;  // per level, elements (f32) == bytes (u8)
   float* norm = nullptr;
@@ -154,6 +165,8 @@ struct fs_stack {
   std::vector<uint8_t*> sm;    // mask support, level l (sm[0] == uni)
   std::vector<float*> acc;     // per level, 3 planes
   std::vector<std::vector<LevelPlanes>> slot;  // [k][l], l = 1 .. L-2
+  std::vector<FramePlanes> cache;              // CACHE: per frame
+  std::vector<FramePlanes> p2;                 // RESIDENT / REFETCH: per batch slot (K)
   uint8_t* out_dev = nullptr;
   std::vector<Alloc> allocs;
   struct Frame {
@@ -164,10 +177,9 @@ struct fs_stack {
     fs_pose pose;
   };
   std::vector<Frame> frames;
-  std::vector<uint8_t*> staging;  // refetch buffers for pass 2 (K), when frames are not resident
+  std::vector<uint8_t*> staging;  // transient frame buffers (K)
   int64_t frame_pitch = 0;        // pitch of owned frame copies
   size_t frame_bytes = 0;
-  bool keep_frames = true;
   size_t pass1_done = 0;          // frames whose pass 1 has been launched
   bool finished = false;
   cudaEvent_t copy_done = nullptr;
@@ -204,26 +216,39 @@ bool build_frame_in(fs_stack* s, const fs_stack::Frame& fr, FrameIn* fi, std::st
   return true;
 }
 
-int launch_pass1_batch(fs_stack* s, size_t begin, size_t end) {
-  Pass1Args a;
+// remap + weights for frames [begin, end): pass 1 (accumulate, and keep
+// the planes in CACHE mode) or pass 2 of RESIDENT / REFETCH (planes into the
+// batch slots, no accumulation).
+int launch_remap_weights_batch(fs_stack* s, const std::vector<fs_stack::Frame>& frames, size_t begin, size_t end,
+                               bool pass1) {
+  RemapWeightArgs a;
   std::memset(&a, 0, sizeof(a));
   a.W = (int32_t)s->W;
   a.H = (int32_t)s->H;
-  a.border = (int32_t)s->border;
   a.window_ok = (s->W >= s->d.contrast_window && s->H >= s->d.contrast_window) ? 1 : 0;
   a.K = (int32_t)(end - begin);
+  a.accumulate = pass1 ? 1 : 0;
   a.first = begin == 0 ? 1 : 0;
   a.norm = s->norm;
-  a.norm_pitch = s->pitch[0];
   a.uni = s->uni;
-  a.uni_pitch = s->pitch[0];
+  a.pitch = s->pitch[0];
   for (size_t k = begin; k < end; ++k) {
     std::string why;
-    if (!build_frame_in(s, s->frames[k], &a.f[k - begin], &why)) return set_err(s->ctx, FS_ERR_INVALID, why);
+    if (!build_frame_in(s, frames[k], &a.f[k - begin], &why)) return set_err(s->ctx, FS_ERR_INVALID, why);
+    if (pass1) {
+      if (s->mode == P2_CACHE) a.out[k - begin] = s->cache[k];
+    } else {
+      a.out[k - begin] = s->p2[k - begin];
+    }
   }
-  cudaError_t e = timed(s->ctx, "pass1", [&] { return launch_pass1(a, s->ctx->stream); });
-  if (e != cudaSuccess) return cuda_err(s->ctx, e, "pass1 launch");
+  cudaError_t e = timed(s->ctx, pass1 ? "pass1" : "remap_weights",
+                        [&] { return launch_remap_weights(a, (int)s->border, s->ctx->stream); });
+  if (e != cudaSuccess) return cuda_err(s->ctx, e, "remap/weights launch");
   return FS_OK;
+}
+
+int launch_pass1_batch(fs_stack* s, size_t begin, size_t end) {
+  return launch_remap_weights_batch(s, s->frames, begin, end, true);
 }
 
 int run_pending_pass1(fs_stack* s, bool flush) {
@@ -472,8 +497,9 @@ int fs_stack_begin(fs_ctx* ctx, const fs_stack_desc* desc, fs_stack** out) {
   if (d.src_width == 0 || d.src_height == 0 || d.frame_count == 0) return set_err(ctx, FS_ERR_INVALID, "empty stack");
   if (d.contrast_window < 3 || (d.contrast_window & 1) == 0)
     return set_err(ctx, FS_ERR_INVALID, "contrast window must be odd and >= 3");
-  if (d.contrast_window > 31) return set_err(ctx, FS_ERR_UNSUPPORTED, "contrast window larger than 31");
-  if (d.level_storage != FS_STORAGE_F32) return set_err(ctx, FS_ERR_UNSUPPORTED, "level storage other than FP32");
+  if (d.contrast_window > 2 * kMaxBorder + 1) return set_err(ctx, FS_ERR_UNSUPPORTED, "contrast window larger than 15");
+  if (d.level_storage != FS_STORAGE_F32 && d.level_storage != FS_STORAGE_F16 && d.level_storage != FS_STORAGE_BF16)
+    return set_err(ctx, FS_ERR_INVALID, "unknown level storage");
   bool aligned = d.input_is_aligned != 0;
   if (aligned ? (d.channels != 3 && d.channels != 4) : d.channels != 3)
     return set_err(ctx, FS_ERR_INVALID, "channels must be 3 (RGB source) or 3/4 (aligned RGB/RGBA)");
@@ -486,6 +512,7 @@ int fs_stack_begin(fs_ctx* ctx, const fs_stack_desc* desc, fs_stack** out) {
   s->d = d;
   s->roi = roi;
   s->aligned = aligned;
+  s->storage = d.level_storage;
   s->W = (uint32_t)(roi.right - roi.left);
   s->H = (uint32_t)(roi.bottom - roi.top);
   s->L = level_count(s->W, s->H);
@@ -506,7 +533,7 @@ int fs_stack_begin(fs_ctx* ctx, const fs_stack_desc* desc, fs_stack** out) {
   };
   int rc;
   void* p;
-  size_t n0 = (size_t)s->pitch[0] * s->H;
+  const size_t n0 = (size_t)s->pitch[0] * s->H;
   if ((rc = stack_alloc(s, n0 * 4, &p)) != FS_OK) return fail(rc);
   s->norm = (float*)p;
   if ((rc = stack_alloc(s, n0, &p)) != FS_OK) return fail(rc);
@@ -520,25 +547,42 @@ int fs_stack_begin(fs_ctx* ctx, const fs_stack_desc* desc, fs_stack** out) {
     if ((rc = stack_alloc(s, (size_t)s->pitch[l] * s->lh[l] * 3 * 4, &p)) != FS_OK) return fail(rc);
     s->acc.push_back((float*)p);
   }
+  const size_t esz = s->storage == FS_STORAGE_F32 ? 4 : 2;
   s->slot.assign(s->K, std::vector<LevelPlanes>(s->L));
   for (uint32_t kk = 0; kk < s->K; ++kk) {
     for (uint32_t l = 1; l + 1 < s->L; ++l) {
-      size_t plane = (size_t)s->pitch[l] * s->lh[l];
+      const size_t plane = (size_t)s->pitch[l] * s->lh[l];
       LevelPlanes lp;
-      if ((rc = stack_alloc(s, plane * 4 * 4 + plane, &p)) != FS_OK) return fail(rc);
-      lp.g = (float*)p;
-      lp.m = lp.g + 3 * plane;
-      lp.s = (uint8_t*)(lp.m + plane);
+      if ((rc = stack_alloc(s, plane * esz * 4 + plane, &p)) != FS_OK) return fail(rc);
+      lp.g = p;
+      lp.m = (uint8_t*)p + plane * esz * 3;
+      lp.s = (uint8_t*)p + plane * esz * 4;
       lp.plane = (int64_t)plane;
       s->slot[kk][l] = lp;
     }
   }
   if ((rc = stack_alloc(s, (size_t)s->W * s->H * 3, &p)) != FS_OK) return fail(rc);
   s->out_dev = (uint8_t*)p;
-  // frame residency: keep every frame on the device when the budget allows
+  // pass-2 source: cache the pass-1 planes (8 B per pixel per frame) when the
+  // budget allows, else keep the frames, else refetch them
   s->frame_pitch = round_up((int64_t)d.src_width * d.channels, 16);
   s->frame_bytes = (size_t)s->frame_pitch * d.src_height;
-  s->keep_frames = ctx->held + s->frame_bytes * d.frame_count <= ctx->budget;
+  const size_t planes_bytes = n0 * 8;
+  const size_t staging_bytes = s->frame_bytes * s->K;
+  if (ctx->held - ctx->pooled + planes_bytes * d.frame_count + staging_bytes <= ctx->budget) {
+    s->mode = P2_CACHE;
+    for (uint32_t f = 0; f < d.frame_count; ++f) {
+      if ((rc = stack_alloc(s, planes_bytes, &p)) != FS_OK) return fail(rc);
+      s->cache.push_back(FramePlanes{(uint32_t*)p, (float*)((uint8_t*)p + n0 * 4)});
+    }
+  } else {
+    const bool keep = ctx->held - ctx->pooled + planes_bytes * s->K + s->frame_bytes * d.frame_count <= ctx->budget;
+    s->mode = keep ? P2_RESIDENT : P2_REFETCH;
+    for (uint32_t kk = 0; kk < s->K; ++kk) {
+      if ((rc = stack_alloc(s, planes_bytes, &p)) != FS_OK) return fail(rc);
+      s->p2.push_back(FramePlanes{(uint32_t*)p, (float*)((uint8_t*)p + n0 * 4)});
+    }
+  }
   cudaEventCreateWithFlags(&s->copy_done, cudaEventDisableTiming);
   *out = s;
   return FS_OK;
@@ -550,7 +594,7 @@ static int add_frame_impl(fs_stack* s, const void* pixels, size_t row_stride, co
   if (s->finished) return set_err(ctx, FS_ERR_STATE, "stack already finished");
   if (s->frames.size() >= s->d.frame_count) return set_err(ctx, FS_ERR_STATE, "more frames than frame_count");
   if (!s->aligned && !pose) return set_err(ctx, FS_ERR_INVALID, "pose required for source frames");
-  size_t row_bytes = (size_t)s->d.src_width * s->d.channels;
+  const size_t row_bytes = (size_t)s->d.src_width * s->d.channels;
   if (row_stride < row_bytes) return set_err(ctx, FS_ERR_MISMATCH, "row stride smaller than the stack's row");
   cudaSetDevice(ctx->device);
   fs_stack::Frame fr;
@@ -559,18 +603,17 @@ static int add_frame_impl(fs_stack* s, const void* pixels, size_t row_stride, co
     fr.px = (const uint8_t*)pixels;
     fr.pitch = (int64_t)row_stride;
   } else {
-    // copy into a device buffer (kept for pass 2 when the budget allows)
-    bool keep = s->keep_frames;
     uint8_t* buf = nullptr;
-    if (keep) {
+    if (s->mode == P2_RESIDENT) {
+      // kept for pass 2
       void* p;
       int rc = stack_alloc(s, s->frame_bytes, &p);
       if (rc != FS_OK) return rc;
       buf = (uint8_t*)p;
       fr.owned = true;
     } else {
-      // transient: reuse a staging slot of the current pass-1 batch
-      size_t slot = s->frames.size() % s->K;
+      // staged for pass 1 only: one buffer per frame of the current batch
+      const size_t slot = s->frames.size() % s->K;
       while (s->staging.size() <= slot) {
         void* p;
         int rc = stack_alloc(s, s->frame_bytes, &p);
@@ -578,15 +621,18 @@ static int add_frame_impl(fs_stack* s, const void* pixels, size_t row_stride, co
         s->staging.push_back((uint8_t*)p);
       }
       if (slot == 0 && s->frames.size() > 0) {
-        // the previous batch must have consumed the slots
+        // the previous batch's pass 1 must be done with the staging buffers
         cudaError_t e = cudaStreamSynchronize(ctx->stream);
         if (e != cudaSuccess) return cuda_err(ctx, e, "synchronize");
       }
       buf = s->staging[slot];
       fr.resident = false;
     }
-    cudaError_t e = cudaMemcpy2DAsync(buf, (size_t)s->frame_pitch, pixels, row_stride, row_bytes, s->d.src_height,
-                                      cudaMemcpyHostToDevice, ctx->copy);
+    // one linear copy when the rows are packed alike (faster than a pitched copy)
+    cudaError_t e = row_stride == (size_t)s->frame_pitch
+                        ? cudaMemcpyAsync(buf, pixels, row_stride * s->d.src_height, cudaMemcpyHostToDevice, ctx->copy)
+                        : cudaMemcpy2DAsync(buf, (size_t)s->frame_pitch, pixels, row_stride, row_bytes,
+                                            s->d.src_height, cudaMemcpyHostToDevice, ctx->copy);
     if (e != cudaSuccess) return cuda_err(ctx, e, "frame upload");
     cudaEventRecord(s->copy_done, ctx->copy);
     cudaStreamWaitEvent(ctx->stream, s->copy_done, 0);
@@ -634,43 +680,41 @@ static int finish_impl(fs_stack* s, fs_frame_fetch_cb refetch, void* user, void*
   }
   // pass 2 in batches of K frames
   const size_t N = s->frames.size();
-  std::vector<fs_stack::Frame> batch_frames;
+  std::vector<fs_stack::Frame> frames = s->frames;
   for (size_t begin = 0; begin < N; begin += s->K) {
-    size_t end = std::min(N, begin + s->K);
-    batch_frames.assign(s->frames.begin() + begin, s->frames.begin() + end);
-    for (size_t k = begin; k < end; ++k) {
-      fs_stack::Frame& fr = batch_frames[k - begin];
-      if (fr.resident) continue;
-      // the frame was only staged for pass 1: fetch it again from the host
-      // (the reference re-decodes, src/stack/pipeline.zig:561-597)
-      if (!refetch) return set_err(ctx, FS_ERR_STATE, "frame not resident and no refetch callback");
-      const void* hp = nullptr;
-      size_t hs = 0;
-      if (refetch(user, (uint32_t)k, &hp, &hs) != 0 || !hp) return set_err(ctx, FS_ERR_INVALID, "refetch callback failed");
-      if (hs < (size_t)s->d.src_width * s->d.channels) return set_err(ctx, FS_ERR_MISMATCH, "refetched row stride too small");
-      uint8_t* buf = s->staging[(k - begin) % s->staging.size()];
-      e = cudaMemcpy2DAsync(buf, (size_t)s->frame_pitch, hp, hs, (size_t)s->d.src_width * s->d.channels,
-                            s->d.src_height, cudaMemcpyHostToDevice, st);
-      if (e != cudaSuccess) return cuda_err(ctx, e, "frame refetch upload");
-      e = cudaStreamSynchronize(st);  // the callback's buffer may be reused after it returns again
-      if (e != cudaSuccess) return cuda_err(ctx, e, "frame refetch upload");
-      fr.px = buf;
-      fr.pitch = s->frame_pitch;
+    const size_t end = std::min(N, begin + s->K);
+    if (s->mode != P2_CACHE) {
+      for (size_t k = begin; k < end; ++k) {
+        fs_stack::Frame& fr = frames[k];
+        if (fr.resident) continue;
+        // the frame was only staged for pass 1: fetch it again from the host
+        // (the reference re-decodes, src/stack/pipeline.zig:561-597)
+        if (!refetch) return set_err(ctx, FS_ERR_STATE, "frame not resident and no refetch callback");
+        const void* hp = nullptr;
+        size_t hs = 0;
+        if (refetch(user, (uint32_t)k, &hp, &hs) != 0 || !hp)
+          return set_err(ctx, FS_ERR_INVALID, "refetch callback failed");
+        if (hs < (size_t)s->d.src_width * s->d.channels)
+          return set_err(ctx, FS_ERR_MISMATCH, "refetched row stride too small");
+        uint8_t* buf = s->staging[(k - begin) % s->staging.size()];
+        e = cudaMemcpy2DAsync(buf, (size_t)s->frame_pitch, hp, hs, (size_t)s->d.src_width * s->d.channels,
+                              s->d.src_height, cudaMemcpyHostToDevice, st);
+        if (e != cudaSuccess) return cuda_err(ctx, e, "frame refetch upload");
+        e = cudaStreamSynchronize(st);  // the callback's buffer may be reused after it returns again
+        if (e != cudaSuccess) return cuda_err(ctx, e, "frame refetch upload");
+        fr.px = buf;
+        fr.pitch = s->frame_pitch;
+      }
+      rc = launch_remap_weights_batch(s, frames, begin, end, false);
+      if (rc != FS_OK) return rc;
     }
     LevelArgs a;
     std::memset(&a, 0, sizeof(a));
     a.levels = (int32_t)s->L;
     a.K = (int32_t)(end - begin);
-    a.border = (int32_t)s->border;
-    a.window_ok = (s->W >= s->d.contrast_window && s->H >= s->d.contrast_window) ? 1 : 0;
     a.inv_count = 1.0f / (float)N;
     a.norm = s->norm;
-    a.uni = s->uni;
-    for (size_t k = begin; k < end; ++k) {
-      std::string why;
-      if (!build_frame_in(s, batch_frames[k - begin], &a.f[k - begin], &why))
-        return set_err(ctx, FS_ERR_INVALID, why);
-    }
+    for (size_t k = begin; k < end; ++k) a.in0[k - begin] = s->mode == P2_CACHE ? s->cache[k] : s->p2[k - begin];
     for (uint32_t l = 0; l + 1 < s->L || (s->L == 1 && l == 0); ++l) {
       a.level = (int32_t)l;
       a.wl = (int32_t)s->lw[l];
@@ -684,7 +728,6 @@ static int finish_impl(fs_stack* s, fs_frame_fetch_cb refetch, void* user, void*
         a.wn = (int32_t)s->lw[l + 1];
         a.hn = (int32_t)s->lh[l + 1];
         a.pitch_n = s->pitch[l + 1];
-        a.sm_n = s->sm[l + 1];
         a.acc_n = s->acc[l + 1];
         a.acc_plane_n = s->pitch[l + 1] * s->lh[l + 1];
       } else {
@@ -695,8 +738,8 @@ static int finish_impl(fs_stack* s, fs_frame_fetch_cb refetch, void* user, void*
         if (l >= 1) a.in[k] = s->slot[k][l];
         if (l + 1 < s->L - 1) a.out[k] = s->slot[k][l + 1];
       }
-      if (l == 0) e = timed(ctx, "level0", [&] { return launch_level0(a, st); });
-      else e = timed(ctx, "level", [&] { return launch_level(a, st); });
+      if (l == 0) e = timed(ctx, "level0", [&] { return launch_level0(a, s->storage, st); });
+      else e = timed(ctx, "level", [&] { return launch_level(a, s->storage, st); });
       if (e != cudaSuccess) return cuda_err(ctx, e, "level launch");
       if (s->L == 1) break;
     }
@@ -730,19 +773,19 @@ static int finish_impl(fs_stack* s, fs_frame_fetch_cb refetch, void* user, void*
     e = timed(ctx, "collapse", [&] { return launch_collapse(c, st); });
     if (e != cudaSuccess) return cuda_err(ctx, e, "collapse");
   }
-  if (device_out) {
-    e = cudaMemcpy2DAsync(out, out_stride, s->out_dev, (size_t)s->W * 3, (size_t)s->W * 3, s->H,
-                          cudaMemcpyDeviceToDevice, st);
-  } else {
-    e = cudaMemcpy2DAsync(out, out_stride, s->out_dev, (size_t)s->W * 3, (size_t)s->W * 3, s->H,
-                          cudaMemcpyDeviceToHost, st);
-  }
+  const cudaMemcpyKind kind = device_out ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+  if (out_stride == (size_t)s->W * 3)
+    e = cudaMemcpyAsync(out, s->out_dev, (size_t)s->W * 3 * s->H, kind, st);
+  else
+    e = cudaMemcpy2DAsync(out, out_stride, s->out_dev, (size_t)s->W * 3, (size_t)s->W * 3, s->H, kind, st);
   if (e != cudaSuccess) return cuda_err(ctx, e, "output copy");
   e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) return cuda_err(ctx, e, "fusion");
   s->finished = true;
   return FS_OK;
 }
+
+int fs_stack_pass2_mode(const fs_stack* s) { return s ? (int)s->mode : -1; }
 
 int fs_stack_finish(fs_stack* stack, fs_frame_fetch_cb refetch, void* user, void* out_pixels, size_t out_stride) {
   return finish_impl(stack, refetch, user, out_pixels, out_stride, false);

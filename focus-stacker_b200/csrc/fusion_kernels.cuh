@@ -11,9 +11,10 @@
 namespace fs {
 
 static constexpr int kMaxBatch = 8;   // frames per pass over per-pixel state (K)
-static constexpr int kTileW = 64;     // level-l tile (output pixels) of the level kernels
+static constexpr int kTileW = 64;     // output tile of every 2-D kernel
 static constexpr int kTileH = 32;
 static constexpr int kThreads = 256;
+static constexpr int kMaxBorder = 7;  // contrast windows 3 .. 15
 
 // One input frame of a batch.
 struct FrameIn {
@@ -21,25 +22,34 @@ struct FrameIn {
   Warp warp;      // kind WARP_ALIGNED for aligned input
 };
 
-// Planes of one pyramid level (FP32 planar RGB, u8 support, FP32 mask).
-struct LevelPlanes {
-  float* g;        // 3 planes: g + c * plane
-  uint8_t* s;      // image support (0/1)
-  float* m;        // normalised mask
-  int64_t plane;   // elements per colour plane (h * pitch)
+// Pass-1 product of one frame kept for pass 2: the remapped frame as packed
+// RGBA words (R | G << 8 | B << 16 | A << 24) and its alpha-weighted local
+// contrast, on the level-0 grid.
+struct FramePlanes {
+  uint32_t* rgba;
+  float* w;
 };
 
-struct Pass1Args {
+// Planes of one pyramid level l >= 1 of one frame: RGB Gaussian (3 planes),
+// normalised mask, image support.  g / m hold `storage` elements.
+struct LevelPlanes {
+  void* g;
+  void* m;
+  uint8_t* s;
+  int64_t plane;  // elements per colour plane (h * pitch)
+};
+
+struct RemapWeightArgs {
   int32_t W, H;          // ROI (level 0) size
-  int32_t border;        // contrast window / 2
   int32_t window_ok;     // W >= window && H >= window
   int32_t K;             // frames in this batch
-  int32_t first;         // 1: weight sums / union start at zero
+  int32_t accumulate;    // 1: add weights into the weight sum / union (pass 1)
+  int32_t first;         // 1: the sums start at zero
   float* norm;
-  int64_t norm_pitch;    // elements
   uint8_t* uni;
-  int64_t uni_pitch;     // bytes
+  int64_t pitch;         // level-0 row pitch (elements; bytes for u8 planes)
   FrameIn f[kMaxBatch];
+  FramePlanes out[kMaxBatch];  // null members: do not store
 };
 
 struct LevelArgs {
@@ -47,21 +57,18 @@ struct LevelArgs {
   int32_t levels;        // L
   int32_t wl, hl;        // level l size
   int32_t wn, hn;        // level l + 1 size
-  int64_t pitch_l, pitch_n;   // elements per row (f32 planes); u8 planes use the same pitch in bytes
+  int64_t pitch_l, pitch_n;   // elements per row; u8 planes use the same pitch in bytes
   int32_t exact_expand;  // max(wl, hl) <= 512: no-wrap expand back to level l
   int32_t K;
-  // level-0 only (frame input)
-  int32_t border, window_ok;
+  // level 0
   float inv_count;       // 1 / N (f32), the reference's default weight
   const float* norm;
-  const uint8_t* uni;
-  FrameIn f[kMaxBatch];
+  FramePlanes in0[kMaxBatch];
   // level >= 1 inputs (per frame in batch)
   LevelPlanes in[kMaxBatch];
   // outputs at level l + 1 (per frame in batch)
   LevelPlanes out[kMaxBatch];
   const uint8_t* sm_l;   // mask support at level l (union at level 0)
-  const uint8_t* sm_n;   // mask support at level l + 1
   float* acc_l;          // accumulator level l, 3 planes
   int64_t acc_plane_l;
   float* acc_n;          // accumulator level l + 1 (used when l + 1 is the top level)
@@ -99,13 +106,9 @@ struct RemapArgs {
   int32_t dst_ch;     // channels + 1
 };
 
-size_t pass1_smem_bytes(int border);
-size_t level0_smem_bytes(int border);
-size_t level_smem_bytes();
-
-cudaError_t launch_pass1(const Pass1Args& a, cudaStream_t s);
-cudaError_t launch_level0(const LevelArgs& a, cudaStream_t s);
-cudaError_t launch_level(const LevelArgs& a, cudaStream_t s);
+cudaError_t launch_remap_weights(const RemapWeightArgs& a, int border, cudaStream_t s);
+cudaError_t launch_level0(const LevelArgs& a, int storage, cudaStream_t s);
+cudaError_t launch_level(const LevelArgs& a, int storage, cudaStream_t s);
 cudaError_t launch_collapse(const CollapseArgs& a, cudaStream_t s);
 cudaError_t launch_mask_support(const MaskSupportArgs& a, cudaStream_t s);
 cudaError_t launch_remap(const RemapArgs& a, cudaStream_t s);
@@ -118,7 +121,7 @@ void synth_pose(uint64_t seed, int scene, uint32_t width, uint32_t height, uint3
 int synth_render(uint64_t seed, int scene, uint32_t width, uint32_t height, uint32_t frame, uint32_t frame_count,
                  void* dev_out, size_t out_stride, fs_pose* pose_out, cudaStream_t stream, const char** why);
 
-// Host evaluation of the no-wrap expand divisor (shared with the kernels).
+// Normaliser of the no-wrap expand (shared by host checks and the kernels).
 FS_HD float exact_expand_divisor(int x, int y, int sw, int sh) {
   const int j = x >> 1, q = y >> 1;
   const bool xe = (x & 1) == 0, ye = (y & 1) == 0;

@@ -52,6 +52,21 @@ __device__ __forceinline__ void load_rgb(const SrcImage& s, int x, int y, float 
   }
 }
 
+// Taps of the fast path as biased floats 2^23 + v (exact, one OR): the
+// differences of two taps are exact without removing the bias.
+__device__ __forceinline__ void load_rgb_biased(const SrcImage& s, int x, int y, float v[3]) {
+  const uint8_t* p = s.px + (int64_t)y * s.pitch + (int64_t)x * s.ch;
+  if (s.ch == 3) {
+    v[0] = __uint_as_float(0x4B000000u | (uint32_t)__ldg(p));
+    v[1] = __uint_as_float(0x4B000000u | (uint32_t)__ldg(p + 1));
+    v[2] = __uint_as_float(0x4B000000u | (uint32_t)__ldg(p + 2));
+  } else {
+    v[0] = __uint_as_float(0x4B000000u | (uint32_t)__ldg(p));
+    v[1] = v[0];
+    v[2] = v[0];
+  }
+}
+
 // Block anchor for the fast path.
 struct Anchor {
   int32_t ix, iy;        // integer part of the anchor's source position
@@ -252,17 +267,17 @@ __device__ __forceinline__ uint32_t sample_fast(const Warp& w, const SrcImage& s
   // cannot change which sampler the reference takes
   if (x0 < 1 || y0 < 1 || x0 > s.w - 3 || y0 > s.h - 3) return sample_exact(w, s, X, Y);
   float v00[3], v10[3], v01[3], v11[3];
-  load_rgb(s, x0, y0, v00);
-  load_rgb(s, x0 + 1, y0, v10);
-  load_rgb(s, x0, y0 + 1, v01);
-  load_rgb(s, x0 + 1, y0 + 1, v11);
+  load_rgb_biased(s, x0, y0, v00);
+  load_rgb_biased(s, x0 + 1, y0, v10);
+  load_rgb_biased(s, x0, y0 + 1, v01);
+  load_rgb_biased(s, x0 + 1, y0 + 1, v11);
   float fxy = fx * fy;
   uint32_t o[3];
   bool tie = false;
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
     float d10 = v10[c] - v00[c], d01 = v01[c] - v00[c], d11 = (v11[c] - v10[c]) - d01;
-    float v = fmaf(fx, d10, v00[c]);
+    float v = fmaf(fx, d10, v00[c] - 8388608.0f);
     v = fmaf(fy, d01, v);
     v = fmaf(fxy, d11, v);
     float k = floorf(v);

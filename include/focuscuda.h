@@ -81,7 +81,8 @@ int fs_ctx_stream(const fs_ctx* ctx, void** stream);
 /* Kernel accounting: number of kernels this context launched so far, and
  * (when timing is enabled) per-kernel launch counts and device time measured
  * with CUDA events on the launching stream.  Kernel names: "pass1",
- * "level0", "level", "collapse", "mask_support", "remap".  Enabling or
+ * "remap_weights" (pass-2 re-remap), "level0", "level", "collapse",
+ * "mask_support", "remap".  Enabling or
  * disabling timing clears the recorded times.  Not part of the reference. */
 uint64_t fs_ctx_launch_count(const fs_ctx* ctx);
 int fs_ctx_set_kernel_timing(fs_ctx* ctx, int enable);
@@ -181,6 +182,13 @@ int fs_stack_finish_device(fs_stack* stack, fs_frame_fetch_cb refetch, void* use
  * finish.  Used to measure error against FP64 evaluations on the 16-bit
  * grid.  Not part of the reference. */
 int fs_stack_set_base_output(fs_stack* stack, float* dev_base, size_t row_stride_elems);
+
+/* Where pass 2 of the stack takes its frames from, chosen by fs_stack_begin
+ * from the HBM budget: 0 = pass-1 planes kept on the device (remapped RGBA +
+ * weight per frame, the reference's cached path), 1 = frames kept on the
+ * device and remapped again, 2 = frames fetched again through the finish
+ * callback and remapped again. */
+int fs_stack_pass2_mode(const fs_stack* stack);
 
 /* Output size of the stack (the ROI). */
 int fs_stack_output_size(const fs_stack* stack, uint32_t* width, uint32_t* height);

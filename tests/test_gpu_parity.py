@@ -245,11 +245,13 @@ def test_refetch_path_matches_resident(torch, ctx):
     ctx.trim()
     before = ctx.device_bytes()
     probe = fsb.PyramidContrastStack(ctx, W, H, F, roi=roi, frames_per_batch=2)
-    state = ctx.device_bytes() - before
+    n0 = (roi.width + 31) // 32 * 32 * roi.height
+    state = ctx.device_bytes() - before - F * n0 * 8  # without the per-frame pass-1 planes
     probe.close()
     ctx.trim()
-    small = fsb.Context(0, hbm_budget_bytes=state + 3 * W * H * 3 + 4096)
+    small = fsb.Context(0, hbm_budget_bytes=state + 2 * n0 * 8 + 3 * W * H * 3 + 4096)
     st = fsb.PyramidContrastStack(small, W, H, F, roi=roi, frames_per_batch=2)
+    assert st.pass2_mode == "refetch"
     for f, p in zip(frames, poses):
         st.add_frame(f, p)
     calls = []
@@ -263,6 +265,45 @@ def test_refetch_path_matches_resident(torch, ctx):
     small.close()
     assert calls == list(range(F))
     assert np.array_equal(out, ref)
+
+
+def test_pass2_modes_give_identical_results(torch, ctx):
+    # cache (pass-1 planes kept), resident (frames kept, remapped again) and
+    # refetch (frames fetched again) must produce the same bytes
+    W, H, F = 240, 160, 6
+    frames, poses = synth_stack(torch, ctx, W, H, F, seed=12)
+    roi = fsb.compute_common_overlap_roi([True] * F, [W] * F, [H] * F, poses)
+    results = {}
+    ctx.trim()
+    before = ctx.device_bytes()
+    probe = fsb.PyramidContrastStack(ctx, W, H, F, roi=roi, frames_per_batch=3)
+    assert probe.pass2_mode == "cache"
+    probe.close()
+    ctx.trim()
+    n0 = (roi.width + 31) // 32 * 32 * roi.height
+    frame_b = (W * 3 + 15) // 16 * 16 * H
+    for budget_extra, want in ((None, "cache"), ("resident", "resident"), ("refetch", "refetch")):
+        if budget_extra is None:
+            c = ctx
+        else:
+            # stack state without the per-frame planes: measure it with a tiny stack of the same geometry
+            c = fsb.Context(0, hbm_budget_bytes=1 << 40)
+            st0 = fsb.PyramidContrastStack(c, W, H, F, roi=roi, frames_per_batch=3)
+            state = c.device_bytes() - F * n0 * 8
+            st0.close()
+            c.close()
+            extra = 3 * n0 * 8 + F * frame_b + 3 * frame_b + 4096 if want == "resident" else 3 * n0 * 8 + 3 * frame_b + 4096
+            c = fsb.Context(0, hbm_budget_bytes=state + extra)
+        st = fsb.PyramidContrastStack(c, W, H, F, roi=roi, frames_per_batch=3)
+        assert st.pass2_mode == want
+        for f, p in zip(frames, poses):
+            st.add_frame(f, p)
+        results[want] = st.finish(refetch=lambda i: frames[i])
+        st.close()
+        if c is not ctx:
+            c.close()
+    assert np.array_equal(results["cache"], results["resident"])
+    assert np.array_equal(results["cache"], results["refetch"])
 
 
 def test_stack_errors(torch, ctx):
