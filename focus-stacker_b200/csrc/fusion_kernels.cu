@@ -81,8 +81,19 @@ __device__ __forceinline__ float window_stddev(uint32_t packed, uint32_t s2, con
 // get 0 (no support).  Optionally also the contrast words.  Work unit: 8x4
 // pixel blocks, one warp each; lane j of a warp forms the double-float
 // anchor of the warp's j-th block and hands it over by shuffle.
+constexpr int kExactQueue = 256;  // deferred exact samples per CTA and frame
+
+// Shared scratch of fill_region: queue of samples the fast path could not
+// decide, processed together after the fast pass so that one lane's tie does
+// not hold its whole warp on the (long) exact path.
+struct ExactQueue {
+  uint32_t count;
+  uint32_t item[kExactQueue];  // ry << 16 | rx
+};
+
 template <int RW, int RH>
-__device__ void fill_region(const FrameIn& f, int W, int H, int rx0, int ry0, uint32_t* reg, uint32_t* kv) {
+__device__ void fill_region(const FrameIn& f, int W, int H, int rx0, int ry0, uint32_t* reg, uint32_t* kv,
+                            ExactQueue* q) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = NT / 32;
   if (f.warp.kind == WARP_ALIGNED) {
     for (int i = threadIdx.x; i < RW * RH; i += NT) {
@@ -102,6 +113,8 @@ __device__ void fill_region(const FrameIn& f, int W, int H, int rx0, int ry0, ui
   constexpr int NBX = (RW + 7) / 8, NBY = (RH + 3) / 4, NB = NBX * NBY;
   const int du = lane & 7, dv = lane >> 3;
   const bool fast_ok = f.warp.kind == WARP_HOMOGRAPHY && !f.warp.guard;
+  if (threadIdx.x == 0) q->count = 0;
+  __syncthreads();
   for (int g0 = warp; g0 < NB; g0 += nwarps * 32) {
     Anchor mine = {};
     bool mine_ok = false;
@@ -119,11 +132,29 @@ __device__ void fill_region(const FrameIn& f, int W, int H, int rx0, int ry0, ui
       if (rx >= RW || ry >= RH) continue;
       const int X = rx0 + rx, Y = ry0 + ry;
       uint32_t v = 0;
-      if (X >= 0 && Y >= 0 && X < W && Y < H)
-        v = aok ? sample_fast(f.warp, f.src, an, du, dv, X, Y) : sample_exact(f.warp, f.src, X, Y);
+      if (X >= 0 && Y >= 0 && X < W && Y < H) {
+        if (!aok) {
+          v = sample_exact(f.warp, f.src, X, Y);  // whole block without an anchor (guarded / lens poses)
+        } else if (!sample_try(f.src, an, du, dv, &v)) {
+          const uint32_t slot = atomicAdd(&q->count, 1u);
+          if (slot < (uint32_t)kExactQueue) {
+            q->item[slot] = ((uint32_t)ry << 16) | (uint32_t)rx;
+            continue;  // filled after the fast pass
+          }
+          v = sample_exact(f.warp, f.src, X, Y);
+        }
+      }
       reg[ry * RW + rx] = v;
       if (kv) kv[ry * RW + rx] = contrast_word(v);
     }
+  }
+  __syncthreads();
+  const uint32_t n = min(q->count, (uint32_t)kExactQueue);
+  for (uint32_t i = threadIdx.x; i < n; i += NT) {
+    const int rx = (int)(q->item[i] & 0xFFFFu), ry = (int)(q->item[i] >> 16);
+    const uint32_t v = sample_exact(f.warp, f.src, rx0 + rx, ry0 + ry);
+    reg[ry * RW + rx] = v;
+    if (kv) kv[ry * RW + rx] = contrast_word(v);
   }
 }
 
@@ -136,7 +167,8 @@ template <int B>
 struct RWLayout {
   static constexpr int RW = TW + 2 * B, RH = TH + 2 * B;
   static constexpr int NWIN = (2 * B + 1) * (2 * B + 1);
-  static constexpr size_t bytes = (size_t)RW * RH * 4 * 2 + (size_t)RH * TW * 4 * 2 + (NWIN + 1) * 4;
+  static constexpr size_t bytes =
+      (size_t)RW * RH * 4 * 2 + (size_t)RH * TW * 4 * 2 + (NWIN + 1) * 4 + sizeof(ExactQueue) + 16;
 };
 
 template <int B>
@@ -149,6 +181,7 @@ __global__ void __launch_bounds__(NT) remap_weights_kernel(const __grid_constant
   uint32_t* h1 = kv + RW * RH;   // packed count | gray sum, rows x TW
   uint32_t* h2 = h1 + RH * TW;   // sum of k^2
   float* inv_den = (float*)(h2 + RH * TW);
+  ExactQueue* queue = (ExactQueue*)(((uintptr_t)(inv_den + Lay::NWIN + 1) + 15) & ~(uintptr_t)15);
   const int x0 = blockIdx.x * TW, y0 = blockIdx.y * TH;
   for (int n = threadIdx.x; n <= Lay::NWIN; n += NT)
     inv_den[n] = n > 1 ? 1.0f / ((float)(n * (n - 1)) * 585225.0f) : 0.0f;
@@ -167,7 +200,7 @@ __global__ void __launch_bounds__(NT) remap_weights_kernel(const __grid_constant
     }
   }
   for (int k = 0; k < a.K; ++k) {
-    fill_region<RW, RH>(a.f[k], a.W, a.H, x0 - B, y0 - B, reg, kv);
+    fill_region<RW, RH>(a.f[k], a.W, a.H, x0 - B, y0 - B, reg, kv, queue);
     __syncthreads();
     // horizontal sliding window sums: region row r, output columns c0 .. c0+7,
     // window = region columns [c, c + 2B]
@@ -276,6 +309,9 @@ cudaError_t launch_remap_weights(const RemapWeightArgs& a, int border, cudaStrea
 //   M region   level-l cols [x0 - 2, x0 + TW], rows [y0 - 2, y0 + TH]
 //              (feeds the level-(l+1) mask on the tile)
 //   N tile     level-(l+1) cols [x1 - 1, x1 + TW/2], rows [y1 - 1, y1 + TH/2]
+// Samples outside the level are staged with support 0 (and value 0), so the
+// support-weighted REDUCE needs no bounds tests: a zero-support tap adds
+// nothing, exactly like the reference's skipped taps.
 namespace {
 
 constexpr int GW = TW + 7, GH = TH + 7;          // G region
@@ -285,15 +321,15 @@ constexpr int TW1 = TW / 2, TH1 = TH / 2;
 constexpr int kTmpFloats = (GH * NW * 4 > NH * TW * 3) ? GH * NW * 4 : NH * TW * 3;
 
 struct __align__(16) LevelSmem {
-  float tmp[kTmpFloats];    // reduce / expand temporaries (read as float4 / float2: first, 16-byte aligned)
+  float4 gs[GH * GW];       // level-l Gaussian (r, g, b) and support (0 / 1)
+  float tmp[kTmpFloats];    // reduce / expand temporaries
   float ng[3][NH * NW];     // level-(l+1) Gaussian (zero outside the level)
   float nm[TH1 * TW1];      // level-(l+1) mask on the tile
   float m[MH * MW];         // level-l mask (M region)
-  uint8_t ns[NH * NW];      // level-(l+1) support
   uint8_t sm[MH * MW];      // level-l mask support (M region)
+  uint8_t ns[NH * NW];      // level-(l+1) support
 };
 static_assert(offsetof(LevelSmem, tmp) % 16 == 0, "tmp is accessed as float4");
-static_assert((kTmpFloats * 4) % 16 == 0, "layout after tmp");
 
 template <typename T> __device__ __forceinline__ float ldv(const T* p, int64_t i);
 template <> __device__ __forceinline__ float ldv<float>(const float* p, int64_t i) { return p[i]; }
@@ -308,91 +344,96 @@ template <> __device__ __forceinline__ void stv<__nv_bfloat16>(__nv_bfloat16* p,
   p[i] = __float2bfloat16_rn(v);
 }
 
-// Level-l Gaussian source in shared memory: packed RGBA at level 0, planar
-// FP32 above.
-struct GPacked {
-  const uint32_t* reg;  // GH x GW
-  __device__ float g(int c, int rx, int ry) const { return chf(reg[ry * GW + rx], c); }
-  __device__ bool s(int rx, int ry) const { return px_alpha(reg[ry * GW + rx]) > 0; }
+// EXPAND taps.  clamped (parent larger than 512), src/fuse/pyramid.zig:
+// 1101-1149, 1748-1775: even 2j uses s[j-1], s[j], s[j+1] -> (a + 6b + c) / 8,
+// odd 2j+1 uses s[j], s[j+1] -> (a + b) / 2, coordinates clamped; vertically
+// the odd row 2i+1 reads row i twice (src/fuse/pyramid.zig:1122-1145).
+// no-wrap (parent at most 512), src/fuse/pyramid.zig:1167-1354: the same taps
+// with zero outside, (a + 6b) + c and 4 (a + b) horizontally, (a + 6b) + c and
+// a + b vertically, then one division by the position-dependent normaliser.
+// Every operation is in the reference's order, so both modes are bit-exact.
+struct Taps {
+  int i0, i1, i2;   // local indices (i2 unused for odd)
+  bool odd;
 };
-struct GPlanar {
-  const float* gp;      // 3 planes of GH x GW
-  const uint8_t* sp;
-  __device__ float g(int c, int rx, int ry) const { return gp[c * GH * GW + ry * GW + rx]; }
-  __device__ bool s(int rx, int ry) const { return sp[ry * GW + rx] != 0; }
-};
-
-// Horizontal stage of EXPAND for output column x from a child row g[]
-// indexed by child column - (cx1 - 1), exactly in the reference's operation
-// order.  clamped (parent larger than 512): src/fuse/pyramid.zig:1748-1775,
-// even 2j: (s[j-1] + 6 s[j] + s[j+1]) * 1/8, odd 2j+1: (s[j] + s[j+1]) * 1/2
-// with clamped coordinates.  no-wrap (parent at most 512):
-// src/fuse/pyramid.zig:1167-1354, (s[j-1] + 6 s[j]) + s[j+1] and
-// 4 (s[j] + s[j+1]) with zero outside (g holds 0 there); the division by the
-// position-dependent normaliser comes after the vertical stage.
-__device__ __forceinline__ float expand_h(const float* g, int x, int cx1, int wc, bool exact) {
-  const int j = x >> 1, o = cx1 - 1;
-  if (!exact) {
-    if ((x & 1) == 0) {
-      float s0 = g[clampi(j - 1, 0, wc - 1) - o], s1 = g[clampi(j, 0, wc - 1) - o], s2 = g[clampi(j + 1, 0, wc - 1) - o];
-      return __fmul_rn(__fadd_rn(__fadd_rn(s0, __fmul_rn(6.0f, s1)), s2), 0.125f);
-    }
-    float s0 = g[clampi(j, 0, wc - 1) - o], s1 = g[clampi(j + 1, 0, wc - 1) - o];
-    return __fmul_rn(__fadd_rn(s0, s1), 0.5f);
+__device__ __forceinline__ Taps expand_taps(int x, int c1, int wc, bool exact) {
+  const int j = x >> 1, o = c1 - 1;
+  Taps t;
+  t.odd = (x & 1) != 0;
+  if (exact) {
+    t.i0 = t.odd ? j - o : j - 1 - o;
+    t.i1 = t.odd ? j + 1 - o : j - o;
+    t.i2 = j + 1 - o;
+  } else {
+    t.i0 = (t.odd ? clampi(j, 0, wc - 1) : clampi(j - 1, 0, wc - 1)) - o;
+    t.i1 = (t.odd ? clampi(j + 1, 0, wc - 1) : clampi(j, 0, wc - 1)) - o;
+    t.i2 = clampi(j + 1, 0, wc - 1) - o;
   }
-  if ((x & 1) == 0) return __fadd_rn(__fadd_rn(g[j - 1 - o], __fmul_rn(6.0f, g[j - o])), g[j + 1 - o]);
-  return __fmul_rn(4.0f, __fadd_rn(g[j - o], g[j + 1 - o]));
+  return t;
 }
-
-// Vertical stage for output (x, y) from horizontal rows
-// hrow[(row - (cy1 - 1)) * rstride + col].  clamped: even 2i:
-// (r[i-1] + 6 r[i] + r[i+1]) * 1/8, odd 2i+1: (r[i] + r[i]) * 1/2 (the
-// reference reads row i twice, src/fuse/pyramid.zig:1122-1145); no-wrap:
-// (r[i-1] + 6 r[i]) + r[i+1] or r[i] + r[i+1] with zero outside, divided by
-// the normaliser.
-__device__ __forceinline__ float expand_v(const float* hrow, int rstride, int col, int x, int y, int cy1, int wc,
-                                          int hc, bool exact) {
-  const int q = y >> 1, o = cy1 - 1;
-  if (!exact) {
-    if ((y & 1) == 0) {
-      float r0 = hrow[(clampi(q - 1, 0, hc - 1) - o) * rstride + col];
-      float r1 = hrow[(clampi(q, 0, hc - 1) - o) * rstride + col];
-      float r2 = hrow[(clampi(q + 1, 0, hc - 1) - o) * rstride + col];
-      return __fmul_rn(__fadd_rn(__fadd_rn(r0, __fmul_rn(6.0f, r1)), r2), 0.125f);
-    }
-    float r0 = hrow[(clampi(q, 0, hc - 1) - o) * rstride + col];
-    return __fmul_rn(__fadd_rn(r0, r0), 0.5f);
+__device__ __forceinline__ float expand_h1(const float* g, const Taps& t, bool exact) {
+  if (exact) {
+    if (t.odd) return __fmul_rn(4.0f, __fadd_rn(g[t.i0], g[t.i1]));
+    return __fadd_rn(__fadd_rn(g[t.i0], __fmul_rn(6.0f, g[t.i1])), g[t.i2]);
   }
-  auto row = [&](int qq) -> float { return (qq < 0 || qq >= hc) ? 0.0f : hrow[(qq - o) * rstride + col]; };
-  float v = ((y & 1) == 0) ? __fadd_rn(__fadd_rn(row(q - 1), __fmul_rn(6.0f, row(q))), row(q + 1))
-                           : __fadd_rn(row(q), row(q + 1));
-  return __fdiv_rn(v, exact_expand_divisor(x, y, wc, hc));
+  if (t.odd) return __fmul_rn(__fadd_rn(g[t.i0], g[t.i1]), 0.5f);
+  return __fmul_rn(__fadd_rn(__fadd_rn(g[t.i0], __fmul_rn(6.0f, g[t.i1])), g[t.i2]), 0.125f);
+}
+// vertical rows of output row y (local row indices of the horizontal stage),
+// -1 for a zero row of the no-wrap mode
+struct Rows {
+  int r0, r1, r2;
+  bool odd;
+};
+__device__ __forceinline__ Rows expand_rows(int y, int c1, int hc, bool exact) {
+  const int q = y >> 1, o = c1 - 1;
+  Rows r;
+  r.odd = (y & 1) != 0;
+  if (exact) {
+    auto z = [&](int v) { return (v < 0 || v >= hc) ? -1 : v - o; };
+    r.r0 = r.odd ? z(q) : z(q - 1);
+    r.r1 = r.odd ? z(q + 1) : z(q);
+    r.r2 = z(q + 1);
+  } else {
+    r.r0 = r.odd ? clampi(q, 0, hc - 1) - o : clampi(q - 1, 0, hc - 1) - o;
+    r.r1 = r.odd ? r.r0 : clampi(q, 0, hc - 1) - o;
+    r.r2 = clampi(q + 1, 0, hc - 1) - o;
+  }
+  return r;
+}
+__device__ __forceinline__ float expand_v1(const float* h, int stride, const Rows& r, bool exact, float div) {
+  auto at = [&](int row) -> float { return row < 0 ? 0.0f : h[row * stride]; };
+  if (exact) {
+    float v = r.odd ? __fadd_rn(at(r.r0), at(r.r1))
+                    : __fadd_rn(__fadd_rn(at(r.r0), __fmul_rn(6.0f, at(r.r1))), at(r.r2));
+    return __fdiv_rn(v, div);
+  }
+  if (r.odd) {
+    const float a = h[r.r0 * stride];
+    return __fmul_rn(__fadd_rn(a, a), 0.5f);
+  }
+  return __fmul_rn(__fadd_rn(__fadd_rn(h[r.r0 * stride], __fmul_rn(6.0f, h[r.r1 * stride])), h[r.r2 * stride]),
+                   0.125f);
 }
 
 // REDUCE with support to the level-(l+1) tile (+ halo for the Gaussian),
 // src/fuse/pyramid.zig:997-1099: 5x5 taps [1 4 6 4 1]^2 over in-range
 // samples with support > 0, value = sum(w v) / sum(w), support = sum(w) > 0.
 // Evaluated separably (rows first); the weights are exact small integers.
-template <typename GS>
-__device__ void reduce_step(const GS& src, LevelSmem& S, const LevelArgs& a, int x0, int y0) {
+__device__ void reduce_step(LevelSmem& S, const LevelArgs& a, int x0, int y0) {
   const int x1 = x0 >> 1, y1 = y0 >> 1;
   float4* th = reinterpret_cast<float4*>(S.tmp);  // [GH][NW]
   for (int i = threadIdx.x; i < GH * NW; i += NT) {
     const int ry = i / NW, jj = i % NW;
-    const int j = x1 - 1 + jj;
-    const int sx0 = 2 * j - 2;
-    const int rx0 = sx0 - (x0 - 4);
+    const float4* row = S.gs + ry * GW + 2 * jj - 2 + 2;  // G region column of tap 0: 2j - 2 - (x0 - 4)
     float v0 = 0.f, v1 = 0.f, v2 = 0.f, ws = 0.f;
-    const bool inner = sx0 >= 0 && sx0 + 4 < a.wl;
 #pragma unroll
     for (int kx = 0; kx < 5; ++kx) {
-      const int sx = sx0 + kx;
-      if (!inner && (sx < 0 || sx >= a.wl)) continue;
-      if (!src.s(rx0 + kx, ry)) continue;
-      const float w = kw(kx);
-      v0 = fmaf(w, src.g(0, rx0 + kx, ry), v0);
-      v1 = fmaf(w, src.g(1, rx0 + kx, ry), v1);
-      v2 = fmaf(w, src.g(2, rx0 + kx, ry), v2);
+      const float4 t = row[kx];
+      const float w = kw(kx) * t.w;
+      v0 = fmaf(w, t.x, v0);
+      v1 = fmaf(w, t.y, v1);
+      v2 = fmaf(w, t.z, v2);
       ws += w;
     }
     th[i] = make_float4(v0, v1, v2, ws);
@@ -402,38 +443,33 @@ __device__ void reduce_step(const GS& src, LevelSmem& S, const LevelArgs& a, int
     const int ii = i / NW, jj = i % NW;
     const int yi = y1 - 1 + ii, xj = x1 - 1 + jj;
     float v0 = 0.f, v1 = 0.f, v2 = 0.f, ws = 0.f;
+    const float4* col = th + (2 * ii) * NW + jj;  // G region row of tap 0: 2 yi - 2 - (y0 - 4)
 #pragma unroll
     for (int ky = 0; ky < 5; ++ky) {
-      const int sy = 2 * yi - 2 + ky;
-      if (sy < 0 || sy >= a.hl) continue;
-      const float4 t = th[(sy - (y0 - 4)) * NW + jj];
+      const float4 t = col[ky * NW];
       const float w = kw(ky);
       v0 = fmaf(w, t.x, v0);
       v1 = fmaf(w, t.y, v1);
       v2 = fmaf(w, t.z, v2);
       ws = fmaf(w, t.w, ws);
     }
-    const bool inside = xj >= 0 && yi >= 0 && xj < a.wn && yi < a.hn;
-    const bool sup = inside && ws > 0.f;
-    S.ng[0][i] = sup ? v0 / ws : 0.f;
-    S.ng[1][i] = sup ? v1 / ws : 0.f;
-    S.ng[2][i] = sup ? v2 / ws : 0.f;
+    const bool sup = xj >= 0 && yi >= 0 && xj < a.wn && yi < a.hn && ws > 0.f;
+    const float r = sup ? __fdividef(1.0f, ws) : 0.0f;
+    S.ng[0][i] = v0 * r;
+    S.ng[1][i] = v1 * r;
+    S.ng[2][i] = v2 * r;
     S.ns[i] = sup ? 1 : 0;
   }
+  float2* tm = reinterpret_cast<float2*>(S.tmp + GH * NW * 4 - MH * TW1 * 2);  // [MH][TW1], disjoint from th rows in use
   __syncthreads();
-  float2* tm = reinterpret_cast<float2*>(S.tmp);  // [MH][TW1]
   for (int i = threadIdx.x; i < MH * TW1; i += NT) {
     const int ry = i / TW1, jj = i % TW1;
-    const int j = x1 + jj;
+    const int base = ry * MW + 2 * jj;  // M region column of tap 0: 2j - 2 - (x0 - 2)
     float v = 0.f, ws = 0.f;
 #pragma unroll
     for (int kx = 0; kx < 5; ++kx) {
-      const int sx = 2 * j - 2 + kx;
-      if (sx < 0 || sx >= a.wl) continue;
-      const int rx = sx - (x0 - 2);
-      if (!S.sm[ry * MW + rx]) continue;
-      const float w = kw(kx);
-      v = fmaf(w, S.m[ry * MW + rx], v);
+      const float w = S.sm[base + kx] ? kw(kx) : 0.0f;
+      v = fmaf(w, S.m[base + kx], v);
       ws += w;
     }
     tm[i] = make_float2(v, ws);
@@ -441,18 +477,15 @@ __device__ void reduce_step(const GS& src, LevelSmem& S, const LevelArgs& a, int
   __syncthreads();
   for (int i = threadIdx.x; i < TH1 * TW1; i += NT) {
     const int ii = i / TW1, jj = i % TW1;
-    const int yi = y1 + ii;
     float v = 0.f, ws = 0.f;
 #pragma unroll
     for (int ky = 0; ky < 5; ++ky) {
-      const int sy = 2 * yi - 2 + ky;
-      if (sy < 0 || sy >= a.hl) continue;
+      const float2 t = tm[(2 * ii + ky) * TW1 + jj];  // M region row of tap 0: 2 yi - 2 - (y0 - 2)
       const float w = kw(ky);
-      const float2 t = tm[(sy - (y0 - 2)) * TW1 + jj];
       v = fmaf(w, t.x, v);
       ws = fmaf(w, t.y, ws);
     }
-    S.nm[i] = ws > 0.f ? v / ws : 0.f;
+    S.nm[i] = ws > 0.f ? v * __fdividef(1.0f, ws) : 0.f;
   }
   __syncthreads();
 }
@@ -491,18 +524,17 @@ __device__ void store_next(const LevelSmem& S, const LevelArgs& a, int x0, int y
 // EXPAND of the level-(l+1) Gaussian back to the level-l tile fused with the
 // weighted Laplacian blend into the accumulator registers:
 // acc += (G_l - EXPAND(G_{l+1})) * M_l  (src/fuse/pyramid.zig:1480-1504).
-template <typename GS>
-__device__ void expand_blend_step(const GS& src, LevelSmem& S, const LevelArgs& a, int x0, int y0,
-                                  float (&acc)[PPT][3]) {
+__device__ void expand_blend_step(LevelSmem& S, const LevelArgs& a, int x0, int y0, float (&acc)[PPT][3]) {
   const int x1 = x0 >> 1, y1 = y0 >> 1;
-  float* hrow = S.tmp;  // [NH][TW][3]
+  float* hrow = S.tmp;  // [NH][3][TW]
   const bool exact = a.exact_expand != 0;
   for (int i = threadIdx.x; i < NH * TW; i += NT) {
     const int ii = i / TW, xx = i % TW;
     const int yi = y1 - 1 + ii;
     if (yi < 0 || yi >= a.hn) continue;
+    const Taps t = expand_taps(x0 + xx, x1, a.wn, exact);
 #pragma unroll
-    for (int c = 0; c < 3; ++c) hrow[i * 3 + c] = expand_h(S.ng[c] + ii * NW, x0 + xx, x1, a.wn, exact);
+    for (int c = 0; c < 3; ++c) hrow[(ii * 3 + c) * TW + xx] = expand_h1(S.ng[c] + ii * NW, t, exact);
   }
   __syncthreads();
 #pragma unroll
@@ -511,11 +543,15 @@ __device__ void expand_blend_step(const GS& src, LevelSmem& S, const LevelArgs& 
     const int xx = p % TW, yy = p / TW;
     const int x = x0 + xx, y = y0 + yy;
     if (x >= a.wl || y >= a.hl) continue;
+    const Rows r = expand_rows(y, y1, a.hn, exact);
+    const float div = exact ? exact_expand_divisor(x, y, a.wn, a.hn) : 1.0f;
     const float m = S.m[(yy + 2) * MW + (xx + 2)];
+    const float4 g = S.gs[(yy + 4) * GW + (xx + 4)];
+    const float gv[3] = {g.x, g.y, g.z};
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      const float e = expand_v(hrow, TW * 3, xx * 3 + c, x, y, y1, a.wn, a.hn, exact);
-      const float lap = __fsub_rn(src.g(c, xx + 4, yy + 4), e);
+      const float e = expand_v1(hrow + c * TW + xx, 3 * TW, r, exact, div);
+      const float lap = __fsub_rn(gv[c], e);
       acc[i][c] = __fadd_rn(acc[i][c], __fmul_rn(lap, m));
     }
   }
@@ -546,8 +582,13 @@ __device__ __forceinline__ void store_acc(const LevelArgs& a, int x0, int y0, co
   }
 }
 
-constexpr size_t kLevel0Extra = (size_t)GH * GW * 4 + (size_t)MH * MW * 4;
-constexpr size_t kLevelExtra = (size_t)3 * GH * GW * 4 + (size_t)GH * GW;
+__device__ __forceinline__ void load_mask_support(LevelSmem& S, const LevelArgs& a, int x0, int y0) {
+  for (int i = threadIdx.x; i < MH * MW; i += NT) {
+    const int X = x0 - 2 + i % MW, Y = y0 - 2 + i / MW;
+    const bool in = X >= 0 && Y >= 0 && X < a.wl && Y < a.hl;
+    S.sm[i] = in ? a.sm_l[(int64_t)Y * a.pitch_l + X] : 0;
+  }
+}
 
 }  // namespace
 
@@ -558,38 +599,32 @@ template <typename T>
 __global__ void __launch_bounds__(NT) level0_kernel(const __grid_constant__ LevelArgs a) {
   extern __shared__ __align__(16) uint8_t smem_raw[];
   LevelSmem& S = *reinterpret_cast<LevelSmem*>(smem_raw);
-  uint32_t* reg = (uint32_t*)(smem_raw + ((sizeof(LevelSmem) + 15) & ~(size_t)15));  // G region
-  float* normr = (float*)(reg + GH * GW);                                           // M region
   const int x0 = blockIdx.x * TW, y0 = blockIdx.y * TH;
-  for (int i = threadIdx.x; i < MH * MW; i += NT) {
-    const int X = x0 - 2 + i % MW, Y = y0 - 2 + i / MW;
-    const bool in = X >= 0 && Y >= 0 && X < a.wl && Y < a.hl;
-    const int64_t o = (int64_t)Y * a.pitch_l + X;
-    S.sm[i] = in ? a.sm_l[o] : 0;
-    normr[i] = in ? a.norm[o] : 0.0f;
-  }
+  load_mask_support(S, a, x0, y0);
   float acc[PPT][3];
   load_acc(a, x0, y0, acc);
-  __syncthreads();
   for (int k = 0; k < a.K; ++k) {
     const FramePlanes& in = a.in0[k];
     for (int i = threadIdx.x; i < GH * GW; i += NT) {
       const int X = x0 - 4 + i % GW, Y = y0 - 4 + i / GW;
-      const bool inb = X >= 0 && Y >= 0 && X < a.wl && Y < a.hl;
-      reg[i] = inb ? in.rgba[(int64_t)Y * a.pitch_l + X] : 0u;
+      float4 g = make_float4(0.f, 0.f, 0.f, 0.f);
+      if (X >= 0 && Y >= 0 && X < a.wl && Y < a.hl) {
+        const uint32_t v = in.rgba[(int64_t)Y * a.pitch_l + X];
+        g = make_float4(chf(v, 0), chf(v, 1), chf(v, 2), px_alpha(v) > 0 ? 1.0f : 0.0f);
+      }
+      S.gs[i] = g;
     }
     for (int i = threadIdx.x; i < MH * MW; i += NT) {
       const int X = x0 - 2 + i % MW, Y = y0 - 2 + i / MW;
       float m = 0.0f;
       if (X >= 0 && Y >= 0 && X < a.wl && Y < a.hl) {
-        const float w = in.w[(int64_t)Y * a.pitch_l + X];
-        const float nv = normr[i];
-        m = nv > 1e-12f ? __fdiv_rn(w, nv) : a.inv_count;
+        const int64_t o = (int64_t)Y * a.pitch_l + X;
+        const float nv = a.norm[o];
+        m = nv > 1e-12f ? __fdiv_rn(in.w[o], nv) : a.inv_count;
       }
       S.m[i] = m;
     }
     __syncthreads();
-    GPacked src{reg};
     if (a.levels == 1) {
       // 1x1 image: the top level is level 0 (src/fuse/pyramid.zig:1605-1649)
 #pragma unroll
@@ -598,14 +633,17 @@ __global__ void __launch_bounds__(NT) level0_kernel(const __grid_constant__ Leve
         const int xx = p % TW, yy = p / TW;
         if (x0 + xx >= a.wl || y0 + yy >= a.hl) continue;
         const float m = S.m[(yy + 2) * MW + (xx + 2)];
-        for (int c = 0; c < 3; ++c) acc[i][c] = __fadd_rn(acc[i][c], __fmul_rn(src.g(c, xx + 4, yy + 4), m));
+        const float4 g = S.gs[(yy + 4) * GW + (xx + 4)];
+        acc[i][0] = __fadd_rn(acc[i][0], __fmul_rn(g.x, m));
+        acc[i][1] = __fadd_rn(acc[i][1], __fmul_rn(g.y, m));
+        acc[i][2] = __fadd_rn(acc[i][2], __fmul_rn(g.z, m));
       }
       __syncthreads();
       continue;
     }
-    reduce_step(src, S, a, x0, y0);
+    reduce_step(S, a, x0, y0);
     store_next<T>(S, a, x0, y0, k);
-    expand_blend_step(src, S, a, x0, y0, acc);
+    expand_blend_step(S, a, x0, y0, acc);
   }
   store_acc(a, x0, y0, acc);
 }
@@ -615,28 +653,22 @@ template <typename T>
 __global__ void __launch_bounds__(NT) level_kernel(const __grid_constant__ LevelArgs a) {
   extern __shared__ __align__(16) uint8_t smem_raw[];
   LevelSmem& S = *reinterpret_cast<LevelSmem*>(smem_raw);
-  float* gpl = (float*)(smem_raw + ((sizeof(LevelSmem) + 15) & ~(size_t)15));
-  uint8_t* spl = (uint8_t*)(gpl + 3 * GH * GW);
   const int x0 = blockIdx.x * TW, y0 = blockIdx.y * TH;
-  for (int i = threadIdx.x; i < MH * MW; i += NT) {
-    const int X = x0 - 2 + i % MW, Y = y0 - 2 + i / MW;
-    const bool in = X >= 0 && Y >= 0 && X < a.wl && Y < a.hl;
-    S.sm[i] = in ? a.sm_l[(int64_t)Y * a.pitch_l + X] : 0;
-  }
+  load_mask_support(S, a, x0, y0);
   float acc[PPT][3];
   load_acc(a, x0, y0, acc);
-  __syncthreads();
   for (int k = 0; k < a.K; ++k) {
     const LevelPlanes& in = a.in[k];
     const T* g = (const T*)in.g;
     const T* mm = (const T*)in.m;
     for (int i = threadIdx.x; i < GH * GW; i += NT) {
       const int X = x0 - 4 + i % GW, Y = y0 - 4 + i / GW;
-      const bool inb = X >= 0 && Y >= 0 && X < a.wl && Y < a.hl;
-      const int64_t o = (int64_t)Y * a.pitch_l + X;
-      spl[i] = inb ? in.s[o] : 0;
-#pragma unroll
-      for (int c = 0; c < 3; ++c) gpl[c * GH * GW + i] = inb ? ldv<T>(g, c * in.plane + o) : 0.0f;
+      float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+      if (X >= 0 && Y >= 0 && X < a.wl && Y < a.hl) {
+        const int64_t o = (int64_t)Y * a.pitch_l + X;
+        v = make_float4(ldv<T>(g, o), ldv<T>(g, in.plane + o), ldv<T>(g, 2 * in.plane + o), in.s[o] ? 1.0f : 0.0f);
+      }
+      S.gs[i] = v;
     }
     for (int i = threadIdx.x; i < MH * MW; i += NT) {
       const int X = x0 - 2 + i % MW, Y = y0 - 2 + i / MW;
@@ -644,10 +676,9 @@ __global__ void __launch_bounds__(NT) level_kernel(const __grid_constant__ Level
       S.m[i] = inb ? ldv<T>(mm, (int64_t)Y * a.pitch_l + X) : 0.0f;
     }
     __syncthreads();
-    GPlanar src{gpl, spl};
-    reduce_step(src, S, a, x0, y0);
+    reduce_step(S, a, x0, y0);
     store_next<T>(S, a, x0, y0, k);
-    expand_blend_step(src, S, a, x0, y0, acc);
+    expand_blend_step(S, a, x0, y0, acc);
   }
   store_acc(a, x0, y0, acc);
 }
@@ -660,52 +691,40 @@ static cudaError_t configure(K kernel, size_t bytes, bool* done) {
   return e;
 }
 
-cudaError_t launch_level0(const LevelArgs& a, int storage, cudaStream_t s) {
-  static bool c0 = false, c1 = false, c2 = false;
-  const size_t sm = sizeof(LevelSmem) + 16 + kLevel0Extra;
+template <template <typename> class KER>
+static cudaError_t launch_levels(const LevelArgs& a, int storage, cudaStream_t s, bool* cfg) {
+  const size_t sm = sizeof(LevelSmem);
   dim3 grid((a.wl + TW - 1) / TW, (a.hl + TH - 1) / TH);
   cudaError_t e;
   switch (storage) {
     case FS_STORAGE_F32:
-      if ((e = configure(level0_kernel<float>, sm, &c0)) != cudaSuccess) return e;
-      level0_kernel<float><<<grid, NT, sm, s>>>(a);
+      if ((e = configure(KER<float>::fn(), sm, &cfg[0])) != cudaSuccess) return e;
+      KER<float>::fn()<<<grid, NT, sm, s>>>(a);
       break;
     case FS_STORAGE_F16:
-      if ((e = configure(level0_kernel<__half>, sm, &c1)) != cudaSuccess) return e;
-      level0_kernel<__half><<<grid, NT, sm, s>>>(a);
+      if ((e = configure(KER<__half>::fn(), sm, &cfg[1])) != cudaSuccess) return e;
+      KER<__half>::fn()<<<grid, NT, sm, s>>>(a);
       break;
     case FS_STORAGE_BF16:
-      if ((e = configure(level0_kernel<__nv_bfloat16>, sm, &c2)) != cudaSuccess) return e;
-      level0_kernel<__nv_bfloat16><<<grid, NT, sm, s>>>(a);
+      if ((e = configure(KER<__nv_bfloat16>::fn(), sm, &cfg[2])) != cudaSuccess) return e;
+      KER<__nv_bfloat16>::fn()<<<grid, NT, sm, s>>>(a);
       break;
     default:
       return cudaErrorInvalidValue;
   }
   return cudaGetLastError();
 }
+template <typename T> struct Level0K { static decltype(&level0_kernel<T>) fn() { return &level0_kernel<T>; } };
+template <typename T> struct LevelK { static decltype(&level_kernel<T>) fn() { return &level_kernel<T>; } };
+
+cudaError_t launch_level0(const LevelArgs& a, int storage, cudaStream_t s) {
+  static bool cfg[3] = {false, false, false};
+  return launch_levels<Level0K>(a, storage, s, cfg);
+}
 
 cudaError_t launch_level(const LevelArgs& a, int storage, cudaStream_t s) {
-  static bool c0 = false, c1 = false, c2 = false;
-  const size_t sm = sizeof(LevelSmem) + 16 + kLevelExtra;
-  dim3 grid((a.wl + TW - 1) / TW, (a.hl + TH - 1) / TH);
-  cudaError_t e;
-  switch (storage) {
-    case FS_STORAGE_F32:
-      if ((e = configure(level_kernel<float>, sm, &c0)) != cudaSuccess) return e;
-      level_kernel<float><<<grid, NT, sm, s>>>(a);
-      break;
-    case FS_STORAGE_F16:
-      if ((e = configure(level_kernel<__half>, sm, &c1)) != cudaSuccess) return e;
-      level_kernel<__half><<<grid, NT, sm, s>>>(a);
-      break;
-    case FS_STORAGE_BF16:
-      if ((e = configure(level_kernel<__nv_bfloat16>, sm, &c2)) != cudaSuccess) return e;
-      level_kernel<__nv_bfloat16><<<grid, NT, sm, s>>>(a);
-      break;
-    default:
-      return cudaErrorInvalidValue;
-  }
-  return cudaGetLastError();
+  static bool cfg[3] = {false, false, false};
+  return launch_levels<LevelK>(a, storage, s, cfg);
 }
 
 // ================================================================ collapse
@@ -713,7 +732,7 @@ cudaError_t launch_level(const LevelArgs& a, int storage, cudaStream_t s) {
 // 0 also quantise trunc(clamp(v + 0.5, 0, 255)) into interleaved RGB.
 __global__ void __launch_bounds__(NT) collapse_kernel(const __grid_constant__ CollapseArgs a) {
   __shared__ float cg[3][NH * NW];
-  __shared__ float hrow[NH * TW * 3];
+  __shared__ float hrow[NH * 3 * TW];
   const int x0 = blockIdx.x * TW, y0 = blockIdx.y * TH;
   const int x1 = x0 >> 1, y1 = y0 >> 1;
   const bool exact = a.exact_expand != 0;
@@ -728,7 +747,8 @@ __global__ void __launch_bounds__(NT) collapse_kernel(const __grid_constant__ Co
     const int ii = i / TW, xx = i % TW;
     const int yi = y1 - 1 + ii;
     if (yi < 0 || yi >= a.hc) continue;
-    for (int c = 0; c < 3; ++c) hrow[i * 3 + c] = expand_h(cg[c] + ii * NW, x0 + xx, x1, a.wc, exact);
+    const Taps t = expand_taps(x0 + xx, x1, a.wc, exact);
+    for (int c = 0; c < 3; ++c) hrow[(ii * 3 + c) * TW + xx] = expand_h1(cg[c] + ii * NW, t, exact);
   }
   __syncthreads();
   for (int i = threadIdx.x; i < TH * TW; i += NT) {
@@ -736,8 +756,10 @@ __global__ void __launch_bounds__(NT) collapse_kernel(const __grid_constant__ Co
     const int x = x0 + xx, y = y0 + yy;
     if (x >= a.wp || y >= a.hp) continue;
     const int64_t o = (int64_t)y * a.pitch_p + x;
+    const Rows r = expand_rows(y, y1, a.hc, exact);
+    const float div = exact ? exact_expand_divisor(x, y, a.wc, a.hc) : 1.0f;
     for (int c = 0; c < 3; ++c) {
-      const float v = expand_v(hrow, TW * 3, xx * 3 + c, x, y, y1, a.wc, a.hc, exact);
+      const float v = expand_v1(hrow + c * TW + xx, 3 * TW, r, exact, div);
       float* p = a.acc_p + c * a.plane_p + o;
       const float nv = __fadd_rn(*p, v);
       if (a.out) {

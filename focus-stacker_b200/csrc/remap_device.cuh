@@ -247,6 +247,47 @@ static __device__ __noinline__ uint32_t sample_exact(const Warp& w, const SrcIma
   return pack_rgba(out[0], out[1], out[2], alpha);
 }
 
+// Fast path only: returns false (leaving *out untouched) when the exact
+// path must decide the sample.
+__device__ __forceinline__ bool sample_try(const SrcImage& s, const Anchor& a, int du, int dv, uint32_t* out) {
+  float fdu = (float)du, fdv = (float)dv;
+  float gd = fmaf(a.gam, fdu, a.eta * fdv);
+  float den = 1.0f + gd;
+  float nx = fmaf(a.am1x, fdu, a.bx * fdv) - fdu * gd;
+  float ny = fmaf(a.ay, fdu, a.bm1y * fdv) - fdv * gd;
+  float rd = __fdividef(1.0f, den);
+  float tx = a.fxh + fmaf(nx, rd, a.fxl);
+  float ty = a.fyh + fmaf(ny, rd, a.fyl);
+  float flx = floorf(tx), fly = floorf(ty);
+  int x0 = a.ix + du + (int)flx;
+  int y0 = a.iy + dv + (int)fly;
+  float fx = tx - flx, fy = ty - fly;
+  if (x0 < 1 || y0 < 1 || x0 > s.w - 3 || y0 > s.h - 3) return false;
+  float v00[3], v10[3], v01[3], v11[3];
+  load_rgb_biased(s, x0, y0, v00);
+  load_rgb_biased(s, x0 + 1, y0, v10);
+  load_rgb_biased(s, x0, y0 + 1, v01);
+  load_rgb_biased(s, x0 + 1, y0 + 1, v11);
+  float fxy = fx * fy;
+  uint32_t o[3];
+  bool tie = false;
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    float d10 = v10[c] - v00[c], d01 = v01[c] - v00[c], d11 = (v11[c] - v10[c]) - d01;
+    float v = fmaf(fx, d10, v00[c] - 8388608.0f);
+    v = fmaf(fy, d01, v);
+    v = fmaf(fxy, d11, v);
+    float k = floorf(v);
+    float fr = v - k;
+    tie = tie || fabsf(fr - 0.5f) < kTieBand;
+    float r = fr > 0.5f ? k + 1.0f : k;
+    o[c] = (uint32_t)fminf(fmaxf(r, 0.0f), 255.0f);
+  }
+  if (tie) return false;
+  *out = pack_rgba(o[0], o[1], o[2], 255u);
+  return true;
+}
+
 // Sample output pixel (X, Y) = anchor pixel + (du, dv).  Falls back to the
 // exact path when the fast path cannot certify the result.
 __device__ __forceinline__ uint32_t sample_fast(const Warp& w, const SrcImage& s, const Anchor& a, int du, int dv,
