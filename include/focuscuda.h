@@ -202,6 +202,24 @@ int fs_stack_destroy(fs_stack* stack);
 int fs_fuse_stack(fs_ctx* ctx, const fs_stack_desc* desc, const void* const* frames, const size_t* row_strides,
                   const fs_pose* poses, void* out_pixels, size_t out_stride);
 
+/* No counterpart in the reference.  Fuse-only fusion (the result of
+ * fs_fuse_stack with input_is_aligned = 1) of 1..8 pre-aligned RGB / RGBA u8
+ * frames already on the current device, written as RGB u8 into dev_out, with
+ * every intermediate plane in a file-scope device array of 40 MiB (8 frames
+ * of 512 x 512 fit; larger stacks are rejected with FS_ERR_UNSUPPORTED).
+ * Needs no context and allocates no device memory, for callers that must not
+ * allocate while they run.  The work is queued on `stream` (cudaStream_t of
+ * the current device, NULL = default stream) and the call returns without
+ * waiting for it.  The first call on a device looks up the array's address
+ * (and loads the module there); make it before any stream capture.  Every
+ * call in the process shares the array: calls must not overlap in time on the
+ * device (order them on one stream or with events), or they corrupt each
+ * other's planes.  A message for a failure goes to err (err_len bytes, may be
+ * NULL). */
+int fs_fuse_aligned_device_static(const void* const* dev_frames, const size_t* row_strides, uint32_t frame_count,
+                                  uint32_t width, uint32_t height, uint32_t channels, uint32_t contrast_window,
+                                  void* dev_out, size_t out_stride, void* stream, char* err, size_t err_len);
+
 /* ------------------------------------------------------ synthetic input */
 
 /* Render frame k of a synthetic focus stack (seeded; see the generator in
