@@ -592,39 +592,99 @@ __device__ __forceinline__ void load_mask_support(LevelSmem& S, const LevelArgs&
 
 }  // namespace
 
+// Asynchronous global -> shared copies (cp.async, 16 B).  src_bytes < 16
+// zero-fills the rest of the 16 bytes; with src_bytes == 0 nothing is read
+// (the address given is still a valid one).
+__device__ __forceinline__ void cp_async16(void* dst, const void* src, int src_bytes) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(d), "l"(src), "r"(src_bytes) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+// Level-0 staging of one frame's pass-1 planes, copied while the previous
+// frame is being reduced and blended.  Rows are 72 words wide starting at
+// column x0 - 4 (16-byte aligned because x0 is a multiple of 64 and the level
+// pitch a multiple of 32 words): G rows y0 - 4 .. y0 + TH + 2 of the RGBA
+// words, M rows y0 - 2 .. y0 + TH of the weights.  Words outside the level are
+// zero (alpha 0: no support).
+constexpr int SW = 72, SCH = SW / 4;  // staged words per row, 16-byte chunks per row
+struct __align__(16) Level0Smem {
+  LevelSmem lv;
+  uint32_t rgba[GH * SW];
+  float w[MH * SW];
+};
+static_assert(offsetof(Level0Smem, rgba) % 16 == 0 && offsetof(Level0Smem, w) % 16 == 0, "cp.async targets");
+static_assert(SW >= GW + 1 && TW % 4 == 0, "staging covers the G region");
+
+__device__ __forceinline__ void stage_rows(void* dst, const void* plane, int64_t pitch, int x0, int ytop, int rows,
+                                           int wl, int hl) {
+  for (int i = threadIdx.x; i < rows * SCH; i += NT) {
+    const int r = i / SCH, c = i % SCH;
+    const int X = x0 - 4 + 4 * c, Y = ytop + r;
+    int n = 0;
+    const uint8_t* src = (const uint8_t*)plane;
+    if (X >= 0 && Y >= 0 && Y < hl && X < wl) {
+      n = min(4, wl - X) * 4;
+      src += ((int64_t)Y * pitch + X) * 4;
+    }
+    cp_async16((uint8_t*)dst + (size_t)i * 16, src, n);
+  }
+}
+
+__device__ __forceinline__ void stage_level0(Level0Smem& S, const LevelArgs& a, const FramePlanes& in, int x0,
+                                             int y0) {
+  stage_rows(S.rgba, in.rgba, a.pitch_l, x0, y0 - 4, GH, a.wl, a.hl);
+  stage_rows(S.w, in.w, a.pitch_l, x0, y0 - 2, MH, a.wl, a.hl);
+  cp_async_commit();
+}
+
 // Level 0 -> 1 for a batch of frames from their pass-1 planes (remapped RGBA
 // and weight): mask = weight / sum (1/N where the sum is <= 1e-12,
-// src/fuse/pyramid.zig:303-316), mask support = union.
+// src/fuse/pyramid.zig:303-316), mask support = union.  Frame k + 1 is
+// copied into the staging rows while frame k is reduced and blended.
 template <typename T>
 __global__ void __launch_bounds__(NT) level0_kernel(const __grid_constant__ LevelArgs a) {
   extern __shared__ __align__(16) uint8_t smem_raw[];
-  LevelSmem& S = *reinterpret_cast<LevelSmem*>(smem_raw);
+  Level0Smem& S0 = *reinterpret_cast<Level0Smem*>(smem_raw);
+  LevelSmem& S = S0.lv;
   const int x0 = blockIdx.x * TW, y0 = blockIdx.y * TH;
+  stage_level0(S0, a, a.in0[0], x0, y0);
   load_mask_support(S, a, x0, y0);
   float acc[PPT][3];
   load_acc(a, x0, y0, acc);
+  constexpr int kMIter = (MH * MW + NT - 1) / NT;
   for (int k = 0; k < a.K; ++k) {
-    const FramePlanes& in = a.in0[k];
-    for (int i = threadIdx.x; i < GH * GW; i += NT) {
-      const int X = x0 - 4 + i % GW, Y = y0 - 4 + i / GW;
-      float4 g = make_float4(0.f, 0.f, 0.f, 0.f);
-      if (X >= 0 && Y >= 0 && X < a.wl && Y < a.hl) {
-        const uint32_t v = in.rgba[(int64_t)Y * a.pitch_l + X];
-        g = make_float4(chf(v, 0), chf(v, 1), chf(v, 2), px_alpha(v) > 0 ? 1.0f : 0.0f);
-      }
-      S.gs[i] = g;
+    // the weight sum of the M region (same for every frame; an L2 hit after
+    // the first frame), loaded before waiting for the staged planes
+    float nvr[kMIter];
+#pragma unroll
+    for (int j = 0; j < kMIter; ++j) {
+      const int i = threadIdx.x + j * NT;
+      const int X = x0 - 2 + i % MW, Y = y0 - 2 + i / MW;
+      nvr[j] = (i < MH * MW && X >= 0 && Y >= 0 && X < a.wl && Y < a.hl) ? __ldg(a.norm + (int64_t)Y * a.pitch_l + X)
+                                                                           : 0.0f;
     }
-    for (int i = threadIdx.x; i < MH * MW; i += NT) {
+    cp_async_wait_all();
+    __syncthreads();
+    for (int i = threadIdx.x; i < GH * GW; i += NT) {
+      const uint32_t v = S0.rgba[(i / GW) * SW + i % GW];
+      S.gs[i] = make_float4(chf(v, 0), chf(v, 1), chf(v, 2), px_alpha(v) > 0 ? 1.0f : 0.0f);
+    }
+#pragma unroll
+    for (int j = 0; j < kMIter; ++j) {
+      const int i = threadIdx.x + j * NT;
+      if (i >= MH * MW) break;
       const int X = x0 - 2 + i % MW, Y = y0 - 2 + i / MW;
       float m = 0.0f;
       if (X >= 0 && Y >= 0 && X < a.wl && Y < a.hl) {
-        const int64_t o = (int64_t)Y * a.pitch_l + X;
-        const float nv = a.norm[o];
-        m = nv > 1e-12f ? __fdiv_rn(in.w[o], nv) : a.inv_count;
+        const float nv = nvr[j];
+        m = nv > 1e-12f ? __fdiv_rn(S0.w[(i / MW) * SW + i % MW + 2], nv) : a.inv_count;
       }
       S.m[i] = m;
     }
     __syncthreads();
+    if (k + 1 < a.K) stage_level0(S0, a, a.in0[k + 1], x0, y0);
     if (a.levels == 1) {
       // 1x1 image: the top level is level 0 (src/fuse/pyramid.zig:1605-1649)
 #pragma unroll
@@ -645,6 +705,7 @@ __global__ void __launch_bounds__(NT) level0_kernel(const __grid_constant__ Leve
     store_next<T>(S, a, x0, y0, k);
     expand_blend_step(S, a, x0, y0, acc);
   }
+  cp_async_wait_all();
   store_acc(a, x0, y0, acc);
 }
 
@@ -693,7 +754,7 @@ static cudaError_t configure(K kernel, size_t bytes, bool* done) {
 
 template <template <typename> class KER>
 static cudaError_t launch_levels(const LevelArgs& a, int storage, cudaStream_t s, bool* cfg) {
-  const size_t sm = sizeof(LevelSmem);
+  const size_t sm = KER<float>::smem();
   dim3 grid((a.wl + TW - 1) / TW, (a.hl + TH - 1) / TH);
   cudaError_t e;
   switch (storage) {
@@ -714,8 +775,14 @@ static cudaError_t launch_levels(const LevelArgs& a, int storage, cudaStream_t s
   }
   return cudaGetLastError();
 }
-template <typename T> struct Level0K { static decltype(&level0_kernel<T>) fn() { return &level0_kernel<T>; } };
-template <typename T> struct LevelK { static decltype(&level_kernel<T>) fn() { return &level_kernel<T>; } };
+template <typename T> struct Level0K {
+  static decltype(&level0_kernel<T>) fn() { return &level0_kernel<T>; }
+  static size_t smem() { return sizeof(Level0Smem); }
+};
+template <typename T> struct LevelK {
+  static decltype(&level_kernel<T>) fn() { return &level_kernel<T>; }
+  static size_t smem() { return sizeof(LevelSmem); }
+};
 
 cudaError_t launch_level0(const LevelArgs& a, int storage, cudaStream_t s) {
   static bool cfg[3] = {false, false, false};
