@@ -79,19 +79,23 @@ __device__ __forceinline__ float window_stddev(uint32_t packed, uint32_t s2, con
 // Fill a shared region of packed RGBA samples for output pixels
 // [rx0, rx0 + RW) x [ry0, ry0 + RH) (ROI coordinates); pixels outside the ROI
 // get 0 (no support).  Optionally also the contrast words.  Work unit: 8x4
-// pixel blocks, one warp each; lane j of a warp forms the double-float
-// anchor of the warp's j-th block and hands it over by shuffle.
-constexpr int kExactQueue = 256;  // deferred exact samples per CTA and frame
+// pixel blocks, one warp each; the blocks' FP64 anchors are formed first, one
+// per thread, into shared memory.
+constexpr int kExactQueue = 256;   // deferred exact samples per CTA and frame
+constexpr int kMaxAnchors = 120;   // 8x4 blocks of the largest region (contrast window 15)
+constexpr int32_t kNoAnchor = INT32_MIN;
 
-// Shared scratch of fill_region: queue of samples the fast path could not
-// decide, processed together after the fast pass so that one lane's tie does
-// not hold its whole warp on the (long) exact path.
-struct ExactQueue {
+// Shared scratch of fill_region: the block anchors of the frame, and a queue
+// of samples the fast path could not decide, processed together after the
+// fast pass so that one lane's tie does not hold its whole warp on the
+// (long) exact path.
+struct __align__(16) ExactQueue {
+  Anchor anchor[kMaxAnchors];
   uint32_t count;
   uint32_t item[kExactQueue];  // ry << 16 | rx
 };
 
-template <int RW, int RH>
+template <int RW, int RH, int KS = RW>
 __device__ void fill_region(const FrameIn& f, int W, int H, int rx0, int ry0, uint32_t* reg, uint32_t* kv,
                             ExactQueue* q) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = NT / 32;
@@ -106,47 +110,46 @@ __device__ void fill_region(const FrameIn& f, int W, int H, int rx0, int ry0, ui
         v = pack_rgba(__ldg(p), __ldg(p + 1), __ldg(p + 2), al);
       }
       reg[i] = v;
-      if (kv) kv[i] = contrast_word(v);
+      if (kv) kv[ry * KS + rx] = contrast_word(v);
     }
     return;
   }
   constexpr int NBX = (RW + 7) / 8, NBY = (RH + 3) / 4, NB = NBX * NBY;
+  static_assert(NB <= kMaxAnchors, "anchor table too small");
   const int du = lane & 7, dv = lane >> 3;
   const bool fast_ok = f.warp.kind == WARP_HOMOGRAPHY && !f.warp.guard;
+  // phase 1: one FP64 anchor per 8x4 block into shared memory
   if (threadIdx.x == 0) q->count = 0;
+  for (int b = threadIdx.x; b < NB; b += NT) {
+    bool ok = false;
+    Anchor an = {};
+    if (fast_ok) an = make_anchor(f.warp, rx0 + (b % NBX) * 8, ry0 + (b / NBX) * 4, &ok);
+    if (!ok) an.ix = kNoAnchor;
+    q->anchor[b] = an;
+  }
   __syncthreads();
-  for (int g0 = warp; g0 < NB; g0 += nwarps * 32) {
-    Anchor mine = {};
-    bool mine_ok = false;
-    {
-      const int bj = g0 + lane * nwarps;
-      if (fast_ok && bj < NB) mine = make_anchor(f.warp, rx0 + (bj % NBX) * 8, ry0 + (bj / NBX) * 4, &mine_ok);
-    }
-    const int cnt = min(32, (NB - g0 + nwarps - 1) / nwarps);
-    for (int j = 0; j < cnt; ++j) {
-      const int blk = g0 + j * nwarps;
-      const int bx = blk % NBX, by = blk / NBX;
-      const bool aok = __shfl_sync(0xffffffffu, mine_ok ? 1 : 0, j) != 0;
-      const Anchor an = shfl_anchor(mine, j);
-      const int rx = bx * 8 + du, ry = by * 4 + dv;
-      if (rx >= RW || ry >= RH) continue;
-      const int X = rx0 + rx, Y = ry0 + ry;
-      uint32_t v = 0;
-      if (X >= 0 && Y >= 0 && X < W && Y < H) {
-        if (!aok) {
-          v = sample_exact(f.warp, f.src, X, Y);  // whole block without an anchor (guarded / lens poses)
-        } else if (!sample_try(f.src, an, du, dv, &v)) {
-          const uint32_t slot = atomicAdd(&q->count, 1u);
-          if (slot < (uint32_t)kExactQueue) {
-            q->item[slot] = ((uint32_t)ry << 16) | (uint32_t)rx;
-            continue;  // filled after the fast pass
-          }
-          v = sample_exact(f.warp, f.src, X, Y);
+  // phase 2: one warp per block, the anchor read as a shared-memory broadcast
+  for (int blk = warp; blk < NB; blk += nwarps) {
+    const int bx = blk % NBX, by = blk / NBX;
+    const int rx = bx * 8 + du, ry = by * 4 + dv;
+    if (rx >= RW || ry >= RH) continue;
+    const Anchor an = q->anchor[blk];
+    const int X = rx0 + rx, Y = ry0 + ry;
+    uint32_t v = 0;
+    if (X >= 0 && Y >= 0 && X < W && Y < H) {
+      if (an.ix == kNoAnchor) {
+        v = sample_exact(f.warp, f.src, X, Y);  // whole block without an anchor (guarded / lens poses)
+      } else if (!sample_try(f.src, an, du, dv, &v)) {
+        const uint32_t slot = atomicAdd(&q->count, 1u);
+        if (slot < (uint32_t)kExactQueue) {
+          q->item[slot] = ((uint32_t)ry << 16) | (uint32_t)rx;
+          continue;  // filled after the fast pass
         }
+        v = sample_exact(f.warp, f.src, X, Y);
       }
-      reg[ry * RW + rx] = v;
-      if (kv) kv[ry * RW + rx] = contrast_word(v);
     }
+    reg[ry * RW + rx] = v;
+    if (kv) kv[ry * KS + rx] = contrast_word(v);
   }
   __syncthreads();
   const uint32_t n = min(q->count, (uint32_t)kExactQueue);
@@ -154,7 +157,7 @@ __device__ void fill_region(const FrameIn& f, int W, int H, int rx0, int ry0, ui
     const int rx = (int)(q->item[i] & 0xFFFFu), ry = (int)(q->item[i] >> 16);
     const uint32_t v = sample_exact(f.warp, f.src, rx0 + rx, ry0 + ry);
     reg[ry * RW + rx] = v;
-    if (kv) kv[ry * RW + rx] = contrast_word(v);
+    if (kv) kv[ry * KS + rx] = contrast_word(v);
   }
 }
 
@@ -166,21 +169,22 @@ __device__ void fill_region(const FrameIn& f, int W, int H, int rx0, int ry0, ui
 template <int B>
 struct RWLayout {
   static constexpr int RW = TW + 2 * B, RH = TH + 2 * B;
+  static constexpr int KS = RW + 1, HS = TW + 1;  // odd strides: lanes on consecutive rows hit distinct banks
   static constexpr int NWIN = (2 * B + 1) * (2 * B + 1);
   static constexpr size_t bytes =
-      (size_t)RW * RH * 4 * 2 + (size_t)RH * TW * 4 * 2 + (NWIN + 1) * 4 + sizeof(ExactQueue) + 16;
+      (size_t)RW * RH * 4 + (size_t)KS * RH * 4 + (size_t)RH * HS * 4 * 2 + (NWIN + 1) * 4 + sizeof(ExactQueue) + 16;
 };
 
 template <int B>
-__global__ void __launch_bounds__(NT) remap_weights_kernel(const __grid_constant__ RemapWeightArgs a) {
+__global__ void __launch_bounds__(NT, 4) remap_weights_kernel(const __grid_constant__ RemapWeightArgs a) {
   using Lay = RWLayout<B>;
-  constexpr int RW = Lay::RW, RH = Lay::RH;
+  constexpr int RW = Lay::RW, RH = Lay::RH, KS = Lay::KS, HS = Lay::HS;
   extern __shared__ __align__(16) uint8_t smem[];
   uint32_t* reg = (uint32_t*)smem;
   uint32_t* kv = reg + RW * RH;
-  uint32_t* h1 = kv + RW * RH;   // packed count | gray sum, rows x TW
-  uint32_t* h2 = h1 + RH * TW;   // sum of k^2
-  float* inv_den = (float*)(h2 + RH * TW);
+  uint32_t* h1 = kv + KS * RH;   // packed count | gray sum, rows x TW (stride HS)
+  uint32_t* h2 = h1 + RH * HS;   // sum of k^2
+  float* inv_den = (float*)(h2 + RH * HS);
   ExactQueue* queue = (ExactQueue*)(((uintptr_t)(inv_den + Lay::NWIN + 1) + 15) & ~(uintptr_t)15);
   const int x0 = blockIdx.x * TW, y0 = blockIdx.y * TH;
   for (int n = threadIdx.x; n <= Lay::NWIN; n += NT)
@@ -200,13 +204,13 @@ __global__ void __launch_bounds__(NT) remap_weights_kernel(const __grid_constant
     }
   }
   for (int k = 0; k < a.K; ++k) {
-    fill_region<RW, RH>(a.f[k], a.W, a.H, x0 - B, y0 - B, reg, kv, queue);
+    fill_region<RW, RH, KS>(a.f[k], a.W, a.H, x0 - B, y0 - B, reg, kv, queue);
     __syncthreads();
     // horizontal sliding window sums: region row r, output columns c0 .. c0+7,
     // window = region columns [c, c + 2B]
     for (int it = threadIdx.x; it < RH * (TW / 8); it += NT) {
-      const int r = it / (TW / 8), c0 = (it % (TW / 8)) * 8;
-      const uint32_t* row = kv + r * RW + c0;
+      const int r = it % RH, c0 = (it / RH) * 8;
+      const uint32_t* row = kv + r * KS + c0;
       uint32_t p = 0, q = 0;
 #pragma unroll
       for (int t = 0; t <= 2 * B; ++t) {
@@ -215,16 +219,16 @@ __global__ void __launch_bounds__(NT) remap_weights_kernel(const __grid_constant
         p += v;
         q += g * g;
       }
-      h1[r * TW + c0] = p;
-      h2[r * TW + c0] = q;
+      h1[r * HS + c0] = p;
+      h2[r * HS + c0] = q;
 #pragma unroll
       for (int c = 1; c < 8; ++c) {
         const uint32_t vin = row[c + 2 * B], vout = row[c - 1];
         const uint32_t gin = vin & 0xFFFFFu, gout = vout & 0xFFFFFu;
         p += vin - vout;
         q += gin * gin - gout * gout;
-        h1[r * TW + c0 + c] = p;
-        h2[r * TW + c0 + c] = q;
+        h1[r * HS + c0 + c] = p;
+        h2[r * HS + c0 + c] = q;
       }
     }
     __syncthreads();
@@ -233,15 +237,15 @@ __global__ void __launch_bounds__(NT) remap_weights_kernel(const __grid_constant
       uint32_t p = 0, q = 0;
 #pragma unroll
       for (int t = 0; t <= 2 * B; ++t) {
-        p += h1[(vr0 + t) * TW + vc];
-        q += h2[(vr0 + t) * TW + vc];
+        p += h1[(vr0 + t) * HS + vc];
+        q += h2[(vr0 + t) * HS + vc];
       }
       const FramePlanes& out = a.out[k];
 #pragma unroll
       for (int i = 0; i < PPT; ++i) {
         if (i > 0) {
-          p += h1[(vr0 + i + 2 * B) * TW + vc] - h1[(vr0 + i - 1) * TW + vc];
-          q += h2[(vr0 + i + 2 * B) * TW + vc] - h2[(vr0 + i - 1) * TW + vc];
+          p += h1[(vr0 + i + 2 * B) * HS + vc] - h1[(vr0 + i - 1) * HS + vc];
+          q += h2[(vr0 + i + 2 * B) * HS + vc] - h2[(vr0 + i - 1) * HS + vc];
         }
         const int Y = y0 + vr0 + i;
         if (X >= a.W || Y >= a.H) continue;
@@ -903,32 +907,30 @@ __global__ void __launch_bounds__(NT) remap_kernel(const __grid_constant__ Remap
   constexpr int NBX = TW / 8, NBY = TH / 4, NB = NBX * NBY;
   const bool fast_ok = a.f.warp.kind == WARP_HOMOGRAPHY && !a.f.warp.guard;
   const int du = lane & 7, dv = lane >> 3;
-  for (int g0 = warp; g0 < NB; g0 += nwarps * 32) {
-    Anchor mine = {};
-    bool mine_ok = false;
-    {
-      const int bj = g0 + lane * nwarps;
-      if (fast_ok && bj < NB) mine = make_anchor(a.f.warp, x0 + (bj % NBX) * 8, y0 + (bj / NBX) * 4, &mine_ok);
-    }
-    const int cnt = min(32, (NB - g0 + nwarps - 1) / nwarps);
-    for (int j = 0; j < cnt; ++j) {
-      const int blk = g0 + j * nwarps;
-      const int AX = x0 + (blk % NBX) * 8, AY = y0 + (blk / NBX) * 4;
-      const bool aok = __shfl_sync(0xffffffffu, mine_ok ? 1 : 0, j) != 0;
-      const Anchor an = shfl_anchor(mine, j);
-      const int X = AX + du, Y = AY + dv;
-      if (X >= a.W || Y >= a.H) continue;
-      const uint32_t v = aok ? sample_fast(a.f.warp, a.f.src, an, du, dv, X, Y) : sample_exact(a.f.warp, a.f.src, X, Y);
-      uint8_t* d = a.dst + (int64_t)Y * a.dst_pitch + (int64_t)X * a.dst_ch;
-      if (a.dst_ch == 4) {
-        d[0] = v & 255u;
-        d[1] = (v >> 8) & 255u;
-        d[2] = (v >> 16) & 255u;
-        d[3] = v >> 24;
-      } else {
-        d[0] = v & 255u;
-        d[1] = v >> 24;
-      }
+  __shared__ Anchor anchor[NB];
+  for (int b = threadIdx.x; b < NB; b += NT) {
+    bool ok = false;
+    Anchor an = {};
+    if (fast_ok) an = make_anchor(a.f.warp, x0 + (b % NBX) * 8, y0 + (b / NBX) * 4, &ok);
+    if (!ok) an.ix = kNoAnchor;
+    anchor[b] = an;
+  }
+  __syncthreads();
+  for (int blk = warp; blk < NB; blk += nwarps) {
+    const int X = x0 + (blk % NBX) * 8 + du, Y = y0 + (blk / NBX) * 4 + dv;
+    if (X >= a.W || Y >= a.H) continue;
+    const Anchor an = anchor[blk];
+    const uint32_t v = an.ix != kNoAnchor ? sample_fast(a.f.warp, a.f.src, an, du, dv, X, Y)
+                                          : sample_exact(a.f.warp, a.f.src, X, Y);
+    uint8_t* d = a.dst + (int64_t)Y * a.dst_pitch + (int64_t)X * a.dst_ch;
+    if (a.dst_ch == 4) {
+      d[0] = v & 255u;
+      d[1] = (v >> 8) & 255u;
+      d[2] = (v >> 16) & 255u;
+      d[3] = v >> 24;
+    } else {
+      d[0] = v & 255u;
+      d[1] = v >> 24;
     }
   }
 }

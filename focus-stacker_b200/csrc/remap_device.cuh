@@ -2,18 +2,20 @@
 // bit-exact with the reference's f64 sampler (src/remap.zig:710-839,
 // 939-970) for 8-bit RGB / gray sources.
 //
-// Precision scheme (no FP64 on the device):
+// Precision scheme:
 //  * the source position is the host-composed projective map evaluated in
-//    double-float (two FP32) as a displacement from the output pixel, good to
-//    ~1e-12 px (fs_common.h, Warp);
-//  * FAST path: per 8x4 pixel block a double-float anchor is formed once, and
-//    each pixel's position offset from the anchor is a small FP32 rational
-//    (error < 1e-7 px).  The FP32 bilinear value is then within 1e-4 of the
-//    exact one; when every channel's value is farther than kTieBand from a
-//    .5 rounding boundary and the 4 taps lie at least one pixel inside the
-//    frame, the result is certain and equals the reference's;
-//  * EXACT path (edge band, near-ties, guarded or lens poses): everything in
-//    double-float, with the reference's edge rules (soft support, alpha =
+//    FP64 as a displacement from the output pixel, good to ~1e-13 px
+//    (fs_common.h, Warp);
+//  * FAST path: per 8x4 pixel block an FP64 anchor is formed once (split
+//    into two FP32 words), and each pixel's position offset from the anchor
+//    is a small FP32 rational (error < 1e-7 px).  The FP32 bilinear value is
+//    then within 1e-4 of the exact one; when every channel's value is farther
+//    than kTieBand from a .5 rounding boundary and the 4 taps lie at least
+//    one pixel inside the frame, the result is certain and equals the
+//    reference's;
+//  * EXACT path (edge band, near-ties, guarded or lens poses): the
+//    reference's f64 sampler op for op (products and sums rounded one by one,
+//    no fused multiply-add), with its edge rules (soft support, alpha =
 //    round(support * 255), empty sample when support <= 0).
 #pragma once
 
@@ -67,183 +69,147 @@ __device__ __forceinline__ void load_rgb_biased(const SrcImage& s, int x, int y,
   }
 }
 
-// Block anchor for the fast path.
-struct Anchor {
+// Block anchor for the fast path (48 bytes: three 16-byte shared loads).
+struct __align__(16) Anchor {
   int32_t ix, iy;        // integer part of the anchor's source position
   float fxh, fxl, fyh, fyl;  // fractional part (double-float)
   float am1x, bx, ay, bm1y, gam, eta;
 };
 
-// Displacement (source - output) of output pixel (X, Y), double-float.
-// Returns false when the denominator is outside the map's valid domain.
-__device__ __forceinline__ bool warp_disp(const Warp& w, float X, float Y, dfl* dx, dfl* dy, dfl* Dout) {
-  dfl dD = df_add(df_mul_f(w.g, X), df_mul_f(w.h, Y));
-  dfl D = df_add_f(dD, 1.0f);
+// Displacement (source - output) of output pixel (X, Y), FP64.  Returns
+// false when the denominator is outside the map's valid domain.
+__device__ __forceinline__ bool warp_disp(const Warp& w, double X, double Y, double* dx, double* dy, double* Dout) {
+  const double dD = fma(w.g, X, w.h * Y);
+  const double D = dD + 1.0;
   if (Dout) *Dout = D;
   if (w.behind_is_void) {
-    if (!(D.hi > 0.0f)) return false;
+    if (!(D > 0.0)) return false;
   } else {
-    if (fabsf(D.hi) < (float)w.eps_den) return false;
+    if (fabs(D) < w.eps_den) return false;
   }
-  dfl nx = df_add(df_add(df_mul_f(w.a, X), df_mul_f(w.b, Y)), w.c);
-  nx = df_sub(nx, df_mul_f(dD, X));
-  dfl ny = df_add(df_add(df_mul_f(w.d, X), df_mul_f(w.e, Y)), w.f);
-  ny = df_sub(ny, df_mul_f(dD, Y));
-  *dx = df_div(nx, D);
-  *dy = df_div(ny, D);
+  const double nx = fma(w.a, X, fma(w.b, Y, w.c)) - dD * X;
+  const double ny = fma(w.d, X, fma(w.e, Y, w.f)) - dD * Y;
+  *dx = nx / D;
+  *dy = ny / D;
   return true;
-}
-
-// Block anchor broadcast from lane `src` of the warp.
-__device__ __forceinline__ Anchor shfl_anchor(const Anchor& a, int src) {
-  const unsigned full = 0xffffffffu;
-  Anchor o;
-  o.ix = __shfl_sync(full, a.ix, src);
-  o.iy = __shfl_sync(full, a.iy, src);
-  o.fxh = __shfl_sync(full, a.fxh, src);
-  o.fxl = __shfl_sync(full, a.fxl, src);
-  o.fyh = __shfl_sync(full, a.fyh, src);
-  o.fyl = __shfl_sync(full, a.fyl, src);
-  o.am1x = __shfl_sync(full, a.am1x, src);
-  o.bx = __shfl_sync(full, a.bx, src);
-  o.ay = __shfl_sync(full, a.ay, src);
-  o.bm1y = __shfl_sync(full, a.bm1y, src);
-  o.gam = __shfl_sync(full, a.gam, src);
-  o.eta = __shfl_sync(full, a.eta, src);
-  return o;
 }
 
 __device__ __forceinline__ Anchor make_anchor(const Warp& w, int X, int Y, bool* ok) {
   Anchor a = {};
-  dfl dx, dy, D;
-  float Xf = (float)X, Yf = (float)Y;
-  *ok = warp_disp(w, Xf, Yf, &dx, &dy, &D);
+  double dx, dy, D;
+  const double Xd = (double)X, Yd = (double)Y;
+  *ok = warp_disp(w, Xd, Yd, &dx, &dy, &D);
   if (!*ok) return a;
-  float flx = df_floor(dx), fly = df_floor(dy);
+  const double flx = floor(dx), fly = floor(dy);
+  if (!(fabs(flx) < 1e8 && fabs(fly) < 1e8)) {
+    *ok = false;
+    return a;
+  }
   a.ix = X + (int)flx;
   a.iy = Y + (int)fly;
-  dfl fx = df_add_f(dx, -flx), fy = df_add_f(dy, -fly);
-  a.fxh = fx.hi; a.fxl = fx.lo;
-  a.fyh = fy.hi; a.fyl = fy.lo;
+  const double fx = dx - flx, fy = dy - fly;  // exact
+  a.fxh = (float)fx;
+  a.fxl = (float)(fx - (double)a.fxh);
+  a.fyh = (float)fy;
+  a.fyl = (float)(fy - (double)a.fyh);
   // x(X+du, Y+dv) - x_a - du = ((alpha-1) du + beta dv - du (gam du + eta dv)) / (1 + gam du + eta dv)
   // with alpha = (h00 - x_a h20) / D, beta = (h01 - x_a h21) / D, gam = h20 / D, eta = h21 / D,
   // h00 = 1 + a, h01 = b, h20 = g, h21 = h and x_a = X + dx.
-  dfl xa = df_add_f(dx, Xf), ya = df_add_f(dy, Yf);
-  dfl dDa = df_sub(D, df_make(1.0f));
-  dfl am1 = df_div(df_sub(df_sub(w.a, df_mul(xa, w.g)), dDa), D);
-  dfl bx = df_div(df_sub(w.b, df_mul(xa, w.h)), D);
-  dfl ay = df_div(df_sub(w.d, df_mul(ya, w.g)), D);
-  dfl bm1 = df_div(df_sub(df_sub(w.e, df_mul(ya, w.h)), dDa), D);
-  a.am1x = am1.hi; a.bx = bx.hi; a.ay = ay.hi; a.bm1y = bm1.hi;
-  a.gam = df_div(w.g, D).hi;
-  a.eta = df_div(w.h, D).hi;
+  const double xa = dx + Xd, ya = dy + Yd, dDa = D - 1.0, rD = 1.0 / D;
+  a.am1x = (float)((w.a - xa * w.g - dDa) * rD);
+  a.bx = (float)((w.b - xa * w.h) * rD);
+  a.ay = (float)((w.d - ya * w.g) * rD);
+  a.bm1y = (float)((w.e - ya * w.h - dDa) * rD);
+  a.gam = (float)(w.g * rD);
+  a.eta = (float)(w.h * rD);
   return a;
 }
 
-// Round-half-away of value / support decided exactly in double-float.
-__device__ __forceinline__ uint32_t df_round_ratio(dfl value, dfl support) {
-  float q = value.hi / support.hi;
-  float k = floorf(q);
-  dfl t = df_sub(value, df_mul_f(support, k + 0.5f));
-  float r = df_sign(t) >= 0 ? k + 1.0f : k;
-  r = fminf(fmaxf(r, 0.0f), 255.0f);
-  return (uint32_t)r;
-}
-
-// Newton radial inverse with the reference's stopping rules, double-float
-// (src/remap.zig:755-786).
-static __device__ dfl df_sqrt(dfl a) {
-  if (a.hi <= 0.0f) return df_make(0.0f);
-  float s = sqrtf(a.hi);
-  dfl s2 = df_two_prod(s, s);
-  dfl r = df_sub(a, s2);
-  float c = r.hi / (2.0f * s);
-  return df_fast_two_sum(s, c);
-}
-
-static __device__ void radial_inverse_df(const Warp& w, dfl dx, dfl dy, dfl* ox, dfl* oy) {
-  dfl q = df_sqrt(df_add(df_mul(dx, dx), df_mul(dy, dy)));
-  if (q.hi < 1e-12f) {
+// Newton radial inverse with the reference's stopping rules and operation
+// order (src/remap.zig:755-786): returns the undistorted offset.
+static __device__ void radial_inverse(const Warp& w, double dx, double dy, double* ox, double* oy) {
+  const double q = __dsqrt_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)));
+  if (q < 1e-12) {
     *ox = dx;
     *oy = dy;
     return;
   }
-  dfl r = q;
+  double r = q;
   for (int it = 0; it < 6; ++it) {
-    dfl r2 = df_mul(df_mul(r, r), w.radial_inv_norm);
-    dfl r4 = df_mul(r2, r2);
-    dfl fac = df_add(df_add(df_add_f(df_mul(w.radial_a, r2), 1.0f), df_mul(w.radial_b, r4)),
-                     df_mul(df_mul(w.radial_c, r4), r2));
-    dfl der = df_add(df_add(w.radial_a, df_mul_f(df_mul(w.radial_b, r2), 2.0f)), df_mul_f(df_mul(w.radial_c, r4), 3.0f));
-    dfl f = df_sub(df_mul(r, fac), q);
-    if (fabsf(f.hi) <= 1e-9f) break;
-    dfl dfd = df_add(fac, df_mul(df_mul_f(df_mul(df_mul(r, r), w.radial_inv_norm), 2.0f), der));
-    if (fabsf(dfd.hi) < 1e-12f) break;
-    r = df_sub(r, df_div(f, dfd));
-    if (r.hi < 0.0f) r = df_make(0.0f);
+    const double r2 = __dmul_rn(__dmul_rn(r, r), w.radial_inv_norm);
+    const double r4 = __dmul_rn(r2, r2);
+    const double fac = __dadd_rn(__dadd_rn(__dadd_rn(1.0, __dmul_rn(w.radial_a, r2)), __dmul_rn(w.radial_b, r4)),
+                                 __dmul_rn(__dmul_rn(w.radial_c, r4), r2));
+    const double fd = __dadd_rn(__dadd_rn(w.radial_a, __dmul_rn(__dmul_rn(2.0, w.radial_b), r2)),
+                                __dmul_rn(__dmul_rn(3.0, w.radial_c), r4));
+    const double f = __dsub_rn(__dmul_rn(r, fac), q);
+    if (fabs(f) <= 1e-9) break;
+    const double df = __dadd_rn(fac, __dmul_rn(__dmul_rn(__dmul_rn(__dmul_rn(2.0, r), r), w.radial_inv_norm), fd));
+    if (fabs(df) < 1e-12) break;
+    r = __dsub_rn(r, __ddiv_rn(f, df));
+    r = fmax(r, 0.0);
   }
-  dfl s = df_div(r, q);
-  *ox = df_mul(dx, s);
-  *oy = df_mul(dy, s);
+  const double sc = __ddiv_rn(r, q);
+  *ox = __dmul_rn(dx, sc);
+  *oy = __dmul_rn(dy, sc);
 }
 
-// Exact sample of output pixel (X, Y) (ROI-relative), all decisions in
-// double-float.  Follows samplePixelBilinearU8 (src/remap.zig:710-753).
+// Exact sample of output pixel (X, Y) (ROI-relative): the reference's f64
+// bilinear sampler (samplePixelBilinearU8, src/remap.zig:710-753, interior
+// :788-839, soft edge :939-994) with products and sums rounded one at a time.
 static __device__ __noinline__ uint32_t sample_exact(const Warp& w, const SrcImage& s, int X, int Y) {
-  dfl dx, dy;
-  float Xf = (float)X, Yf = (float)Y;
-  if (!warp_disp(w, Xf, Yf, &dx, &dy, nullptr)) return 0u;
+  double dx, dy;
+  const double Xd = (double)X, Yd = (double)Y;
+  if (!warp_disp(w, Xd, Yd, &dx, &dy, nullptr)) return 0u;
   int x0, y0;
-  dfl fx, fy;
+  double fx, fy;
   if (w.kind == WARP_RADIAL) {
-    dfl px = df_sub(df_add_f(dx, Xf), w.src_cx), py = df_sub(df_add_f(dy, Yf), w.src_cy);
-    dfl ux, uy;
-    radial_inverse_df(w, px, py, &ux, &uy);
-    dfl sx = df_add(w.src_cx, ux), sy = df_add(w.src_cy, uy);
-    float flx = df_floor(sx), fly = df_floor(sy);
-    if (!(fabsf(flx) < 1e8f && fabsf(fly) < 1e8f)) return 0u;
+    double ux, uy;
+    radial_inverse(w, __dsub_rn(dx + Xd, w.src_cx), __dsub_rn(dy + Yd, w.src_cy), &ux, &uy);
+    const double sx = __dadd_rn(w.src_cx, ux), sy = __dadd_rn(w.src_cy, uy);
+    const double flx = floor(sx), fly = floor(sy);
+    if (!(fabs(flx) < 1e8 && fabs(fly) < 1e8)) return 0u;
     x0 = (int)flx;
     y0 = (int)fly;
-    fx = df_add_f(sx, -flx);
-    fy = df_add_f(sy, -fly);
+    fx = sx - flx;
+    fy = sy - fly;
   } else {
-    float flx = df_floor(dx), fly = df_floor(dy);
-    if (!(fabsf(flx) < 1e8f && fabsf(fly) < 1e8f)) return 0u;
+    const double flx = floor(dx), fly = floor(dy);
+    if (!(fabs(flx) < 1e8 && fabs(fly) < 1e8)) return 0u;
     x0 = X + (int)flx;
     y0 = Y + (int)fly;
-    fx = df_add_f(dx, -flx);
-    fy = df_add_f(dy, -fly);
+    fx = dx - flx;
+    fy = dy - fly;
   }
-  dfl one = df_make(1.0f);
-  dfl omfx = df_sub(one, fx), omfy = df_sub(one, fy);
-  dfl wt[4] = {df_mul(omfx, omfy), df_mul(fx, omfy), df_mul(omfx, fy), df_mul(fx, fy)};
-  int tx[4] = {x0, x0 + 1, x0, x0 + 1};
-  int ty[4] = {y0, y0, y0 + 1, y0 + 1};
+  const double omfx = __dsub_rn(1.0, fx), omfy = __dsub_rn(1.0, fy);
+  const double wt[4] = {__dmul_rn(omfx, omfy), __dmul_rn(fx, omfy), __dmul_rn(omfx, fy), __dmul_rn(fx, fy)};
+  const int tx[4] = {x0, x0 + 1, x0, x0 + 1};
+  const int ty[4] = {y0, y0, y0 + 1, y0 + 1};
   bool inb[4];
   bool all_in = true;
+#pragma unroll
   for (int i = 0; i < 4; ++i) {
     inb[i] = tx[i] >= 0 && ty[i] >= 0 && tx[i] < s.w && ty[i] < s.h;
     all_in = all_in && inb[i];
   }
-  dfl support = df_make(0.0f);
+  double support = 0.0;
+#pragma unroll
   for (int i = 0; i < 4; ++i)
-    if (inb[i]) support = df_add(support, wt[i]);
-  if (df_sign(support) <= 0) return 0u;
-  dfl val[3] = {df_make(0.0f), df_make(0.0f), df_make(0.0f)};
+    if (inb[i]) support = __dadd_rn(support, wt[i]);
+  if (!(support > 0.0)) return 0u;
+  double val[3] = {0.0, 0.0, 0.0};
+#pragma unroll
   for (int i = 0; i < 4; ++i) {
     if (!inb[i]) continue;
     float v[3];
     load_rgb(s, tx[i], ty[i], v);
-    for (int c = 0; c < 3; ++c) val[c] = df_add(val[c], df_mul_f(wt[i], v[c]));
+#pragma unroll
+    for (int c = 0; c < 3; ++c) val[c] = __dadd_rn(val[c], __dmul_rn((double)v[c], wt[i]));
   }
   uint32_t out[3];
-  for (int c = 0; c < 3; ++c) out[c] = df_round_ratio(val[c], support);
-  uint32_t alpha;
-  if (all_in) {
-    alpha = 255u;
-  } else {
-    alpha = df_round_ratio(df_mul_f(support, 255.0f), df_make(1.0f));
-  }
+#pragma unroll
+  for (int c = 0; c < 3; ++c) out[c] = (uint32_t)fmin(fmax(round(__ddiv_rn(val[c], support)), 0.0), 255.0);
+  const uint32_t alpha = all_in ? 255u : (uint32_t)fmin(fmax(round(__dmul_rn(support, 255.0)), 0.0), 255.0);
   return pack_rgba(out[0], out[1], out[2], alpha);
 }
 

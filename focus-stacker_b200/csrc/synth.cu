@@ -249,10 +249,7 @@ int synth_render(uint64_t seed, int scene, uint32_t width, uint32_t height, uint
     fs_rect full = {0, 0, (int32_t)width, (int32_t)height};
     Warp w;
     if (!compose_warp(pose, width, height, full, &w, why)) return FS_ERR_INVALID;
-    double a = (double)w.a.hi + w.a.lo, b = (double)w.b.hi + w.b.lo, c = (double)w.c.hi + w.c.lo;
-    double d = (double)w.d.hi + w.d.lo, e = (double)w.e.hi + w.e.lo, f = (double)w.f.hi + w.f.lo;
-    double g = (double)w.g.hi + w.g.lo, h = (double)w.h.hi + w.h.lo;
-    double H[9] = {1 + a, b, c, d, 1 + e, f, g, h, 1};
+    double H[9] = {1 + w.a, w.b, w.c, w.d, 1 + w.e, w.f, w.g, w.h, 1};
     if (!invert3(H, Hs)) {
       if (why) *why = "singular synthetic pose";
       return FS_ERR_INVALID;

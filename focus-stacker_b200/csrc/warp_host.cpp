@@ -69,12 +69,6 @@ double radial_inv_norm(uint32_t w, uint32_t h) {  // src/optimize.zig:4150-4156
   return d >= 1e-12 ? 1.0 / d : 1.0;
 }
 
-dfl to_df(double v) {
-  float hi = (float)v;
-  float lo = (float)(v - (double)hi);
-  return {hi, lo};
-}
-
 // Projective map (in homogeneous form) from ROI-relative output pixels to
 // source pixels (centre included), and whether a radial inverse follows.
 struct Composed {
@@ -169,20 +163,20 @@ bool compose_warp(const fs_pose& pose, uint32_t src_w, uint32_t src_h, const fs_
   Warp w;
   std::memset(&w, 0, sizeof(w));
   w.kind = c.radial ? WARP_RADIAL : WARP_HOMOGRAPHY;
-  w.a = to_df(n[0][0] - 1.0);
-  w.b = to_df(n[0][1]);
-  w.c = to_df(n[0][2]);
-  w.d = to_df(n[1][0]);
-  w.e = to_df(n[1][1] - 1.0);
-  w.f = to_df(n[1][2]);
-  w.g = to_df(n[2][0]);
-  w.h = to_df(n[2][1]);
-  w.src_cx = to_df(c.src_cx);
-  w.src_cy = to_df(c.src_cy);
-  w.radial_a = to_df(pose.radial_a);
-  w.radial_b = to_df(pose.radial_b);
-  w.radial_c = to_df(pose.radial_c);
-  w.radial_inv_norm = to_df(c.inv_norm);
+  w.a = n[0][0] - 1.0;
+  w.b = n[0][1];
+  w.c = n[0][2];
+  w.d = n[1][0];
+  w.e = n[1][1] - 1.0;
+  w.f = n[1][2];
+  w.g = n[2][0];
+  w.h = n[2][1];
+  w.src_cx = c.src_cx;
+  w.src_cy = c.src_cy;
+  w.radial_a = pose.radial_a;
+  w.radial_b = pose.radial_b;
+  w.radial_c = pose.radial_c;
+  w.radial_inv_norm = c.inv_norm;
   // The denominator D = 1 + g X + h Y is affine: its extremes over the ROI
   // are at the corners.  The reference treats rays behind the camera as
   // empty samples (basic chain) or only rejects |denominator| < 1e-12 (lens
