@@ -60,7 +60,7 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-case", action="store_true",
-                    help="small case for ncu: 4 frames, no e2e / CPU legs, one timed step")
+                    help="small case for ncu: 8 frames of 4000x3000, no e2e / CPU legs, one timed step")
     return ap.parse_args()
 
 
@@ -178,8 +178,10 @@ def algorithmic_bytes(roi_w, roi_h, frames, k, mode="cache", storage_bytes=4):
 
 
 def profile_traffic(kernel: str):
-    """Per-launch DRAM traffic of `kernel` on this workload from a committed
-    ncu summary (profiles/<kernel>_*.md, line `traffic_bytes_per_launch: N`)."""
+    """DRAM traffic of `kernel` per frame-pixel from a committed ncu summary
+    (profiles/<kernel>_*.md, line `traffic_bytes_per_frame_px: N`), measured on
+    the small profiling case; the per-launch figure scales it by the frame-pixels
+    a launch processes."""
     pdir = os.path.join(ROOT, "profiles")
     if not os.path.isdir(pdir):
         return None
@@ -188,7 +190,7 @@ def profile_traffic(kernel: str):
             continue
         with open(os.path.join(pdir, name)) as fh:
             for line in fh:
-                if line.strip().startswith("traffic_bytes_per_launch:"):
+                if line.strip().startswith("traffic_bytes_per_frame_px:"):
                     try:
                         return float(line.split(":", 1)[1].strip().split()[0])
                     except ValueError:
@@ -291,7 +293,7 @@ def main():
         torch.cuda.set_device(local)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", local))
     if args.profile_case:
-        args.frames, args.steps, args.warmup = 4, 1, 1
+        args.frames, args.width, args.height, args.steps, args.warmup = 8, 4000, 3000, 1, 1
         args.no_e2e = args.no_cpu_baseline = True
     fsb = load_package()
     dev = local
@@ -360,7 +362,8 @@ def main():
     peak, peak_kind = measured_hbm_peak()
     per_launch = alg[dom] / max(1, n_dom)
     achieved = per_launch / (ms_dom / max(1, n_dom) / 1e3) / 1e9
-    traffic = profile_traffic(dom)
+    traffic_fp = profile_traffic(dom)
+    traffic = round(traffic_fp * px / max(1, n_dom)) if traffic_fp else None
     roofline = {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4), "traffic": traffic, "peak_source": peak_kind,
                 "alg_bytes_per_launch": per_launch, "launches_per_step": n_dom,

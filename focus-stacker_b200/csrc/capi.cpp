@@ -15,6 +15,7 @@
 #include <cstring>
 #include <map>
 #include <mutex>
+#include <set>
 #include <string>
 #include <vector>
 
@@ -49,6 +50,10 @@ struct fs_ctx {
   // stack of the same geometry (counted in `held`); fs_ctx_trim frees them.
   std::multimap<size_t, void*> pool;
   uint64_t pooled = 0;
+  // Live stacks: fs_destroy releases their device memory and detaches them,
+  // so that a later fs_stack_destroy of a stack that outlived its context
+  // only frees the host record.
+  std::set<fs_stack*> stacks;
 };
 
 namespace {
@@ -183,6 +188,7 @@ struct fs_stack {
   size_t pass1_done = 0;          // frames whose pass 1 has been launched
   bool finished = false;
   cudaEvent_t copy_done = nullptr;
+  cudaEvent_t batch_done[2] = {nullptr, nullptr};  // pass 1 of the last two batches (staging reuse)
   float* base_out = nullptr;      // optional device buffer for the collapsed base (RGB f32)
   int64_t base_pitch = 0;         // elements
 };
@@ -190,6 +196,19 @@ struct fs_stack {
 namespace {
 
 uint32_t in_channels(const fs_stack* s) { return s->d.channels; }
+
+// Free a stack's device memory and events and cut it from its context (the
+// context's streams must be idle).
+void detach_stack(fs_stack* s) {
+  if (!s->ctx) return;
+  for (auto& a : s->allocs) dev_free(s->ctx, a.p, a.bytes);
+  s->allocs.clear();
+  if (s->copy_done) cudaEventDestroy(s->copy_done);
+  for (cudaEvent_t& ev : s->batch_done)
+    if (ev) cudaEventDestroy(ev), ev = nullptr;
+  s->copy_done = nullptr;
+  s->ctx = nullptr;
+}
 
 int stack_alloc(fs_stack* s, size_t bytes, void** out) {
   int rc = dev_alloc(s->ctx, bytes, out);
@@ -256,6 +275,8 @@ int run_pending_pass1(fs_stack* s, bool flush) {
     size_t begin = s->pass1_done, end = std::min(s->frames.size(), begin + s->K);
     int rc = launch_pass1_batch(s, begin, end);
     if (rc != FS_OK) return rc;
+    cudaError_t e = cudaEventRecord(s->batch_done[(begin / s->K) % 2], s->ctx->stream);
+    if (e != cudaSuccess) return cuda_err(s->ctx, e, "pass-1 event");
     s->pass1_done = end;
   }
   return FS_OK;
@@ -320,6 +341,9 @@ void fs_destroy(fs_ctx* ctx) {
   if (!ctx) return;
   cudaSetDevice(ctx->device);
   cudaStreamSynchronize(ctx->stream);
+  cudaStreamSynchronize(ctx->copy);
+  for (fs_stack* s : ctx->stacks) detach_stack(s);
+  ctx->stacks.clear();
   pool_trim(ctx);
   for (auto& t : ctx->timings) {
     cudaEventDestroy(t.start);
@@ -509,6 +533,7 @@ int fs_stack_begin(fs_ctx* ctx, const fs_stack_desc* desc, fs_stack** out) {
   cudaSetDevice(ctx->device);
   fs_stack* s = new fs_stack();
   s->ctx = ctx;
+  ctx->stacks.insert(s);
   s->d = d;
   s->roi = roi;
   s->aligned = aligned;
@@ -568,7 +593,7 @@ int fs_stack_begin(fs_ctx* ctx, const fs_stack_desc* desc, fs_stack** out) {
   s->frame_pitch = round_up((int64_t)d.src_width * d.channels, 16);
   s->frame_bytes = (size_t)s->frame_pitch * d.src_height;
   const size_t planes_bytes = n0 * 8;
-  const size_t staging_bytes = s->frame_bytes * s->K;
+  const size_t staging_bytes = s->frame_bytes * std::min<size_t>(2 * (size_t)s->K, d.frame_count);
   if (ctx->held - ctx->pooled + planes_bytes * d.frame_count + staging_bytes <= ctx->budget) {
     s->mode = P2_CACHE;
     for (uint32_t f = 0; f < d.frame_count; ++f) {
@@ -584,12 +609,15 @@ int fs_stack_begin(fs_ctx* ctx, const fs_stack_desc* desc, fs_stack** out) {
     }
   }
   cudaEventCreateWithFlags(&s->copy_done, cudaEventDisableTiming);
+  cudaEventCreateWithFlags(&s->batch_done[0], cudaEventDisableTiming);
+  cudaEventCreateWithFlags(&s->batch_done[1], cudaEventDisableTiming);
   *out = s;
   return FS_OK;
 }
 
 static int add_frame_impl(fs_stack* s, const void* pixels, size_t row_stride, const fs_pose* pose, bool device) {
   if (!s || !pixels) return FS_ERR_INVALID;
+  if (!s->ctx) return FS_ERR_STATE;  // its context was destroyed
   fs_ctx* ctx = s->ctx;
   if (s->finished) return set_err(ctx, FS_ERR_STATE, "stack already finished");
   if (s->frames.size() >= s->d.frame_count) return set_err(ctx, FS_ERR_STATE, "more frames than frame_count");
@@ -612,18 +640,20 @@ static int add_frame_impl(fs_stack* s, const void* pixels, size_t row_stride, co
       buf = (uint8_t*)p;
       fr.owned = true;
     } else {
-      // staged for pass 1 only: one buffer per frame of the current batch
-      const size_t slot = s->frames.size() % s->K;
+      // staged for pass 1 only: two batches of buffers, so that frames of
+      // the next batch upload while pass 1 of the current one runs
+      const size_t nslots = 2 * (size_t)s->K;
+      const size_t slot = s->frames.size() % nslots;
       while (s->staging.size() <= slot) {
         void* p;
         int rc = stack_alloc(s, s->frame_bytes, &p);
         if (rc != FS_OK) return rc;
         s->staging.push_back((uint8_t*)p);
       }
-      if (slot == 0 && s->frames.size() > 0) {
-        // the previous batch's pass 1 must be done with the staging buffers
-        cudaError_t e = cudaStreamSynchronize(ctx->stream);
-        if (e != cudaSuccess) return cuda_err(ctx, e, "synchronize");
+      if (slot % s->K == 0 && s->frames.size() >= nslots) {
+        // pass 1 of the batch two back read these buffers: the upload waits for it
+        cudaError_t e = cudaStreamWaitEvent(ctx->copy, s->batch_done[(s->frames.size() / s->K) % 2], 0);
+        if (e != cudaSuccess) return cuda_err(ctx, e, "staging reuse");
       }
       buf = s->staging[slot];
       fr.resident = false;
@@ -657,6 +687,7 @@ int fs_stack_add_frame_device(fs_stack* stack, const void* dev_pixels, size_t ro
 static int finish_impl(fs_stack* s, fs_frame_fetch_cb refetch, void* user, void* out, size_t out_stride,
                        bool device_out) {
   if (!s || !out) return FS_ERR_INVALID;
+  if (!s->ctx) return FS_ERR_STATE;  // its context was destroyed
   fs_ctx* ctx = s->ctx;
   if (s->finished) return set_err(ctx, FS_ERR_STATE, "stack already finished");
   if (s->frames.size() != s->d.frame_count)
@@ -797,6 +828,7 @@ int fs_stack_finish_device(fs_stack* stack, fs_frame_fetch_cb refetch, void* use
 
 int fs_stack_set_base_output(fs_stack* s, float* dev_base, size_t row_stride_elems) {
   if (!s) return FS_ERR_INVALID;
+  if (!s->ctx) return FS_ERR_STATE;
   if (dev_base && row_stride_elems < (size_t)s->W * 3) return set_err(s->ctx, FS_ERR_INVALID, "base stride too small");
   s->base_out = dev_base;
   s->base_pitch = (int64_t)row_stride_elems;
@@ -812,12 +844,15 @@ int fs_stack_output_size(const fs_stack* s, uint32_t* width, uint32_t* height) {
 
 int fs_stack_destroy(fs_stack* s) {
   if (!s) return FS_ERR_INVALID;
-  fs_ctx* ctx = s->ctx;
-  cudaSetDevice(ctx->device);
-  cudaStreamSynchronize(ctx->stream);
-  cudaStreamSynchronize(ctx->copy);
-  for (auto& a : s->allocs) dev_release(ctx, a.p, a.bytes);
-  if (s->copy_done) cudaEventDestroy(s->copy_done);
+  if (fs_ctx* ctx = s->ctx) {
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    cudaStreamSynchronize(ctx->copy);
+    for (auto& a : s->allocs) dev_release(ctx, a.p, a.bytes);
+    s->allocs.clear();
+    ctx->stacks.erase(s);
+    detach_stack(s);
+  }
   delete s;
   return FS_OK;
 }

@@ -249,7 +249,8 @@ def test_refetch_path_matches_resident(torch, ctx):
     state = ctx.device_bytes() - before - F * n0 * 8  # without the per-frame pass-1 planes
     probe.close()
     ctx.trim()
-    small = fsb.Context(0, hbm_budget_bytes=state + 2 * n0 * 8 + 3 * W * H * 3 + 4096)
+    # per-batch planes for K = 2 frames and two batches of staging buffers
+    small = fsb.Context(0, hbm_budget_bytes=state + 2 * n0 * 8 + 4 * W * H * 3 + 4096)
     st = fsb.PyramidContrastStack(small, W, H, F, roi=roi, frames_per_batch=2)
     assert st.pass2_mode == "refetch"
     for f, p in zip(frames, poses):
@@ -270,7 +271,7 @@ def test_refetch_path_matches_resident(torch, ctx):
 def test_pass2_modes_give_identical_results(torch, ctx):
     # cache (pass-1 planes kept), resident (frames kept, remapped again) and
     # refetch (frames fetched again) must produce the same bytes
-    W, H, F = 240, 160, 6
+    W, H, F = 240, 160, 8
     frames, poses = synth_stack(torch, ctx, W, H, F, seed=12)
     roi = fsb.compute_common_overlap_roi([True] * F, [W] * F, [H] * F, poses)
     results = {}
@@ -292,7 +293,8 @@ def test_pass2_modes_give_identical_results(torch, ctx):
             state = c.device_bytes() - F * n0 * 8
             st0.close()
             c.close()
-            extra = 3 * n0 * 8 + F * frame_b + 3 * frame_b + 4096 if want == "resident" else 3 * n0 * 8 + 3 * frame_b + 4096
+            # resident: K = 3 batch planes + every frame; refetch: K planes + two batches of staging
+            extra = 3 * n0 * 8 + F * frame_b + 3 * frame_b + 4096 if want == "resident" else 3 * n0 * 8 + 6 * frame_b + 4096
             c = fsb.Context(0, hbm_budget_bytes=state + extra)
         st = fsb.PyramidContrastStack(c, W, H, F, roi=roi, frames_per_batch=3)
         assert st.pass2_mode == want
@@ -332,3 +334,14 @@ def test_stack_errors(torch, ctx):
     with pytest.raises(fsb.FocusCudaError) as e:
         fsb.PyramidContrastStack(fsb.Context(0, hbm_budget_bytes=1024), 640, 480, 2)
     assert e.value.code == "FS_ERR_BUDGET"
+
+
+def test_stack_outliving_its_context(torch):
+    # destroying a context releases its stacks' device memory; the stack
+    # handles stay valid for fs_stack_destroy and report a state error
+    c = fsb.Context(0)
+    st = fsb.PyramidContrastStack(c, 64, 48, 2, aligned=True)
+    c.close()
+    with pytest.raises(fsb.FocusCudaError):
+        st.add_frame(np.zeros((48, 64, 3), np.uint8))
+    st.close()
