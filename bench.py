@@ -25,6 +25,7 @@ from __future__ import annotations
 
 import argparse
 import json
+import math
 import os
 import statistics
 import subprocess
@@ -59,6 +60,9 @@ def parse():
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-forms", action="store_true", help="skip the precision / serving / batched legs")
+    ap.add_argument("--precision-frames", type=int, default=143,
+                    help="frames of the precision-form stack (7952x5304 each)")
     ap.add_argument("--profile-case", action="store_true",
                     help="small case for ncu: 8 frames of 4000x3000, no e2e / CPU legs, one timed step")
     return ap.parse_args()
@@ -198,6 +202,77 @@ def profile_traffic(kernel: str):
     return None
 
 
+def timed_steps(torch, stream, step, steps, warmup):
+    """Mean device time of `step` over `steps` runs after `warmup` runs, CUDA
+    events on the library's stream."""
+    for _ in range(warmup):
+        step()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        step()
+    e1.record(stream)
+    e1.synchronize()
+    return e0.elapsed_time(e1) / steps
+
+
+def precision_form(fsb, torch, dev, seed, frames_n, W=7952, H=5304, steps=2, warmup=1):
+    """Precision form: the same stack with pyramid levels stored in FP32, FP16
+    and BF16 (weight sums, blends and accumulators FP32 in all three).  Reports
+    throughput of each and the error of the reduced forms against the FP32
+    path's collapsed base on this stack (the FP32 path itself is held to 1/257
+    of the FP64 oracle by the test suite, which also measures the reduced forms
+    against the FP64 oracle directly)."""
+    ctx = fsb.Context(dev)
+    frames, poses = [], []
+    for k in range(frames_n):
+        buf = torch.empty((H, W, 3), dtype=torch.uint8, device=f"cuda:{dev}")
+        poses.append(fsb.synth_frame_device(ctx, seed, fsb.SCENE_PRODUCTION, W, H, k, frames_n, buf, W * 3))
+        frames.append(buf)
+    roi = fsb.compute_common_overlap_roi([True] * frames_n, [W] * frames_n, [H] * frames_n, poses)
+    out = torch.empty((roi.height, roi.width, 3), dtype=torch.uint8, device=f"cuda:{dev}")
+    stream = torch.cuda.ExternalStream(ctx.stream_handle(), device=f"cuda:{dev}")
+    px = frames_n * roi.width * roi.height
+    res = {"workload": f"{frames_n}x{W}x{H} RGB u8 synthetic focus stack (production scene), ROI "
+                       f"{roi.width}x{roi.height}, frames streamed through device-resident accumulators"}
+    bases = {}
+    for storage in (fsb.STORAGE_F32, fsb.STORAGE_F16, fsb.STORAGE_BF16):
+        name = fsb.STORAGE_NAMES[storage]
+        info = {}
+
+        def step(base=None):
+            st = fsb.PyramidContrastStack(ctx, W, H, frames_n, roi=roi, level_storage=storage)
+            info["pass2"] = st.pass2_mode
+            if base is not None:
+                st.set_base_output(base, roi.width * 3)
+            for f, p in zip(frames, poses):
+                st.add_frame_device(f, W * 3, p)
+            st.finish_device(out, roi.width * 3)
+            st.close()
+
+        base = torch.empty((roi.height, roi.width, 3), dtype=torch.float32, device=f"cuda:{dev}")
+        step(base)
+        ms = timed_steps(torch, stream, step, steps, warmup)
+        bases[storage] = base
+        res[name] = {"value": round(px / (ms / 1e3) / 1e6, 2), "unit": UNIT, "ms_per_step": round(ms, 3),
+                     "pass2": info["pass2"]}
+    ref = bases[fsb.STORAGE_F32].double()
+    for storage in (fsb.STORAGE_F16, fsb.STORAGE_BF16):
+        d = (bases[storage].double() - ref).abs()
+        mse = float((d * d).mean())
+        res[fsb.STORAGE_NAMES[storage]]["vs_f32_path"] = {
+            "max_abs": float(d.max()), "max_abs_lsb16": float(d.max()) * 257.0,
+            "psnr_db": float("inf") if mse == 0 else 10.0 * math.log10(255.0 ** 2 / mse)}
+        res[fsb.STORAGE_NAMES[storage]]["speedup_vs_f32"] = round(
+            res[fsb.STORAGE_NAMES[storage]]["value"] / res["f32"]["value"], 3)
+    del frames, bases, ref
+    ctx.close()
+    torch.cuda.empty_cache()
+    return res
+
+
 def measured_hbm_peak():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
@@ -294,7 +369,7 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", local))
     if args.profile_case:
         args.frames, args.width, args.height, args.steps, args.warmup = 8, 4000, 3000, 1, 1
-        args.no_e2e = args.no_cpu_baseline = True
+        args.no_e2e = args.no_cpu_baseline = args.no_forms = True
     fsb = load_package()
     dev = local
     F, W, H = args.frames, args.width, args.height
@@ -407,6 +482,13 @@ def main():
                "d2h_bytes_per_step": roi.width * roi.height * 3, "ms_per_step": dt * 1e3}
         del hframes
 
+    forms = None
+    if not args.no_forms:
+        del frames
+        ctx.trim()
+        torch.cuda.empty_cache()
+        forms = {"precision": precision_form(fsb, torch, dev, args.seed + rank, args.precision_frames)}
+
     cpu = None
     if not args.no_cpu_baseline and rank == 0 and world == 1:
         cpu = cpu_baseline(fsb, steps=1, warmup=1, sample=(4, 3976, 2652), ctx=ctx, torch=torch)
@@ -417,7 +499,7 @@ def main():
                 "vs_baseline": None, "dtype": "f32", "data": "synthetic",
                 "config": dict(workload_config(args, roi, k_eff), pass2=mode_used["mode"]),
                 "e2e": e2e, "gpu_launches": launches, "clocks": clock_info, "roofline": roofline,
-                "cpu_baseline": cpu, "kernels": kernel_table, "pipeline_roofline": pipeline}
+                "cpu_baseline": cpu, "kernels": kernel_table, "pipeline_roofline": pipeline, "forms": forms}
         print(json.dumps(line), flush=True)
     ctx.close()
     if dist:

@@ -402,6 +402,28 @@ def fuse_aligned_images(ctx: Context, images: Sequence[np.ndarray], contrast_win
         return st.finish()
 
 
+# ------------------------------------------------------------ precision form
+STORAGE_F32 = 0   # pyramid levels stored in FP32 (the plain method)
+STORAGE_F16 = 1   # levels stored in FP16, blends and accumulators in FP32
+STORAGE_BF16 = 2  # levels stored in BF16, blends and accumulators in FP32
+STORAGE_NAMES = {STORAGE_F32: "f32", STORAGE_F16: "f16", STORAGE_BF16: "bf16"}
+
+
+def error_vs_reference(base: np.ndarray, ref_base: np.ndarray, out: Optional[np.ndarray] = None,
+                       ref_out: Optional[np.ndarray] = None) -> dict:
+    """Error of a fused result against a reference evaluation (the FP64
+    oracle): max-abs and PSNR (peak 255) of the collapsed base before
+    quantisation, in 8-bit units and in LSBs of a 16-bit output (x 257), and
+    the largest u8 output difference when both outputs are given."""
+    d = np.abs(np.asarray(base, np.float64) - np.asarray(ref_base, np.float64))
+    mse = float(np.mean(d * d))
+    r = {"max_abs": float(d.max()), "max_abs_lsb16": float(d.max() * 257.0),
+         "psnr_db": float("inf") if mse == 0 else float(10.0 * np.log10(255.0 ** 2 / mse))}
+    if out is not None and ref_out is not None:
+        r["max_u8_diff"] = int(np.abs(out.astype(np.int16) - ref_out.astype(np.int16)).max())
+    return r
+
+
 # ------------------------------------------------------------------ synthetic
 SCENE_SMALL = 0       # blur <= 3 px, shifts +-20 px, roll +-0.2 deg (1024x768-class stacks)
 SCENE_PRODUCTION = 1  # blur <= 8 px, shifts +-60 px, roll +-0.3 deg (7952x5304-class stacks)
