@@ -63,6 +63,9 @@ def parse():
     ap.add_argument("--no-forms", action="store_true", help="skip the precision / serving / batched legs")
     ap.add_argument("--precision-frames", type=int, default=143,
                     help="frames of the precision-form stack (7952x5304 each)")
+    ap.add_argument("--serving-requests", type=int, default=500, help="requests per arrival rate (serving form)")
+    ap.add_argument("--serving-rates", default="20,40", help="swept Poisson arrival rates, requests/s")
+    ap.add_argument("--serving-budget-gb", type=float, default=120.0)
     ap.add_argument("--profile-case", action="store_true",
                     help="small case for ncu: 8 frames of 4000x3000, no e2e / CPU legs, one timed step")
     return ap.parse_args()
@@ -271,6 +274,35 @@ def precision_form(fsb, torch, dev, seed, frames_n, W=7952, H=5304, steps=2, war
     ctx.close()
     torch.cuda.empty_cache()
     return res
+
+
+def serving_form(fsb, torch, dev, seed, n_requests, rates, budget_gb, workers=8):
+    """Serving form: Poisson request streams (sizes 640x480 .. 6000x4000 with
+    4-40 frames, 5 % 7952x5304 stacks of up to 143 frames) admitted against an
+    HBM budget; frames are device-resident (a synthetic pool per size, as a
+    GPU decoder would leave them) and streamed one at a time into each stack."""
+    sv = fsb.serving
+    ctx = fsb.Context(dev)
+    sizes = list(sv.SIZE_MIX) + [sv.LARGE]
+    depth = {s: 40 for s in sv.SIZE_MIX}
+    depth[sv.LARGE] = 143
+    pool = sv.SynthFramePool(ctx, torch, dev, seed, sizes, depth)
+    out = {"workload": f"{n_requests} Poisson requests per rate; sizes {list(sv.SIZE_MIX)} with 4-40 frames, 5% "
+                       f"7952x5304 with 4-143 frames; {budget_gb:g} GB HBM budget; {workers} workers; "
+                       f"device-resident frames",
+           "rates": {}}
+    with sv.StackServer(dev, hbm_budget_bytes=int(budget_gb * 1e9), workers=workers, prewarm=True) as srv:
+        # warm-up: one request of each size
+        warm = [sv.StackRequest(i, 0.0, w, h, 4) for i, (w, h) in enumerate(sizes)]
+        srv.serve(warm, pool.roi, pool.frame, torch)
+        for rate in rates:
+            reqs = sv.poisson_stream(n_requests, rate, seed=seed * 1000 + int(rate))
+            rep = srv.serve(reqs, pool.roi, pool.frame, torch)
+            out["rates"][f"{rate:g}"] = rep.summary()
+    del pool
+    ctx.close()
+    torch.cuda.empty_cache()
+    return out
 
 
 def measured_hbm_peak():
@@ -488,6 +520,10 @@ def main():
         ctx.trim()
         torch.cuda.empty_cache()
         forms = {"precision": precision_form(fsb, torch, dev, args.seed + rank, args.precision_frames)}
+        if args.serving_requests > 0:
+            rates = [float(x) for x in args.serving_rates.split(",") if x]
+            forms["serving"] = serving_form(fsb, torch, dev, args.seed + rank, args.serving_requests, rates,
+                                            args.serving_budget_gb)
 
     cpu = None
     if not args.no_cpu_baseline and rank == 0 and world == 1:

@@ -23,11 +23,11 @@ STATUS_NAMES = {
 # Every function the header declares (checked by the CPU tests).
 EXPORTED = (
     "fs_create", "fs_destroy", "fs_last_error", "fs_status_string", "fs_api_version", "fs_ctx_device_bytes",
-    "fs_ctx_synchronize", "fs_ctx_trim", "fs_ctx_stream", "fs_ctx_launch_count", "fs_ctx_set_kernel_timing", "fs_ctx_kernel_stats",
+    "fs_ctx_synchronize", "fs_ctx_trim", "fs_ctx_reserve", "fs_ctx_set_budget", "fs_ctx_stream", "fs_ctx_launch_count", "fs_ctx_set_kernel_timing", "fs_ctx_kernel_stats",
     "fs_pose_default", "fs_compute_roi", "fs_inverse_map_points", "fs_forward_map_points", "fs_exact_expand_divisor",
     "fs_remap_frame", "fs_remap_frame_device",
     "fs_stack_begin", "fs_stack_add_frame", "fs_stack_add_frame_device", "fs_stack_finish",
-    "fs_stack_finish_device", "fs_stack_set_base_output", "fs_stack_pass2_mode", "fs_stack_output_size", "fs_stack_destroy", "fs_fuse_stack",
+    "fs_stack_finish_device", "fs_stack_set_base_output", "fs_stack_pass2_mode", "fs_stack_footprint", "fs_stack_output_size", "fs_stack_destroy", "fs_fuse_stack",
     "fs_fuse_aligned_device_static", "fs_synth_frame_device", "fs_synth_pose",
 )
 
@@ -88,6 +88,8 @@ def _bind(L):
     L.fs_ctx_device_bytes.restype = u64
     L.fs_ctx_synchronize.argtypes = [ctx]
     L.fs_ctx_trim.argtypes = [ctx]
+    L.fs_ctx_reserve.argtypes = [ctx, u64]
+    L.fs_ctx_set_budget.argtypes = [ctx, u64]
     L.fs_ctx_stream.argtypes = [ctx, P(vp)]
     L.fs_ctx_launch_count.argtypes = [ctx]
     L.fs_ctx_launch_count.restype = u64
@@ -110,6 +112,7 @@ def _bind(L):
     L.fs_stack_output_size.argtypes = [vp, P(u32), P(u32)]
     L.fs_stack_set_base_output.argtypes = [vp, vp, sz]
     L.fs_stack_pass2_mode.argtypes = [vp]
+    L.fs_stack_footprint.argtypes = [P(FsStackDesc), u64, i32, P(u64), P(i32)]
     L.fs_stack_destroy.argtypes = [vp]
     L.fs_fuse_stack.argtypes = [ctx, P(FsStackDesc), P(vp), P(sz), P(FsPose), vp, sz]
     L.fs_fuse_aligned_device_static.argtypes = [P(vp), P(sz), u32, u32, u32, u32, u32, vp, sz, vp,

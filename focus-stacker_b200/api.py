@@ -185,6 +185,14 @@ class Context:
     def trim(self):
         _check(L().fs_ctx_trim(self.handle), self.handle)
 
+    def reserve(self, nbytes: int):
+        """Grow the device's shared memory pool by nbytes (kept cached)."""
+        _check(L().fs_ctx_reserve(self.handle, int(nbytes)), self.handle)
+
+    def set_budget(self, hbm_budget_bytes: int):
+        """Change the HBM budget later allocations and pass-2 mode choices use."""
+        _check(L().fs_ctx_set_budget(self.handle, int(hbm_budget_bytes)), self.handle)
+
     def stream_handle(self) -> int:
         """cudaStream_t of the context (e.g. for torch.cuda.ExternalStream)."""
         v = ctypes.c_void_p()
@@ -270,6 +278,38 @@ def remap_rigid_image_device(ctx: Context, src, src_stride: int, width: int, hei
 
 
 # --------------------------------------------------------------------- fusion
+PASS2_MODES = ("cache", "resident", "refetch")
+
+
+def stack_desc(src_width: int, src_height: int, frame_count: int, roi: Optional[Rect] = None, channels: int = 3,
+               contrast_window: int = 5, aligned: bool = False, frames_per_batch: int = 0,
+               level_storage: int = 0) -> _lib.FsStackDesc:
+    d = _lib.FsStackDesc()
+    d.src_width, d.src_height = src_width, src_height
+    d.has_roi = 1 if roi is not None else 0
+    if roi is not None:
+        d.roi = roi.to_c()
+    d.channels = channels
+    d.sample_bits = 8
+    d.frame_count = frame_count
+    d.contrast_window = contrast_window
+    d.input_is_aligned = 1 if aligned else 0
+    d.level_storage = level_storage
+    d.frames_per_batch = frames_per_batch
+    return d
+
+
+def stack_footprint(desc: _lib.FsStackDesc, available_bytes: int, host_frames: bool = True):
+    """(device bytes, pass-2 mode, fits) of a stack when `available_bytes` of
+    budget are free; allocates nothing."""
+    b, m = ctypes.c_uint64(), ctypes.c_int32()
+    rc = L().fs_stack_footprint(ctypes.byref(desc), int(available_bytes), 1 if host_frames else 0, ctypes.byref(b),
+                                ctypes.byref(m))
+    if rc not in (_lib.FS_OK, 3):
+        raise FocusCudaError(rc, "fs_stack_footprint")
+    return int(b.value), PASS2_MODES[m.value], rc == _lib.FS_OK
+
+
 class PyramidContrastStack:
     """Streaming two-pass pyramid-contrast fusion on the device (fs_stack).
 
@@ -280,18 +320,8 @@ class PyramidContrastStack:
                  channels: int = 3, contrast_window: int = 5, aligned: bool = False, frames_per_batch: int = 0,
                  level_storage: int = 0):
         self.ctx = ctx
-        d = _lib.FsStackDesc()
-        d.src_width, d.src_height = src_width, src_height
-        d.has_roi = 1 if roi is not None else 0
-        if roi is not None:
-            d.roi = roi.to_c()
-        d.channels = channels
-        d.sample_bits = 8
-        d.frame_count = frame_count
-        d.contrast_window = contrast_window
-        d.input_is_aligned = 1 if aligned else 0
-        d.level_storage = level_storage
-        d.frames_per_batch = frames_per_batch
+        d = stack_desc(src_width, src_height, frame_count, roi, channels, contrast_window, aligned, frames_per_batch,
+                       level_storage)
         self.desc = d
         h = ctypes.c_void_p()
         _check(L().fs_stack_begin(ctx.handle, ctypes.byref(d), ctypes.byref(h)), ctx.handle)

@@ -46,10 +46,13 @@ struct fs_ctx {
   bool timing = false;
   std::vector<KernelTiming> timings;
   uint64_t launches = 0;
-  // Device buffers released by finished stacks, kept for reuse by the next
-  // stack of the same geometry (counted in `held`); fs_ctx_trim frees them.
-  std::multimap<size_t, void*> pool;
-  uint64_t pooled = 0;
+  // Stream-ordered memory pool of the device, shared by every context of
+  // the process on it: buffers are allocated and freed on a context's
+  // streams (no device-wide synchronisation) and freed memory stays cached in
+  // the pool for later stacks of any context until fs_ctx_trim.  The budget
+  // counts live buffers (`held`); the cache never exceeds the peak of live
+  // buffers of all contexts together.
+  cudaMemPool_t mempool = nullptr;
   // Live stacks: fs_destroy releases their device memory and detaches them,
   // so that a later fs_stack_destroy of a stack that outlived its context
   // only frees the host record.
@@ -75,51 +78,61 @@ int cuda_err(fs_ctx* ctx, cudaError_t e, const char* what) {
   return set_err(ctx, FS_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
 }
 
-void pool_trim(fs_ctx* ctx) {
-  for (auto& kv : ctx->pool) {
-    cudaFree(kv.second);
-    ctx->held -= std::min<uint64_t>(ctx->held, kv.first);
+// The device's shared pool (created once; cached memory is kept until trimmed).
+cudaMemPool_t device_pool(int device) {
+  static std::mutex mu;
+  static std::map<int, cudaMemPool_t> pools;
+  std::lock_guard<std::mutex> g(mu);
+  auto it = pools.find(device);
+  if (it != pools.end()) return it->second;
+  cudaMemPoolProps props;
+  std::memset(&props, 0, sizeof(props));
+  props.allocType = cudaMemAllocationTypePinned;
+  props.handleTypes = cudaMemHandleTypeNone;
+  props.location.type = cudaMemLocationTypeDevice;
+  props.location.id = device;
+  cudaMemPool_t pool = nullptr;
+  if (cudaMemPoolCreate(&pool, &props) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
   }
-  ctx->pool.clear();
-  ctx->pooled = 0;
+  uint64_t keep = UINT64_MAX;
+  cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  pools[device] = pool;
+  return pool;
 }
 
-int dev_alloc(fs_ctx* ctx, size_t bytes, void** out) {
+// Release the pool's cached (freed) memory; waits for the context's streams.
+void pool_trim(fs_ctx* ctx) {
+  cudaStreamSynchronize(ctx->stream);
+  cudaStreamSynchronize(ctx->copy);
+  if (ctx->mempool) cudaMemPoolTrimTo(ctx->mempool, 0);
+}
+
+// Buffer from the device pool, ordered on `on` (the compute stream by
+// default; frame buffers that the copy stream fills first are allocated on
+// the copy stream, so that uploads never wait for queued kernels).
+int dev_alloc(fs_ctx* ctx, size_t bytes, void** out, cudaStream_t on = nullptr) {
   if (bytes == 0) bytes = 16;
-  auto it = ctx->pool.find(bytes);
-  if (it != ctx->pool.end()) {
-    *out = it->second;
-    ctx->pool.erase(it);
-    ctx->pooled -= bytes;
-    return FS_OK;
-  }
-  if (ctx->held + bytes > ctx->budget && ctx->pooled > 0) pool_trim(ctx);
   if (ctx->held + bytes > ctx->budget)
     return set_err(ctx, FS_ERR_BUDGET, "device memory budget exceeded (" + std::to_string(ctx->held + bytes) +
                                            " > " + std::to_string(ctx->budget) + " bytes)");
-  cudaError_t e = cudaMalloc(out, bytes);
+  cudaError_t e = cudaMallocFromPoolAsync(out, bytes, ctx->mempool, on ? on : ctx->stream);
   if (e != cudaSuccess) {
     cudaGetLastError();
-    return set_err(ctx, FS_ERR_OOM, std::string("cudaMalloc failed: ") + cudaGetErrorString(e));
+    return set_err(ctx, FS_ERR_OOM, std::string("device allocation failed: ") + cudaGetErrorString(e));
   }
   ctx->held += bytes;
   return FS_OK;
 }
 
+// Stream-ordered free; callers make sure the copy stream is done with the
+// buffer (stacks synchronise both streams before releasing).
 void dev_free(fs_ctx* ctx, void* p, size_t bytes) {
   if (!p) return;
-  cudaFree(p);
+  cudaFreeAsync(p, ctx->stream);
   if (bytes == 0) bytes = 16;
   ctx->held -= std::min<uint64_t>(ctx->held, bytes);
-}
-
-// Return a buffer to the context's pool (stream-ordered: callers synchronize
-// the stream before releasing).
-void dev_release(fs_ctx* ctx, void* p, size_t bytes) {
-  if (!p) return;
-  if (bytes == 0) bytes = 16;
-  ctx->pool.emplace(bytes, p);
-  ctx->pooled += bytes;
 }
 
 // Launch wrapper: counts launches and optionally brackets them with events
@@ -210,8 +223,8 @@ void detach_stack(fs_stack* s) {
   s->ctx = nullptr;
 }
 
-int stack_alloc(fs_stack* s, size_t bytes, void** out) {
-  int rc = dev_alloc(s->ctx, bytes, out);
+int stack_alloc(fs_stack* s, size_t bytes, void** out, cudaStream_t on = nullptr) {
+  int rc = dev_alloc(s->ctx, bytes, out, on);
   if (rc == FS_OK) s->allocs.push_back({*out, bytes == 0 ? 16 : bytes});
   return rc;
 }
@@ -328,7 +341,8 @@ int fs_create(int device, uint64_t hbm_budget_bytes, fs_ctx** out) {
   size_t free_b = 0, total_b = 0;
   cudaMemGetInfo(&free_b, &total_b);
   c->budget = hbm_budget_bytes ? hbm_budget_bytes : (uint64_t)(free_b / 2);
-  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
+  c->mempool = device_pool(device);
+  if (!c->mempool || cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaStreamCreateWithFlags(&c->copy, cudaStreamNonBlocking) != cudaSuccess) {
     delete c;
     return FS_ERR_CUDA;
@@ -360,6 +374,27 @@ const char* fs_last_error(const fs_ctx* ctx) {
 }
 
 uint64_t fs_ctx_device_bytes(const fs_ctx* ctx) { return ctx ? ctx->held : 0; }
+
+int fs_ctx_set_budget(fs_ctx* ctx, uint64_t hbm_budget_bytes) {
+  if (!ctx || hbm_budget_bytes == 0) return FS_ERR_INVALID;
+  ctx->budget = hbm_budget_bytes;
+  return FS_OK;
+}
+
+int fs_ctx_reserve(fs_ctx* ctx, uint64_t bytes) {
+  if (!ctx) return FS_ERR_INVALID;
+  if (bytes == 0) return FS_OK;
+  cudaSetDevice(ctx->device);
+  void* p = nullptr;
+  cudaError_t e = cudaMallocFromPoolAsync(&p, bytes, ctx->mempool, ctx->stream);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return set_err(ctx, FS_ERR_OOM, std::string("reserve: ") + cudaGetErrorString(e));
+  }
+  e = cudaFreeAsync(p, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  return e == cudaSuccess ? FS_OK : cuda_err(ctx, e, "reserve");
+}
 
 int fs_ctx_trim(fs_ctx* ctx) {
   if (!ctx) return FS_ERR_INVALID;
@@ -513,45 +548,120 @@ int fs_remap_frame_device(fs_ctx* ctx, const void* src, size_t src_stride, uint3
 }
 
 // ------------------------------------------------------------------- stacks
+namespace {
+
+// Validation of a stack description (null when valid; the status in *code).
+const char* check_desc(const fs_stack_desc& d, int* code) {
+  *code = FS_ERR_INVALID;
+  if (d.sample_bits != 8) {
+    *code = FS_ERR_UNSUPPORTED;
+    return "only 8-bit samples are implemented";
+  }
+  if (d.src_width == 0 || d.src_height == 0 || d.frame_count == 0) return "empty stack";
+  if (d.contrast_window < 3 || (d.contrast_window & 1) == 0) return "contrast window must be odd and >= 3";
+  if (d.contrast_window > 2 * kMaxBorder + 1) {
+    *code = FS_ERR_UNSUPPORTED;
+    return "contrast window larger than 15";
+  }
+  if (d.level_storage != FS_STORAGE_F32 && d.level_storage != FS_STORAGE_F16 && d.level_storage != FS_STORAGE_BF16)
+    return "unknown level storage";
+  const bool aligned = d.input_is_aligned != 0;
+  if (aligned ? (d.channels != 3 && d.channels != 4) : d.channels != 3)
+    return "channels must be 3 (RGB source) or 3/4 (aligned RGB/RGBA)";
+  if (!aligned && d.has_roi && (d.roi.right <= d.roi.left || d.roi.bottom <= d.roi.top)) return "empty roi";
+  return nullptr;
+}
+
+// Geometry and device-memory plan of a stack: what fs_stack_begin allocates
+// (fixed state, per-frame or per-batch planes) and what add_frame adds later
+// (upload staging or kept frames).
+struct StackPlan {
+  fs_rect roi;
+  uint32_t W, H, L, K;
+  std::vector<uint32_t> lw, lh;
+  std::vector<int64_t> pitch;
+  size_t fixed = 0;          // weight sum, union, supports, accumulators, level slots, output
+  size_t planes = 0;         // pass-1 planes of one frame (RGBA + weight)
+  size_t frame_bytes = 0;    // one device copy of a source frame
+  int64_t frame_pitch = 0;
+  size_t staging_slots = 0;  // frame buffers of the two-batch upload ring
+};
+
+StackPlan plan_stack(const fs_stack_desc& d) {
+  StackPlan p;
+  const bool aligned = d.input_is_aligned != 0;
+  p.roi = d.has_roi && !aligned ? d.roi : fs_rect{0, 0, (int32_t)d.src_width, (int32_t)d.src_height};
+  p.W = (uint32_t)(p.roi.right - p.roi.left);
+  p.H = (uint32_t)(p.roi.bottom - p.roi.top);
+  p.L = level_count(p.W, p.H);
+  const uint32_t k = d.frames_per_batch ? d.frames_per_batch : 8;
+  p.K = std::max(1u, std::min<uint32_t>(std::min<uint32_t>(k, (uint32_t)kMaxBatch), d.frame_count));
+  uint32_t w = p.W, h = p.H;
+  for (uint32_t l = 0; l < p.L; ++l) {
+    p.lw.push_back(w);
+    p.lh.push_back(h);
+    p.pitch.push_back(round_up(w, 32));
+    w = next_level_size(w);
+    h = next_level_size(h);
+  }
+  const size_t esz = d.level_storage == FS_STORAGE_F32 ? 4 : 2;
+  const size_t n0 = (size_t)p.pitch[0] * p.H;
+  p.fixed = n0 * 4 + n0;                                                            // weight sum, union
+  for (uint32_t l = 1; l < p.L; ++l) p.fixed += (size_t)p.pitch[l] * p.lh[l];       // mask support
+  for (uint32_t l = 0; l < p.L; ++l) p.fixed += (size_t)p.pitch[l] * p.lh[l] * 12;  // accumulators
+  for (uint32_t l = 1; l + 1 < p.L; ++l) p.fixed += p.K * ((size_t)p.pitch[l] * p.lh[l] * (esz * 4 + 1));
+  p.fixed += (size_t)p.W * p.H * 3;  // output
+  p.planes = n0 * 8;
+  p.frame_pitch = round_up((int64_t)d.src_width * d.channels, 16);
+  p.frame_bytes = (size_t)p.frame_pitch * d.src_height;
+  p.staging_slots = std::min<size_t>(2 * (size_t)p.K, d.frame_count);
+  return p;
+}
+
+// Device bytes of a stack over its life in pass-2 mode `mode`; the upload
+// staging ring counts when frames come from host memory.
+uint64_t plan_bytes(const StackPlan& p, uint32_t frames, Pass2Mode mode, bool host_frames) {
+  const uint64_t staging = host_frames ? (uint64_t)p.frame_bytes * p.staging_slots : 0;
+  switch (mode) {
+    case P2_CACHE: return p.fixed + (uint64_t)p.planes * frames + staging;
+    case P2_RESIDENT: return p.fixed + (uint64_t)p.planes * p.K + (uint64_t)p.frame_bytes * frames;
+    default: return p.fixed + (uint64_t)p.planes * p.K + staging;
+  }
+}
+
+// Pass-2 mode for `available` device bytes: cache the pass-1 planes when they
+// fit, else keep the frames, else refetch them.
+Pass2Mode choose_mode(const StackPlan& p, uint32_t frames, uint64_t available, bool host_frames) {
+  if (plan_bytes(p, frames, P2_CACHE, host_frames) <= available) return P2_CACHE;
+  if (plan_bytes(p, frames, P2_RESIDENT, host_frames) <= available) return P2_RESIDENT;
+  return P2_REFETCH;
+}
+
+}  // namespace
+
 int fs_stack_begin(fs_ctx* ctx, const fs_stack_desc* desc, fs_stack** out) {
   if (!ctx || !desc || !out) return set_err(ctx, FS_ERR_INVALID, "null argument");
   *out = nullptr;
   const fs_stack_desc& d = *desc;
-  if (d.sample_bits != 8) return set_err(ctx, FS_ERR_UNSUPPORTED, "only 8-bit samples are implemented");
-  if (d.src_width == 0 || d.src_height == 0 || d.frame_count == 0) return set_err(ctx, FS_ERR_INVALID, "empty stack");
-  if (d.contrast_window < 3 || (d.contrast_window & 1) == 0)
-    return set_err(ctx, FS_ERR_INVALID, "contrast window must be odd and >= 3");
-  if (d.contrast_window > 2 * kMaxBorder + 1) return set_err(ctx, FS_ERR_UNSUPPORTED, "contrast window larger than 15");
-  if (d.level_storage != FS_STORAGE_F32 && d.level_storage != FS_STORAGE_F16 && d.level_storage != FS_STORAGE_BF16)
-    return set_err(ctx, FS_ERR_INVALID, "unknown level storage");
-  bool aligned = d.input_is_aligned != 0;
-  if (aligned ? (d.channels != 3 && d.channels != 4) : d.channels != 3)
-    return set_err(ctx, FS_ERR_INVALID, "channels must be 3 (RGB source) or 3/4 (aligned RGB/RGBA)");
-  fs_rect roi = d.has_roi ? d.roi : fs_rect{0, 0, (int32_t)d.src_width, (int32_t)d.src_height};
-  if (aligned) roi = fs_rect{0, 0, (int32_t)d.src_width, (int32_t)d.src_height};
-  if (roi.right <= roi.left || roi.bottom <= roi.top) return set_err(ctx, FS_ERR_INVALID, "empty roi");
+  int code = FS_OK;
+  if (const char* why = check_desc(d, &code)) return set_err(ctx, code, why);
   cudaSetDevice(ctx->device);
+  const StackPlan plan = plan_stack(d);
   fs_stack* s = new fs_stack();
   s->ctx = ctx;
   ctx->stacks.insert(s);
   s->d = d;
-  s->roi = roi;
-  s->aligned = aligned;
+  s->roi = plan.roi;
+  s->aligned = d.input_is_aligned != 0;
   s->storage = d.level_storage;
-  s->W = (uint32_t)(roi.right - roi.left);
-  s->H = (uint32_t)(roi.bottom - roi.top);
-  s->L = level_count(s->W, s->H);
+  s->W = plan.W;
+  s->H = plan.H;
+  s->L = plan.L;
   s->border = d.contrast_window / 2;
-  uint32_t k = d.frames_per_batch ? d.frames_per_batch : 8;
-  s->K = std::max(1u, std::min<uint32_t>(std::min<uint32_t>(k, (uint32_t)kMaxBatch), d.frame_count));
-  uint32_t w = s->W, h = s->H;
-  for (uint32_t l = 0; l < s->L; ++l) {
-    s->lw.push_back(w);
-    s->lh.push_back(h);
-    s->pitch.push_back(round_up(w, 32));
-    w = next_level_size(w);
-    h = next_level_size(h);
-  }
+  s->K = plan.K;
+  s->lw = plan.lw;
+  s->lh = plan.lh;
+  s->pitch = plan.pitch;
   auto fail = [&](int rc) {
     fs_stack_destroy(s);
     return rc;
@@ -588,21 +698,20 @@ int fs_stack_begin(fs_ctx* ctx, const fs_stack_desc* desc, fs_stack** out) {
   }
   if ((rc = stack_alloc(s, (size_t)s->W * s->H * 3, &p)) != FS_OK) return fail(rc);
   s->out_dev = (uint8_t*)p;
-  // pass-2 source: cache the pass-1 planes (8 B per pixel per frame) when the
-  // budget allows, else keep the frames, else refetch them
-  s->frame_pitch = round_up((int64_t)d.src_width * d.channels, 16);
-  s->frame_bytes = (size_t)s->frame_pitch * d.src_height;
-  const size_t planes_bytes = n0 * 8;
-  const size_t staging_bytes = s->frame_bytes * std::min<size_t>(2 * (size_t)s->K, d.frame_count);
-  if (ctx->held - ctx->pooled + planes_bytes * d.frame_count + staging_bytes <= ctx->budget) {
-    s->mode = P2_CACHE;
+  // pass-2 source from what the budget leaves (this stack's fixed state is
+  // already held and part of every mode's bytes)
+  s->frame_pitch = plan.frame_pitch;
+  s->frame_bytes = plan.frame_bytes;
+  const uint64_t in_use = ctx->held;
+  const uint64_t available = ctx->budget + plan.fixed > in_use ? ctx->budget + plan.fixed - in_use : 0;
+  s->mode = choose_mode(plan, d.frame_count, available, true);
+  const size_t planes_bytes = plan.planes;
+  if (s->mode == P2_CACHE) {
     for (uint32_t f = 0; f < d.frame_count; ++f) {
       if ((rc = stack_alloc(s, planes_bytes, &p)) != FS_OK) return fail(rc);
       s->cache.push_back(FramePlanes{(uint32_t*)p, (float*)((uint8_t*)p + n0 * 4)});
     }
   } else {
-    const bool keep = ctx->held - ctx->pooled + planes_bytes * s->K + s->frame_bytes * d.frame_count <= ctx->budget;
-    s->mode = keep ? P2_RESIDENT : P2_REFETCH;
     for (uint32_t kk = 0; kk < s->K; ++kk) {
       if ((rc = stack_alloc(s, planes_bytes, &p)) != FS_OK) return fail(rc);
       s->p2.push_back(FramePlanes{(uint32_t*)p, (float*)((uint8_t*)p + n0 * 4)});
@@ -635,7 +744,7 @@ static int add_frame_impl(fs_stack* s, const void* pixels, size_t row_stride, co
     if (s->mode == P2_RESIDENT) {
       // kept for pass 2
       void* p;
-      int rc = stack_alloc(s, s->frame_bytes, &p);
+      int rc = stack_alloc(s, s->frame_bytes, &p, ctx->copy);
       if (rc != FS_OK) return rc;
       buf = (uint8_t*)p;
       fr.owned = true;
@@ -646,7 +755,7 @@ static int add_frame_impl(fs_stack* s, const void* pixels, size_t row_stride, co
       const size_t slot = s->frames.size() % nslots;
       while (s->staging.size() <= slot) {
         void* p;
-        int rc = stack_alloc(s, s->frame_bytes, &p);
+        int rc = stack_alloc(s, s->frame_bytes, &p, ctx->copy);
         if (rc != FS_OK) return rc;
         s->staging.push_back((uint8_t*)p);
       }
@@ -818,6 +927,18 @@ static int finish_impl(fs_stack* s, fs_frame_fetch_cb refetch, void* user, void*
 
 int fs_stack_pass2_mode(const fs_stack* s) { return s ? (int)s->mode : -1; }
 
+int fs_stack_footprint(const fs_stack_desc* desc, uint64_t available_bytes, int host_frames, uint64_t* bytes,
+                       int* mode) {
+  if (!desc || !bytes) return FS_ERR_INVALID;
+  int code = FS_OK;
+  if (check_desc(*desc, &code)) return code;
+  const StackPlan plan = plan_stack(*desc);
+  const Pass2Mode m = choose_mode(plan, desc->frame_count, available_bytes, host_frames != 0);
+  *bytes = plan_bytes(plan, desc->frame_count, m, host_frames != 0);
+  if (mode) *mode = (int)m;
+  return *bytes <= available_bytes ? FS_OK : FS_ERR_BUDGET;
+}
+
 int fs_stack_finish(fs_stack* stack, fs_frame_fetch_cb refetch, void* user, void* out_pixels, size_t out_stride) {
   return finish_impl(stack, refetch, user, out_pixels, out_stride, false);
 }
@@ -848,7 +969,7 @@ int fs_stack_destroy(fs_stack* s) {
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
     cudaStreamSynchronize(ctx->copy);
-    for (auto& a : s->allocs) dev_release(ctx, a.p, a.bytes);
+    for (auto& a : s->allocs) dev_free(ctx, a.p, a.bytes);
     s->allocs.clear();
     ctx->stacks.erase(s);
     detach_stack(s);

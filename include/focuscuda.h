@@ -67,14 +67,25 @@ void fs_destroy(fs_ctx* ctx);
 const char* fs_last_error(const fs_ctx* ctx);
 const char* fs_status_string(int status);
 int fs_api_version(void);
-/* Bytes of device memory the context currently holds. */
+/* Bytes of device memory in the context's live buffers (what its budget
+ * counts). */
 uint64_t fs_ctx_device_bytes(const fs_ctx* ctx);
 /* Wait for all work queued on the context's stream. */
 int fs_ctx_synchronize(fs_ctx* ctx);
-/* Device buffers of destroyed stacks stay in a per-context pool (still
- * counted against the budget) and are reused by later stacks of the same
- * geometry; fs_ctx_trim frees them.  Not part of the reference. */
+/* Buffers come from a stream-ordered memory pool shared by the contexts of
+ * the process on a device (allocation and release never synchronise the
+ * device); memory of destroyed stacks stays cached in the pool for later
+ * stacks.  fs_ctx_trim waits for the context's streams and returns the
+ * cached memory to the device.  Not part of the reference. */
 int fs_ctx_trim(fs_ctx* ctx);
+/* Grow the shared pool's cache by `bytes` (allocate and release), so that
+ * later stacks find their memory without growing the pool; for a serving
+ * process that takes its HBM budget up front.  Not part of the reference. */
+int fs_ctx_reserve(fs_ctx* ctx, uint64_t bytes);
+/* Change the context's HBM budget (later allocations and pass-2 mode choices
+ * use it; memory already held is not released).  Used by a serving loop that
+ * hands each admitted stack its reservation.  Not part of the reference. */
+int fs_ctx_set_budget(fs_ctx* ctx, uint64_t hbm_budget_bytes);
 /* The CUDA stream (cudaStream_t) all of the context's kernels run on, for
  * callers that order their own work or record events against it. */
 int fs_ctx_stream(const fs_ctx* ctx, void** stream);
@@ -189,6 +200,16 @@ int fs_stack_set_base_output(fs_stack* stack, float* dev_base, size_t row_stride
  * device and remapped again, 2 = frames fetched again through the finish
  * callback and remapped again. */
 int fs_stack_pass2_mode(const fs_stack* stack);
+
+/* Device bytes a stack of `desc` holds over its life when `available_bytes`
+ * of budget are free, and the pass-2 mode it would pick there (0 cache, 1
+ * resident, 2 refetch); host_frames != 0 counts the upload staging ring.
+ * FS_ERR_BUDGET when not even the refetch mode fits.  Allocates nothing; the
+ * admission test of a serving loop (the analogue of --memory-fraction,
+ * src/memory_budget.zig:3-53, applied per request).  Not part of the
+ * reference. */
+int fs_stack_footprint(const fs_stack_desc* desc, uint64_t available_bytes, int host_frames, uint64_t* bytes,
+                       int* mode);
 
 /* Output size of the stack (the ROI). */
 int fs_stack_output_size(const fs_stack* stack, uint32_t* width, uint32_t* height);

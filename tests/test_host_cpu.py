@@ -182,3 +182,87 @@ def test_clamped_expand_closed_form_is_bitwise_the_reference(sw, sh, dw, dh):
     ref = oracle.expand_rgb(src, dw, dh)
     got = _expand_closed_form(src, dw, dh)
     assert np.array_equal(got.view(np.uint32), ref.view(np.uint32))
+
+
+# ------------------------------------------------------------ serving (host)
+def test_stack_footprint_modes_follow_the_budget():
+    d = fsb.stack_desc(7952, 5304, 30, fsb.Rect(82, 63, 7872, 5243))
+    cache, m_cache, ok = fsb.stack_footprint(d, 1 << 50)
+    assert m_cache == "cache" and ok
+    resident, m_res, ok = fsb.stack_footprint(d, cache - 1)
+    assert m_res == "resident" and ok and resident < cache
+    refetch, m_ref, ok = fsb.stack_footprint(d, resident - 1)
+    assert m_ref == "refetch" and ok and refetch < resident
+    b, _, ok = fsb.stack_footprint(d, refetch - 1)
+    assert not ok and b == refetch
+    # device-resident frames need no upload staging
+    dev_cache, _, _ = fsb.stack_footprint(d, 1 << 50, host_frames=False)
+    assert dev_cache < cache
+    # FP16 level storage shrinks the level slots
+    d16 = fsb.stack_desc(7952, 5304, 30, fsb.Rect(82, 63, 7872, 5243), level_storage=fsb.STORAGE_F16)
+    assert fsb.stack_footprint(d16, 1 << 50)[0] < cache
+
+
+def test_stack_footprint_rejects_bad_desc():
+    with pytest.raises(fsb.FocusCudaError):
+        fsb.stack_footprint(fsb.stack_desc(64, 48, 2, contrast_window=4), 1 << 40)
+
+
+class _FakeCtx:
+    def __init__(self):
+        self.budget = None
+        self.trims = 0
+
+    def set_budget(self, b):
+        self.budget = b
+
+    def trim(self):
+        self.trims += 1
+
+    def reserve(self, n):
+        pass
+
+    def close(self):
+        pass
+
+
+def test_server_admission_respects_the_budget():
+    srv = fsb.serving.StackServer(hbm_budget_bytes=40 * 10**9, workers=3, context_factory=_FakeCtx,
+                                  max_stack_fraction=1.0)
+    big = fsb.serving.StackRequest(0, 0.0, 7952, 5304, 30)
+    roi = fsb.Rect(0, 0, 7952, 5304)
+    need = fsb.stack_footprint(fsb.stack_desc(7952, 5304, 30, roi), 1 << 50)[0]
+    w1, b1 = srv._try_admit(big, roi)
+    assert b1 == need and w1.busy and w1.ctx.budget == need
+    w2, b2 = srv._try_admit(fsb.serving.StackRequest(1, 0.0, 7952, 5304, 30), roi)
+    assert w2 is not w1 and b1 + b2 <= srv.budget
+    # a third one only fits in a smaller mode or not at all
+    third = srv._try_admit(fsb.serving.StackRequest(2, 0.0, 7952, 5304, 30), roi)
+    if third is not None:
+        assert b1 + b2 + third[1] <= srv.budget
+    # memory cached by idle workers is released before a smaller mode is taken
+    srv2 = fsb.serving.StackServer(hbm_budget_bytes=need + 10**6, workers=2, context_factory=_FakeCtx,
+                                   max_stack_fraction=1.0)
+    srv2.workers[1].cached = 10**9
+    w, b = srv2._try_admit(big, roi)
+    assert srv2.workers[1].ctx.trims == 1 and srv2.workers[1].cached == 0 and w is srv2.workers[0] and b == need
+
+
+def test_server_caps_one_stacks_share_of_the_budget():
+    roi = fsb.Rect(0, 0, 7952, 5304)
+    srv = fsb.serving.StackServer(hbm_budget_bytes=40 * 10**9, workers=2, context_factory=_FakeCtx,
+                                  max_stack_fraction=0.25)
+    w, b = srv._try_admit(fsb.serving.StackRequest(0, 0.0, 7952, 5304, 30), roi)
+    assert b <= 10 * 10**9
+    assert b < fsb.stack_footprint(fsb.stack_desc(7952, 5304, 30, roi), 1 << 50)[0]
+
+
+def test_poisson_stream_shape():
+    reqs = fsb.serving.poisson_stream(400, 50.0, seed=3)
+    assert len(reqs) == 400
+    t = [r.arrival_s for r in reqs]
+    assert all(b > a for a, b in zip(t, t[1:]))
+    assert 4.0 < t[-1] < 12.0  # ~ n / rate
+    sizes = {(r.width, r.height) for r in reqs}
+    assert sizes <= set(fsb.serving.SIZE_MIX) | {fsb.serving.LARGE}
+    assert all(4 <= r.frames <= (143 if (r.width, r.height) == fsb.serving.LARGE else 40) for r in reqs)
