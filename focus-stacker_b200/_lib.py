@@ -28,6 +28,8 @@ EXPORTED = (
     "fs_remap_frame", "fs_remap_frame_device",
     "fs_stack_begin", "fs_stack_add_frame", "fs_stack_add_frame_device", "fs_stack_finish",
     "fs_stack_finish_device", "fs_stack_set_base_output", "fs_stack_pass2_mode", "fs_stack_footprint", "fs_stack_output_size", "fs_stack_destroy", "fs_fuse_stack",
+    "fs_batch_create", "fs_batch_run", "fs_batch_stack_count", "fs_batch_pass2_mode", "fs_batch_uses_graph",
+    "fs_batch_destroy",
     "fs_fuse_aligned_device_static", "fs_synth_frame_device", "fs_synth_pose",
 )
 
@@ -117,5 +119,12 @@ def _bind(L):
     L.fs_fuse_stack.argtypes = [ctx, P(FsStackDesc), P(vp), P(sz), P(FsPose), vp, sz]
     L.fs_fuse_aligned_device_static.argtypes = [P(vp), P(sz), u32, u32, u32, u32, u32, vp, sz, vp,
                                                 ctypes.c_char_p, sz]
+    L.fs_batch_create.argtypes = [ctx, u32, P(FsStackDesc), P(P(vp)), P(sz), P(P(FsPose)), P(vp), P(sz), u32, i32,
+                                  P(vp)]
+    L.fs_batch_run.argtypes = [vp]
+    L.fs_batch_stack_count.argtypes = [vp]
+    L.fs_batch_pass2_mode.argtypes = [vp, u32]
+    L.fs_batch_uses_graph.argtypes = [vp]
+    L.fs_batch_destroy.argtypes = [vp]
     L.fs_synth_frame_device.argtypes = [ctx, u64, i32, u32, u32, u32, u32, vp, sz, P(FsPose)]
     L.fs_synth_pose.argtypes = [u64, i32, u32, u32, u32, u32, P(FsPose)]

@@ -19,7 +19,7 @@ from __future__ import annotations
 import ctypes
 import enum
 from dataclasses import dataclass, fields
-from typing import Optional, Sequence
+from typing import List, Optional, Sequence
 
 import numpy as np
 
@@ -430,6 +430,92 @@ def fuse_aligned_images(ctx: Context, images: Sequence[np.ndarray], contrast_win
                 raise FocusCudaError(7, "MismatchedImageSizes" if im.shape[:2] != (h, w) else "MismatchedImageFormats")
             st.add_frame(im)
         return st.finish()
+
+
+# ------------------------------------------------------------- batched form
+@dataclass
+class BatchStack:
+    """One stack of a StackBatch: device frames (objects with data_ptr(), all
+    of one size), their poses (None for aligned input), the ROI (None: full
+    frame) and a device output of ROI size (RGB u8)."""
+    frames: Sequence
+    poses: Optional[Sequence]
+    roi: Optional[Rect]
+    out: object
+    width: int
+    height: int
+    channels: int = 3
+    aligned: bool = False
+
+
+class StackBatch:
+    """Batched form (fs_batch_*): many independent stacks over device frames,
+    spread over `lanes` streams and run as one captured CUDA graph from the
+    second run on.  Frames are read at the same addresses on every run."""
+
+    def __init__(self, ctx: Context, stacks: Sequence[BatchStack], lanes: int = 4, pass2_mode: int = -1,
+                 contrast_window: int = 5, frames_per_batch: int = 0, level_storage: int = 0):
+        self.ctx = ctx
+        n = len(stacks)
+        descs = (_lib.FsStackDesc * n)()
+        frame_lists, pose_lists = [], []
+        strides = (ctypes.c_size_t * n)()
+        outs = (ctypes.c_void_p * n)()
+        out_strides = (ctypes.c_size_t * n)()
+        self.out_sizes = []
+        for i, st in enumerate(stacks):
+            descs[i] = stack_desc(st.width, st.height, len(st.frames), st.roi, st.channels, contrast_window,
+                                  st.aligned, frames_per_batch, level_storage)
+            fl = (ctypes.c_void_p * len(st.frames))(*[_ptr(f) for f in st.frames])
+            frame_lists.append(fl)
+            strides[i] = st.width * st.channels
+            if st.poses is not None:
+                pl = (_lib.FsPose * len(st.poses))(*[p.to_c() for p in st.poses])
+            else:
+                pl = None
+            pose_lists.append(pl)
+            outs[i] = _ptr(st.out)
+            w = st.roi.width if (st.roi is not None and not st.aligned) else st.width
+            h = st.roi.height if (st.roi is not None and not st.aligned) else st.height
+            out_strides[i] = w * 3
+            self.out_sizes.append((w, h))
+        fptrs = (ctypes.POINTER(ctypes.c_void_p) * n)(*[ctypes.cast(f, ctypes.POINTER(ctypes.c_void_p))
+                                                         for f in frame_lists])
+        pptrs = (ctypes.POINTER(_lib.FsPose) * n)(*[ctypes.cast(p, ctypes.POINTER(_lib.FsPose)) if p is not None
+                                                     else ctypes.POINTER(_lib.FsPose)() for p in pose_lists])
+        any_pose = any(p is not None for p in pose_lists)
+        h = ctypes.c_void_p()
+        self._keep = (descs, frame_lists, pose_lists, strides, outs, out_strides, fptrs, pptrs, list(stacks))
+        _check(L().fs_batch_create(ctx.handle, n, descs, fptrs, strides, pptrs if any_pose else None, outs,
+                                   out_strides, lanes, pass2_mode, ctypes.byref(h)), ctx.handle)
+        self.handle = h
+
+    def run(self):
+        _check(L().fs_batch_run(self.handle), self.ctx.handle)
+
+    @property
+    def uses_graph(self) -> bool:
+        return bool(L().fs_batch_uses_graph(self.handle))
+
+    def pass2_modes(self) -> List[str]:
+        return [PASS2_MODES[L().fs_batch_pass2_mode(self.handle, i)] for i in range(len(self.out_sizes))]
+
+    def close(self):
+        if self.handle:
+            L().fs_batch_destroy(self.handle)
+            self.handle = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 # ------------------------------------------------------------ precision form

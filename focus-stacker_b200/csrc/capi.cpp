@@ -639,7 +639,8 @@ Pass2Mode choose_mode(const StackPlan& p, uint32_t frames, uint64_t available, b
 
 }  // namespace
 
-int fs_stack_begin(fs_ctx* ctx, const fs_stack_desc* desc, fs_stack** out) {
+// forced_mode >= 0: pass-2 mode chosen by the caller (batches plan it)
+static int begin_impl(fs_ctx* ctx, const fs_stack_desc* desc, fs_stack** out, int forced_mode) {
   if (!ctx || !desc || !out) return set_err(ctx, FS_ERR_INVALID, "null argument");
   *out = nullptr;
   const fs_stack_desc& d = *desc;
@@ -704,7 +705,7 @@ int fs_stack_begin(fs_ctx* ctx, const fs_stack_desc* desc, fs_stack** out) {
   s->frame_bytes = plan.frame_bytes;
   const uint64_t in_use = ctx->held;
   const uint64_t available = ctx->budget + plan.fixed > in_use ? ctx->budget + plan.fixed - in_use : 0;
-  s->mode = choose_mode(plan, d.frame_count, available, true);
+  s->mode = forced_mode >= 0 ? (Pass2Mode)forced_mode : choose_mode(plan, d.frame_count, available, true);
   const size_t planes_bytes = plan.planes;
   if (s->mode == P2_CACHE) {
     for (uint32_t f = 0; f < d.frame_count; ++f) {
@@ -723,6 +724,8 @@ int fs_stack_begin(fs_ctx* ctx, const fs_stack_desc* desc, fs_stack** out) {
   *out = s;
   return FS_OK;
 }
+
+int fs_stack_begin(fs_ctx* ctx, const fs_stack_desc* desc, fs_stack** out) { return begin_impl(ctx, desc, out, -1); }
 
 static int add_frame_impl(fs_stack* s, const void* pixels, size_t row_stride, const fs_pose* pose, bool device) {
   if (!s || !pixels) return FS_ERR_INVALID;
@@ -794,7 +797,7 @@ int fs_stack_add_frame_device(fs_stack* stack, const void* dev_pixels, size_t ro
 }
 
 static int finish_impl(fs_stack* s, fs_frame_fetch_cb refetch, void* user, void* out, size_t out_stride,
-                       bool device_out) {
+                       bool device_out, bool wait = true) {
   if (!s || !out) return FS_ERR_INVALID;
   if (!s->ctx) return FS_ERR_STATE;  // its context was destroyed
   fs_ctx* ctx = s->ctx;
@@ -919,8 +922,10 @@ static int finish_impl(fs_stack* s, fs_frame_fetch_cb refetch, void* user, void*
   else
     e = cudaMemcpy2DAsync(out, out_stride, s->out_dev, (size_t)s->W * 3, (size_t)s->W * 3, s->H, kind, st);
   if (e != cudaSuccess) return cuda_err(ctx, e, "output copy");
-  e = cudaStreamSynchronize(st);
-  if (e != cudaSuccess) return cuda_err(ctx, e, "fusion");
+  if (wait) {
+    e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return cuda_err(ctx, e, "fusion");
+  }
   s->finished = true;
   return FS_OK;
 }
@@ -1014,3 +1019,204 @@ int fs_synth_frame_device(fs_ctx* ctx, uint64_t seed, int scene, uint32_t width,
 }
 
 }  // extern "C"
+
+// ================================================================= batches
+// Batched form: many independent stacks over device-resident frames, spread
+// over `lanes` contexts (streams) and run as one CUDA graph: the first
+// fs_batch_run executes the work directly (and configures the kernels), the
+// second captures the same launch sequence, every later run replays it with
+// one graph launch.  Every stack's state is re-initialised by the kernels of
+// the run itself (pass 1 writes the weight sum and union of the first batch,
+// pass 2 clears the accumulators), so a replay recomputes every stack from
+// the frames at the same device addresses.
+struct fs_batch {
+  fs_ctx* parent = nullptr;
+  std::vector<fs_ctx*> lanes;
+  struct Item {
+    fs_stack* stack = nullptr;
+    int lane = 0;
+    std::vector<const void*> frames;
+    size_t stride = 0;
+    std::vector<fs_pose> poses;
+    void* out = nullptr;
+    size_t out_stride = 0;
+  };
+  std::vector<Item> items;
+  std::vector<cudaEvent_t> join;
+  std::vector<int> planned;  // pass-2 mode of each stack
+  uint64_t charged = 0;      // device bytes counted against the parent's budget
+  cudaEvent_t fork = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  int runs = 0;
+};
+
+namespace {
+
+int batch_enqueue(fs_batch* b) {
+  for (auto& it : b->items) {
+    fs_stack* s = it.stack;
+    s->frames.clear();
+    s->pass1_done = 0;
+    s->finished = false;
+    for (size_t k = 0; k < it.frames.size(); ++k) {
+      const fs_pose* pose = s->aligned ? nullptr : &it.poses[k];
+      int rc = add_frame_impl(s, it.frames[k], it.stride, pose, true);
+      if (rc != FS_OK) return rc;
+    }
+    int rc = finish_impl(s, nullptr, nullptr, it.out, it.out_stride, true, false);
+    if (rc != FS_OK) return rc;
+  }
+  return FS_OK;
+}
+
+// Fork every lane from the parent stream, enqueue, join back.
+int batch_enqueue_forked(fs_batch* b) {
+  fs_ctx* P = b->parent;
+  cudaEventRecord(b->fork, P->stream);
+  for (fs_ctx* l : b->lanes) cudaStreamWaitEvent(l->stream, b->fork, 0);
+  int rc = batch_enqueue(b);
+  for (size_t i = 0; i < b->lanes.size(); ++i) {
+    cudaEventRecord(b->join[i], b->lanes[i]->stream);
+    cudaStreamWaitEvent(P->stream, b->join[i], 0);
+  }
+  return rc;
+}
+
+}  // namespace
+
+int fs_batch_create(fs_ctx* ctx, uint32_t n, const fs_stack_desc* descs, const void* const* const* frames,
+                    const size_t* row_strides, const fs_pose* const* poses, void* const* dev_out,
+                    const size_t* out_strides, uint32_t lanes, int pass2_mode, fs_batch** out) {
+  if (!ctx || !descs || !frames || !row_strides || !dev_out || !out_strides || !out || n == 0)
+    return set_err(ctx, FS_ERR_INVALID, "null argument");
+  if (pass2_mode < -1 || pass2_mode > 1) return set_err(ctx, FS_ERR_INVALID, "pass2_mode must be -1, 0 or 1");
+  *out = nullptr;
+  lanes = std::max(1u, std::min(lanes, n));
+  cudaSetDevice(ctx->device);
+  fs_batch* b = new fs_batch();
+  b->parent = ctx;
+  auto fail = [&](int rc) {
+    fs_batch_destroy(b);
+    return rc;
+  };
+  // plan: footprints in the requested (or best affordable) mode, stacks to
+  // the least-loaded lane by frame-pixels, largest first
+  std::vector<uint64_t> bytes(n);
+  std::vector<double> work(n);
+  uint64_t total = 0;
+  for (uint32_t i = 0; i < n; ++i) {
+    int code = FS_OK;
+    if (const char* why = check_desc(descs[i], &code)) return fail(set_err(ctx, code, why));
+    if (!frames[i]) return fail(set_err(ctx, FS_ERR_INVALID, "null frame list"));
+    if (!descs[i].input_is_aligned && !poses) return fail(set_err(ctx, FS_ERR_INVALID, "poses required"));
+    const StackPlan plan = plan_stack(descs[i]);
+    const uint64_t left = ctx->budget > ctx->held + total ? ctx->budget - ctx->held - total : 0;
+    Pass2Mode m = pass2_mode == 0 ? P2_CACHE : pass2_mode == 1 ? P2_RESIDENT : choose_mode(plan, descs[i].frame_count, left, true);
+    if (m == P2_REFETCH) m = P2_RESIDENT;
+    b->planned.push_back((int)m);
+    bytes[i] = plan_bytes(plan, descs[i].frame_count, m, true);
+    total += bytes[i];
+    work[i] = (double)descs[i].frame_count * plan.W * plan.H;
+  }
+  if (ctx->held + total > ctx->budget)
+    return fail(set_err(ctx, FS_ERR_BUDGET, "batch needs " + std::to_string(total) + " device bytes, budget leaves " +
+                                               std::to_string(ctx->budget > ctx->held ? ctx->budget - ctx->held : 0)));
+  std::vector<uint32_t> order(n);
+  for (uint32_t i = 0; i < n; ++i) order[i] = i;
+  std::sort(order.begin(), order.end(), [&](uint32_t a, uint32_t c) { return work[a] > work[c]; });
+  std::vector<double> load(lanes, 0.0);
+  std::vector<uint64_t> lane_bytes(lanes, 0);
+  b->items.resize(n);
+  for (uint32_t i : order) {
+    const int l = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+    load[l] += work[i];
+    lane_bytes[l] += bytes[i];
+    b->items[i].lane = l;
+  }
+  for (uint32_t l = 0; l < lanes; ++l) {
+    fs_ctx* c = nullptr;
+    int rc = fs_create(ctx->device, std::max<uint64_t>(lane_bytes[l], 1), &c);
+    if (rc != FS_OK) return fail(rc);
+    b->lanes.push_back(c);
+    cudaEvent_t ev;
+    cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+    b->join.push_back(ev);
+  }
+  cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming);
+  // stacks in lane order; each sees its lane's remaining budget, so it picks
+  // the mode its footprint was planned for
+  for (uint32_t i = 0; i < n; ++i) {
+    auto& it = b->items[i];
+    fs_ctx* lc = b->lanes[it.lane];
+    int rc = begin_impl(lc, &descs[i], &it.stack, b->planned[i]);
+    if (rc != FS_OK) return fail(set_err(ctx, rc, std::string("stack begin: ") + fs_last_error(lc)));
+    it.frames.assign(frames[i], frames[i] + descs[i].frame_count);
+    it.stride = row_strides[i];
+    if (!descs[i].input_is_aligned) it.poses.assign(poses[i], poses[i] + descs[i].frame_count);
+    it.out = dev_out[i];
+    it.out_stride = out_strides[i];
+    if (!it.out || it.out_stride < (size_t)it.stack->W * 3) return fail(set_err(ctx, FS_ERR_INVALID, "bad output"));
+  }
+  ctx->held += total;  // the lanes' memory counts against the parent's budget
+  b->charged = total;
+  b->runs = 0;
+  *out = b;
+  return FS_OK;
+}
+
+int fs_batch_run(fs_batch* b) {
+  if (!b) return FS_ERR_INVALID;
+  fs_ctx* P = b->parent;
+  cudaSetDevice(P->device);
+  cudaError_t e;
+  if (b->runs == 0) {
+    int rc = batch_enqueue_forked(b);  // direct execution, configures every kernel
+    if (rc != FS_OK) return rc;
+  } else {
+    if (!b->exec) {
+      e = cudaStreamBeginCapture(P->stream, cudaStreamCaptureModeRelaxed);
+      if (e != cudaSuccess) return cuda_err(P, e, "begin capture");
+      int rc = batch_enqueue_forked(b);
+      cudaGraph_t g = nullptr;
+      e = cudaStreamEndCapture(P->stream, &g);
+      if (rc != FS_OK) {
+        if (g) cudaGraphDestroy(g);
+        return rc;
+      }
+      if (e != cudaSuccess) return cuda_err(P, e, "end capture");
+      b->graph = g;
+      e = cudaGraphInstantiate(&b->exec, g, 0);
+      if (e != cudaSuccess) return cuda_err(P, e, "graph instantiate");
+    }
+    e = cudaGraphLaunch(b->exec, P->stream);
+    if (e != cudaSuccess) return cuda_err(P, e, "graph launch");
+  }
+  e = cudaStreamSynchronize(P->stream);
+  if (e != cudaSuccess) return cuda_err(P, e, "batch");
+  ++b->runs;
+  return FS_OK;
+}
+
+int fs_batch_stack_count(const fs_batch* b) { return b ? (int)b->items.size() : -1; }
+
+int fs_batch_pass2_mode(const fs_batch* b, uint32_t i) {
+  return (b && i < b->items.size()) ? (int)b->items[i].stack->mode : -1;
+}
+
+int fs_batch_uses_graph(const fs_batch* b) { return (b && b->exec) ? 1 : 0; }
+
+int fs_batch_destroy(fs_batch* b) {
+  if (!b) return FS_ERR_INVALID;
+  if (b->parent) cudaStreamSynchronize(b->parent->stream);
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  for (auto& it : b->items)
+    if (it.stack) fs_stack_destroy(it.stack);
+  for (fs_ctx* c : b->lanes) fs_destroy(c);
+  for (cudaEvent_t ev : b->join) cudaEventDestroy(ev);
+  if (b->fork) cudaEventDestroy(b->fork);
+  if (b->parent) b->parent->held -= std::min(b->parent->held, b->charged);
+  delete b;
+  return FS_OK;
+}

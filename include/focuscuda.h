@@ -241,6 +241,33 @@ int fs_fuse_aligned_device_static(const void* const* dev_frames, const size_t* r
                                   uint32_t width, uint32_t height, uint32_t channels, uint32_t contrast_window,
                                   void* dev_out, size_t out_stride, void* stream, char* err, size_t err_len);
 
+/* ---------------------------------------------------------------- batches */
+
+/* Batched form (not part of the reference): n independent stacks over
+ * frames already in device memory, fused together.  Stack i has desc[i],
+ * frames[i][0 .. frame_count-1] (device pointers, row stride row_strides[i]),
+ * poses[i] (NULL list for aligned input) and a device RGB u8 output
+ * dev_out[i] (row stride out_strides[i]).  The stacks are spread over `lanes`
+ * streams, largest first to the least-loaded lane, and each keeps its device
+ * state for the life of the batch (counted against ctx's budget; pass2_mode
+ * -1 picks per stack what the budget allows, 0 caches the pass-1 planes, 1
+ * keeps only the frames and remaps them again).  The first fs_batch_run
+ * executes the work directly; the second captures the same launches into a
+ * CUDA graph, which every later run replays with one graph launch, reading
+ * the frames at the same addresses (refill them in place between runs).
+ * Each run returns when every output is written. */
+typedef struct fs_batch fs_batch;
+int fs_batch_create(fs_ctx* ctx, uint32_t n, const fs_stack_desc* descs, const void* const* const* frames,
+                    const size_t* row_strides, const fs_pose* const* poses, void* const* dev_out,
+                    const size_t* out_strides, uint32_t lanes, int pass2_mode, fs_batch** out);
+int fs_batch_run(fs_batch* batch);
+int fs_batch_stack_count(const fs_batch* batch);
+/* Pass-2 mode of stack i (0 cache, 1 resident). */
+int fs_batch_pass2_mode(const fs_batch* batch, uint32_t i);
+/* 1 once runs replay a captured graph. */
+int fs_batch_uses_graph(const fs_batch* batch);
+int fs_batch_destroy(fs_batch* batch);
+
 /* ------------------------------------------------------ synthetic input */
 
 /* Render frame k of a synthetic focus stack (seeded; see the generator in
