@@ -203,6 +203,9 @@ struct fs_stack {
   cudaEvent_t copy_done = nullptr;
   cudaEvent_t batch_done[2] = {nullptr, nullptr};  // pass 1 of the last two batches (staging reuse)
   float* base_out = nullptr;      // optional device buffer for the collapsed base (RGB f32)
+  uint32_t fp_level = 0;          // first level run one frame per CTA (none: >= L - 1)
+  float* contrib = nullptr;       // per-frame blend contributions of those levels
+  float* contrib_top = nullptr;   // and of the top level
   int64_t base_pitch = 0;         // elements
 };
 
@@ -585,7 +588,14 @@ struct StackPlan {
   size_t frame_bytes = 0;    // one device copy of a source frame
   int64_t frame_pitch = 0;
   size_t staging_slots = 0;  // frame buffers of the two-batch upload ring
+  uint32_t fp_level = 0;     // first level l >= 1 run one frame per CTA (L - 1: none)
+  size_t contrib = 0, contrib_top = 0;  // bytes of the contribution buffers
 };
+
+// Levels with fewer 64x32 tiles than this run one frame per CTA (grid.z = K)
+// and add the frames' contributions in order afterwards: a small level has
+// too few tiles to fill the GPU when each CTA walks all K frames.
+constexpr uint32_t kFrameParallelTiles = 592;
 
 StackPlan plan_stack(const fs_stack_desc& d) {
   StackPlan p;
@@ -615,6 +625,21 @@ StackPlan plan_stack(const fs_stack_desc& d) {
   p.frame_pitch = round_up((int64_t)d.src_width * d.channels, 16);
   p.frame_bytes = (size_t)p.frame_pitch * d.src_height;
   p.staging_slots = std::min<size_t>(2 * (size_t)p.K, d.frame_count);
+  p.fp_level = p.L > 1 ? p.L - 1 : 1;
+  if (p.K > 1) {
+    for (uint32_t l = 1; l + 1 < p.L; ++l) {
+      const uint32_t tiles = ((p.lw[l] + kTileW - 1) / kTileW) * ((p.lh[l] + kTileH - 1) / kTileH);
+      if (tiles < kFrameParallelTiles) {
+        p.fp_level = l;
+        break;
+      }
+    }
+  }
+  if (p.fp_level + 1 < p.L) {
+    p.contrib = (size_t)p.K * 3 * p.pitch[p.fp_level] * p.lh[p.fp_level] * 4;
+    p.contrib_top = (size_t)p.K * 3 * p.pitch[p.L - 1] * p.lh[p.L - 1] * 4;
+    p.fixed += p.contrib + p.contrib_top;
+  }
   return p;
 }
 
@@ -699,6 +724,13 @@ static int begin_impl(fs_ctx* ctx, const fs_stack_desc* desc, fs_stack** out, in
   }
   if ((rc = stack_alloc(s, (size_t)s->W * s->H * 3, &p)) != FS_OK) return fail(rc);
   s->out_dev = (uint8_t*)p;
+  s->fp_level = plan.fp_level;
+  if (plan.contrib) {
+    if ((rc = stack_alloc(s, plan.contrib, &p)) != FS_OK) return fail(rc);
+    s->contrib = (float*)p;
+    if ((rc = stack_alloc(s, plan.contrib_top, &p)) != FS_OK) return fail(rc);
+    s->contrib_top = (float*)p;
+  }
   // pass-2 source from what the budget leaves (this stack's fixed state is
   // already held and part of every mode's bytes)
   s->frame_pitch = plan.frame_pitch;
@@ -881,9 +913,24 @@ static int finish_impl(fs_stack* s, fs_frame_fetch_cb refetch, void* user, void*
         if (l >= 1) a.in[k] = s->slot[k][l];
         if (l + 1 < s->L - 1) a.out[k] = s->slot[k][l + 1];
       }
+      const bool fp = l >= 1 && l >= s->fp_level && s->contrib && a.K > 1;
+      a.frame_parallel = fp ? 1 : 0;
+      a.contrib = fp ? s->contrib : nullptr;
+      a.contrib_top = fp ? s->contrib_top : nullptr;
       if (l == 0) e = timed(ctx, "level0", [&] { return launch_level0(a, s->storage, st); });
       else e = timed(ctx, "level", [&] { return launch_level(a, s->storage, st); });
       if (e != cudaSuccess) return cuda_err(ctx, e, "level launch");
+      if (fp) {
+        // the frames' contributions into the accumulators, in frame order
+        e = timed(ctx, "level", [&] {
+          return launch_sum_contrib(a.acc_l, a.acc_plane_l, a.pitch_l, a.wl, a.hl, s->contrib, a.K, st);
+        });
+        if (e == cudaSuccess && l + 1 == s->L - 1)
+          e = timed(ctx, "level", [&] {
+            return launch_sum_contrib(a.acc_n, a.acc_plane_n, a.pitch_n, a.wn, a.hn, s->contrib_top, a.K, st);
+          });
+        if (e != cudaSuccess) return cuda_err(ctx, e, "contribution sum");
+      }
       if (s->L == 1) break;
     }
   }

@@ -507,7 +507,11 @@ __device__ void store_next(const LevelSmem& S, const LevelArgs& a, int x0, int y
     if (xj >= a.wn || yi >= a.hn) continue;
     const int ni = (ii + 1) * NW + (jj + 1);
     const int64_t o = (int64_t)yi * a.pitch_n + xj;
-    if (top) {
+    if (top && a.frame_parallel) {
+      const float m = S.nm[i];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) a.contrib_top[(int64_t)(k * 3 + c) * a.acc_plane_n + o] = __fmul_rn(S.ng[c][ni], m);
+    } else if (top) {
       const float m = S.nm[i];
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
@@ -721,8 +725,15 @@ __global__ void __launch_bounds__(NT) level_kernel(const __grid_constant__ Level
   const int x0 = blockIdx.x * TW, y0 = blockIdx.y * TH;
   load_mask_support(S, a, x0, y0);
   float acc[PPT][3];
-  load_acc(a, x0, y0, acc);
-  for (int k = 0; k < a.K; ++k) {
+  // frame-parallel: this CTA blends frame blockIdx.z alone, from zero
+  const int kb = a.frame_parallel ? (int)blockIdx.z : 0, ke = a.frame_parallel ? kb + 1 : a.K;
+  if (a.frame_parallel) {
+#pragma unroll
+    for (int i = 0; i < PPT; ++i) acc[i][0] = acc[i][1] = acc[i][2] = 0.0f;
+  } else {
+    load_acc(a, x0, y0, acc);
+  }
+  for (int k = kb; k < ke; ++k) {
     const LevelPlanes& in = a.in[k];
     const T* g = (const T*)in.g;
     const T* mm = (const T*)in.m;
@@ -745,7 +756,42 @@ __global__ void __launch_bounds__(NT) level_kernel(const __grid_constant__ Level
     store_next<T>(S, a, x0, y0, k);
     expand_blend_step(S, a, x0, y0, acc);
   }
-  store_acc(a, x0, y0, acc);
+  if (a.frame_parallel) {
+    // 0 + (lap * m) is the product itself, so the ordered sum below adds
+    // exactly the terms the sequential loop adds
+#pragma unroll
+    for (int i = 0; i < PPT; ++i) {
+      const int p = threadIdx.x + i * NT;
+      const int X = x0 + p % TW, Y = y0 + p / TW;
+      if (X < a.wl && Y < a.hl) {
+        const int64_t o = (int64_t)Y * a.pitch_l + X;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) a.contrib[(int64_t)(kb * 3 + c) * a.acc_plane_l + o] = acc[i][c];
+      }
+    }
+  } else {
+    store_acc(a, x0, y0, acc);
+  }
+}
+
+__global__ void sum_contrib_kernel(float* acc, int64_t plane, int64_t pitch, int w, int h, const float* contrib,
+                                   int K) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (int64_t)w * h) return;
+  const int64_t o = (i / w) * pitch + i % w;
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    float v = acc[c * plane + o];
+    for (int k = 0; k < K; ++k) v = __fadd_rn(v, contrib[(int64_t)(k * 3 + c) * plane + o]);
+    acc[c * plane + o] = v;
+  }
+}
+
+cudaError_t launch_sum_contrib(float* acc, int64_t plane, int64_t pitch, int w, int h, const float* contrib, int K,
+                               cudaStream_t s) {
+  const int64_t n = (int64_t)w * h;
+  sum_contrib_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(acc, plane, pitch, w, h, contrib, K);
+  return cudaGetLastError();
 }
 
 template <typename K>
@@ -759,7 +805,7 @@ static cudaError_t configure(K kernel, size_t bytes, bool* done) {
 template <template <typename> class KER>
 static cudaError_t launch_levels(const LevelArgs& a, int storage, cudaStream_t s, bool* cfg) {
   const size_t sm = KER<float>::smem();
-  dim3 grid((a.wl + TW - 1) / TW, (a.hl + TH - 1) / TH);
+  dim3 grid((a.wl + TW - 1) / TW, (a.hl + TH - 1) / TH, a.frame_parallel ? a.K : 1);
   cudaError_t e;
   switch (storage) {
     case FS_STORAGE_F32:

@@ -73,6 +73,13 @@ struct LevelArgs {
   int64_t acc_plane_l;
   float* acc_n;          // accumulator level l + 1 (used when l + 1 is the top level)
   int64_t acc_plane_n;
+  // frame-parallel launch (grid.z = K, one frame per CTA): each frame's
+  // blend contribution goes to contrib[k] (3 planes of acc_plane_l floats;
+  // contrib_top[k], 3 planes of acc_plane_n, for the top level) and
+  // launch_sum_contrib adds them to the accumulator in frame order
+  int32_t frame_parallel;
+  float* contrib;
+  float* contrib_top;
 };
 
 struct CollapseArgs {
@@ -110,6 +117,9 @@ cudaError_t launch_remap_weights(const RemapWeightArgs& a, int border, cudaStrea
 cudaError_t launch_level0(const LevelArgs& a, int storage, cudaStream_t s);
 cudaError_t launch_level(const LevelArgs& a, int storage, cudaStream_t s);
 cudaError_t launch_collapse(const CollapseArgs& a, cudaStream_t s);
+// acc[c] += contrib[k][c] for k = 0 .. K-1 in order (w x h level, plane stride `plane`).
+cudaError_t launch_sum_contrib(float* acc, int64_t plane, int64_t pitch, int w, int h, const float* contrib, int K,
+                               cudaStream_t s);
 cudaError_t launch_mask_support(const MaskSupportArgs& a, cudaStream_t s);
 cudaError_t launch_remap(const RemapArgs& a, cudaStream_t s);
 cudaError_t launch_quantize(const float* acc, int64_t plane, int64_t pitch, int w, int h, uint8_t* out,
