@@ -12,7 +12,10 @@ pass 2, collapse and quantise.
          larger than L2, so no flush is needed);
   e2e    the same metric through the public API from pinned host frames: the
          host->device copy of every frame and the device->host copy of the
-         fused output are inside the timed region.
+         fused output are inside the timed region.  Stacks run back to back
+         with --e2e-lanes of them in flight (one context each), so that the
+         next stack's uploads overlap the previous stack's pass 2; the
+         latency of one stack alone is reported beside it.
 
 `--impl reference` times the CPU oracle (the C++ restatement of the
 reference's Zig path; the Zig reference cannot be built in this image) on
@@ -59,6 +62,9 @@ def parse():
     ap.add_argument("--batch", type=int, default=0, help="frames per pass over per-pixel state (0 = library default)")
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--e2e-lanes", type=int, default=1,
+                    help="stacks in flight in the e2e leg (each on its own context): the next stack's uploads "
+                         "overlap the previous stack's pass 2")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-forms", action="store_true", help="skip the precision / serving / batched legs")
     ap.add_argument("--precision-frames", type=int, default=143,
@@ -531,29 +537,58 @@ def main():
             h = torch.empty(f.shape, dtype=torch.uint8, pin_memory=True)
             h.copy_(f)
             hframes.append(h.numpy())
-        hout = torch.empty((roi.height, roi.width, 3), dtype=torch.uint8, pin_memory=True).numpy()
+        lanes = max(1, args.e2e_lanes)
+        ctxs = [ctx] + [fsb.Context(dev) for _ in range(lanes - 1)]
+        houts = [torch.empty((roi.height, roi.width, 3), dtype=torch.uint8, pin_memory=True).numpy()
+                 for _ in range(lanes)]
 
-        def step_e2e():
-            st = fsb.PyramidContrastStack(ctx, W, H, F, roi=roi, frames_per_batch=args.batch)
+        def step_e2e(lane=0):
+            st = fsb.PyramidContrastStack(ctxs[lane], W, H, F, roi=roi, frames_per_batch=args.batch)
             for f, p in zip(hframes, poses):
                 st.add_frame(f, p)
-            st.finish_into(hout)
+            st.finish_into(houts[lane])
             st.close()
 
-        step_e2e()
+        for lane in range(lanes):
+            step_e2e(lane)
+        # latency of one stack alone
+        t0 = time.perf_counter()
+        for _ in range(2):
+            step_e2e()
+        lat = (time.perf_counter() - t0) / 2
+        # stacks back to back, `lanes` in flight: every step still uploads its
+        # frames from pinned host memory and reads its fused result back
+        n_e2e = max(lanes, min(args.steps, 4) * lanes)
+        errors = []
+
+        def lane_worker(lane):
+            try:
+                for _ in range(n_e2e // lanes):
+                    step_e2e(lane)
+            except BaseException as exc:  # reported below
+                errors.append(exc)
+
         if dist:
             dist.barrier()
         t0 = time.perf_counter()
-        n_e2e = max(1, min(args.steps, 5))
-        for _ in range(n_e2e):
-            step_e2e()
+        threads = [threading.Thread(target=lane_worker, args=(lane,)) for lane in range(lanes)]
+        for th in threads:
+            th.start()
+        for th in threads:
+            th.join()
         dt = (time.perf_counter() - t0) / n_e2e
+        if errors:
+            raise errors[0]
         if dist:
-            t = torch.tensor([dt], device=f"cuda:{dev}")
+            t = torch.tensor([dt, lat], device=f"cuda:{dev}")
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            dt = float(t.item())
+            dt, lat = float(t[0].item()), float(t[1].item())
         e2e = {"value": world * px / dt / 1e6, "unit": UNIT, "h2d_bytes_per_step": F * W * H * 3,
-               "d2h_bytes_per_step": roi.width * roi.height * 3, "ms_per_step": dt * 1e3}
+               "d2h_bytes_per_step": roi.width * roi.height * 3, "ms_per_step": dt * 1e3,
+               "stacks_in_flight": lanes, "steps": n_e2e, "single_stack_latency_ms": lat * 1e3,
+               "single_stack_value": world * px / lat / 1e6}
+        for c in ctxs[1:]:
+            c.close()
         del hframes
 
     forms = None

@@ -98,6 +98,10 @@ cudaMemPool_t device_pool(int device) {
   }
   uint64_t keep = UINT64_MAX;
   cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  // reuse memory only once its free has completed: a stream of one context
+  // must never be made to wait for another context's queued work
+  int no = 0;
+  cudaMemPoolSetAttribute(pool, cudaMemPoolReuseAllowInternalDependencies, &no);
   pools[device] = pool;
   return pool;
 }

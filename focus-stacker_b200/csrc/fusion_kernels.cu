@@ -30,6 +30,13 @@ namespace {
 
 constexpr int TW = kTileW, TH = kTileH, NT = kThreads;
 constexpr int PPT = TW * TH / NT;  // output pixels per thread
+static_assert((NT / TW) * PPT == TH, "accumulator strips cover the tile");
+// Tile pixel (row-major index) of a thread's i-th accumulator: each thread
+// owns a column strip of PPT consecutive rows (column tid % TW), so that the
+// vertical EXPAND of neighbouring rows shares its source rows in registers.
+__device__ __forceinline__ int acc_pixel(int i) {
+  return ((int)(threadIdx.x / TW) * PPT + i) * TW + (int)(threadIdx.x % TW);
+}
 
 __device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
 __device__ __forceinline__ float kw(int i) { return (i == 0 || i == 4) ? 1.0f : ((i == 1 || i == 3) ? 4.0f : 6.0f); }
@@ -545,20 +552,46 @@ __device__ void expand_blend_step(LevelSmem& S, const LevelArgs& a, int x0, int 
     for (int c = 0; c < 3; ++c) hrow[(ii * 3 + c) * TW + xx] = expand_h1(S.ng[c] + ii * NW, t, exact);
   }
   __syncthreads();
+  // vertical EXPAND down this thread's strip: output rows yy0 .. yy0 + 7
+  // (yy0 even) read level-(l+1) rows q0 - 1 .. q0 + 4, q0 = (y0 + yy0) / 2,
+  // loaded once into registers (clamped rows for the clamped mode, zero
+  // outside the level for the no-wrap mode; the same operands expand_rows
+  // and expand_v1 select for each row)
+  const int xx = threadIdx.x % TW, yy0 = (threadIdx.x / TW) * PPT;
+  const int x = x0 + xx;
+  const int q0 = (y0 + yy0) >> 1;
+  constexpr int NR = PPT / 2 + 2;
+  float hv[3][NR];
+#pragma unroll
+  for (int k = 0; k < NR; ++k) {
+    int q = q0 - 1 + k;
+    bool zero = false;
+    if (exact) zero = q < 0 || q >= a.hn;
+    else q = clampi(q, 0, a.hn - 1);
+    const int lr = q - (y1 - 1);  // row of hrow
+#pragma unroll
+    for (int c = 0; c < 3; ++c) hv[c][k] = zero ? 0.0f : hrow[(lr * 3 + c) * TW + xx];
+  }
 #pragma unroll
   for (int i = 0; i < PPT; ++i) {
-    const int p = threadIdx.x + i * NT;
-    const int xx = p % TW, yy = p / TW;
-    const int x = x0 + xx, y = y0 + yy;
+    const int yy = yy0 + i, y = y0 + yy;
     if (x >= a.wl || y >= a.hl) continue;
-    const Rows r = expand_rows(y, y1, a.hn, exact);
+    const int j = i >> 1;
     const float div = exact ? exact_expand_divisor(x, y, a.wn, a.hn) : 1.0f;
     const float m = S.m[(yy + 2) * MW + (xx + 2)];
     const float4 g = S.gs[(yy + 4) * GW + (xx + 4)];
     const float gv[3] = {g.x, g.y, g.z};
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      const float e = expand_v1(hrow + c * TW + xx, 3 * TW, r, exact, div);
+      float e;
+      if ((i & 1) == 0) {  // even row: rows q - 1, q, q + 1
+        const float v = __fadd_rn(__fadd_rn(hv[c][j], __fmul_rn(6.0f, hv[c][j + 1])), hv[c][j + 2]);
+        e = exact ? __fdiv_rn(v, div) : __fmul_rn(v, 0.125f);
+      } else if (exact) {  // odd row, no-wrap: rows q, q + 1
+        e = __fdiv_rn(__fadd_rn(hv[c][j + 1], hv[c][j + 2]), div);
+      } else {  // odd row, clamped: row q read twice
+        e = __fmul_rn(__fadd_rn(hv[c][j + 1], hv[c][j + 1]), 0.5f);
+      }
       const float lap = __fsub_rn(gv[c], e);
       acc[i][c] = __fadd_rn(acc[i][c], __fmul_rn(lap, m));
     }
@@ -569,7 +602,7 @@ __device__ void expand_blend_step(LevelSmem& S, const LevelArgs& a, int x0, int 
 __device__ __forceinline__ void load_acc(const LevelArgs& a, int x0, int y0, float (&acc)[PPT][3]) {
 #pragma unroll
   for (int i = 0; i < PPT; ++i) {
-    const int p = threadIdx.x + i * NT;
+    const int p = acc_pixel(i);
     const int X = x0 + p % TW, Y = y0 + p / TW;
     const bool in = X < a.wl && Y < a.hl;
     const int64_t o = (int64_t)Y * a.pitch_l + X;
@@ -580,7 +613,7 @@ __device__ __forceinline__ void load_acc(const LevelArgs& a, int x0, int y0, flo
 __device__ __forceinline__ void store_acc(const LevelArgs& a, int x0, int y0, const float (&acc)[PPT][3]) {
 #pragma unroll
   for (int i = 0; i < PPT; ++i) {
-    const int p = threadIdx.x + i * NT;
+    const int p = acc_pixel(i);
     const int X = x0 + p % TW, Y = y0 + p / TW;
     if (X < a.wl && Y < a.hl) {
       const int64_t o = (int64_t)Y * a.pitch_l + X;
@@ -697,7 +730,7 @@ __global__ void __launch_bounds__(NT) level0_kernel(const __grid_constant__ Leve
       // 1x1 image: the top level is level 0 (src/fuse/pyramid.zig:1605-1649)
 #pragma unroll
       for (int i = 0; i < PPT; ++i) {
-        const int p = threadIdx.x + i * NT;
+        const int p = acc_pixel(i);
         const int xx = p % TW, yy = p / TW;
         if (x0 + xx >= a.wl || y0 + yy >= a.hl) continue;
         const float m = S.m[(yy + 2) * MW + (xx + 2)];
@@ -761,7 +794,7 @@ __global__ void __launch_bounds__(NT) level_kernel(const __grid_constant__ Level
     // exactly the terms the sequential loop adds
 #pragma unroll
     for (int i = 0; i < PPT; ++i) {
-      const int p = threadIdx.x + i * NT;
+      const int p = acc_pixel(i);
       const int X = x0 + p % TW, Y = y0 + p / TW;
       if (X < a.wl && Y < a.hl) {
         const int64_t o = (int64_t)Y * a.pitch_l + X;
