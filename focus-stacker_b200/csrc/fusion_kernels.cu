@@ -434,69 +434,100 @@ __device__ __forceinline__ float expand_v1(const float* h, int stride, const Row
 __device__ void reduce_step(LevelSmem& S, const LevelArgs& a, int x0, int y0) {
   const int x1 = x0 >> 1, y1 = y0 >> 1;
   float4* th = reinterpret_cast<float4*>(S.tmp);  // [GH][NW]
-  for (int i = threadIdx.x; i < GH * NW; i += NT) {
-    const int ry = i / NW, jj = i % NW;
-    const float4* row = S.gs + ry * GW + 2 * jj - 2 + 2;  // G region column of tap 0: 2j - 2 - (x0 - 4)
-    float v0 = 0.f, v1 = 0.f, v2 = 0.f, ws = 0.f;
+  // horizontal, two neighbouring outputs per thread (they share 3 of their
+  // 5 taps); each output sums its taps in the same order as alone
+  static_assert(NW % 2 == 0 && NH % 2 == 0 && TW1 % 2 == 0 && TH1 % 2 == 0, "output pairs");
+  for (int i = threadIdx.x; i < GH * (NW / 2); i += NT) {
+    const int ry = i / (NW / 2), jj = 2 * (i % (NW / 2));
+    const float4* row = S.gs + ry * GW + 2 * jj;  // G region column of tap 0: 2j - 2 - (x0 - 4)
+    float4 t[7];
 #pragma unroll
-    for (int kx = 0; kx < 5; ++kx) {
-      const float4 t = row[kx];
-      const float w = kw(kx) * t.w;
-      v0 = fmaf(w, t.x, v0);
-      v1 = fmaf(w, t.y, v1);
-      v2 = fmaf(w, t.z, v2);
-      ws += w;
+    for (int u = 0; u < 7; ++u) t[u] = row[u];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      float v0 = 0.f, v1 = 0.f, v2 = 0.f, ws = 0.f;
+#pragma unroll
+      for (int kx = 0; kx < 5; ++kx) {
+        const float4 tk = t[2 * h + kx];
+        const float w = kw(kx) * tk.w;
+        v0 = fmaf(w, tk.x, v0);
+        v1 = fmaf(w, tk.y, v1);
+        v2 = fmaf(w, tk.z, v2);
+        ws += w;
+      }
+      th[ry * NW + jj + h] = make_float4(v0, v1, v2, ws);
     }
-    th[i] = make_float4(v0, v1, v2, ws);
   }
   __syncthreads();
-  for (int i = threadIdx.x; i < NH * NW; i += NT) {
-    const int ii = i / NW, jj = i % NW;
-    const int yi = y1 - 1 + ii, xj = x1 - 1 + jj;
-    float v0 = 0.f, v1 = 0.f, v2 = 0.f, ws = 0.f;
+  for (int i = threadIdx.x; i < (NH / 2) * NW; i += NT) {
+    const int ii = 2 * (i / NW), jj = i % NW;
     const float4* col = th + (2 * ii) * NW + jj;  // G region row of tap 0: 2 yi - 2 - (y0 - 4)
+    float4 t[7];
 #pragma unroll
-    for (int ky = 0; ky < 5; ++ky) {
-      const float4 t = col[ky * NW];
-      const float w = kw(ky);
-      v0 = fmaf(w, t.x, v0);
-      v1 = fmaf(w, t.y, v1);
-      v2 = fmaf(w, t.z, v2);
-      ws = fmaf(w, t.w, ws);
+    for (int u = 0; u < 7; ++u) t[u] = col[u * NW];
+    const int xj = x1 - 1 + jj;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int yi = y1 - 1 + ii + h;
+      float v0 = 0.f, v1 = 0.f, v2 = 0.f, ws = 0.f;
+#pragma unroll
+      for (int ky = 0; ky < 5; ++ky) {
+        const float4 tk = t[2 * h + ky];
+        const float w = kw(ky);
+        v0 = fmaf(w, tk.x, v0);
+        v1 = fmaf(w, tk.y, v1);
+        v2 = fmaf(w, tk.z, v2);
+        ws = fmaf(w, tk.w, ws);
+      }
+      const bool sup = xj >= 0 && yi >= 0 && xj < a.wn && yi < a.hn && ws > 0.f;
+      const float r = sup ? __fdividef(1.0f, ws) : 0.0f;
+      const int o = (ii + h) * NW + jj;
+      S.ng[0][o] = v0 * r;
+      S.ng[1][o] = v1 * r;
+      S.ng[2][o] = v2 * r;
+      S.ns[o] = sup ? 1 : 0;
     }
-    const bool sup = xj >= 0 && yi >= 0 && xj < a.wn && yi < a.hn && ws > 0.f;
-    const float r = sup ? __fdividef(1.0f, ws) : 0.0f;
-    S.ng[0][i] = v0 * r;
-    S.ng[1][i] = v1 * r;
-    S.ng[2][i] = v2 * r;
-    S.ns[i] = sup ? 1 : 0;
   }
   float2* tm = reinterpret_cast<float2*>(S.tmp + GH * NW * 4 - MH * TW1 * 2);  // [MH][TW1], disjoint from th rows in use
   __syncthreads();
-  for (int i = threadIdx.x; i < MH * TW1; i += NT) {
-    const int ry = i / TW1, jj = i % TW1;
+  for (int i = threadIdx.x; i < MH * (TW1 / 2); i += NT) {
+    const int ry = i / (TW1 / 2), jj = 2 * (i % (TW1 / 2));
     const int base = ry * MW + 2 * jj;  // M region column of tap 0: 2j - 2 - (x0 - 2)
-    float v = 0.f, ws = 0.f;
+    float mv[7], sw[7];
 #pragma unroll
-    for (int kx = 0; kx < 5; ++kx) {
-      const float w = S.sm[base + kx] ? kw(kx) : 0.0f;
-      v = fmaf(w, S.m[base + kx], v);
-      ws += w;
+    for (int u = 0; u < 7; ++u) {
+      mv[u] = S.m[base + u];
+      sw[u] = S.sm[base + u] ? 1.0f : 0.0f;
     }
-    tm[i] = make_float2(v, ws);
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      float v = 0.f, ws = 0.f;
+#pragma unroll
+      for (int kx = 0; kx < 5; ++kx) {
+        const float w = sw[2 * h + kx] != 0.0f ? kw(kx) : 0.0f;
+        v = fmaf(w, mv[2 * h + kx], v);
+        ws += w;
+      }
+      tm[ry * TW1 + jj + h] = make_float2(v, ws);
+    }
   }
   __syncthreads();
-  for (int i = threadIdx.x; i < TH1 * TW1; i += NT) {
-    const int ii = i / TW1, jj = i % TW1;
-    float v = 0.f, ws = 0.f;
+  for (int i = threadIdx.x; i < (TH1 / 2) * TW1; i += NT) {
+    const int ii = 2 * (i / TW1), jj = i % TW1;
+    float2 t[7];
 #pragma unroll
-    for (int ky = 0; ky < 5; ++ky) {
-      const float2 t = tm[(2 * ii + ky) * TW1 + jj];  // M region row of tap 0: 2 yi - 2 - (y0 - 2)
-      const float w = kw(ky);
-      v = fmaf(w, t.x, v);
-      ws = fmaf(w, t.y, ws);
+    for (int u = 0; u < 7; ++u) t[u] = tm[(2 * ii + u) * TW1 + jj];  // M region row of tap 0: 2 yi - 2 - (y0 - 2)
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      float v = 0.f, ws = 0.f;
+#pragma unroll
+      for (int ky = 0; ky < 5; ++ky) {
+        const float w = kw(ky);
+        v = fmaf(w, t[2 * h + ky].x, v);
+        ws = fmaf(w, t[2 * h + ky].y, ws);
+      }
+      S.nm[(ii + h) * TW1 + jj] = ws > 0.f ? v * __fdividef(1.0f, ws) : 0.f;
     }
-    S.nm[i] = ws > 0.f ? v * __fdividef(1.0f, ws) : 0.f;
   }
   __syncthreads();
 }
@@ -543,13 +574,39 @@ __device__ void expand_blend_step(LevelSmem& S, const LevelArgs& a, int x0, int 
   const int x1 = x0 >> 1, y1 = y0 >> 1;
   float* hrow = S.tmp;  // [NH][3][TW]
   const bool exact = a.exact_expand != 0;
-  for (int i = threadIdx.x; i < NH * TW; i += NT) {
-    const int ii = i / TW, xx = i % TW;
+  // horizontal EXPAND, an even/odd output pair per thread: both read the
+  // level-(l+1) columns j - 1, j, j + 1 (clamped, or zero outside the level
+  // in the no-wrap mode), j = x / 2, with the operations of expand_h1
+  for (int i = threadIdx.x; i < NH * (TW / 2); i += NT) {
+    const int ii = i / (TW / 2), pp = i % (TW / 2);
     const int yi = y1 - 1 + ii;
     if (yi < 0 || yi >= a.hn) continue;
-    const Taps t = expand_taps(x0 + xx, x1, a.wn, exact);
+    const int j = x1 + pp, o = x1 - 1;
+    int ia, ib, ic;
+    if (exact) {
+      ia = pp;
+      ib = pp + 1;
+      ic = pp + 2;
+    } else {
+      ia = clampi(j - 1, 0, a.wn - 1) - o;
+      ib = clampi(j, 0, a.wn - 1) - o;
+      ic = clampi(j + 1, 0, a.wn - 1) - o;
+    }
 #pragma unroll
-    for (int c = 0; c < 3; ++c) hrow[(ii * 3 + c) * TW + xx] = expand_h1(S.ng[c] + ii * NW, t, exact);
+    for (int c = 0; c < 3; ++c) {
+      const float* g = S.ng[c] + ii * NW;
+      const float A = g[ia], B = g[ib], C = g[ic];
+      float ev, od;
+      if (exact) {
+        ev = __fadd_rn(__fadd_rn(A, __fmul_rn(6.0f, B)), C);
+        od = __fmul_rn(4.0f, __fadd_rn(B, C));
+      } else {
+        ev = __fmul_rn(__fadd_rn(__fadd_rn(A, __fmul_rn(6.0f, B)), C), 0.125f);
+        od = __fmul_rn(__fadd_rn(B, C), 0.5f);
+      }
+      hrow[(ii * 3 + c) * TW + 2 * pp] = ev;
+      hrow[(ii * 3 + c) * TW + 2 * pp + 1] = od;
+    }
   }
   __syncthreads();
   // vertical EXPAND down this thread's strip: output rows yy0 .. yy0 + 7
