@@ -89,8 +89,9 @@ __device__ __forceinline__ bool warp_disp(const Warp& w, double X, double Y, dou
   }
   const double nx = fma(w.a, X, fma(w.b, Y, w.c)) - dD * X;
   const double ny = fma(w.d, X, fma(w.e, Y, w.f)) - dD * Y;
-  *dx = nx / D;
-  *dy = ny / D;
+  const double rD = 1.0 / D;  // one division; x rD is within an ulp of / D
+  *dx = nx * rD;
+  *dy = ny * rD;
   return true;
 }
 
@@ -208,9 +209,36 @@ static __device__ __noinline__ uint32_t sample_exact(const Warp& w, const SrcIma
   }
   uint32_t out[3];
 #pragma unroll
-  for (int c = 0; c < 3; ++c) out[c] = (uint32_t)fmin(fmax(round(__ddiv_rn(val[c], support)), 0.0), 255.0);
+  for (int c = 0; c < 3; ++c) {
+    // value / 1 is the value: skip the division when the weights sum to 1
+    const double q = support == 1.0 ? val[c] : __ddiv_rn(val[c], support);
+    out[c] = (uint32_t)fmin(fmax(round(q), 0.0), 255.0);
+  }
   const uint32_t alpha = all_in ? 255u : (uint32_t)fmin(fmax(round(__dmul_rn(support, 255.0)), 0.0), 255.0);
   return pack_rgba(out[0], out[1], out[2], alpha);
+}
+
+// floor of v (|v| < 2^22) and its integer, without the float-to-int
+// conversion unit: the nearest integer from adding and removing 1.5 * 2^23,
+// minus one where that rounded up.
+__device__ __forceinline__ float floor_small(float v, int* iv) {
+  const float t = __fadd_rn(v, 12582912.0f);
+  const float r = __fsub_rn(t, 12582912.0f);
+  const bool up = r > v;
+  *iv = (__float_as_int(t) - 0x4B400000) - (up ? 1 : 0);
+  return up ? __fsub_rn(r, 1.0f) : r;
+}
+
+// Nearest integer of v (|v| < 2^22), clamped to 0..255, by adding and
+// removing 1.5 * 2^23 (no float-to-int conversion), and the distance |v - r|:
+// a value farther than 0.5 - kTieBand from r lies within kTieBand of a .5
+// rounding boundary, where the FP32 evaluation cannot decide the reference's
+// half-away rounding.  Away from those boundaries nearest rounding is it.
+__device__ __forceinline__ uint32_t round_near_u8(float v, float* dist) {
+  const float t = __fadd_rn(v, 12582912.0f);
+  *dist = fabsf(__fsub_rn(v, __fsub_rn(t, 12582912.0f)));
+  const int r = __float_as_int(t) - 0x4B400000;
+  return (uint32_t)min(max(r, 0), 255);
 }
 
 // Fast path only: returns false (leaving *out untouched) when the exact
@@ -224,9 +252,10 @@ __device__ __forceinline__ bool sample_try(const SrcImage& s, const Anchor& a, i
   float rd = __fdividef(1.0f, den);
   float tx = a.fxh + fmaf(nx, rd, a.fxl);
   float ty = a.fyh + fmaf(ny, rd, a.fyl);
-  float flx = floorf(tx), fly = floorf(ty);
-  int x0 = a.ix + du + (int)flx;
-  int y0 = a.iy + dv + (int)fly;
+  int ixf, iyf;
+  const float flx = floor_small(tx, &ixf), fly = floor_small(ty, &iyf);
+  int x0 = a.ix + du + ixf;
+  int y0 = a.iy + dv + iyf;
   float fx = tx - flx, fy = ty - fly;
   if (x0 < 1 || y0 < 1 || x0 > s.w - 3 || y0 > s.h - 3) return false;
   float v00[3], v10[3], v01[3], v11[3];
@@ -236,19 +265,18 @@ __device__ __forceinline__ bool sample_try(const SrcImage& s, const Anchor& a, i
   load_rgb_biased(s, x0 + 1, y0 + 1, v11);
   float fxy = fx * fy;
   uint32_t o[3];
-  bool tie = false;
+  float dmax = 0.0f;
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
     float d10 = v10[c] - v00[c], d01 = v01[c] - v00[c], d11 = (v11[c] - v10[c]) - d01;
     float v = fmaf(fx, d10, v00[c] - 8388608.0f);
     v = fmaf(fy, d01, v);
     v = fmaf(fxy, d11, v);
-    float k = floorf(v);
-    float fr = v - k;
-    tie = tie || fabsf(fr - 0.5f) < kTieBand;
-    float r = fr > 0.5f ? k + 1.0f : k;
-    o[c] = (uint32_t)fminf(fmaxf(r, 0.0f), 255.0f);
+    float d;
+    o[c] = round_near_u8(v, &d);
+    dmax = fmaxf(dmax, d);
   }
+  const bool tie = dmax > 0.5f - kTieBand;
   if (tie) return false;
   *out = pack_rgba(o[0], o[1], o[2], 255u);
   return true;
@@ -266,9 +294,10 @@ __device__ __forceinline__ uint32_t sample_fast(const Warp& w, const SrcImage& s
   float rd = __fdividef(1.0f, den);
   float tx = a.fxh + fmaf(nx, rd, a.fxl);
   float ty = a.fyh + fmaf(ny, rd, a.fyl);
-  float flx = floorf(tx), fly = floorf(ty);
-  int x0 = a.ix + du + (int)flx;
-  int y0 = a.iy + dv + (int)fly;
+  int ixf, iyf;
+  const float flx = floor_small(tx, &ixf), fly = floor_small(ty, &iyf);
+  int x0 = a.ix + du + ixf;
+  int y0 = a.iy + dv + iyf;
   float fx = tx - flx, fy = ty - fly;
   // taps at least one pixel inside on every side: the floor decision then
   // cannot change which sampler the reference takes
@@ -280,19 +309,18 @@ __device__ __forceinline__ uint32_t sample_fast(const Warp& w, const SrcImage& s
   load_rgb_biased(s, x0 + 1, y0 + 1, v11);
   float fxy = fx * fy;
   uint32_t o[3];
-  bool tie = false;
+  float dmax = 0.0f;
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
     float d10 = v10[c] - v00[c], d01 = v01[c] - v00[c], d11 = (v11[c] - v10[c]) - d01;
     float v = fmaf(fx, d10, v00[c] - 8388608.0f);
     v = fmaf(fy, d01, v);
     v = fmaf(fxy, d11, v);
-    float k = floorf(v);
-    float fr = v - k;
-    tie = tie || fabsf(fr - 0.5f) < kTieBand;
-    float r = fr > 0.5f ? k + 1.0f : k;
-    o[c] = (uint32_t)fminf(fmaxf(r, 0.0f), 255.0f);
+    float d;
+    o[c] = round_near_u8(v, &d);
+    dmax = fmaxf(dmax, d);
   }
+  const bool tie = dmax > 0.5f - kTieBand;
   if (tie) return sample_exact(w, s, X, Y);
   return pack_rgba(o[0], o[1], o[2], 255u);
 }
