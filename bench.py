@@ -155,20 +155,21 @@ def algorithmic_bytes(roi_w, roi_h, frames, k, mode="cache", storage_bytes=4):
     read once per remap, per-pixel state (weight sum, union, accumulators) is
     read and written once per batch of k frames.  mode "cache": pass 1 keeps
     the remapped frame (RGBA, 4 B) and its weight (4 B) for pass 2; "recompute":
-    pass 2 remaps again into per-batch slots.  Returns {kernel: bytes per step}
-    and the pipeline total."""
+    pass 2 remaps again into per-batch slots; "laps": pass 1 also builds the
+    Gaussian/Laplacian pyramids ("image") and pass 2 only the masks and the
+    blend.  Returns {kernel: bytes per step} and the pipeline total."""
     sz = level_sizes(roi_w, roi_h)
     A = [w * h for w, h in sz]
     L = len(sz)
     batches = -(-frames // k)
     s = storage_bytes
     b = {}
-    keep = 8 if mode == "cache" else 0
+    keep = 8 if mode in ("cache", "laps") else 0
     # pass 1: frame 3 B/px (+ kept planes 8 B/px); weight sum f32 and union u8
     # read+write per batch (the first batch only writes)
     b["pass1"] = frames * (3 + keep) * A[0] + batches * 10 * A[0] - 5 * A[0]
     # pass-2 re-remap (recompute mode): frame 3 B/px read, planes 8 B/px written
-    b["remap_weights"] = 0 if mode == "cache" else frames * 11 * A[0]
+    b["remap_weights"] = 0 if mode in ("cache", "laps") else frames * 11 * A[0]
     # level 0: planes 8 B/px read; level-1 Gaussian/mask (4 s B) + support (1 B)
     # written at 1/4 area; weight sum 4 + union 1 read and accumulator 24
     # read+write per batch
@@ -189,6 +190,25 @@ def algorithmic_bytes(roi_w, roi_h, frames, k, mode="cache", storage_bytes=4):
     for l in range(L - 1, 0, -1):
         col += 12 * A[l] + (24 * A[l - 1] if l - 1 > 0 else 15 * A[0])
     b["collapse"] = col
+    b["image"] = 0
+    b["blend0"] = 0
+    if mode == "laps":
+        # pass 1 builds each frame's Gaussian/Laplacian pyramid: RGBA read,
+        # per level the Laplacian written (12 B) and the next Gaussian and
+        # support written (3s + 1) and read again by the next level;
+        # pass 2 reads weights and Laplacians and writes / reads the masks
+        img = 4 * A[0]
+        for l in range(L - 1):
+            img += 12 * A[l] + (3 * s + 1) * A[l + 1] + ((3 * s + 1) * A[l] if l >= 1 else 0)
+        b["image"] = frames * img
+        b["blend0"] = frames * 16 * A[0] + 16 * A[0]
+        b["level0"] = frames * (4 * A[0] + s * l1) + batches * 5 * A[0]
+        lv = 0
+        for l in range(1, L - 1):
+            nxt = A[l + 1] if l + 1 < L - 1 else 0
+            top = A[l + 1] * 24 * batches if l + 1 == L - 1 else 0
+            lv += frames * (s * A[l] + 12 * A[l] + s * nxt) + batches * 25 * A[l] + top
+        b["level"] = lv
     return b, sum(b.values())
 
 
@@ -504,14 +524,14 @@ def main():
     ctx.set_kernel_timing(True)
     step()
     stats = {}
-    for name in ("pass1", "remap_weights", "level0", "level", "collapse", "mask_support"):
+    for name in ("pass1", "image", "remap_weights", "blend0", "level0", "level", "collapse", "mask_support"):
         n, tot = ctx.kernel_stats(name)
         stats[name] = (n, tot)
     ctx.set_kernel_timing(False)
     k_default = 8 if args.batch == 0 else args.batch
     k_eff = max(1, min(k_default, 8, F))
     alg, alg_total = algorithmic_bytes(roi.width, roi.height, F, k_eff,
-                                       "cache" if mode_used["mode"] == "cache" else "recompute")
+                                       mode_used["mode"] if mode_used["mode"] in ("cache", "laps") else "recompute")
     dom = max(stats, key=lambda n: stats[n][1])
     n_dom, ms_dom = stats[dom]
     peak, peak_kind = measured_hbm_peak()

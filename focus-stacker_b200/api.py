@@ -278,7 +278,7 @@ def remap_rigid_image_device(ctx: Context, src, src_stride: int, width: int, hei
 
 
 # --------------------------------------------------------------------- fusion
-PASS2_MODES = ("cache", "resident", "refetch")
+PASS2_MODES = ("cache", "resident", "refetch", "laps")
 
 
 def stack_desc(src_width: int, src_height: int, frame_count: int, roi: Optional[Rect] = None, channels: int = 3,
@@ -331,7 +331,7 @@ class PyramidContrastStack:
         self.out_width, self.out_height = w.value, hh.value
         self._keep = []
 
-    PASS2_MODES = ("cache", "resident", "refetch")
+    PASS2_MODES = PASS2_MODES
 
     @property
     def pass2_mode(self) -> str:

@@ -170,7 +170,12 @@ int64_t round_up(int64_t v, int64_t m) { return (v + m - 1) / m * m; }
 //  RESIDENT  frames stay on the device and pass 2 remaps them again;
 //  REFETCH   frames are only staged; pass 2 asks the caller for them again
 //            and remaps them (src/stack/pipeline.zig:561-597).
-enum Pass2Mode { P2_CACHE = 0, P2_RESIDENT = 1, P2_REFETCH = 2 };
+//  LAPS      pass 1 also builds each frame's Gaussian/Laplacian pyramid (it
+//            does not depend on the weight sum) and keeps its Laplacians and
+//            weight; pass 2 is then only the mask pyramid and the blend.  Same
+//            operations, so the same bytes as the other modes; it moves most
+//            of pass 2 into pass 1, which overlaps the frame uploads.
+enum Pass2Mode { P2_CACHE = 0, P2_RESIDENT = 1, P2_REFETCH = 2, P2_LAPS = 3 };
 
 struct fs_stack {
   fs_ctx* ctx = nullptr;
@@ -188,7 +193,12 @@ struct fs_stack {
   std::vector<float*> acc;     // per level, 3 planes
   std::vector<std::vector<LevelPlanes>> slot;  // [k][l], l = 1 .. L-2
   std::vector<FramePlanes> cache;              // CACHE: per frame
-  std::vector<FramePlanes> p2;                 // RESIDENT / REFETCH: per batch slot (K)
+  std::vector<FramePlanes> p2;                 // RESIDENT / REFETCH / LAPS: per batch slot (K)
+  std::vector<float*> wplane;                  // LAPS: per frame, its weight (level 0)
+  std::vector<std::vector<float*>> lap;        // LAPS: per frame, Laplacian of levels 0 .. L-2
+  std::vector<float*> gtop;                    // LAPS: per frame, Gaussian of the top level
+  std::vector<const float*> tab_host;          // LAPS: level-0 Laplacian then weight pointers, all frames
+  const float** tab = nullptr;                 // the same table on the device
   uint8_t* out_dev = nullptr;
   std::vector<Alloc> allocs;
   struct Frame {
@@ -276,6 +286,7 @@ int launch_remap_weights_batch(fs_stack* s, const std::vector<fs_stack::Frame>& 
     if (!build_frame_in(s, frames[k], &a.f[k - begin], &why)) return set_err(s->ctx, FS_ERR_INVALID, why);
     if (pass1) {
       if (s->mode == P2_CACHE) a.out[k - begin] = s->cache[k];
+      if (s->mode == P2_LAPS) a.out[k - begin] = FramePlanes{s->p2[k - begin].rgba, s->wplane[k]};
     } else {
       a.out[k - begin] = s->p2[k - begin];
     }
@@ -286,8 +297,55 @@ int launch_remap_weights_batch(fs_stack* s, const std::vector<fs_stack::Frame>& 
   return FS_OK;
 }
 
+// Geometry of the step from level l to l + 1 (the fields every level kernel
+// reads), frames of the batch left to the caller.
+void level_geometry(const fs_stack* s, uint32_t l, LevelArgs* a) {
+  a->level = (int32_t)l;
+  a->wl = (int32_t)s->lw[l];
+  a->hl = (int32_t)s->lh[l];
+  a->pitch_l = s->pitch[l];
+  a->exact_expand = std::max(s->lw[l], s->lh[l]) <= kExactExpandMaxDim ? 1 : 0;
+  a->sm_l = s->sm[l];
+  a->acc_l = s->acc[l];
+  a->acc_plane_l = s->pitch[l] * s->lh[l];
+  if (l + 1 < s->L) {
+    a->wn = (int32_t)s->lw[l + 1];
+    a->hn = (int32_t)s->lh[l + 1];
+    a->pitch_n = s->pitch[l + 1];
+    a->acc_n = s->acc[l + 1];
+    a->acc_plane_n = s->pitch[l + 1] * s->lh[l + 1];
+  } else {
+    a->wn = a->hn = 1;
+    a->pitch_n = 32;
+  }
+}
+
+// LAPS pass 1: the Gaussian / Laplacian pyramid of frames [begin, end), one
+// frame per CTA, from their remapped RGBA in the batch slots.
+int launch_image_pyramid(fs_stack* s, size_t begin, size_t end) {
+  LevelArgs a;
+  std::memset(&a, 0, sizeof(a));
+  a.levels = (int32_t)s->L;
+  a.K = (int32_t)(end - begin);
+  for (uint32_t l = 0; l + 1 < s->L; ++l) {
+    level_geometry(s, l, &a);
+    for (size_t k = 0; k < (size_t)a.K; ++k) {
+      a.in0[k] = s->p2[k];
+      if (l >= 1) a.in[k] = s->slot[k][l];
+      a.out[k] = l + 1 < s->L - 1 ? s->slot[k][l + 1] : LevelPlanes{};
+      a.lap[k] = s->lap[begin + k][l];
+      a.gtop[k] = s->gtop[begin + k];
+    }
+    cudaError_t e = timed(s->ctx, "image", [&] { return launch_img_level(a, s->storage, s->ctx->stream); });
+    if (e != cudaSuccess) return cuda_err(s->ctx, e, "image pyramid launch");
+  }
+  return FS_OK;
+}
+
 int launch_pass1_batch(fs_stack* s, size_t begin, size_t end) {
-  return launch_remap_weights_batch(s, s->frames, begin, end, true);
+  int rc = launch_remap_weights_batch(s, s->frames, begin, end, true);
+  if (rc == FS_OK && s->mode == P2_LAPS) rc = launch_image_pyramid(s, begin, end);
+  return rc;
 }
 
 int run_pending_pass1(fs_stack* s, bool flush) {
@@ -594,6 +652,7 @@ struct StackPlan {
   size_t staging_slots = 0;  // frame buffers of the two-batch upload ring
   uint32_t fp_level = 0;     // first level l >= 1 run one frame per CTA (L - 1: none)
   size_t contrib = 0, contrib_top = 0;  // bytes of the contribution buffers
+  size_t laps_frame = 0;                // LAPS: weight + Laplacians + top Gaussian of one frame
 };
 
 // Levels with fewer 64x32 tiles than this run one frame per CTA (grid.z = K)
@@ -639,6 +698,11 @@ StackPlan plan_stack(const fs_stack_desc& d) {
       }
     }
   }
+  if (p.L >= 3) {
+    p.laps_frame = n0 * 4;
+    for (uint32_t l = 0; l + 1 < p.L; ++l) p.laps_frame += (size_t)p.pitch[l] * p.lh[l] * 12;
+    p.laps_frame += (size_t)p.pitch[p.L - 1] * p.lh[p.L - 1] * 12;
+  }
   if (p.fp_level + 1 < p.L) {
     p.contrib = (size_t)p.K * 3 * p.pitch[p.fp_level] * p.lh[p.fp_level] * 4;
     p.contrib_top = (size_t)p.K * 3 * p.pitch[p.L - 1] * p.lh[p.L - 1] * 4;
@@ -652,6 +716,8 @@ StackPlan plan_stack(const fs_stack_desc& d) {
 uint64_t plan_bytes(const StackPlan& p, uint32_t frames, Pass2Mode mode, bool host_frames) {
   const uint64_t staging = host_frames ? (uint64_t)p.frame_bytes * p.staging_slots : 0;
   switch (mode) {
+    case P2_LAPS:
+      return p.fixed + (uint64_t)p.planes / 2 * p.K + ((uint64_t)p.laps_frame + 2 * sizeof(float*)) * frames + staging;
     case P2_CACHE: return p.fixed + (uint64_t)p.planes * frames + staging;
     case P2_RESIDENT: return p.fixed + (uint64_t)p.planes * p.K + (uint64_t)p.frame_bytes * frames;
     default: return p.fixed + (uint64_t)p.planes * p.K + staging;
@@ -661,6 +727,7 @@ uint64_t plan_bytes(const StackPlan& p, uint32_t frames, Pass2Mode mode, bool ho
 // Pass-2 mode for `available` device bytes: cache the pass-1 planes when they
 // fit, else keep the frames, else refetch them.
 Pass2Mode choose_mode(const StackPlan& p, uint32_t frames, uint64_t available, bool host_frames) {
+  if (p.laps_frame && plan_bytes(p, frames, P2_LAPS, host_frames) <= available) return P2_LAPS;
   if (plan_bytes(p, frames, P2_CACHE, host_frames) <= available) return P2_CACHE;
   if (plan_bytes(p, frames, P2_RESIDENT, host_frames) <= available) return P2_RESIDENT;
   return P2_REFETCH;
@@ -743,7 +810,32 @@ static int begin_impl(fs_ctx* ctx, const fs_stack_desc* desc, fs_stack** out, in
   const uint64_t available = ctx->budget + plan.fixed > in_use ? ctx->budget + plan.fixed - in_use : 0;
   s->mode = forced_mode >= 0 ? (Pass2Mode)forced_mode : choose_mode(plan, d.frame_count, available, true);
   const size_t planes_bytes = plan.planes;
-  if (s->mode == P2_CACHE) {
+  if (s->mode == P2_LAPS) {
+    for (uint32_t kk = 0; kk < s->K; ++kk) {
+      if ((rc = stack_alloc(s, n0 * 4, &p)) != FS_OK) return fail(rc);
+      s->p2.push_back(FramePlanes{(uint32_t*)p, nullptr});
+    }
+    for (uint32_t f = 0; f < d.frame_count; ++f) {
+      if ((rc = stack_alloc(s, plan.laps_frame, &p)) != FS_OK) return fail(rc);
+      uint8_t* q = (uint8_t*)p;
+      s->wplane.push_back((float*)q);
+      q += n0 * 4;
+      std::vector<float*> lv;
+      for (uint32_t l = 0; l + 1 < s->L; ++l) {
+        lv.push_back((float*)q);
+        q += (size_t)s->pitch[l] * s->lh[l] * 12;
+      }
+      s->lap.push_back(lv);
+      s->gtop.push_back((float*)q);
+    }
+    for (uint32_t f = 0; f < d.frame_count; ++f) s->tab_host.push_back(s->lap[f][0]);
+    for (uint32_t f = 0; f < d.frame_count; ++f) s->tab_host.push_back(s->wplane[f]);
+    if ((rc = stack_alloc(s, s->tab_host.size() * sizeof(float*), &p)) != FS_OK) return fail(rc);
+    s->tab = (const float**)p;
+    if (cudaMemcpyAsync(p, s->tab_host.data(), s->tab_host.size() * sizeof(float*), cudaMemcpyHostToDevice,
+                        ctx->stream) != cudaSuccess)
+      return fail(cuda_err(ctx, cudaGetLastError(), "frame table upload"));
+  } else if (s->mode == P2_CACHE) {
     for (uint32_t f = 0; f < d.frame_count; ++f) {
       if ((rc = stack_alloc(s, planes_bytes, &p)) != FS_OK) return fail(rc);
       s->cache.push_back(FramePlanes{(uint32_t*)p, (float*)((uint8_t*)p + n0 * 4)});
@@ -859,10 +951,18 @@ static int finish_impl(fs_stack* s, fs_frame_fetch_cb refetch, void* user, void*
   }
   // pass 2 in batches of K frames
   const size_t N = s->frames.size();
+  if (s->mode == P2_LAPS) {
+    // level-0 blend of every frame at once, streaming over the Laplacians
+    e = timed(ctx, "blend0", [&] {
+      return launch_blend0(s->acc[0], s->pitch[0] * s->lh[0], s->pitch[0], (int)s->W, (int)s->H, s->norm, s->tab,
+                           (float* const*)(s->tab + N), (int)N, 1.0f / (float)N, st);
+    });
+    if (e != cudaSuccess) return cuda_err(ctx, e, "level-0 blend");
+  }
   std::vector<fs_stack::Frame> frames = s->frames;
   for (size_t begin = 0; begin < N; begin += s->K) {
     const size_t end = std::min(N, begin + s->K);
-    if (s->mode != P2_CACHE) {
+    if (s->mode == P2_RESIDENT || s->mode == P2_REFETCH) {
       for (size_t k = begin; k < end; ++k) {
         fs_stack::Frame& fr = frames[k];
         if (fr.resident) continue;
@@ -893,7 +993,11 @@ static int finish_impl(fs_stack* s, fs_frame_fetch_cb refetch, void* user, void*
     a.K = (int32_t)(end - begin);
     a.inv_count = 1.0f / (float)N;
     a.norm = s->norm;
-    for (size_t k = begin; k < end; ++k) a.in0[k - begin] = s->mode == P2_CACHE ? s->cache[k] : s->p2[k - begin];
+    const bool laps = s->mode == P2_LAPS;
+    for (size_t k = begin; k < end; ++k) {
+      a.in0[k - begin] = s->mode == P2_CACHE ? s->cache[k] : laps ? FramePlanes{nullptr, s->wplane[k]} : s->p2[k - begin];
+      if (laps) a.gtop[k - begin] = s->gtop[k];
+    }
     for (uint32_t l = 0; l + 1 < s->L || (s->L == 1 && l == 0); ++l) {
       a.level = (int32_t)l;
       a.wl = (int32_t)s->lw[l];
@@ -916,12 +1020,14 @@ static int finish_impl(fs_stack* s, fs_frame_fetch_cb refetch, void* user, void*
       for (size_t k = 0; k < (size_t)a.K; ++k) {
         if (l >= 1) a.in[k] = s->slot[k][l];
         if (l + 1 < s->L - 1) a.out[k] = s->slot[k][l + 1];
+        if (laps) a.lap[k] = s->lap[begin + k][l];
       }
       const bool fp = l >= 1 && l >= s->fp_level && s->contrib && a.K > 1;
       a.frame_parallel = fp ? 1 : 0;
       a.contrib = fp ? s->contrib : nullptr;
       a.contrib_top = fp ? s->contrib_top : nullptr;
-      if (l == 0) e = timed(ctx, "level0", [&] { return launch_level0(a, s->storage, st); });
+      if (laps) e = timed(ctx, l == 0 ? "level0" : "level", [&] { return launch_mask_level(a, s->storage, st); });
+      else if (l == 0) e = timed(ctx, "level0", [&] { return launch_level0(a, s->storage, st); });
       else e = timed(ctx, "level", [&] { return launch_level(a, s->storage, st); });
       if (e != cudaSuccess) return cuda_err(ctx, e, "level launch");
       if (fp) {

@@ -332,6 +332,7 @@ constexpr int TW1 = TW / 2, TH1 = TH / 2;
 constexpr int kTmpFloats = (GH * NW * 4 > NH * TW * 3) ? GH * NW * 4 : NH * TW * 3;
 
 struct __align__(16) LevelSmem {
+  static constexpr int kTmOffset = GH * NW * 4 - MH * TW1 * 2;  // mask REDUCE rows at the end of tmp
   float4 gs[GH * GW];       // level-l Gaussian (r, g, b) and support (0 / 1)
   float tmp[kTmpFloats];    // reduce / expand temporaries
   float ng[3][NH * NW];     // level-(l+1) Gaussian (zero outside the level)
@@ -431,7 +432,8 @@ __device__ __forceinline__ float expand_v1(const float* h, int stride, const Row
 // src/fuse/pyramid.zig:997-1099: 5x5 taps [1 4 6 4 1]^2 over in-range
 // samples with support > 0, value = sum(w v) / sum(w), support = sum(w) > 0.
 // Evaluated separably (rows first); the weights are exact small integers.
-__device__ void reduce_step(LevelSmem& S, const LevelArgs& a, int x0, int y0) {
+template <class SM>
+__device__ void reduce_image_step(SM& S, const LevelArgs& a, int x0, int y0) {
   const int x1 = x0 >> 1, y1 = y0 >> 1;
   float4* th = reinterpret_cast<float4*>(S.tmp);  // [GH][NW]
   // horizontal, two neighbouring outputs per thread (they share 3 of their
@@ -488,8 +490,13 @@ __device__ void reduce_step(LevelSmem& S, const LevelArgs& a, int x0, int y0) {
       S.ns[o] = sup ? 1 : 0;
     }
   }
-  float2* tm = reinterpret_cast<float2*>(S.tmp + GH * NW * 4 - MH * TW1 * 2);  // [MH][TW1], disjoint from th rows in use
   __syncthreads();
+}
+
+// Mask half of the REDUCE (level-l mask with the level-l mask support).
+template <class SM>
+__device__ void reduce_mask_step(SM& S) {
+  float2* tm = reinterpret_cast<float2*>(S.tmp + SM::kTmOffset);  // [MH][TW1]
   for (int i = threadIdx.x; i < MH * (TW1 / 2); i += NT) {
     const int ry = i / (TW1 / 2), jj = 2 * (i % (TW1 / 2));
     const int base = ry * MW + 2 * jj;  // M region column of tap 0: 2j - 2 - (x0 - 2)
@@ -532,6 +539,11 @@ __device__ void reduce_step(LevelSmem& S, const LevelArgs& a, int x0, int y0) {
   __syncthreads();
 }
 
+__device__ __forceinline__ void reduce_step(LevelSmem& S, const LevelArgs& a, int x0, int y0) {
+  reduce_image_step(S, a, x0, y0);
+  reduce_mask_step(S);
+}
+
 // Store the level-(l+1) tile (Gaussian, support, mask) of one frame, or add
 // it into the top accumulator when l + 1 is the last level
 // (src/fuse/pyramid.zig:1533-1554, 1605-1649).
@@ -570,7 +582,11 @@ __device__ void store_next(const LevelSmem& S, const LevelArgs& a, int x0, int y
 // EXPAND of the level-(l+1) Gaussian back to the level-l tile fused with the
 // weighted Laplacian blend into the accumulator registers:
 // acc += (G_l - EXPAND(G_{l+1})) * M_l  (src/fuse/pyramid.zig:1480-1504).
-__device__ void expand_blend_step(LevelSmem& S, const LevelArgs& a, int x0, int y0, float (&acc)[PPT][3]) {
+// LAP: store the Laplacian G_l - EXPAND(G_{l+1}) of the tile into lap (3
+// planes of acc_plane_l floats, level pitch) instead of blending it.
+template <bool LAP = false, class SM = LevelSmem>
+__device__ void expand_blend_step(SM& S, const LevelArgs& a, int x0, int y0, float (&acc)[PPT][3],
+                                  float* lap_out = nullptr) {
   const int x1 = x0 >> 1, y1 = y0 >> 1;
   float* hrow = S.tmp;  // [NH][3][TW]
   const bool exact = a.exact_expand != 0;
@@ -635,7 +651,8 @@ __device__ void expand_blend_step(LevelSmem& S, const LevelArgs& a, int x0, int 
     if (x >= a.wl || y >= a.hl) continue;
     const int j = i >> 1;
     const float div = exact ? exact_expand_divisor(x, y, a.wn, a.hn) : 1.0f;
-    const float m = S.m[(yy + 2) * MW + (xx + 2)];
+    float m = 0.0f;
+    if constexpr (!LAP) m = S.m[(yy + 2) * MW + (xx + 2)];
     const float4 g = S.gs[(yy + 4) * GW + (xx + 4)];
     const float gv[3] = {g.x, g.y, g.z};
 #pragma unroll
@@ -650,7 +667,8 @@ __device__ void expand_blend_step(LevelSmem& S, const LevelArgs& a, int x0, int 
         e = __fmul_rn(__fadd_rn(hv[c][j + 1], hv[c][j + 1]), 0.5f);
       }
       const float lap = __fsub_rn(gv[c], e);
-      acc[i][c] = __fadd_rn(acc[i][c], __fmul_rn(lap, m));
+      if (LAP) lap_out[c * a.acc_plane_l + (int64_t)y * a.pitch_l + x] = lap;
+      else acc[i][c] = __fadd_rn(acc[i][c], __fmul_rn(lap, m));
     }
   }
   __syncthreads();
@@ -680,7 +698,8 @@ __device__ __forceinline__ void store_acc(const LevelArgs& a, int x0, int y0, co
   }
 }
 
-__device__ __forceinline__ void load_mask_support(LevelSmem& S, const LevelArgs& a, int x0, int y0) {
+template <class SM>
+__device__ __forceinline__ void load_mask_support(SM& S, const LevelArgs& a, int x0, int y0) {
   for (int i = threadIdx.x; i < MH * MW; i += NT) {
     const int X = x0 - 2 + i % MW, Y = y0 - 2 + i / MW;
     const bool in = X >= 0 && Y >= 0 && X < a.wl && Y < a.hl;
@@ -862,6 +881,267 @@ __global__ void __launch_bounds__(NT) level_kernel(const __grid_constant__ Level
   } else {
     store_acc(a, x0, y0, acc);
   }
+}
+
+// ================================================== split pyramid kernels
+// The image half (pass 1, as the frames arrive) and the mask half (pass 2,
+// once the weight sum is complete) of a level step, with the Laplacians in
+// HBM between them.  Every operation is the one of the fused kernels above,
+// in the same order, so both give identical accumulators.
+namespace {
+
+struct __align__(16) ImgSmem {
+  float4 gs[GH * GW];
+  float tmp[kTmpFloats];
+  float ng[3][NH * NW];
+  uint8_t ns[NH * NW];
+};
+static_assert(offsetof(ImgSmem, tmp) % 16 == 0, "tmp is accessed as float4");
+
+struct __align__(16) MaskSmem {
+  static constexpr int kTmOffset = 0;
+  float tmp[MH * TW1 * 2];
+  float nm[TH1 * TW1];
+  float m[MH * MW];
+  uint8_t sm[MH * MW];
+};
+
+template <typename T>
+__device__ void store_next_image(const ImgSmem& S, const LevelArgs& a, int x0, int y0, int k) {
+  const int x1 = x0 >> 1, y1 = y0 >> 1;
+  const bool top = a.level + 1 == a.levels - 1;
+  for (int i = threadIdx.x; i < TH1 * TW1; i += NT) {
+    const int ii = i / TW1, jj = i % TW1;
+    const int xj = x1 + jj, yi = y1 + ii;
+    if (xj >= a.wn || yi >= a.hn) continue;
+    const int ni = (ii + 1) * NW + (jj + 1);
+    const int64_t o = (int64_t)yi * a.pitch_n + xj;
+    if (top) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) a.gtop[k][c * a.acc_plane_n + o] = S.ng[c][ni];
+    } else {
+      const LevelPlanes& out = a.out[k];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) stv<T>((T*)out.g, c * out.plane + o, S.ng[c][ni]);
+      out.s[o] = S.ns[ni];
+    }
+  }
+}
+
+template <typename T>
+__device__ void store_next_mask(const MaskSmem& S, const LevelArgs& a, int x0, int y0, int k) {
+  const int x1 = x0 >> 1, y1 = y0 >> 1;
+  const bool top = a.level + 1 == a.levels - 1;
+  for (int i = threadIdx.x; i < TH1 * TW1; i += NT) {
+    const int ii = i / TW1, jj = i % TW1;
+    const int xj = x1 + jj, yi = y1 + ii;
+    if (xj >= a.wn || yi >= a.hn) continue;
+    const int64_t o = (int64_t)yi * a.pitch_n + xj;
+    if (top) {
+      const float m = S.nm[i];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const float t = __fmul_rn(a.gtop[k][c * a.acc_plane_n + o], m);
+        if (a.frame_parallel) {
+          a.contrib_top[(int64_t)(k * 3 + c) * a.acc_plane_n + o] = t;
+        } else {
+          float* acc = a.acc_n + c * a.acc_plane_n + o;
+          *acc = __fadd_rn(*acc, t);
+        }
+      }
+    } else {
+      stv<T>((T*)a.out[k].m, o, S.nm[i]);
+    }
+  }
+}
+
+}  // namespace
+
+template <typename T, bool L0>
+__global__ void __launch_bounds__(NT) img_kernel(const __grid_constant__ LevelArgs a) {
+  extern __shared__ __align__(16) uint8_t smem_raw[];
+  ImgSmem& S = *reinterpret_cast<ImgSmem*>(smem_raw);
+  const int x0 = blockIdx.x * TW, y0 = blockIdx.y * TH, k = blockIdx.z;
+  for (int i = threadIdx.x; i < GH * GW; i += NT) {
+    const int X = x0 - 4 + i % GW, Y = y0 - 4 + i / GW;
+    float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (X >= 0 && Y >= 0 && X < a.wl && Y < a.hl) {
+      const int64_t o = (int64_t)Y * a.pitch_l + X;
+      if constexpr (L0) {
+        const uint32_t q = a.in0[k].rgba[o];
+        v = make_float4(chf(q, 0), chf(q, 1), chf(q, 2), px_alpha(q) > 0 ? 1.0f : 0.0f);
+      } else {
+        const LevelPlanes& in = a.in[k];
+        const T* g = (const T*)in.g;
+        v = make_float4(ldv<T>(g, o), ldv<T>(g, in.plane + o), ldv<T>(g, 2 * in.plane + o), in.s[o] ? 1.0f : 0.0f);
+      }
+    }
+    S.gs[i] = v;
+  }
+  __syncthreads();
+  reduce_image_step(S, a, x0, y0);
+  store_next_image<T>(S, a, x0, y0, k);
+  float unused[PPT][3];
+  expand_blend_step<true>(S, a, x0, y0, unused, a.lap[k]);
+}
+
+// L0: level 0, whose blend over all frames blend0_kernel does; this kernel
+// then only reduces the masks (one frame per CTA).
+template <typename T, bool L0>
+__global__ void __launch_bounds__(NT) mask_kernel(const __grid_constant__ LevelArgs a) {
+  extern __shared__ __align__(16) uint8_t smem_raw[];
+  MaskSmem& S = *reinterpret_cast<MaskSmem*>(smem_raw);
+  const int x0 = blockIdx.x * TW, y0 = blockIdx.y * TH;
+  load_mask_support(S, a, x0, y0);
+  float acc[PPT][3];
+  const bool fpar = L0 || a.frame_parallel;
+  const int kb = fpar ? (int)blockIdx.z : 0, ke = fpar ? kb + 1 : a.K;
+  if constexpr (L0) {
+  } else if (a.frame_parallel) {
+#pragma unroll
+    for (int i = 0; i < PPT; ++i) acc[i][0] = acc[i][1] = acc[i][2] = 0.0f;
+  } else {
+    load_acc(a, x0, y0, acc);
+  }
+  for (int k = kb; k < ke; ++k) {
+    for (int i = threadIdx.x; i < MH * MW; i += NT) {
+      const int X = x0 - 2 + i % MW, Y = y0 - 2 + i / MW;
+      float m = 0.0f;
+      if (X >= 0 && Y >= 0 && X < a.wl && Y < a.hl) {
+        const int64_t o = (int64_t)Y * a.pitch_l + X;
+        if constexpr (L0) {
+          m = a.in0[k].w[o];  // normalised by blend0_kernel
+        } else {
+          m = ldv<T>((const T*)a.in[k].m, o);
+        }
+      }
+      S.m[i] = m;
+    }
+    __syncthreads();
+    reduce_mask_step(S);
+    store_next_mask<T>(S, a, x0, y0, k);
+    if constexpr (L0) continue;
+    const float* lap = a.lap[k];
+#pragma unroll
+    for (int i = 0; i < PPT; ++i) {
+      const int p = acc_pixel(i);
+      const int xx = p % TW, yy = p / TW;
+      const int X = x0 + xx, Y = y0 + yy;
+      if (X >= a.wl || Y >= a.hl) continue;
+      const int64_t o = (int64_t)Y * a.pitch_l + X;
+      const float m = S.m[(yy + 2) * MW + (xx + 2)];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) acc[i][c] = __fadd_rn(acc[i][c], __fmul_rn(lap[c * a.acc_plane_l + o], m));
+    }
+    __syncthreads();
+  }
+  if constexpr (L0) return;
+  if (a.frame_parallel) {
+#pragma unroll
+    for (int i = 0; i < PPT; ++i) {
+      const int p = acc_pixel(i);
+      const int X = x0 + p % TW, Y = y0 + p / TW;
+      if (X < a.wl && Y < a.hl) {
+        const int64_t o = (int64_t)Y * a.pitch_l + X;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) a.contrib[(int64_t)(kb * 3 + c) * a.acc_plane_l + o] = acc[i][c];
+      }
+    }
+  } else {
+    store_acc(a, x0, y0, acc);
+  }
+}
+
+// Level-0 blend of a whole stack in frame order, one pixel per thread:
+// acc = sum over frames of lap_k * (w_k / weight sum) (1 / N where the sum
+// is <= 1e-12), the same products and sums the per-batch kernels form.
+// The normalised mask replaces each frame's weight in place (the level-0
+// mask REDUCE then reads it without dividing again).
+__global__ void blend0_kernel(float* acc, int64_t plane, int64_t pitch, int w, int h, const float* norm,
+                              const float* const* lap, float* const* wgt, int frames, float inv_count) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (int64_t)w * h) return;
+  const int64_t o = (i / w) * pitch + i % w;
+  const float nv = norm[o];
+  float a0 = 0.0f, a1 = 0.0f, a2 = 0.0f;
+  constexpr int U = 4;  // frames whose loads are issued together
+  for (int k0 = 0; k0 < frames; k0 += U) {
+    float l0[U], l1[U], l2[U], wv[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      if (k0 + u < frames) {
+        const float* lk = lap[k0 + u];
+        l0[u] = __ldg(lk + o);
+        l1[u] = __ldg(lk + plane + o);
+        l2[u] = __ldg(lk + 2 * plane + o);
+        wv[u] = wgt[k0 + u][o];
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      if (k0 + u < frames) {
+        const float m = nv > 1e-12f ? __fdiv_rn(wv[u], nv) : inv_count;
+        wgt[k0 + u][o] = m;
+        a0 = __fadd_rn(a0, __fmul_rn(l0[u], m));
+        a1 = __fadd_rn(a1, __fmul_rn(l1[u], m));
+        a2 = __fadd_rn(a2, __fmul_rn(l2[u], m));
+      }
+    }
+  }
+  acc[o] = a0;
+  acc[plane + o] = a1;
+  acc[2 * plane + o] = a2;
+}
+
+cudaError_t launch_blend0(float* acc, int64_t plane, int64_t pitch, int w, int h, const float* norm,
+                          const float* const* lap, float* const* wgt, int frames, float inv_count,
+                          cudaStream_t s) {
+  const int64_t n = (int64_t)w * h;
+  blend0_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(acc, plane, pitch, w, h, norm, lap, wgt, frames,
+                                                           inv_count);
+  return cudaGetLastError();
+}
+
+template <template <typename, bool> class KER, bool L0>
+static cudaError_t launch_split(const LevelArgs& a, int storage, cudaStream_t s, bool* cfg, bool img) {
+  dim3 grid((a.wl + TW - 1) / TW, (a.hl + TH - 1) / TH, (img || L0 || a.frame_parallel) ? a.K : 1);
+  const size_t sm = img ? sizeof(ImgSmem) : sizeof(MaskSmem);
+  cudaError_t e;
+  switch (storage) {
+    case FS_STORAGE_F32:
+      if ((e = configure(KER<float, L0>::kernel, sm, &cfg[0])) != cudaSuccess) return e;
+      KER<float, L0>::kernel<<<grid, NT, sm, s>>>(a);
+      break;
+    case FS_STORAGE_F16:
+      if ((e = configure(KER<__half, L0>::kernel, sm, &cfg[1])) != cudaSuccess) return e;
+      KER<__half, L0>::kernel<<<grid, NT, sm, s>>>(a);
+      break;
+    case FS_STORAGE_BF16:
+      if ((e = configure(KER<__nv_bfloat16, L0>::kernel, sm, &cfg[2])) != cudaSuccess) return e;
+      KER<__nv_bfloat16, L0>::kernel<<<grid, NT, sm, s>>>(a);
+      break;
+    default:
+      return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+template <typename T, bool L0> struct ImgK {
+  static constexpr auto kernel = img_kernel<T, L0>;
+};
+template <typename T, bool L0> struct MaskK {
+  static constexpr auto kernel = mask_kernel<T, L0>;
+};
+
+cudaError_t launch_img_level(const LevelArgs& a, int storage, cudaStream_t s) {
+  static bool cfg0[3] = {false, false, false}, cfg1[3] = {false, false, false};
+  return a.level == 0 ? launch_split<ImgK, true>(a, storage, s, cfg0, true)
+                      : launch_split<ImgK, false>(a, storage, s, cfg1, true);
+}
+
+cudaError_t launch_mask_level(const LevelArgs& a, int storage, cudaStream_t s) {
+  static bool cfg0[3] = {false, false, false}, cfg1[3] = {false, false, false};
+  return a.level == 0 ? launch_split<MaskK, true>(a, storage, s, cfg0, false)
+                      : launch_split<MaskK, false>(a, storage, s, cfg1, false);
 }
 
 __global__ void sum_contrib_kernel(float* acc, int64_t plane, int64_t pitch, int w, int h, const float* contrib,

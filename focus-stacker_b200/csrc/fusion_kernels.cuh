@@ -80,6 +80,11 @@ struct LevelArgs {
   int32_t frame_parallel;
   float* contrib;
   float* contrib_top;
+  // split pyramid (launch_img_level / launch_mask_level): frame k's
+  // Laplacian planes at level l (3 planes of acc_plane_l floats) and its top
+  // Gaussian (3 planes of acc_plane_n floats, written when l + 1 is the top)
+  float* lap[kMaxBatch];
+  float* gtop[kMaxBatch];
 };
 
 struct CollapseArgs {
@@ -117,6 +122,22 @@ cudaError_t launch_remap_weights(const RemapWeightArgs& a, int border, cudaStrea
 cudaError_t launch_level0(const LevelArgs& a, int storage, cudaStream_t s);
 cudaError_t launch_level(const LevelArgs& a, int storage, cudaStream_t s);
 cudaError_t launch_collapse(const CollapseArgs& a, cudaStream_t s);
+// Split pyramid: the image half of a level step for the batch's frames, one
+// frame per CTA (grid.z = K): Gaussian REDUCE to level l + 1 (slots out[k],
+// or gtop[k] at the top) and the Laplacian of level l into lap[k]; level 0
+// reads the remapped RGBA planes in0[k].rgba.
+cudaError_t launch_img_level(const LevelArgs& a, int storage, cudaStream_t s);
+// The mask half: normalised mask (level 0 from in0[k].w and the weight sum),
+// its REDUCE to level l + 1 (out[k].m) and acc_l += lap[k] * mask in frame
+// order (frame-parallel with contributions when a.frame_parallel).
+cudaError_t launch_mask_level(const LevelArgs& a, int storage, cudaStream_t s);
+// Level-0 blend of all frames of a stack (device tables of each frame's
+// level-0 Laplacian and weight planes), written over acc; each weight plane
+// is replaced by the frame's normalised mask.  The level-0 launch of
+// launch_mask_level then reads those masks.
+cudaError_t launch_blend0(float* acc, int64_t plane, int64_t pitch, int w, int h, const float* norm,
+                          const float* const* lap, float* const* wgt, int frames, float inv_count,
+                          cudaStream_t s);
 // acc[c] += contrib[k][c] for k = 0 .. K-1 in order (w x h level, plane stride `plane`).
 cudaError_t launch_sum_contrib(float* acc, int64_t plane, int64_t pitch, int w, int h, const float* contrib, int K,
                                cudaStream_t s);

@@ -241,16 +241,16 @@ def test_refetch_path_matches_resident(torch, ctx):
     frames, poses = synth_stack(torch, ctx, W, H, F, seed=8)
     roi = fsb.compute_common_overlap_roi([True] * F, [W] * F, [H] * F, poses)
     ref, _ = gpu_fuse(ctx, torch, frames, poses, roi, k=2)
-    # a budget that fits the stack state but not every frame copy
-    ctx.trim()
-    before = ctx.device_bytes()
-    probe = fsb.PyramidContrastStack(ctx, W, H, F, roi=roi, frames_per_batch=2)
-    n0 = (roi.width + 31) // 32 * 32 * roi.height
-    state = ctx.device_bytes() - before - F * n0 * 8  # without the per-frame pass-1 planes
-    probe.close()
-    ctx.trim()
-    # per-batch planes for K = 2 frames and two batches of staging buffers
-    small = fsb.Context(0, hbm_budget_bytes=state + 2 * n0 * 8 + 4 * W * H * 3 + 4096)
+    # a budget that fits the stack in the refetch mode only
+    b = fsb.stack_footprint(fsb.stack_desc(W, H, F, roi, frames_per_batch=2), 1 << 50)[0]
+    while True:
+        b2, mode, ok = fsb.stack_footprint(fsb.stack_desc(W, H, F, roi, frames_per_batch=2), b - 1)
+        if not ok:
+            break
+        b = b2
+        if mode == "refetch":
+            break
+    small = fsb.Context(0, hbm_budget_bytes=b)
     st = fsb.PyramidContrastStack(small, W, H, F, roi=roi, frames_per_batch=2)
     assert st.pass2_mode == "refetch"
     for f, p in zip(frames, poses):
@@ -269,44 +269,35 @@ def test_refetch_path_matches_resident(torch, ctx):
 
 
 def test_pass2_modes_give_identical_results(torch, ctx):
-    # cache (pass-1 planes kept), resident (frames kept, remapped again) and
-    # refetch (frames fetched again) must produce the same bytes
+    # laps (pass 1 builds the Laplacians), cache (pass-1 planes kept),
+    # resident (frames kept, remapped again) and refetch (frames fetched
+    # again) must produce the same bytes; each budget is the footprint of its
+    # mode, the largest the stack picks there
     W, H, F = 240, 160, 8
     frames, poses = synth_stack(torch, ctx, W, H, F, seed=12)
     roi = fsb.compute_common_overlap_roi([True] * F, [W] * F, [H] * F, poses)
+    d = fsb.stack_desc(W, H, F, roi, frames_per_batch=3)
+    budgets = {}
+    avail = 1 << 50
+    while True:
+        b, mode, ok = fsb.stack_footprint(d, avail)
+        if not ok:
+            break
+        budgets.setdefault(mode, b)
+        avail = b - 1
+    assert set(budgets) == {"laps", "cache", "resident", "refetch"}
     results = {}
-    ctx.trim()
-    before = ctx.device_bytes()
-    probe = fsb.PyramidContrastStack(ctx, W, H, F, roi=roi, frames_per_batch=3)
-    assert probe.pass2_mode == "cache"
-    probe.close()
-    ctx.trim()
-    n0 = (roi.width + 31) // 32 * 32 * roi.height
-    frame_b = (W * 3 + 15) // 16 * 16 * H
-    for budget_extra, want in ((None, "cache"), ("resident", "resident"), ("refetch", "refetch")):
-        if budget_extra is None:
-            c = ctx
-        else:
-            # stack state without the per-frame planes: measure it with a tiny stack of the same geometry
-            c = fsb.Context(0, hbm_budget_bytes=1 << 40)
-            st0 = fsb.PyramidContrastStack(c, W, H, F, roi=roi, frames_per_batch=3)
-            state = c.device_bytes() - F * n0 * 8
-            st0.close()
-            c.close()
-            # resident: K = 3 batch planes + every frame; refetch: K planes + two batches of staging
-            extra = 3 * n0 * 8 + F * frame_b + 3 * frame_b + 4096 if want == "resident" else 3 * n0 * 8 + 6 * frame_b + 4096
-            c = fsb.Context(0, hbm_budget_bytes=state + extra)
+    for want, budget in budgets.items():
+        c = fsb.Context(0, hbm_budget_bytes=budget)
         st = fsb.PyramidContrastStack(c, W, H, F, roi=roi, frames_per_batch=3)
         assert st.pass2_mode == want
         for f, p in zip(frames, poses):
             st.add_frame(f, p)
         results[want] = st.finish(refetch=lambda i: frames[i])
         st.close()
-        if c is not ctx:
-            c.close()
-    assert np.array_equal(results["cache"], results["resident"])
-    assert np.array_equal(results["cache"], results["refetch"])
-
+        c.close()
+    for m in ("cache", "resident", "refetch"):
+        assert np.array_equal(results["laps"], results[m]), m
 
 def test_stack_errors(torch, ctx):
     W, H = 64, 48

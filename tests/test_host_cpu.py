@@ -187,8 +187,10 @@ def test_clamped_expand_closed_form_is_bitwise_the_reference(sw, sh, dw, dh):
 # ------------------------------------------------------------ serving (host)
 def test_stack_footprint_modes_follow_the_budget():
     d = fsb.stack_desc(7952, 5304, 30, fsb.Rect(82, 63, 7872, 5243))
-    cache, m_cache, ok = fsb.stack_footprint(d, 1 << 50)
-    assert m_cache == "cache" and ok
+    laps, m_laps, ok = fsb.stack_footprint(d, 1 << 50)
+    assert m_laps == "laps" and ok
+    cache, m_cache, ok = fsb.stack_footprint(d, laps - 1)
+    assert m_cache == "cache" and ok and cache < laps
     resident, m_res, ok = fsb.stack_footprint(d, cache - 1)
     assert m_res == "resident" and ok and resident < cache
     refetch, m_ref, ok = fsb.stack_footprint(d, resident - 1)
@@ -196,11 +198,11 @@ def test_stack_footprint_modes_follow_the_budget():
     b, _, ok = fsb.stack_footprint(d, refetch - 1)
     assert not ok and b == refetch
     # device-resident frames need no upload staging
-    dev_cache, _, _ = fsb.stack_footprint(d, 1 << 50, host_frames=False)
-    assert dev_cache < cache
+    dev_laps, _, _ = fsb.stack_footprint(d, 1 << 50, host_frames=False)
+    assert dev_laps < laps
     # FP16 level storage shrinks the level slots
     d16 = fsb.stack_desc(7952, 5304, 30, fsb.Rect(82, 63, 7872, 5243), level_storage=fsb.STORAGE_F16)
-    assert fsb.stack_footprint(d16, 1 << 50)[0] < cache
+    assert fsb.stack_footprint(d16, 1 << 50)[0] < laps
 
 
 def test_stack_footprint_rejects_bad_desc():
@@ -227,7 +229,7 @@ class _FakeCtx:
 
 
 def test_server_admission_respects_the_budget():
-    srv = fsb.serving.StackServer(hbm_budget_bytes=40 * 10**9, workers=3, context_factory=_FakeCtx,
+    srv = fsb.serving.StackServer(hbm_budget_bytes=80 * 10**9, workers=3, context_factory=_FakeCtx,
                                   max_stack_fraction=1.0)
     big = fsb.serving.StackRequest(0, 0.0, 7952, 5304, 30)
     roi = fsb.Rect(0, 0, 7952, 5304)
