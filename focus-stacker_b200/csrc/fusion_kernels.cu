@@ -962,21 +962,40 @@ __global__ void __launch_bounds__(NT) img_kernel(const __grid_constant__ LevelAr
   extern __shared__ __align__(16) uint8_t smem_raw[];
   ImgSmem& S = *reinterpret_cast<ImgSmem*>(smem_raw);
   const int x0 = blockIdx.x * TW, y0 = blockIdx.y * TH, k = blockIdx.z;
-  for (int i = threadIdx.x; i < GH * GW; i += NT) {
-    const int X = x0 - 4 + i % GW, Y = y0 - 4 + i / GW;
-    float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-    if (X >= 0 && Y >= 0 && X < a.wl && Y < a.hl) {
-      const int64_t o = (int64_t)Y * a.pitch_l + X;
-      if constexpr (L0) {
-        const uint32_t q = a.in0[k].rgba[o];
-        v = make_float4(chf(q, 0), chf(q, 1), chf(q, 2), px_alpha(q) > 0 ? 1.0f : 0.0f);
-      } else {
-        const LevelPlanes& in = a.in[k];
-        const T* g = (const T*)in.g;
-        v = make_float4(ldv<T>(g, o), ldv<T>(g, in.plane + o), ldv<T>(g, 2 * in.plane + o), in.s[o] ? 1.0f : 0.0f);
+  // region loads issued together (all in flight before the first store)
+  constexpr int NI = (GH * GW + NT - 1) / NT, HALF = (NI + 1) / 2;
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    float4 v[HALF];
+#pragma unroll
+    for (int j = 0; j < HALF; ++j) {
+      const int i = threadIdx.x + (h * HALF + j) * NT;
+      const int X = x0 - 4 + i % GW, Y = y0 - 4 + i / GW;
+      v[j] = make_float4(0.f, 0.f, 0.f, 0.f);
+      if (i < GH * GW && X >= 0 && Y >= 0 && X < a.wl && Y < a.hl) {
+        const int64_t o = (int64_t)Y * a.pitch_l + X;
+        if constexpr (L0) {
+          const uint32_t q = __ldg(a.in0[k].rgba + o);
+          v[j] = make_float4(__uint_as_float(q), 0.f, 0.f, 0.f);
+        } else {
+          const LevelPlanes& in = a.in[k];
+          const T* g = (const T*)in.g;
+          v[j] = make_float4(ldv<T>(g, o), ldv<T>(g, in.plane + o), ldv<T>(g, 2 * in.plane + o),
+                             in.s[o] ? 1.0f : 0.0f);
+        }
       }
     }
-    S.gs[i] = v;
+#pragma unroll
+    for (int j = 0; j < HALF; ++j) {
+      const int i = threadIdx.x + (h * HALF + j) * NT;
+      if (i >= GH * GW) continue;
+      if constexpr (L0) {
+        const uint32_t q = __float_as_uint(v[j].x);
+        S.gs[i] = make_float4(chf(q, 0), chf(q, 1), chf(q, 2), px_alpha(q) > 0 ? 1.0f : 0.0f);
+      } else {
+        S.gs[i] = v[j];
+      }
+    }
   }
   __syncthreads();
   reduce_image_step(S, a, x0, y0);
@@ -1004,18 +1023,30 @@ __global__ void __launch_bounds__(NT) mask_kernel(const __grid_constant__ LevelA
     load_acc(a, x0, y0, acc);
   }
   for (int k = kb; k < ke; ++k) {
-    for (int i = threadIdx.x; i < MH * MW; i += NT) {
-      const int X = x0 - 2 + i % MW, Y = y0 - 2 + i / MW;
-      float m = 0.0f;
-      if (X >= 0 && Y >= 0 && X < a.wl && Y < a.hl) {
-        const int64_t o = (int64_t)Y * a.pitch_l + X;
-        if constexpr (L0) {
-          m = a.in0[k].w[o];  // normalised by blend0_kernel
-        } else {
-          m = ldv<T>((const T*)a.in[k].m, o);
+    // loads issued together (level >= 1 in two halves, for registers)
+    constexpr int NM = (MH * MW + NT - 1) / NT, NH2 = L0 ? 1 : 2, HM = (NM + NH2 - 1) / NH2;
+#pragma unroll
+    for (int h = 0; h < NH2; ++h) {
+      float mv[HM];
+#pragma unroll
+      for (int j = 0; j < HM; ++j) {
+        const int i = threadIdx.x + (h * HM + j) * NT;
+        const int X = x0 - 2 + i % MW, Y = y0 - 2 + i / MW;
+        mv[j] = 0.0f;
+        if (i < MH * MW && X >= 0 && Y >= 0 && X < a.wl && Y < a.hl) {
+          const int64_t o = (int64_t)Y * a.pitch_l + X;
+          if constexpr (L0) {
+            mv[j] = a.in0[k].w[o];  // normalised by blend0_kernel
+          } else {
+            mv[j] = ldv<T>((const T*)a.in[k].m, o);
+          }
         }
       }
-      S.m[i] = m;
+#pragma unroll
+      for (int j = 0; j < HM; ++j) {
+        const int i = threadIdx.x + (h * HM + j) * NT;
+        if (i < MH * MW) S.m[i] = mv[j];
+      }
     }
     __syncthreads();
     reduce_mask_step(S);
