@@ -329,10 +329,14 @@ constexpr int GW = TW + 7, GH = TH + 7;          // G region
 constexpr int MW = TW + 3, MH = TH + 3;          // M region
 constexpr int NW = TW / 2 + 2, NH = TH / 2 + 2;  // level l+1 tile + halo
 constexpr int TW1 = TW / 2, TH1 = TH / 2;
-constexpr int kTmpFloats = (GH * NW * 4 > NH * TW * 3) ? GH * NW * 4 : NH * TW * 3;
+// Row strides of the REDUCE temporaries, padded so that lanes on
+// consecutive rows hit distinct shared-memory banks.
+constexpr int THS = NW + 1;   // horizontal image sums (float4)
+constexpr int TMS = TW1 + 1;  // horizontal mask sums (float2)
+constexpr int kTmpFloats = (GH * THS * 4 > NH * TW * 3) ? GH * THS * 4 : NH * TW * 3;
 
 struct __align__(16) LevelSmem {
-  static constexpr int kTmOffset = GH * NW * 4 - MH * TW1 * 2;  // mask REDUCE rows at the end of tmp
+  static constexpr int kTmOffset = kTmpFloats - MH * TMS * 2;  // mask REDUCE rows at the end of tmp
   float4 gs[GH * GW];       // level-l Gaussian (r, g, b) and support (0 / 1)
   float tmp[kTmpFloats];    // reduce / expand temporaries
   float ng[3][NH * NW];     // level-(l+1) Gaussian (zero outside the level)
@@ -435,12 +439,12 @@ __device__ __forceinline__ float expand_v1(const float* h, int stride, const Row
 template <class SM>
 __device__ void reduce_image_step(SM& S, const LevelArgs& a, int x0, int y0) {
   const int x1 = x0 >> 1, y1 = y0 >> 1;
-  float4* th = reinterpret_cast<float4*>(S.tmp);  // [GH][NW]
+  float4* th = reinterpret_cast<float4*>(S.tmp);  // [GH][THS]
   // horizontal, two neighbouring outputs per thread (they share 3 of their
   // 5 taps); each output sums its taps in the same order as alone
   static_assert(NW % 2 == 0 && NH % 2 == 0 && TW1 % 2 == 0 && TH1 % 2 == 0, "output pairs");
   for (int i = threadIdx.x; i < GH * (NW / 2); i += NT) {
-    const int ry = i / (NW / 2), jj = 2 * (i % (NW / 2));
+    const int ry = i % GH, jj = 2 * (i / GH);  // lanes on consecutive rows
     const float4* row = S.gs + ry * GW + 2 * jj;  // G region column of tap 0: 2j - 2 - (x0 - 4)
     float4 t[7];
 #pragma unroll
@@ -457,16 +461,16 @@ __device__ void reduce_image_step(SM& S, const LevelArgs& a, int x0, int y0) {
         v2 = fmaf(w, tk.z, v2);
         ws += w;
       }
-      th[ry * NW + jj + h] = make_float4(v0, v1, v2, ws);
+      th[ry * THS + jj + h] = make_float4(v0, v1, v2, ws);
     }
   }
   __syncthreads();
   for (int i = threadIdx.x; i < (NH / 2) * NW; i += NT) {
     const int ii = 2 * (i / NW), jj = i % NW;
-    const float4* col = th + (2 * ii) * NW + jj;  // G region row of tap 0: 2 yi - 2 - (y0 - 4)
+    const float4* col = th + (2 * ii) * THS + jj;  // G region row of tap 0: 2 yi - 2 - (y0 - 4)
     float4 t[7];
 #pragma unroll
-    for (int u = 0; u < 7; ++u) t[u] = col[u * NW];
+    for (int u = 0; u < 7; ++u) t[u] = col[u * THS];
     const int xj = x1 - 1 + jj;
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
@@ -496,9 +500,9 @@ __device__ void reduce_image_step(SM& S, const LevelArgs& a, int x0, int y0) {
 // Mask half of the REDUCE (level-l mask with the level-l mask support).
 template <class SM>
 __device__ void reduce_mask_step(SM& S) {
-  float2* tm = reinterpret_cast<float2*>(S.tmp + SM::kTmOffset);  // [MH][TW1]
+  float2* tm = reinterpret_cast<float2*>(S.tmp + SM::kTmOffset);  // [MH][TMS]
   for (int i = threadIdx.x; i < MH * (TW1 / 2); i += NT) {
-    const int ry = i / (TW1 / 2), jj = 2 * (i % (TW1 / 2));
+    const int ry = i % MH, jj = 2 * (i / MH);  // lanes on consecutive rows
     const int base = ry * MW + 2 * jj;  // M region column of tap 0: 2j - 2 - (x0 - 2)
     float mv[7], sw[7];
 #pragma unroll
@@ -515,7 +519,7 @@ __device__ void reduce_mask_step(SM& S) {
         v = fmaf(w, mv[2 * h + kx], v);
         ws += w;
       }
-      tm[ry * TW1 + jj + h] = make_float2(v, ws);
+      tm[ry * TMS + jj + h] = make_float2(v, ws);
     }
   }
   __syncthreads();
@@ -523,7 +527,7 @@ __device__ void reduce_mask_step(SM& S) {
     const int ii = 2 * (i / TW1), jj = i % TW1;
     float2 t[7];
 #pragma unroll
-    for (int u = 0; u < 7; ++u) t[u] = tm[(2 * ii + u) * TW1 + jj];  // M region row of tap 0: 2 yi - 2 - (y0 - 2)
+    for (int u = 0; u < 7; ++u) t[u] = tm[(2 * ii + u) * TMS + jj];  // M region row of tap 0: 2 yi - 2 - (y0 - 2)
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
       float v = 0.f, ws = 0.f;
@@ -900,7 +904,7 @@ static_assert(offsetof(ImgSmem, tmp) % 16 == 0, "tmp is accessed as float4");
 
 struct __align__(16) MaskSmem {
   static constexpr int kTmOffset = 0;
-  float tmp[MH * TW1 * 2];
+  float tmp[MH * TMS * 2];
   float nm[TH1 * TW1];
   float m[MH * MW];
   uint8_t sm[MH * MW];
