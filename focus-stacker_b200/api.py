@@ -299,6 +299,14 @@ def stack_desc(src_width: int, src_height: int, frame_count: int, roi: Optional[
     return d
 
 
+def stack_mode_bytes(desc: _lib.FsStackDesc, mode: str, host_frames: bool = True) -> int:
+    """Device bytes of a stack in pass-2 mode `mode`; allocates nothing."""
+    b = ctypes.c_uint64()
+    _check(L().fs_stack_mode_bytes(ctypes.byref(desc), PASS2_MODES.index(mode), 1 if host_frames else 0,
+                                   ctypes.byref(b)))
+    return int(b.value)
+
+
 def stack_footprint(desc: _lib.FsStackDesc, available_bytes: int, host_frames: bool = True):
     """(device bytes, pass-2 mode, fits) of a stack when `available_bytes` of
     budget are free; allocates nothing."""
@@ -318,13 +326,16 @@ class PyramidContrastStack:
 
     def __init__(self, ctx: Context, src_width: int, src_height: int, frame_count: int, roi: Optional[Rect] = None,
                  channels: int = 3, contrast_window: int = 5, aligned: bool = False, frames_per_batch: int = 0,
-                 level_storage: int = 0):
+                 level_storage: int = 0, pass2_mode: Optional[str] = None):
+        """pass2_mode: None picks the mode from the context's budget; "cache",
+        "resident", "refetch" or "laps" imposes one."""
         self.ctx = ctx
         d = stack_desc(src_width, src_height, frame_count, roi, channels, contrast_window, aligned, frames_per_batch,
                        level_storage)
         self.desc = d
         h = ctypes.c_void_p()
-        _check(L().fs_stack_begin(ctx.handle, ctypes.byref(d), ctypes.byref(h)), ctx.handle)
+        mode = -1 if pass2_mode is None else PASS2_MODES.index(pass2_mode)
+        _check(L().fs_stack_begin_mode(ctx.handle, ctypes.byref(d), mode, ctypes.byref(h)), ctx.handle)
         self.handle = h
         w, hh = ctypes.c_uint32(), ctypes.c_uint32()
         L().fs_stack_output_size(h, ctypes.byref(w), ctypes.byref(hh))

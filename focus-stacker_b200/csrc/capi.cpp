@@ -855,6 +855,13 @@ static int begin_impl(fs_ctx* ctx, const fs_stack_desc* desc, fs_stack** out, in
 
 int fs_stack_begin(fs_ctx* ctx, const fs_stack_desc* desc, fs_stack** out) { return begin_impl(ctx, desc, out, -1); }
 
+int fs_stack_begin_mode(fs_ctx* ctx, const fs_stack_desc* desc, int pass2_mode, fs_stack** out) {
+  if (pass2_mode < -1 || pass2_mode > 3) return set_err(ctx, FS_ERR_INVALID, "unknown pass-2 mode");
+  if (desc && pass2_mode == P2_LAPS && plan_stack(*desc).laps_frame == 0)
+    return set_err(ctx, FS_ERR_UNSUPPORTED, "the laps mode needs at least 3 pyramid levels");
+  return begin_impl(ctx, desc, out, pass2_mode);
+}
+
 static int add_frame_impl(fs_stack* s, const void* pixels, size_t row_stride, const fs_pose* pose, bool device) {
   if (!s || !pixels) return FS_ERR_INVALID;
   if (!s->ctx) return FS_ERR_STATE;  // its context was destroyed
@@ -1088,6 +1095,16 @@ static int finish_impl(fs_stack* s, fs_frame_fetch_cb refetch, void* user, void*
 }
 
 int fs_stack_pass2_mode(const fs_stack* s) { return s ? (int)s->mode : -1; }
+
+int fs_stack_mode_bytes(const fs_stack_desc* desc, int pass2_mode, int host_frames, uint64_t* bytes) {
+  if (!desc || !bytes || pass2_mode < 0 || pass2_mode > 3) return FS_ERR_INVALID;
+  int code = FS_OK;
+  if (check_desc(*desc, &code)) return code;
+  const StackPlan plan = plan_stack(*desc);
+  if (pass2_mode == P2_LAPS && plan.laps_frame == 0) return FS_ERR_UNSUPPORTED;
+  *bytes = plan_bytes(plan, desc->frame_count, (Pass2Mode)pass2_mode, host_frames != 0);
+  return FS_OK;
+}
 
 int fs_stack_footprint(const fs_stack_desc* desc, uint64_t available_bytes, int host_frames, uint64_t* bytes,
                        int* mode) {

@@ -7,11 +7,11 @@ Admission is the per-request form of the reference's memory budget
 (--memory-fraction, src/memory_budget.zig:3-53): a request is admitted when
 the device bytes its stack will hold (fs_stack_footprint, computed without
 allocating) fit in the budget left by the stacks in flight.  The stack's
-pass-2 mode is the best one that fits both that remainder and a cap on one
-stack's share of the budget (keeping the pass-1 planes, the reference's
-cached path, else keeping the frames); requests wait in arrival order
-otherwise.  Each worker owns a context (its own streams), so stacks in flight
-overlap on the device; memory comes from the device's shared stream-ordered
+pass-2 mode is the first of `modes` (memory-lean first: keeping the pass-1
+planes, the reference's cached path, else keeping the frames) that fits both
+that remainder and a cap on one stack's share of the budget; requests wait
+in arrival order otherwise.  Each worker owns a context (its own streams),
+so stacks in flight overlap on the device; memory comes from the device's shared stream-ordered
 pool, and a worker's context budget is set to the reservation of the stack it
 runs.
 
@@ -105,6 +105,7 @@ class _Worker:
         self.ctx = ctx
         self.busy = False
         self.reserved = 0  # footprint of the stack in flight
+        self.mode = None   # its pass-2 mode
         self.cached = 0    # upper bound of the memory its last stack left cached in the pool
 
 
@@ -116,11 +117,12 @@ class StackServer:
 
     def __init__(self, device: int = 0, hbm_budget_bytes: int = 120 * 10**9, workers: int = 4,
                  frames_per_batch: int = 0, context_factory=None, max_stack_fraction: float = 0.25,
-                 prewarm: bool = False):
+                 prewarm: bool = False, modes=("cache", "resident")):
         self.device = device
         self.budget = int(hbm_budget_bytes)
         self.frames_per_batch = frames_per_batch
         self.max_stack = int(self.budget * max_stack_fraction)
+        self.modes = tuple(modes)
         make = context_factory or (lambda: api.Context(device, hbm_budget_bytes=self.budget))
         self.workers = [_Worker(make()) for _ in range(workers)]
         if prewarm and self.workers:
@@ -149,13 +151,18 @@ class StackServer:
         w = idle[0]
         desc = api.stack_desc(req.width, req.height, req.frames, roi, level_storage=req.level_storage,
                               frames_per_batch=self.frames_per_batch)
-        # best mode once idle workers' cached memory is released; the
-        # footprint counts the upload staging ring as the stack's own mode
-        # choice does, so that both pick the same mode
+        # the first mode that fits once idle workers' cached memory is
+        # released (bytes with the upload staging ring; the stack is begun in
+        # exactly that mode)
         busy = sum(o.reserved for o in self.workers if o.busy)
         avail = min(max(0, self.budget - busy), self.max_stack)
-        nbytes, mode, fits = api.stack_footprint(desc, avail, host_frames=True)
-        if not fits or mode == "refetch":
+        mode, nbytes = None, 0
+        for m in self.modes:  # memory-lean modes first: more stacks in flight
+            b = api.stack_mode_bytes(desc, m, host_frames=True)
+            if b <= avail:
+                mode, nbytes = m, b
+                break
+        if mode is None:
             return None
         if nbytes > self.budget - self._in_use(w):
             for o in self.workers:
@@ -164,6 +171,7 @@ class StackServer:
                     o.cached = 0
         w.busy = True
         w.reserved = nbytes
+        w.mode = mode
         w.ctx.set_budget(max(nbytes, 1))
         return w, nbytes
 
@@ -189,7 +197,7 @@ class StackServer:
                 tb = now()
                 st = api.PyramidContrastStack(w.ctx, req.width, req.height, req.frames, roi=roi,
                                               level_storage=req.level_storage,
-                                              frames_per_batch=self.frames_per_batch)
+                                              frames_per_batch=self.frames_per_batch, pass2_mode=w.mode)
                 mode = st.pass2_mode
                 out = torch.empty((roi.height, roi.width, 3), dtype=torch.uint8, device=f"cuda:{self.device}")
                 t_begin = now() - tb

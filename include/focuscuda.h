@@ -210,6 +210,13 @@ int fs_stack_pass2_mode(const fs_stack* stack);
  * reference. */
 int fs_stack_footprint(const fs_stack_desc* desc, uint64_t available_bytes, int host_frames, uint64_t* bytes,
                        int* mode);
+/* Device bytes of a stack of `desc` in pass-2 mode pass2_mode (0 cache, 1
+ * resident, 2 refetch, 3 laps), and fs_stack_begin with that mode imposed
+ * (-1: chosen from the budget as fs_stack_begin does); for a caller that
+ * trades memory for speed itself (a serving loop keeps more stacks in flight
+ * with the cache mode than with laps).  Not part of the reference. */
+int fs_stack_mode_bytes(const fs_stack_desc* desc, int pass2_mode, int host_frames, uint64_t* bytes);
+int fs_stack_begin_mode(fs_ctx* ctx, const fs_stack_desc* desc, int pass2_mode, fs_stack** out);
 
 /* Output size of the stack (the ROI). */
 int fs_stack_output_size(const fs_stack* stack, uint32_t* width, uint32_t* height);

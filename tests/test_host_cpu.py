@@ -205,6 +205,15 @@ def test_stack_footprint_modes_follow_the_budget():
     assert fsb.stack_footprint(d16, 1 << 50)[0] < laps
 
 
+def test_mode_bytes_order():
+    d = fsb.stack_desc(7952, 5304, 30, fsb.Rect(82, 63, 7872, 5243))
+    b = {m: fsb.stack_mode_bytes(d, m) for m in ("laps", "cache", "resident", "refetch")}
+    assert b["laps"] > b["cache"] > b["resident"] > b["refetch"]
+    assert fsb.stack_footprint(d, b["cache"])[:2] == (b["cache"], "cache")
+    with pytest.raises(fsb.FocusCudaError):  # two levels only: no laps mode
+        fsb.stack_mode_bytes(fsb.stack_desc(2, 1, 2), "laps")
+
+
 def test_stack_footprint_rejects_bad_desc():
     with pytest.raises(fsb.FocusCudaError):
         fsb.stack_footprint(fsb.stack_desc(64, 48, 2, contrast_window=4), 1 << 40)
@@ -233,7 +242,7 @@ def test_server_admission_respects_the_budget():
                                   max_stack_fraction=1.0)
     big = fsb.serving.StackRequest(0, 0.0, 7952, 5304, 30)
     roi = fsb.Rect(0, 0, 7952, 5304)
-    need = fsb.stack_footprint(fsb.stack_desc(7952, 5304, 30, roi), 1 << 50)[0]
+    need = fsb.stack_mode_bytes(fsb.stack_desc(7952, 5304, 30, roi), "cache")
     w1, b1 = srv._try_admit(big, roi)
     assert b1 == need and w1.busy and w1.ctx.budget == need
     w2, b2 = srv._try_admit(fsb.serving.StackRequest(1, 0.0, 7952, 5304, 30), roi)
@@ -242,7 +251,7 @@ def test_server_admission_respects_the_budget():
     third = srv._try_admit(fsb.serving.StackRequest(2, 0.0, 7952, 5304, 30), roi)
     if third is not None:
         assert b1 + b2 + third[1] <= srv.budget
-    # memory cached by idle workers is released before a smaller mode is taken
+    # memory cached by idle workers is released before a leaner mode is taken
     srv2 = fsb.serving.StackServer(hbm_budget_bytes=need + 10**6, workers=2, context_factory=_FakeCtx,
                                    max_stack_fraction=1.0)
     srv2.workers[1].cached = 10**9
@@ -256,7 +265,7 @@ def test_server_caps_one_stacks_share_of_the_budget():
                                   max_stack_fraction=0.25)
     w, b = srv._try_admit(fsb.serving.StackRequest(0, 0.0, 7952, 5304, 30), roi)
     assert b <= 10 * 10**9
-    assert b < fsb.stack_footprint(fsb.stack_desc(7952, 5304, 30, roi), 1 << 50)[0]
+    assert b < fsb.stack_mode_bytes(fsb.stack_desc(7952, 5304, 30, roi), "cache")
 
 
 def test_poisson_stream_shape():
