@@ -206,6 +206,7 @@ struct fs_stack {
     int64_t pitch = 0;
     bool owned = false;
     bool resident = true;         // false: transient staging copy, pass 2 refetches it
+    int slot = -1;                // staging buffer of a transient copy
     fs_pose pose;
   };
   std::vector<Frame> frames;
@@ -215,7 +216,7 @@ struct fs_stack {
   size_t pass1_done = 0;          // frames whose pass 1 has been launched
   bool finished = false;
   cudaEvent_t copy_done = nullptr;
-  cudaEvent_t batch_done[2] = {nullptr, nullptr};  // pass 1 of the last two batches (staging reuse)
+  std::vector<cudaEvent_t> slot_done;  // per staging buffer: the remap that last read it
   float* base_out = nullptr;      // optional device buffer for the collapsed base (RGB f32)
   uint32_t fp_level = 0;          // first level run one frame per CTA (none: >= L - 1)
   float* contrib = nullptr;       // per-frame blend contributions of those levels
@@ -234,8 +235,9 @@ void detach_stack(fs_stack* s) {
   for (auto& a : s->allocs) dev_free(s->ctx, a.p, a.bytes);
   s->allocs.clear();
   if (s->copy_done) cudaEventDestroy(s->copy_done);
-  for (cudaEvent_t& ev : s->batch_done)
+  for (cudaEvent_t& ev : s->slot_done)
     if (ev) cudaEventDestroy(ev), ev = nullptr;
+  s->slot_done.clear();
   s->copy_done = nullptr;
   s->ctx = nullptr;
 }
@@ -342,19 +344,27 @@ int launch_image_pyramid(fs_stack* s, size_t begin, size_t end) {
   return FS_OK;
 }
 
-int launch_pass1_batch(fs_stack* s, size_t begin, size_t end) {
-  int rc = launch_remap_weights_batch(s, s->frames, begin, end, true);
-  if (rc == FS_OK && s->mode == P2_LAPS) rc = launch_image_pyramid(s, begin, end);
-  return rc;
-}
+// Pass 1 runs in batches of K frames as they arrive; the last frames of the
+// stack go in smaller batches (each of the last kTailFrames on arrival), so
+// that little pass-1 work is left once the last frame is in.
+constexpr size_t kTailFrames = 2;
 
 int run_pending_pass1(fs_stack* s, bool flush) {
-  while (s->frames.size() - s->pass1_done >= s->K || (flush && s->frames.size() > s->pass1_done)) {
+  for (;;) {
+    const size_t pending = s->frames.size() - s->pass1_done;
+    const size_t to_come = s->d.frame_count - s->frames.size();
+    if (!(pending >= s->K || (pending > 0 && (flush || to_come <= kTailFrames)))) break;
     size_t begin = s->pass1_done, end = std::min(s->frames.size(), begin + s->K);
-    int rc = launch_pass1_batch(s, begin, end);
+    int rc = launch_remap_weights_batch(s, s->frames, begin, end, true);
     if (rc != FS_OK) return rc;
-    cudaError_t e = cudaEventRecord(s->batch_done[(begin / s->K) % 2], s->ctx->stream);
-    if (e != cudaSuccess) return cuda_err(s->ctx, e, "pass-1 event");
+    // the staging buffers of these frames are free for reuse after this remap
+    for (size_t f = begin; f < end; ++f) {
+      const int slot = s->frames[f].slot;
+      if (slot < 0) continue;
+      cudaError_t e = cudaEventRecord(s->slot_done[slot], s->ctx->stream);
+      if (e != cudaSuccess) return cuda_err(s->ctx, e, "pass-1 event");
+    }
+    if (s->mode == P2_LAPS && (rc = launch_image_pyramid(s, begin, end)) != FS_OK) return rc;
     s->pass1_done = end;
   }
   return FS_OK;
@@ -847,8 +857,6 @@ static int begin_impl(fs_ctx* ctx, const fs_stack_desc* desc, fs_stack** out, in
     }
   }
   cudaEventCreateWithFlags(&s->copy_done, cudaEventDisableTiming);
-  cudaEventCreateWithFlags(&s->batch_done[0], cudaEventDisableTiming);
-  cudaEventCreateWithFlags(&s->batch_done[1], cudaEventDisableTiming);
   *out = s;
   return FS_OK;
 }
@@ -896,14 +904,18 @@ static int add_frame_impl(fs_stack* s, const void* pixels, size_t row_stride, co
         int rc = stack_alloc(s, s->frame_bytes, &p, ctx->copy);
         if (rc != FS_OK) return rc;
         s->staging.push_back((uint8_t*)p);
+        cudaEvent_t ev;
+        cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+        s->slot_done.push_back(ev);
       }
-      if (slot % s->K == 0 && s->frames.size() >= nslots) {
-        // pass 1 of the batch two back read these buffers: the upload waits for it
-        cudaError_t e = cudaStreamWaitEvent(ctx->copy, s->batch_done[(s->frames.size() / s->K) % 2], 0);
+      if (s->frames.size() >= nslots) {
+        // the remap of the frame 2K back read this buffer: the upload waits for it
+        cudaError_t e = cudaStreamWaitEvent(ctx->copy, s->slot_done[slot], 0);
         if (e != cudaSuccess) return cuda_err(ctx, e, "staging reuse");
       }
       buf = s->staging[slot];
       fr.resident = false;
+      fr.slot = (int)slot;
     }
     // one linear copy when the rows are packed alike (faster than a pitched copy)
     cudaError_t e = row_stride == (size_t)s->frame_pitch
