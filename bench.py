@@ -201,7 +201,7 @@ def algorithmic_bytes(roi_w, roi_h, frames, k, mode="cache", storage_bytes=4):
         for l in range(L - 1):
             img += 12 * A[l] + (3 * s + 1) * A[l + 1] + ((3 * s + 1) * A[l] if l >= 1 else 0)
         b["image"] = frames * img
-        b["blend0"] = frames * 16 * A[0] + 16 * A[0]
+        b["blend0"] = frames * 20 * A[0] + 16 * A[0]  # Laplacian 12 + weight 4 read, mask 4 written
         b["level0"] = frames * (4 * A[0] + s * l1) + batches * 5 * A[0]
         lv = 0
         for l in range(1, L - 1):
