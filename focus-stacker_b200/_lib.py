@@ -27,7 +27,8 @@ EXPORTED = (
     "fs_pose_default", "fs_compute_roi", "fs_inverse_map_points", "fs_forward_map_points", "fs_exact_expand_divisor",
     "fs_remap_frame", "fs_remap_frame_device",
     "fs_stack_begin", "fs_stack_add_frame", "fs_stack_add_frame_device", "fs_stack_finish",
-    "fs_stack_finish_device", "fs_stack_set_base_output", "fs_stack_pass2_mode", "fs_stack_footprint", "fs_stack_mode_bytes", "fs_stack_begin_mode", "fs_stack_output_size", "fs_stack_destroy", "fs_fuse_stack",
+    "fs_stack_finish_device", "fs_stack_set_base_output", "fs_stack_pass2_mode", "fs_stack_footprint", "fs_stack_mode_bytes", "fs_stack_begin_mode",
+    "fs_stack_set_frame_total", "fs_stack_end_pass1", "fs_stack_blend", "fs_stack_collapse", "fs_stack_buffer", "fs_stack_output_size", "fs_stack_destroy", "fs_fuse_stack",
     "fs_batch_create", "fs_batch_run", "fs_batch_stack_count", "fs_batch_pass2_mode", "fs_batch_uses_graph",
     "fs_batch_destroy",
     "fs_fuse_aligned_device_static", "fs_synth_frame_device", "fs_synth_pose",
@@ -117,6 +118,11 @@ def _bind(L):
     L.fs_stack_footprint.argtypes = [P(FsStackDesc), u64, i32, P(u64), P(i32)]
     L.fs_stack_mode_bytes.argtypes = [P(FsStackDesc), i32, i32, P(u64)]
     L.fs_stack_begin_mode.argtypes = [ctx, P(FsStackDesc), i32, P(vp)]
+    L.fs_stack_set_frame_total.argtypes = [vp, u32]
+    L.fs_stack_end_pass1.argtypes = [vp]
+    L.fs_stack_blend.argtypes = [vp, FETCH_CB, vp]
+    L.fs_stack_collapse.argtypes = [vp, vp, sz, i32]
+    L.fs_stack_buffer.argtypes = [vp, i32, u32, P(vp), P(u64), P(ctypes.c_int64), P(u32), P(u32)]
     L.fs_stack_destroy.argtypes = [vp]
     L.fs_fuse_stack.argtypes = [ctx, P(FsStackDesc), P(vp), P(sz), P(FsPose), vp, sz]
     L.fs_fuse_aligned_device_static.argtypes = [P(vp), P(sz), u32, u32, u32, u32, u32, vp, sz, vp,

@@ -279,6 +279,23 @@ def remap_rigid_image_device(ctx: Context, src, src_stride: int, width: int, hei
 
 # --------------------------------------------------------------------- fusion
 PASS2_MODES = ("cache", "resident", "refetch", "laps")
+BUFFER_WEIGHT_SUM, BUFFER_UNION, BUFFER_ACCUMULATOR = 0, 1, 2
+
+
+class DeviceBuffer:
+    """A device buffer of a stack, exposed through __cuda_array_interface__
+    (torch.as_tensor(buf, device="cuda") is a view, not a copy); `width` and
+    `height` give the valid region inside the pitched rows.  Keeps its stack
+    alive."""
+
+    def __init__(self, ptr: int, shape, typestr: str, width: int, height: int, owner):
+        self.ptr, self.shape, self.typestr = ptr, tuple(shape), typestr
+        self.width, self.height, self._owner = width, height, owner
+
+    @property
+    def __cuda_array_interface__(self):
+        return {"shape": self.shape, "typestr": self.typestr, "data": (self.ptr, False), "version": 2,
+                "strides": None}
 
 
 def stack_desc(src_width: int, src_height: int, frame_count: int, roi: Optional[Rect] = None, channels: int = 3,
@@ -380,6 +397,42 @@ class PyramidContrastStack:
     def finish_device(self, dst, dst_stride: int, refetch=None):
         cb = self._make_cb(refetch)
         _check(L().fs_stack_finish_device(self.handle, cb, None, _ptr(dst), dst_stride), self.ctx.handle)
+
+    # ---------------------------------------------- phases (frame shards)
+    def set_frame_total(self, frame_total: int):
+        """Frames of the whole stack when this one holds a shard of them."""
+        _check(L().fs_stack_set_frame_total(self.handle, frame_total), self.ctx.handle)
+
+    def end_pass1(self):
+        _check(L().fs_stack_end_pass1(self.handle), self.ctx.handle)
+
+    def blend(self, refetch=None):
+        cb = self._make_cb(refetch)
+        _check(L().fs_stack_blend(self.handle, cb, None), self.ctx.handle)
+
+    def collapse(self) -> np.ndarray:
+        out = np.zeros((self.out_height, self.out_width, 3), np.uint8)
+        _check(L().fs_stack_collapse(self.handle, out.ctypes.data_as(ctypes.c_void_p), self.out_width * 3, 0),
+               self.ctx.handle)
+        return out
+
+    def collapse_device(self, dst, dst_stride: int):
+        _check(L().fs_stack_collapse(self.handle, _ptr(dst), dst_stride, 1), self.ctx.handle)
+
+    def buffer(self, which: int, level: int = 0) -> "DeviceBuffer":
+        """Device view (with __cuda_array_interface__) of the weight sum, the
+        union support or a level's accumulator (3 x height x pitch)."""
+        p, b = ctypes.c_void_p(), ctypes.c_uint64()
+        pitch, w, h = ctypes.c_int64(), ctypes.c_uint32(), ctypes.c_uint32()
+        _check(L().fs_stack_buffer(self.handle, which, level, ctypes.byref(p), ctypes.byref(b), ctypes.byref(pitch),
+                                   ctypes.byref(w), ctypes.byref(h)), self.ctx.handle)
+        if which == BUFFER_ACCUMULATOR:
+            shape, typestr = (3, h.value, pitch.value), "<f4"
+        elif which == BUFFER_WEIGHT_SUM:
+            shape, typestr = (h.value, pitch.value), "<f4"
+        else:
+            shape, typestr = (h.value, pitch.value), "|u1"
+        return DeviceBuffer(int(p.value), shape, typestr, w.value, h.value, self)
 
     def _make_cb(self, refetch):
         held = []

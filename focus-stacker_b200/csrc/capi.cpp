@@ -219,6 +219,8 @@ struct fs_stack {
   std::vector<cudaEvent_t> slot_done;  // per staging buffer: the remap that last read it
   float* base_out = nullptr;      // optional device buffer for the collapsed base (RGB f32)
   uint32_t fp_level = 0;          // first level run one frame per CTA (none: >= L - 1)
+  uint32_t frame_total = 0;       // frames of the whole stack when this one holds a shard (0: its own)
+  int phase = 0;                  // 0 adding frames, 1 pass 1 done, 2 blended
   float* contrib = nullptr;       // per-frame blend contributions of those levels
   float* contrib_top = nullptr;   // and of the top level
   int64_t base_pitch = 0;         // elements
@@ -943,6 +945,9 @@ int fs_stack_add_frame_device(fs_stack* stack, const void* dev_pixels, size_t ro
   return add_frame_impl(stack, dev_pixels, row_stride, pose, true);
 }
 
+static int pass2_impl(fs_stack* s, fs_frame_fetch_cb refetch, void* user);
+static int collapse_impl(fs_stack* s, void* out, size_t out_stride, bool device_out, bool wait);
+
 static int finish_impl(fs_stack* s, fs_frame_fetch_cb refetch, void* user, void* out, size_t out_stride,
                        bool device_out, bool wait = true) {
   if (!s || !out) return FS_ERR_INVALID;
@@ -953,8 +958,25 @@ static int finish_impl(fs_stack* s, fs_frame_fetch_cb refetch, void* user, void*
     return set_err(ctx, FS_ERR_STATE, "fewer frames added than frame_count");
   if (out_stride < (size_t)s->W * 3) return set_err(ctx, FS_ERR_INVALID, "output stride too small");
   cudaSetDevice(ctx->device);
-  int rc = run_pending_pass1(s, true);
-  if (rc != FS_OK) return rc;
+  int rc;
+  if (s->phase < 1) {
+    if ((rc = run_pending_pass1(s, true)) != FS_OK) return rc;
+    s->phase = 1;
+  }
+  if (s->phase < 2) {
+    if ((rc = pass2_impl(s, refetch, user)) != FS_OK) return rc;
+    s->phase = 2;
+  }
+  if ((rc = collapse_impl(s, out, out_stride, device_out, wait)) != FS_OK) return rc;
+  s->finished = true;
+  return FS_OK;
+}
+
+// Pass 2: mask-support pyramid, accumulators cleared, the blend of every
+// frame into them (in the stack's pass-2 mode).
+static int pass2_impl(fs_stack* s, fs_frame_fetch_cb refetch, void* user) {
+  fs_ctx* ctx = s->ctx;
+  int rc;
   cudaStream_t st = ctx->stream;
   cudaError_t e;
   // mask-support pyramid (frame independent)
@@ -968,13 +990,15 @@ static int finish_impl(fs_stack* s, fs_frame_fetch_cb refetch, void* user, void*
     e = cudaMemsetAsync(s->acc[l], 0, (size_t)s->pitch[l] * s->lh[l] * 3 * 4, st);
     if (e != cudaSuccess) return cuda_err(ctx, e, "accumulator clear");
   }
-  // pass 2 in batches of K frames
+  // pass 2 in batches of K frames; the mask fallback 1/N counts every frame
+  // of the stack, also those of other shards
   const size_t N = s->frames.size();
+  const float inv_count = 1.0f / (float)(s->frame_total ? s->frame_total : N);
   if (s->mode == P2_LAPS) {
     // level-0 blend of every frame at once, streaming over the Laplacians
     e = timed(ctx, "blend0", [&] {
       return launch_blend0(s->acc[0], s->pitch[0] * s->lh[0], s->pitch[0], (int)s->W, (int)s->H, s->norm, s->tab,
-                           (float* const*)(s->tab + N), (int)N, 1.0f / (float)N, st);
+                           (float* const*)(s->tab + N), (int)N, inv_count, st);
     });
     if (e != cudaSuccess) return cuda_err(ctx, e, "level-0 blend");
   }
@@ -1010,7 +1034,7 @@ static int finish_impl(fs_stack* s, fs_frame_fetch_cb refetch, void* user, void*
     std::memset(&a, 0, sizeof(a));
     a.levels = (int32_t)s->L;
     a.K = (int32_t)(end - begin);
-    a.inv_count = 1.0f / (float)N;
+    a.inv_count = inv_count;
     a.norm = s->norm;
     const bool laps = s->mode == P2_LAPS;
     for (size_t k = begin; k < end; ++k) {
@@ -1063,7 +1087,15 @@ static int finish_impl(fs_stack* s, fs_frame_fetch_cb refetch, void* user, void*
       if (s->L == 1) break;
     }
   }
-  // collapse + quantise (src/fuse/pyramid.zig:223-269)
+  return FS_OK;
+}
+
+// Collapse of the accumulator pyramid and the quantised output
+// (src/fuse/pyramid.zig:223-269).
+static int collapse_impl(fs_stack* s, void* out, size_t out_stride, bool device_out, bool wait) {
+  fs_ctx* ctx = s->ctx;
+  cudaStream_t st = ctx->stream;
+  cudaError_t e;
   if (s->L == 1) {
     e = timed(ctx, "collapse", [&] {
       return launch_quantize(s->acc[0], s->pitch[0] * s->lh[0], s->pitch[0], (int)s->W, (int)s->H, s->out_dev,
@@ -1102,7 +1134,6 @@ static int finish_impl(fs_stack* s, fs_frame_fetch_cb refetch, void* user, void*
     e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) return cuda_err(ctx, e, "fusion");
   }
-  s->finished = true;
   return FS_OK;
 }
 
@@ -1128,6 +1159,74 @@ int fs_stack_footprint(const fs_stack_desc* desc, uint64_t available_bytes, int 
   *bytes = plan_bytes(plan, desc->frame_count, m, host_frames != 0);
   if (mode) *mode = (int)m;
   return *bytes <= available_bytes ? FS_OK : FS_ERR_BUDGET;
+}
+
+// ------------------------------------------------ phases (frame-sharded stacks)
+static int phase_check(fs_stack* s, int want) {
+  if (!s) return FS_ERR_INVALID;
+  if (!s->ctx) return FS_ERR_STATE;
+  if (s->finished) return set_err(s->ctx, FS_ERR_STATE, "stack already finished");
+  if (s->frames.size() != s->d.frame_count) return set_err(s->ctx, FS_ERR_STATE, "fewer frames added than frame_count");
+  if (s->phase != want) return set_err(s->ctx, FS_ERR_STATE, "stack phase out of order");
+  cudaSetDevice(s->ctx->device);
+  return FS_OK;
+}
+
+int fs_stack_set_frame_total(fs_stack* s, uint32_t frame_total) {
+  if (!s) return FS_ERR_INVALID;
+  if (!s->ctx) return FS_ERR_STATE;
+  if (frame_total < s->d.frame_count) return set_err(s->ctx, FS_ERR_INVALID, "total below this stack's frames");
+  s->frame_total = frame_total;
+  return FS_OK;
+}
+
+int fs_stack_end_pass1(fs_stack* s) {
+  int rc = phase_check(s, 0);
+  if (rc != FS_OK) return rc;
+  if ((rc = run_pending_pass1(s, true)) != FS_OK) return rc;
+  cudaError_t e = cudaStreamSynchronize(s->ctx->stream);
+  if (e != cudaSuccess) return cuda_err(s->ctx, e, "pass 1");
+  s->phase = 1;
+  return FS_OK;
+}
+
+int fs_stack_blend(fs_stack* s, fs_frame_fetch_cb refetch, void* user) {
+  int rc = phase_check(s, 1);
+  if (rc != FS_OK) return rc;
+  if ((rc = pass2_impl(s, refetch, user)) != FS_OK) return rc;
+  cudaError_t e = cudaStreamSynchronize(s->ctx->stream);
+  if (e != cudaSuccess) return cuda_err(s->ctx, e, "pass 2");
+  s->phase = 2;
+  return FS_OK;
+}
+
+int fs_stack_collapse(fs_stack* s, void* out_pixels, size_t out_stride, int device_out) {
+  int rc = phase_check(s, 2);
+  if (rc != FS_OK) return rc;
+  if (!out_pixels) return FS_ERR_INVALID;
+  if (out_stride < (size_t)s->W * 3) return set_err(s->ctx, FS_ERR_INVALID, "output stride too small");
+  if ((rc = collapse_impl(s, out_pixels, out_stride, device_out != 0, true)) != FS_OK) return rc;
+  s->finished = true;
+  return FS_OK;
+}
+
+int fs_stack_buffer(fs_stack* s, int which, uint32_t level, void** ptr, uint64_t* bytes, int64_t* pitch,
+                    uint32_t* width, uint32_t* height) {
+  if (!s || !ptr || !bytes) return FS_ERR_INVALID;
+  if (!s->ctx) return FS_ERR_STATE;
+  if (level >= s->L || (which != FS_BUFFER_ACCUMULATOR && level != 0))
+    return set_err(s->ctx, FS_ERR_INVALID, "no such buffer");
+  const size_t plane = (size_t)s->pitch[level] * s->lh[level];
+  switch (which) {
+    case FS_BUFFER_WEIGHT_SUM: *ptr = s->norm; *bytes = plane * 4; break;
+    case FS_BUFFER_UNION: *ptr = s->uni; *bytes = plane; break;
+    case FS_BUFFER_ACCUMULATOR: *ptr = s->acc[level]; *bytes = plane * 12; break;
+    default: return set_err(s->ctx, FS_ERR_INVALID, "no such buffer");
+  }
+  if (pitch) *pitch = s->pitch[level];
+  if (width) *width = s->lw[level];
+  if (height) *height = s->lh[level];
+  return FS_OK;
 }
 
 int fs_stack_finish(fs_stack* stack, fs_frame_fetch_cb refetch, void* user, void* out_pixels, size_t out_stride) {
@@ -1245,6 +1344,7 @@ int batch_enqueue(fs_batch* b) {
     s->frames.clear();
     s->pass1_done = 0;
     s->finished = false;
+    s->phase = 0;
     for (size_t k = 0; k < it.frames.size(); ++k) {
       const fs_pose* pose = s->aligned ? nullptr : &it.poses[k];
       int rc = add_frame_impl(s, it.frames[k], it.stride, pose, true);

@@ -223,6 +223,33 @@ int fs_stack_output_size(const fs_stack* stack, uint32_t* width, uint32_t* heigh
 
 int fs_stack_destroy(fs_stack* stack);
 
+/* Frame-sharded stacks (not part of the reference).  A stack split over
+ * several GPUs holds a contiguous shard of the frames on each; finish then
+ * runs in phases with two exchanges between them:
+ *   fs_stack_set_frame_total(s, N)   N = frames of the whole stack (the mask
+ *                                    fallback 1/N of src/fuse/pyramid.zig:303-316)
+ *   fs_stack_end_pass1(s)            pass 1 of the shard's frames done;
+ *     -> sum the FS_BUFFER_WEIGHT_SUM buffers and take the maximum of the
+ *        FS_BUFFER_UNION buffers over all shards, in place (e.g. NCCL);
+ *   fs_stack_blend(s, refetch, user) pass 2 of the shard's frames into the
+ *                                    accumulators (FS_BUFFER_ACCUMULATOR, one
+ *                                    per level, 3 planes of pitch x height f32);
+ *     -> sum the accumulators of all shards into one stack's;
+ *   fs_stack_collapse(s, out, stride, device_out)  on that stack.
+ * fs_stack_finish is the three phases with no exchange.  The sums over
+ * shards change the order of the FP32 additions, so results match a single
+ * stack to rounding, not bit for bit (the remap and the alpha do not
+ * change). */
+enum { FS_BUFFER_WEIGHT_SUM = 0, FS_BUFFER_UNION = 1, FS_BUFFER_ACCUMULATOR = 2 };
+int fs_stack_set_frame_total(fs_stack* stack, uint32_t frame_total);
+int fs_stack_end_pass1(fs_stack* stack);
+int fs_stack_blend(fs_stack* stack, fs_frame_fetch_cb refetch, void* user);
+int fs_stack_collapse(fs_stack* stack, void* out_pixels, size_t out_stride, int device_out);
+/* Device buffer `which` (level: accumulators only; 0 otherwise), its bytes,
+ * row pitch in elements and size. */
+int fs_stack_buffer(fs_stack* stack, int which, uint32_t level, void** ptr, uint64_t* bytes, int64_t* pitch,
+                    uint32_t* width, uint32_t* height);
+
 /* One-shot form over host frames already in memory: begin, add every frame
  * in order, finish.  Replaces runCollapsedPyramidStackPass
  * (src/stack/pipeline.zig:314-359) / runCollapsedPyramidPass
