@@ -197,7 +197,9 @@ struct fs_stack {
   std::vector<float*> wplane;                  // LAPS: per frame, its weight (level 0)
   std::vector<std::vector<float*>> lap;        // LAPS: per frame, Laplacian of levels 0 .. L-2
   std::vector<float*> gtop;                    // LAPS: per frame, Gaussian of the top level
-  std::vector<const float*> tab_host;          // LAPS: level-0 Laplacian then weight pointers, all frames
+  std::vector<std::vector<void*>> mplane;      // LAPS: per frame, mask of levels 1 .. L-2 (storage type)
+  std::vector<float*> mtop;                    // LAPS: per frame, mask of the top level (f32)
+  std::vector<const float*> tab_host;          // LAPS: per level, Laplacian then mask pointers of all frames
   const float** tab = nullptr;                 // the same table on the device
   uint8_t* out_dev = nullptr;
   std::vector<Alloc> allocs;
@@ -664,7 +666,7 @@ struct StackPlan {
   size_t staging_slots = 0;  // frame buffers of the two-batch upload ring
   uint32_t fp_level = 0;     // first level l >= 1 run one frame per CTA (L - 1: none)
   size_t contrib = 0, contrib_top = 0;  // bytes of the contribution buffers
-  size_t laps_frame = 0;                // LAPS: weight + Laplacians + top Gaussian of one frame
+  size_t laps_frame = 0;                // LAPS: weight, Laplacians, top Gaussian and masks of one frame
 };
 
 // Levels with fewer 64x32 tiles than this run one frame per CTA (grid.z = K)
@@ -713,7 +715,9 @@ StackPlan plan_stack(const fs_stack_desc& d) {
   if (p.L >= 3) {
     p.laps_frame = n0 * 4;
     for (uint32_t l = 0; l + 1 < p.L; ++l) p.laps_frame += (size_t)p.pitch[l] * p.lh[l] * 12;
-    p.laps_frame += (size_t)p.pitch[p.L - 1] * p.lh[p.L - 1] * 12;
+    p.laps_frame += (size_t)p.pitch[p.L - 1] * p.lh[p.L - 1] * 12;  // top Gaussian
+    for (uint32_t l = 1; l + 1 < p.L; ++l) p.laps_frame += (size_t)p.pitch[l] * p.lh[l] * esz;  // masks
+    p.laps_frame += (size_t)p.pitch[p.L - 1] * p.lh[p.L - 1] * 4;  // top mask
   }
   if (p.fp_level + 1 < p.L) {
     p.contrib = (size_t)p.K * 3 * p.pitch[p.fp_level] * p.lh[p.fp_level] * 4;
@@ -729,7 +733,8 @@ uint64_t plan_bytes(const StackPlan& p, uint32_t frames, Pass2Mode mode, bool ho
   const uint64_t staging = host_frames ? (uint64_t)p.frame_bytes * p.staging_slots : 0;
   switch (mode) {
     case P2_LAPS:
-      return p.fixed + (uint64_t)p.planes / 2 * p.K + ((uint64_t)p.laps_frame + 2 * sizeof(float*)) * frames + staging;
+      return p.fixed + (uint64_t)p.planes / 2 * p.K + ((uint64_t)p.laps_frame + 2 * p.L * sizeof(float*)) * frames +
+             staging;
     case P2_CACHE: return p.fixed + (uint64_t)p.planes * frames + staging;
     case P2_RESIDENT: return p.fixed + (uint64_t)p.planes * p.K + (uint64_t)p.frame_bytes * frames;
     default: return p.fixed + (uint64_t)p.planes * p.K + staging;
@@ -839,9 +844,22 @@ static int begin_impl(fs_ctx* ctx, const fs_stack_desc* desc, fs_stack** out, in
       }
       s->lap.push_back(lv);
       s->gtop.push_back((float*)q);
+      q += (size_t)s->pitch[s->L - 1] * s->lh[s->L - 1] * 12;
+      std::vector<void*> mv(s->L, nullptr);
+      for (uint32_t l = 1; l + 1 < s->L; ++l) {
+        mv[l] = q;
+        q += (size_t)s->pitch[l] * s->lh[l] * esz;
+      }
+      s->mplane.push_back(mv);
+      s->mtop.push_back((float*)q);
     }
-    for (uint32_t f = 0; f < d.frame_count; ++f) s->tab_host.push_back(s->lap[f][0]);
-    for (uint32_t f = 0; f < d.frame_count; ++f) s->tab_host.push_back(s->wplane[f]);
+    // per level: Laplacian (top: Gaussian) then mask (level 0: weight) of every frame
+    for (uint32_t l = 0; l < s->L; ++l) {
+      for (uint32_t f = 0; f < d.frame_count; ++f)
+        s->tab_host.push_back(l + 1 < s->L ? s->lap[f][l] : s->gtop[f]);
+      for (uint32_t f = 0; f < d.frame_count; ++f)
+        s->tab_host.push_back(l == 0 ? s->wplane[f] : l + 1 < s->L ? (const float*)s->mplane[f][l] : s->mtop[f]);
+    }
     if ((rc = stack_alloc(s, s->tab_host.size() * sizeof(float*), &p)) != FS_OK) return fail(rc);
     s->tab = (const float**)p;
     if (cudaMemcpyAsync(p, s->tab_host.data(), s->tab_host.size() * sizeof(float*), cudaMemcpyHostToDevice,
@@ -986,7 +1004,8 @@ static int pass2_impl(fs_stack* s, fs_frame_fetch_cb refetch, void* user) {
     e = timed(ctx, "mask_support", [&] { return launch_mask_support(m, st); });
     if (e != cudaSuccess) return cuda_err(ctx, e, "mask support");
   }
-  for (uint32_t l = 0; l < s->L; ++l) {
+  // (the LAPS blends write every accumulator level whole)
+  for (uint32_t l = 0; l < s->L && s->mode != P2_LAPS; ++l) {
     e = cudaMemsetAsync(s->acc[l], 0, (size_t)s->pitch[l] * s->lh[l] * 3 * 4, st);
     if (e != cudaSuccess) return cuda_err(ctx, e, "accumulator clear");
   }
@@ -996,11 +1015,42 @@ static int pass2_impl(fs_stack* s, fs_frame_fetch_cb refetch, void* user) {
   const float inv_count = 1.0f / (float)(s->frame_total ? s->frame_total : N);
   if (s->mode == P2_LAPS) {
     // level-0 blend of every frame at once, streaming over the Laplacians
+    // (it also turns each frame's weight into its normalised mask)
     e = timed(ctx, "blend0", [&] {
       return launch_blend0(s->acc[0], s->pitch[0] * s->lh[0], s->pitch[0], (int)s->W, (int)s->H, s->norm, s->tab,
                            (float* const*)(s->tab + N), (int)N, inv_count, st);
     });
     if (e != cudaSuccess) return cuda_err(ctx, e, "level-0 blend");
+    // the mask pyramid of every frame, level by level (one frame per grid z)
+    for (uint32_t l = 0; l + 1 < s->L; ++l) {
+      MaskReduceArgs m;
+      m.in = (const void* const*)(s->tab + (size_t)l * 2 * N + N);
+      m.out = (void* const*)(s->tab + (size_t)(l + 1) * 2 * N + N);
+      m.sm = s->sm[l];
+      m.wl = (int32_t)s->lw[l];
+      m.hl = (int32_t)s->lh[l];
+      m.wn = (int32_t)s->lw[l + 1];
+      m.hn = (int32_t)s->lh[l + 1];
+      m.pitch_l = s->pitch[l];
+      m.pitch_n = s->pitch[l + 1];
+      const int in_storage = l == 0 ? FS_STORAGE_F32 : s->storage;
+      const int out_storage = l + 2 < s->L ? s->storage : FS_STORAGE_F32;
+      e = timed(ctx, l == 0 ? "level0" : "level",
+                [&] { return launch_mask_reduce(m, (int)N, in_storage, out_storage, st); });
+      if (e != cudaSuccess) return cuda_err(ctx, e, "mask reduce");
+    }
+    // the blend of levels 1 .. L-1 over every frame (top: Gaussian x mask)
+    for (uint32_t l = 1; l < s->L; ++l) {
+      const float* const* lap = s->tab + (size_t)l * 2 * N;
+      const void* const* msk = (const void* const*)(s->tab + (size_t)l * 2 * N + N);
+      const int storage = l + 1 < s->L ? s->storage : FS_STORAGE_F32;
+      e = timed(ctx, "level", [&] {
+        return launch_blend(s->acc[l], s->pitch[l] * s->lh[l], s->pitch[l], (int)s->lw[l], (int)s->lh[l], lap, msk,
+                            (int)N, storage, st);
+      });
+      if (e != cudaSuccess) return cuda_err(ctx, e, "level blend");
+    }
+    return FS_OK;
   }
   std::vector<fs_stack::Frame> frames = s->frames;
   for (size_t begin = 0; begin < N; begin += s->K) {
@@ -1036,11 +1086,7 @@ static int pass2_impl(fs_stack* s, fs_frame_fetch_cb refetch, void* user) {
     a.K = (int32_t)(end - begin);
     a.inv_count = inv_count;
     a.norm = s->norm;
-    const bool laps = s->mode == P2_LAPS;
-    for (size_t k = begin; k < end; ++k) {
-      a.in0[k - begin] = s->mode == P2_CACHE ? s->cache[k] : laps ? FramePlanes{nullptr, s->wplane[k]} : s->p2[k - begin];
-      if (laps) a.gtop[k - begin] = s->gtop[k];
-    }
+    for (size_t k = begin; k < end; ++k) a.in0[k - begin] = s->mode == P2_CACHE ? s->cache[k] : s->p2[k - begin];
     for (uint32_t l = 0; l + 1 < s->L || (s->L == 1 && l == 0); ++l) {
       a.level = (int32_t)l;
       a.wl = (int32_t)s->lw[l];
@@ -1063,14 +1109,12 @@ static int pass2_impl(fs_stack* s, fs_frame_fetch_cb refetch, void* user) {
       for (size_t k = 0; k < (size_t)a.K; ++k) {
         if (l >= 1) a.in[k] = s->slot[k][l];
         if (l + 1 < s->L - 1) a.out[k] = s->slot[k][l + 1];
-        if (laps) a.lap[k] = s->lap[begin + k][l];
       }
       const bool fp = l >= 1 && l >= s->fp_level && s->contrib && a.K > 1;
       a.frame_parallel = fp ? 1 : 0;
       a.contrib = fp ? s->contrib : nullptr;
       a.contrib_top = fp ? s->contrib_top : nullptr;
-      if (laps) e = timed(ctx, l == 0 ? "level0" : "level", [&] { return launch_mask_level(a, s->storage, st); });
-      else if (l == 0) e = timed(ctx, "level0", [&] { return launch_level0(a, s->storage, st); });
+      if (l == 0) e = timed(ctx, "level0", [&] { return launch_level0(a, s->storage, st); });
       else e = timed(ctx, "level", [&] { return launch_level(a, s->storage, st); });
       if (e != cudaSuccess) return cuda_err(ctx, e, "level launch");
       if (fp) {

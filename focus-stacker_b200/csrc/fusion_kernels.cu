@@ -21,6 +21,7 @@
 #include <cuda_runtime.h>
 
 #include <cstddef>
+#include <type_traits>
 
 #include "fusion_kernels.cuh"
 
@@ -902,14 +903,6 @@ struct __align__(16) ImgSmem {
 };
 static_assert(offsetof(ImgSmem, tmp) % 16 == 0, "tmp is accessed as float4");
 
-struct __align__(16) MaskSmem {
-  static constexpr int kTmOffset = 0;
-  float tmp[MH * TMS * 2];
-  float nm[TH1 * TW1];
-  float m[MH * MW];
-  uint8_t sm[MH * MW];
-};
-
 template <typename T>
 __device__ void store_next_image(const ImgSmem& S, const LevelArgs& a, int x0, int y0, int k) {
   const int x1 = x0 >> 1, y1 = y0 >> 1;
@@ -928,33 +921,6 @@ __device__ void store_next_image(const ImgSmem& S, const LevelArgs& a, int x0, i
 #pragma unroll
       for (int c = 0; c < 3; ++c) stv<T>((T*)out.g, c * out.plane + o, S.ng[c][ni]);
       out.s[o] = S.ns[ni];
-    }
-  }
-}
-
-template <typename T>
-__device__ void store_next_mask(const MaskSmem& S, const LevelArgs& a, int x0, int y0, int k) {
-  const int x1 = x0 >> 1, y1 = y0 >> 1;
-  const bool top = a.level + 1 == a.levels - 1;
-  for (int i = threadIdx.x; i < TH1 * TW1; i += NT) {
-    const int ii = i / TW1, jj = i % TW1;
-    const int xj = x1 + jj, yi = y1 + ii;
-    if (xj >= a.wn || yi >= a.hn) continue;
-    const int64_t o = (int64_t)yi * a.pitch_n + xj;
-    if (top) {
-      const float m = S.nm[i];
-#pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        const float t = __fmul_rn(a.gtop[k][c * a.acc_plane_n + o], m);
-        if (a.frame_parallel) {
-          a.contrib_top[(int64_t)(k * 3 + c) * a.acc_plane_n + o] = t;
-        } else {
-          float* acc = a.acc_n + c * a.acc_plane_n + o;
-          *acc = __fadd_rn(*acc, t);
-        }
-      }
-    } else {
-      stv<T>((T*)a.out[k].m, o, S.nm[i]);
     }
   }
 }
@@ -1008,85 +974,6 @@ __global__ void __launch_bounds__(NT) img_kernel(const __grid_constant__ LevelAr
   expand_blend_step<true>(S, a, x0, y0, unused, a.lap[k]);
 }
 
-// L0: level 0, whose blend over all frames blend0_kernel does; this kernel
-// then only reduces the masks (one frame per CTA).
-template <typename T, bool L0>
-__global__ void __launch_bounds__(NT) mask_kernel(const __grid_constant__ LevelArgs a) {
-  extern __shared__ __align__(16) uint8_t smem_raw[];
-  MaskSmem& S = *reinterpret_cast<MaskSmem*>(smem_raw);
-  const int x0 = blockIdx.x * TW, y0 = blockIdx.y * TH;
-  load_mask_support(S, a, x0, y0);
-  float acc[PPT][3];
-  const bool fpar = L0 || a.frame_parallel;
-  const int kb = fpar ? (int)blockIdx.z : 0, ke = fpar ? kb + 1 : a.K;
-  if constexpr (L0) {
-  } else if (a.frame_parallel) {
-#pragma unroll
-    for (int i = 0; i < PPT; ++i) acc[i][0] = acc[i][1] = acc[i][2] = 0.0f;
-  } else {
-    load_acc(a, x0, y0, acc);
-  }
-  for (int k = kb; k < ke; ++k) {
-    // loads issued together (level >= 1 in two halves, for registers)
-    constexpr int NM = (MH * MW + NT - 1) / NT, NH2 = L0 ? 1 : 2, HM = (NM + NH2 - 1) / NH2;
-#pragma unroll
-    for (int h = 0; h < NH2; ++h) {
-      float mv[HM];
-#pragma unroll
-      for (int j = 0; j < HM; ++j) {
-        const int i = threadIdx.x + (h * HM + j) * NT;
-        const int X = x0 - 2 + i % MW, Y = y0 - 2 + i / MW;
-        mv[j] = 0.0f;
-        if (i < MH * MW && X >= 0 && Y >= 0 && X < a.wl && Y < a.hl) {
-          const int64_t o = (int64_t)Y * a.pitch_l + X;
-          if constexpr (L0) {
-            mv[j] = a.in0[k].w[o];  // normalised by blend0_kernel
-          } else {
-            mv[j] = ldv<T>((const T*)a.in[k].m, o);
-          }
-        }
-      }
-#pragma unroll
-      for (int j = 0; j < HM; ++j) {
-        const int i = threadIdx.x + (h * HM + j) * NT;
-        if (i < MH * MW) S.m[i] = mv[j];
-      }
-    }
-    __syncthreads();
-    reduce_mask_step(S);
-    store_next_mask<T>(S, a, x0, y0, k);
-    if constexpr (L0) continue;
-    const float* lap = a.lap[k];
-#pragma unroll
-    for (int i = 0; i < PPT; ++i) {
-      const int p = acc_pixel(i);
-      const int xx = p % TW, yy = p / TW;
-      const int X = x0 + xx, Y = y0 + yy;
-      if (X >= a.wl || Y >= a.hl) continue;
-      const int64_t o = (int64_t)Y * a.pitch_l + X;
-      const float m = S.m[(yy + 2) * MW + (xx + 2)];
-#pragma unroll
-      for (int c = 0; c < 3; ++c) acc[i][c] = __fadd_rn(acc[i][c], __fmul_rn(lap[c * a.acc_plane_l + o], m));
-    }
-    __syncthreads();
-  }
-  if constexpr (L0) return;
-  if (a.frame_parallel) {
-#pragma unroll
-    for (int i = 0; i < PPT; ++i) {
-      const int p = acc_pixel(i);
-      const int X = x0 + p % TW, Y = y0 + p / TW;
-      if (X < a.wl && Y < a.hl) {
-        const int64_t o = (int64_t)Y * a.pitch_l + X;
-#pragma unroll
-        for (int c = 0; c < 3; ++c) a.contrib[(int64_t)(kb * 3 + c) * a.acc_plane_l + o] = acc[i][c];
-      }
-    }
-  } else {
-    store_acc(a, x0, y0, acc);
-  }
-}
-
 // Level-0 blend of a whole stack in frame order, one pixel per thread:
 // acc = sum over frames of lap_k * (w_k / weight sum) (1 / N where the sum
 // is <= 1e-12), the same products and sums the per-batch kernels form.
@@ -1128,6 +1015,202 @@ __global__ void blend0_kernel(float* acc, int64_t plane, int64_t pitch, int w, i
   acc[2 * plane + o] = a2;
 }
 
+// Blend of one level over all frames in order, one pixel per thread (the
+// products and sums of the per-batch kernels, from acc = 0).
+template <typename T>
+__global__ void blend_kernel(float* acc, int64_t plane, int64_t pitch, int w, int h, const float* const* lap,
+                             const void* const* mask, int frames) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (int64_t)w * h) return;
+  const int64_t o = (i / w) * pitch + i % w;
+  float a0 = 0.0f, a1 = 0.0f, a2 = 0.0f;
+  constexpr int U = 4;
+  for (int k0 = 0; k0 < frames; k0 += U) {
+    float l0[U], l1[U], l2[U], mv[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      if (k0 + u < frames) {
+        const float* lk = lap[k0 + u];
+        l0[u] = __ldg(lk + o);
+        l1[u] = __ldg(lk + plane + o);
+        l2[u] = __ldg(lk + 2 * plane + o);
+        mv[u] = ldv<T>((const T*)mask[k0 + u], o);
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      if (k0 + u < frames) {
+        a0 = __fadd_rn(a0, __fmul_rn(l0[u], mv[u]));
+        a1 = __fadd_rn(a1, __fmul_rn(l1[u], mv[u]));
+        a2 = __fadd_rn(a2, __fmul_rn(l2[u], mv[u]));
+      }
+    }
+  }
+  acc[o] = a0;
+  acc[plane + o] = a1;
+  acc[2 * plane + o] = a2;
+}
+
+cudaError_t launch_blend(float* acc, int64_t plane, int64_t pitch, int w, int h, const float* const* lap,
+                         const void* const* mask, int frames, int storage, cudaStream_t s) {
+  const int64_t n = (int64_t)w * h;
+  const unsigned blocks = (unsigned)((n + 255) / 256);
+  switch (storage) {
+    case FS_STORAGE_F32: blend_kernel<float><<<blocks, 256, 0, s>>>(acc, plane, pitch, w, h, lap, mask, frames); break;
+    case FS_STORAGE_F16: blend_kernel<__half><<<blocks, 256, 0, s>>>(acc, plane, pitch, w, h, lap, mask, frames); break;
+    case FS_STORAGE_BF16:
+      blend_kernel<__nv_bfloat16><<<blocks, 256, 0, s>>>(acc, plane, pitch, w, h, lap, mask, frames);
+      break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
+// Mask REDUCE, streaming: each thread owns two neighbouring level-(l+1)
+// columns and a strip of kReduceRows rows, and slides a five-row window of
+// horizontal sums down the level-l mask (two new rows per output row), with
+// the taps of a row in one vector load plus its two edges.  The products and
+// sums are reduce_mask_step's, in its order: per row
+// v = sum_kx fma(s ? kw : 0, m, v), ws = sum_kx (s ? kw : 0); per column
+// v = sum_ky fma(kw, v_row, v), ws likewise; mask = ws > 0 ? v * (1 / ws) : 0.
+// Taps outside the level count as support 0 and value 0 (a row outside
+// contributes 0 to both sums, as its five zero-support taps do there).
+constexpr int kReduceRows = 8, kReduceWarps = 4;
+
+template <typename T>
+__device__ __forceinline__ void ld4(const T* p, float* v) {
+  if constexpr (std::is_same<T, float>::value) {
+    const float4 q = *reinterpret_cast<const float4*>(p);
+    v[0] = q.x; v[1] = q.y; v[2] = q.z; v[3] = q.w;
+  } else {
+    const uint2 q = *reinterpret_cast<const uint2*>(p);
+    const T* h = reinterpret_cast<const T*>(&q);
+#pragma unroll
+    for (int u = 0; u < 4; ++u) v[u] = ldv<T>(h, u);
+  }
+}
+
+template <typename T>
+__device__ __forceinline__ void ld2(const T* p, float* v) {
+  if constexpr (std::is_same<T, float>::value) {
+    const float2 q = *reinterpret_cast<const float2*>(p);
+    v[0] = q.x; v[1] = q.y;
+  } else {
+    const uint32_t q = *reinterpret_cast<const uint32_t*>(p);
+    const T* h = reinterpret_cast<const T*>(&q);
+    v[0] = ldv<T>(h, 0);
+    v[1] = ldv<T>(h, 1);
+  }
+}
+
+// Horizontal sums of level-l row r for output columns j0, j0 + 1.
+template <typename T>
+__device__ __forceinline__ void reduce_row(const T* in, const uint8_t* sm, int64_t pitch, int wl, int hl, int r,
+                                           int j0, float* v, float* ws) {
+  float m[7], sw[7];
+#pragma unroll
+  for (int u = 0; u < 7; ++u) m[u] = sw[u] = 0.0f;
+  if (r >= 0 && r < hl) {
+    const int c = 2 * j0;  // a multiple of 4: the vector loads are aligned
+    const T* row = in + (int64_t)r * pitch;
+    const uint8_t* srow = sm + (int64_t)r * pitch;
+    // columns c .. c + 3 lie inside the row's pitch (c < wl, pitch a multiple of 32)
+    ld4<T>(row + c, m + 2);
+    const uint32_t s4 = *reinterpret_cast<const uint32_t*>(srow + c);
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const bool in_level = c + u < wl;
+      sw[2 + u] = in_level && ((s4 >> (8 * u)) & 0xffu) ? 1.0f : 0.0f;
+      if (!in_level) m[2 + u] = 0.0f;
+    }
+    if (c > 0) {
+      ld2<T>(row + c - 2, m);
+      const uint32_t s2 = *reinterpret_cast<const uint16_t*>(srow + c - 2);
+      sw[0] = (s2 & 0xffu) ? 1.0f : 0.0f;
+      sw[1] = (s2 >> 8) ? 1.0f : 0.0f;
+    }
+    if (c + 4 < wl) {
+      m[6] = ldv<T>(row, c + 4);
+      sw[6] = srow[c + 4] ? 1.0f : 0.0f;
+    }
+  }
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    float a = 0.f, b = 0.f;
+#pragma unroll
+    for (int kx = 0; kx < 5; ++kx) {
+      const float w = sw[2 * h + kx] != 0.0f ? kw(kx) : 0.0f;
+      a = fmaf(w, m[2 * h + kx], a);
+      b += w;
+    }
+    v[h] = a;
+    ws[h] = b;
+  }
+}
+
+template <typename TI, typename TO>
+__global__ void __launch_bounds__(32 * kReduceWarps) mask_reduce_kernel(const __grid_constant__ MaskReduceArgs a) {
+  const int j0 = 2 * (int)(blockIdx.x * 32 + threadIdx.x);
+  const int i0 = (int)(blockIdx.y * kReduceWarps + threadIdx.y) * kReduceRows;
+  if (j0 >= a.wn || i0 >= a.hn) return;  // no barriers below
+  const int i1 = min(i0 + kReduceRows, a.hn);
+  const TI* in = (const TI*)a.in[blockIdx.z];
+  TO* out = (TO*)a.out[blockIdx.z];
+  // window of horizontal sums: rows 2i - 2 .. 2i + 2 for output row i
+  float hv[5][2], hw[5][2];
+#pragma unroll
+  for (int u = 0; u < 3; ++u) reduce_row<TI>(in, a.sm, a.pitch_l, a.wl, a.hl, 2 * i0 - 2 + u, j0, hv[u], hw[u]);
+  for (int i = i0; i < i1; ++i) {
+    reduce_row<TI>(in, a.sm, a.pitch_l, a.wl, a.hl, 2 * i + 1, j0, hv[3], hw[3]);
+    reduce_row<TI>(in, a.sm, a.pitch_l, a.wl, a.hl, 2 * i + 2, j0, hv[4], hw[4]);
+    TO* orow = out + (int64_t)i * a.pitch_n;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      float v = 0.f, ws = 0.f;
+#pragma unroll
+      for (int ky = 0; ky < 5; ++ky) {
+        v = fmaf(kw(ky), hv[ky][h], v);
+        ws = fmaf(kw(ky), hw[ky][h], ws);
+      }
+      if (j0 + h < a.wn) stv<TO>(orow, j0 + h, ws > 0.f ? v * __fdividef(1.0f, ws) : 0.f);
+    }
+#pragma unroll
+    for (int u = 0; u < 3; ++u) {
+      hv[u][0] = hv[u + 2][0];
+      hv[u][1] = hv[u + 2][1];
+      hw[u][0] = hw[u + 2][0];
+      hw[u][1] = hw[u + 2][1];
+    }
+  }
+}
+
+template <typename TI>
+static cudaError_t launch_mask_reduce_in(const MaskReduceArgs& a, dim3 grid, dim3 block, int out_storage,
+                                         cudaStream_t s) {
+  switch (out_storage) {
+    case FS_STORAGE_F32: mask_reduce_kernel<TI, float><<<grid, block, 0, s>>>(a); break;
+    case FS_STORAGE_F16: mask_reduce_kernel<TI, __half><<<grid, block, 0, s>>>(a); break;
+    case FS_STORAGE_BF16: mask_reduce_kernel<TI, __nv_bfloat16><<<grid, block, 0, s>>>(a); break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_mask_reduce(const MaskReduceArgs& a, int frames, int in_storage, int out_storage,
+                               cudaStream_t s) {
+  if (frames <= 0 || frames > 65535) return cudaErrorInvalidValue;
+  const dim3 block(32, kReduceWarps);
+  const dim3 grid((unsigned)((a.wn + 63) / 64), (unsigned)((a.hn + kReduceWarps * kReduceRows - 1) /
+                                                              (kReduceWarps * kReduceRows)),
+                  (unsigned)frames);
+  switch (in_storage) {
+    case FS_STORAGE_F32: return launch_mask_reduce_in<float>(a, grid, block, out_storage, s);
+    case FS_STORAGE_F16: return launch_mask_reduce_in<__half>(a, grid, block, out_storage, s);
+    case FS_STORAGE_BF16: return launch_mask_reduce_in<__nv_bfloat16>(a, grid, block, out_storage, s);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
 cudaError_t launch_blend0(float* acc, int64_t plane, int64_t pitch, int w, int h, const float* norm,
                           const float* const* lap, float* const* wgt, int frames, float inv_count,
                           cudaStream_t s) {
@@ -1138,9 +1221,9 @@ cudaError_t launch_blend0(float* acc, int64_t plane, int64_t pitch, int w, int h
 }
 
 template <template <typename, bool> class KER, bool L0>
-static cudaError_t launch_split(const LevelArgs& a, int storage, cudaStream_t s, bool* cfg, bool img) {
-  dim3 grid((a.wl + TW - 1) / TW, (a.hl + TH - 1) / TH, (img || L0 || a.frame_parallel) ? a.K : 1);
-  const size_t sm = img ? sizeof(ImgSmem) : sizeof(MaskSmem);
+static cudaError_t launch_split(const LevelArgs& a, int storage, cudaStream_t s, bool* cfg) {
+  dim3 grid((a.wl + TW - 1) / TW, (a.hl + TH - 1) / TH, a.K);
+  const size_t sm = sizeof(ImgSmem);
   cudaError_t e;
   switch (storage) {
     case FS_STORAGE_F32:
@@ -1163,20 +1246,11 @@ static cudaError_t launch_split(const LevelArgs& a, int storage, cudaStream_t s,
 template <typename T, bool L0> struct ImgK {
   static constexpr auto kernel = img_kernel<T, L0>;
 };
-template <typename T, bool L0> struct MaskK {
-  static constexpr auto kernel = mask_kernel<T, L0>;
-};
 
 cudaError_t launch_img_level(const LevelArgs& a, int storage, cudaStream_t s) {
   static bool cfg0[3] = {false, false, false}, cfg1[3] = {false, false, false};
-  return a.level == 0 ? launch_split<ImgK, true>(a, storage, s, cfg0, true)
-                      : launch_split<ImgK, false>(a, storage, s, cfg1, true);
-}
-
-cudaError_t launch_mask_level(const LevelArgs& a, int storage, cudaStream_t s) {
-  static bool cfg0[3] = {false, false, false}, cfg1[3] = {false, false, false};
-  return a.level == 0 ? launch_split<MaskK, true>(a, storage, s, cfg0, false)
-                      : launch_split<MaskK, false>(a, storage, s, cfg1, false);
+  return a.level == 0 ? launch_split<ImgK, true>(a, storage, s, cfg0)
+                      : launch_split<ImgK, false>(a, storage, s, cfg1);
 }
 
 __global__ void sum_contrib_kernel(float* acc, int64_t plane, int64_t pitch, int w, int h, const float* contrib,

@@ -80,7 +80,7 @@ struct LevelArgs {
   int32_t frame_parallel;
   float* contrib;
   float* contrib_top;
-  // split pyramid (launch_img_level / launch_mask_level): frame k's
+  // split pyramid (launch_img_level): frame k's
   // Laplacian planes at level l (3 planes of acc_plane_l floats) and its top
   // Gaussian (3 planes of acc_plane_n floats, written when l + 1 is the top)
   float* lap[kMaxBatch];
@@ -100,6 +100,20 @@ struct CollapseArgs {
   float* base;                // final level, optional: collapsed base before quantisation (RGB f32)
   int64_t base_pitch;         // elements per row
 };
+
+// Mask REDUCE of one level for every frame of a stack, one frame per grid z:
+// level-(l+1) mask = support-weighted 5x5 REDUCE of the level-l mask with the
+// level-l union support (src/fuse/pyramid.zig:997-1043), the products and
+// sums of the level kernels' mask REDUCE in the same order.
+struct MaskReduceArgs {
+  const void* const* in;  // per frame: level-l mask (level 0: the normalised weight plane)
+  void* const* out;       // per frame: level-(l+1) mask
+  const uint8_t* sm;      // level-l union support
+  int32_t wl, hl, wn, hn;
+  int64_t pitch_l, pitch_n;
+};
+// Storage of in / out masks: 0 f32, 1 f16, 2 bf16.
+cudaError_t launch_mask_reduce(const MaskReduceArgs& a, int frames, int in_storage, int out_storage, cudaStream_t s);
 
 struct MaskSupportArgs {
   const uint8_t* src;
@@ -127,14 +141,14 @@ cudaError_t launch_collapse(const CollapseArgs& a, cudaStream_t s);
 // or gtop[k] at the top) and the Laplacian of level l into lap[k]; level 0
 // reads the remapped RGBA planes in0[k].rgba.
 cudaError_t launch_img_level(const LevelArgs& a, int storage, cudaStream_t s);
-// The mask half: normalised mask (level 0 from in0[k].w and the weight sum),
-// its REDUCE to level l + 1 (out[k].m) and acc_l += lap[k] * mask in frame
-// order (frame-parallel with contributions when a.frame_parallel).
-cudaError_t launch_mask_level(const LevelArgs& a, int storage, cudaStream_t s);
+// acc = sum over frames k, in order, of lap[k] (3 planes of `plane`) times
+// mask[k] (storage T: 0 f32, 1 f16, 2 bf16), written over acc.
+cudaError_t launch_blend(float* acc, int64_t plane, int64_t pitch, int w, int h, const float* const* lap,
+                         const void* const* mask, int frames, int storage, cudaStream_t s);
 // Level-0 blend of all frames of a stack (device tables of each frame's
 // level-0 Laplacian and weight planes), written over acc; each weight plane
-// is replaced by the frame's normalised mask.  The level-0 launch of
-// launch_mask_level then reads those masks.
+// is replaced by the frame's normalised mask, which launch_mask_reduce then
+// reads.
 cudaError_t launch_blend0(float* acc, int64_t plane, int64_t pitch, int w, int h, const float* norm,
                           const float* const* lap, float* const* wgt, int frames, float inv_count,
                           cudaStream_t s);
