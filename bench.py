@@ -195,19 +195,24 @@ def algorithmic_bytes(roi_w, roi_h, frames, k, mode="cache", storage_bytes=4):
     if mode == "laps":
         # pass 1 builds each frame's Gaussian/Laplacian pyramid: RGBA read,
         # per level the Laplacian written (12 B) and the next Gaussian and
-        # support written (3s + 1) and read again by the next level;
-        # pass 2 reads weights and Laplacians and writes / reads the masks
+        # support written (3s + 1) and read again by the next level
         img = 4 * A[0]
         for l in range(L - 1):
             img += 12 * A[l] + (3 * s + 1) * A[l + 1] + ((3 * s + 1) * A[l] if l >= 1 else 0)
         b["image"] = frames * img
         b["blend0"] = frames * 20 * A[0] + 16 * A[0]  # Laplacian 12 + weight 4 read, mask 4 written
-        b["level0"] = frames * (4 * A[0] + s * l1) + batches * 5 * A[0]
+        # level 0: mask REDUCE of every frame (mask 4 B read, level-1 mask
+        # written in storage type) and the union support read once
+        b["level0"] = frames * (4 * A[0] + (s if L > 2 else 4) * l1) + A[0]
+        # levels >= 1: mask REDUCE (mask read, next mask written; the top one
+        # in f32; support once) and the blend of each level over all frames
+        # (Laplacian 12 B and mask read per frame, accumulator 12 B written)
         lv = 0
-        for l in range(1, L - 1):
-            nxt = A[l + 1] if l + 1 < L - 1 else 0
-            top = A[l + 1] * 24 * batches if l + 1 == L - 1 else 0
-            lv += frames * (s * A[l] + 12 * A[l] + s * nxt) + batches * 25 * A[l] + top
+        for l in range(1, L):
+            ms = s if l + 1 < L else 4
+            if l + 1 < L:
+                lv += frames * (ms * A[l] + (s if l + 2 < L else 4) * A[l + 1]) + A[l]
+            lv += frames * (12 + ms) * A[l] + 12 * A[l]
         b["level"] = lv
     return b, sum(b.values())
 
