@@ -1211,6 +1211,238 @@ cudaError_t launch_mask_reduce(const MaskReduceArgs& a, int frames, int in_stora
   }
 }
 
+// ------------------------------------------------ streaming image pyramid
+// One frame's pyramid step l -> l + 1 for the levels whose EXPAND clamps
+// (exact_expand == 0), without shared memory: each lane owns the level-(l+1)
+// column pair J0 = 2p, J1 = 2p + 1 and the level-l columns c = 4p .. 4p + 3,
+// and walks down a strip of kImgRows level-(l+1) rows.  A five-row window of
+// horizontal REDUCE sums (level-l rows 2r - 2 .. 2r + 2) gives level-(l+1)
+// row r; the EXPAND's horizontal pass takes the neighbouring columns J0 - 1
+// and J1 + 1 from the adjacent lanes (shuffles), so lanes 0 and 31 of a warp
+// only feed their neighbours and kImgPairs lanes emit.  The Laplacian of
+// level-l rows 2q, 2q + 1 is emitted once row q + 1 is known.  Products and
+// sums are those of reduce_image_step and expand_blend_step (clamped mode),
+// in their order.
+constexpr int kImgRows = 32, kImgWarps = 4, kImgPairs = 30;
+
+// Horizontal REDUCE sums (v0, v1, v2, weight) of level-l row y for the lane's
+// two level-(l+1) columns; samples outside the level count as zero.
+template <typename T, bool L0>
+__device__ __forceinline__ void img_row(const LevelArgs& a, int k, int y, int c, bool live, float4 (&hs)[2]) {
+  float4 t[7];
+#pragma unroll
+  for (int u = 0; u < 7; ++u) t[u] = make_float4(0.f, 0.f, 0.f, 0.f);
+  if (live && y >= 0 && y < a.hl) {
+    const int64_t ro = (int64_t)y * a.pitch_l;
+    // columns c .. c + 3 lie inside the row's pitch (c < wl, pitch a multiple of 32)
+    if constexpr (L0) {
+      const uint32_t* row = a.in0[k].rgba + ro;
+      uint32_t w[7] = {0u, 0u, 0u, 0u, 0u, 0u, 0u};
+      const uint4 q4 = *reinterpret_cast<const uint4*>(row + c);
+      w[2] = q4.x;
+      w[3] = q4.y;
+      w[4] = q4.z;
+      w[5] = q4.w;
+      if (c > 0) {
+        const uint2 q2 = *reinterpret_cast<const uint2*>(row + c - 2);
+        w[0] = q2.x;
+        w[1] = q2.y;
+      }
+      if (c + 4 < a.wl) w[6] = row[c + 4];
+#pragma unroll
+      for (int u = 0; u < 7; ++u) {
+        const bool in = u < 2 || u == 6 || c + u - 2 < a.wl;  // u < 2, u == 6: zero words when outside
+        if (in) t[u] = make_float4(chf(w[u], 0), chf(w[u], 1), chf(w[u], 2), px_alpha(w[u]) > 0 ? 1.0f : 0.0f);
+      }
+    } else {
+      const LevelPlanes& in = a.in[k];
+      const T* g = (const T*)in.g + ro;
+      const uint8_t* sp = in.s + ro;
+      float v[3][7];
+#pragma unroll
+      for (int ch = 0; ch < 3; ++ch) {
+        const T* gc = g + ch * in.plane;
+        ld4<T>(gc + c, v[ch] + 2);
+        v[ch][0] = v[ch][1] = v[ch][6] = 0.0f;
+        if (c > 0) ld2<T>(gc + c - 2, v[ch]);
+        if (c + 4 < a.wl) v[ch][6] = ldv<T>(gc, c + 4);
+      }
+      const uint32_t s4 = *reinterpret_cast<const uint32_t*>(sp + c);
+      const uint32_t s2 = c > 0 ? *reinterpret_cast<const uint16_t*>(sp + c - 2) : 0u;
+      const uint32_t s6 = c + 4 < a.wl ? sp[c + 4] : 0u;
+      const uint32_t sb[7] = {s2 & 0xffu, s2 >> 8, s4 & 0xffu, (s4 >> 8) & 0xffu, (s4 >> 16) & 0xffu, s4 >> 24, s6};
+#pragma unroll
+      for (int u = 0; u < 7; ++u) {
+        const bool in = u < 2 || u == 6 || c + u - 2 < a.wl;
+        if (in) t[u] = make_float4(v[0][u], v[1][u], v[2][u], sb[u] ? 1.0f : 0.0f);
+      }
+    }
+  }
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    float v0 = 0.f, v1 = 0.f, v2 = 0.f, ws = 0.f;
+#pragma unroll
+    for (int kx = 0; kx < 5; ++kx) {
+      const float4 tk = t[2 * h + kx];
+      const float w = kw(kx) * tk.w;
+      v0 = fmaf(w, tk.x, v0);
+      v1 = fmaf(w, tk.y, v1);
+      v2 = fmaf(w, tk.z, v2);
+      ws += w;
+    }
+    hs[h] = make_float4(v0, v1, v2, ws);
+  }
+}
+
+template <typename T, bool L0>
+__global__ void __launch_bounds__(32 * kImgWarps) img_stream_kernel(const __grid_constant__ LevelArgs a) {
+  const int lane = (int)threadIdx.x, k = (int)blockIdx.z;
+  const int first = ((int)blockIdx.x * kImgWarps + (int)threadIdx.y) * kImgPairs;  // pair of lane 1
+  if (2 * first >= a.wn) return;  // the whole warp: none of its pairs is in the level
+  const int p = first + lane - 1;
+  const int J0 = 2 * p, c = 4 * p;
+  const bool live = p >= 0 && J0 < a.wn;
+  const bool emit = live && lane >= 1 && lane <= kImgPairs;
+  const bool j1in = J0 + 1 < a.wn, rin = J0 + 2 < a.wn;
+  const int i0 = (int)blockIdx.y * kImgRows;
+  const int i1 = min(i0 + kImgRows, a.hn);
+  float4 win[5][2];
+  float Hm2[3][4], Hm1[3][4], Hc[3][4];
+#pragma unroll
+  for (int ch = 0; ch < 3; ++ch)
+#pragma unroll
+    for (int u = 0; u < 4; ++u) Hm2[ch][u] = Hm1[ch][u] = 0.0f;
+  int r = i0 > 0 ? i0 - 1 : 0;
+#pragma unroll
+  for (int u = 0; u < 3; ++u) img_row<T, L0>(a, k, 2 * r - 2 + u, c, live, win[u]);
+  for (; r <= i1; ++r) {
+    img_row<T, L0>(a, k, 2 * r + 1, c, live, win[3]);
+    img_row<T, L0>(a, k, 2 * r + 2, c, live, win[4]);
+    if (r < a.hn) {  // warp-uniform
+      // REDUCE: level-(l+1) row r, columns J0, J0 + 1
+      float g[2][3];
+      bool sp[2];
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        float v0 = 0.f, v1 = 0.f, v2 = 0.f, ws = 0.f;
+#pragma unroll
+        for (int ky = 0; ky < 5; ++ky) {
+          const float4 t = win[ky][h];
+          const float w = kw(ky);
+          v0 = fmaf(w, t.x, v0);
+          v1 = fmaf(w, t.y, v1);
+          v2 = fmaf(w, t.z, v2);
+          ws = fmaf(w, t.w, ws);
+        }
+        sp[h] = live && J0 + h < a.wn && ws > 0.f;
+        const float rc = sp[h] ? __fdividef(1.0f, ws) : 0.0f;
+        g[h][0] = v0 * rc;
+        g[h][1] = v1 * rc;
+        g[h][2] = v2 * rc;
+      }
+      if (emit && r >= i0 && r < i1) {
+        const LevelPlanes& out = a.out[k];
+        const int64_t o = (int64_t)r * a.pitch_n + J0;
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          if (J0 + h >= a.wn) continue;
+#pragma unroll
+          for (int ch = 0; ch < 3; ++ch) stv<T>((T*)out.g, ch * out.plane + o + h, g[h][ch]);
+          out.s[o + h] = sp[h] ? 1 : 0;
+        }
+      }
+      // horizontal EXPAND of row r onto columns c .. c + 3 (clamped)
+#pragma unroll
+      for (int ch = 0; ch < 3; ++ch) {
+        const float gA = g[0][ch], gB = j1in ? g[1][ch] : gA;
+        float gL = __shfl_up_sync(0xffffffffu, gB, 1);
+        const float gRn = __shfl_down_sync(0xffffffffu, gA, 1);
+        if (p == 0) gL = gA;
+        const float gR = rin ? gRn : gB;
+        Hc[ch][0] = __fmul_rn(__fadd_rn(__fadd_rn(gL, __fmul_rn(6.0f, gA)), gB), 0.125f);
+        Hc[ch][1] = __fmul_rn(__fadd_rn(gA, gB), 0.5f);
+        Hc[ch][2] = __fmul_rn(__fadd_rn(__fadd_rn(gA, __fmul_rn(6.0f, gB)), gR), 0.125f);
+        Hc[ch][3] = __fmul_rn(__fadd_rn(gB, gR), 0.5f);
+      }
+      if (r == 0) {  // row -1 clamps to row 0
+#pragma unroll
+        for (int ch = 0; ch < 3; ++ch)
+#pragma unroll
+          for (int u = 0; u < 4; ++u) Hm1[ch][u] = Hc[ch][u];
+      }
+    } else {  // row hn clamps to row hn - 1
+#pragma unroll
+      for (int ch = 0; ch < 3; ++ch)
+#pragma unroll
+        for (int u = 0; u < 4; ++u) Hc[ch][u] = Hm1[ch][u];
+    }
+    // Laplacian of level-l rows 2q, 2q + 1, q = r - 1
+    if (emit && r >= i0 + 1) {
+#pragma unroll
+      for (int yy = 0; yy < 2; ++yy) {
+        const int y = 2 * (r - 1) + yy;
+        if (y >= a.hl) break;
+        const int64_t ro = (int64_t)y * a.pitch_l;
+        float gv[3][4];
+        if constexpr (L0) {
+          const uint4 q4 = *reinterpret_cast<const uint4*>(a.in0[k].rgba + ro + c);
+          const uint32_t w[4] = {q4.x, q4.y, q4.z, q4.w};
+#pragma unroll
+          for (int ch = 0; ch < 3; ++ch)
+#pragma unroll
+            for (int u = 0; u < 4; ++u) gv[ch][u] = chf(w[u], ch);
+        } else {
+          const LevelPlanes& in = a.in[k];
+#pragma unroll
+          for (int ch = 0; ch < 3; ++ch) ld4<T>((const T*)in.g + ch * in.plane + ro + c, gv[ch]);
+        }
+        float* lp = a.lap[k] + ro + c;
+#pragma unroll
+        for (int ch = 0; ch < 3; ++ch) {
+          float lv[4];
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            const float e = yy == 0
+                ? __fmul_rn(__fadd_rn(__fadd_rn(Hm2[ch][u], __fmul_rn(6.0f, Hm1[ch][u])), Hc[ch][u]), 0.125f)
+                : __fmul_rn(__fadd_rn(Hm1[ch][u], Hm1[ch][u]), 0.5f);
+            lv[u] = __fsub_rn(gv[ch][u], e);
+          }
+          float* lc = lp + ch * a.acc_plane_l;
+          if (c + 3 < a.wl) {
+            *reinterpret_cast<float4*>(lc) = make_float4(lv[0], lv[1], lv[2], lv[3]);
+          } else {
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+              if (c + u < a.wl) lc[u] = lv[u];
+          }
+        }
+      }
+    }
+#pragma unroll
+    for (int ch = 0; ch < 3; ++ch)
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        Hm2[ch][u] = Hm1[ch][u];
+        Hm1[ch][u] = Hc[ch][u];
+      }
+#pragma unroll
+    for (int u = 0; u < 3; ++u) {
+      win[u][0] = win[u + 2][0];
+      win[u][1] = win[u + 2][1];
+    }
+  }
+}
+
+template <typename T, bool L0>
+static cudaError_t launch_img_stream(const LevelArgs& a, cudaStream_t s) {
+  const int pairs = (a.wn + 1) / 2;
+  const int warps = (pairs + kImgPairs - 1) / kImgPairs;
+  const dim3 grid((unsigned)((warps + kImgWarps - 1) / kImgWarps), (unsigned)((a.hn + kImgRows - 1) / kImgRows),
+                  (unsigned)a.K);
+  img_stream_kernel<T, L0><<<grid, dim3(32, kImgWarps), 0, s>>>(a);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_blend0(float* acc, int64_t plane, int64_t pitch, int w, int h, const float* norm,
                           const float* const* lap, float* const* wgt, int frames, float inv_count,
                           cudaStream_t s) {
@@ -1249,6 +1481,20 @@ template <typename T, bool L0> struct ImgK {
 
 cudaError_t launch_img_level(const LevelArgs& a, int storage, cudaStream_t s) {
   static bool cfg0[3] = {false, false, false}, cfg1[3] = {false, false, false};
+  // clamped-EXPAND levels (never followed by the top level): streaming kernel
+  if (!a.exact_expand && a.level + 2 < a.levels) {
+    switch (storage) {
+      case FS_STORAGE_F32:
+        return a.level == 0 ? launch_img_stream<float, true>(a, s) : launch_img_stream<float, false>(a, s);
+      case FS_STORAGE_F16:
+        return a.level == 0 ? launch_img_stream<__half, true>(a, s) : launch_img_stream<__half, false>(a, s);
+      case FS_STORAGE_BF16:
+        return a.level == 0 ? launch_img_stream<__nv_bfloat16, true>(a, s)
+                            : launch_img_stream<__nv_bfloat16, false>(a, s);
+      default:
+        return cudaErrorInvalidValue;
+    }
+  }
   return a.level == 0 ? launch_split<ImgK, true>(a, storage, s, cfg0)
                       : launch_split<ImgK, false>(a, storage, s, cfg1);
 }

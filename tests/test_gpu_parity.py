@@ -299,6 +299,26 @@ def test_pass2_modes_give_identical_results(torch, ctx):
     for m in ("cache", "resident", "refetch"):
         assert np.array_equal(results["laps"], results[m]), m
 
+@pytest.mark.parametrize("storage", [fsb.STORAGE_F32, fsb.STORAGE_F16, fsb.STORAGE_BF16])
+def test_laps_large_levels_match_cache(torch, ctx, storage):
+    # levels wider than 512 take the streaming pyramid kernel in laps mode;
+    # odd, non-multiple-of-4 level sizes exercise its edge columns and rows
+    W, H, F = 1203, 917, 4
+    frames, poses = synth_stack(torch, ctx, W, H, F, seed=21)
+    roi = fsb.compute_common_overlap_roi([True] * F, [W] * F, [H] * F, poses)
+    assert max(roi.width, roi.height) > 1024
+    results = {}
+    for mode in ("laps", "cache"):
+        st = fsb.PyramidContrastStack(ctx, W, H, F, roi=roi, frames_per_batch=3, level_storage=storage,
+                                      pass2_mode=mode)
+        assert st.pass2_mode == mode
+        for f, p in zip(frames, poses):
+            st.add_frame(f, p)
+        results[mode] = st.finish()
+        st.close()
+    assert np.array_equal(results["laps"], results["cache"])
+
+
 def test_stack_errors(torch, ctx):
     W, H = 64, 48
     frames, poses = synth_stack(torch, ctx, W, H, 2, seed=2)
