@@ -1215,15 +1215,15 @@ cudaError_t launch_mask_reduce(const MaskReduceArgs& a, int frames, int in_stora
 // One frame's pyramid step l -> l + 1 for the levels whose EXPAND clamps
 // (exact_expand == 0), without shared memory: each lane owns the level-(l+1)
 // column pair J0 = 2p, J1 = 2p + 1 and the level-l columns c = 4p .. 4p + 3,
-// and walks down a strip of kImgRows level-(l+1) rows.  A five-row window of
-// horizontal REDUCE sums (level-l rows 2r - 2 .. 2r + 2) gives level-(l+1)
-// row r; the EXPAND's horizontal pass takes the neighbouring columns J0 - 1
+// and walks down a strip of level-(l+1) rows.  Horizontal REDUCE sums of
+// level-l rows 2r - 2 .. 2r + 2, added up in tap order as they arrive, give
+// level-(l+1) row r; the EXPAND's horizontal pass takes the neighbouring columns J0 - 1
 // and J1 + 1 from the adjacent lanes (shuffles), so lanes 0 and 31 of a warp
 // only feed their neighbours and kImgPairs lanes emit.  The Laplacian of
 // level-l rows 2q, 2q + 1 is emitted once row q + 1 is known.  Products and
 // sums are those of reduce_image_step and expand_blend_step (clamped mode),
 // in their order.
-constexpr int kImgRows = 32, kImgWarps = 4, kImgPairs = 30;
+constexpr int kImgWarps = 4, kImgPairs = 30;
 
 // Horizontal REDUCE sums (v0, v1, v2, weight) of level-l row y for the lane's
 // two level-(l+1) columns; samples outside the level count as zero.
@@ -1294,8 +1294,13 @@ __device__ __forceinline__ void img_row(const LevelArgs& a, int k, int y, int c,
   }
 }
 
+// One vertical REDUCE tap: v = fma(w, row, v) on value and weight sums.
+__device__ __forceinline__ float4 vtap(float w, float4 t, float4 v) {
+  return make_float4(fmaf(w, t.x, v.x), fmaf(w, t.y, v.y), fmaf(w, t.z, v.z), fmaf(w, t.w, v.w));
+}
+
 template <typename T, bool L0>
-__global__ void __launch_bounds__(32 * kImgWarps) img_stream_kernel(const __grid_constant__ LevelArgs a) {
+__global__ void __launch_bounds__(32 * kImgWarps) img_stream_kernel(const __grid_constant__ LevelArgs a, int rows) {
   const int lane = (int)threadIdx.x, k = (int)blockIdx.z;
   const int first = ((int)blockIdx.x * kImgWarps + (int)threadIdx.y) * kImgPairs;  // pair of lane 1
   if (2 * first >= a.wn) return;  // the whole warp: none of its pairs is in the level
@@ -1304,41 +1309,56 @@ __global__ void __launch_bounds__(32 * kImgWarps) img_stream_kernel(const __grid
   const bool live = p >= 0 && J0 < a.wn;
   const bool emit = live && lane >= 1 && lane <= kImgPairs;
   const bool j1in = J0 + 1 < a.wn, rin = J0 + 2 < a.wn;
-  const int i0 = (int)blockIdx.y * kImgRows;
-  const int i1 = min(i0 + kImgRows, a.hn);
-  float4 win[5][2];
+  const int i0 = (int)blockIdx.y * rows;
+  const int i1 = min(i0 + rows, a.hn);
+  const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
+  // vertical REDUCE sums in tap order (level-l rows 2r - 2 .. 2r + 2 for
+  // level-(l+1) row r): cur = row r with taps 0 .. 2, nxt = row r + 1 with
+  // tap 0; the level-l rows 2r + 1, 2r + 2 complete cur, advance nxt and
+  // start row r + 2
+  float4 cur[2], nxt[2];
   float Hm2[3][4], Hm1[3][4], Hc[3][4];
 #pragma unroll
   for (int ch = 0; ch < 3; ++ch)
 #pragma unroll
     for (int u = 0; u < 4; ++u) Hm2[ch][u] = Hm1[ch][u] = 0.0f;
   int r = i0 > 0 ? i0 - 1 : 0;
+  {
+    float4 t0[2], t1[2], t2[2];
+    img_row<T, L0>(a, k, 2 * r - 2, c, live, t0);
+    img_row<T, L0>(a, k, 2 * r - 1, c, live, t1);
+    img_row<T, L0>(a, k, 2 * r, c, live, t2);
 #pragma unroll
-  for (int u = 0; u < 3; ++u) img_row<T, L0>(a, k, 2 * r - 2 + u, c, live, win[u]);
+    for (int h = 0; h < 2; ++h) {
+      cur[h] = vtap(kw(2), t2[h], vtap(kw(1), t1[h], vtap(kw(0), t0[h], zero)));
+      nxt[h] = vtap(kw(0), t2[h], zero);
+    }
+  }
   for (; r <= i1; ++r) {
-    img_row<T, L0>(a, k, 2 * r + 1, c, live, win[3]);
-    img_row<T, L0>(a, k, 2 * r + 2, c, live, win[4]);
+    float4 fin[2];
+    {
+      float4 t3[2], t4[2];
+      img_row<T, L0>(a, k, 2 * r + 1, c, live, t3);
+      img_row<T, L0>(a, k, 2 * r + 2, c, live, t4);
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        fin[h] = vtap(kw(4), t4[h], vtap(kw(3), t3[h], cur[h]));
+        cur[h] = vtap(kw(2), t4[h], vtap(kw(1), t3[h], nxt[h]));
+        nxt[h] = vtap(kw(0), t4[h], zero);
+      }
+    }
     if (r < a.hn) {  // warp-uniform
       // REDUCE: level-(l+1) row r, columns J0, J0 + 1
       float g[2][3];
       bool sp[2];
 #pragma unroll
       for (int h = 0; h < 2; ++h) {
-        float v0 = 0.f, v1 = 0.f, v2 = 0.f, ws = 0.f;
-#pragma unroll
-        for (int ky = 0; ky < 5; ++ky) {
-          const float4 t = win[ky][h];
-          const float w = kw(ky);
-          v0 = fmaf(w, t.x, v0);
-          v1 = fmaf(w, t.y, v1);
-          v2 = fmaf(w, t.z, v2);
-          ws = fmaf(w, t.w, ws);
-        }
+        const float ws = fin[h].w;
         sp[h] = live && J0 + h < a.wn && ws > 0.f;
         const float rc = sp[h] ? __fdividef(1.0f, ws) : 0.0f;
-        g[h][0] = v0 * rc;
-        g[h][1] = v1 * rc;
-        g[h][2] = v2 * rc;
+        g[h][0] = fin[h].x * rc;
+        g[h][1] = fin[h].y * rc;
+        g[h][2] = fin[h].z * rc;
       }
       if (emit && r >= i0 && r < i1) {
         const LevelPlanes& out = a.out[k];
@@ -1425,21 +1445,20 @@ __global__ void __launch_bounds__(32 * kImgWarps) img_stream_kernel(const __grid
         Hm2[ch][u] = Hm1[ch][u];
         Hm1[ch][u] = Hc[ch][u];
       }
-#pragma unroll
-    for (int u = 0; u < 3; ++u) {
-      win[u][0] = win[u + 2][0];
-      win[u][1] = win[u + 2][1];
-    }
   }
 }
 
+// Rows per strip: 32, halved (down to 8) while the grid would give fewer
+// than 8 CTAs per SM.
 template <typename T, bool L0>
 static cudaError_t launch_img_stream(const LevelArgs& a, cudaStream_t s) {
   const int pairs = (a.wn + 1) / 2;
   const int warps = (pairs + kImgPairs - 1) / kImgPairs;
-  const dim3 grid((unsigned)((warps + kImgWarps - 1) / kImgWarps), (unsigned)((a.hn + kImgRows - 1) / kImgRows),
-                  (unsigned)a.K);
-  img_stream_kernel<T, L0><<<grid, dim3(32, kImgWarps), 0, s>>>(a);
+  const int bx = (warps + kImgWarps - 1) / kImgWarps;
+  int rows = 32;
+  while (rows > 8 && (int64_t)bx * ((a.hn + rows - 1) / rows) * a.K < 8 * 148) rows /= 2;
+  const dim3 grid((unsigned)bx, (unsigned)((a.hn + rows - 1) / rows), (unsigned)a.K);
+  img_stream_kernel<T, L0><<<grid, dim3(32, kImgWarps), 0, s>>>(a, rows);
   return cudaGetLastError();
 }
 
