@@ -263,22 +263,37 @@ __device__ __forceinline__ bool sample_try(const SrcImage& s, const Anchor& a, i
   load_rgb_biased(s, x0 + 1, y0, v10);
   load_rgb_biased(s, x0, y0 + 1, v01);
   load_rgb_biased(s, x0 + 1, y0 + 1, v11);
-  float fxy = fx * fy;
-  uint32_t o[3];
-  float dmax = 0.0f;
-#pragma unroll
-  for (int c = 0; c < 3; ++c) {
-    float d10 = v10[c] - v00[c], d01 = v01[c] - v00[c], d11 = (v11[c] - v10[c]) - d01;
-    float v = fmaf(fx, d10, v00[c] - 8388608.0f);
-    v = fmaf(fy, d01, v);
-    v = fmaf(fxy, d11, v);
-    float d;
-    o[c] = round_near_u8(v, &d);
-    dmax = fmaxf(dmax, d);
+  const float fxy = fx * fy;
+  // red and green as FP32 pairs (each lane of a pair rounds exactly like the
+  // scalar operation: a - b is fma(b, -1, a)), blue alone; the same
+  // operations in the same order as sample_fast
+  const float2 m1 = make_float2(-1.0f, -1.0f);
+  const float2 a00 = make_float2(v00[0], v00[1]), a10 = make_float2(v10[0], v10[1]);
+  const float2 a01 = make_float2(v01[0], v01[1]), a11 = make_float2(v11[0], v11[1]);
+  const float2 d10 = __ffma2_rn(a00, m1, a10), d01 = __ffma2_rn(a00, m1, a01);
+  const float2 d11 = __ffma2_rn(d01, m1, __ffma2_rn(a10, m1, a11));
+  float2 v = __fadd2_rn(a00, make_float2(-8388608.0f, -8388608.0f));
+  v = __ffma2_rn(make_float2(fx, fx), d10, v);
+  v = __ffma2_rn(make_float2(fy, fy), d01, v);
+  v = __ffma2_rn(make_float2(fxy, fxy), d11, v);
+  float vb;
+  {
+    const float e10 = v10[2] - v00[2], e01 = v01[2] - v00[2], e11 = (v11[2] - v10[2]) - e01;
+    vb = fmaf(fx, e10, v00[2] - 8388608.0f);
+    vb = fmaf(fy, e01, vb);
+    vb = fmaf(fxy, e11, vb);
   }
-  const bool tie = dmax > 0.5f - kTieBand;
-  if (tie) return false;
-  *out = pack_rgba(o[0], o[1], o[2], 255u);
+  // nearest integers by adding and removing 1.5 * 2^23: t's low byte is the
+  // integer (a bilinear value of bytes lies in [0, 255] up to ~1e-4)
+  const float2 M = make_float2(12582912.0f, 12582912.0f);
+  const float2 t = __fadd2_rn(v, M);
+  const float2 dl = __ffma2_rn(__fadd2_rn(t, make_float2(-12582912.0f, -12582912.0f)), m1, v);
+  const float tb = __fadd_rn(vb, 12582912.0f);
+  const float db = __fsub_rn(vb, __fsub_rn(tb, 12582912.0f));
+  const float dmax = fmaxf(fmaxf(fabsf(dl.x), fabsf(dl.y)), fabsf(db));
+  if (dmax > 0.5f - kTieBand) return false;
+  const uint32_t rg = __byte_perm(__float_as_uint(t.x), __float_as_uint(t.y), 0x0040u);
+  *out = __byte_perm(rg, __float_as_uint(tb), 0x0410u) | 0xFF000000u;
   return true;
 }
 
