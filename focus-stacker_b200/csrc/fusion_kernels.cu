@@ -184,7 +184,7 @@ struct RWLayout {
 };
 
 template <int B>
-__global__ void __launch_bounds__(NT, 4) remap_weights_kernel(const __grid_constant__ RemapWeightArgs a) {
+__global__ void __launch_bounds__(NT, 5) remap_weights_kernel(const __grid_constant__ RemapWeightArgs a) {
   using Lay = RWLayout<B>;
   constexpr int RW = Lay::RW, RH = Lay::RH, KS = Lay::KS, HS = Lay::HS;
   extern __shared__ __align__(16) uint8_t smem[];
@@ -1294,10 +1294,75 @@ __device__ __forceinline__ void img_row(const LevelArgs& a, int k, int y, int c,
   }
 }
 
-// One vertical REDUCE tap: v = fma(w, row, v) on value and weight sums.
-__device__ __forceinline__ float4 vtap(float w, float4 t, float4 v) {
-  return make_float4(fmaf(w, t.x, v.x), fmaf(w, t.y, v.y), fmaf(w, t.z, v.z), fmaf(w, t.w, v.w));
+// Level 0 in integers: the samples are bytes and the weights 1, 4, 6 (or 0
+// without support), so every partial sum of the FP32 REDUCE is an integer
+// below 2^16 and exact; the integer sums equal it bit for bit.  Horizontal
+// sums of one row for the lane's two columns: the channel bytes of taps
+// 0..3 gathered into one word each and dot-multiplied with the tap weights
+// (zeroed where alpha is 0), plus tap 4.
+__device__ __forceinline__ void img_row_u8(const LevelArgs& a, int k, int y, int c, bool live, int4 (&hs)[2]) {
+  uint32_t w[7] = {0u, 0u, 0u, 0u, 0u, 0u, 0u};
+  if (live && y >= 0 && y < a.hl) {
+    const uint32_t* row = a.in0[k].rgba + (int64_t)y * a.pitch_l;
+    const uint4 q4 = *reinterpret_cast<const uint4*>(row + c);  // inside the row's pitch
+    w[2] = q4.x;
+    w[3] = q4.y;
+    w[4] = q4.z;
+    w[5] = q4.w;
+    if (c + 3 >= a.wl) {  // words past the level's last column
+#pragma unroll
+      for (int u = 2; u < 6; ++u)
+        if (c + u - 2 >= a.wl) w[u] = 0u;
+    }
+    if (c > 0) {
+      const uint2 q2 = *reinterpret_cast<const uint2*>(row + c - 2);
+      w[0] = q2.x;
+      w[1] = q2.y;
+    }
+    if (c + 4 < a.wl) w[6] = row[c + 4];
+  }
+  constexpr uint32_t kW = 0x04060401u;  // tap weights 1, 4, 6, 4 (tap 4: 1)
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const uint32_t b0 = w[2 * h], b1 = w[2 * h + 1], b2 = w[2 * h + 2], b3 = w[2 * h + 3], b4 = w[2 * h + 4];
+    const uint32_t al = __byte_perm(__byte_perm(b0, b1, 0x0073u), __byte_perm(b2, b3, 0x0073u), 0x5410u);
+    const uint32_t wt = __vcmpne4(al, 0u) & kW;
+    const bool s4 = (b4 >> 24) != 0u;
+    int v[3];
+#pragma unroll
+    for (int ch = 0; ch < 3; ++ch) {
+      const uint32_t sel = (uint32_t)ch | ((uint32_t)(4 + ch) << 4);
+      const uint32_t g = __byte_perm(__byte_perm(b0, b1, sel), __byte_perm(b2, b3, sel), 0x5410u);
+      v[ch] = (int)__dp4a(g, wt, s4 ? (b4 >> (8 * ch)) & 0xffu : 0u);
+    }
+    hs[h] = make_int4(v[0], v[1], v[2], (int)__dp4a(wt, 0x01010101u, s4 ? 1u : 0u));
+  }
 }
+
+// One vertical REDUCE tap: v = fma(w, row, v) on value and weight sums
+// (integer sums at level 0).
+__device__ __forceinline__ float4 vtap(int w, float4 t, float4 v) {
+  const float f = (float)w;
+  return make_float4(fmaf(f, t.x, v.x), fmaf(f, t.y, v.y), fmaf(f, t.z, v.z), fmaf(f, t.w, v.w));
+}
+__device__ __forceinline__ int4 vtap(int w, int4 t, int4 v) {
+  return make_int4(v.x + w * t.x, v.y + w * t.y, v.z + w * t.z, v.w + w * t.w);
+}
+template <class A> __device__ __forceinline__ A acc_zero();
+template <> __device__ __forceinline__ float4 acc_zero<float4>() { return make_float4(0.f, 0.f, 0.f, 0.f); }
+template <> __device__ __forceinline__ int4 acc_zero<int4>() { return make_int4(0, 0, 0, 0); }
+// exact float of a non-negative integer below 2^23
+__device__ __forceinline__ float small_int_float(int v) { return __int_as_float(0x4B000000 | v) - 8388608.0f; }
+__device__ __forceinline__ float4 acc_float(float4 v) { return v; }
+__device__ __forceinline__ float4 acc_float(int4 v) {
+  return make_float4(small_int_float(v.x), small_int_float(v.y), small_int_float(v.z), small_int_float(v.w));
+}
+template <typename T, bool L0, class A>
+__device__ __forceinline__ void row_sums(const LevelArgs& a, int k, int y, int c, bool live, A (&hs)[2]) {
+  if constexpr (L0) img_row_u8(a, k, y, c, live, hs);
+  else img_row<T, false>(a, k, y, c, live, hs);
+}
+__device__ __forceinline__ int kwi(int i) { return (i == 0 || i == 4) ? 1 : ((i == 1 || i == 3) ? 4 : 6); }
 
 template <typename T, bool L0>
 __global__ void __launch_bounds__(32 * kImgWarps) img_stream_kernel(const __grid_constant__ LevelArgs a, int rows) {
@@ -1311,12 +1376,13 @@ __global__ void __launch_bounds__(32 * kImgWarps) img_stream_kernel(const __grid
   const bool j1in = J0 + 1 < a.wn, rin = J0 + 2 < a.wn;
   const int i0 = (int)blockIdx.y * rows;
   const int i1 = min(i0 + rows, a.hn);
-  const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
+  using Acc = typename std::conditional<L0, int4, float4>::type;
+  const Acc zero = acc_zero<Acc>();
   // vertical REDUCE sums in tap order (level-l rows 2r - 2 .. 2r + 2 for
   // level-(l+1) row r): cur = row r with taps 0 .. 2, nxt = row r + 1 with
   // tap 0; the level-l rows 2r + 1, 2r + 2 complete cur, advance nxt and
   // start row r + 2
-  float4 cur[2], nxt[2];
+  Acc cur[2], nxt[2];
   float Hm2[3][4], Hm1[3][4], Hc[3][4];
 #pragma unroll
   for (int ch = 0; ch < 3; ++ch)
@@ -1324,27 +1390,27 @@ __global__ void __launch_bounds__(32 * kImgWarps) img_stream_kernel(const __grid
     for (int u = 0; u < 4; ++u) Hm2[ch][u] = Hm1[ch][u] = 0.0f;
   int r = i0 > 0 ? i0 - 1 : 0;
   {
-    float4 t0[2], t1[2], t2[2];
-    img_row<T, L0>(a, k, 2 * r - 2, c, live, t0);
-    img_row<T, L0>(a, k, 2 * r - 1, c, live, t1);
-    img_row<T, L0>(a, k, 2 * r, c, live, t2);
+    Acc t0[2], t1[2], t2[2];
+    row_sums<T, L0>(a, k, 2 * r - 2, c, live, t0);
+    row_sums<T, L0>(a, k, 2 * r - 1, c, live, t1);
+    row_sums<T, L0>(a, k, 2 * r, c, live, t2);
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
-      cur[h] = vtap(kw(2), t2[h], vtap(kw(1), t1[h], vtap(kw(0), t0[h], zero)));
-      nxt[h] = vtap(kw(0), t2[h], zero);
+      cur[h] = vtap(kwi(2), t2[h], vtap(kwi(1), t1[h], vtap(kwi(0), t0[h], zero)));
+      nxt[h] = vtap(kwi(0), t2[h], zero);
     }
   }
   for (; r <= i1; ++r) {
     float4 fin[2];
     {
-      float4 t3[2], t4[2];
-      img_row<T, L0>(a, k, 2 * r + 1, c, live, t3);
-      img_row<T, L0>(a, k, 2 * r + 2, c, live, t4);
+      Acc t3[2], t4[2];
+      row_sums<T, L0>(a, k, 2 * r + 1, c, live, t3);
+      row_sums<T, L0>(a, k, 2 * r + 2, c, live, t4);
 #pragma unroll
       for (int h = 0; h < 2; ++h) {
-        fin[h] = vtap(kw(4), t4[h], vtap(kw(3), t3[h], cur[h]));
-        cur[h] = vtap(kw(2), t4[h], vtap(kw(1), t3[h], nxt[h]));
-        nxt[h] = vtap(kw(0), t4[h], zero);
+        fin[h] = acc_float(vtap(kwi(4), t4[h], vtap(kwi(3), t3[h], cur[h])));
+        cur[h] = vtap(kwi(2), t4[h], vtap(kwi(1), t3[h], nxt[h]));
+        nxt[h] = vtap(kwi(0), t4[h], zero);
       }
     }
     if (r < a.hn) {  // warp-uniform
