@@ -13,9 +13,9 @@ pass 2, collapse and quantise.
   e2e    the same metric through the public API from pinned host frames: the
          host->device copy of every frame and the device->host copy of the
          fused output are inside the timed region.  Stacks run back to back
-         with --e2e-lanes of them in flight (one context each), so that the
-         next stack's uploads overlap the previous stack's pass 2; the
-         latency of one stack alone is reported beside it.
+         on one context, two in flight: each stack's pass 2, collapse and
+         D2H (finish_into_async) run while the next stack's frames upload;
+         the latency of one stack alone is reported beside it.
 
 `--impl reference` times the CPU oracle (the C++ restatement of the
 reference's Zig path; the Zig reference cannot be built in this image) on
@@ -62,9 +62,6 @@ def parse():
     ap.add_argument("--batch", type=int, default=0, help="frames per pass over per-pixel state (0 = library default)")
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--e2e-lanes", type=int, default=1,
-                    help="stacks in flight in the e2e leg (each on its own context): the next stack's uploads "
-                         "overlap the previous stack's pass 2")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-forms", action="store_true", help="skip the precision / serving / batched legs")
     ap.add_argument("--precision-frames", type=int, default=143,
@@ -562,58 +559,57 @@ def main():
             h = torch.empty(f.shape, dtype=torch.uint8, pin_memory=True)
             h.copy_(f)
             hframes.append(h.numpy())
-        lanes = max(1, args.e2e_lanes)
-        ctxs = [ctx] + [fsb.Context(dev) for _ in range(lanes - 1)]
         houts = [torch.empty((roi.height, roi.width, 3), dtype=torch.uint8, pin_memory=True).numpy()
-                 for _ in range(lanes)]
+                 for _ in range(2)]
 
-        def step_e2e(lane=0):
-            st = fsb.PyramidContrastStack(ctxs[lane], W, H, F, roi=roi, frames_per_batch=args.batch)
+        def new_stack(i):
+            st = fsb.PyramidContrastStack(ctx, W, H, F, roi=roi, frames_per_batch=args.batch)
             for f, p in zip(hframes, poses):
                 st.add_frame(f, p)
-            st.finish_into(houts[lane])
+            return st
+
+        def run_stacks(n):
+            # stack i's pass 2, collapse and D2H run while stack i + 1's
+            # frames upload: finish_into_async, then wait on the previous one
+            prev = None
+            for i in range(n):
+                st = new_stack(i)
+                st.finish_into_async(houts[i % 2])
+                if prev is not None:
+                    prev.wait()
+                    prev.close()
+                prev = st
+            prev.wait()
+            prev.close()
+
+        def single_stack():
+            st = new_stack(0)
+            st.finish_into(houts[0])
             st.close()
 
-        for lane in range(lanes):
-            step_e2e(lane)
+        run_stacks(2)
         # latency of one stack alone
+        single_stack()
         t0 = time.perf_counter()
         for _ in range(2):
-            step_e2e()
+            single_stack()
         lat = (time.perf_counter() - t0) / 2
-        # stacks back to back, `lanes` in flight: every step still uploads its
-        # frames from pinned host memory and reads its fused result back
-        n_e2e = max(lanes, min(args.steps, 4) * lanes)
-        errors = []
-
-        def lane_worker(lane):
-            try:
-                for _ in range(n_e2e // lanes):
-                    step_e2e(lane)
-            except BaseException as exc:  # reported below
-                errors.append(exc)
-
+        # stacks back to back: every step still uploads its frames from pinned
+        # host memory and reads its fused result back
+        n_e2e = max(3, min(args.steps, 6))
         if dist:
             dist.barrier()
         t0 = time.perf_counter()
-        threads = [threading.Thread(target=lane_worker, args=(lane,)) for lane in range(lanes)]
-        for th in threads:
-            th.start()
-        for th in threads:
-            th.join()
+        run_stacks(n_e2e)
         dt = (time.perf_counter() - t0) / n_e2e
-        if errors:
-            raise errors[0]
         if dist:
             t = torch.tensor([dt, lat], device=f"cuda:{dev}")
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             dt, lat = float(t[0].item()), float(t[1].item())
         e2e = {"value": world * px / dt / 1e6, "unit": UNIT, "h2d_bytes_per_step": F * W * H * 3,
                "d2h_bytes_per_step": roi.width * roi.height * 3, "ms_per_step": dt * 1e3,
-               "stacks_in_flight": lanes, "steps": n_e2e, "single_stack_latency_ms": lat * 1e3,
+               "stacks_in_flight": 2, "steps": n_e2e, "single_stack_latency_ms": lat * 1e3,
                "single_stack_value": world * px / lat / 1e6}
-        for c in ctxs[1:]:
-            c.close()
         del hframes
 
     forms = None

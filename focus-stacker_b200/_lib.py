@@ -27,7 +27,7 @@ EXPORTED = (
     "fs_pose_default", "fs_compute_roi", "fs_inverse_map_points", "fs_forward_map_points", "fs_exact_expand_divisor",
     "fs_remap_frame", "fs_remap_frame_device",
     "fs_stack_begin", "fs_stack_add_frame", "fs_stack_add_frame_device", "fs_stack_finish",
-    "fs_stack_finish_device", "fs_stack_set_base_output", "fs_stack_pass2_mode", "fs_stack_footprint", "fs_stack_mode_bytes", "fs_stack_begin_mode",
+    "fs_stack_finish_device", "fs_stack_finish_async", "fs_stack_wait", "fs_stack_set_base_output", "fs_stack_pass2_mode", "fs_stack_footprint", "fs_stack_mode_bytes", "fs_stack_begin_mode",
     "fs_stack_set_frame_total", "fs_stack_end_pass1", "fs_stack_blend", "fs_stack_collapse", "fs_stack_buffer", "fs_stack_output_size", "fs_stack_destroy", "fs_fuse_stack",
     "fs_batch_create", "fs_batch_run", "fs_batch_stack_count", "fs_batch_pass2_mode", "fs_batch_uses_graph",
     "fs_batch_destroy",
@@ -112,6 +112,8 @@ def _bind(L):
     L.fs_stack_add_frame_device.argtypes = [vp, vp, sz, P(FsPose)]
     L.fs_stack_finish.argtypes = [vp, FETCH_CB, vp, vp, sz]
     L.fs_stack_finish_device.argtypes = [vp, FETCH_CB, vp, vp, sz]
+    L.fs_stack_finish_async.argtypes = [vp, FETCH_CB, vp, vp, sz]
+    L.fs_stack_wait.argtypes = [vp]
     L.fs_stack_output_size.argtypes = [vp, P(u32), P(u32)]
     L.fs_stack_set_base_output.argtypes = [vp, vp, sz]
     L.fs_stack_pass2_mode.argtypes = [vp]

@@ -398,6 +398,19 @@ class PyramidContrastStack:
         cb = self._make_cb(refetch)
         _check(L().fs_stack_finish_device(self.handle, cb, None, _ptr(dst), dst_stride), self.ctx.handle)
 
+    def finish_into_async(self, out: np.ndarray, refetch=None):
+        """Queue pass 2, the collapse and the copy of the fused image into
+        `out` (best pinned host memory) and return; `wait()` blocks until the
+        image is there.  The next stack on the same context can be fed in the
+        meantime, so that its uploads overlap this stack's pass 2."""
+        cb = self._make_cb(refetch)
+        self._keep.append(out)
+        rc = L().fs_stack_finish_async(self.handle, cb, None, out.ctypes.data, out.strides[0])
+        _check(rc, self.ctx.handle)
+
+    def wait(self):
+        _check(L().fs_stack_wait(self.handle), self.ctx.handle)
+
     # ---------------------------------------------- phases (frame shards)
     def set_frame_total(self, frame_total: int):
         """Frames of the whole stack when this one holds a shard of them."""

@@ -218,6 +218,7 @@ struct fs_stack {
   size_t pass1_done = 0;          // frames whose pass 1 has been launched
   bool finished = false;
   cudaEvent_t copy_done = nullptr;
+  cudaEvent_t done = nullptr;     // recorded after the output copy of fs_stack_finish_async
   std::vector<cudaEvent_t> slot_done;  // per staging buffer: the remap that last read it
   float* base_out = nullptr;      // optional device buffer for the collapsed base (RGB f32)
   uint32_t fp_level = 0;          // first level run one frame per CTA (none: >= L - 1)
@@ -239,10 +240,12 @@ void detach_stack(fs_stack* s) {
   for (auto& a : s->allocs) dev_free(s->ctx, a.p, a.bytes);
   s->allocs.clear();
   if (s->copy_done) cudaEventDestroy(s->copy_done);
+  if (s->done) cudaEventDestroy(s->done);
   for (cudaEvent_t& ev : s->slot_done)
     if (ev) cudaEventDestroy(ev), ev = nullptr;
   s->slot_done.clear();
   s->copy_done = nullptr;
+  s->done = nullptr;
   s->ctx = nullptr;
 }
 
@@ -966,8 +969,10 @@ int fs_stack_add_frame_device(fs_stack* stack, const void* dev_pixels, size_t ro
 static int pass2_impl(fs_stack* s, fs_frame_fetch_cb refetch, void* user);
 static int collapse_impl(fs_stack* s, void* out, size_t out_stride, bool device_out, bool wait);
 
+// wait: block until the output is written; mark_done: record the stack's
+// done event after the output copy (fs_stack_finish_async / fs_stack_wait).
 static int finish_impl(fs_stack* s, fs_frame_fetch_cb refetch, void* user, void* out, size_t out_stride,
-                       bool device_out, bool wait = true) {
+                       bool device_out, bool wait = true, bool mark_done = false) {
   if (!s || !out) return FS_ERR_INVALID;
   if (!s->ctx) return FS_ERR_STATE;  // its context was destroyed
   fs_ctx* ctx = s->ctx;
@@ -986,6 +991,11 @@ static int finish_impl(fs_stack* s, fs_frame_fetch_cb refetch, void* user, void*
     s->phase = 2;
   }
   if ((rc = collapse_impl(s, out, out_stride, device_out, wait)) != FS_OK) return rc;
+  if (mark_done) {
+    cudaError_t e = s->done ? cudaSuccess : cudaEventCreateWithFlags(&s->done, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventRecord(s->done, ctx->stream);
+    if (e != cudaSuccess) return cuda_err(ctx, e, "finish event");
+  }
   s->finished = true;
   return FS_OK;
 }
@@ -1281,6 +1291,22 @@ int fs_stack_finish_device(fs_stack* stack, fs_frame_fetch_cb refetch, void* use
   return finish_impl(stack, refetch, user, dev_out, out_stride, true);
 }
 
+int fs_stack_finish_async(fs_stack* stack, fs_frame_fetch_cb refetch, void* user, void* out_pixels,
+                          size_t out_stride) {
+  return finish_impl(stack, refetch, user, out_pixels, out_stride, false, false, true);
+}
+
+int fs_stack_wait(fs_stack* s) {
+  if (!s) return FS_ERR_INVALID;
+  if (!s->ctx) return FS_ERR_STATE;
+  if (!s->finished) return set_err(s->ctx, FS_ERR_STATE, "stack not finished");
+  if (!s->done) return FS_OK;  // finished synchronously
+  cudaSetDevice(s->ctx->device);
+  const cudaError_t e = cudaEventSynchronize(s->done);
+  if (e != cudaSuccess) return cuda_err(s->ctx, e, "fusion");
+  return FS_OK;
+}
+
 int fs_stack_set_base_output(fs_stack* s, float* dev_base, size_t row_stride_elems) {
   if (!s) return FS_ERR_INVALID;
   if (!s->ctx) return FS_ERR_STATE;
@@ -1301,8 +1327,15 @@ int fs_stack_destroy(fs_stack* s) {
   if (!s) return FS_ERR_INVALID;
   if (fs_ctx* ctx = s->ctx) {
     cudaSetDevice(ctx->device);
-    cudaStreamSynchronize(ctx->stream);
-    cudaStreamSynchronize(ctx->copy);
+    if (s->done) {
+      // finished asynchronously: its last work is the output copy, and the
+      // stream-ordered frees below follow it (later stacks' work queued on
+      // the streams need not drain)
+      cudaEventSynchronize(s->done);
+    } else {
+      cudaStreamSynchronize(ctx->stream);
+      cudaStreamSynchronize(ctx->copy);
+    }
     for (auto& a : s->allocs) dev_free(ctx, a.p, a.bytes);
     s->allocs.clear();
     ctx->stacks.erase(s);

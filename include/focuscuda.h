@@ -188,6 +188,18 @@ int fs_stack_finish(fs_stack* stack, fs_frame_fetch_cb refetch, void* user, void
 /* Same with a device output buffer. */
 int fs_stack_finish_device(fs_stack* stack, fs_frame_fetch_cb refetch, void* user, void* dev_out, size_t out_stride);
 
+/* fs_stack_finish without the wait: pass 2, the collapse and the copy of the
+ * fused image into `out_pixels` (pinned host memory, or any host memory the
+ * caller keeps alive) are queued on the context's stream and the call
+ * returns; fs_stack_wait blocks until the image is in `out_pixels`.  The next
+ * stack of the same context can be begun and fed meanwhile, so that its
+ * frame uploads overlap this stack's pass 2 (the reference fuses stacks one
+ * after another; this is the pipelined form of fs_stack_finish).
+ * fs_stack_destroy waits for this stack's work only. */
+int fs_stack_finish_async(fs_stack* stack, fs_frame_fetch_cb refetch, void* user, void* out_pixels,
+                          size_t out_stride);
+int fs_stack_wait(fs_stack* stack);
+
 /* Optional: also write the collapsed level-0 base before quantisation
  * (interleaved RGB FP32, device memory, row stride in elements) during
  * finish.  Used to measure error against FP64 evaluations on the 16-bit

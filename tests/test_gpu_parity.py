@@ -347,6 +347,41 @@ def test_stack_errors(torch, ctx):
     assert e.value.code == "FS_ERR_BUDGET"
 
 
+def test_pipelined_finish_matches_sync(torch, ctx):
+    # stack A's pass 2 is queued (finish_into_async) while stack B's frames
+    # upload on the same context; both images equal the synchronous ones
+    W, H, F = 640, 480, 5
+    frames_a, poses_a = synth_stack(torch, ctx, W, H, F, seed=31)
+    frames_b, poses_b = synth_stack(torch, ctx, W, H, F, seed=32)
+    roi = fsb.compute_common_overlap_roi([True] * F, [W] * F, [H] * F, poses_a)
+    roi_b = fsb.compute_common_overlap_roi([True] * F, [W] * F, [H] * F, poses_b)
+
+    def sync(frames, poses, r):
+        st = fsb.PyramidContrastStack(ctx, W, H, F, roi=r)
+        for f, p in zip(frames, poses):
+            st.add_frame(f, p)
+        out = st.finish()
+        st.close()
+        return out
+
+    ref_a, ref_b = sync(frames_a, poses_a, roi), sync(frames_b, poses_b, roi_b)
+    out_a = np.zeros_like(ref_a)
+    out_b = np.zeros_like(ref_b)
+    a = fsb.PyramidContrastStack(ctx, W, H, F, roi=roi)
+    for f, p in zip(frames_a, poses_a):
+        a.add_frame(f, p)
+    a.finish_into_async(out_a)
+    b = fsb.PyramidContrastStack(ctx, W, H, F, roi=roi_b)
+    for f, p in zip(frames_b, poses_b):
+        b.add_frame(f, p)
+    a.wait()
+    a.close()
+    b.finish_into_async(out_b)
+    b.close()  # waits for its own work
+    assert np.array_equal(out_a, ref_a)
+    assert np.array_equal(out_b, ref_b)
+
+
 def test_stack_outliving_its_context(torch):
     # destroying a context releases its stacks' device memory; the stack
     # handles stay valid for fs_stack_destroy and report a state error
