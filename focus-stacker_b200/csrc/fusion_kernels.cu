@@ -103,6 +103,28 @@ struct __align__(16) ExactQueue {
   uint32_t item[kExactQueue];  // ry << 16 | rx
 };
 
+// The FP64 anchors of a region's 8x4 blocks into shared memory, one per
+// thread from thread `first` on, and the exact queue emptied.  The kernel
+// runs it for the next frame while the current one's window sums are formed
+// (the anchors are last read by the current frame's fast pass).
+template <int RW, int RH>
+__device__ __forceinline__ void region_anchors(const FrameIn& f, int rx0, int ry0, ExactQueue* q, int first) {
+  constexpr int NBX = (RW + 7) / 8, NBY = (RH + 3) / 4, NB = NBX * NBY;
+  static_assert(NB <= kMaxAnchors && NB <= NT, "anchor table too small");
+  if (f.warp.kind == WARP_ALIGNED) return;
+  const bool fast_ok = f.warp.kind == WARP_HOMOGRAPHY && !f.warp.guard;
+  if ((int)threadIdx.x == first) q->count = 0;
+  const int b = (int)threadIdx.x - first;
+  if (b >= 0 && b < NB) {
+    bool ok = false;
+    Anchor an = {};
+    if (fast_ok) an = make_anchor(f.warp, rx0 + (b % NBX) * 8, ry0 + (b / NBX) * 4, &ok);
+    if (!ok) an.ix = kNoAnchor;
+    q->anchor[b] = an;
+  }
+}
+
+// Remap of the region: the anchors (region_anchors) are in place.
 template <int RW, int RH, int KS = RW>
 __device__ void fill_region(const FrameIn& f, int W, int H, int rx0, int ry0, uint32_t* reg, uint32_t* kv,
                             ExactQueue* q) {
@@ -125,18 +147,7 @@ __device__ void fill_region(const FrameIn& f, int W, int H, int rx0, int ry0, ui
   constexpr int NBX = (RW + 7) / 8, NBY = (RH + 3) / 4, NB = NBX * NBY;
   static_assert(NB <= kMaxAnchors, "anchor table too small");
   const int du = lane & 7, dv = lane >> 3;
-  const bool fast_ok = f.warp.kind == WARP_HOMOGRAPHY && !f.warp.guard;
-  // phase 1: one FP64 anchor per 8x4 block into shared memory
-  if (threadIdx.x == 0) q->count = 0;
-  for (int b = threadIdx.x; b < NB; b += NT) {
-    bool ok = false;
-    Anchor an = {};
-    if (fast_ok) an = make_anchor(f.warp, rx0 + (b % NBX) * 8, ry0 + (b / NBX) * 4, &ok);
-    if (!ok) an.ix = kNoAnchor;
-    q->anchor[b] = an;
-  }
-  __syncthreads();
-  // phase 2: one warp per block, the anchor read as a shared-memory broadcast
+  // one warp per block, the anchor read as a shared-memory broadcast
   for (int blk = warp; blk < NB; blk += nwarps) {
     const int bx = blk % NBX, by = blk / NBX;
     const int rx = bx * 8 + du, ry = by * 4 + dv;
@@ -211,6 +222,9 @@ __global__ void __launch_bounds__(NT, 5) remap_weights_kernel(const __grid_const
       if (a.uni[(int64_t)Y * a.pitch + X]) umask |= 1u << i;
     }
   }
+  constexpr int kAnchorThreads = ((RW + 7) / 8) * ((RH + 3) / 4);
+  if (a.K > 0) region_anchors<RW, RH>(a.f[0], x0 - B, y0 - B, queue, 0);
+  __syncthreads();
   for (int k = 0; k < a.K; ++k) {
     fill_region<RW, RH, KS>(a.f[k], a.W, a.H, x0 - B, y0 - B, reg, kv, queue);
     __syncthreads();
@@ -239,6 +253,8 @@ __global__ void __launch_bounds__(NT, 5) remap_weights_kernel(const __grid_const
         h2[r * HS + c0 + c] = q;
       }
     }
+    // the next frame's anchors, on the threads with one row item (the last ones)
+    if (k + 1 < a.K) region_anchors<RW, RH>(a.f[k + 1], x0 - B, y0 - B, queue, NT - kAnchorThreads);
     __syncthreads();
     // vertical sliding sums down column vc -> weights of rows vr0 .. vr0+7
     {
