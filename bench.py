@@ -565,7 +565,7 @@ def main():
         def new_stack(i):
             st = fsb.PyramidContrastStack(ctx, W, H, F, roi=roi, frames_per_batch=args.batch)
             for f, p in zip(hframes, poses):
-                st.add_frame(f, p)
+                st.add_frame_async(f, p)  # uploads queued back to back (pinned frames stay put)
             return st
 
         def run_stacks(n):

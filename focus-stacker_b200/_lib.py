@@ -26,7 +26,7 @@ EXPORTED = (
     "fs_ctx_synchronize", "fs_ctx_trim", "fs_ctx_reserve", "fs_ctx_set_budget", "fs_ctx_stream", "fs_ctx_launch_count", "fs_ctx_set_kernel_timing", "fs_ctx_kernel_stats",
     "fs_pose_default", "fs_compute_roi", "fs_inverse_map_points", "fs_forward_map_points", "fs_exact_expand_divisor",
     "fs_remap_frame", "fs_remap_frame_device",
-    "fs_stack_begin", "fs_stack_add_frame", "fs_stack_add_frame_device", "fs_stack_finish",
+    "fs_stack_begin", "fs_stack_add_frame", "fs_stack_add_frame_async", "fs_stack_add_frame_device", "fs_stack_finish",
     "fs_stack_finish_device", "fs_stack_finish_async", "fs_stack_wait", "fs_stack_set_base_output", "fs_stack_pass2_mode", "fs_stack_footprint", "fs_stack_mode_bytes", "fs_stack_begin_mode",
     "fs_stack_set_frame_total", "fs_stack_end_pass1", "fs_stack_blend", "fs_stack_collapse", "fs_stack_buffer", "fs_stack_output_size", "fs_stack_destroy", "fs_fuse_stack",
     "fs_batch_create", "fs_batch_run", "fs_batch_stack_count", "fs_batch_pass2_mode", "fs_batch_uses_graph",
@@ -109,6 +109,7 @@ def _bind(L):
         f.argtypes = [ctx, vp, sz, u32, u32, u32, P(FsPose), P(FsRect), vp, sz]
     L.fs_stack_begin.argtypes = [ctx, P(FsStackDesc), P(vp)]
     L.fs_stack_add_frame.argtypes = [vp, vp, sz, P(FsPose)]
+    L.fs_stack_add_frame_async.argtypes = [vp, vp, sz, P(FsPose)]
     L.fs_stack_add_frame_device.argtypes = [vp, vp, sz, P(FsPose)]
     L.fs_stack_finish.argtypes = [vp, FETCH_CB, vp, vp, sz]
     L.fs_stack_finish_device.argtypes = [vp, FETCH_CB, vp, vp, sz]

@@ -378,6 +378,17 @@ class PyramidContrastStack:
                                     ctypes.byref(p) if p is not None else None)
         _check(rc, self.ctx.handle)
 
+    def add_frame_async(self, pixels: np.ndarray, pose=None):
+        """add_frame without waiting for the upload; `pixels` (best pinned
+        memory) is kept referenced and must not change until finish or wait
+        has returned."""
+        pixels = np.ascontiguousarray(pixels)
+        self._keep.append(pixels)
+        p = _pose(pose).to_c() if pose is not None else None
+        rc = L().fs_stack_add_frame_async(self.handle, pixels.ctypes.data, pixels.shape[1] * pixels.shape[2],
+                                          ctypes.byref(p) if p is not None else None)
+        _check(rc, self.ctx.handle)
+
     def add_frame_device(self, buf, row_stride: int, pose=None):
         p = _pose(pose).to_c() if pose is not None else None
         self._keep.append(buf)

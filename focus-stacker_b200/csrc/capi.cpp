@@ -893,7 +893,10 @@ int fs_stack_begin_mode(fs_ctx* ctx, const fs_stack_desc* desc, int pass2_mode, 
   return begin_impl(ctx, desc, out, pass2_mode);
 }
 
-static int add_frame_impl(fs_stack* s, const void* pixels, size_t row_stride, const fs_pose* pose, bool device) {
+// wait_copy: return only once a host frame's upload has completed (the
+// caller may reuse its buffer); without it the upload is only queued.
+static int add_frame_impl(fs_stack* s, const void* pixels, size_t row_stride, const fs_pose* pose, bool device,
+                          bool wait_copy = true) {
   if (!s || !pixels) return FS_ERR_INVALID;
   if (!s->ctx) return FS_ERR_STATE;  // its context was destroyed
   fs_ctx* ctx = s->ctx;
@@ -949,8 +952,10 @@ static int add_frame_impl(fs_stack* s, const void* pixels, size_t row_stride, co
     cudaEventRecord(s->copy_done, ctx->copy);
     cudaStreamWaitEvent(ctx->stream, s->copy_done, 0);
     // the caller may reuse its buffer once this returns
-    e = cudaEventSynchronize(s->copy_done);
-    if (e != cudaSuccess) return cuda_err(ctx, e, "frame upload");
+    if (wait_copy) {
+      e = cudaEventSynchronize(s->copy_done);
+      if (e != cudaSuccess) return cuda_err(ctx, e, "frame upload");
+    }
     fr.px = buf;
     fr.pitch = s->frame_pitch;
   }
@@ -960,6 +965,10 @@ static int add_frame_impl(fs_stack* s, const void* pixels, size_t row_stride, co
 
 int fs_stack_add_frame(fs_stack* stack, const void* pixels, size_t row_stride, const fs_pose* pose) {
   return add_frame_impl(stack, pixels, row_stride, pose, false);
+}
+
+int fs_stack_add_frame_async(fs_stack* stack, const void* pixels, size_t row_stride, const fs_pose* pose) {
+  return add_frame_impl(stack, pixels, row_stride, pose, false, false);
 }
 
 int fs_stack_add_frame_device(fs_stack* stack, const void* dev_pixels, size_t row_stride, const fs_pose* pose) {

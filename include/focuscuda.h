@@ -169,6 +169,12 @@ int fs_stack_begin(fs_ctx* ctx, const fs_stack_desc* desc, fs_stack** out);
  * buffer copied before the call returns; `pose` is ignored for aligned input. */
 int fs_stack_add_frame(fs_stack* stack, const void* pixels, size_t row_stride, const fs_pose* pose);
 
+/* fs_stack_add_frame without waiting for the upload: the copy is queued and
+ * the call returns, so that a stack's uploads run back to back.  The host
+ * buffer (best pinned) must stay valid and unchanged until fs_stack_finish
+ * or fs_stack_wait has returned. */
+int fs_stack_add_frame_async(fs_stack* stack, const void* pixels, size_t row_stride, const fs_pose* pose);
+
 /* Same with a device pointer; the buffer must stay valid and unchanged until
  * fs_stack_finish returns (pass 2 reads it again). */
 int fs_stack_add_frame_device(fs_stack* stack, const void* dev_pixels, size_t row_stride, const fs_pose* pose);

@@ -349,7 +349,8 @@ def test_stack_errors(torch, ctx):
 
 def test_pipelined_finish_matches_sync(torch, ctx):
     # stack A's pass 2 is queued (finish_into_async) while stack B's frames
-    # upload on the same context; both images equal the synchronous ones
+    # upload on the same context, every upload queued without a wait
+    # (add_frame_async); both images equal the synchronous ones
     W, H, F = 640, 480, 5
     frames_a, poses_a = synth_stack(torch, ctx, W, H, F, seed=31)
     frames_b, poses_b = synth_stack(torch, ctx, W, H, F, seed=32)
@@ -369,11 +370,11 @@ def test_pipelined_finish_matches_sync(torch, ctx):
     out_b = np.zeros_like(ref_b)
     a = fsb.PyramidContrastStack(ctx, W, H, F, roi=roi)
     for f, p in zip(frames_a, poses_a):
-        a.add_frame(f, p)
+        a.add_frame_async(f, p)
     a.finish_into_async(out_a)
     b = fsb.PyramidContrastStack(ctx, W, H, F, roi=roi_b)
     for f, p in zip(frames_b, poses_b):
-        b.add_frame(f, p)
+        b.add_frame_async(f, p)
     a.wait()
     a.close()
     b.finish_into_async(out_b)
