@@ -1316,8 +1316,11 @@ __device__ __forceinline__ void img_row(const LevelArgs& a, int k, int y, int c,
 // sums of one row for the lane's two columns: the channel bytes of taps
 // 0..3 gathered into one word each and dot-multiplied with the tap weights
 // (zeroed where alpha is 0), plus tap 4.
-__device__ __forceinline__ void img_row_u8(const LevelArgs& a, int k, int y, int c, bool live, int4 (&hs)[2]) {
-  uint32_t w[7] = {0u, 0u, 0u, 0u, 0u, 0u, 0u};
+// The words of level-0 row y under the lane's taps (columns c - 2 .. c + 4);
+// only loads, so that the next rows can be fetched while this one is summed.
+__device__ __forceinline__ void load_row_u8(const LevelArgs& a, int k, int y, int c, bool live, uint32_t (&w)[7]) {
+#pragma unroll
+  for (int u = 0; u < 7; ++u) w[u] = 0u;
   if (live && y >= 0 && y < a.hl) {
     const uint32_t* row = a.in0[k].rgba + (int64_t)y * a.pitch_l;
     const uint4 q4 = *reinterpret_cast<const uint4*>(row + c);  // inside the row's pitch
@@ -1325,11 +1328,6 @@ __device__ __forceinline__ void img_row_u8(const LevelArgs& a, int k, int y, int
     w[3] = q4.y;
     w[4] = q4.z;
     w[5] = q4.w;
-    if (c + 3 >= a.wl) {  // words past the level's last column
-#pragma unroll
-      for (int u = 2; u < 6; ++u)
-        if (c + u - 2 >= a.wl) w[u] = 0u;
-    }
     if (c > 0) {
       const uint2 q2 = *reinterpret_cast<const uint2*>(row + c - 2);
       w[0] = q2.x;
@@ -1337,6 +1335,12 @@ __device__ __forceinline__ void img_row_u8(const LevelArgs& a, int k, int y, int
     }
     if (c + 4 < a.wl) w[6] = row[c + 4];
   }
+}
+
+__device__ __forceinline__ void sum_row_u8(const uint32_t (&wr)[7], int c, int wl, int4 (&hs)[2]) {
+  uint32_t w[7];
+#pragma unroll
+  for (int u = 0; u < 7; ++u) w[u] = (u < 2 || u == 6 || c + u - 2 < wl) ? wr[u] : 0u;  // words past the level
   constexpr uint32_t kW = 0x04060401u;  // tap weights 1, 4, 6, 4 (tap 4: 1)
 #pragma unroll
   for (int h = 0; h < 2; ++h) {
@@ -1353,6 +1357,12 @@ __device__ __forceinline__ void img_row_u8(const LevelArgs& a, int k, int y, int
     }
     hs[h] = make_int4(v[0], v[1], v[2], (int)__dp4a(wt, 0x01010101u, s4 ? 1u : 0u));
   }
+}
+
+__device__ __forceinline__ void img_row_u8(const LevelArgs& a, int k, int y, int c, bool live, int4 (&hs)[2]) {
+  uint32_t w[7];
+  load_row_u8(a, k, y, c, live, w);
+  sum_row_u8(w, c, a.wl, hs);
 }
 
 // One vertical REDUCE tap: v = fma(w, row, v) on value and weight sums
@@ -1416,12 +1426,32 @@ __global__ void __launch_bounds__(32 * kImgWarps) img_stream_kernel(const __grid
       nxt[h] = vtap(kwi(0), t2[h], zero);
     }
   }
+  uint32_t n3[7], n4[7];  // level 0: the words of the next two rows, fetched one step ahead
+  if constexpr (L0) {
+    load_row_u8(a, k, 2 * r + 1, c, live, n3);
+    load_row_u8(a, k, 2 * r + 2, c, live, n4);
+  }
   for (; r <= i1; ++r) {
     float4 fin[2];
     {
       Acc t3[2], t4[2];
-      row_sums<T, L0>(a, k, 2 * r + 1, c, live, t3);
-      row_sums<T, L0>(a, k, 2 * r + 2, c, live, t4);
+      if constexpr (L0) {
+        uint32_t w3[7], w4[7];
+#pragma unroll
+        for (int u = 0; u < 7; ++u) {
+          w3[u] = n3[u];
+          w4[u] = n4[u];
+        }
+        if (r < i1) {
+          load_row_u8(a, k, 2 * r + 3, c, live, n3);
+          load_row_u8(a, k, 2 * r + 4, c, live, n4);
+        }
+        sum_row_u8(w3, c, a.wl, t3);
+        sum_row_u8(w4, c, a.wl, t4);
+      } else {
+        row_sums<T, L0>(a, k, 2 * r + 1, c, live, t3);
+        row_sums<T, L0>(a, k, 2 * r + 2, c, live, t4);
+      }
 #pragma unroll
       for (int h = 0; h < 2; ++h) {
         fin[h] = acc_float(vtap(kwi(4), t4[h], vtap(kwi(3), t3[h], cur[h])));
