@@ -1123,44 +1123,49 @@ __device__ __forceinline__ void ld2(const T* p, float* v) {
 template <typename T>
 __device__ __forceinline__ void reduce_row(const T* in, const uint8_t* sm, int64_t pitch, int wl, int hl, int r,
                                            int j0, float* v, float* ws) {
-  float m[7], sw[7];
+  float m[7];
+  uint32_t s4 = 0u, s2 = 0u, s6 = 0u;  // support bytes of taps 2..5, 0..1 and 6
 #pragma unroll
-  for (int u = 0; u < 7; ++u) m[u] = sw[u] = 0.0f;
+  for (int u = 0; u < 7; ++u) m[u] = 0.0f;
+  const int c = 2 * j0;  // a multiple of 4: the vector loads are aligned
   if (r >= 0 && r < hl) {
-    const int c = 2 * j0;  // a multiple of 4: the vector loads are aligned
     const T* row = in + (int64_t)r * pitch;
     const uint8_t* srow = sm + (int64_t)r * pitch;
     // columns c .. c + 3 lie inside the row's pitch (c < wl, pitch a multiple of 32)
     ld4<T>(row + c, m + 2);
-    const uint32_t s4 = *reinterpret_cast<const uint32_t*>(srow + c);
-#pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      const bool in_level = c + u < wl;
-      sw[2 + u] = in_level && ((s4 >> (8 * u)) & 0xffu) ? 1.0f : 0.0f;
-      if (!in_level) m[2 + u] = 0.0f;
-    }
+    s4 = *reinterpret_cast<const uint32_t*>(srow + c);
     if (c > 0) {
       ld2<T>(row + c - 2, m);
-      const uint32_t s2 = *reinterpret_cast<const uint16_t*>(srow + c - 2);
-      sw[0] = (s2 & 0xffu) ? 1.0f : 0.0f;
-      sw[1] = (s2 >> 8) ? 1.0f : 0.0f;
+      s2 = *reinterpret_cast<const uint16_t*>(srow + c - 2);
     }
     if (c + 4 < wl) {
       m[6] = ldv<T>(row, c + 4);
-      sw[6] = srow[c + 4] ? 1.0f : 0.0f;
+      s6 = srow[c + 4];
     }
   }
+  if (c + 3 >= wl) s4 &= (1u << (8 * (wl - c))) - 1u;  // columns past the level: no support (wl - c in 1..3)
+  // a tap without support adds nothing: fma(kw, 0, a) = a = fma(0, m, a), so
+  // the value sums take the supported samples (zero elsewhere) with the
+  // weights 1, 4, 6, 4, 1, and the weight sums (integers <= 16) come from
+  // the support bytes as dot products
+  const uint32_t nz0 = __vcmpne4(__byte_perm(s2, s4, 0x5410u), 0u);  // taps 0..3
+  const uint32_t nz1 = __vcmpne4(s4, 0u);                            // taps 2..5
+  float mp[7];
+  mp[0] = (nz0 & 0x000000ffu) ? m[0] : 0.0f;
+  mp[1] = (nz0 & 0x0000ff00u) ? m[1] : 0.0f;
+#pragma unroll
+  for (int u = 0; u < 4; ++u) mp[2 + u] = (nz1 & (0xffu << (8 * u))) ? m[2 + u] : 0.0f;
+  mp[6] = s6 ? m[6] : 0.0f;
+  constexpr uint32_t kW = 0x04060401u;
+  const int w0 = (int)__dp4a(nz0 & kW, 0x01010101u, (nz1 >> 16) & 1u);
+  const int w1 = (int)__dp4a(nz1 & kW, 0x01010101u, s6 ? 1u : 0u);
 #pragma unroll
   for (int h = 0; h < 2; ++h) {
-    float a = 0.f, b = 0.f;
+    float a = 0.f;
 #pragma unroll
-    for (int kx = 0; kx < 5; ++kx) {
-      const float w = sw[2 * h + kx] != 0.0f ? kw(kx) : 0.0f;
-      a = fmaf(w, m[2 * h + kx], a);
-      b += w;
-    }
+    for (int kx = 0; kx < 5; ++kx) a = fmaf(kw(kx), mp[2 * h + kx], a);
     v[h] = a;
-    ws[h] = b;
+    ws[h] = __int_as_float(0x4B000000 | (h == 0 ? w0 : w1)) - 8388608.0f;  // exact
   }
 }
 
@@ -1415,11 +1420,27 @@ __global__ void __launch_bounds__(32 * kImgWarps) img_stream_kernel(const __grid
 #pragma unroll
     for (int u = 0; u < 4; ++u) Hm2[ch][u] = Hm1[ch][u] = 0.0f;
   int r = i0 > 0 ? i0 - 1 : 0;
+  // level 0: the lane's four words of level-l rows 2r - 2, 2r - 1, 2r at the
+  // top of step r (the Laplacian rows emitted at step r are the first two)
+  uint4 ringR = make_uint4(0u, 0u, 0u, 0u), ringQ = ringR, ringP = ringR;
   {
     Acc t0[2], t1[2], t2[2];
-    row_sums<T, L0>(a, k, 2 * r - 2, c, live, t0);
-    row_sums<T, L0>(a, k, 2 * r - 1, c, live, t1);
-    row_sums<T, L0>(a, k, 2 * r, c, live, t2);
+    if constexpr (L0) {
+      uint32_t w0[7], w1[7], w2[7];
+      load_row_u8(a, k, 2 * r - 2, c, live, w0);
+      load_row_u8(a, k, 2 * r - 1, c, live, w1);
+      load_row_u8(a, k, 2 * r, c, live, w2);
+      sum_row_u8(w0, c, a.wl, t0);
+      sum_row_u8(w1, c, a.wl, t1);
+      sum_row_u8(w2, c, a.wl, t2);
+      ringR = make_uint4(w0[2], w0[3], w0[4], w0[5]);
+      ringQ = make_uint4(w1[2], w1[3], w1[4], w1[5]);
+      ringP = make_uint4(w2[2], w2[3], w2[4], w2[5]);
+    } else {
+      row_sums<T, L0>(a, k, 2 * r - 2, c, live, t0);
+      row_sums<T, L0>(a, k, 2 * r - 1, c, live, t1);
+      row_sums<T, L0>(a, k, 2 * r, c, live, t2);
+    }
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
       cur[h] = vtap(kwi(2), t2[h], vtap(kwi(1), t1[h], vtap(kwi(0), t0[h], zero)));
@@ -1433,6 +1454,7 @@ __global__ void __launch_bounds__(32 * kImgWarps) img_stream_kernel(const __grid
   }
   for (; r <= i1; ++r) {
     float4 fin[2];
+    uint4 c3 = make_uint4(0u, 0u, 0u, 0u), c4 = c3;  // level 0: words of rows 2r + 1, 2r + 2
     {
       Acc t3[2], t4[2];
       if constexpr (L0) {
@@ -1448,6 +1470,8 @@ __global__ void __launch_bounds__(32 * kImgWarps) img_stream_kernel(const __grid
         }
         sum_row_u8(w3, c, a.wl, t3);
         sum_row_u8(w4, c, a.wl, t4);
+        c3 = make_uint4(w3[2], w3[3], w3[4], w3[5]);
+        c4 = make_uint4(w4[2], w4[3], w4[4], w4[5]);
       } else {
         row_sums<T, L0>(a, k, 2 * r + 1, c, live, t3);
         row_sums<T, L0>(a, k, 2 * r + 2, c, live, t4);
@@ -1517,7 +1541,7 @@ __global__ void __launch_bounds__(32 * kImgWarps) img_stream_kernel(const __grid
         const int64_t ro = (int64_t)y * a.pitch_l;
         float gv[3][4];
         if constexpr (L0) {
-          const uint4 q4 = *reinterpret_cast<const uint4*>(a.in0[k].rgba + ro + c);
+          const uint4 q4 = yy == 0 ? ringR : ringQ;  // rows 2r - 2, 2r - 1
           const uint32_t w[4] = {q4.x, q4.y, q4.z, q4.w};
 #pragma unroll
           for (int ch = 0; ch < 3; ++ch)
@@ -1557,6 +1581,11 @@ __global__ void __launch_bounds__(32 * kImgWarps) img_stream_kernel(const __grid
         Hm2[ch][u] = Hm1[ch][u];
         Hm1[ch][u] = Hc[ch][u];
       }
+    if constexpr (L0) {
+      ringR = ringP;
+      ringQ = c3;
+      ringP = c4;
+    }
   }
 }
 
