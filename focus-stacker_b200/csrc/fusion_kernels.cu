@@ -128,7 +128,6 @@ __device__ __forceinline__ void region_anchors(const FrameIn& f, int rx0, int ry
 template <int RW, int RH, int KS = RW>
 __device__ void fill_region(const FrameIn& f, int W, int H, int rx0, int ry0, uint32_t* reg, uint32_t* kv,
                             ExactQueue* q) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = NT / 32;
   if (f.warp.kind == WARP_ALIGNED) {
     for (int i = threadIdx.x; i < RW * RH; i += NT) {
       const int rx = i % RW, ry = i / RW;
@@ -146,13 +145,13 @@ __device__ void fill_region(const FrameIn& f, int W, int H, int rx0, int ry0, ui
   }
   constexpr int NBX = (RW + 7) / 8, NBY = (RH + 3) / 4, NB = NBX * NBY;
   static_assert(NB <= kMaxAnchors, "anchor table too small");
-  const int du = lane & 7, dv = lane >> 3;
-  // one warp per block, the anchor read as a shared-memory broadcast
-  for (int blk = warp; blk < NB; blk += nwarps) {
-    const int bx = blk % NBX, by = blk / NBX;
-    const int rx = bx * 8 + du, ry = by * 4 + dv;
-    if (rx >= RW || ry >= RH) continue;
-    const Anchor an = q->anchor[blk];
+  // region pixels in row order over all threads (a warp's 32 pixels lie in
+  // one or two rows: coalesced taps and stores, and no idle lanes in the
+  // region's last block column); each reads its 8x4 block's anchor
+  for (int i = threadIdx.x; i < RW * RH; i += NT) {
+    const int ry = i / RW, rx = i - ry * RW;
+    const int du = rx & 7, dv = ry & 3;
+    const Anchor an = q->anchor[(ry >> 2) * NBX + (rx >> 3)];
     const int X = rx0 + rx, Y = ry0 + ry;
     uint32_t v = 0;
     if (X >= 0 && Y >= 0 && X < W && Y < H) {
