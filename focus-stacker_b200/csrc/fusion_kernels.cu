@@ -4,17 +4,29 @@
 //                          (window 2B+1) -> alpha weight; pass 1 adds it to
 //                          the weight sum (frame order) and union support and
 //                          can keep the remapped frame + weight for pass 2
+// Pass 2 of the batch modes (CACHE / RESIDENT / REFETCH):
 // level0_kernel            normalise the weights -> level-0 mask; REDUCE of
 //                          frame and mask to level 1; EXPAND back; Laplacian
 //                          x mask into the level-0 accumulator
 // level_kernel<T>          the same step for level l >= 1 from HBM planes
 //                          stored as T (f32 / f16 / bf16)
+// The split pyramid (LAPS mode):
+// img_stream_kernel<T, L0> pass 1, each frame's Gaussian REDUCE and Laplacian
+//                          on the clamped-EXPAND levels, streaming down
+//                          column strips without shared memory
+// img_kernel<T, L0>        the same on the small (no-wrap) levels, per tile
+// blend0_kernel            pass 2, level 0: masks = w / weight sum, blend of
+//                          every frame in order, one pixel per thread
+// mask_reduce_kernel       each frame's mask pyramid, one level per launch
+// blend_kernel<T>          the blend of one level l >= 1 over every frame
+// Both:
 // collapse_kernel          parent += EXPAND(child); quantise at level 0
 //
-// All of it is stencil work on CUDA cores (no tensor cores).  64x32 output
-// tiles are staged in shared memory with their halos; the frames of a batch
-// (K <= 8) run inside one CTA so per-pixel state (weight sums, accumulators)
-// is read and written once per batch, while every FP32 sum keeps the
+// All of it is stencil work on CUDA cores (no tensor cores).  The tile
+// kernels stage 64x32 output tiles in shared memory with their halos, the
+// frames of a batch (K <= 8) inside one CTA so that per-pixel state (weight
+// sums, accumulators) is read and written once per batch; the streaming
+// kernels keep their windows in registers.  Every FP32 sum keeps the
 // reference's frame order.
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
