@@ -1257,81 +1257,63 @@ cudaError_t launch_mask_reduce(const MaskReduceArgs& a, int frames, int in_stora
 // in their order.
 constexpr int kImgWarps = 4, kImgPairs = 30;
 
-// Horizontal REDUCE sums (v0, v1, v2, weight) of level-l row y for the lane's
-// two level-(l+1) columns; samples outside the level count as zero.
-template <typename T, bool L0>
+// Horizontal REDUCE sums (v0, v1, v2, weight) of level-l row y (l >= 1) for
+// the lane's two level-(l+1) columns.  A tap without support adds nothing
+// (fma(w, 0, s) = s = fma(0, v, s)), so the value sums take the supported
+// samples (zero elsewhere) with the weights 1, 4, 6, 4, 1, and the weight
+// sums (integers <= 16) come from the support bytes as dot products; samples
+// outside the level have no support.
+template <typename T>
 __device__ __forceinline__ void img_row(const LevelArgs& a, int k, int y, int c, bool live, float4 (&hs)[2]) {
-  float4 t[7];
+  float v[3][7];
+  uint32_t s4 = 0u, s2 = 0u, s6 = 0u;  // support bytes of taps 2..5, 0..1 and 6
 #pragma unroll
-  for (int u = 0; u < 7; ++u) t[u] = make_float4(0.f, 0.f, 0.f, 0.f);
+  for (int ch = 0; ch < 3; ++ch)
+#pragma unroll
+    for (int u = 0; u < 7; ++u) v[ch][u] = 0.0f;
   if (live && y >= 0 && y < a.hl) {
     const int64_t ro = (int64_t)y * a.pitch_l;
     // columns c .. c + 3 lie inside the row's pitch (c < wl, pitch a multiple of 32)
-    if constexpr (L0) {
-      const uint32_t* row = a.in0[k].rgba + ro;
-      uint32_t w[7] = {0u, 0u, 0u, 0u, 0u, 0u, 0u};
-      const uint4 q4 = *reinterpret_cast<const uint4*>(row + c);
-      w[2] = q4.x;
-      w[3] = q4.y;
-      w[4] = q4.z;
-      w[5] = q4.w;
-      if (c > 0) {
-        const uint2 q2 = *reinterpret_cast<const uint2*>(row + c - 2);
-        w[0] = q2.x;
-        w[1] = q2.y;
-      }
-      if (c + 4 < a.wl) w[6] = row[c + 4];
+    const LevelPlanes& in = a.in[k];
+    const T* g = (const T*)in.g + ro;
+    const uint8_t* sp = in.s + ro;
 #pragma unroll
-      for (int u = 0; u < 7; ++u) {
-        const bool in = u < 2 || u == 6 || c + u - 2 < a.wl;  // u < 2, u == 6: zero words when outside
-        if (in) t[u] = make_float4(chf(w[u], 0), chf(w[u], 1), chf(w[u], 2), px_alpha(w[u]) > 0 ? 1.0f : 0.0f);
-      }
-    } else {
-      const LevelPlanes& in = a.in[k];
-      const T* g = (const T*)in.g + ro;
-      const uint8_t* sp = in.s + ro;
-      float v[3][7];
-#pragma unroll
-      for (int ch = 0; ch < 3; ++ch) {
-        const T* gc = g + ch * in.plane;
-        ld4<T>(gc + c, v[ch] + 2);
-        v[ch][0] = v[ch][1] = v[ch][6] = 0.0f;
-        if (c > 0) ld2<T>(gc + c - 2, v[ch]);
-        if (c + 4 < a.wl) v[ch][6] = ldv<T>(gc, c + 4);
-      }
-      const uint32_t s4 = *reinterpret_cast<const uint32_t*>(sp + c);
-      const uint32_t s2 = c > 0 ? *reinterpret_cast<const uint16_t*>(sp + c - 2) : 0u;
-      const uint32_t s6 = c + 4 < a.wl ? sp[c + 4] : 0u;
-      const uint32_t sb[7] = {s2 & 0xffu, s2 >> 8, s4 & 0xffu, (s4 >> 8) & 0xffu, (s4 >> 16) & 0xffu, s4 >> 24, s6};
-#pragma unroll
-      for (int u = 0; u < 7; ++u) {
-        const bool in = u < 2 || u == 6 || c + u - 2 < a.wl;
-        if (in) t[u] = make_float4(v[0][u], v[1][u], v[2][u], sb[u] ? 1.0f : 0.0f);
-      }
+    for (int ch = 0; ch < 3; ++ch) {
+      const T* gc = g + ch * in.plane;
+      ld4<T>(gc + c, v[ch] + 2);
+      if (c > 0) ld2<T>(gc + c - 2, v[ch]);
+      if (c + 4 < a.wl) v[ch][6] = ldv<T>(gc, c + 4);
     }
+    s4 = *reinterpret_cast<const uint32_t*>(sp + c);
+    if (c > 0) s2 = *reinterpret_cast<const uint16_t*>(sp + c - 2);
+    if (c + 4 < a.wl) s6 = sp[c + 4];
+    if (c + 3 >= a.wl) s4 &= (1u << (8 * (a.wl - c))) - 1u;  // columns past the level (wl - c in 1..3)
   }
+  const uint32_t nz0 = __vcmpne4(__byte_perm(s2, s4, 0x5410u), 0u);  // taps 0..3
+  const uint32_t nz1 = __vcmpne4(s4, 0u);                            // taps 2..5
+  bool sup[7];
+  sup[0] = (nz0 & 0x000000ffu) != 0u;
+  sup[1] = (nz0 & 0x0000ff00u) != 0u;
+#pragma unroll
+  for (int u = 0; u < 4; ++u) sup[2 + u] = (nz1 & (0xffu << (8 * u))) != 0u;
+  sup[6] = s6 != 0u;
+  constexpr uint32_t kW = 0x04060401u;
+  const int wsum[2] = {(int)__dp4a(nz0 & kW, 0x01010101u, (nz1 >> 16) & 1u),
+                       (int)__dp4a(nz1 & kW, 0x01010101u, s6 ? 1u : 0u)};
 #pragma unroll
   for (int h = 0; h < 2; ++h) {
-    float v0 = 0.f, v1 = 0.f, v2 = 0.f, ws = 0.f;
+    float acc[3];
 #pragma unroll
-    for (int kx = 0; kx < 5; ++kx) {
-      const float4 tk = t[2 * h + kx];
-      const float w = kw(kx) * tk.w;
-      v0 = fmaf(w, tk.x, v0);
-      v1 = fmaf(w, tk.y, v1);
-      v2 = fmaf(w, tk.z, v2);
-      ws += w;
+    for (int ch = 0; ch < 3; ++ch) {
+      float sum = 0.f;
+#pragma unroll
+      for (int kx = 0; kx < 5; ++kx) sum = fmaf(kw(kx), sup[2 * h + kx] ? v[ch][2 * h + kx] : 0.0f, sum);
+      acc[ch] = sum;
     }
-    hs[h] = make_float4(v0, v1, v2, ws);
+    hs[h] = make_float4(acc[0], acc[1], acc[2], __int_as_float(0x4B000000 | wsum[h]) - 8388608.0f);
   }
 }
 
-// Level 0 in integers: the samples are bytes and the weights 1, 4, 6 (or 0
-// without support), so every partial sum of the FP32 REDUCE is an integer
-// below 2^16 and exact; the integer sums equal it bit for bit.  Horizontal
-// sums of one row for the lane's two columns: the channel bytes of taps
-// 0..3 gathered into one word each and dot-multiplied with the tap weights
-// (zeroed where alpha is 0), plus tap 4.
 // The words of level-0 row y under the lane's taps (columns c - 2 .. c + 4);
 // only loads, so that the next rows can be fetched while this one is summed.
 __device__ __forceinline__ void load_row_u8(const LevelArgs& a, int k, int y, int c, bool live, uint32_t (&w)[7]) {
@@ -1353,6 +1335,12 @@ __device__ __forceinline__ void load_row_u8(const LevelArgs& a, int k, int y, in
   }
 }
 
+// Level 0 in integers: the samples are bytes and the weights 1, 4, 6 (or 0
+// without support), so every partial sum of the FP32 REDUCE is an integer
+// below 2^16 and exact; the integer sums equal it bit for bit.  Horizontal
+// sums of one row for the lane's two columns: the channel bytes of taps
+// 0..3 gathered into one word each and dot-multiplied with the tap weights
+// (zeroed where alpha is 0), plus tap 4.
 __device__ __forceinline__ void sum_row_u8(const uint32_t (&wr)[7], int c, int wl, int4 (&hs)[2]) {
   uint32_t w[7];
 #pragma unroll
@@ -1402,7 +1390,7 @@ __device__ __forceinline__ float4 acc_float(int4 v) {
 template <typename T, bool L0, class A>
 __device__ __forceinline__ void row_sums(const LevelArgs& a, int k, int y, int c, bool live, A (&hs)[2]) {
   if constexpr (L0) img_row_u8(a, k, y, c, live, hs);
-  else img_row<T, false>(a, k, y, c, live, hs);
+  else img_row<T>(a, k, y, c, live, hs);
 }
 __device__ __forceinline__ int kwi(int i) { return (i == 0 || i == 4) ? 1 : ((i == 1 || i == 3) ? 4 : 6); }
 
