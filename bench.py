@@ -404,8 +404,20 @@ def cpu_sample_frames(fsb, sample, seed, ctx=None, torch=None):
     return frames, poses
 
 
-def cpu_baseline(fsb, steps=1, warmup=0, sample=CPU_SAMPLE, seed=1, ctx=None, torch=None):
-    """Time the oracle (C++ restatement, all host threads) on a bounded sample."""
+def cpu_model() -> str:
+    try:
+        with open("/proc/cpuinfo") as fh:
+            for line in fh:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def cpu_baseline(fsb, steps=1, warmup=0, sample=CPU_SAMPLE, seed=1, ctx=None, torch=None, single_thread=False):
+    """Time the oracle (C++ restatement, all host threads) on a bounded sample;
+    with single_thread, also one thread on the sample's first two frames."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
     F, W, H = sample
@@ -422,10 +434,17 @@ def cpu_baseline(fsb, steps=1, warmup=0, sample=CPU_SAMPLE, seed=1, ctx=None, to
             times.append(dt)
     t = statistics.median(times)
     px = F * roi.width * roi.height
-    return {"value": px / t / 1e6, "unit": UNIT, "cores": cores, "kind": "port",
-            "sample": f"{F} frames of {W}x{H} (ROI {roi.width}x{roi.height}), same scene recipe, "
-                      f"oracle stack_fuse (remap + pyramid-contrast, FP32) with {cores} threads, "
-                      f"median of {len(times)} runs: {t:.2f} s"}
+    out = {"value": px / t / 1e6, "unit": UNIT, "cores": cores, "kind": "port", "cpu_model": cpu_model(),
+           "sample": f"{F} frames of {W}x{H} (ROI {roi.width}x{roi.height}), same scene recipe, "
+                     f"oracle stack_fuse (remap + pyramid-contrast, FP32) with {cores} threads, "
+                     f"median of {len(times)} runs: {t:.2f} s"}
+    if single_thread and F >= 2:
+        t0 = time.perf_counter()
+        oracle.stack_fuse(frames[:2], pd[:2], roi.as_tuple(), jobs=1)
+        t1 = time.perf_counter() - t0
+        out["single_thread"] = {"value": 2 * roi.width * roi.height / t1 / 1e6, "unit": UNIT,
+                                "sample": f"the sample's first 2 frames, 1 thread: {t1:.2f} s"}
+    return out
 
 
 def run_reference(args, rank, world):
@@ -629,7 +648,7 @@ def main():
 
     cpu = None
     if not args.no_cpu_baseline and rank == 0 and world == 1:
-        cpu = cpu_baseline(fsb, steps=1, warmup=1, sample=(4, 3976, 2652), ctx=ctx, torch=torch)
+        cpu = cpu_baseline(fsb, steps=1, warmup=1, sample=(4, 3976, 2652), ctx=ctx, torch=torch, single_thread=True)
 
     if rank == 0:
         line = {"metric": METRIC, "value": round(value, 2), "unit": UNIT, "n_gpus": world, "steps": args.steps,
