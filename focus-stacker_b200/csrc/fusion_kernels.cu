@@ -32,12 +32,32 @@
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstddef>
 #include <type_traits>
 
 #include "fusion_kernels.cuh"
 
 namespace fs {
+
+// cudaFuncSetAttribute acts on the current device: a kernel's raised
+// dynamic shared-memory limit is remembered per device (ordinals below 64;
+// larger ones set it on every launch), so that one process can drive
+// several GPUs, from several threads.
+struct DeviceOnce {
+  std::atomic<uint64_t> done{0};
+  template <class F>
+  cudaError_t run(F&& set) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    const uint64_t bit = dev >= 0 && dev < 64 ? (1ull << dev) : 0ull;
+    if (bit && (done.load(std::memory_order_acquire) & bit)) return cudaSuccess;
+    e = set();
+    if (e == cudaSuccess && bit) done.fetch_or(bit, std::memory_order_release);
+    return e;
+  }
+};
 
 namespace {
 
@@ -314,13 +334,12 @@ __global__ void __launch_bounds__(NT, 5) remap_weights_kernel(const __grid_const
 
 template <int B>
 static cudaError_t launch_rw(const RemapWeightArgs& a, cudaStream_t s) {
-  static bool configured = false;
+  static DeviceOnce configured;
   const size_t sm = RWLayout<B>::bytes;
-  if (!configured) {
-    cudaError_t e = cudaFuncSetAttribute(remap_weights_kernel<B>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    if (e != cudaSuccess) return e;
-    configured = true;
-  }
+  cudaError_t e = configured.run([&] {
+    return cudaFuncSetAttribute(remap_weights_kernel<B>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  });
+  if (e != cudaSuccess) return e;
   dim3 grid((a.W + TW - 1) / TW, (a.H + TH - 1) / TH);
   remap_weights_kernel<B><<<grid, NT, sm, s>>>(a);
   return cudaGetLastError();
@@ -1612,7 +1631,7 @@ cudaError_t launch_blend0(float* acc, int64_t plane, int64_t pitch, int w, int h
 }
 
 template <template <typename, bool> class KER, bool L0>
-static cudaError_t launch_split(const LevelArgs& a, int storage, cudaStream_t s, bool* cfg) {
+static cudaError_t launch_split(const LevelArgs& a, int storage, cudaStream_t s, DeviceOnce* cfg) {
   dim3 grid((a.wl + TW - 1) / TW, (a.hl + TH - 1) / TH, a.K);
   const size_t sm = sizeof(ImgSmem);
   cudaError_t e;
@@ -1639,7 +1658,7 @@ template <typename T, bool L0> struct ImgK {
 };
 
 cudaError_t launch_img_level(const LevelArgs& a, int storage, cudaStream_t s) {
-  static bool cfg0[3] = {false, false, false}, cfg1[3] = {false, false, false};
+  static DeviceOnce cfg0[3], cfg1[3];
   // clamped-EXPAND levels (never followed by the top level): streaming kernel
   if (!a.exact_expand && a.level + 2 < a.levels) {
     switch (storage) {
@@ -1679,15 +1698,12 @@ cudaError_t launch_sum_contrib(float* acc, int64_t plane, int64_t pitch, int w, 
 }
 
 template <typename K>
-static cudaError_t configure(K kernel, size_t bytes, bool* done) {
-  if (*done) return cudaSuccess;
-  cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-  if (e == cudaSuccess) *done = true;
-  return e;
+static cudaError_t configure(K kernel, size_t bytes, DeviceOnce* done) {
+  return done->run([&] { return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes); });
 }
 
 template <template <typename> class KER>
-static cudaError_t launch_levels(const LevelArgs& a, int storage, cudaStream_t s, bool* cfg) {
+static cudaError_t launch_levels(const LevelArgs& a, int storage, cudaStream_t s, DeviceOnce* cfg) {
   const size_t sm = KER<float>::smem();
   dim3 grid((a.wl + TW - 1) / TW, (a.hl + TH - 1) / TH, a.frame_parallel ? a.K : 1);
   cudaError_t e;
@@ -1719,12 +1735,12 @@ template <typename T> struct LevelK {
 };
 
 cudaError_t launch_level0(const LevelArgs& a, int storage, cudaStream_t s) {
-  static bool cfg[3] = {false, false, false};
+  static DeviceOnce cfg[3];
   return launch_levels<Level0K>(a, storage, s, cfg);
 }
 
 cudaError_t launch_level(const LevelArgs& a, int storage, cudaStream_t s) {
-  static bool cfg[3] = {false, false, false};
+  static DeviceOnce cfg[3];
   return launch_levels<LevelK>(a, storage, s, cfg);
 }
 
