@@ -1,0 +1,67 @@
+"""CPU checks of bench.py: the reference arm's JSON line (it times the oracle
+on the host cores, so it runs here) and the per-kernel byte model."""
+import json
+import os
+import subprocess
+import sys
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+sys.path.insert(0, ROOT)
+
+import bench  # noqa: E402
+
+
+def run_bench(args, env_extra=None, timeout=600):
+    env = dict(os.environ)
+    env.update(env_extra or {})
+    p = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py")] + args, capture_output=True, text=True,
+                       timeout=timeout, env=env, cwd=ROOT)
+    return p
+
+
+def test_reference_arm_prints_the_contract_line():
+    p = run_bench(["--impl", "reference", "--steps", "1", "--warmup", "0"])
+    assert p.returncode == 0, p.stderr[-2000:]
+    line = json.loads(p.stdout.strip().splitlines()[-1])
+    assert line["impl"] == "reference"
+    assert line["metric"] == bench.METRIC and line["unit"] == bench.UNIT
+    assert line["higher_is_better"] is True and line["value"] > 0
+    cb = line["cpu_baseline"]
+    assert cb["kind"] == "port" and cb["cores"] >= 1 and cb["value"] == line["value"] and cb["sample"]
+    e2e = line["e2e"]
+    assert e2e["value"] == line["value"] and e2e["unit"] == line["unit"]
+    assert e2e["h2d_bytes_per_step"] == 0 and e2e["d2h_bytes_per_step"] == 0
+
+
+def test_reference_arm_runs_on_rank_zero_only():
+    p = run_bench(["--impl", "reference", "--steps", "1", "--warmup", "0"],
+                  {"RANK": "1", "WORLD_SIZE": "2", "LOCAL_RANK": "1"}, timeout=120)
+    assert p.returncode == 0, p.stderr[-2000:]
+    assert p.stdout.strip() == ""
+
+
+def test_level_sizes_halve_with_ceil_down_to_one():
+    sizes = bench.level_sizes(7872, 5243)
+    assert len(sizes) == 14 and sizes[0] == (7872, 5243) and sizes[1] == (3936, 2622) and sizes[-1] == (1, 1)
+    assert bench.level_sizes(1, 1) == [(1, 1)]
+
+
+@pytest.mark.parametrize("mode", ["laps", "cache", "recompute"])
+def test_algorithmic_bytes_model(mode):
+    w, h, f, k = 7872, 5243, 30, 8
+    per_kernel, total = bench.algorithmic_bytes(w, h, f, k, mode, 4)
+    assert set(per_kernel) == {"pass1", "image", "remap_weights", "blend0", "level0", "level", "collapse",
+                               "mask_support"}
+    assert all(v >= 0 for v in per_kernel.values()) and total == sum(per_kernel.values())
+    per_px = total / (f * w * h)
+    # pass 1 reads the 3 B frame; laps and cache also keep 8 B of planes
+    assert per_kernel["pass1"] / (f * w * h) > (11 if mode in ("laps", "cache") else 3)
+    assert 25 < per_px < 100
+    if mode == "laps":
+        assert per_kernel["image"] > 0 and per_kernel["blend0"] > 0 and per_kernel["remap_weights"] == 0
+    if mode == "recompute":
+        assert per_kernel["remap_weights"] > 0
+    # FP16 storage moves fewer level bytes
+    assert bench.algorithmic_bytes(w, h, f, k, mode, 2)[1] < total
