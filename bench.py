@@ -22,7 +22,9 @@ reference's Zig path; the Zig reference cannot be built in this image) on
 the host cores for the same metric, on a bounded sample of the workload.
 
 Multi-GPU: one process per GPU (torchrun), each rank fuses its own stack
-(independent stacks, no data-path collective; weak scaling).
+(independent stacks, no data-path collective; weak scaling).  The CPU
+baseline and the precision / serving / batched forms run at N = 1 only, so
+that a scaling run holds its GPUs for the headline legs alone.
 """
 from __future__ import annotations
 
@@ -632,7 +634,7 @@ def main():
         del hframes
 
     forms = None
-    if not args.no_forms:
+    if not args.no_forms and world == 1:
         del frames
         ctx.trim()
         torch.cuda.empty_cache()
