@@ -608,7 +608,7 @@ def main():
             st.finish_into(houts[0])
             st.close()
 
-        run_stacks(2)
+        run_stacks(3)
         # latency of one stack alone
         single_stack()
         t0 = time.perf_counter()

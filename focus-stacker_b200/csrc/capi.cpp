@@ -41,6 +41,7 @@ struct fs_ctx {
   uint64_t held = 0;
   cudaStream_t stream = nullptr;
   cudaStream_t copy = nullptr;
+  cudaStream_t idle = nullptr;  // given no work: frees of finished stacks take effect at once
   std::string err;
   mutable std::mutex mu;
   bool timing = false;
@@ -132,9 +133,9 @@ int dev_alloc(fs_ctx* ctx, size_t bytes, void** out, cudaStream_t on = nullptr) 
 
 // Stream-ordered free; callers make sure the copy stream is done with the
 // buffer (stacks synchronise both streams before releasing).
-void dev_free(fs_ctx* ctx, void* p, size_t bytes) {
+void dev_free(fs_ctx* ctx, void* p, size_t bytes, cudaStream_t on = nullptr) {
   if (!p) return;
-  cudaFreeAsync(p, ctx->stream);
+  cudaFreeAsync(p, on ? on : ctx->stream);
   if (bytes == 0) bytes = 16;
   ctx->held -= std::min<uint64_t>(ctx->held, bytes);
 }
@@ -425,7 +426,8 @@ int fs_create(int device, uint64_t hbm_budget_bytes, fs_ctx** out) {
   c->budget = hbm_budget_bytes ? hbm_budget_bytes : (uint64_t)(free_b / 2);
   c->mempool = device_pool(device);
   if (!c->mempool || cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
-      cudaStreamCreateWithFlags(&c->copy, cudaStreamNonBlocking) != cudaSuccess) {
+      cudaStreamCreateWithFlags(&c->copy, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&c->idle, cudaStreamNonBlocking) != cudaSuccess) {
     delete c;
     return FS_ERR_CUDA;
   }
@@ -447,6 +449,7 @@ void fs_destroy(fs_ctx* ctx) {
   }
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   if (ctx->copy) cudaStreamDestroy(ctx->copy);
+  if (ctx->idle) cudaStreamDestroy(ctx->idle);
   delete ctx;
 }
 
@@ -1336,16 +1339,20 @@ int fs_stack_destroy(fs_stack* s) {
   if (!s) return FS_ERR_INVALID;
   if (fs_ctx* ctx = s->ctx) {
     cudaSetDevice(ctx->device);
+    cudaStream_t free_on = ctx->stream;
     if (s->done) {
-      // finished asynchronously: its last work is the output copy, and the
-      // stream-ordered frees below follow it (later stacks' work queued on
-      // the streams need not drain)
+      // finished asynchronously: its last work is the output copy, so once
+      // that is done nothing of it is in flight; its memory is freed on the
+      // idle stream, where the frees complete at once and the pool can hand
+      // it to the next stacks (the later stacks' work queued on the context's
+      // streams need not drain first)
       cudaEventSynchronize(s->done);
+      free_on = ctx->idle;
     } else {
       cudaStreamSynchronize(ctx->stream);
       cudaStreamSynchronize(ctx->copy);
     }
-    for (auto& a : s->allocs) dev_free(ctx, a.p, a.bytes);
+    for (auto& a : s->allocs) dev_free(ctx, a.p, a.bytes, free_on);
     s->allocs.clear();
     ctx->stacks.erase(s);
     detach_stack(s);
