@@ -1,4 +1,5 @@
 """CPU tests of the library's host logic and closed forms (no GPU needed)."""
+import ctypes
 import math
 import os
 
@@ -26,6 +27,20 @@ def test_status_strings_and_version():
     assert L.fs_api_version() == 1
     assert L.fs_status_string(0) == b"ok"
     assert L.fs_status_string(3) == b"device memory budget exceeded"
+
+
+def test_stack_entry_points_reject_null_handles():
+    # argument checks run before any CUDA call, so they hold without a GPU
+    L = fsb._lib.lib()
+    invalid = 1  # FS_ERR_INVALID
+    pixels = np.zeros(16, np.uint8)
+    out = np.zeros(16, np.uint8)
+    assert L.fs_stack_wait(None) == invalid
+    assert L.fs_stack_add_frame_async(None, pixels.ctypes.data, 16, None) == invalid
+    assert L.fs_stack_add_frame(None, pixels.ctypes.data, 16, None) == invalid
+    cb = ctypes.cast(None, fsb._lib.FETCH_CB)
+    assert L.fs_stack_finish_async(None, cb, None, out.ctypes.data, 16) == invalid
+    assert L.fs_stack_finish(None, cb, None, out.ctypes.data, 16) == invalid
 
 
 def test_context_without_gpu_reports_no_device():
