@@ -24,7 +24,6 @@
 #include <string.h>
 
 #include <algorithm>
-#include <mutex>
 
 #include "../../include/focuscuda.h"
 #include "fusion_kernels.cuh"
@@ -34,12 +33,8 @@ namespace {
 
 // 40 MiB: 8 aligned frames of 512 x 512, or fewer / smaller frames, fit.
 constexpr size_t kStaticScratchBytes = 40ull << 20;
-constexpr int kStaticMaxDevices = 64;
 
 __device__ __align__(256) unsigned char g_static_scratch[kStaticScratchBytes];
-
-std::mutex g_setup_mu;
-unsigned char* g_scratch_ptr[kStaticMaxDevices] = {};
 
 void put_err(char* err, size_t err_len, const char* fmt, ...) __attribute__((format(printf, 3, 4)));
 void put_err(char* err, size_t err_len, const char* fmt, ...) {
@@ -50,8 +45,12 @@ void put_err(char* err, size_t err_len, const char* fmt, ...) {
   va_end(ap);
 }
 
-// Device address of the scratch array on the current device, looked up once
-// per device (the lookup also loads the module there if it is not loaded).
+// Device address of the scratch array in the current device's context.  The
+// first call on a device loads the module there (the set-up step: make it
+// before any stream capture); later calls are a table lookup in the CUDA
+// runtime.  The address is looked up on every call and never cached, so a
+// device that was reset, or another context made current, gets the address
+// of its own copy of the array.
 int scratch_on_current_device(unsigned char** out, char* err, size_t err_len) {
   int dev = -1;
   cudaError_t e = cudaGetDevice(&dev);
@@ -59,22 +58,14 @@ int scratch_on_current_device(unsigned char** out, char* err, size_t err_len) {
     put_err(err, err_len, "cudaGetDevice: %s", cudaGetErrorString(e));
     return FS_ERR_NO_DEVICE;
   }
-  if (dev < 0 || dev >= kStaticMaxDevices) {
-    put_err(err, err_len, "device %d beyond the %d devices the static scratch tracks", dev, kStaticMaxDevices);
-    return FS_ERR_UNSUPPORTED;
+  void* p = nullptr;
+  e = cudaGetSymbolAddress(&p, g_static_scratch);
+  if (e != cudaSuccess || !p) {
+    put_err(err, err_len, "cudaGetSymbolAddress(static scratch) on device %d: %s", dev,
+            e != cudaSuccess ? cudaGetErrorString(e) : "null address");
+    return e == cudaErrorNoKernelImageForDevice || e == cudaErrorInvalidDevice ? FS_ERR_NO_DEVICE : FS_ERR_CUDA;
   }
-  std::lock_guard<std::mutex> lock(g_setup_mu);
-  if (!g_scratch_ptr[dev]) {
-    void* p = nullptr;
-    e = cudaGetSymbolAddress(&p, g_static_scratch);
-    if (e != cudaSuccess || !p) {
-      put_err(err, err_len, "cudaGetSymbolAddress(static scratch) on device %d: %s", dev,
-              e != cudaSuccess ? cudaGetErrorString(e) : "null address");
-      return e == cudaErrorNoKernelImageForDevice || e == cudaErrorInvalidDevice ? FS_ERR_NO_DEVICE : FS_ERR_CUDA;
-    }
-    g_scratch_ptr[dev] = (unsigned char*)p;
-  }
-  *out = g_scratch_ptr[dev];
+  *out = (unsigned char*)p;
   return FS_OK;
 }
 

@@ -283,8 +283,13 @@ int fs_fuse_stack(fs_ctx* ctx, const fs_stack_desc* desc, const void* const* fra
  * Needs no context and allocates no device memory, for callers that must not
  * allocate while they run.  The work is queued on `stream` (cudaStream_t of
  * the current device, NULL = default stream) and the call returns without
- * waiting for it.  The first call on a device looks up the array's address
- * (and loads the module there); make it before any stream capture.  Every
+ * waiting for it.  The first call on a device loads the module there (the
+ * set-up; make it before any stream capture); every call looks the array's
+ * address up again in the current context, so a reset device or another
+ * context never gets a stale address.  The 40 MiB are reserved on a device
+ * when the module loads there (at the first static call with lazy module
+ * loading, at context creation with CUDA_MODULE_LOADING=EAGER) and lie outside
+ * every fs_ctx budget.  Every
  * call in the process shares the array: calls must not overlap in time on the
  * device (order them on one stream or with events), or they corrupt each
  * other's planes.  A message for a failure goes to err (err_len bytes, may be
