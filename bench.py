@@ -48,8 +48,6 @@ METRIC = "fused MPix*frames/s (plain FP32 pyramid-contrast, remap+fuse)"
 UNIT = "MPix*frames/s"
 
 FRAMES, WIDTH, HEIGHT = 30, 7952, 5304
-# CPU samples: frames x width x height of the same scene (bounded CPU work)
-CPU_SAMPLE = (3, 1988, 1326)
 
 
 def parse():
@@ -387,23 +385,44 @@ def measured_hbm_peak():
 
 
 # ----------------------------------------------------------- CPU baseline
-def cpu_sample_frames(fsb, sample, seed, ctx=None, torch=None):
-    """Sample frames of the production scene: rendered on the GPU when a
-    context is given, else on the CPU (the reference arm touches no GPU)."""
-    F, W, H = sample
-    frames, poses = [], []
-    for k in range(F):
-        if ctx is not None:
-            buf = torch.empty((H, W, 3), dtype=torch.uint8, device=f"cuda:{ctx.device}")
-            poses.append(fsb.synth_frame_device(ctx, seed, fsb.SCENE_PRODUCTION, W, H, k, F, buf, W * 3))
-            frames.append(buf.cpu().numpy())
-        else:
-            from importlib import import_module
-            synth_cpu = import_module("focus_stacker_b200.synth_cpu")
-            img, pose = synth_cpu.synth_frame_cpu(seed, fsb.SCENE_PRODUCTION, W, H, k, F)
-            frames.append(img)
-            poses.append(pose)
-    return frames, poses
+# The CPU legs (cpu_baseline of this arm, and the --impl reference arm) load
+# nothing of the library: poses, ROI and frames come from the oracle (its
+# restatement of the reference's ROI and of the synthetic scene), and the timed
+# work is the oracle's stack_fuse, built with -march=native on the host that
+# runs it (strict IEEE all the same).  The sample is a full-width band of ROI
+# rows of the same 30 x 7952 x 5304 stack (all frames, the same poses, the
+# ROI's full width and so the same 14 pyramid levels); its source rows are the
+# only ones rendered.
+CPU_BAND_ROWS = 384
+
+
+def _oracle():
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    return oracle
+
+
+def cpu_band_sample(F, W, H, seed, rows=CPU_BAND_ROWS, jobs=None):
+    """Frames, poses, the stack's ROI and a band of ROI rows (left, top,
+    right, bottom) for the CPU legs; frames are rendered only where the band
+    samples them."""
+    oracle = _oracle()
+    jobs = jobs or os.cpu_count() or 1
+    poses = [oracle.synth_pose(seed, oracle.SCENE_PRODUCTION, W, H, k, F) for k in range(F)]
+    roi = oracle.compute_roi(poses, [W] * F, [H] * F)
+    left, top, right, bottom = roi
+    rows = min(rows, bottom - top)
+    b_top = top + (bottom - top - rows) // 2
+    band = (left, b_top, right, b_top + rows)
+    frames = []
+    for k, p in enumerate(poses):
+        ys = [oracle.inverse_point(p, W, H, float(x), float(y))[1]
+              for x in (left, (left + right) / 2, right) for y in (band[1], band[3])]
+        y0 = max(0, int(math.floor(min(ys))) - 4)
+        y1 = min(H, int(math.ceil(max(ys))) + 5)
+        frames.append(oracle.synth_frame(seed, oracle.SCENE_PRODUCTION, W, H, k, F, rows=(y0, y1 - y0), jobs=jobs,
+                                         native=True))
+    return frames, poses, roi, band
 
 
 def cpu_model() -> str:
@@ -417,59 +436,87 @@ def cpu_model() -> str:
     return "unknown"
 
 
-def cpu_baseline(fsb, steps=1, warmup=0, sample=CPU_SAMPLE, seed=1, ctx=None, torch=None, single_thread=False):
-    """Time the oracle (C++ restatement, all host threads) on a bounded sample;
-    with single_thread, also one thread on the sample's first two frames."""
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle
-    F, W, H = sample
-    frames, poses = cpu_sample_frames(fsb, sample, seed, ctx, torch)
-    roi = fsb.compute_common_overlap_roi([True] * F, [W] * F, [H] * F, poses)
-    cores = os.cpu_count() or 1
-    pd = [p.as_dict() for p in poses]
+def cpu_fuse_timed(sample, steps, warmup, jobs=None):
+    """Median seconds of the oracle's remap + pyramid-contrast fusion of the
+    band sample (all host threads), over `steps` runs after `warmup` runs."""
+    oracle = _oracle()
+    frames, poses, _, band = sample
+    jobs = jobs or os.cpu_count() or 1
     times = []
     for i in range(warmup + steps):
         t0 = time.perf_counter()
-        oracle.stack_fuse(frames, pd, roi.as_tuple(), jobs=cores)
+        oracle.stack_fuse(frames, poses, band, jobs=jobs, native=True)
         dt = time.perf_counter() - t0
         if i >= warmup:
             times.append(dt)
+    return times
+
+
+def band_desc(sample, F, W, H):
+    band = sample[3]
+    bw, bh = band[2] - band[0], band[3] - band[1]
+    return (f"{F} frames of {W}x{H} (production scene, the bench's poses), ROI band {bw}x{bh} (rows "
+            f"{band[1]}..{band[3]} of the stack's ROI, full ROI width, {len(level_sizes(bw, bh))} levels), oracle "
+            f"stack_fuse (remap + pyramid-contrast, FP32, built -O3 -march=native -ffp-contract=off)")
+
+
+def cpu_baseline(F, W, H, seed, single_thread=False):
+    """cpu_baseline leg: the oracle on the band sample with every host thread
+    (one warm-up, one timed run), and one thread on two of its frames."""
+    oracle = _oracle()
+    sample = cpu_band_sample(F, W, H, seed)
+    frames, poses, _, band = sample
+    cores = os.cpu_count() or 1
+    times = cpu_fuse_timed(sample, steps=1, warmup=1, jobs=cores)
     t = statistics.median(times)
-    px = F * roi.width * roi.height
+    px = F * (band[2] - band[0]) * (band[3] - band[1])
     out = {"value": px / t / 1e6, "unit": UNIT, "cores": cores, "kind": "port", "cpu_model": cpu_model(),
-           "sample": f"{F} frames of {W}x{H} (ROI {roi.width}x{roi.height}), same scene recipe, "
-                     f"oracle stack_fuse (remap + pyramid-contrast, FP32) with {cores} threads, "
-                     f"median of {len(times)} runs: {t:.2f} s"}
-    if single_thread and F >= 2:
+           "sample": band_desc(sample, F, W, H) + f", {cores} threads, {t:.2f} s per run"}
+    if single_thread:
         t0 = time.perf_counter()
-        oracle.stack_fuse(frames[:2], pd[:2], roi.as_tuple(), jobs=1)
+        oracle.stack_fuse(frames[:2], poses[:2], band, jobs=1, native=True)
         t1 = time.perf_counter() - t0
-        out["single_thread"] = {"value": 2 * roi.width * roi.height / t1 / 1e6, "unit": UNIT,
-                                "sample": f"the sample's first 2 frames, 1 thread: {t1:.2f} s"}
+        out["single_thread"] = {"value": 2 * (band[2] - band[0]) * (band[3] - band[1]) / t1 / 1e6, "unit": UNIT,
+                                "sample": f"the band's first 2 frames, 1 thread: {t1:.2f} s"}
     return out
 
 
 def run_reference(args, rank, world):
+    """--impl reference: the oracle (the C++ restatement of the reference's
+    Zig path; the Zig reference cannot be built in this image) on the host
+    cores, same metric and config as this arm, each step one fusion of the
+    band sample.  Rank 0 alone runs it; other ranks exit without work."""
     if rank != 0:
         return
-    fsb = load_package()
-    cb = cpu_baseline(fsb, steps=args.steps, warmup=args.warmup)
-    line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": UNIT, "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,
+    F, W, H = args.frames, args.width, args.height
+    sample = cpu_band_sample(F, W, H, args.seed)
+    cores = os.cpu_count() or 1
+    times = cpu_fuse_timed(sample, steps=args.steps, warmup=args.warmup, jobs=cores)
+    t = statistics.mean(times)
+    band = sample[3]
+    px = F * (band[2] - band[0]) * (band[3] - band[1])
+    value = px / t / 1e6
+    cb = {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "cpu_model": cpu_model(),
+          "sample": band_desc(sample, F, W, H) + f", {cores} threads, mean of {len(times)} runs after "
+                    f"{args.warmup} warm-up: {t:.2f} s per run"}
+    roi = sample[2]
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": workload_config(args, None, 0),
+            "config": workload_config(args, roi),
             "cpu_baseline": cb,
-            "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 
-def workload_config(args, roi, k):
+def workload_config(args, roi):
+    """The workload, the same in both arms: roi = (left, top, right, bottom)
+    of the stack's common-overlap ROI."""
+    rw, rh = roi[2] - roi[0], roi[3] - roi[1]
     return {"workload": f"{args.frames}x{args.width}x{args.height} RGB u8 synthetic focus stack "
                         "(production scene), remap + pyramid-contrast, FP32 levels",
             "frames": args.frames, "src": [args.width, args.height],
-            "roi": roi.as_tuple() if roi is not None else None,
-            "levels": len(level_sizes(roi.width, roi.height)) if roi is not None else None,
-            "frames_per_batch": k, "contrast_window": 5,
+            "roi": list(roi), "levels": len(level_sizes(rw, rh)), "contrast_window": 5,
             "l2": "inputs (frames x W x H x 3 B) larger than the 126 MB L2; no flush",
             "parallelism": f"replicas x{args.gpus} (one stack per GPU)"}
 
@@ -650,13 +697,13 @@ def main():
 
     cpu = None
     if not args.no_cpu_baseline and rank == 0 and world == 1:
-        cpu = cpu_baseline(fsb, steps=1, warmup=1, sample=(4, 3976, 2652), ctx=ctx, torch=torch, single_thread=True)
+        cpu = cpu_baseline(F, W, H, args.seed + rank, single_thread=True)
 
     if rank == 0:
         line = {"metric": METRIC, "value": round(value, 2), "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": round(ms, 4), "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-                "config": dict(workload_config(args, roi, k_eff), pass2=mode_used["mode"]),
+                "config": workload_config(args, roi.as_tuple()), "pass2": mode_used["mode"], "frames_per_batch": k_eff,
                 "e2e": e2e, "gpu_launches": launches, "clocks": clock_info, "roofline": roofline,
                 "cpu_baseline": cpu, "kernels": kernel_table, "pipeline_roofline": pipeline, "forms": forms}
         print(json.dumps(line), flush=True)

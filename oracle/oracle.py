@@ -8,6 +8,7 @@ this module, as the checker; the shipped library never calls it.
 from __future__ import annotations
 
 import ctypes
+import hashlib
 import os
 import subprocess
 
@@ -15,13 +16,7 @@ import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB_PATH = os.path.join(_HERE, "_build", "liboracle.so")
-_lib = None
-
-POSE_FIELDS = (
-    "yaw", "pitch", "roll", "hfov_delta", "trans_x", "trans_y", "trans_z",
-    "translation_plane_yaw", "translation_plane_pitch", "radial_a", "radial_b",
-    "radial_c", "center_shift_x", "center_shift_y", "base_hfov_degrees",
-)
+_libs = {}
 
 
 def build() -> str:
@@ -30,14 +25,48 @@ def build() -> str:
     return _LIB_PATH
 
 
-def lib():
-    global _lib
-    if _lib is None:
-        if not os.path.exists(_LIB_PATH):
-            build()
-        _lib = ctypes.CDLL(_LIB_PATH)
-        _bind(_lib)
-    return _lib
+def _native_path() -> str:
+    """The -march=native build for this host's CPU (one directory per CPU
+    model and flag set, built on first use): the timed CPU baseline."""
+    key = ""
+    try:
+        with open("/proc/cpuinfo") as fh:
+            for line in fh:
+                if line.startswith(("model name", "flags")):
+                    key += line
+                if line.strip() == "":
+                    break
+    except OSError:
+        key = "unknown"
+    tag = hashlib.sha1(key.encode()).hexdigest()[:12]
+    out = os.path.join(_HERE, "_build", "native-" + tag)
+    subprocess.run(["make", "-s", "-C", _HERE, "native", "NATIVE_OUT=" + out], check=True)
+    return os.path.join(out, "liboracle.so")
+
+
+def lib(native: bool = False):
+    """The oracle library: the portable build (parity checks), or with
+    native=True the -march=native build for this host (timed baselines; the
+    same strict-IEEE arithmetic, so the same results)."""
+    key = "native" if native else "portable"
+    if key not in _libs:
+        if native:
+            path = _native_path()
+        else:
+            path = _LIB_PATH
+            if not os.path.exists(path):
+                build()
+        L = ctypes.CDLL(path)
+        _bind(L)
+        _libs[key] = L
+    return _libs[key]
+
+
+POSE_FIELDS = (
+    "yaw", "pitch", "roll", "hfov_delta", "trans_x", "trans_y", "trans_z",
+    "translation_plane_yaw", "translation_plane_pitch", "radial_a", "radial_b",
+    "radial_c", "center_shift_x", "center_shift_y", "base_hfov_degrees",
+)
 
 
 class _Pose(ctypes.Structure):
@@ -88,6 +117,8 @@ def _bind(L):
     L.oracle_fuse_aligned.restype = i32
     L.oracle_stack_fuse.argtypes = [P(vp), sz, u32, u32, i32, P(_Pose), P(ctypes.c_int32), u32, i32, i32, vp, dp]
     L.oracle_stack_fuse.restype = i32
+    L.oracle_synth_pose.argtypes = [ctypes.c_uint64, i32, u32, u32, u32, u32, P(_Pose)]
+    L.oracle_synth_render.argtypes = [ctypes.c_uint64, i32, u32, u32, u32, u32, u32, u32, vp, sz, i32]
 
 
 def _ptr(a: np.ndarray, ctype=None):
@@ -217,8 +248,9 @@ def fuse_aligned(frames, window=5, jobs=1, precision=32, want_base=False):
     return (out, base) if want_base else out
 
 
-def stack_fuse(sources, poses, roi=None, window=5, jobs=1, precision=32, want_base=False):
-    """sources: list of HxWx3 uint8/uint16 frames; poses: list of pose dicts."""
+def stack_fuse(sources, poses, roi=None, window=5, jobs=1, precision=32, want_base=False, native=False):
+    """sources: list of HxWx3 uint8/uint16 frames; poses: list of pose dicts.
+    native=True runs the -march=native build (timed baselines)."""
     sources = [np.ascontiguousarray(s) for s in sources]
     h, w = sources[0].shape[:2]
     bits = 8 if sources[0].dtype == np.uint8 else 16
@@ -229,8 +261,32 @@ def stack_fuse(sources, poses, roi=None, window=5, jobs=1, precision=32, want_ba
     out = np.zeros((oh, ow, 3), sources[0].dtype)
     base = np.zeros((oh, ow, 3), np.float64) if want_base else None
     r = np.asarray(roi, np.int32)
-    rc = lib().oracle_stack_fuse(ptrs, len(sources), w, h, bits, pose_array(poses), _ptr(r, ctypes.c_int32), window,
+    rc = lib(native).oracle_stack_fuse(ptrs, len(sources), w, h, bits, pose_array(poses), _ptr(r, ctypes.c_int32),
+                                       window,
                                  jobs, precision, _ptr(out), _ptr(base, ctypes.c_double) if want_base else None)
     if rc != 0:
         raise RuntimeError("oracle_stack_fuse failed")
     return (out, base) if want_base else out
+
+
+# ------------------------------------------------------ synthetic stacks
+SCENE_SMALL, SCENE_PRODUCTION = 0, 1
+
+
+def synth_pose(seed, scene, width, height, frame, frame_count) -> dict:
+    """Pose of synthetic frame `frame` as a dict of ImagePose fields (the
+    device generator's draws)."""
+    p = (_Pose * 1)()
+    lib().oracle_synth_pose(seed, scene, width, height, frame, frame_count, p)
+    return dict(zip(POSE_FIELDS, list(p[0].v)))
+
+
+def synth_frame(seed, scene, width, height, frame, frame_count, rows=None, jobs=1, native=False):
+    """Synthetic frame `frame` rendered on the CPU (HxWx3 uint8).  rows =
+    (first, count) renders only those rows; the others stay zero and untouched
+    (their pages are never written)."""
+    img = np.zeros((height, width, 3), np.uint8)
+    r0, n = (0, height) if rows is None else rows
+    lib(native).oracle_synth_render(seed, scene, width, height, frame, frame_count, max(0, r0), max(0, n),
+                                    _ptr(img), width * 3, jobs)
+    return img

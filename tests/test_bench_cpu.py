@@ -21,8 +21,11 @@ def run_bench(args, env_extra=None, timeout=600):
     return p
 
 
+SMALL = ["--frames", "4", "--width", "2048", "--height", "1536"]
+
+
 def test_reference_arm_prints_the_contract_line():
-    p = run_bench(["--impl", "reference", "--steps", "1", "--warmup", "0"])
+    p = run_bench(["--impl", "reference", "--steps", "1", "--warmup", "0"] + SMALL)
     assert p.returncode == 0, p.stderr[-2000:]
     line = json.loads(p.stdout.strip().splitlines()[-1])
     assert line["impl"] == "reference"
@@ -33,10 +36,32 @@ def test_reference_arm_prints_the_contract_line():
     e2e = line["e2e"]
     assert e2e["value"] == line["value"] and e2e["unit"] == line["unit"]
     assert e2e["h2d_bytes_per_step"] == 0 and e2e["d2h_bytes_per_step"] == 0
+    # the same workload description as the GPU arm: the ROI is the oracle's
+    # restatement of the reference's computeCommonOverlapRoi
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    poses = [oracle.synth_pose(1, oracle.SCENE_PRODUCTION, 2048, 1536, k, 4) for k in range(4)]
+    roi = oracle.compute_roi(poses, [2048] * 4, [1536] * 4)
+    cfg = line["config"]
+    assert cfg["roi"] == list(roi) and cfg["frames"] == 4 and cfg["src"] == [2048, 1536]
+    assert cfg["levels"] == len(bench.level_sizes(roi[2] - roi[0], roi[3] - roi[1]))
+
+
+def test_reference_arm_loads_only_the_oracle():
+    """The CPU arm maps no part of the CUDA library: frames, poses and the ROI
+    come from the oracle."""
+    code = ("import runpy, sys; sys.argv = ['bench.py', '--impl', 'reference', '--steps', '1', '--warmup', '0', "
+            + ", ".join(repr(a) for a in SMALL) + "]; runpy.run_path('bench.py', run_name='__main__'); "
+            "maps = open('/proc/self/maps').read(); "
+            "print('LIBS', sorted({l.split()[-1] for l in maps.splitlines() if '.so' in l and 'repo' in l}))")
+    p = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=600, cwd=ROOT)
+    assert p.returncode == 0, p.stderr[-2000:]
+    libs = [ln for ln in p.stdout.splitlines() if ln.startswith("LIBS")][0]
+    assert "libfocuscuda" not in libs and "liboracle" in libs, libs
 
 
 def test_reference_arm_runs_on_rank_zero_only():
-    p = run_bench(["--impl", "reference", "--steps", "1", "--warmup", "0"],
+    p = run_bench(["--impl", "reference", "--steps", "1", "--warmup", "0"] + SMALL,
                   {"RANK": "1", "WORLD_SIZE": "2", "LOCAL_RANK": "1"}, timeout=120)
     assert p.returncode == 0, p.stderr[-2000:]
     assert p.stdout.strip() == ""

@@ -292,3 +292,20 @@ def test_poisson_stream_shape():
     sizes = {(r.width, r.height) for r in reqs}
     assert sizes <= set(fsb.serving.SIZE_MIX) | {fsb.serving.LARGE}
     assert all(4 <= r.frames <= (143 if (r.width, r.height) == fsb.serving.LARGE else 40) for r in reqs)
+
+
+@pytest.mark.parametrize("scene,frame", [(0, 0), (0, 5), (1, 3), (1, 29)])
+def test_oracle_synthetic_poses_equal_the_library_generator(scene, frame):
+    """The CPU legs of bench.py draw poses from the oracle's restatement of
+    the generator; they must be the library's poses."""
+    got = oracle.synth_pose(1, scene, 7952, 5304, frame, 30)
+    want = fsb.synth_pose(1, scene, 7952, 5304, frame, 30).as_dict()
+    assert got == want
+
+
+def test_oracle_synthetic_frame_rows_and_statistics():
+    full = oracle.synth_frame(3, oracle.SCENE_SMALL, 320, 240, 2, 8, jobs=4)
+    part = oracle.synth_frame(3, oracle.SCENE_SMALL, 320, 240, 2, 8, rows=(100, 20), jobs=3)
+    assert np.array_equal(part[100:120], full[100:120])
+    assert not part[:100].any() and not part[120:].any()
+    assert 90 < full.mean() < 160 and 15 < full.std() < 60
