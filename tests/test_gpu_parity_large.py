@@ -1,0 +1,132 @@
+"""GPU parity at large levels and at the production stack size, through the
+C ABI, against the CPU oracle.
+
+The reference expands with the clamped separable filter whenever a level
+side exceeds 512 (src/fuse/pyramid.zig:859-861, 1101-1149, 1748-1775); only
+stacks whose ROI is wider than 2048 take that path at levels 1 and 2 too.
+These tests fuse such stacks in every pass-2 mode (laps: the streaming image
+pyramid kernels; cache / resident / refetch: the tiled level kernels with
+exact_expand = 0; collapse in the clamped mode at each of those levels) and
+the full 30 x 7952 x 5304 production stack, and compare each with the
+oracle's FP32 evaluation: collapsed base within one 16-bit LSB (1/257 in
+8-bit units), u8 output within 1, and the remap's alpha bit-exact.
+"""
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+from __graft_entry__ import load_package
+
+fsb = load_package()
+pytestmark = pytest.mark.gpu
+
+LSB16 = 1.0 / 257.0
+JOBS = os.cpu_count() or 1
+
+
+@pytest.fixture(scope="module")
+def torch():
+    t = pytest.importorskip("torch")
+    if not t.cuda.is_available():
+        pytest.skip("no CUDA device")
+    return t
+
+
+@pytest.fixture(scope="module")
+def ctx(torch):
+    c = fsb.Context(0)
+    yield c
+    c.close()
+
+
+def synth(torch, ctx, W, H, F, seed, scene):
+    frames, poses = [], []
+    for k in range(F):
+        buf = torch.empty((H, W, 3), dtype=torch.uint8, device="cuda:0")
+        poses.append(fsb.synth_frame_device(ctx, seed, scene, W, H, k, F, buf, W * 3))
+        frames.append(buf.cpu().numpy())
+    return frames, poses
+
+
+def fuse(torch, ctx, frames, poses, roi, mode, frames_per_batch=0):
+    H, W = frames[0].shape[:2]
+    st = fsb.PyramidContrastStack(ctx, W, H, len(frames), roi=roi, pass2_mode=mode,
+                                  frames_per_batch=frames_per_batch)
+    assert st.pass2_mode == mode
+    base = torch.zeros((roi.height, roi.width, 3), dtype=torch.float32, device="cuda:0")
+    st.set_base_output(base, roi.width * 3)
+    for f, p in zip(frames, poses):
+        st.add_frame(f, p)
+    out = st.finish(refetch=lambda i: frames[i])
+    st.close()
+    return out, base.cpu().numpy().astype(np.float64)
+
+
+def check(out, base, ref_out, ref_base):
+    d = np.abs(base - ref_base)
+    assert d.max() <= LSB16, f"max |base diff| = {d.max()} ({d.max() * 257:.3f} LSB16)"
+    du = np.abs(out.astype(np.int32) - ref_out.astype(np.int32))
+    assert du.max() <= 1, int(du.max())
+
+
+@pytest.fixture(scope="module")
+def wide_stack(torch, ctx):
+    # ROI about 2500 x 1760: levels 0, 1 and 2 (1250, 625 wide) expand with
+    # the clamped filter, levels 3 and up with the no-wrap one
+    W, H, F = 2560, 1800, 4
+    frames, poses = synth(torch, ctx, W, H, F, seed=77, scene=fsb.SCENE_SMALL)
+    roi = fsb.compute_common_overlap_roi([True] * F, [W] * F, [H] * F, poses)
+    assert roi.width > 2048 and (roi.width + 3) // 4 > 512
+    ref = oracle.stack_fuse(frames, [p.as_dict() for p in poses], roi.as_tuple(), jobs=JOBS, want_base=True)
+    return frames, poses, roi, ref
+
+
+@pytest.mark.parametrize("mode", ["laps", "cache", "resident", "refetch"])
+def test_clamped_expand_levels_match_oracle(torch, ctx, wide_stack, mode):
+    frames, poses, roi, (ref_out, ref_base) = wide_stack
+    out, base = fuse(torch, ctx, frames, poses, roi, mode, frames_per_batch=3)
+    check(out, base, ref_out, ref_base)
+
+
+def test_clamped_expand_levels_reduced_storage_within_u8(torch, ctx, wide_stack):
+    # FP16 level storage on the same stack: u8 output within 1 of the oracle
+    frames, poses, roi, (ref_out, _) = wide_stack
+    H, W = frames[0].shape[:2]
+    st = fsb.PyramidContrastStack(ctx, W, H, len(frames), roi=roi, level_storage=fsb.STORAGE_F16)
+    for f, p in zip(frames, poses):
+        st.add_frame(f, p)
+    out = st.finish()
+    st.close()
+    assert np.abs(out.astype(np.int32) - ref_out.astype(np.int32)).max() <= 1
+
+
+def _mem_available_gb():
+    try:
+        with open("/proc/meminfo") as fh:
+            for line in fh:
+                if line.startswith("MemAvailable:"):
+                    return int(line.split()[1]) / 1e6
+    except OSError:
+        pass
+    return 0.0
+
+
+def test_production_stack_matches_oracle(torch, ctx):
+    """The benchmark's stack itself: 30 frames of 7952 x 5304 (production
+    scene, ROI about 7872 x 5243, 14 levels), in the mode the library picks
+    for it, against the oracle on every host thread (about a minute)."""
+    if _mem_available_gb() < 24:
+        pytest.skip("the oracle's evaluation of this stack needs about 16 GB of host memory")
+    W, H, F = 7952, 5304, 30
+    frames, poses = synth(torch, ctx, W, H, F, seed=1, scene=fsb.SCENE_PRODUCTION)
+    roi = fsb.compute_common_overlap_roi([True] * F, [W] * F, [H] * F, poses)
+    assert roi.as_tuple() == oracle.compute_roi([p.as_dict() for p in poses], [W] * F, [H] * F)
+    st = fsb.PyramidContrastStack(ctx, W, H, F, roi=roi)
+    mode = st.pass2_mode
+    st.close()
+    out, base = fuse(torch, ctx, frames, poses, roi, mode)
+    ref_out, ref_base = oracle.stack_fuse(frames, [p.as_dict() for p in poses], roi.as_tuple(), jobs=JOBS,
+                                          want_base=True)
+    check(out, base, ref_out, ref_base)
