@@ -154,7 +154,9 @@ def algorithmic_bytes(roi_w, roi_h, frames, k, mode="cache", storage_bytes=4):
     the remapped frame (RGBA, 4 B) and its weight (4 B) for pass 2; "recompute":
     pass 2 remaps again into per-batch slots; "laps": pass 1 also builds the
     Gaussian/Laplacian pyramids ("image") and pass 2 only the masks and the
-    blend.  Returns {kernel: bytes per step} and the pipeline total."""
+    blend, with level 0 fused into pass 1 (remap, weights, level-1 REDUCE,
+    Laplacian x weight summed over frames; pass 2 divides that sum by the
+    weight sum).  Returns {kernel: bytes per step} and the pipeline total."""
     sz = level_sizes(roi_w, roi_h)
     A = [w * h for w, h in sz]
     L = len(sz)
@@ -190,17 +192,23 @@ def algorithmic_bytes(roi_w, roi_h, frames, k, mode="cache", storage_bytes=4):
     b["image"] = 0
     b["blend0"] = 0
     if mode == "laps":
-        # pass 1 builds each frame's Gaussian/Laplacian pyramid: RGBA read,
-        # per level the Laplacian written (12 B) and the next Gaussian and
-        # support written (3s + 1) and read again by the next level
-        img = 4 * A[0]
-        for l in range(L - 1):
-            img += 12 * A[l] + (3 * s + 1) * A[l + 1] + ((3 * s + 1) * A[l] if l >= 1 else 0)
+        # fused pass 1: frame 3 B/px read, weight (4 B) and level-1 Gaussian
+        # + support (3s + 1 B at 1/4 area) written per frame; weight sum f32,
+        # union u8 and the level-0 sum A_w (3 x f32) read + written per batch
+        # (the first batch only writes); A_u touches the window border only
+        b["pass1"] = frames * (3 * A[0] + 4 * A[0] + (3 * s + 1) * l1) + batches * 34 * A[0] - 17 * A[0]
+        # levels >= 1 of each frame's image pyramid: read G_l + support,
+        # write the Laplacian (12 B) and G_{l+1} + support (the top one f32)
+        img = 0
+        for l in range(1, L - 1):
+            nxt = (3 * s + 1) * A[l + 1] if l + 2 < L else 12 * A[l + 1]
+            img += (3 * s + 1) * A[l] + 12 * A[l] + nxt
         b["image"] = frames * img
-        b["blend0"] = frames * 20 * A[0] + 16 * A[0]  # Laplacian 12 + weight 4 read, mask 4 written
-        # level 0: mask REDUCE of every frame (mask 4 B read, level-1 mask
-        # written in storage type) and the union support read once
-        b["level0"] = frames * (4 * A[0] + (s if L > 2 else 4) * l1) + A[0]
+        # finalize: A_w (12) and the weight sum (4) read, acc0 (12) written
+        b["blend0"] = 28 * A[0]
+        # level 0: mask REDUCE of every frame from its weight and the weight
+        # sum (w 4 B per frame, N and the union once), level-1 mask written
+        b["level0"] = frames * (4 * A[0] + (s if L > 2 else 4) * l1) + 5 * A[0]
         # levels >= 1: mask REDUCE (mask read, next mask written; the top one
         # in f32; support once) and the blend of each level over all frames
         # (Laplacian 12 B and mask read per frame, accumulator 12 B written)

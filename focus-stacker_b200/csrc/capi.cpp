@@ -172,10 +172,14 @@ int64_t round_up(int64_t v, int64_t m) { return (v + m - 1) / m * m; }
 //  REFETCH   frames are only staged; pass 2 asks the caller for them again
 //            and remaps them (src/stack/pipeline.zig:561-597).
 //  LAPS      pass 1 also builds each frame's Gaussian/Laplacian pyramid (it
-//            does not depend on the weight sum) and keeps its Laplacians and
-//            weight; pass 2 is then only the mask pyramid and the blend.  Same
-//            operations, so the same bytes as the other modes; it moves most
-//            of pass 2 into pass 1, which overlaps the frame uploads.
+//            does not depend on the weight sum): one fused kernel remaps,
+//            weights, reduces to level 1 and blends level 0 as A_w += lap0 * w
+//            (divided by the weight sum once it is complete), and the levels
+//            above keep their Laplacians and the frame its weight; pass 2 is
+//            then only the mask pyramid and the blend of levels >= 1.  Level 0
+//            rounds in another order than the batch modes (within a few ulp of
+//            the accumulator); the levels above give the same bytes.  It moves
+//            most of pass 2 into pass 1, which overlaps the frame uploads.
 enum Pass2Mode { P2_CACHE = 0, P2_RESIDENT = 1, P2_REFETCH = 2, P2_LAPS = 3 };
 
 struct fs_stack {
@@ -194,9 +198,10 @@ struct fs_stack {
   std::vector<float*> acc;     // per level, 3 planes
   std::vector<std::vector<LevelPlanes>> slot;  // [k][l], l = 1 .. L-2
   std::vector<FramePlanes> cache;              // CACHE: per frame
-  std::vector<FramePlanes> p2;                 // RESIDENT / REFETCH / LAPS: per batch slot (K)
+  std::vector<FramePlanes> p2;                 // RESIDENT / REFETCH: per batch slot (K)
   std::vector<float*> wplane;                  // LAPS: per frame, its weight (level 0)
-  std::vector<std::vector<float*>> lap;        // LAPS: per frame, Laplacian of levels 0 .. L-2
+  std::vector<std::vector<float*>> lap;        // LAPS: per frame, Laplacian of levels 1 .. L-2 ([0] unused)
+  float* au = nullptr;                         // LAPS: sum of level-0 Laplacians where the weight sum <= 1e-12
   std::vector<float*> gtop;                    // LAPS: per frame, Gaussian of the top level
   std::vector<std::vector<void*>> mplane;      // LAPS: per frame, mask of levels 1 .. L-2 (storage type)
   std::vector<float*> mtop;                    // LAPS: per frame, mask of the top level (f32)
@@ -296,7 +301,6 @@ int launch_remap_weights_batch(fs_stack* s, const std::vector<fs_stack::Frame>& 
     if (!build_frame_in(s, frames[k], &a.f[k - begin], &why)) return set_err(s->ctx, FS_ERR_INVALID, why);
     if (pass1) {
       if (s->mode == P2_CACHE) a.out[k - begin] = s->cache[k];
-      if (s->mode == P2_LAPS) a.out[k - begin] = FramePlanes{s->p2[k - begin].rgba, s->wplane[k]};
     } else {
       a.out[k - begin] = s->p2[k - begin];
     }
@@ -330,18 +334,49 @@ void level_geometry(const fs_stack* s, uint32_t l, LevelArgs* a) {
   }
 }
 
-// LAPS pass 1: the Gaussian / Laplacian pyramid of frames [begin, end), one
-// frame per CTA, from their remapped RGBA in the batch slots.
+// LAPS pass 1, level 0 of frames [begin, end): remap, weights (weight sum
+// and union), level-1 Gaussian into the batch slots, A_w += lap0 * w.
+int launch_lap0_batch(fs_stack* s, size_t begin, size_t end) {
+  Lap0Args a;
+  std::memset(&a, 0, sizeof(a));
+  a.W = (int32_t)s->W;
+  a.H = (int32_t)s->H;
+  a.window_ok = (s->W >= s->d.contrast_window && s->H >= s->d.contrast_window) ? 1 : 0;
+  a.K = (int32_t)(end - begin);
+  a.first = begin == 0 ? 1 : 0;
+  a.exact_expand = std::max(s->lw[0], s->lh[0]) <= kExactExpandMaxDim ? 1 : 0;
+  a.wn = (int32_t)s->lw[1];
+  a.hn = (int32_t)s->lh[1];
+  a.storage = s->storage;
+  a.pitch = s->pitch[0];
+  a.pitch_n = s->pitch[1];
+  a.plane = s->pitch[0] * s->lh[0];
+  a.norm = s->norm;
+  a.uni = s->uni;
+  a.aw = s->acc[0];
+  a.au = s->au;
+  for (size_t k = begin; k < end; ++k) {
+    std::string why;
+    if (!build_frame_in(s, s->frames[k], &a.f[k - begin], &why)) return set_err(s->ctx, FS_ERR_INVALID, why);
+    a.w[k - begin] = s->wplane[k];
+    a.g1[k - begin] = s->slot[k - begin][1];
+  }
+  cudaError_t e = timed(s->ctx, "pass1", [&] { return launch_lap0(a, (int)s->border, s->ctx->stream); });
+  if (e != cudaSuccess) return cuda_err(s->ctx, e, "fused pass-1 launch");
+  return FS_OK;
+}
+
+// LAPS pass 1: the Gaussian / Laplacian pyramid of levels >= 1 of frames
+// [begin, end) from their level-1 Gaussians in the batch slots.
 int launch_image_pyramid(fs_stack* s, size_t begin, size_t end) {
   LevelArgs a;
   std::memset(&a, 0, sizeof(a));
   a.levels = (int32_t)s->L;
   a.K = (int32_t)(end - begin);
-  for (uint32_t l = 0; l + 1 < s->L; ++l) {
+  for (uint32_t l = 1; l + 1 < s->L; ++l) {
     level_geometry(s, l, &a);
     for (size_t k = 0; k < (size_t)a.K; ++k) {
-      a.in0[k] = s->p2[k];
-      if (l >= 1) a.in[k] = s->slot[k][l];
+      a.in[k] = s->slot[k][l];
       a.out[k] = l + 1 < s->L - 1 ? s->slot[k][l + 1] : LevelPlanes{};
       a.lap[k] = s->lap[begin + k][l];
       a.gtop[k] = s->gtop[begin + k];
@@ -363,7 +398,8 @@ int run_pending_pass1(fs_stack* s, bool flush) {
     const size_t to_come = s->d.frame_count - s->frames.size();
     if (!(pending >= s->K || (pending > 0 && (flush || to_come <= kTailFrames)))) break;
     size_t begin = s->pass1_done, end = std::min(s->frames.size(), begin + s->K);
-    int rc = launch_remap_weights_batch(s, s->frames, begin, end, true);
+    int rc = s->mode == P2_LAPS ? launch_lap0_batch(s, begin, end)
+                                : launch_remap_weights_batch(s, s->frames, begin, end, true);
     if (rc != FS_OK) return rc;
     // the staging buffers of these frames are free for reuse after this remap
     for (size_t f = begin; f < end; ++f) {
@@ -673,6 +709,7 @@ struct StackPlan {
   uint32_t fp_level = 0;     // first level l >= 1 run one frame per CTA (L - 1: none)
   size_t contrib = 0, contrib_top = 0;  // bytes of the contribution buffers
   size_t laps_frame = 0;                // LAPS: weight, Laplacians, top Gaussian and masks of one frame
+  size_t laps_fixed = 0;                // LAPS: the level-0 Laplacian sum of the fallback pixels
 };
 
 // Levels with fewer 64x32 tiles than this run one frame per CTA (grid.z = K)
@@ -720,10 +757,11 @@ StackPlan plan_stack(const fs_stack_desc& d) {
   }
   if (p.L >= 3) {
     p.laps_frame = n0 * 4;
-    for (uint32_t l = 0; l + 1 < p.L; ++l) p.laps_frame += (size_t)p.pitch[l] * p.lh[l] * 12;
+    for (uint32_t l = 1; l + 1 < p.L; ++l) p.laps_frame += (size_t)p.pitch[l] * p.lh[l] * 12;
     p.laps_frame += (size_t)p.pitch[p.L - 1] * p.lh[p.L - 1] * 12;  // top Gaussian
     for (uint32_t l = 1; l + 1 < p.L; ++l) p.laps_frame += (size_t)p.pitch[l] * p.lh[l] * esz;  // masks
     p.laps_frame += (size_t)p.pitch[p.L - 1] * p.lh[p.L - 1] * 4;  // top mask
+    p.laps_fixed = n0 * 12;
   }
   if (p.fp_level + 1 < p.L) {
     p.contrib = (size_t)p.K * 3 * p.pitch[p.fp_level] * p.lh[p.fp_level] * 4;
@@ -739,8 +777,7 @@ uint64_t plan_bytes(const StackPlan& p, uint32_t frames, Pass2Mode mode, bool ho
   const uint64_t staging = host_frames ? (uint64_t)p.frame_bytes * p.staging_slots : 0;
   switch (mode) {
     case P2_LAPS:
-      return p.fixed + (uint64_t)p.planes / 2 * p.K + ((uint64_t)p.laps_frame + 2 * p.L * sizeof(float*)) * frames +
-             staging;
+      return p.fixed + p.laps_fixed + ((uint64_t)p.laps_frame + 2 * p.L * sizeof(float*)) * frames + staging;
     case P2_CACHE: return p.fixed + (uint64_t)p.planes * frames + staging;
     case P2_RESIDENT: return p.fixed + (uint64_t)p.planes * p.K + (uint64_t)p.frame_bytes * frames;
     default: return p.fixed + (uint64_t)p.planes * p.K + staging;
@@ -834,17 +871,15 @@ static int begin_impl(fs_ctx* ctx, const fs_stack_desc* desc, fs_stack** out, in
   s->mode = forced_mode >= 0 ? (Pass2Mode)forced_mode : choose_mode(plan, d.frame_count, available, true);
   const size_t planes_bytes = plan.planes;
   if (s->mode == P2_LAPS) {
-    for (uint32_t kk = 0; kk < s->K; ++kk) {
-      if ((rc = stack_alloc(s, n0 * 4, &p)) != FS_OK) return fail(rc);
-      s->p2.push_back(FramePlanes{(uint32_t*)p, nullptr});
-    }
+    if ((rc = stack_alloc(s, plan.laps_fixed, &p)) != FS_OK) return fail(rc);
+    s->au = (float*)p;
     for (uint32_t f = 0; f < d.frame_count; ++f) {
       if ((rc = stack_alloc(s, plan.laps_frame, &p)) != FS_OK) return fail(rc);
       uint8_t* q = (uint8_t*)p;
       s->wplane.push_back((float*)q);
       q += n0 * 4;
-      std::vector<float*> lv;
-      for (uint32_t l = 0; l + 1 < s->L; ++l) {
+      std::vector<float*> lv(1, nullptr);  // level 0 is blended by the fused pass-1 kernel
+      for (uint32_t l = 1; l + 1 < s->L; ++l) {
         lv.push_back((float*)q);
         q += (size_t)s->pitch[l] * s->lh[l] * 12;
       }
@@ -1036,13 +1071,13 @@ static int pass2_impl(fs_stack* s, fs_frame_fetch_cb refetch, void* user) {
   const size_t N = s->frames.size();
   const float inv_count = 1.0f / (float)(s->frame_total ? s->frame_total : N);
   if (s->mode == P2_LAPS) {
-    // level-0 blend of every frame at once, streaming over the Laplacians
-    // (it also turns each frame's weight into its normalised mask)
+    // level 0: the weighted Laplacian sum of pass 1 divided by the complete
+    // weight sum (the 1/N fallback from the plain sum)
     e = timed(ctx, "blend0", [&] {
-      return launch_blend0(s->acc[0], s->pitch[0] * s->lh[0], s->pitch[0], (int)s->W, (int)s->H, s->norm, s->tab,
-                           (float* const*)(s->tab + N), (int)N, inv_count, st);
+      return launch_finalize0(s->acc[0], s->au, s->norm, s->pitch[0] * s->lh[0], s->pitch[0], (int)s->W, (int)s->H,
+                              inv_count, st);
     });
-    if (e != cudaSuccess) return cuda_err(ctx, e, "level-0 blend");
+    if (e != cudaSuccess) return cuda_err(ctx, e, "level-0 finalize");
     // the mask pyramid of every frame, level by level (one frame per grid z)
     for (uint32_t l = 0; l + 1 < s->L; ++l) {
       MaskReduceArgs m;
@@ -1055,6 +1090,9 @@ static int pass2_impl(fs_stack* s, fs_frame_fetch_cb refetch, void* user) {
       m.hn = (int32_t)s->lh[l + 1];
       m.pitch_l = s->pitch[l];
       m.pitch_n = s->pitch[l + 1];
+      // level 0: each frame's raw weight, normalised by the weight sum on the fly
+      m.norm = l == 0 ? s->norm : nullptr;
+      m.inv_count = inv_count;
       const int in_storage = l == 0 ? FS_STORAGE_F32 : s->storage;
       const int out_storage = l + 2 < s->L ? s->storage : FS_STORAGE_F32;
       e = timed(ctx, l == 0 ? "level0" : "level",

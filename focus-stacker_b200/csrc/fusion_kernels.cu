@@ -11,13 +11,16 @@
 // level_kernel<T>          the same step for level l >= 1 from HBM planes
 //                          stored as T (f32 / f16 / bf16)
 // The split pyramid (LAPS mode):
-// img_stream_kernel<T, L0> pass 1, each frame's Gaussian REDUCE and Laplacian
-//                          on the clamped-EXPAND levels, streaming down
+// lap0_kernel<B>           pass 1, level 0 fused: remap -> weight -> level-1
+//                          Gaussian REDUCE -> EXPAND -> sum over frames of
+//                          Laplacian x weight (divided by the weight sum in
+//                          pass 2, finalize0_kernel)
+// img_stream_kernel<T>     pass 1, each frame's Gaussian REDUCE and Laplacian
+//                          on the clamped-EXPAND levels >= 1, streaming down
 //                          column strips without shared memory
-// img_kernel<T, L0>        the same on the small (no-wrap) levels, per tile
-// blend0_kernel            pass 2, level 0: masks = w / weight sum, blend of
-//                          every frame in order, one pixel per thread
+// img_kernel<T>            the same on the small (no-wrap) levels, per tile
 // mask_reduce_kernel       each frame's mask pyramid, one level per launch
+//                          (level 0 normalises the weights on the fly)
 // blend_kernel<T>          the blend of one level l >= 1 over every frame
 // Both:
 // collapse_kernel          parent += EXPAND(child); quantise at level 0
@@ -58,6 +61,12 @@ struct DeviceOnce {
     return e;
   }
 };
+
+// Raise a kernel's dynamic shared-memory limit once per device.
+template <typename K>
+static cudaError_t configure(K kernel, size_t bytes, DeviceOnce* done) {
+  return done->run([&] { return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes); });
+}
 
 namespace {
 
@@ -973,7 +982,7 @@ __device__ void store_next_image(const ImgSmem& S, const LevelArgs& a, int x0, i
 
 }  // namespace
 
-template <typename T, bool L0>
+template <typename T>
 __global__ void __launch_bounds__(NT) img_kernel(const __grid_constant__ LevelArgs a) {
   extern __shared__ __align__(16) uint8_t smem_raw[];
   ImgSmem& S = *reinterpret_cast<ImgSmem*>(smem_raw);
@@ -990,27 +999,15 @@ __global__ void __launch_bounds__(NT) img_kernel(const __grid_constant__ LevelAr
       v[j] = make_float4(0.f, 0.f, 0.f, 0.f);
       if (i < GH * GW && X >= 0 && Y >= 0 && X < a.wl && Y < a.hl) {
         const int64_t o = (int64_t)Y * a.pitch_l + X;
-        if constexpr (L0) {
-          const uint32_t q = __ldg(a.in0[k].rgba + o);
-          v[j] = make_float4(__uint_as_float(q), 0.f, 0.f, 0.f);
-        } else {
-          const LevelPlanes& in = a.in[k];
-          const T* g = (const T*)in.g;
-          v[j] = make_float4(ldv<T>(g, o), ldv<T>(g, in.plane + o), ldv<T>(g, 2 * in.plane + o),
-                             in.s[o] ? 1.0f : 0.0f);
-        }
+        const LevelPlanes& in = a.in[k];
+        const T* g = (const T*)in.g;
+        v[j] = make_float4(ldv<T>(g, o), ldv<T>(g, in.plane + o), ldv<T>(g, 2 * in.plane + o), in.s[o] ? 1.0f : 0.0f);
       }
     }
 #pragma unroll
     for (int j = 0; j < HALF; ++j) {
       const int i = threadIdx.x + (h * HALF + j) * NT;
-      if (i >= GH * GW) continue;
-      if constexpr (L0) {
-        const uint32_t q = __float_as_uint(v[j].x);
-        S.gs[i] = make_float4(chf(q, 0), chf(q, 1), chf(q, 2), px_alpha(q) > 0 ? 1.0f : 0.0f);
-      } else {
-        S.gs[i] = v[j];
-      }
+      if (i < GH * GW) S.gs[i] = v[j];
     }
   }
   __syncthreads();
@@ -1018,47 +1015,6 @@ __global__ void __launch_bounds__(NT) img_kernel(const __grid_constant__ LevelAr
   store_next_image<T>(S, a, x0, y0, k);
   float unused[PPT][3];
   expand_blend_step<true>(S, a, x0, y0, unused, a.lap[k]);
-}
-
-// Level-0 blend of a whole stack in frame order, one pixel per thread:
-// acc = sum over frames of lap_k * (w_k / weight sum) (1 / N where the sum
-// is <= 1e-12), the same products and sums the per-batch kernels form.
-// The normalised mask replaces each frame's weight in place (the level-0
-// mask REDUCE then reads it without dividing again).
-__global__ void blend0_kernel(float* acc, int64_t plane, int64_t pitch, int w, int h, const float* norm,
-                              const float* const* lap, float* const* wgt, int frames, float inv_count) {
-  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= (int64_t)w * h) return;
-  const int64_t o = (i / w) * pitch + i % w;
-  const float nv = norm[o];
-  float a0 = 0.0f, a1 = 0.0f, a2 = 0.0f;
-  constexpr int U = 4;  // frames whose loads are issued together
-  for (int k0 = 0; k0 < frames; k0 += U) {
-    float l0[U], l1[U], l2[U], wv[U];
-#pragma unroll
-    for (int u = 0; u < U; ++u) {
-      if (k0 + u < frames) {
-        const float* lk = lap[k0 + u];
-        l0[u] = __ldg(lk + o);
-        l1[u] = __ldg(lk + plane + o);
-        l2[u] = __ldg(lk + 2 * plane + o);
-        wv[u] = wgt[k0 + u][o];
-      }
-    }
-#pragma unroll
-    for (int u = 0; u < U; ++u) {
-      if (k0 + u < frames) {
-        const float m = nv > 1e-12f ? __fdiv_rn(wv[u], nv) : inv_count;
-        wgt[k0 + u][o] = m;
-        a0 = __fadd_rn(a0, __fmul_rn(l0[u], m));
-        a1 = __fadd_rn(a1, __fmul_rn(l1[u], m));
-        a2 = __fadd_rn(a2, __fmul_rn(l2[u], m));
-      }
-    }
-  }
-  acc[o] = a0;
-  acc[plane + o] = a1;
-  acc[2 * plane + o] = a2;
 }
 
 // Blend of one level over all frames in order, one pixel per thread (the
@@ -1149,10 +1105,14 @@ __device__ __forceinline__ void ld2(const T* p, float* v) {
   }
 }
 
-// Horizontal sums of level-l row r for output columns j0, j0 + 1.
-template <typename T>
+// Horizontal sums of level-l row r for output columns j0, j0 + 1.  N0: the
+// level-0 row of a LAPS stack, `in` holding a frame's raw weights, each tap
+// normalised on the fly (w / N where N > 1e-12, else inv_count; the division
+// blend0 of the reference's normalizeWeightsInto, src/fuse/pyramid.zig:303-316).
+template <typename T, bool N0 = false>
 __device__ __forceinline__ void reduce_row(const T* in, const uint8_t* sm, int64_t pitch, int wl, int hl, int r,
-                                           int j0, float* v, float* ws) {
+                                           int j0, float* v, float* ws, const float* norm = nullptr,
+                                           float inv_count = 0.0f) {
   float m[7];
   uint32_t s4 = 0u, s2 = 0u, s6 = 0u;  // support bytes of taps 2..5, 0..1 and 6
 #pragma unroll
@@ -1171,6 +1131,19 @@ __device__ __forceinline__ void reduce_row(const T* in, const uint8_t* sm, int64
     if (c + 4 < wl) {
       m[6] = ldv<T>(row, c + 4);
       s6 = srow[c + 4];
+    }
+    if constexpr (N0) {
+      // taps past the level or without support are masked out below, whatever
+      // their quotient
+      const float* nrow = norm + (int64_t)r * pitch;
+      float nv[7];
+#pragma unroll
+      for (int u = 0; u < 7; ++u) nv[u] = 1.0f;
+      ld4<float>(nrow + c, nv + 2);
+      if (c > 0) ld2<float>(nrow + c - 2, nv);
+      if (c + 4 < wl) nv[6] = nrow[c + 4];
+#pragma unroll
+      for (int u = 0; u < 7; ++u) m[u] = nv[u] > 1e-12f ? __fdiv_rn(m[u], nv[u]) : inv_count;
     }
   }
   if (c + 3 >= wl) s4 &= (1u << (8 * (wl - c))) - 1u;  // columns past the level: no support (wl - c in 1..3)
@@ -1199,7 +1172,7 @@ __device__ __forceinline__ void reduce_row(const T* in, const uint8_t* sm, int64
   }
 }
 
-template <typename TI, typename TO>
+template <typename TI, typename TO, bool N0 = false>
 __global__ void __launch_bounds__(32 * kReduceWarps) mask_reduce_kernel(const __grid_constant__ MaskReduceArgs a) {
   const int j0 = 2 * (int)(blockIdx.x * 32 + threadIdx.x);
   const int i0 = (int)(blockIdx.y * kReduceWarps + threadIdx.y) * kReduceRows;
@@ -1210,10 +1183,11 @@ __global__ void __launch_bounds__(32 * kReduceWarps) mask_reduce_kernel(const __
   // window of horizontal sums: rows 2i - 2 .. 2i + 2 for output row i
   float hv[5][2], hw[5][2];
 #pragma unroll
-  for (int u = 0; u < 3; ++u) reduce_row<TI>(in, a.sm, a.pitch_l, a.wl, a.hl, 2 * i0 - 2 + u, j0, hv[u], hw[u]);
+  for (int u = 0; u < 3; ++u)
+    reduce_row<TI, N0>(in, a.sm, a.pitch_l, a.wl, a.hl, 2 * i0 - 2 + u, j0, hv[u], hw[u], a.norm, a.inv_count);
   for (int i = i0; i < i1; ++i) {
-    reduce_row<TI>(in, a.sm, a.pitch_l, a.wl, a.hl, 2 * i + 1, j0, hv[3], hw[3]);
-    reduce_row<TI>(in, a.sm, a.pitch_l, a.wl, a.hl, 2 * i + 2, j0, hv[4], hw[4]);
+    reduce_row<TI, N0>(in, a.sm, a.pitch_l, a.wl, a.hl, 2 * i + 1, j0, hv[3], hw[3], a.norm, a.inv_count);
+    reduce_row<TI, N0>(in, a.sm, a.pitch_l, a.wl, a.hl, 2 * i + 2, j0, hv[4], hw[4], a.norm, a.inv_count);
     TO* orow = out + (int64_t)i * a.pitch_n;
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
@@ -1235,13 +1209,13 @@ __global__ void __launch_bounds__(32 * kReduceWarps) mask_reduce_kernel(const __
   }
 }
 
-template <typename TI>
+template <typename TI, bool N0 = false>
 static cudaError_t launch_mask_reduce_in(const MaskReduceArgs& a, dim3 grid, dim3 block, int out_storage,
                                          cudaStream_t s) {
   switch (out_storage) {
-    case FS_STORAGE_F32: mask_reduce_kernel<TI, float><<<grid, block, 0, s>>>(a); break;
-    case FS_STORAGE_F16: mask_reduce_kernel<TI, __half><<<grid, block, 0, s>>>(a); break;
-    case FS_STORAGE_BF16: mask_reduce_kernel<TI, __nv_bfloat16><<<grid, block, 0, s>>>(a); break;
+    case FS_STORAGE_F32: mask_reduce_kernel<TI, float, N0><<<grid, block, 0, s>>>(a); break;
+    case FS_STORAGE_F16: mask_reduce_kernel<TI, __half, N0><<<grid, block, 0, s>>>(a); break;
+    case FS_STORAGE_BF16: mask_reduce_kernel<TI, __nv_bfloat16, N0><<<grid, block, 0, s>>>(a); break;
     default: return cudaErrorInvalidValue;
   }
   return cudaGetLastError();
@@ -1254,6 +1228,10 @@ cudaError_t launch_mask_reduce(const MaskReduceArgs& a, int frames, int in_stora
   const dim3 grid((unsigned)((a.wn + 63) / 64), (unsigned)((a.hn + kReduceWarps * kReduceRows - 1) /
                                                               (kReduceWarps * kReduceRows)),
                   (unsigned)frames);
+  if (a.norm) {  // level 0 of a LAPS stack: raw weights, normalised on the fly
+    if (in_storage != FS_STORAGE_F32) return cudaErrorInvalidValue;
+    return launch_mask_reduce_in<float, true>(a, grid, block, out_storage, s);
+  }
   switch (in_storage) {
     case FS_STORAGE_F32: return launch_mask_reduce_in<float>(a, grid, block, out_storage, s);
     case FS_STORAGE_F16: return launch_mask_reduce_in<__half>(a, grid, block, out_storage, s);
@@ -1333,27 +1311,6 @@ __device__ __forceinline__ void img_row(const LevelArgs& a, int k, int y, int c,
   }
 }
 
-// The words of level-0 row y under the lane's taps (columns c - 2 .. c + 4);
-// only loads, so that the next rows can be fetched while this one is summed.
-__device__ __forceinline__ void load_row_u8(const LevelArgs& a, int k, int y, int c, bool live, uint32_t (&w)[7]) {
-#pragma unroll
-  for (int u = 0; u < 7; ++u) w[u] = 0u;
-  if (live && y >= 0 && y < a.hl) {
-    const uint32_t* row = a.in0[k].rgba + (int64_t)y * a.pitch_l;
-    const uint4 q4 = *reinterpret_cast<const uint4*>(row + c);  // inside the row's pitch
-    w[2] = q4.x;
-    w[3] = q4.y;
-    w[4] = q4.z;
-    w[5] = q4.w;
-    if (c > 0) {
-      const uint2 q2 = *reinterpret_cast<const uint2*>(row + c - 2);
-      w[0] = q2.x;
-      w[1] = q2.y;
-    }
-    if (c + 4 < a.wl) w[6] = row[c + 4];
-  }
-}
-
 // Level 0 in integers: the samples are bytes and the weights 1, 4, 6 (or 0
 // without support), so every partial sum of the FP32 REDUCE is an integer
 // below 2^16 and exact; the integer sums equal it bit for bit.  Horizontal
@@ -1382,38 +1339,16 @@ __device__ __forceinline__ void sum_row_u8(const uint32_t (&wr)[7], int c, int w
   }
 }
 
-__device__ __forceinline__ void img_row_u8(const LevelArgs& a, int k, int y, int c, bool live, int4 (&hs)[2]) {
-  uint32_t w[7];
-  load_row_u8(a, k, y, c, live, w);
-  sum_row_u8(w, c, a.wl, hs);
-}
-
-// One vertical REDUCE tap: v = fma(w, row, v) on value and weight sums
-// (integer sums at level 0).
+// One vertical REDUCE tap: v = fma(w, row, v) on value and weight sums.
 __device__ __forceinline__ float4 vtap(int w, float4 t, float4 v) {
   const float f = (float)w;
   return make_float4(fmaf(f, t.x, v.x), fmaf(f, t.y, v.y), fmaf(f, t.z, v.z), fmaf(f, t.w, v.w));
 }
-__device__ __forceinline__ int4 vtap(int w, int4 t, int4 v) {
-  return make_int4(v.x + w * t.x, v.y + w * t.y, v.z + w * t.z, v.w + w * t.w);
-}
-template <class A> __device__ __forceinline__ A acc_zero();
-template <> __device__ __forceinline__ float4 acc_zero<float4>() { return make_float4(0.f, 0.f, 0.f, 0.f); }
-template <> __device__ __forceinline__ int4 acc_zero<int4>() { return make_int4(0, 0, 0, 0); }
 // exact float of a non-negative integer below 2^23
 __device__ __forceinline__ float small_int_float(int v) { return __int_as_float(0x4B000000 | v) - 8388608.0f; }
-__device__ __forceinline__ float4 acc_float(float4 v) { return v; }
-__device__ __forceinline__ float4 acc_float(int4 v) {
-  return make_float4(small_int_float(v.x), small_int_float(v.y), small_int_float(v.z), small_int_float(v.w));
-}
-template <typename T, bool L0, class A>
-__device__ __forceinline__ void row_sums(const LevelArgs& a, int k, int y, int c, bool live, A (&hs)[2]) {
-  if constexpr (L0) img_row_u8(a, k, y, c, live, hs);
-  else img_row<T>(a, k, y, c, live, hs);
-}
 __device__ __forceinline__ int kwi(int i) { return (i == 0 || i == 4) ? 1 : ((i == 1 || i == 3) ? 4 : 6); }
 
-template <typename T, bool L0>
+template <typename T>
 __global__ void __launch_bounds__(32 * kImgWarps) img_stream_kernel(const __grid_constant__ LevelArgs a, int rows) {
   const int lane = (int)threadIdx.x, k = (int)blockIdx.z;
   const int first = ((int)blockIdx.x * kImgWarps + (int)threadIdx.y) * kImgPairs;  // pair of lane 1
@@ -1425,78 +1360,38 @@ __global__ void __launch_bounds__(32 * kImgWarps) img_stream_kernel(const __grid
   const bool j1in = J0 + 1 < a.wn, rin = J0 + 2 < a.wn;
   const int i0 = (int)blockIdx.y * rows;
   const int i1 = min(i0 + rows, a.hn);
-  using Acc = typename std::conditional<L0, int4, float4>::type;
-  const Acc zero = acc_zero<Acc>();
+  const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
   // vertical REDUCE sums in tap order (level-l rows 2r - 2 .. 2r + 2 for
   // level-(l+1) row r): cur = row r with taps 0 .. 2, nxt = row r + 1 with
   // tap 0; the level-l rows 2r + 1, 2r + 2 complete cur, advance nxt and
   // start row r + 2
-  Acc cur[2], nxt[2];
+  float4 cur[2], nxt[2];
   float Hm2[3][4], Hm1[3][4], Hc[3][4];
 #pragma unroll
   for (int ch = 0; ch < 3; ++ch)
 #pragma unroll
     for (int u = 0; u < 4; ++u) Hm2[ch][u] = Hm1[ch][u] = 0.0f;
   int r = i0 > 0 ? i0 - 1 : 0;
-  // level 0: the lane's four words of level-l rows 2r - 2, 2r - 1, 2r at the
-  // top of step r (the Laplacian rows emitted at step r are the first two)
-  uint4 ringR = make_uint4(0u, 0u, 0u, 0u), ringQ = ringR, ringP = ringR;
   {
-    Acc t0[2], t1[2], t2[2];
-    if constexpr (L0) {
-      uint32_t w0[7], w1[7], w2[7];
-      load_row_u8(a, k, 2 * r - 2, c, live, w0);
-      load_row_u8(a, k, 2 * r - 1, c, live, w1);
-      load_row_u8(a, k, 2 * r, c, live, w2);
-      sum_row_u8(w0, c, a.wl, t0);
-      sum_row_u8(w1, c, a.wl, t1);
-      sum_row_u8(w2, c, a.wl, t2);
-      ringR = make_uint4(w0[2], w0[3], w0[4], w0[5]);
-      ringQ = make_uint4(w1[2], w1[3], w1[4], w1[5]);
-      ringP = make_uint4(w2[2], w2[3], w2[4], w2[5]);
-    } else {
-      row_sums<T, L0>(a, k, 2 * r - 2, c, live, t0);
-      row_sums<T, L0>(a, k, 2 * r - 1, c, live, t1);
-      row_sums<T, L0>(a, k, 2 * r, c, live, t2);
-    }
+    float4 t0[2], t1[2], t2[2];
+    img_row<T>(a, k, 2 * r - 2, c, live, t0);
+    img_row<T>(a, k, 2 * r - 1, c, live, t1);
+    img_row<T>(a, k, 2 * r, c, live, t2);
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
       cur[h] = vtap(kwi(2), t2[h], vtap(kwi(1), t1[h], vtap(kwi(0), t0[h], zero)));
       nxt[h] = vtap(kwi(0), t2[h], zero);
     }
   }
-  uint32_t n3[7], n4[7];  // level 0: the words of the next two rows, fetched one step ahead
-  if constexpr (L0) {
-    load_row_u8(a, k, 2 * r + 1, c, live, n3);
-    load_row_u8(a, k, 2 * r + 2, c, live, n4);
-  }
   for (; r <= i1; ++r) {
     float4 fin[2];
-    uint4 c3 = make_uint4(0u, 0u, 0u, 0u), c4 = c3;  // level 0: words of rows 2r + 1, 2r + 2
     {
-      Acc t3[2], t4[2];
-      if constexpr (L0) {
-        uint32_t w3[7], w4[7];
-#pragma unroll
-        for (int u = 0; u < 7; ++u) {
-          w3[u] = n3[u];
-          w4[u] = n4[u];
-        }
-        if (r < i1) {
-          load_row_u8(a, k, 2 * r + 3, c, live, n3);
-          load_row_u8(a, k, 2 * r + 4, c, live, n4);
-        }
-        sum_row_u8(w3, c, a.wl, t3);
-        sum_row_u8(w4, c, a.wl, t4);
-        c3 = make_uint4(w3[2], w3[3], w3[4], w3[5]);
-        c4 = make_uint4(w4[2], w4[3], w4[4], w4[5]);
-      } else {
-        row_sums<T, L0>(a, k, 2 * r + 1, c, live, t3);
-        row_sums<T, L0>(a, k, 2 * r + 2, c, live, t4);
-      }
+      float4 t3[2], t4[2];
+      img_row<T>(a, k, 2 * r + 1, c, live, t3);
+      img_row<T>(a, k, 2 * r + 2, c, live, t4);
 #pragma unroll
       for (int h = 0; h < 2; ++h) {
-        fin[h] = acc_float(vtap(kwi(4), t4[h], vtap(kwi(3), t3[h], cur[h])));
+        fin[h] = vtap(kwi(4), t4[h], vtap(kwi(3), t3[h], cur[h]));
         cur[h] = vtap(kwi(2), t4[h], vtap(kwi(1), t3[h], nxt[h]));
         nxt[h] = vtap(kwi(0), t4[h], zero);
       }
@@ -1558,18 +1453,9 @@ __global__ void __launch_bounds__(32 * kImgWarps) img_stream_kernel(const __grid
         if (y >= a.hl) break;
         const int64_t ro = (int64_t)y * a.pitch_l;
         float gv[3][4];
-        if constexpr (L0) {
-          const uint4 q4 = yy == 0 ? ringR : ringQ;  // rows 2r - 2, 2r - 1
-          const uint32_t w[4] = {q4.x, q4.y, q4.z, q4.w};
+        const LevelPlanes& in = a.in[k];
 #pragma unroll
-          for (int ch = 0; ch < 3; ++ch)
-#pragma unroll
-            for (int u = 0; u < 4; ++u) gv[ch][u] = chf(w[u], ch);
-        } else {
-          const LevelPlanes& in = a.in[k];
-#pragma unroll
-          for (int ch = 0; ch < 3; ++ch) ld4<T>((const T*)in.g + ch * in.plane + ro + c, gv[ch]);
-        }
+        for (int ch = 0; ch < 3; ++ch) ld4<T>((const T*)in.g + ch * in.plane + ro + c, gv[ch]);
         float* lp = a.lap[k] + ro + c;
 #pragma unroll
         for (int ch = 0; ch < 3; ++ch) {
@@ -1599,17 +1485,12 @@ __global__ void __launch_bounds__(32 * kImgWarps) img_stream_kernel(const __grid
         Hm2[ch][u] = Hm1[ch][u];
         Hm1[ch][u] = Hc[ch][u];
       }
-    if constexpr (L0) {
-      ringR = ringP;
-      ringQ = c3;
-      ringP = c4;
-    }
   }
 }
 
 // Rows per strip: 32, halved (down to 8) while the grid would give fewer
 // than 8 CTAs per SM.
-template <typename T, bool L0>
+template <typename T>
 static cudaError_t launch_img_stream(const LevelArgs& a, cudaStream_t s) {
   const int pairs = (a.wn + 1) / 2;
   const int warps = (pairs + kImgPairs - 1) / kImgPairs;
@@ -1617,64 +1498,32 @@ static cudaError_t launch_img_stream(const LevelArgs& a, cudaStream_t s) {
   int rows = 32;
   while (rows > 8 && (int64_t)bx * ((a.hn + rows - 1) / rows) * a.K < 8 * 148) rows /= 2;
   const dim3 grid((unsigned)bx, (unsigned)((a.hn + rows - 1) / rows), (unsigned)a.K);
-  img_stream_kernel<T, L0><<<grid, dim3(32, kImgWarps), 0, s>>>(a, rows);
+  img_stream_kernel<T><<<grid, dim3(32, kImgWarps), 0, s>>>(a, rows);
   return cudaGetLastError();
 }
 
-cudaError_t launch_blend0(float* acc, int64_t plane, int64_t pitch, int w, int h, const float* norm,
-                          const float* const* lap, float* const* wgt, int frames, float inv_count,
-                          cudaStream_t s) {
-  const int64_t n = (int64_t)w * h;
-  blend0_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(acc, plane, pitch, w, h, norm, lap, wgt, frames,
-                                                           inv_count);
-  return cudaGetLastError();
-}
-
-template <template <typename, bool> class KER, bool L0>
-static cudaError_t launch_split(const LevelArgs& a, int storage, cudaStream_t s, DeviceOnce* cfg) {
+template <typename T>
+static cudaError_t launch_img_tile(const LevelArgs& a, cudaStream_t s, DeviceOnce* cfg) {
   dim3 grid((a.wl + TW - 1) / TW, (a.hl + TH - 1) / TH, a.K);
   const size_t sm = sizeof(ImgSmem);
-  cudaError_t e;
-  switch (storage) {
-    case FS_STORAGE_F32:
-      if ((e = configure(KER<float, L0>::kernel, sm, &cfg[0])) != cudaSuccess) return e;
-      KER<float, L0>::kernel<<<grid, NT, sm, s>>>(a);
-      break;
-    case FS_STORAGE_F16:
-      if ((e = configure(KER<__half, L0>::kernel, sm, &cfg[1])) != cudaSuccess) return e;
-      KER<__half, L0>::kernel<<<grid, NT, sm, s>>>(a);
-      break;
-    case FS_STORAGE_BF16:
-      if ((e = configure(KER<__nv_bfloat16, L0>::kernel, sm, &cfg[2])) != cudaSuccess) return e;
-      KER<__nv_bfloat16, L0>::kernel<<<grid, NT, sm, s>>>(a);
-      break;
-    default:
-      return cudaErrorInvalidValue;
-  }
+  cudaError_t e = configure(img_kernel<T>, sm, cfg);
+  if (e != cudaSuccess) return e;
+  img_kernel<T><<<grid, NT, sm, s>>>(a);
   return cudaGetLastError();
 }
-template <typename T, bool L0> struct ImgK {
-  static constexpr auto kernel = img_kernel<T, L0>;
-};
 
 cudaError_t launch_img_level(const LevelArgs& a, int storage, cudaStream_t s) {
-  static DeviceOnce cfg0[3], cfg1[3];
+  static DeviceOnce cfg[3];
+  if (a.level < 1) return cudaErrorInvalidValue;  // level 0 is part of the fused pass-1 kernel
   // clamped-EXPAND levels (never followed by the top level): streaming kernel
-  if (!a.exact_expand && a.level + 2 < a.levels) {
-    switch (storage) {
-      case FS_STORAGE_F32:
-        return a.level == 0 ? launch_img_stream<float, true>(a, s) : launch_img_stream<float, false>(a, s);
-      case FS_STORAGE_F16:
-        return a.level == 0 ? launch_img_stream<__half, true>(a, s) : launch_img_stream<__half, false>(a, s);
-      case FS_STORAGE_BF16:
-        return a.level == 0 ? launch_img_stream<__nv_bfloat16, true>(a, s)
-                            : launch_img_stream<__nv_bfloat16, false>(a, s);
-      default:
-        return cudaErrorInvalidValue;
-    }
+  const bool stream = !a.exact_expand && a.level + 2 < a.levels;
+  switch (storage) {
+    case FS_STORAGE_F32: return stream ? launch_img_stream<float>(a, s) : launch_img_tile<float>(a, s, &cfg[0]);
+    case FS_STORAGE_F16: return stream ? launch_img_stream<__half>(a, s) : launch_img_tile<__half>(a, s, &cfg[1]);
+    case FS_STORAGE_BF16:
+      return stream ? launch_img_stream<__nv_bfloat16>(a, s) : launch_img_tile<__nv_bfloat16>(a, s, &cfg[2]);
+    default: return cudaErrorInvalidValue;
   }
-  return a.level == 0 ? launch_split<ImgK, true>(a, storage, s, cfg0)
-                      : launch_split<ImgK, false>(a, storage, s, cfg1);
 }
 
 __global__ void sum_contrib_kernel(float* acc, int64_t plane, int64_t pitch, int w, int h, const float* contrib,
@@ -1697,10 +1546,6 @@ cudaError_t launch_sum_contrib(float* acc, int64_t plane, int64_t pitch, int w, 
   return cudaGetLastError();
 }
 
-template <typename K>
-static cudaError_t configure(K kernel, size_t bytes, DeviceOnce* done) {
-  return done->run([&] { return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes); });
-}
 
 template <template <typename> class KER>
 static cudaError_t launch_levels(const LevelArgs& a, int storage, cudaStream_t s, DeviceOnce* cfg) {
@@ -1742,6 +1587,364 @@ cudaError_t launch_level0(const LevelArgs& a, int storage, cudaStream_t s) {
 cudaError_t launch_level(const LevelArgs& a, int storage, cudaStream_t s) {
   static DeviceOnce cfg[3];
   return launch_levels<LevelK>(a, storage, s, cfg);
+}
+
+// ============================================== fused pass 1 (LAPS mode)
+// One kernel for the level-0 part of a frame's pyramid, as the frames
+// arrive: remap the 64x32 tile plus halo into shared memory, local-contrast
+// weight w (added to the weight sum and union as in remap_weights_kernel),
+// support-aware REDUCE of the remapped tile to the level-1 Gaussian (exact
+// integer sums, as the streaming kernel forms them), EXPAND back, and the
+// Laplacian G0 - EXPAND(G1) of the tile weighted by w into the per-pixel sum
+// A_w = sum over frames of lap0 * w.  The level-0 blend of the reference,
+// acc0 = sum_k lap0_k * (w_k / N) (src/fuse/pyramid.zig:303-316, 1556-1603),
+// equals A_w / N: N is the same for every frame at a pixel, so the division
+// moves out of the sum (finalize0_kernel applies it once the weight sum is
+// complete; the FP32 rounding of the two orders differs by a few ulp of the
+// accumulator).  Where N stays <= 1e-12 the reference uses the mask 1/F for
+// every frame instead; those pixels (in practice the window border of the
+// ROI) also keep A_u = sum of lap0 in global memory, touched only while the
+// weight sum so far is <= 1e-12 (it never decreases: the weights are
+// non-negative).  Per frame the kernel keeps only w (for the mask pyramid of
+// pass 2) and the level-1 Gaussian with its support (for the image pyramid
+// of the levels above): no level-0 Laplacian, remapped frame or normalised
+// mask goes through HBM.
+namespace {
+
+template <int B>
+struct Lap0Layout {
+  static constexpr int R0 = B > 4 ? B : 4;  // region halo left / top (REDUCE of the level-1 halo needs 4)
+  static constexpr int R1 = B > 3 ? B : 3;  // right / bottom
+  static constexpr int RW = TW + R0 + R1, RH = TH + R0 + R1;
+  static constexpr int KS = RW + 1;         // contrast-word row stride (odd: distinct banks per row)
+  static constexpr int CH = TH + 2 * B;     // rows of the window sums
+  static constexpr int HS = TW + 1;
+  static constexpr int NWIN = (2 * B + 1) * (2 * B + 1);
+  static constexpr int RR = R0 - 4;         // region row / column of REDUCE tap 0 of halo output 0
+  static constexpr int RRows = 2 * NH + 3;  // region rows the REDUCE reads
+  static constexpr int TS = NW + 1;         // row stride of the horizontal REDUCE sums
+};
+
+template <int B>
+struct __align__(16) Lap0Smem {
+  using Lay = Lap0Layout<B>;
+  ExactQueue queue;
+  uint32_t reg[Lay::RH * Lay::RW];   // remapped RGBA words of the region
+  uint32_t kv[Lay::RH * Lay::KS];    // contrast words of the region
+  union {
+    struct {
+      uint32_t h1[Lay::CH * Lay::HS];  // horizontal window sums: count | gray sum
+      uint32_t h2[Lay::CH * Lay::HS];  // sum of gray^2
+    } win;
+    float hrow[NH * 3 * TW];           // horizontal EXPAND rows (after the window sums are used)
+  } u;
+  uint2 th[Lay::RRows * Lay::TS];    // horizontal REDUCE sums: R | G << 16, B | weight << 16
+  float ng[3][NH * NW];              // level-1 Gaussian on the tile + 1-sample halo (0 outside the level)
+  float inv_den[Lay::NWIN + 1];
+};
+
+template <typename T>
+__device__ __forceinline__ void store_sample(void* plane, int64_t i, float v) { stv<T>((T*)plane, i, v); }
+
+__device__ __forceinline__ void store_level_sample(void* plane, int storage, int64_t i, float v) {
+  if (storage == FS_STORAGE_F16) store_sample<__half>(plane, i, v);
+  else if (storage == FS_STORAGE_BF16) store_sample<__nv_bfloat16>(plane, i, v);
+  else store_sample<float>(plane, i, v);
+}
+
+}  // namespace
+
+template <int B>
+__global__ void __launch_bounds__(NT, 2) lap0_kernel(const __grid_constant__ Lap0Args a) {
+  using Lay = Lap0Layout<B>;
+  constexpr int RW = Lay::RW, RH = Lay::RH, KS = Lay::KS, HS = Lay::HS, R0 = Lay::R0, TS = Lay::TS;
+  extern __shared__ __align__(16) uint8_t smem_raw[];
+  Lap0Smem<B>& S = *reinterpret_cast<Lap0Smem<B>*>(smem_raw);
+  const int x0 = blockIdx.x * TW, y0 = blockIdx.y * TH;
+  const int x1 = x0 >> 1, y1 = y0 >> 1;
+  for (int n = threadIdx.x; n <= Lay::NWIN; n += NT)
+    S.inv_den[n] = n > 1 ? 1.0f / ((float)(n * (n - 1)) * 585225.0f) : 0.0f;
+  // own pixels: column vc, rows vr0 .. vr0 + 7 of the tile (window sums,
+  // weights, EXPAND and the blend all use this ownership)
+  const int vc = threadIdx.x % TW, vr0 = (threadIdx.x / TW) * PPT;
+  const int X = x0 + vc;
+  float nacc[PPT], aw[PPT][3], wv[PPT];
+  uint32_t umask = 0;
+#pragma unroll
+  for (int i = 0; i < PPT; ++i) {
+    const int Y = y0 + vr0 + i;
+    nacc[i] = 0.0f;
+    aw[i][0] = aw[i][1] = aw[i][2] = 0.0f;
+    if (!a.first && X < a.W && Y < a.H) {
+      const int64_t o = (int64_t)Y * a.pitch + X;
+      nacc[i] = a.norm[o];
+      if (a.uni[o]) umask |= 1u << i;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) aw[i][c] = a.aw[c * a.plane + o];
+    }
+  }
+  constexpr int kAnchorThreads = ((RW + 7) / 8) * ((RH + 3) / 4);
+  if (a.K > 0) region_anchors<RW, RH>(a.f[0], x0 - R0, y0 - R0, &S.queue, 0);
+  __syncthreads();
+  const bool exact = a.exact_expand != 0;
+  for (int k = 0; k < a.K; ++k) {
+    // A: the region's remapped words and contrast words
+    fill_region<RW, RH, KS>(a.f[k], a.W, a.H, x0 - R0, y0 - R0, S.reg, S.kv, &S.queue);
+    __syncthreads();
+    // B: horizontal window sums (rows R0 - B .. R0 + TH + B - 1 of the
+    // region, output columns c0 .. c0 + 7) and horizontal REDUCE sums (region
+    // rows RR .. RR + 38, level-1 halo columns jj, jj + 1 from 7 taps)
+    constexpr int kWinItems = Lay::CH * (TW / 8);
+    constexpr int kRedItems = Lay::RRows * (NW / 2);
+    for (int it = threadIdx.x; it < kWinItems + kRedItems; it += NT) {
+      if (it < kWinItems) {
+        const int r = it % Lay::CH, c0 = (it / Lay::CH) * 8;
+        const uint32_t* row = S.kv + (r + R0 - B) * KS + c0 + R0 - B;
+        uint32_t p = 0, q = 0;
+#pragma unroll
+        for (int t = 0; t <= 2 * B; ++t) {
+          const uint32_t v = row[t];
+          const uint32_t g = v & 0xFFFFFu;
+          p += v;
+          q += g * g;
+        }
+        S.u.win.h1[r * HS + c0] = p;
+        S.u.win.h2[r * HS + c0] = q;
+#pragma unroll
+        for (int c = 1; c < 8; ++c) {
+          const uint32_t vin = row[c + 2 * B], vout = row[c - 1];
+          const uint32_t gin = vin & 0xFFFFFu, gout = vout & 0xFFFFFu;
+          p += vin - vout;
+          q += gin * gin - gout * gout;
+          S.u.win.h1[r * HS + c0 + c] = p;
+          S.u.win.h2[r * HS + c0 + c] = q;
+        }
+      } else {
+        const int j = it - kWinItems;
+        const int r = j % Lay::RRows, jj = 2 * (j / Lay::RRows);
+        const uint32_t* row = S.reg + (r + Lay::RR) * RW + 2 * jj + Lay::RR;
+        uint32_t w7[7];
+#pragma unroll
+        for (int u = 0; u < 7; ++u) w7[u] = row[u];
+        int4 hs[2];
+        sum_row_u8(w7, 2, 1 << 30, hs);  // region words outside the ROI are 0 (no support)
+#pragma unroll
+        for (int h = 0; h < 2; ++h)
+          S.th[r * TS + jj + h] = make_uint2((uint32_t)hs[h].x | ((uint32_t)hs[h].y << 16),
+                                             (uint32_t)hs[h].z | ((uint32_t)hs[h].w << 16));
+      }
+    }
+    if (k + 1 < a.K) region_anchors<RW, RH>(a.f[k + 1], x0 - R0, y0 - R0, &S.queue, NT - kAnchorThreads);
+    __syncthreads();
+    // C1: vertical window sums -> this frame's weights of the own pixels
+    {
+      uint32_t p = 0, q = 0;
+#pragma unroll
+      for (int t = 0; t <= 2 * B; ++t) {
+        p += S.u.win.h1[(vr0 + t) * HS + vc];
+        q += S.u.win.h2[(vr0 + t) * HS + vc];
+      }
+      float* wout = a.w[k];
+#pragma unroll
+      for (int i = 0; i < PPT; ++i) {
+        if (i > 0) {
+          p += S.u.win.h1[(vr0 + i + 2 * B) * HS + vc] - S.u.win.h1[(vr0 + i - 1) * HS + vc];
+          q += S.u.win.h2[(vr0 + i + 2 * B) * HS + vc] - S.u.win.h2[(vr0 + i - 1) * HS + vc];
+        }
+        const int Y = y0 + vr0 + i;
+        wv[i] = 0.0f;
+        if (X >= a.W || Y >= a.H) continue;
+        const uint32_t own = S.reg[(vr0 + i + R0) * RW + (vc + R0)];
+        const uint32_t al = px_alpha(own);
+        float w = 0.0f;
+        if (a.window_ok && al > 0 && X >= B && Y >= B && X < a.W - B && Y < a.H - B)
+          w = __fmul_rn(window_stddev<B>(p, q, S.inv_den), alpha_support(al));
+        wv[i] = w;
+        nacc[i] = __fadd_rn(nacc[i], w);
+        if (al > 0) umask |= 1u << i;
+        wout[(int64_t)Y * a.pitch + X] = w;
+      }
+    }
+    // C2: vertical REDUCE -> level-1 Gaussian of the tile and its halo
+    // (rows ii, ii + 1 per item), the tile's own samples stored for the
+    // levels above
+    {
+      const LevelPlanes& g1 = a.g1[k];
+      for (int it = threadIdx.x; it < (NH / 2) * NW; it += NT) {
+        const int ii = 2 * (it / NW), jj = it % NW;
+        uint2 t[7];
+#pragma unroll
+        for (int u = 0; u < 7; ++u) t[u] = S.th[(2 * ii + u) * TS + jj];
+        const int xj = x1 - 1 + jj;
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          uint32_t sx = 0, sy = 0;
+#pragma unroll
+          for (int ky = 0; ky < 5; ++ky) {
+            sx += (uint32_t)kwi(ky) * t[2 * h + ky].x;  // 16-bit lanes stay below 2^16
+            sy += (uint32_t)kwi(ky) * t[2 * h + ky].y;
+          }
+          const int yi = y1 - 1 + ii + h;
+          const float ws = small_int_float((int)(sy >> 16));
+          const bool sup = xj >= 0 && yi >= 0 && xj < a.wn && yi < a.hn && ws > 0.f;
+          const float rc = sup ? __fdividef(1.0f, ws) : 0.0f;
+          const float g[3] = {small_int_float((int)(sx & 0xFFFFu)) * rc, small_int_float((int)(sx >> 16)) * rc,
+                              small_int_float((int)(sy & 0xFFFFu)) * rc};
+          const int o = (ii + h) * NW + jj;
+#pragma unroll
+          for (int c = 0; c < 3; ++c) S.ng[c][o] = g[c];
+          if (ii + h >= 1 && ii + h <= TH1 && jj >= 1 && jj <= TW1 && xj < a.wn && yi < a.hn) {
+            const int64_t go = (int64_t)yi * a.pitch_n + xj;
+#pragma unroll
+            for (int c = 0; c < 3; ++c) store_level_sample(g1.g, a.storage, c * g1.plane + go, g[c]);
+            g1.s[go] = sup ? 1 : 0;
+          }
+        }
+      }
+    }
+    __syncthreads();
+    // D: horizontal EXPAND of the level-1 rows (the operations of
+    // expand_blend_step)
+    float* hrow = S.u.hrow;
+    for (int i = threadIdx.x; i < NH * (TW / 2); i += NT) {
+      const int ii = i / (TW / 2), pp = i % (TW / 2);
+      const int yi = y1 - 1 + ii;
+      if (yi < 0 || yi >= a.hn) continue;
+      const int j = x1 + pp, o = x1 - 1;
+      int ia, ib, ic;
+      if (exact) {
+        ia = pp;
+        ib = pp + 1;
+        ic = pp + 2;
+      } else {
+        ia = clampi(j - 1, 0, a.wn - 1) - o;
+        ib = clampi(j, 0, a.wn - 1) - o;
+        ic = clampi(j + 1, 0, a.wn - 1) - o;
+      }
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const float* g = S.ng[c] + ii * NW;
+        const float A = g[ia], Bv = g[ib], C = g[ic];
+        float ev, od;
+        if (exact) {
+          ev = __fadd_rn(__fadd_rn(A, __fmul_rn(6.0f, Bv)), C);
+          od = __fmul_rn(4.0f, __fadd_rn(Bv, C));
+        } else {
+          ev = __fmul_rn(__fadd_rn(__fadd_rn(A, __fmul_rn(6.0f, Bv)), C), 0.125f);
+          od = __fmul_rn(__fadd_rn(Bv, C), 0.5f);
+        }
+        hrow[(ii * 3 + c) * TW + 2 * pp] = ev;
+        hrow[(ii * 3 + c) * TW + 2 * pp + 1] = od;
+      }
+    }
+    __syncthreads();
+    // E: vertical EXPAND down the own strip, Laplacian, A_w += lap0 * w
+    {
+      const int q0 = (y0 + vr0) >> 1;
+      constexpr int NR = PPT / 2 + 2;
+      float hv[3][NR];
+#pragma unroll
+      for (int r = 0; r < NR; ++r) {
+        int q = q0 - 1 + r;
+        bool zero = false;
+        if (exact) zero = q < 0 || q >= a.hn;
+        else q = clampi(q, 0, a.hn - 1);
+        const int lr = q - (y1 - 1);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) hv[c][r] = zero ? 0.0f : hrow[(lr * 3 + c) * TW + vc];
+      }
+      const bool first_frame = a.first && k == 0;
+#pragma unroll
+      for (int i = 0; i < PPT; ++i) {
+        const int y = y0 + vr0 + i;
+        if (X >= a.W || y >= a.H) continue;
+        const int j = i >> 1;
+        const float div = exact ? exact_expand_divisor(X, y, a.wn, a.hn) : 1.0f;
+        const uint32_t g0 = S.reg[(vr0 + i + R0) * RW + (vc + R0)];
+        const bool fallback = nacc[i] <= 1e-12f;  // the weight sum so far: A_u still needed here
+        const int64_t o = (int64_t)y * a.pitch + X;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          float e;
+          if ((i & 1) == 0) {
+            const float v = __fadd_rn(__fadd_rn(hv[c][j], __fmul_rn(6.0f, hv[c][j + 1])), hv[c][j + 2]);
+            e = exact ? __fdiv_rn(v, div) : __fmul_rn(v, 0.125f);
+          } else if (exact) {
+            e = __fdiv_rn(__fadd_rn(hv[c][j + 1], hv[c][j + 2]), div);
+          } else {
+            e = __fmul_rn(__fadd_rn(hv[c][j + 1], hv[c][j + 1]), 0.5f);
+          }
+          const float lap = __fsub_rn(chf(g0, c), e);
+          aw[i][c] = __fadd_rn(aw[i][c], __fmul_rn(lap, wv[i]));
+          if (fallback) {
+            float* pu = a.au + c * a.plane + o;
+            *pu = first_frame ? lap : __fadd_rn(*pu, lap);
+          }
+        }
+      }
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int i = 0; i < PPT; ++i) {
+    const int Y = y0 + vr0 + i;
+    if (X < a.W && Y < a.H) {
+      const int64_t o = (int64_t)Y * a.pitch + X;
+      a.norm[o] = nacc[i];
+      a.uni[o] = (uint8_t)((umask >> i) & 1u);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) a.aw[c * a.plane + o] = aw[i][c];
+    }
+  }
+}
+
+template <int B>
+static cudaError_t launch_lap0_b(const Lap0Args& a, cudaStream_t s) {
+  static DeviceOnce configured;
+  const size_t sm = sizeof(Lap0Smem<B>);
+  cudaError_t e = configured.run(
+      [&] { return cudaFuncSetAttribute(lap0_kernel<B>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm); });
+  if (e != cudaSuccess) return e;
+  dim3 grid((a.W + TW - 1) / TW, (a.H + TH - 1) / TH);
+  lap0_kernel<B><<<grid, NT, sm, s>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_lap0(const Lap0Args& a, int border, cudaStream_t s) {
+  if (a.K < 1 || a.K > kMaxBatch) return cudaErrorInvalidValue;
+  switch (border) {
+    case 1: return launch_lap0_b<1>(a, s);
+    case 2: return launch_lap0_b<2>(a, s);
+    case 3: return launch_lap0_b<3>(a, s);
+    case 4: return launch_lap0_b<4>(a, s);
+    case 5: return launch_lap0_b<5>(a, s);
+    case 6: return launch_lap0_b<6>(a, s);
+    case 7: return launch_lap0_b<7>(a, s);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+// Level-0 accumulator of a LAPS stack once the weight sum N is complete:
+// acc0 = A_w / N where N > 1e-12, else A_u / F (the reference's mask 1/F for
+// every frame), written over A_w (acc0 and A_w share the buffer).
+__global__ void finalize0_kernel(float* acc, const float* au, const float* norm, int64_t plane, int64_t pitch, int w,
+                                 int h, float inv_count) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (int64_t)w * h) return;
+  const int64_t o = (i / w) * pitch + i % w;
+  const float nv = norm[o];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    const int64_t q = c * plane + o;
+    acc[q] = nv > 1e-12f ? __fdiv_rn(acc[q], nv) : __fmul_rn(au[q], inv_count);
+  }
+}
+
+cudaError_t launch_finalize0(float* acc, const float* au, const float* norm, int64_t plane, int64_t pitch, int w,
+                             int h, float inv_count, cudaStream_t s) {
+  const int64_t n = (int64_t)w * h;
+  finalize0_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(acc, au, norm, plane, pitch, w, h, inv_count);
+  return cudaGetLastError();
 }
 
 // ================================================================ collapse

@@ -87,6 +87,28 @@ struct LevelArgs {
   float* gtop[kMaxBatch];
 };
 
+// Fused pass 1 of the LAPS mode (lap0_kernel): a batch of frames remapped,
+// weighted, reduced to level 1 and blended at level 0 as A_w += lap0 * w.
+struct Lap0Args {
+  int32_t W, H;            // ROI (level 0) size
+  int32_t window_ok;       // W >= window && H >= window
+  int32_t K;               // frames in this batch
+  int32_t first;           // 1: first batch of the stack (sums start at zero)
+  int32_t exact_expand;    // max(W, H) <= 512: no-wrap EXPAND back to level 0
+  int32_t wn, hn;          // level-1 size
+  int32_t storage;         // level-1 Gaussian storage (fs_level_storage)
+  int32_t pad0;
+  int64_t pitch, pitch_n;  // level-0 / level-1 row pitch (elements)
+  int64_t plane;           // level-0 plane (pitch * H elements)
+  float* norm;             // weight sum N
+  uint8_t* uni;            // union support
+  float* aw;               // A_w = sum of lap0 * w, 3 planes
+  float* au;               // A_u = sum of lap0 while N <= 1e-12, 3 planes
+  FrameIn f[kMaxBatch];
+  float* w[kMaxBatch];         // per frame: its level-0 weight plane
+  LevelPlanes g1[kMaxBatch];   // per frame: level-1 Gaussian (storage) and support
+};
+
 struct CollapseArgs {
   int32_t wp, hp, wc, hc;     // parent / child sizes
   int64_t pitch_p, pitch_c;
@@ -106,11 +128,16 @@ struct CollapseArgs {
 // level-l union support (src/fuse/pyramid.zig:997-1043), the products and
 // sums of the level kernels' mask REDUCE in the same order.
 struct MaskReduceArgs {
-  const void* const* in;  // per frame: level-l mask (level 0: the normalised weight plane)
+  const void* const* in;  // per frame: level-l mask (level 0: the frame's weight plane, see norm)
   void* const* out;       // per frame: level-(l+1) mask
   const uint8_t* sm;      // level-l union support
   int32_t wl, hl, wn, hn;
   int64_t pitch_l, pitch_n;
+  // level 0 of a LAPS stack: `in` holds each frame's raw weight w and the
+  // mask is formed on the fly, w / N where N > 1e-12 else inv_count
+  // (src/fuse/pyramid.zig:303-316); null at levels >= 1
+  const float* norm;
+  float inv_count;
 };
 // Storage of in / out masks: 0 f32, 1 f16, 2 bf16.
 cudaError_t launch_mask_reduce(const MaskReduceArgs& a, int frames, int in_storage, int out_storage, cudaStream_t s);
@@ -133,25 +160,22 @@ struct RemapArgs {
 };
 
 cudaError_t launch_remap_weights(const RemapWeightArgs& a, int border, cudaStream_t s);
+cudaError_t launch_lap0(const Lap0Args& a, int border, cudaStream_t s);
+// acc0 = A_w / N where N > 1e-12, else A_u * inv_count (acc0 written over A_w).
+cudaError_t launch_finalize0(float* acc, const float* au, const float* norm, int64_t plane, int64_t pitch, int w,
+                             int h, float inv_count, cudaStream_t s);
 cudaError_t launch_level0(const LevelArgs& a, int storage, cudaStream_t s);
 cudaError_t launch_level(const LevelArgs& a, int storage, cudaStream_t s);
 cudaError_t launch_collapse(const CollapseArgs& a, cudaStream_t s);
-// Split pyramid: the image half of a level step for the batch's frames, one
-// frame per CTA (grid.z = K): Gaussian REDUCE to level l + 1 (slots out[k],
-// or gtop[k] at the top) and the Laplacian of level l into lap[k]; level 0
-// reads the remapped RGBA planes in0[k].rgba.
+// Split pyramid: the image half of a level step l >= 1 for the batch's
+// frames, one frame per CTA (grid.z = K): Gaussian REDUCE to level l + 1
+// (slots out[k], or gtop[k] at the top) and the Laplacian of level l into
+// lap[k] (level 0 is part of the fused pass-1 kernel, launch_lap0).
 cudaError_t launch_img_level(const LevelArgs& a, int storage, cudaStream_t s);
 // acc = sum over frames k, in order, of lap[k] (3 planes of `plane`) times
 // mask[k] (storage T: 0 f32, 1 f16, 2 bf16), written over acc.
 cudaError_t launch_blend(float* acc, int64_t plane, int64_t pitch, int w, int h, const float* const* lap,
                          const void* const* mask, int frames, int storage, cudaStream_t s);
-// Level-0 blend of all frames of a stack (device tables of each frame's
-// level-0 Laplacian and weight planes), written over acc; each weight plane
-// is replaced by the frame's normalised mask, which launch_mask_reduce then
-// reads.
-cudaError_t launch_blend0(float* acc, int64_t plane, int64_t pitch, int w, int h, const float* norm,
-                          const float* const* lap, float* const* wgt, int frames, float inv_count,
-                          cudaStream_t s);
 // acc[c] += contrib[k][c] for k = 0 .. K-1 in order (w x h level, plane stride `plane`).
 cudaError_t launch_sum_contrib(float* acc, int64_t plane, int64_t pitch, int w, int h, const float* contrib, int K,
                                cudaStream_t s);

@@ -34,8 +34,10 @@ def make_stacks(torch, ctx, specs, seed):
 
 
 def alone(torch, ctx, st, storage, k=0):
+    # the batch runs the cache / resident modes (the same kernels, the same
+    # bytes); the laps mode blends level 0 in another rounding order
     s = fsb.PyramidContrastStack(ctx, st.width, st.height, len(st.frames), roi=st.roi, level_storage=storage,
-                                 frames_per_batch=k)
+                                 frames_per_batch=k, pass2_mode="cache")
     for f, p in zip(st.frames, st.poses):
         s.add_frame_device(f, st.width * 3, p)
     out = s.finish()

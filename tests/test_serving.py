@@ -42,11 +42,13 @@ def test_mixed_stream_same_alone_and_in_the_mix(torch):
     assert s["p50_latency_ms"] <= s["p99_latency_ms"]
     for r in rep.results:
         assert r.done_s >= r.admitted_s >= r.arrival_s
-    # alone: the same frames through a fresh context, one stack at a time
+    # alone: the same frames through a fresh context, one stack at a time, in
+    # the cache mode (the server admits stacks in the cache / resident modes,
+    # which give the same bytes)
     alone_ctx = fsb.Context(0)
     for req, res in zip(sorted(reqs, key=lambda r: r.arrival_s), rep.results):
         roi = pool.roi(req)
-        st = fsb.PyramidContrastStack(alone_ctx, req.width, req.height, req.frames, roi=roi)
+        st = fsb.PyramidContrastStack(alone_ctx, req.width, req.height, req.frames, roi=roi, pass2_mode="cache")
         for i in range(req.frames):
             buf, stride, pose = pool.frame(req, i)
             st.add_frame_device(buf, stride, pose)

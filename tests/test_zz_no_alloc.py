@@ -6,8 +6,8 @@ server that reserved its HBM when it started and accounts for every byte, or
 an interactive loop whose own kernels would stall behind the plugin's
 cudaMalloc / cudaFree.  This entry point keeps every plane in a fixed
 file-scope device array instead.  Checked here:
-  * it gives the same bytes as the context-backed fuse-only path
-    (fuse_aligned_images: the same kernels in the same order), on two calls
+  * it gives the same bytes as the context-backed fuse-only path in the
+    cache mode (the same kernels in the same order), on two calls
     in a row and with stacks of different sizes back to back, so planes one
     call leaves in the shared array never leak into the next;
   * it is within one u8 LSB of the oracle's fuse-only fusion;
@@ -99,6 +99,17 @@ class StaticCall:
         return rows[:, :self.w * 3].reshape(self.h, self.w, 3).copy(), rows[:, self.w * 3:].copy()
 
 
+def context_fuse(ctx, frames, window):
+    """The context-backed fuse-only path in the cache mode, which runs the
+    kernels of the static path in the same order."""
+    h, w, c = frames[0].shape
+    with fsb.PyramidContrastStack(ctx, w, h, len(frames), channels=c, contrast_window=window, aligned=True,
+                                  pass2_mode="cache") as st:
+        for im in frames:
+            st.add_frame(im)
+        return st.finish()
+
+
 def static_fuse(torch, frames, window):
     call = StaticCall(torch, frames, window)
     call.run()
@@ -117,7 +128,7 @@ def test_static_fusion_equals_context_path_back_to_back(torch, ctx):
     for seed, w, h, n, c, win in CASES + CASES[:1]:
         frames = aligned_stack(seed, w, h, n, c)
         got = static_fuse(torch, frames, win)
-        want = fsb.fuse_aligned_images(ctx, frames, contrast_window=win)
+        want = context_fuse(ctx, frames, win)
         diff = np.abs(got.astype(np.int16) - want.astype(np.int16))
         assert np.array_equal(got, want), ((w, h, n, c), int(diff.max()), int((diff > 0).sum()))
     # two calls in a row on the same stack give the same bytes
@@ -143,7 +154,7 @@ def test_static_fusion_padded_output_rows(torch, ctx):
     call = StaticCall(torch, frames, win, pad=64)
     call.run()
     img, pad = call.result()
-    assert np.array_equal(img, fsb.fuse_aligned_images(ctx, frames, contrast_window=win))
+    assert np.array_equal(img, context_fuse(ctx, frames, win))
     assert (pad == 7).all(), "bytes past the image columns were written"
 
 
