@@ -25,7 +25,7 @@ EXPORTED = (
     "fs_create", "fs_destroy", "fs_last_error", "fs_status_string", "fs_api_version", "fs_ctx_device_bytes",
     "fs_ctx_synchronize", "fs_ctx_trim", "fs_ctx_reserve", "fs_ctx_set_budget", "fs_ctx_stream", "fs_ctx_launch_count", "fs_ctx_set_kernel_timing", "fs_ctx_kernel_stats",
     "fs_pose_default", "fs_compute_roi", "fs_inverse_map_points", "fs_forward_map_points", "fs_exact_expand_divisor",
-    "fs_remap_frame", "fs_remap_frame_device",
+    "fs_remap_frame", "fs_remap_frame_device", "fs_remap_frame16", "fs_remap_frame16_device",
     "fs_stack_begin", "fs_stack_add_frame", "fs_stack_add_frame_async", "fs_stack_add_frame_device", "fs_stack_finish",
     "fs_stack_finish_device", "fs_stack_finish_async", "fs_stack_wait", "fs_stack_set_base_output", "fs_stack_pass2_mode", "fs_stack_footprint", "fs_stack_mode_bytes", "fs_stack_begin_mode",
     "fs_stack_set_frame_total", "fs_stack_end_pass1", "fs_stack_blend", "fs_stack_collapse", "fs_stack_buffer", "fs_stack_output_size", "fs_stack_destroy", "fs_fuse_stack",
@@ -105,7 +105,7 @@ def _bind(L):
     L.fs_forward_map_points.argtypes = [P(FsPose), u32, u32, sz, P(ctypes.c_double), P(ctypes.c_double)]
     L.fs_exact_expand_divisor.argtypes = [i32, i32, i32, i32]
     L.fs_exact_expand_divisor.restype = ctypes.c_float
-    for f in (L.fs_remap_frame, L.fs_remap_frame_device):
+    for f in (L.fs_remap_frame, L.fs_remap_frame_device, L.fs_remap_frame16, L.fs_remap_frame16_device):
         f.argtypes = [ctx, vp, sz, u32, u32, u32, P(FsPose), P(FsRect), vp, sz]
     L.fs_stack_begin.argtypes = [ctx, P(FsStackDesc), P(vp)]
     L.fs_stack_add_frame.argtypes = [vp, vp, sz, P(FsPose)]

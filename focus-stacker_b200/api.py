@@ -253,17 +253,19 @@ def exact_expand_divisor(x: int, y: int, src_w: int, src_h: int) -> float:
 
 # ---------------------------------------------------------------------- remap
 def remap_rigid_image(ctx: Context, src: np.ndarray, pose, roi: Optional[Rect] = None) -> np.ndarray:
-    """src: HxW (gray) or HxWx3 uint8.  Returns the ROI-sized image with an extra alpha channel."""
+    """src: HxW (gray) or HxWx3, uint8 or uint16 (remapU8 / remapU16).
+    Returns the ROI-sized image with an extra alpha channel, same sample type."""
     src = np.ascontiguousarray(src)
-    if src.dtype != np.uint8:
-        raise FocusCudaError(8, "only 8-bit samples are implemented")
+    if src.dtype not in (np.uint8, np.uint16):
+        raise FocusCudaError(8, "samples must be uint8 or uint16")
     h, w = src.shape[:2]
     ch = 1 if src.ndim == 2 else src.shape[2]
     r = roi or Rect(0, 0, w, h)
-    out = np.zeros((r.height, r.width, ch + 1), np.uint8)
+    out = np.zeros((r.height, r.width, ch + 1), src.dtype)
     p = _pose(pose).to_c()
-    rc = L().fs_remap_frame(ctx.handle, src.ctypes.data, w * ch, w, h, ch, ctypes.byref(p),
-                            ctypes.byref(r.to_c()), out.ctypes.data, r.width * (ch + 1))
+    fn = L().fs_remap_frame16 if src.dtype == np.uint16 else L().fs_remap_frame
+    rc = fn(ctx.handle, src.ctypes.data, src.strides[0], w, h, ch, ctypes.byref(p), ctypes.byref(r.to_c()),
+            out.ctypes.data, out.strides[0])
     _check(rc, ctx.handle)
     return out
 
@@ -300,14 +302,14 @@ class DeviceBuffer:
 
 def stack_desc(src_width: int, src_height: int, frame_count: int, roi: Optional[Rect] = None, channels: int = 3,
                contrast_window: int = 5, aligned: bool = False, frames_per_batch: int = 0,
-               level_storage: int = 0) -> _lib.FsStackDesc:
+               level_storage: int = 0, sample_bits: int = 8) -> _lib.FsStackDesc:
     d = _lib.FsStackDesc()
     d.src_width, d.src_height = src_width, src_height
     d.has_roi = 1 if roi is not None else 0
     if roi is not None:
         d.roi = roi.to_c()
     d.channels = channels
-    d.sample_bits = 8
+    d.sample_bits = sample_bits
     d.frame_count = frame_count
     d.contrast_window = contrast_window
     d.input_is_aligned = 1 if aligned else 0
@@ -343,12 +345,14 @@ class PyramidContrastStack:
 
     def __init__(self, ctx: Context, src_width: int, src_height: int, frame_count: int, roi: Optional[Rect] = None,
                  channels: int = 3, contrast_window: int = 5, aligned: bool = False, frames_per_batch: int = 0,
-                 level_storage: int = 0, pass2_mode: Optional[str] = None):
+                 level_storage: int = 0, pass2_mode: Optional[str] = None, sample_bits: int = 8):
         """pass2_mode: None picks the mode from the context's budget; "cache",
-        "resident", "refetch" or "laps" imposes one."""
+        "resident", "refetch" or "laps" imposes one.  sample_bits 16: uint16
+        frames in and a uint16 image out (FP32 levels; resident / refetch)."""
         self.ctx = ctx
         d = stack_desc(src_width, src_height, frame_count, roi, channels, contrast_window, aligned, frames_per_batch,
-                       level_storage)
+                       level_storage, sample_bits)
+        self.dtype = np.uint16 if sample_bits == 16 else np.uint8
         self.desc = d
         h = ctypes.c_void_p()
         mode = -1 if pass2_mode is None else PASS2_MODES.index(pass2_mode)
@@ -373,8 +377,10 @@ class PyramidContrastStack:
 
     def add_frame(self, pixels: np.ndarray, pose=None):
         pixels = np.ascontiguousarray(pixels)
+        if pixels.dtype != self.dtype:
+            raise FocusCudaError(7, "MismatchedImageFormats")
         p = _pose(pose).to_c() if pose is not None else None
-        rc = L().fs_stack_add_frame(self.handle, pixels.ctypes.data, pixels.shape[1] * pixels.shape[2],
+        rc = L().fs_stack_add_frame(self.handle, pixels.ctypes.data, pixels.strides[0],
                                     ctypes.byref(p) if p is not None else None)
         _check(rc, self.ctx.handle)
 
@@ -383,9 +389,11 @@ class PyramidContrastStack:
         memory) is kept referenced and must not change until finish or wait
         has returned."""
         pixels = np.ascontiguousarray(pixels)
+        if pixels.dtype != self.dtype:
+            raise FocusCudaError(7, "MismatchedImageFormats")
         self._keep.append(pixels)
         p = _pose(pose).to_c() if pose is not None else None
-        rc = L().fs_stack_add_frame_async(self.handle, pixels.ctypes.data, pixels.shape[1] * pixels.shape[2],
+        rc = L().fs_stack_add_frame_async(self.handle, pixels.ctypes.data, pixels.strides[0],
                                           ctypes.byref(p) if p is not None else None)
         _check(rc, self.ctx.handle)
 
@@ -396,7 +404,7 @@ class PyramidContrastStack:
         _check(rc, self.ctx.handle)
 
     def finish(self, refetch=None) -> np.ndarray:
-        out = np.zeros((self.out_height, self.out_width, 3), np.uint8)
+        out = np.zeros((self.out_height, self.out_width, 3), self.dtype)
         self.finish_into(out, refetch)
         return out
 
@@ -435,8 +443,8 @@ class PyramidContrastStack:
         _check(L().fs_stack_blend(self.handle, cb, None), self.ctx.handle)
 
     def collapse(self) -> np.ndarray:
-        out = np.zeros((self.out_height, self.out_width, 3), np.uint8)
-        _check(L().fs_stack_collapse(self.handle, out.ctypes.data_as(ctypes.c_void_p), self.out_width * 3, 0),
+        out = np.zeros((self.out_height, self.out_width, 3), self.dtype)
+        _check(L().fs_stack_collapse(self.handle, out.ctypes.data_as(ctypes.c_void_p), out.strides[0], 0),
                self.ctx.handle)
         return out
 
@@ -466,7 +474,7 @@ class PyramidContrastStack:
                 arr = np.ascontiguousarray(refetch(int(index)))
                 held.append(arr)
                 pixels[0] = arr.ctypes.data
-                stride[0] = arr.shape[1] * arr.shape[2]
+                stride[0] = arr.strides[0]
                 return 0
             except Exception:
                 return 1
@@ -498,8 +506,9 @@ def fuse_remapped_images(ctx: Context, sources: Sequence[np.ndarray], poses: Seq
     """Stack path: remap every active frame through its pose into the ROI and
     fuse with pyramid-contrast (runCollapsedPyramidStackPass)."""
     h, w = sources[0].shape[:2]
+    bits = 16 if sources[0].dtype == np.uint16 else 8
     with PyramidContrastStack(ctx, w, h, len(sources), roi=roi, channels=3, contrast_window=contrast_window,
-                              frames_per_batch=frames_per_batch) as st:
+                              frames_per_batch=frames_per_batch, sample_bits=bits) as st:
         for src, pose in zip(sources, poses):
             if src.shape[:2] != (h, w):
                 raise FocusCudaError(7, "MismatchedImageSizes")
@@ -511,8 +520,9 @@ def fuse_aligned_images(ctx: Context, images: Sequence[np.ndarray], contrast_win
                         frames_per_batch: int = 0) -> np.ndarray:
     """Fuse-only path (focus_fuse_zig): pre-aligned RGB or RGBA frames."""
     h, w, c = images[0].shape
+    bits = 16 if images[0].dtype == np.uint16 else 8
     with PyramidContrastStack(ctx, w, h, len(images), channels=c, contrast_window=contrast_window, aligned=True,
-                              frames_per_batch=frames_per_batch) as st:
+                              frames_per_batch=frames_per_batch, sample_bits=bits) as st:
         for im in images:
             if im.shape != (h, w, c):
                 raise FocusCudaError(7, "MismatchedImageSizes" if im.shape[:2] != (h, w) else "MismatchedImageFormats")

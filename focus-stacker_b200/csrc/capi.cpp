@@ -199,6 +199,8 @@ struct fs_stack {
   std::vector<std::vector<LevelPlanes>> slot;  // [k][l], l = 1 .. L-2
   std::vector<FramePlanes> cache;              // CACHE: per frame
   std::vector<FramePlanes> p2;                 // RESIDENT / REFETCH: per batch slot (K)
+  std::vector<LevelPlanes> slot0;              // 16-bit frames: level-0 planes per batch slot (K)
+  uint32_t bps = 1;                            // bytes per sample (1: u8, 2: u16)
   std::vector<float*> wplane;                  // LAPS: per frame, its weight (level 0)
   std::vector<std::vector<float*>> lap;        // LAPS: per frame, Laplacian of levels 1 .. L-2 ([0] unused)
   float* au = nullptr;                         // LAPS: sum of level-0 Laplacians where the weight sum <= 1e-12
@@ -334,6 +336,39 @@ void level_geometry(const fs_stack* s, uint32_t l, LevelArgs* a) {
   }
 }
 
+// 16-bit frames [begin, end): pass 1 (weight sum and union) or pass 2
+// (level-0 planes into the batch slots).
+int launch_remap16_batch(fs_stack* s, const std::vector<fs_stack::Frame>& frames, size_t begin, size_t end,
+                         bool pass1, float inv_count) {
+  Remap16Args a;
+  std::memset(&a, 0, sizeof(a));
+  a.W = (int32_t)s->W;
+  a.H = (int32_t)s->H;
+  a.window_ok = (s->W >= s->d.contrast_window && s->H >= s->d.contrast_window) ? 1 : 0;
+  a.K = (int32_t)(end - begin);
+  a.accumulate = pass1 ? 1 : 0;
+  a.first = begin == 0 ? 1 : 0;
+  a.inv_count = inv_count;
+  a.norm = s->norm;
+  a.uni = s->uni;
+  a.pitch = s->pitch[0];
+  for (size_t k = begin; k < end; ++k) {
+    std::string why;
+    if (!build_frame_in(s, frames[k], &a.f[k - begin], &why)) return set_err(s->ctx, FS_ERR_INVALID, why);
+    if (!pass1) a.out[k - begin] = s->slot0[k - begin];
+  }
+  cudaError_t e = timed(s->ctx, pass1 ? "pass1" : "remap_weights",
+                        [&] { return launch_remap16_weights(a, (int)s->border, s->ctx->stream); });
+  if (e != cudaSuccess) return cuda_err(s->ctx, e, "16-bit remap/weights launch");
+  if (!pass1 && s->L == 1) {
+    e = timed(s->ctx, "level0", [&] {
+      return launch_blend_single_level(s->acc[0], s->pitch[0] * s->lh[0], a, s->ctx->stream);
+    });
+    if (e != cudaSuccess) return cuda_err(s->ctx, e, "single-level blend");
+  }
+  return FS_OK;
+}
+
 // LAPS pass 1, level 0 of frames [begin, end): remap, weights (weight sum
 // and union), level-1 Gaussian into the batch slots, A_w += lap0 * w.
 int launch_lap0_batch(fs_stack* s, size_t begin, size_t end) {
@@ -399,6 +434,7 @@ int run_pending_pass1(fs_stack* s, bool flush) {
     if (!(pending >= s->K || (pending > 0 && (flush || to_come <= kTailFrames)))) break;
     size_t begin = s->pass1_done, end = std::min(s->frames.size(), begin + s->K);
     int rc = s->mode == P2_LAPS ? launch_lap0_batch(s, begin, end)
+             : s->bps == 2      ? launch_remap16_batch(s, s->frames, begin, end, true, 0.0f)
                                 : launch_remap_weights_batch(s, s->frames, begin, end, true);
     if (rc != FS_OK) return rc;
     // the staging buffers of these frames are free for reuse after this remap
@@ -607,14 +643,15 @@ float fs_exact_expand_divisor(int x, int y, int src_w, int src_h) { return exact
 // ------------------------------------------------------------------- remap
 static int remap_impl(fs_ctx* ctx, const void* src, size_t src_stride, uint32_t width, uint32_t height,
                       uint32_t channels, const fs_pose* pose, const fs_rect* roi, void* dst, size_t dst_stride,
-                      bool device) {
+                      bool device, int bytes_per_sample = 1) {
   if (!ctx || !src || !dst || !pose) return set_err(ctx, FS_ERR_INVALID, "null argument");
   if (channels != 1 && channels != 3) return set_err(ctx, FS_ERR_UNSUPPORTED, "remap supports 1 or 3 channels");
   if (width == 0 || height == 0) return set_err(ctx, FS_ERR_INVALID, "empty frame");
   fs_rect r = roi ? *roi : fs_rect{0, 0, (int32_t)width, (int32_t)height};
   if (r.right <= r.left || r.bottom <= r.top) return set_err(ctx, FS_ERR_INVALID, "empty roi");
   uint32_t ow = (uint32_t)(r.right - r.left), oh = (uint32_t)(r.bottom - r.top);
-  if (src_stride < (size_t)width * channels || dst_stride < (size_t)ow * (channels + 1))
+  if (src_stride < (size_t)width * channels * bytes_per_sample ||
+      dst_stride < (size_t)ow * (channels + 1) * bytes_per_sample)
     return set_err(ctx, FS_ERR_INVALID, "row stride too small");
   cudaSetDevice(ctx->device);
   RemapArgs a;
@@ -646,7 +683,9 @@ static int remap_impl(fs_ctx* ctx, const void* src, size_t src_stride, uint32_t 
   a.f.src.pitch = (int64_t)src_stride;
   a.dst = (uint8_t*)ddst;
   a.dst_pitch = (int64_t)dst_stride;
-  cudaError_t e = timed(ctx, "remap", [&] { return launch_remap(a, ctx->stream); });
+  cudaError_t e = timed(ctx, "remap", [&] {
+    return bytes_per_sample == 2 ? launch_remap16(a, ctx->stream) : launch_remap(a, ctx->stream);
+  });
   if (e == cudaSuccess && !device) e = cudaMemcpyAsync(dst, ddst, dbytes, cudaMemcpyDeviceToHost, ctx->stream);
   cudaError_t e2 = cudaStreamSynchronize(ctx->stream);
   if (!device) {
@@ -663,6 +702,17 @@ int fs_remap_frame(fs_ctx* ctx, const void* src, size_t src_stride, uint32_t wid
   return remap_impl(ctx, src, src_stride, width, height, channels, pose, roi, dst, dst_stride, false);
 }
 
+int fs_remap_frame16(fs_ctx* ctx, const void* src, size_t src_stride, uint32_t width, uint32_t height,
+                     uint32_t channels, const fs_pose* pose, const fs_rect* roi, void* dst, size_t dst_stride) {
+  return remap_impl(ctx, src, src_stride, width, height, channels, pose, roi, dst, dst_stride, false, 2);
+}
+
+int fs_remap_frame16_device(fs_ctx* ctx, const void* src, size_t src_stride, uint32_t width, uint32_t height,
+                            uint32_t channels, const fs_pose* pose, const fs_rect* roi, void* dst,
+                            size_t dst_stride) {
+  return remap_impl(ctx, src, src_stride, width, height, channels, pose, roi, dst, dst_stride, true, 2);
+}
+
 int fs_remap_frame_device(fs_ctx* ctx, const void* src, size_t src_stride, uint32_t width, uint32_t height,
                           uint32_t channels, const fs_pose* pose, const fs_rect* roi, void* dst, size_t dst_stride) {
   return remap_impl(ctx, src, src_stride, width, height, channels, pose, roi, dst, dst_stride, true);
@@ -674,9 +724,10 @@ namespace {
 // Validation of a stack description (null when valid; the status in *code).
 const char* check_desc(const fs_stack_desc& d, int* code) {
   *code = FS_ERR_INVALID;
-  if (d.sample_bits != 8) {
+  if (d.sample_bits != 8 && d.sample_bits != 16) return "sample_bits must be 8 or 16";
+  if (d.sample_bits == 16 && d.level_storage != FS_STORAGE_F32) {
     *code = FS_ERR_UNSUPPORTED;
-    return "only 8-bit samples are implemented";
+    return "16-bit samples need FP32 level storage (FP16 tops out at 65504, BF16 keeps 8 bits)";
   }
   if (d.src_width == 0 || d.src_height == 0 || d.frame_count == 0) return "empty stack";
   if (d.contrast_window < 3 || (d.contrast_window & 1) == 0) return "contrast window must be odd and >= 3";
@@ -735,14 +786,17 @@ StackPlan plan_stack(const fs_stack_desc& d) {
     h = next_level_size(h);
   }
   const size_t esz = d.level_storage == FS_STORAGE_F32 ? 4 : 2;
+  const size_t bps = d.sample_bits == 16 ? 2 : 1;
   const size_t n0 = (size_t)p.pitch[0] * p.H;
   p.fixed = n0 * 4 + n0;                                                            // weight sum, union
   for (uint32_t l = 1; l < p.L; ++l) p.fixed += (size_t)p.pitch[l] * p.lh[l];       // mask support
   for (uint32_t l = 0; l < p.L; ++l) p.fixed += (size_t)p.pitch[l] * p.lh[l] * 12;  // accumulators
   for (uint32_t l = 1; l + 1 < p.L; ++l) p.fixed += p.K * ((size_t)p.pitch[l] * p.lh[l] * (esz * 4 + 1));
-  p.fixed += (size_t)p.W * p.H * 3;  // output
-  p.planes = n0 * 8;
-  p.frame_pitch = round_up((int64_t)d.src_width * d.channels, 16);
+  p.fixed += (size_t)p.W * p.H * 3 * bps;  // output
+  // per frame (cache) or batch slot: remapped RGBA + weight; 16-bit frames:
+  // level-0 Gaussian (3 f32 planes), normalised mask (f32) and support (u8)
+  p.planes = bps == 2 ? n0 * 17 : n0 * 8;
+  p.frame_pitch = round_up((int64_t)d.src_width * d.channels * (int64_t)bps, 16);
   p.frame_bytes = (size_t)p.frame_pitch * d.src_height;
   p.staging_slots = std::min<size_t>(2 * (size_t)p.K, d.frame_count);
   p.fp_level = p.L > 1 ? p.L - 1 : 1;
@@ -755,7 +809,7 @@ StackPlan plan_stack(const fs_stack_desc& d) {
       }
     }
   }
-  if (p.L >= 3) {
+  if (p.L >= 3 && bps == 1) {
     p.laps_frame = n0 * 4;
     for (uint32_t l = 1; l + 1 < p.L; ++l) p.laps_frame += (size_t)p.pitch[l] * p.lh[l] * 12;
     p.laps_frame += (size_t)p.pitch[p.L - 1] * p.lh[p.L - 1] * 12;  // top Gaussian
@@ -786,9 +840,9 @@ uint64_t plan_bytes(const StackPlan& p, uint32_t frames, Pass2Mode mode, bool ho
 
 // Pass-2 mode for `available` device bytes: cache the pass-1 planes when they
 // fit, else keep the frames, else refetch them.
-Pass2Mode choose_mode(const StackPlan& p, uint32_t frames, uint64_t available, bool host_frames) {
+Pass2Mode choose_mode(const StackPlan& p, uint32_t frames, uint64_t available, bool host_frames, bool wide) {
   if (p.laps_frame && plan_bytes(p, frames, P2_LAPS, host_frames) <= available) return P2_LAPS;
-  if (plan_bytes(p, frames, P2_CACHE, host_frames) <= available) return P2_CACHE;
+  if (!wide && plan_bytes(p, frames, P2_CACHE, host_frames) <= available) return P2_CACHE;
   if (plan_bytes(p, frames, P2_RESIDENT, host_frames) <= available) return P2_RESIDENT;
   return P2_REFETCH;
 }
@@ -811,6 +865,7 @@ static int begin_impl(fs_ctx* ctx, const fs_stack_desc* desc, fs_stack** out, in
   s->roi = plan.roi;
   s->aligned = d.input_is_aligned != 0;
   s->storage = d.level_storage;
+  s->bps = d.sample_bits == 16 ? 2 : 1;
   s->W = plan.W;
   s->H = plan.H;
   s->L = plan.L;
@@ -853,7 +908,7 @@ static int begin_impl(fs_ctx* ctx, const fs_stack_desc* desc, fs_stack** out, in
       s->slot[kk][l] = lp;
     }
   }
-  if ((rc = stack_alloc(s, (size_t)s->W * s->H * 3, &p)) != FS_OK) return fail(rc);
+  if ((rc = stack_alloc(s, (size_t)s->W * s->H * 3 * s->bps, &p)) != FS_OK) return fail(rc);
   s->out_dev = (uint8_t*)p;
   s->fp_level = plan.fp_level;
   if (plan.contrib) {
@@ -868,7 +923,8 @@ static int begin_impl(fs_ctx* ctx, const fs_stack_desc* desc, fs_stack** out, in
   s->frame_bytes = plan.frame_bytes;
   const uint64_t in_use = ctx->held;
   const uint64_t available = ctx->budget + plan.fixed > in_use ? ctx->budget + plan.fixed - in_use : 0;
-  s->mode = forced_mode >= 0 ? (Pass2Mode)forced_mode : choose_mode(plan, d.frame_count, available, true);
+  s->mode = forced_mode >= 0 ? (Pass2Mode)forced_mode
+                             : choose_mode(plan, d.frame_count, available, true, d.sample_bits == 16);
   const size_t planes_bytes = plan.planes;
   if (s->mode == P2_LAPS) {
     if ((rc = stack_alloc(s, plan.laps_fixed, &p)) != FS_OK) return fail(rc);
@@ -911,6 +967,12 @@ static int begin_impl(fs_ctx* ctx, const fs_stack_desc* desc, fs_stack** out, in
       if ((rc = stack_alloc(s, planes_bytes, &p)) != FS_OK) return fail(rc);
       s->cache.push_back(FramePlanes{(uint32_t*)p, (float*)((uint8_t*)p + n0 * 4)});
     }
+  } else if (s->bps == 2) {
+    // level-0 Gaussian (3 f32 planes), normalised mask and support per batch slot
+    for (uint32_t kk = 0; kk < s->K; ++kk) {
+      if ((rc = stack_alloc(s, planes_bytes, &p)) != FS_OK) return fail(rc);
+      s->slot0.push_back(LevelPlanes{p, (uint8_t*)p + n0 * 12, (uint8_t*)p + n0 * 16, (int64_t)n0});
+    }
   } else {
     for (uint32_t kk = 0; kk < s->K; ++kk) {
       if ((rc = stack_alloc(s, planes_bytes, &p)) != FS_OK) return fail(rc);
@@ -926,8 +988,10 @@ int fs_stack_begin(fs_ctx* ctx, const fs_stack_desc* desc, fs_stack** out) { ret
 
 int fs_stack_begin_mode(fs_ctx* ctx, const fs_stack_desc* desc, int pass2_mode, fs_stack** out) {
   if (pass2_mode < -1 || pass2_mode > 3) return set_err(ctx, FS_ERR_INVALID, "unknown pass-2 mode");
+  if (desc && desc->sample_bits == 16 && (pass2_mode == P2_CACHE || pass2_mode == P2_LAPS))
+    return set_err(ctx, FS_ERR_UNSUPPORTED, "16-bit stacks run the resident or refetch mode");
   if (desc && pass2_mode == P2_LAPS && plan_stack(*desc).laps_frame == 0)
-    return set_err(ctx, FS_ERR_UNSUPPORTED, "the laps mode needs at least 3 pyramid levels");
+    return set_err(ctx, FS_ERR_UNSUPPORTED, "the laps mode needs at least 3 pyramid levels (8-bit samples)");
   return begin_impl(ctx, desc, out, pass2_mode);
 }
 
@@ -941,7 +1005,7 @@ static int add_frame_impl(fs_stack* s, const void* pixels, size_t row_stride, co
   if (s->finished) return set_err(ctx, FS_ERR_STATE, "stack already finished");
   if (s->frames.size() >= s->d.frame_count) return set_err(ctx, FS_ERR_STATE, "more frames than frame_count");
   if (!s->aligned && !pose) return set_err(ctx, FS_ERR_INVALID, "pose required for source frames");
-  const size_t row_bytes = (size_t)s->d.src_width * s->d.channels;
+  const size_t row_bytes = (size_t)s->d.src_width * s->d.channels * s->bps;
   if (row_stride < row_bytes) return set_err(ctx, FS_ERR_MISMATCH, "row stride smaller than the stack's row");
   cudaSetDevice(ctx->device);
   fs_stack::Frame fr;
@@ -1026,7 +1090,7 @@ static int finish_impl(fs_stack* s, fs_frame_fetch_cb refetch, void* user, void*
   if (s->finished) return set_err(ctx, FS_ERR_STATE, "stack already finished");
   if (s->frames.size() != s->d.frame_count)
     return set_err(ctx, FS_ERR_STATE, "fewer frames added than frame_count");
-  if (out_stride < (size_t)s->W * 3) return set_err(ctx, FS_ERR_INVALID, "output stride too small");
+  if (out_stride < (size_t)s->W * 3 * s->bps) return set_err(ctx, FS_ERR_INVALID, "output stride too small");
   cudaSetDevice(ctx->device);
   int rc;
   if (s->phase < 1) {
@@ -1126,19 +1190,21 @@ static int pass2_impl(fs_stack* s, fs_frame_fetch_cb refetch, void* user) {
         size_t hs = 0;
         if (refetch(user, (uint32_t)k, &hp, &hs) != 0 || !hp)
           return set_err(ctx, FS_ERR_INVALID, "refetch callback failed");
-        if (hs < (size_t)s->d.src_width * s->d.channels)
-          return set_err(ctx, FS_ERR_MISMATCH, "refetched row stride too small");
+        const size_t row_bytes = (size_t)s->d.src_width * s->d.channels * s->bps;
+        if (hs < row_bytes) return set_err(ctx, FS_ERR_MISMATCH, "refetched row stride too small");
         uint8_t* buf = s->staging[(k - begin) % s->staging.size()];
-        e = cudaMemcpy2DAsync(buf, (size_t)s->frame_pitch, hp, hs, (size_t)s->d.src_width * s->d.channels,
-                              s->d.src_height, cudaMemcpyHostToDevice, st);
+        e = cudaMemcpy2DAsync(buf, (size_t)s->frame_pitch, hp, hs, row_bytes, s->d.src_height,
+                              cudaMemcpyHostToDevice, st);
         if (e != cudaSuccess) return cuda_err(ctx, e, "frame refetch upload");
         e = cudaStreamSynchronize(st);  // the callback's buffer may be reused after it returns again
         if (e != cudaSuccess) return cuda_err(ctx, e, "frame refetch upload");
         fr.px = buf;
         fr.pitch = s->frame_pitch;
       }
-      rc = launch_remap_weights_batch(s, frames, begin, end, false);
+      rc = s->bps == 2 ? launch_remap16_batch(s, frames, begin, end, false, inv_count)
+                       : launch_remap_weights_batch(s, frames, begin, end, false);
       if (rc != FS_OK) return rc;
+      if (s->bps == 2 && s->L == 1) continue;  // blended with the planes (1 x 1 stack)
     }
     LevelArgs a;
     std::memset(&a, 0, sizeof(a));
@@ -1146,7 +1212,10 @@ static int pass2_impl(fs_stack* s, fs_frame_fetch_cb refetch, void* user) {
     a.K = (int32_t)(end - begin);
     a.inv_count = inv_count;
     a.norm = s->norm;
-    for (size_t k = begin; k < end; ++k) a.in0[k - begin] = s->mode == P2_CACHE ? s->cache[k] : s->p2[k - begin];
+    for (size_t k = begin; k < end; ++k) {
+      if (s->bps == 2) a.in[k - begin] = s->slot0[k - begin];  // level 0 of 16-bit frames: f32 planes
+      else a.in0[k - begin] = s->mode == P2_CACHE ? s->cache[k] : s->p2[k - begin];
+    }
     for (uint32_t l = 0; l + 1 < s->L || (s->L == 1 && l == 0); ++l) {
       a.level = (int32_t)l;
       a.wl = (int32_t)s->lw[l];
@@ -1174,7 +1243,8 @@ static int pass2_impl(fs_stack* s, fs_frame_fetch_cb refetch, void* user) {
       a.frame_parallel = fp ? 1 : 0;
       a.contrib = fp ? s->contrib : nullptr;
       a.contrib_top = fp ? s->contrib_top : nullptr;
-      if (l == 0) e = timed(ctx, "level0", [&] { return launch_level0(a, s->storage, st); });
+      if (l == 0 && s->bps == 2) e = timed(ctx, "level0", [&] { return launch_level(a, FS_STORAGE_F32, st); });
+      else if (l == 0) e = timed(ctx, "level0", [&] { return launch_level0(a, s->storage, st); });
       else e = timed(ctx, "level", [&] { return launch_level(a, s->storage, st); });
       if (e != cudaSuccess) return cuda_err(ctx, e, "level launch");
       if (fp) {
@@ -1203,7 +1273,7 @@ static int collapse_impl(fs_stack* s, void* out, size_t out_stride, bool device_
   if (s->L == 1) {
     e = timed(ctx, "collapse", [&] {
       return launch_quantize(s->acc[0], s->pitch[0] * s->lh[0], s->pitch[0], (int)s->W, (int)s->H, s->out_dev,
-                             (int64_t)s->W * 3, s->base_out, s->base_pitch, st);
+                             (int64_t)s->W * 3 * s->bps, s->base_out, s->base_pitch, s->bps == 2, st);
     });
     if (e != cudaSuccess) return cuda_err(ctx, e, "quantise");
   }
@@ -1222,17 +1292,19 @@ static int collapse_impl(fs_stack* s, void* out, size_t out_stride, bool device_
     c.acc_c = s->acc[l];
     c.plane_c = s->pitch[l] * s->lh[l];
     c.out = l == 1 ? s->out_dev : nullptr;
-    c.out_pitch = (int64_t)s->W * 3;
+    c.out_pitch = (int64_t)s->W * 3 * s->bps;
+    c.out16 = s->bps == 2 ? 1 : 0;
     c.base = l == 1 ? s->base_out : nullptr;
     c.base_pitch = s->base_pitch;
     e = timed(ctx, "collapse", [&] { return launch_collapse(c, st); });
     if (e != cudaSuccess) return cuda_err(ctx, e, "collapse");
   }
   const cudaMemcpyKind kind = device_out ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
-  if (out_stride == (size_t)s->W * 3)
-    e = cudaMemcpyAsync(out, s->out_dev, (size_t)s->W * 3 * s->H, kind, st);
+  const size_t row = (size_t)s->W * 3 * s->bps;
+  if (out_stride == row)
+    e = cudaMemcpyAsync(out, s->out_dev, row * s->H, kind, st);
   else
-    e = cudaMemcpy2DAsync(out, out_stride, s->out_dev, (size_t)s->W * 3, (size_t)s->W * 3, s->H, kind, st);
+    e = cudaMemcpy2DAsync(out, out_stride, s->out_dev, row, row, s->H, kind, st);
   if (e != cudaSuccess) return cuda_err(ctx, e, "output copy");
   if (wait) {
     e = cudaStreamSynchronize(st);
@@ -1249,6 +1321,7 @@ int fs_stack_mode_bytes(const fs_stack_desc* desc, int pass2_mode, int host_fram
   if (check_desc(*desc, &code)) return code;
   const StackPlan plan = plan_stack(*desc);
   if (pass2_mode == P2_LAPS && plan.laps_frame == 0) return FS_ERR_UNSUPPORTED;
+  if (desc->sample_bits == 16 && pass2_mode == P2_CACHE) return FS_ERR_UNSUPPORTED;
   *bytes = plan_bytes(plan, desc->frame_count, (Pass2Mode)pass2_mode, host_frames != 0);
   return FS_OK;
 }
@@ -1259,7 +1332,7 @@ int fs_stack_footprint(const fs_stack_desc* desc, uint64_t available_bytes, int 
   int code = FS_OK;
   if (check_desc(*desc, &code)) return code;
   const StackPlan plan = plan_stack(*desc);
-  const Pass2Mode m = choose_mode(plan, desc->frame_count, available_bytes, host_frames != 0);
+  const Pass2Mode m = choose_mode(plan, desc->frame_count, available_bytes, host_frames != 0, desc->sample_bits == 16);
   *bytes = plan_bytes(plan, desc->frame_count, m, host_frames != 0);
   if (mode) *mode = (int)m;
   return *bytes <= available_bytes ? FS_OK : FS_ERR_BUDGET;
@@ -1308,7 +1381,7 @@ int fs_stack_collapse(fs_stack* s, void* out_pixels, size_t out_stride, int devi
   int rc = phase_check(s, 2);
   if (rc != FS_OK) return rc;
   if (!out_pixels) return FS_ERR_INVALID;
-  if (out_stride < (size_t)s->W * 3) return set_err(s->ctx, FS_ERR_INVALID, "output stride too small");
+  if (out_stride < (size_t)s->W * 3 * s->bps) return set_err(s->ctx, FS_ERR_INVALID, "output stride too small");
   if ((rc = collapse_impl(s, out_pixels, out_stride, device_out != 0, true)) != FS_OK) return rc;
   s->finished = true;
   return FS_OK;
@@ -1525,11 +1598,14 @@ int fs_batch_create(fs_ctx* ctx, uint32_t n, const fs_stack_desc* descs, const v
   for (uint32_t i = 0; i < n; ++i) {
     int code = FS_OK;
     if (const char* why = check_desc(descs[i], &code)) return fail(set_err(ctx, code, why));
+    if (descs[i].sample_bits != 8) return fail(set_err(ctx, FS_ERR_UNSUPPORTED, "batches take 8-bit stacks"));
     if (!frames[i]) return fail(set_err(ctx, FS_ERR_INVALID, "null frame list"));
     if (!descs[i].input_is_aligned && !poses) return fail(set_err(ctx, FS_ERR_INVALID, "poses required"));
     const StackPlan plan = plan_stack(descs[i]);
     const uint64_t left = ctx->budget > ctx->held + total ? ctx->budget - ctx->held - total : 0;
-    Pass2Mode m = pass2_mode == 0 ? P2_CACHE : pass2_mode == 1 ? P2_RESIDENT : choose_mode(plan, descs[i].frame_count, left, true);
+    Pass2Mode m = pass2_mode == 0 ? P2_CACHE
+                  : pass2_mode == 1 ? P2_RESIDENT
+                                    : choose_mode(plan, descs[i].frame_count, left, true, descs[i].sample_bits == 16);
     if (m == P2_REFETCH) m = P2_RESIDENT;
     b->planned.push_back((int)m);
     bytes[i] = plan_bytes(plan, descs[i].frame_count, m, true);

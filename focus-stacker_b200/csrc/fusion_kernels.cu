@@ -1983,8 +1983,13 @@ __global__ void __launch_bounds__(NT) collapse_kernel(const __grid_constant__ Co
       float* p = a.acc_p + c * a.plane_p + o;
       const float nv = __fadd_rn(*p, v);
       if (a.out) {
-        const float q8 = fminf(fmaxf(__fadd_rn(nv, 0.5f), 0.0f), 255.0f);
-        a.out[(int64_t)y * a.out_pitch + (int64_t)x * 3 + c] = (uint8_t)q8;
+        if (a.out16) {
+          const float q = fminf(fmaxf(__fadd_rn(nv, 0.5f), 0.0f), 65535.0f);
+          reinterpret_cast<uint16_t*>(a.out + (int64_t)y * a.out_pitch)[(int64_t)x * 3 + c] = (uint16_t)q;
+        } else {
+          const float q8 = fminf(fmaxf(__fadd_rn(nv, 0.5f), 0.0f), 255.0f);
+          a.out[(int64_t)y * a.out_pitch + (int64_t)x * 3 + c] = (uint8_t)q8;
+        }
         if (a.base) a.base[(int64_t)y * a.base_pitch + (int64_t)x * 3 + c] = nv;
       } else {
         *p = nv;
@@ -2001,20 +2006,25 @@ cudaError_t launch_collapse(const CollapseArgs& a, cudaStream_t s) {
 
 // Quantise a single-level accumulator (1x1 images have no collapse step).
 __global__ void quantize_kernel(const float* acc, int64_t plane, int64_t pitch, int w, int h, uint8_t* out,
-                                int64_t out_pitch, float* base, int64_t base_pitch) {
+                                int64_t out_pitch, float* base, int64_t base_pitch, int out16) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= w * h) return;
   const int x = i % w, y = i / w;
   for (int c = 0; c < 3; ++c) {
     const float v = acc[c * plane + (int64_t)y * pitch + x];
-    out[(int64_t)y * out_pitch + x * 3 + c] = (uint8_t)fminf(fmaxf(__fadd_rn(v, 0.5f), 0.0f), 255.0f);
+    if (out16)
+      reinterpret_cast<uint16_t*>(out + (int64_t)y * out_pitch)[x * 3 + c] =
+          (uint16_t)fminf(fmaxf(__fadd_rn(v, 0.5f), 0.0f), 65535.0f);
+    else
+      out[(int64_t)y * out_pitch + x * 3 + c] = (uint8_t)fminf(fmaxf(__fadd_rn(v, 0.5f), 0.0f), 255.0f);
     if (base) base[(int64_t)y * base_pitch + x * 3 + c] = v;
   }
 }
 
 cudaError_t launch_quantize(const float* acc, int64_t plane, int64_t pitch, int w, int h, uint8_t* out,
-                            int64_t out_pitch, float* base, int64_t base_pitch, cudaStream_t s) {
-  quantize_kernel<<<(w * h + 255) / 256, 256, 0, s>>>(acc, plane, pitch, w, h, out, out_pitch, base, base_pitch);
+                            int64_t out_pitch, float* base, int64_t base_pitch, int out16, cudaStream_t s) {
+  quantize_kernel<<<(w * h + 255) / 256, 256, 0, s>>>(acc, plane, pitch, w, h, out, out_pitch, base, base_pitch,
+                                                      out16);
   return cudaGetLastError();
 }
 

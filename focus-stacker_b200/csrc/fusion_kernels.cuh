@@ -117,8 +117,9 @@ struct CollapseArgs {
   int64_t plane_p;
   const float* acc_c;
   int64_t plane_c;
-  uint8_t* out;               // final level: interleaved RGB u8 output, else null
-  int64_t out_pitch;
+  uint8_t* out;               // final level: interleaved RGB output (u8, or u16 with out16), else null
+  int64_t out_pitch;          // bytes per output row
+  int32_t out16;              // 1: u16 output samples (clamped to 65535), 0: u8
   float* base;                // final level, optional: collapsed base before quantisation (RGB f32)
   int64_t base_pitch;         // elements per row
 };
@@ -160,6 +161,28 @@ struct RemapArgs {
 };
 
 cudaError_t launch_remap_weights(const RemapWeightArgs& a, int border, cudaStream_t s);
+
+// 16-bit frames (fusion16.cu): pass 1 (accumulate = 1: weight sum and union)
+// or pass 2 (out[k]: the frame's level-0 Gaussian as 3 f32 planes, its
+// normalised mask (f32) and support (u8), plane = pitch * H elements).
+struct Remap16Args {
+  int32_t W, H;
+  int32_t window_ok;
+  int32_t K;
+  int32_t accumulate;
+  int32_t first;
+  float inv_count;       // 1 / N, the mask where the weight sum is <= 1e-12
+  float* norm;
+  uint8_t* uni;
+  int64_t pitch;
+  FrameIn f[kMaxBatch];  // src.px: u16 samples, src.pitch in bytes
+  LevelPlanes out[kMaxBatch];
+};
+cudaError_t launch_remap16_weights(const Remap16Args& a, int border, cudaStream_t s);
+// Standalone u16 remap: dst holds dst_ch u16 samples per pixel.
+cudaError_t launch_remap16(const RemapArgs& a, cudaStream_t s);
+// 1 x 1 stacks: acc += G0_k * m_k over the batch (a.out planes, a.K frames).
+cudaError_t launch_blend_single_level(float* acc, int64_t acc_plane, const Remap16Args& a, cudaStream_t s);
 cudaError_t launch_lap0(const Lap0Args& a, int border, cudaStream_t s);
 // acc0 = A_w / N where N > 1e-12, else A_u * inv_count (acc0 written over A_w).
 cudaError_t launch_finalize0(float* acc, const float* au, const float* norm, int64_t plane, int64_t pitch, int w,
@@ -182,7 +205,7 @@ cudaError_t launch_sum_contrib(float* acc, int64_t plane, int64_t pitch, int w, 
 cudaError_t launch_mask_support(const MaskSupportArgs& a, cudaStream_t s);
 cudaError_t launch_remap(const RemapArgs& a, cudaStream_t s);
 cudaError_t launch_quantize(const float* acc, int64_t plane, int64_t pitch, int w, int h, uint8_t* out,
-                            int64_t out_pitch, float* base, int64_t base_pitch, cudaStream_t s);
+                            int64_t out_pitch, float* base, int64_t base_pitch, int out16, cudaStream_t s);
 
 // Synthetic stacks (synth.cu).
 void synth_pose(uint64_t seed, int scene, uint32_t width, uint32_t height, uint32_t frame, uint32_t frame_count,

@@ -270,7 +270,7 @@ extern "C" int fs_fuse_aligned_device_static(const void* const* dev_frames, cons
   // collapse straight into the caller's output
   if (L == 1) {
     e = launch_quantize(acc[0], lay.pitch[0] * lay.lh[0], lay.pitch[0], (int)width, (int)height, (uint8_t*)dev_out,
-                        (int64_t)out_stride, nullptr, 0, st);
+                        (int64_t)out_stride, nullptr, 0, 0, st);
     if (e != cudaSuccess) return fail(e, "quantise launch");
   }
   for (uint32_t l = L - 1; l >= 1 && L > 1; --l) {

@@ -4,8 +4,8 @@
  *
  * Plain C types only: pointers, sizes, PODs.  Every call returns an fs_status
  * (0 = FS_OK); fs_last_error() gives a message for the last failure on a
- * context.  Pixel buffers are interleaved, row-major, u8 (8-bit samples),
- * with an explicit row stride in bytes.
+ * context.  Pixel buffers are interleaved, row-major, u8 or u16 samples
+ * (fs_stack_desc.sample_bits), with an explicit row stride in bytes.
  *
  * Each entry point names the reference (asingleoat/focus-stacker, Zig)
  * interface it replaces; paths are relative to the reference project root.
@@ -31,7 +31,7 @@ typedef enum fs_status {
   FS_ERR_TIMEOUT = 5,     /* a bounded device wait gave up                   */
   FS_ERR_STATE = 6,       /* call out of order (e.g. frame after finish)     */
   FS_ERR_MISMATCH = 7,    /* frame size / format differs from the stack's    */
-  FS_ERR_UNSUPPORTED = 8, /* valid but not implemented (e.g. 16-bit fusion)  */
+  FS_ERR_UNSUPPORTED = 8, /* valid but not implemented (e.g. 16-bit FP16 levels) */
   FS_ERR_NO_DEVICE = 9    /* no CUDA device / library built for another arch */
 } fs_status;
 
@@ -142,6 +142,16 @@ int fs_remap_frame(fs_ctx* ctx, const void* src, size_t src_stride, uint32_t wid
 int fs_remap_frame_device(fs_ctx* ctx, const void* src, size_t src_stride, uint32_t width, uint32_t height,
                           uint32_t channels, const fs_pose* pose, const fs_rect* roi, void* dst, size_t dst_stride);
 
+/* The u16 twins: 16-bit samples in and out, alpha 65535 inside the frame and
+ * round(support * 65535) on its edge; replaces remap.remapRigidImage on u16
+ * images (remapU16, src/remap.zig:280-336, 443-541, 841-937).  Strides in
+ * bytes. */
+int fs_remap_frame16(fs_ctx* ctx, const void* src, size_t src_stride, uint32_t width, uint32_t height,
+                     uint32_t channels, const fs_pose* pose, const fs_rect* roi, void* dst, size_t dst_stride);
+int fs_remap_frame16_device(fs_ctx* ctx, const void* src, size_t src_stride, uint32_t width, uint32_t height,
+                            uint32_t channels, const fs_pose* pose, const fs_rect* roi, void* dst,
+                            size_t dst_stride);
+
 /* ------------------------------------------------------- fusion (stacks) */
 
 typedef struct fs_stack_desc {
@@ -149,7 +159,7 @@ typedef struct fs_stack_desc {
   int32_t has_roi;                /* 0: output = full frame; 1: output = roi          */
   fs_rect roi;                    /* output region in aligned-frame coordinates       */
   uint32_t channels;              /* 3 = RGB source frames; aligned input: 3 or 4     */
-  uint32_t sample_bits;           /* 8                                                */
+  uint32_t sample_bits;           /* 8 (u8) or 16 (u16; FP32 levels, output u16)     */
   uint32_t frame_count;           /* active frames that will be added (N)             */
   uint32_t contrast_window;       /* odd >= 3, default 5 (--contrast-window-size)     */
   int32_t input_is_aligned;       /* 1: frames are pre-aligned (focus_fuse_zig path)  */
