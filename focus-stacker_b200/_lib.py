@@ -28,7 +28,7 @@ EXPORTED = (
     "fs_remap_frame", "fs_remap_frame_device", "fs_remap_frame16", "fs_remap_frame16_device",
     "fs_stack_begin", "fs_stack_add_frame", "fs_stack_add_frame_async", "fs_stack_add_frame_device", "fs_stack_finish",
     "fs_stack_finish_device", "fs_stack_finish_async", "fs_stack_wait", "fs_stack_set_base_output", "fs_stack_pass2_mode", "fs_stack_footprint", "fs_stack_mode_bytes", "fs_stack_begin_mode",
-    "fs_stack_set_frame_total", "fs_stack_end_pass1", "fs_stack_blend", "fs_stack_collapse", "fs_stack_buffer", "fs_stack_output_size", "fs_stack_destroy", "fs_fuse_stack",
+    "fs_stack_set_method", "fs_stack_set_frame_total", "fs_stack_end_pass1", "fs_stack_blend", "fs_stack_collapse", "fs_stack_buffer", "fs_stack_output_size", "fs_stack_destroy", "fs_fuse_stack",
     "fs_batch_create", "fs_batch_run", "fs_batch_stack_count", "fs_batch_pass2_mode", "fs_batch_uses_graph",
     "fs_batch_destroy",
     "fs_fuse_aligned_device_static", "fs_synth_frame_device", "fs_synth_pose",
@@ -121,6 +121,7 @@ def _bind(L):
     L.fs_stack_footprint.argtypes = [P(FsStackDesc), u64, i32, P(u64), P(i32)]
     L.fs_stack_mode_bytes.argtypes = [P(FsStackDesc), i32, i32, P(u64)]
     L.fs_stack_begin_mode.argtypes = [ctx, P(FsStackDesc), i32, P(vp)]
+    L.fs_stack_set_method.argtypes = [vp, i32, ctypes.c_float]
     L.fs_stack_set_frame_total.argtypes = [vp, u32]
     L.fs_stack_end_pass1.argtypes = [vp]
     L.fs_stack_blend.argtypes = [vp, FETCH_CB, vp]

@@ -103,6 +103,7 @@ class Method(enum.Enum):
     PYRAMID_CONTRAST = "pyramid-contrast"
     HYBRID_PYRAMID_CONTRAST = "hybrid-pyramid-contrast"
     CUDA_PYRAMID_CONTRAST = "cuda-pyramid-contrast"
+    CUDA_HYBRID_PYRAMID_CONTRAST = "cuda-hybrid-pyramid-contrast"
 
     def cli_name(self) -> str:
         return self.value
@@ -281,7 +282,12 @@ def remap_rigid_image_device(ctx: Context, src, src_stride: int, width: int, hei
 
 # --------------------------------------------------------------------- fusion
 PASS2_MODES = ("cache", "resident", "refetch", "laps")
-BUFFER_WEIGHT_SUM, BUFFER_UNION, BUFFER_ACCUMULATOR = 0, 1, 2
+# fs_stack_set_method: the fusion methods the stack runs on the device, and
+# the default weight of the hard image's levels (--hybrid-sharpness,
+# src/fuse/pyramid.zig:11)
+FUSION_METHODS = ("pyramid-contrast", "hybrid-pyramid-contrast")
+HYBRID_SHARPNESS = 0.35
+BUFFER_WEIGHT_SUM, BUFFER_UNION, BUFFER_ACCUMULATOR, BUFFER_HARD = 0, 1, 2, 3
 
 
 class DeviceBuffer:
@@ -345,7 +351,8 @@ class PyramidContrastStack:
 
     def __init__(self, ctx: Context, src_width: int, src_height: int, frame_count: int, roi: Optional[Rect] = None,
                  channels: int = 3, contrast_window: int = 5, aligned: bool = False, frames_per_batch: int = 0,
-                 level_storage: int = 0, pass2_mode: Optional[str] = None, sample_bits: int = 8):
+                 level_storage: int = 0, pass2_mode: Optional[str] = None, sample_bits: int = 8,
+                 method: str = "pyramid-contrast", hybrid_sharpness: float = HYBRID_SHARPNESS):
         """pass2_mode: None picks the mode from the context's budget; "cache",
         "resident", "refetch" or "laps" imposes one.  sample_bits 16: uint16
         frames in and a uint16 image out (FP32 levels; resident / refetch)."""
@@ -358,6 +365,11 @@ class PyramidContrastStack:
         mode = -1 if pass2_mode is None else PASS2_MODES.index(pass2_mode)
         _check(L().fs_stack_begin_mode(ctx.handle, ctypes.byref(d), mode, ctypes.byref(h)), ctx.handle)
         self.handle = h
+        if method not in FUSION_METHODS:
+            self.close()
+            raise FocusCudaError(1, f"unknown fusion method {method!r}")
+        if method != "pyramid-contrast":
+            _check(L().fs_stack_set_method(h, FUSION_METHODS.index(method), hybrid_sharpness), ctx.handle)
         w, hh = ctypes.c_uint32(), ctypes.c_uint32()
         L().fs_stack_output_size(h, ctypes.byref(w), ctypes.byref(hh))
         self.out_width, self.out_height = w.value, hh.value
@@ -462,6 +474,8 @@ class PyramidContrastStack:
             shape, typestr = (3, h.value, pitch.value), "<f4"
         elif which == BUFFER_WEIGHT_SUM:
             shape, typestr = (h.value, pitch.value), "<f4"
+        elif which == BUFFER_HARD:
+            shape, typestr = (h.value, pitch.value), "<i4"  # RGBA words (bit pattern of u32)
         else:
             shape, typestr = (h.value, pitch.value), "|u1"
         return DeviceBuffer(int(p.value), shape, typestr, w.value, h.value, self)
@@ -502,13 +516,16 @@ class PyramidContrastStack:
 
 
 def fuse_remapped_images(ctx: Context, sources: Sequence[np.ndarray], poses: Sequence, roi: Optional[Rect],
-                         contrast_window: int = 5, frames_per_batch: int = 0) -> np.ndarray:
+                         contrast_window: int = 5, frames_per_batch: int = 0, method: str = "pyramid-contrast",
+                         hybrid_sharpness: float = HYBRID_SHARPNESS) -> np.ndarray:
     """Stack path: remap every active frame through its pose into the ROI and
-    fuse with pyramid-contrast (runCollapsedPyramidStackPass)."""
+    fuse with pyramid-contrast (runCollapsedPyramidStackPass), or with
+    method="hybrid-pyramid-contrast" the hybrid branch of the same driver."""
     h, w = sources[0].shape[:2]
     bits = 16 if sources[0].dtype == np.uint16 else 8
     with PyramidContrastStack(ctx, w, h, len(sources), roi=roi, channels=3, contrast_window=contrast_window,
-                              frames_per_batch=frames_per_batch, sample_bits=bits) as st:
+                              frames_per_batch=frames_per_batch, sample_bits=bits, method=method,
+                              hybrid_sharpness=hybrid_sharpness) as st:
         for src, pose in zip(sources, poses):
             if src.shape[:2] != (h, w):
                 raise FocusCudaError(7, "MismatchedImageSizes")

@@ -201,6 +201,10 @@ struct fs_stack {
   std::vector<FramePlanes> p2;                 // RESIDENT / REFETCH: per batch slot (K)
   std::vector<LevelPlanes> slot0;              // 16-bit frames: level-0 planes per batch slot (K)
   uint32_t bps = 1;                            // bytes per sample (1: u8, 2: u16)
+  int method = FS_METHOD_PYRAMID_CONTRAST;     // fs_stack_set_method
+  float hybrid_mix = 0.35f;                    // hybrid: weight of the hard image's levels
+  float* best = nullptr;                       // hybrid: per pixel the winning weight
+  uint32_t* hard = nullptr;                    // hybrid: per pixel the winning frame's RGBA word
   std::vector<float*> wplane;                  // LAPS: per frame, its weight (level 0)
   std::vector<std::vector<float*>> lap;        // LAPS: per frame, Laplacian of levels 1 .. L-2 ([0] unused)
   float* au = nullptr;                         // LAPS: sum of level-0 Laplacians where the weight sum <= 1e-12
@@ -390,6 +394,8 @@ int launch_lap0_batch(fs_stack* s, size_t begin, size_t end) {
   a.uni = s->uni;
   a.aw = s->acc[0];
   a.au = s->au;
+  a.best = s->best;
+  a.hard = s->hard;
   for (size_t k = begin; k < end; ++k) {
     std::string why;
     if (!build_frame_in(s, s->frames[k], &a.f[k - begin], &why)) return set_err(s->ctx, FS_ERR_INVALID, why);
@@ -1206,6 +1212,16 @@ static int pass2_impl(fs_stack* s, fs_frame_fetch_cb refetch, void* user) {
       if (rc != FS_OK) return rc;
       if (s->bps == 2 && s->L == 1) continue;  // blended with the planes (1 x 1 stack)
     }
+    if (s->best) {
+      // hybrid: the hardmask winners of this batch, from its pass-2 planes
+      FramePlanes pl[kMaxBatch];
+      for (size_t k = begin; k < end; ++k) pl[k - begin] = s->mode == P2_CACHE ? s->cache[k] : s->p2[k - begin];
+      e = timed(ctx, "winners", [&] {
+        return launch_winners(pl, (int)(end - begin), s->best, s->hard, begin == 0 ? 1 : 0, (int)s->W, (int)s->H,
+                              s->pitch[0], st);
+      });
+      if (e != cudaSuccess) return cuda_err(ctx, e, "winners");
+    }
     LevelArgs a;
     std::memset(&a, 0, sizeof(a));
     a.levels = (int32_t)s->L;
@@ -1264,16 +1280,16 @@ static int pass2_impl(fs_stack* s, fs_frame_fetch_cb refetch, void* user) {
   return FS_OK;
 }
 
-// Collapse of the accumulator pyramid and the quantised output
-// (src/fuse/pyramid.zig:223-269).
-static int collapse_impl(fs_stack* s, void* out, size_t out_stride, bool device_out, bool wait) {
+// Collapse kernels of the accumulator pyramid into the quantised output
+// out_dev, with the collapsed base into `base` when given.
+static int collapse_kernels(fs_stack* s, float* base) {
   fs_ctx* ctx = s->ctx;
   cudaStream_t st = ctx->stream;
   cudaError_t e;
   if (s->L == 1) {
     e = timed(ctx, "collapse", [&] {
       return launch_quantize(s->acc[0], s->pitch[0] * s->lh[0], s->pitch[0], (int)s->W, (int)s->H, s->out_dev,
-                             (int64_t)s->W * 3 * s->bps, s->base_out, s->base_pitch, s->bps == 2, st);
+                             (int64_t)s->W * 3 * s->bps, base, s->base_pitch, s->bps == 2, st);
     });
     if (e != cudaSuccess) return cuda_err(ctx, e, "quantise");
   }
@@ -1294,11 +1310,100 @@ static int collapse_impl(fs_stack* s, void* out, size_t out_stride, bool device_
     c.out = l == 1 ? s->out_dev : nullptr;
     c.out_pitch = (int64_t)s->W * 3 * s->bps;
     c.out16 = s->bps == 2 ? 1 : 0;
-    c.base = l == 1 ? s->base_out : nullptr;
+    c.base = l == 1 ? base : nullptr;
     c.base_pitch = s->base_pitch;
     e = timed(ctx, "collapse", [&] { return launch_collapse(c, st); });
     if (e != cudaSuccess) return cuda_err(ctx, e, "collapse");
   }
+  return FS_OK;
+}
+
+// hybrid-pyramid-contrast: the plain Laplacian pyramids of the soft image
+// (the pyramid-contrast output in out_dev) and of the hard image (the
+// winners' colours), merged into the accumulator pyramid
+// (mergeHybridImages, src/fuse/pyramid.zig:271-301; hard levels from
+// hybrid_hard_level_start = 2, hybrid_hard_level_count = 4, :9-10).
+static int hybrid_merge(fs_stack* s) {
+  fs_ctx* ctx = s->ctx;
+  cudaStream_t st = ctx->stream;
+  cudaError_t e;
+  std::vector<float*> gs(s->L), gh(s->L);
+  for (uint32_t l = 0; l < s->L; ++l) {
+    void* p;
+    const size_t bytes = (size_t)s->pitch[l] * s->lh[l] * 12;
+    int rc = stack_alloc(s, bytes, &p);
+    if (rc == FS_OK) {
+      gs[l] = (float*)p;
+      rc = stack_alloc(s, bytes, &p);
+    }
+    if (rc != FS_OK) return rc;
+    gh[l] = (float*)p;
+  }
+  auto plane = [&](uint32_t l) { return s->pitch[l] * s->lh[l]; };
+  e = timed(ctx, "hybrid", [&] {
+    return launch_rgb_to_planes(s->out_dev, (int64_t)s->W * 3, 3, gs[0], plane(0), s->pitch[0], (int)s->W, (int)s->H,
+                                st);
+  });
+  if (e == cudaSuccess)
+    e = timed(ctx, "hybrid", [&] {
+      return launch_rgb_to_planes((const uint8_t*)s->hard, s->pitch[0] * 4, 4, gh[0], plane(0), s->pitch[0],
+                                  (int)s->W, (int)s->H, st);
+    });
+  for (uint32_t l = 0; e == cudaSuccess && l + 1 < s->L; ++l) {
+    for (std::vector<float*>* g : {&gs, &gh}) {
+      e = timed(ctx, "hybrid", [&] {
+        return launch_reduce_plain((*g)[l], plane(l), s->pitch[l], (int)s->lw[l], (int)s->lh[l], (*g)[l + 1],
+                                   plane(l + 1), s->pitch[l + 1], (int)s->lw[l + 1], (int)s->lh[l + 1], st);
+      });
+      if (e != cudaSuccess) break;
+    }
+  }
+  const uint32_t hs = std::min<uint32_t>(2, s->L), he = std::min<uint32_t>(hs + 4, s->L);
+  for (uint32_t l = 0; e == cudaSuccess && l + 1 < s->L; ++l) {
+    MergeArgs m;
+    std::memset(&m, 0, sizeof(m));
+    m.wp = (int32_t)s->lw[l];
+    m.hp = (int32_t)s->lh[l];
+    m.wc = (int32_t)s->lw[l + 1];
+    m.hc = (int32_t)s->lh[l + 1];
+    m.pitch_p = s->pitch[l];
+    m.pitch_c = s->pitch[l + 1];
+    m.plane_p = plane(l);
+    m.plane_c = plane(l + 1);
+    m.exact_expand = std::max(s->lw[l], s->lh[l]) <= kExactExpandMaxDim ? 1 : 0;
+    m.mixed = l >= hs && l < he ? 1 : 0;
+    m.mix = s->hybrid_mix;
+    m.soft_p = gs[l];
+    m.hard_p = gh[l];
+    m.soft_c = gs[l + 1];
+    m.hard_c = gh[l + 1];
+    m.acc = s->acc[l];
+    e = timed(ctx, "hybrid", [&] { return launch_merge_level(m, st); });
+  }
+  if (e == cudaSuccess) {
+    const uint32_t t = s->L - 1;
+    e = timed(ctx, "hybrid", [&] {
+      return launch_merge_top(gs[t], gh[t], s->acc[t], plane(t), s->pitch[t], (int)s->lw[t], (int)s->lh[t],
+                              t >= hs && t < he ? 1 : 0, s->hybrid_mix, st);
+    });
+  }
+  if (e != cudaSuccess) return cuda_err(ctx, e, "hybrid merge");
+  return FS_OK;
+}
+
+// Collapse of the accumulator pyramid and the quantised output
+// (src/fuse/pyramid.zig:223-269); the hybrid method collapses twice (the
+// soft image, then the merged pyramid).
+static int collapse_impl(fs_stack* s, void* out, size_t out_stride, bool device_out, bool wait) {
+  fs_ctx* ctx = s->ctx;
+  cudaStream_t st = ctx->stream;
+  cudaError_t e;
+  int rc;
+  if (s->best) {
+    if ((rc = collapse_kernels(s, nullptr)) != FS_OK) return rc;
+    if ((rc = hybrid_merge(s)) != FS_OK) return rc;
+  }
+  if ((rc = collapse_kernels(s, s->base_out)) != FS_OK) return rc;
   const cudaMemcpyKind kind = device_out ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
   const size_t row = (size_t)s->W * 3 * s->bps;
   if (out_stride == row)
@@ -1309,6 +1414,31 @@ static int collapse_impl(fs_stack* s, void* out, size_t out_stride, bool device_
   if (wait) {
     e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) return cuda_err(ctx, e, "fusion");
+  }
+  return FS_OK;
+}
+
+int fs_stack_set_method(fs_stack* s, int method, float hybrid_sharpness) {
+  if (!s) return FS_ERR_INVALID;
+  if (!s->ctx) return FS_ERR_STATE;
+  if (method != FS_METHOD_PYRAMID_CONTRAST && method != FS_METHOD_HYBRID_PYRAMID_CONTRAST)
+    return set_err(s->ctx, FS_ERR_INVALID, "unknown fusion method");
+  if (!(hybrid_sharpness >= 0.0f && hybrid_sharpness <= 1.0f))  // parseSharpness, src/fuse/config.zig:269-273
+    return set_err(s->ctx, FS_ERR_INVALID, "hybrid sharpness must be in [0, 1]");
+  if (!s->frames.empty() || s->finished) return set_err(s->ctx, FS_ERR_STATE, "method set after the first frame");
+  if (s->frame_total) return set_err(s->ctx, FS_ERR_UNSUPPORTED, "the hybrid method does not run frame-sharded");
+  s->method = method;
+  s->hybrid_mix = hybrid_sharpness;
+  if (method == FS_METHOD_HYBRID_PYRAMID_CONTRAST && !s->best) {
+    if (s->bps != 1) return set_err(s->ctx, FS_ERR_UNSUPPORTED, "the hybrid method takes 8-bit samples");
+    cudaSetDevice(s->ctx->device);
+    const size_t n0 = (size_t)s->pitch[0] * s->H;
+    void* p;
+    int rc = stack_alloc(s, n0 * 4, &p);
+    if (rc != FS_OK) return rc;
+    s->best = (float*)p;
+    if ((rc = stack_alloc(s, n0 * 4, &p)) != FS_OK) return rc;
+    s->hard = (uint32_t*)p;
   }
   return FS_OK;
 }
@@ -1353,6 +1483,7 @@ int fs_stack_set_frame_total(fs_stack* s, uint32_t frame_total) {
   if (!s) return FS_ERR_INVALID;
   if (!s->ctx) return FS_ERR_STATE;
   if (frame_total < s->d.frame_count) return set_err(s->ctx, FS_ERR_INVALID, "total below this stack's frames");
+  if (s->best) return set_err(s->ctx, FS_ERR_UNSUPPORTED, "the hybrid method does not run frame-sharded");
   s->frame_total = frame_total;
   return FS_OK;
 }
@@ -1398,6 +1529,11 @@ int fs_stack_buffer(fs_stack* s, int which, uint32_t level, void** ptr, uint64_t
     case FS_BUFFER_WEIGHT_SUM: *ptr = s->norm; *bytes = plane * 4; break;
     case FS_BUFFER_UNION: *ptr = s->uni; *bytes = plane; break;
     case FS_BUFFER_ACCUMULATOR: *ptr = s->acc[level]; *bytes = plane * 12; break;
+    case FS_BUFFER_HARD:
+      if (!s->hard) return set_err(s->ctx, FS_ERR_INVALID, "no hard image (pyramid-contrast stack)");
+      *ptr = s->hard;
+      *bytes = plane * 4;
+      break;
     default: return set_err(s->ctx, FS_ERR_INVALID, "no such buffer");
   }
   if (pitch) *pitch = s->pitch[level];

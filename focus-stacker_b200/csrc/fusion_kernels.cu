@@ -36,6 +36,7 @@
 #include <cuda_runtime.h>
 
 #include <atomic>
+#include <cmath>
 #include <cstddef>
 #include <type_traits>
 
@@ -1654,7 +1655,7 @@ __device__ __forceinline__ void store_level_sample(void* plane, int storage, int
 
 }  // namespace
 
-template <int B>
+template <int B, bool HARD>
 __global__ void __launch_bounds__(NT, 2) lap0_kernel(const __grid_constant__ Lap0Args a) {
   using Lay = Lap0Layout<B>;
   constexpr int RW = Lay::RW, RH = Lay::RH, KS = Lay::KS, HS = Lay::HS, R0 = Lay::R0, TS = Lay::TS;
@@ -1669,18 +1670,28 @@ __global__ void __launch_bounds__(NT, 2) lap0_kernel(const __grid_constant__ Lap
   const int vc = threadIdx.x % TW, vr0 = (threadIdx.x / TW) * PPT;
   const int X = x0 + vc;
   float nacc[PPT], aw[PPT][3], wv[PPT];
+  float best[HARD ? PPT : 1];      // hybrid: the winner's weight and RGBA word
+  uint32_t hard[HARD ? PPT : 1];
   uint32_t umask = 0;
 #pragma unroll
   for (int i = 0; i < PPT; ++i) {
     const int Y = y0 + vr0 + i;
     nacc[i] = 0.0f;
     aw[i][0] = aw[i][1] = aw[i][2] = 0.0f;
+    if constexpr (HARD) {
+      best[i] = -INFINITY;
+      hard[i] = 0u;
+    }
     if (!a.first && X < a.W && Y < a.H) {
       const int64_t o = (int64_t)Y * a.pitch + X;
       nacc[i] = a.norm[o];
       if (a.uni[o]) umask |= 1u << i;
 #pragma unroll
       for (int c = 0; c < 3; ++c) aw[i][c] = a.aw[c * a.plane + o];
+      if constexpr (HARD) {
+        best[i] = a.best[o];
+        hard[i] = a.hard[o];
+      }
     }
   }
   constexpr int kAnchorThreads = ((RW + 7) / 8) * ((RH + 3) / 4);
@@ -1760,6 +1771,12 @@ __global__ void __launch_bounds__(NT, 2) lap0_kernel(const __grid_constant__ Lap
         if (a.window_ok && al > 0 && X >= B && Y >= B && X < a.W - B && Y < a.H - B)
           w = __fmul_rn(window_stddev<B>(p, q, S.inv_den), alpha_support(al));
         wv[i] = w;
+        if constexpr (HARD) {
+          if (w > best[i]) {  // strictly larger weights win (src/fuse/blend.zig:259-261)
+            best[i] = w;
+            hard[i] = own;
+          }
+        }
         nacc[i] = __fadd_rn(nacc[i], w);
         if (al > 0) umask |= 1u << i;
         wout[(int64_t)Y * a.pitch + X] = w;
@@ -1894,20 +1911,27 @@ __global__ void __launch_bounds__(NT, 2) lap0_kernel(const __grid_constant__ Lap
       a.uni[o] = (uint8_t)((umask >> i) & 1u);
 #pragma unroll
       for (int c = 0; c < 3; ++c) a.aw[c * a.plane + o] = aw[i][c];
+      if constexpr (HARD) {
+        a.best[o] = best[i];
+        a.hard[o] = hard[i];
+      }
     }
   }
 }
 
-template <int B>
-static cudaError_t launch_lap0_b(const Lap0Args& a, cudaStream_t s) {
+template <int B, bool HARD>
+static cudaError_t launch_lap0_bh(const Lap0Args& a, cudaStream_t s) {
   static DeviceOnce configured;
   const size_t sm = sizeof(Lap0Smem<B>);
-  cudaError_t e = configured.run(
-      [&] { return cudaFuncSetAttribute(lap0_kernel<B>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm); });
+  cudaError_t e = configure(lap0_kernel<B, HARD>, sm, &configured);
   if (e != cudaSuccess) return e;
   dim3 grid((a.W + TW - 1) / TW, (a.H + TH - 1) / TH);
-  lap0_kernel<B><<<grid, NT, sm, s>>>(a);
+  lap0_kernel<B, HARD><<<grid, NT, sm, s>>>(a);
   return cudaGetLastError();
+}
+template <int B>
+static cudaError_t launch_lap0_b(const Lap0Args& a, cudaStream_t s) {
+  return a.best ? launch_lap0_bh<B, true>(a, s) : launch_lap0_bh<B, false>(a, s);
 }
 
 cudaError_t launch_lap0(const Lap0Args& a, int border, cudaStream_t s) {
@@ -2025,6 +2049,187 @@ cudaError_t launch_quantize(const float* acc, int64_t plane, int64_t pitch, int 
                             int64_t out_pitch, float* base, int64_t base_pitch, int out16, cudaStream_t s) {
   quantize_kernel<<<(w * h + 255) / 256, 256, 0, s>>>(acc, plane, pitch, w, h, out, out_pitch, base, base_pitch,
                                                       out16);
+  return cudaGetLastError();
+}
+
+// ================================================================ hybrid
+// hybrid-pyramid-contrast (src/stack/pipeline.zig:177-236): the
+// pyramid-contrast image ("soft"), the hardmask-contrast image ("hard": per
+// pixel the colour of the first frame, in order, with the strictly largest
+// weight x alpha support, blend.updateWinners, src/fuse/blend.zig:188-289)
+// and their Laplacian merge (mergeHybridImages, src/fuse/pyramid.zig:271-301).
+
+// Winners over a batch's pass-2 planes (remapped RGBA word and alpha-weighted
+// contrast: the reference's effectiveWeightU8 of the same weight).
+struct WinnersArgs {
+  FramePlanes planes[kMaxBatch];
+  int32_t K, first, w, h;
+  int64_t pitch;
+  float* best;
+  uint32_t* hard;
+};
+
+__global__ void winners_kernel(const __grid_constant__ WinnersArgs a) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (int64_t)a.w * a.h) return;
+  const int64_t o = (i / a.w) * a.pitch + i % a.w;
+  float b = a.first ? -INFINITY : a.best[o];
+  uint32_t hw = a.first ? 0u : a.hard[o];
+  for (int k = 0; k < a.K; ++k) {
+    const float wk = a.planes[k].w[o];
+    if (wk > b) {
+      b = wk;
+      hw = a.planes[k].rgba[o];
+    }
+  }
+  a.best[o] = b;
+  a.hard[o] = hw;
+}
+
+cudaError_t launch_winners(const FramePlanes* planes, int K, float* best, uint32_t* hard, int first, int w, int h,
+                           int64_t pitch, cudaStream_t s) {
+  if (K < 1 || K > kMaxBatch) return cudaErrorInvalidValue;
+  WinnersArgs a;
+  for (int k = 0; k < K; ++k) a.planes[k] = planes[k];
+  a.K = K;
+  a.first = first;
+  a.w = w;
+  a.h = h;
+  a.pitch = pitch;
+  a.best = best;
+  a.hard = hard;
+  const int64_t n = (int64_t)w * h;
+  winners_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+__global__ void rgb_to_planes_kernel(const uint8_t* src, int64_t src_pitch, int px_bytes, float* dst, int64_t plane,
+                                     int64_t pitch, int w, int h) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (int64_t)w * h) return;
+  const int64_t x = i % w, y = i / w;
+  const uint8_t* p = src + y * src_pitch + x * px_bytes;
+  const int64_t o = y * pitch + x;
+#pragma unroll
+  for (int c = 0; c < 3; ++c) dst[c * plane + o] = (float)p[c];
+}
+
+cudaError_t launch_rgb_to_planes(const uint8_t* src, int64_t src_pitch, int px_bytes, float* dst, int64_t plane,
+                                 int64_t pitch, int w, int h, cudaStream_t s) {
+  const int64_t n = (int64_t)w * h;
+  rgb_to_planes_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(src, src_pitch, px_bytes, dst, plane, pitch, w,
+                                                                   h);
+  return cudaGetLastError();
+}
+
+namespace {
+__device__ __forceinline__ int clamp_coord(int c, int limit) { return c <= 0 ? 0 : (c >= limit ? limit - 1 : c); }
+// (a + 4 b + 6 c + 4 d + e) * (1 / 16), left to right, no contraction
+__device__ __forceinline__ float five_tap(float a, float b, float c, float d, float e) {
+  float v = __fadd_rn(a, __fmul_rn(4.0f, b));
+  v = __fadd_rn(v, __fmul_rn(6.0f, c));
+  v = __fadd_rn(v, __fmul_rn(4.0f, d));
+  v = __fadd_rn(v, e);
+  return __fmul_rn(v, 0.0625f);
+}
+}  // namespace
+
+// One output sample per thread: five clamped source rows, each reduced
+// horizontally (horizontalReduceRgbRow), then combined vertically.
+__global__ void reduce_plain_kernel(const float* src, int64_t splane, int64_t spitch, int sw, int sh, float* dst,
+                                    int64_t dplane, int64_t dpitch, int dw, int dh) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (int64_t)dw * dh) return;
+  const int dx = (int)(i % dw), dy = (int)(i / dw);
+  int xs[5];
+#pragma unroll
+  for (int k = 0; k < 5; ++k) xs[k] = clamp_coord(2 * dx + k - 2, sw);
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    const float* pl = src + c * splane;
+    float r[5];
+#pragma unroll
+    for (int ky = 0; ky < 5; ++ky) {
+      const float* row = pl + (int64_t)clamp_coord(2 * dy + ky - 2, sh) * spitch;
+      r[ky] = five_tap(row[xs[0]], row[xs[1]], row[xs[2]], row[xs[3]], row[xs[4]]);
+    }
+    dst[c * dplane + (int64_t)dy * dpitch + dx] = five_tap(r[0], r[1], r[2], r[3], r[4]);
+  }
+}
+
+cudaError_t launch_reduce_plain(const float* src, int64_t splane, int64_t spitch, int sw, int sh, float* dst,
+                                int64_t dplane, int64_t dpitch, int dw, int dh, cudaStream_t s) {
+  const int64_t n = (int64_t)dw * dh;
+  reduce_plain_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(src, splane, spitch, sw, sh, dst, dplane, dpitch,
+                                                                  dw, dh);
+  return cudaGetLastError();
+}
+
+// Laplacians of the soft and hard pyramids at level l (G_l - EXPAND(G_{l+1}),
+// expandRgb in both boundary modes, the operations of collapse_kernel) and
+// the merged level: soft + (hard - soft) * mix inside the hard range, soft
+// elsewhere.
+__global__ void __launch_bounds__(NT) merge_level_kernel(const __grid_constant__ MergeArgs a) {
+  __shared__ float cg[2][3][NH * NW];
+  __shared__ float hrow[2][NH * 3 * TW];
+  const int x0 = blockIdx.x * TW, y0 = blockIdx.y * TH;
+  const int x1 = x0 >> 1, y1 = y0 >> 1;
+  const bool exact = a.exact_expand != 0;
+  for (int i = threadIdx.x; i < NH * NW; i += NT) {
+    const int X = x1 - 1 + i % NW, Y = y1 - 1 + i / NW;
+    const bool in = X >= 0 && Y >= 0 && X < a.wc && Y < a.hc;
+    const int64_t o = (int64_t)Y * a.pitch_c + X;
+    for (int c = 0; c < 3; ++c) {
+      cg[0][c][i] = in ? a.soft_c[c * a.plane_c + o] : 0.0f;
+      cg[1][c][i] = in ? a.hard_c[c * a.plane_c + o] : 0.0f;
+    }
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < NH * TW; i += NT) {
+    const int ii = i / TW, xx = i % TW;
+    const int yi = y1 - 1 + ii;
+    if (yi < 0 || yi >= a.hc) continue;
+    const Taps t = expand_taps(x0 + xx, x1, a.wc, exact);
+    for (int v = 0; v < 2; ++v)
+      for (int c = 0; c < 3; ++c) hrow[v][(ii * 3 + c) * TW + xx] = expand_h1(cg[v][c] + ii * NW, t, exact);
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < TH * TW; i += NT) {
+    const int yy = i / TW, xx = i % TW;
+    const int x = x0 + xx, y = y0 + yy;
+    if (x >= a.wp || y >= a.hp) continue;
+    const int64_t o = (int64_t)y * a.pitch_p + x;
+    const Rows r = expand_rows(y, y1, a.hc, exact);
+    const float div = exact ? exact_expand_divisor(x, y, a.wc, a.hc) : 1.0f;
+    for (int c = 0; c < 3; ++c) {
+      const float ls = __fsub_rn(a.soft_p[c * a.plane_p + o], expand_v1(hrow[0] + c * TW + xx, 3 * TW, r, exact, div));
+      const float lh = __fsub_rn(a.hard_p[c * a.plane_p + o], expand_v1(hrow[1] + c * TW + xx, 3 * TW, r, exact, div));
+      a.acc[c * a.plane_p + o] = a.mixed ? __fadd_rn(ls, __fmul_rn(__fsub_rn(lh, ls), a.mix)) : ls;
+    }
+  }
+}
+
+cudaError_t launch_merge_level(const MergeArgs& a, cudaStream_t s) {
+  dim3 grid((a.wp + TW - 1) / TW, (a.hp + TH - 1) / TH);
+  merge_level_kernel<<<grid, NT, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+__global__ void merge_top_kernel(const float* soft, const float* hard, float* acc, int64_t plane, int64_t pitch, int w,
+                                 int h, int mixed, float mix) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (int64_t)w * h) return;
+  const int64_t o = (i / w) * pitch + i % w;
+  for (int c = 0; c < 3; ++c) {
+    const float sv = soft[c * plane + o], hv = hard[c * plane + o];
+    acc[c * plane + o] = mixed ? __fadd_rn(sv, __fmul_rn(__fsub_rn(hv, sv), mix)) : sv;
+  }
+}
+
+cudaError_t launch_merge_top(const float* soft, const float* hard, float* acc, int64_t plane, int64_t pitch, int w,
+                             int h, int mixed, float mix, cudaStream_t s) {
+  const int64_t n = (int64_t)w * h;
+  merge_top_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(soft, hard, acc, plane, pitch, w, h, mixed, mix);
   return cudaGetLastError();
 }
 

@@ -107,6 +107,10 @@ struct Lap0Args {
   FrameIn f[kMaxBatch];
   float* w[kMaxBatch];         // per frame: its level-0 weight plane
   LevelPlanes g1[kMaxBatch];   // per frame: level-1 Gaussian (storage) and support
+  // hybrid method only (null otherwise): per pixel the largest weight so far
+  // and the RGBA word of the frame that holds it (blend.updateWinners)
+  float* best;
+  uint32_t* hard;
 };
 
 struct CollapseArgs {
@@ -184,6 +188,37 @@ cudaError_t launch_remap16(const RemapArgs& a, cudaStream_t s);
 // 1 x 1 stacks: acc += G0_k * m_k over the batch (a.out planes, a.K frames).
 cudaError_t launch_blend_single_level(float* acc, int64_t acc_plane, const Remap16Args& a, cudaStream_t s);
 cudaError_t launch_lap0(const Lap0Args& a, int border, cudaStream_t s);
+// hybrid-pyramid-contrast (src/stack/pipeline.zig:177-236): winners of the
+// hardmask method over a batch of frames' pass-2 planes (first batch: best
+// weights start at -inf), the plain Laplacian pyramids of the soft and hard
+// images and their merge (src/fuse/pyramid.zig:271-301, 418-488).
+cudaError_t launch_winners(const FramePlanes* planes, int K, float* best, uint32_t* hard, int first, int w, int h,
+                           int64_t pitch, cudaStream_t s);
+// Level 0 of a pyramid: interleaved RGB(A) u8 samples (bytes per pixel 3 or
+// 4) to three f32 planes (fillRgbBase of an image without alpha).
+cudaError_t launch_rgb_to_planes(const uint8_t* src, int64_t src_pitch, int px_bytes, float* dst, int64_t plane,
+                                 int64_t pitch, int w, int h, cudaStream_t s);
+// Plain clamped five-tap REDUCE of three planes (reduceRgbRowsSequential,
+// src/fuse/pyramid.zig:950-995, 1725-1746).
+cudaError_t launch_reduce_plain(const float* src, int64_t splane, int64_t spitch, int sw, int sh, float* dst,
+                                int64_t dplane, int64_t dpitch, int dw, int dh, cudaStream_t s);
+struct MergeArgs {
+  int32_t wp, hp, wc, hc;       // level l and level l + 1 sizes
+  int64_t pitch_p, pitch_c, plane_p, plane_c;
+  int32_t exact_expand;         // max(wp, hp) <= 512
+  int32_t mixed;                // level inside the hard range: soft + (hard - soft) * mix
+  float mix;
+  const float* soft_p;          // Gaussians of the soft / hard images at level l and l + 1
+  const float* hard_p;
+  const float* soft_c;
+  const float* hard_c;
+  float* acc;                   // merged Laplacian of level l (pitch_p, plane_p)
+};
+cudaError_t launch_merge_level(const MergeArgs& a, cudaStream_t s);
+// The top level: the Gaussians themselves, mixed when inside the hard range.
+cudaError_t launch_merge_top(const float* soft, const float* hard, float* acc, int64_t plane, int64_t pitch, int w,
+                             int h, int mixed, float mix, cudaStream_t s);
+
 // acc0 = A_w / N where N > 1e-12, else A_u * inv_count (acc0 written over A_w).
 cudaError_t launch_finalize0(float* acc, const float* au, const float* norm, int64_t plane, int64_t pitch, int w,
                              int h, float inv_count, cudaStream_t s);

@@ -246,6 +246,17 @@ int fs_stack_footprint(const fs_stack_desc* desc, uint64_t available_bytes, int 
 int fs_stack_mode_bytes(const fs_stack_desc* desc, int pass2_mode, int host_frames, uint64_t* bytes);
 int fs_stack_begin_mode(fs_ctx* ctx, const fs_stack_desc* desc, int pass2_mode, fs_stack** out);
 
+/* Fusion method of the stack (Method, src/fuse/config.zig:10-24):
+ * FS_METHOD_PYRAMID_CONTRAST (the default) or
+ * FS_METHOD_HYBRID_PYRAMID_CONTRAST, the pyramid-contrast image merged with
+ * the hardmask-contrast image at pyramid levels 2..5 with weight
+ * hybrid_sharpness in [0, 1] (--hybrid-sharpness, default 0.35): replaces the
+ * hybrid branch of src/stack/pipeline.zig:177-236 (runRemappedSinglePass +
+ * mergeHybridImages, src/fuse/pyramid.zig:271-301).  Call before the first
+ * frame; the hybrid method takes 8-bit samples and no frame shards. */
+enum { FS_METHOD_PYRAMID_CONTRAST = 0, FS_METHOD_HYBRID_PYRAMID_CONTRAST = 1 };
+int fs_stack_set_method(fs_stack* stack, int method, float hybrid_sharpness);
+
 /* Output size of the stack (the ROI). */
 int fs_stack_output_size(const fs_stack* stack, uint32_t* width, uint32_t* height);
 
@@ -268,13 +279,14 @@ int fs_stack_destroy(fs_stack* stack);
  * shards change the order of the FP32 additions, so results match a single
  * stack to rounding, not bit for bit (the remap and the alpha do not
  * change). */
-enum { FS_BUFFER_WEIGHT_SUM = 0, FS_BUFFER_UNION = 1, FS_BUFFER_ACCUMULATOR = 2 };
+enum { FS_BUFFER_WEIGHT_SUM = 0, FS_BUFFER_UNION = 1, FS_BUFFER_ACCUMULATOR = 2, FS_BUFFER_HARD = 3 };
 int fs_stack_set_frame_total(fs_stack* stack, uint32_t frame_total);
 int fs_stack_end_pass1(fs_stack* stack);
 int fs_stack_blend(fs_stack* stack, fs_frame_fetch_cb refetch, void* user);
 int fs_stack_collapse(fs_stack* stack, void* out_pixels, size_t out_stride, int device_out);
 /* Device buffer `which` (level: accumulators only; 0 otherwise), its bytes,
- * row pitch in elements and size. */
+ * row pitch in elements and size.  FS_BUFFER_HARD (hybrid method): per pixel
+ * the RGBA word (R | G << 8 | B << 16 | A << 24) of the hardmask winner. */
 int fs_stack_buffer(fs_stack* stack, int which, uint32_t level, void** ptr, uint64_t* bytes, int64_t* pitch,
                     uint32_t* width, uint32_t* height);
 

@@ -1272,8 +1272,9 @@ void oracle_reduce_scalar_with_support(uint32_t sw, uint32_t sh, const float* sr
   uint32_t dw = nextLevelSize(sw), dh = nextLevelSize(sh);
   reduceWithSupportRows<float, 1>(sw, sh, src, support, dw, dst, dst_support, 0, dh);
 }
-// plain clamped five-tap reduce (reduceRgbRowsSequential, src/fuse/pyramid.zig:950-995),
-// only used by the reference's uniform-image known-answer test.
+// plain clamped five-tap reduce (reduceRgbRowsSequential, src/fuse/pyramid.zig:950-995):
+// the reference's uniform-image known-answer test and the Laplacian pyramids
+// of the hybrid method (buildImageLaplacianPyramid, src/fuse/pyramid.zig:418-488).
 void oracle_reduce_rgb_plain(uint32_t sw, uint32_t sh, const float* src, float* dst) {
   uint32_t dw = nextLevelSize(sw), dh = nextLevelSize(sh);
   std::vector<float> rows(5 * (size_t)dw * 3);
@@ -1391,6 +1392,116 @@ int oracle_stack_fuse(const void* const* sources, size_t count, uint32_t width, 
     ptrs[k] = remapped[k].data();
   }
   return oracle_fuse_aligned(ptrs.data(), count, ow, oh, 1, sample_bits, window, jobs, precision, out_rgb, base_out);
+}
+
+
+// blend.updateWinners (src/fuse/blend.zig:188-289) over n pixels of one image
+// (3 colour channels + extra_channels, u8 or u16): where the weight times the
+// alpha support (effectiveWeightU8/U16: f32(alpha) / 255 or / 65535) is
+// strictly larger than best, it becomes best and the pixel's colour is
+// copied into out (3 samples per pixel).
+void oracle_update_winners(const void* image, size_t n, int extra_channels, int sample_bits, const float* weights,
+                           float* best, void* out) {
+  const size_t st = 3 + (size_t)extra_channels;
+  for (size_t i = 0; i < n; ++i) {
+    float wgt = weights[i];
+    if (extra_channels) {
+      const float al = sample_bits == 8 ? (float)((const uint8_t*)image)[i * st + 3]
+                                        : (float)((const uint16_t*)image)[i * st + 3];
+      wgt = wgt * (al / (sample_bits == 8 ? 255.0f : 65535.0f));
+    }
+    if (wgt <= best[i]) continue;
+    best[i] = wgt;
+    for (int c = 0; c < 3; ++c) {
+      if (sample_bits == 8) ((uint8_t*)out)[i * 3 + c] = ((const uint8_t*)image)[i * st + c];
+      else ((uint16_t*)out)[i * 3 + c] = ((const uint16_t*)image)[i * st + c];
+    }
+  }
+}
+
+// mergeHybridImages (src/fuse/pyramid.zig:271-301) of two interleaved RGB
+// images (u8 or u16): Laplacian pyramids by buildImageLaplacianPyramid
+// (src/fuse/pyramid.zig:418-488: plain clamped REDUCE, expandRgb), levels
+// [hard_start, hard_start + hard_count) mixed as soft + (hard - soft) * mix,
+// the others soft's, collapsed and quantised (base_out: the collapsed base).
+void oracle_hybrid_merge(const void* soft, const void* hard, uint32_t ow, uint32_t oh, int sample_bits,
+                         uint32_t hard_start, uint32_t hard_count, float mix, int jobs, void* out_rgb,
+                         double* base_out) {
+  const size_t n = (size_t)ow * oh;
+  const size_t L = computeLevelCount(ow, oh);
+  auto laplacians = [&](const void* img) {
+    std::vector<Level<float>> g(L);
+    g[0].w = ow;
+    g[0].h = oh;
+    g[0].px.resize(n * 3);
+    for (size_t i = 0; i < n * 3; ++i)
+      g[0].px[i] = sample_bits == 8 ? (float)((const uint8_t*)img)[i] : (float)((const uint16_t*)img)[i];
+    for (size_t l = 1; l < L; ++l) {
+      g[l].w = nextLevelSize(g[l - 1].w);
+      g[l].h = nextLevelSize(g[l - 1].h);
+      g[l].px.resize((size_t)g[l].w * g[l].h * 3);
+      oracle_reduce_rgb_plain(g[l - 1].w, g[l - 1].h, g[l - 1].px.data(), g[l].px.data());
+    }
+    for (size_t l = 0; l + 1 < L; ++l) {
+      std::vector<float> ex(g[l].px.size());
+      expandRgb<float>(g[l].w, g[l].h, g[l + 1].w, g[l + 1].h, g[l + 1].px.data(), ex.data(), jobs);
+      for (size_t i = 0; i < ex.size(); ++i) g[l].px[i] = g[l].px[i] - ex[i];
+    }
+    return g;
+  };
+  std::vector<Level<float>> ls = laplacians(soft), lh = laplacians(hard);
+  Pyramid<float> P;
+  P.init(ow, oh);
+  const size_t hs = std::min<size_t>(hard_start, L), he = std::min<size_t>(hs + hard_count, L);
+  for (size_t l = 0; l < L; ++l) {
+    auto& dst = P.acc[l].px;
+    for (size_t i = 0; i < dst.size(); ++i)
+      dst[i] = (l >= hs && l < he) ? ls[l].px[i] + (lh[l].px[i] - ls[l].px[i]) * mix : ls[l].px[i];
+  }
+  std::vector<float> b(n * 3);
+  collapse<float>(P, sample_bits, out_rgb, b.data(), jobs);
+  if (base_out) for (size_t i = 0; i < n * 3; ++i) base_out[i] = b[i];
+}
+
+// hybrid-pyramid-contrast, stack path (src/stack/pipeline.zig:177-236): the
+// pyramid-contrast output ("soft"), the hardmask-contrast output ("hard":
+// runRemappedSinglePass with blend.updateWinners, src/stack/pipeline.zig:
+// 245-310, src/fuse/blend.zig:188-289 -- per pixel the colour of the first
+// frame, in order, whose weight x alpha/max is largest; best weights start at
+// -inf) and mergeHybridImages (src/fuse/pyramid.zig:271-301): Laplacian
+// pyramids of both images (plain clamped REDUCE, expandRgb), levels
+// [hard_start, hard_start + hard_count) mixed as soft + (hard - soft) * mix,
+// the others soft's, collapsed and quantised.  hard_out (optional) receives
+// the hard image.
+int oracle_stack_fuse_hybrid(const void* const* sources, size_t count, uint32_t width, uint32_t height,
+                             int sample_bits, const or_pose* poses, const int32_t* roi4, uint32_t window, int jobs,
+                             uint32_t hard_start, uint32_t hard_count, float mix, void* out_rgb, double* base_out,
+                             void* hard_out) {
+  if (count == 0) return -1;
+  Rect roi = roi4 ? Rect{roi4[0], roi4[1], roi4[2], roi4[3]} : Rect{0, 0, (int32_t)width, (int32_t)height};
+  const uint32_t ow = (uint32_t)(roi.right - roi.left), oh = (uint32_t)(roi.bottom - roi.top);
+  const size_t n = (size_t)ow * oh, bps = sample_bits == 8 ? 1 : 2;
+  std::vector<uint8_t> soft(n * 3 * bps), hard(n * 3 * bps, 0);
+  int rc = oracle_stack_fuse(sources, count, width, height, sample_bits, poses, roi4, window, jobs, 32, soft.data(),
+                             nullptr);
+  if (rc != 0) return rc;
+  std::vector<float> best(n, -INFINITY);
+  std::vector<uint8_t> remapped(n * 4 * bps);
+  std::vector<float> gray, sup, w;
+  for (size_t k = 0; k < count; ++k) {
+    oracle_remap(sources[k], width, height, 3, sample_bits, &poses[k], roi4, jobs, remapped.data());
+    Frame im{remapped.data(), ow, oh, 3, 1, sample_bits};
+    // computeWeightMapForRemapped: the contrast weights before applySupport
+    gray.resize(n); sup.resize(n); w.resize(n);
+    fillAverageFromLoaded(gray.data(), im);
+    fillBinarySupport(im, sup.data());
+    computeLocalContrastWeights(gray.data(), ow, oh, sup.data(), window, jobs, w.data());
+    oracle_update_winners(remapped.data(), n, 1, sample_bits, w.data(), best.data(), hard.data());
+  }
+  if (hard_out) std::memcpy(hard_out, hard.data(), hard.size());
+  oracle_hybrid_merge(soft.data(), hard.data(), ow, oh, sample_bits, hard_start, hard_count, mix, jobs, out_rgb,
+                      base_out);
+  return 0;
 }
 
 }  // extern "C"

@@ -117,6 +117,13 @@ def _bind(L):
     L.oracle_fuse_aligned.restype = i32
     L.oracle_stack_fuse.argtypes = [P(vp), sz, u32, u32, i32, P(_Pose), P(ctypes.c_int32), u32, i32, i32, vp, dp]
     L.oracle_stack_fuse.restype = i32
+    L.oracle_update_winners.argtypes = [vp, sz, i32, i32, fp, fp, vp]
+    L.oracle_update_winners.restype = None
+    L.oracle_stack_fuse_hybrid.argtypes = [P(vp), sz, u32, u32, i32, P(_Pose), P(ctypes.c_int32), u32, i32, u32, u32,
+                                           ctypes.c_float, vp, dp, vp]
+    L.oracle_stack_fuse_hybrid.restype = i32
+    L.oracle_hybrid_merge.argtypes = [vp, vp, u32, u32, i32, u32, u32, ctypes.c_float, i32, vp, dp]
+    L.oracle_hybrid_merge.restype = None
     L.oracle_synth_pose.argtypes = [ctypes.c_uint64, i32, u32, u32, u32, u32, P(_Pose)]
     L.oracle_synth_render.argtypes = [ctypes.c_uint64, i32, u32, u32, u32, u32, u32, u32, vp, sz, i32]
 
@@ -267,6 +274,60 @@ def stack_fuse(sources, poses, roi=None, window=5, jobs=1, precision=32, want_ba
     if rc != 0:
         raise RuntimeError("oracle_stack_fuse failed")
     return (out, base) if want_base else out
+
+
+def update_winners(image: np.ndarray, weights: np.ndarray, best: np.ndarray, out: np.ndarray):
+    """blend.updateWinners on one image (HxWx3 or HxWx4, uint8/uint16):
+    best (float32) and out (HxWx3) are updated in place."""
+    image = np.ascontiguousarray(image)
+    weights = np.ascontiguousarray(weights, np.float32)
+    assert best.dtype == np.float32 and best.flags.c_contiguous and out.flags.c_contiguous
+    h, w, c = image.shape
+    lib().oracle_update_winners(_ptr(image), h * w, c - 3, 8 if image.dtype == np.uint8 else 16,
+                                _ptr(weights, ctypes.c_float), _ptr(best, ctypes.c_float), _ptr(out))
+
+
+HYBRID_HARD_LEVEL_START, HYBRID_HARD_LEVEL_COUNT, HYBRID_SHARPNESS = 2, 4, 0.35
+
+
+def stack_fuse_hybrid(sources, poses, roi=None, window=5, jobs=1, mix=HYBRID_SHARPNESS,
+                      hard_start=HYBRID_HARD_LEVEL_START, hard_count=HYBRID_HARD_LEVEL_COUNT, want_base=False,
+                      want_hard=False):
+    """hybrid-pyramid-contrast of a stack (src/stack/pipeline.zig:177-236)."""
+    sources = [np.ascontiguousarray(s) for s in sources]
+    h, w = sources[0].shape[:2]
+    bits = 8 if sources[0].dtype == np.uint8 else 16
+    if roi is None:
+        roi = (0, 0, w, h)
+    ow, oh = roi[2] - roi[0], roi[3] - roi[1]
+    ptrs = (ctypes.c_void_p * len(sources))(*[s.ctypes.data for s in sources])
+    out = np.zeros((oh, ow, 3), sources[0].dtype)
+    base = np.zeros((oh, ow, 3), np.float64)
+    hard = np.zeros((oh, ow, 3), sources[0].dtype)
+    r = np.asarray(roi, np.int32)
+    rc = lib().oracle_stack_fuse_hybrid(ptrs, len(sources), w, h, bits, pose_array(poses), _ptr(r, ctypes.c_int32),
+                                        window, jobs, hard_start, hard_count, mix, _ptr(out),
+                                        _ptr(base, ctypes.c_double), _ptr(hard))
+    if rc != 0:
+        raise RuntimeError("oracle_stack_fuse_hybrid failed")
+    res = [out]
+    if want_base:
+        res.append(base)
+    if want_hard:
+        res.append(hard)
+    return tuple(res) if len(res) > 1 else out
+
+
+def hybrid_merge(soft: np.ndarray, hard: np.ndarray, mix=HYBRID_SHARPNESS, hard_start=HYBRID_HARD_LEVEL_START,
+                 hard_count=HYBRID_HARD_LEVEL_COUNT, jobs=1):
+    """mergeHybridImages of two HxWx3 images; returns (image, base)."""
+    soft, hard = np.ascontiguousarray(soft), np.ascontiguousarray(hard)
+    h, w = soft.shape[:2]
+    out = np.zeros_like(soft)
+    base = np.zeros((h, w, 3), np.float64)
+    lib().oracle_hybrid_merge(_ptr(soft), _ptr(hard), w, h, 8 if soft.dtype == np.uint8 else 16, hard_start,
+                              hard_count, mix, jobs, _ptr(out), _ptr(base, ctypes.c_double))
+    return out, base
 
 
 # ------------------------------------------------------ synthetic stacks

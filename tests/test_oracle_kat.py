@@ -128,3 +128,34 @@ def test_contrast_depends_on_partition_only_by_rounding():
     w1 = oracle.weight_map(img, 5, jobs=1)
     w4 = oracle.weight_map(img, 5, jobs=4)
     assert np.allclose(w1, w4, rtol=1e-5, atol=1e-7)
+
+
+def test_update_winners_prefers_higher_weight():
+    # src/fuse/blend.zig:316-349
+    best = np.full(2, -np.inf, np.float32)
+    out = np.zeros((1, 2, 3), np.uint8)
+    image = np.array([[[1, 2, 3], [4, 5, 6]]], np.uint8)
+    oracle.update_winners(image, np.array([[0.1, 0.2]], np.float32), best, out)
+    assert out.ravel().tolist() == [1, 2, 3, 4, 5, 6]
+
+
+def test_update_winners_discounts_low_support_alpha():
+    # src/fuse/blend.zig:351-401
+    best = np.full(1, -np.inf, np.float32)
+    out = np.zeros((1, 1, 3), np.uint8)
+    oracle.update_winners(np.array([[[200, 10, 10, 32]]], np.uint8), np.array([[1.0]], np.float32), best, out)
+    oracle.update_winners(np.array([[[10, 200, 10, 255]]], np.uint8), np.array([[0.2]], np.float32), best, out)
+    assert out.ravel().tolist() == [10, 200, 10]
+
+
+def test_hybrid_with_zero_mix_is_the_pyramid_output_reconstructed():
+    # mergeHybridImages with hard_mix 0 collapses soft's own Laplacian
+    # pyramid, which reconstructs the quantised soft image (u8 within 1)
+    rng = np.random.default_rng(4)
+    frames = [np.clip(rng.normal(128, 40, (48, 64, 3)), 0, 255).astype(np.uint8) for _ in range(3)]
+    poses = [{}] * 3
+    soft = oracle.stack_fuse(frames, poses)
+    out, hard = oracle.stack_fuse_hybrid(frames, poses, mix=0.0, want_hard=True)
+    assert np.abs(out.astype(int) - soft.astype(int)).max() <= 1
+    # the hard image takes every pixel from one of the frames
+    assert all(any((hard[y, x] == f[y, x]).all() for f in frames) for y in range(0, 48, 7) for x in range(0, 64, 9))
