@@ -198,11 +198,11 @@ def algorithmic_bytes(roi_w, roi_h, frames, k, mode="cache", storage_bytes=4):
         # (the first batch only writes); A_u touches the window border only
         b["pass1"] = frames * (3 * A[0] + 4 * A[0] + (3 * s + 1) * l1) + batches * 34 * A[0] - 17 * A[0]
         # levels >= 1 of each frame's image pyramid: read G_l + support,
-        # write the Laplacian (12 B) and G_{l+1} + support (the top one f32)
+        # write the Laplacian (3s B) and G_{l+1} + support (the top one f32)
         img = 0
         for l in range(1, L - 1):
             nxt = (3 * s + 1) * A[l + 1] if l + 2 < L else 12 * A[l + 1]
-            img += (3 * s + 1) * A[l] + 12 * A[l] + nxt
+            img += (3 * s + 1) * A[l] + 3 * s * A[l] + nxt
         b["image"] = frames * img
         # finalize: A_w (12) and the weight sum (4) read, acc0 (12) written
         b["blend0"] = 28 * A[0]
@@ -211,13 +211,14 @@ def algorithmic_bytes(roi_w, roi_h, frames, k, mode="cache", storage_bytes=4):
         b["level0"] = frames * (4 * A[0] + (s if L > 2 else 4) * l1) + 5 * A[0]
         # levels >= 1: mask REDUCE (mask read, next mask written; the top one
         # in f32; support once) and the blend of each level over all frames
-        # (Laplacian 12 B and mask read per frame, accumulator 12 B written)
+        # (Laplacian 3s B (the top Gaussian 12 B) and mask read per frame,
+        # accumulator 12 B written)
         lv = 0
         for l in range(1, L):
             ms = s if l + 1 < L else 4
             if l + 1 < L:
                 lv += frames * (ms * A[l] + (s if l + 2 < L else 4) * A[l + 1]) + A[l]
-            lv += frames * (12 + ms) * A[l] + 12 * A[l]
+            lv += frames * ((3 * ms) + ms) * A[l] + 12 * A[l]
         b["level"] = lv
     return b, sum(b.values())
 

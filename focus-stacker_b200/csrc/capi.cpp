@@ -206,7 +206,7 @@ struct fs_stack {
   float* best = nullptr;                       // hybrid: per pixel the winning weight
   uint32_t* hard = nullptr;                    // hybrid: per pixel the winning frame's RGBA word
   std::vector<float*> wplane;                  // LAPS: per frame, its weight (level 0)
-  std::vector<std::vector<float*>> lap;        // LAPS: per frame, Laplacian of levels 1 .. L-2 ([0] unused)
+  std::vector<std::vector<void*>> lap;         // LAPS: per frame, Laplacian of levels 1 .. L-2 (storage; [0] unused)
   float* au = nullptr;                         // LAPS: sum of level-0 Laplacians where the weight sum <= 1e-12
   std::vector<float*> gtop;                    // LAPS: per frame, Gaussian of the top level
   std::vector<std::vector<void*>> mplane;      // LAPS: per frame, mask of levels 1 .. L-2 (storage type)
@@ -817,7 +817,7 @@ StackPlan plan_stack(const fs_stack_desc& d) {
   }
   if (p.L >= 3 && bps == 1) {
     p.laps_frame = n0 * 4;
-    for (uint32_t l = 1; l + 1 < p.L; ++l) p.laps_frame += (size_t)p.pitch[l] * p.lh[l] * 12;
+    for (uint32_t l = 1; l + 1 < p.L; ++l) p.laps_frame += (size_t)p.pitch[l] * p.lh[l] * 3 * esz;
     p.laps_frame += (size_t)p.pitch[p.L - 1] * p.lh[p.L - 1] * 12;  // top Gaussian
     for (uint32_t l = 1; l + 1 < p.L; ++l) p.laps_frame += (size_t)p.pitch[l] * p.lh[l] * esz;  // masks
     p.laps_frame += (size_t)p.pitch[p.L - 1] * p.lh[p.L - 1] * 4;  // top mask
@@ -940,10 +940,10 @@ static int begin_impl(fs_ctx* ctx, const fs_stack_desc* desc, fs_stack** out, in
       uint8_t* q = (uint8_t*)p;
       s->wplane.push_back((float*)q);
       q += n0 * 4;
-      std::vector<float*> lv(1, nullptr);  // level 0 is blended by the fused pass-1 kernel
+      std::vector<void*> lv(1, nullptr);  // level 0 is blended by the fused pass-1 kernel
       for (uint32_t l = 1; l + 1 < s->L; ++l) {
-        lv.push_back((float*)q);
-        q += (size_t)s->pitch[l] * s->lh[l] * 12;
+        lv.push_back(q);
+        q += (size_t)s->pitch[l] * s->lh[l] * 3 * esz;
       }
       s->lap.push_back(lv);
       s->gtop.push_back((float*)q);
@@ -959,7 +959,7 @@ static int begin_impl(fs_ctx* ctx, const fs_stack_desc* desc, fs_stack** out, in
     // per level: Laplacian (top: Gaussian) then mask (level 0: weight) of every frame
     for (uint32_t l = 0; l < s->L; ++l) {
       for (uint32_t f = 0; f < d.frame_count; ++f)
-        s->tab_host.push_back(l + 1 < s->L ? s->lap[f][l] : s->gtop[f]);
+        s->tab_host.push_back(l + 1 < s->L ? (const float*)s->lap[f][l] : s->gtop[f]);
       for (uint32_t f = 0; f < d.frame_count; ++f)
         s->tab_host.push_back(l == 0 ? s->wplane[f] : l + 1 < s->L ? (const float*)s->mplane[f][l] : s->mtop[f]);
     }
@@ -1171,7 +1171,7 @@ static int pass2_impl(fs_stack* s, fs_frame_fetch_cb refetch, void* user) {
     }
     // the blend of levels 1 .. L-1 over every frame (top: Gaussian x mask)
     for (uint32_t l = 1; l < s->L; ++l) {
-      const float* const* lap = s->tab + (size_t)l * 2 * N;
+      const void* const* lap = (const void* const*)(s->tab + (size_t)l * 2 * N);
       const void* const* msk = (const void* const*)(s->tab + (size_t)l * 2 * N + N);
       const int storage = l + 1 < s->L ? s->storage : FS_STORAGE_F32;
       e = timed(ctx, "level", [&] {

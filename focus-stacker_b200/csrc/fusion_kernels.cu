@@ -645,9 +645,9 @@ __device__ void store_next(const LevelSmem& S, const LevelArgs& a, int x0, int y
 // acc += (G_l - EXPAND(G_{l+1})) * M_l  (src/fuse/pyramid.zig:1480-1504).
 // LAP: store the Laplacian G_l - EXPAND(G_{l+1}) of the tile into lap (3
 // planes of acc_plane_l floats, level pitch) instead of blending it.
-template <bool LAP = false, class SM = LevelSmem>
+template <bool LAP = false, class SM = LevelSmem, typename TL = float>
 __device__ void expand_blend_step(SM& S, const LevelArgs& a, int x0, int y0, float (&acc)[PPT][3],
-                                  float* lap_out = nullptr) {
+                                  TL* lap_out = nullptr) {
   const int x1 = x0 >> 1, y1 = y0 >> 1;
   float* hrow = S.tmp;  // [NH][3][TW]
   const bool exact = a.exact_expand != 0;
@@ -728,7 +728,7 @@ __device__ void expand_blend_step(SM& S, const LevelArgs& a, int x0, int y0, flo
         e = __fmul_rn(__fadd_rn(hv[c][j + 1], hv[c][j + 1]), 0.5f);
       }
       const float lap = __fsub_rn(gv[c], e);
-      if (LAP) lap_out[c * a.acc_plane_l + (int64_t)y * a.pitch_l + x] = lap;
+      if (LAP) stv<TL>(lap_out, c * a.acc_plane_l + (int64_t)y * a.pitch_l + x, lap);
       else acc[i][c] = __fadd_rn(acc[i][c], __fmul_rn(lap, m));
     }
   }
@@ -1015,13 +1015,13 @@ __global__ void __launch_bounds__(NT) img_kernel(const __grid_constant__ LevelAr
   reduce_image_step(S, a, x0, y0);
   store_next_image<T>(S, a, x0, y0, k);
   float unused[PPT][3];
-  expand_blend_step<true>(S, a, x0, y0, unused, a.lap[k]);
+  expand_blend_step<true, ImgSmem, T>(S, a, x0, y0, unused, (T*)a.lap[k]);
 }
 
 // Blend of one level over all frames in order, one pixel per thread (the
 // products and sums of the per-batch kernels, from acc = 0).
 template <typename T>
-__global__ void blend_kernel(float* acc, int64_t plane, int64_t pitch, int w, int h, const float* const* lap,
+__global__ void blend_kernel(float* acc, int64_t plane, int64_t pitch, int w, int h, const void* const* lap,
                              const void* const* mask, int frames) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= (int64_t)w * h) return;
@@ -1033,10 +1033,10 @@ __global__ void blend_kernel(float* acc, int64_t plane, int64_t pitch, int w, in
 #pragma unroll
     for (int u = 0; u < U; ++u) {
       if (k0 + u < frames) {
-        const float* lk = lap[k0 + u];
-        l0[u] = __ldg(lk + o);
-        l1[u] = __ldg(lk + plane + o);
-        l2[u] = __ldg(lk + 2 * plane + o);
+        const T* lk = (const T*)lap[k0 + u];
+        l0[u] = ldv<T>(lk, o);
+        l1[u] = ldv<T>(lk, plane + o);
+        l2[u] = ldv<T>(lk, 2 * plane + o);
         mv[u] = ldv<T>((const T*)mask[k0 + u], o);
       }
     }
@@ -1054,7 +1054,7 @@ __global__ void blend_kernel(float* acc, int64_t plane, int64_t pitch, int w, in
   acc[2 * plane + o] = a2;
 }
 
-cudaError_t launch_blend(float* acc, int64_t plane, int64_t pitch, int w, int h, const float* const* lap,
+cudaError_t launch_blend(float* acc, int64_t plane, int64_t pitch, int w, int h, const void* const* lap,
                          const void* const* mask, int frames, int storage, cudaStream_t s) {
   const int64_t n = (int64_t)w * h;
   const unsigned blocks = (unsigned)((n + 255) / 256);
@@ -1103,6 +1103,19 @@ __device__ __forceinline__ void ld2(const T* p, float* v) {
     const T* h = reinterpret_cast<const T*>(&q);
     v[0] = ldv<T>(h, 0);
     v[1] = ldv<T>(h, 1);
+  }
+}
+
+// Four consecutive samples, one vector store (16 bytes of f32, 8 of f16/bf16).
+template <typename T>
+__device__ __forceinline__ void st4(T* p, const float* v) {
+  if constexpr (std::is_same<T, float>::value) {
+    *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
+  } else {
+    T h[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) stv<T>(h, u, v[u]);
+    *reinterpret_cast<uint2*>(p) = *reinterpret_cast<const uint2*>(h);
   }
 }
 
@@ -1457,7 +1470,7 @@ __global__ void __launch_bounds__(32 * kImgWarps) img_stream_kernel(const __grid
         const LevelPlanes& in = a.in[k];
 #pragma unroll
         for (int ch = 0; ch < 3; ++ch) ld4<T>((const T*)in.g + ch * in.plane + ro + c, gv[ch]);
-        float* lp = a.lap[k] + ro + c;
+        T* lp = (T*)a.lap[k] + ro + c;
 #pragma unroll
         for (int ch = 0; ch < 3; ++ch) {
           float lv[4];
@@ -1468,13 +1481,13 @@ __global__ void __launch_bounds__(32 * kImgWarps) img_stream_kernel(const __grid
                 : __fmul_rn(__fadd_rn(Hm1[ch][u], Hm1[ch][u]), 0.5f);
             lv[u] = __fsub_rn(gv[ch][u], e);
           }
-          float* lc = lp + ch * a.acc_plane_l;
+          T* lc = lp + ch * a.acc_plane_l;
           if (c + 3 < a.wl) {
-            *reinterpret_cast<float4*>(lc) = make_float4(lv[0], lv[1], lv[2], lv[3]);
+            st4<T>(lc, lv);
           } else {
 #pragma unroll
             for (int u = 0; u < 4; ++u)
-              if (c + u < a.wl) lc[u] = lv[u];
+              if (c + u < a.wl) stv<T>(lc, u, lv[u]);
           }
         }
       }

@@ -80,10 +80,10 @@ struct LevelArgs {
   int32_t frame_parallel;
   float* contrib;
   float* contrib_top;
-  // split pyramid (launch_img_level): frame k's
-  // Laplacian planes at level l (3 planes of acc_plane_l floats) and its top
+  // split pyramid (launch_img_level): frame k's Laplacian planes at level l
+  // (3 planes of acc_plane_l samples in the level storage type) and its top
   // Gaussian (3 planes of acc_plane_n floats, written when l + 1 is the top)
-  float* lap[kMaxBatch];
+  void* lap[kMaxBatch];
   float* gtop[kMaxBatch];
 };
 
@@ -231,8 +231,8 @@ cudaError_t launch_collapse(const CollapseArgs& a, cudaStream_t s);
 // lap[k] (level 0 is part of the fused pass-1 kernel, launch_lap0).
 cudaError_t launch_img_level(const LevelArgs& a, int storage, cudaStream_t s);
 // acc = sum over frames k, in order, of lap[k] (3 planes of `plane`) times
-// mask[k] (storage T: 0 f32, 1 f16, 2 bf16), written over acc.
-cudaError_t launch_blend(float* acc, int64_t plane, int64_t pitch, int w, int h, const float* const* lap,
+// mask[k] (both in storage T: 0 f32, 1 f16, 2 bf16), written over acc.
+cudaError_t launch_blend(float* acc, int64_t plane, int64_t pitch, int w, int h, const void* const* lap,
                          const void* const* mask, int frames, int storage, cudaStream_t s);
 // acc[c] += contrib[k][c] for k = 0 .. K-1 in order (w x h level, plane stride `plane`).
 cudaError_t launch_sum_contrib(float* acc, int64_t plane, int64_t pitch, int w, int h, const float* contrib, int K,
