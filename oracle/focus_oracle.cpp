@@ -1504,4 +1504,55 @@ int oracle_stack_fuse_hybrid(const void* const* sources, size_t count, uint32_t 
   return 0;
 }
 
+
+// The pass-2 stages of one frame and the collapse, over an accumulator
+// pyramid held by the caller (levels 0 .. L-1 of interleaved RGB f32,
+// concatenated): accumulateImage (src/fuse/pyramid.zig:190-204, the mask and
+// image pyramids of the frame and the weighted blend) and
+// collapseToImageWithJobs (src/fuse/pyramid.zig:223-269).  They let a test
+// split a stack over several processes the way the library's phase entry
+// points do.
+size_t oracle_pyramid_floats(uint32_t width, uint32_t height) {
+  size_t n = 0;
+  for (size_t l = 0, L = computeLevelCount(width, height); l < L; ++l) {
+    n += (size_t)width * height * 3;
+    width = nextLevelSize(width);
+    height = nextLevelSize(height);
+  }
+  return n;
+}
+
+static void load_acc(Pyramid<float>& P, const float* acc) {
+  size_t off = 0;
+  for (auto& lv : P.acc) {
+    std::copy(acc + off, acc + off + lv.px.size(), lv.px.begin());
+    off += lv.px.size();
+  }
+}
+
+void oracle_pyramid_accumulate(const void* frame, uint32_t width, uint32_t height, int extra_channels,
+                               int sample_bits, const float* normalized_mask, const float* union_support, float* acc,
+                               int jobs) {
+  Pyramid<float> P;
+  P.init(width, height);
+  load_acc(P, acc);
+  accumulateImage<float>(Frame{frame, width, height, 3, extra_channels, sample_bits}, normalized_mask, union_support,
+                         P, jobs);
+  size_t off = 0;
+  for (auto& lv : P.acc) {
+    std::copy(lv.px.begin(), lv.px.end(), acc + off);
+    off += lv.px.size();
+  }
+}
+
+void oracle_pyramid_collapse(const float* acc, uint32_t width, uint32_t height, int sample_bits, void* out_rgb,
+                             double* base_out, int jobs) {
+  Pyramid<float> P;
+  P.init(width, height);
+  load_acc(P, acc);
+  std::vector<float> b((size_t)width * height * 3);
+  collapse<float>(P, sample_bits, out_rgb, b.data(), jobs);
+  if (base_out) for (size_t i = 0; i < b.size(); ++i) base_out[i] = b[i];
+}
+
 }  // extern "C"

@@ -124,6 +124,12 @@ def _bind(L):
     L.oracle_stack_fuse_hybrid.restype = i32
     L.oracle_hybrid_merge.argtypes = [vp, vp, u32, u32, i32, u32, u32, ctypes.c_float, i32, vp, dp]
     L.oracle_hybrid_merge.restype = None
+    L.oracle_pyramid_floats.argtypes = [u32, u32]
+    L.oracle_pyramid_floats.restype = sz
+    L.oracle_pyramid_accumulate.argtypes = [vp, u32, u32, i32, i32, fp, fp, fp, i32]
+    L.oracle_pyramid_accumulate.restype = None
+    L.oracle_pyramid_collapse.argtypes = [fp, u32, u32, i32, vp, dp, i32]
+    L.oracle_pyramid_collapse.restype = None
     L.oracle_synth_pose.argtypes = [ctypes.c_uint64, i32, u32, u32, u32, u32, P(_Pose)]
     L.oracle_synth_render.argtypes = [ctypes.c_uint64, i32, u32, u32, u32, u32, u32, u32, vp, sz, i32]
 
@@ -327,6 +333,33 @@ def hybrid_merge(soft: np.ndarray, hard: np.ndarray, mix=HYBRID_SHARPNESS, hard_
     base = np.zeros((h, w, 3), np.float64)
     lib().oracle_hybrid_merge(_ptr(soft), _ptr(hard), w, h, 8 if soft.dtype == np.uint8 else 16, hard_start,
                               hard_count, mix, jobs, _ptr(out), _ptr(base, ctypes.c_double))
+    return out, base
+
+
+def pyramid_floats(width, height) -> int:
+    """Floats of an accumulator pyramid (all levels, interleaved RGB)."""
+    return int(lib().oracle_pyramid_floats(width, height))
+
+
+def pyramid_accumulate(frame: np.ndarray, normalized_mask: np.ndarray, union_support: np.ndarray, acc: np.ndarray,
+                       jobs=1):
+    """Pass 2 of one aligned frame (HxWx3/4) into acc (float32, in place)."""
+    frame = np.ascontiguousarray(frame)
+    h, w, c = frame.shape
+    m = np.ascontiguousarray(normalized_mask, np.float32)
+    u = np.ascontiguousarray(union_support, np.float32)
+    assert acc.dtype == np.float32 and acc.flags.c_contiguous and acc.size == pyramid_floats(w, h)
+    lib().oracle_pyramid_accumulate(_ptr(frame), w, h, c - 3, 8 if frame.dtype == np.uint8 else 16,
+                                    _ptr(m, ctypes.c_float), _ptr(u, ctypes.c_float), _ptr(acc, ctypes.c_float), jobs)
+
+
+def pyramid_collapse(acc: np.ndarray, width, height, sample_bits=8, jobs=1):
+    """Collapse and quantise an accumulator pyramid; returns (image, base)."""
+    acc = np.ascontiguousarray(acc, np.float32)
+    out = np.zeros((height, width, 3), np.uint8 if sample_bits == 8 else np.uint16)
+    base = np.zeros((height, width, 3), np.float64)
+    lib().oracle_pyramid_collapse(_ptr(acc, ctypes.c_float), width, height, sample_bits, _ptr(out),
+                                  _ptr(base, ctypes.c_double), jobs)
     return out, base
 
 

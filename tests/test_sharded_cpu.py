@@ -1,7 +1,11 @@
 """Frame-sharded orchestration (fuse_sharded) on world_size 2 over gloo, on
-CPU: a stand-in stack with the library's phase interface (pass-1 weight sum
-and union, pass-2 accumulators normalised by the global weight sum, collapse)
-must give, split over two ranks, what one stack over all frames gives."""
+CPU.  Each rank holds an oracle-backed stack with the library's phase
+interface: pass 1 gives the shard's weight sum and union (the oracle's
+weight maps), pass 2 blends the shard's frames into an FP32 accumulator
+pyramid with masks normalised by the weight sum of the whole stack (the
+oracle's accumulateImage), and the root collapses the summed pyramids.  Split
+over two ranks, the fused image must be the oracle's fusion of all frames in
+one stack, to the rounding that the changed order of FP32 sums allows."""
 import os
 import socket
 
@@ -12,55 +16,67 @@ import torch
 import torch.distributed as dist
 import torch.multiprocessing as mp
 
+import oracle
 from __graft_entry__ import load_package
 
 fsb = load_package()
 
-W, H, P, F = 13, 9, 16, 7  # valid width, height, pitch, frames
+W, H, F = 96, 64, 7  # aligned frame size, frames
 
 
-def frame(k):
-    rng = np.random.default_rng(100 + k)
-    img = rng.uniform(0, 255, (H, W)).astype(np.float32)
-    w = rng.uniform(0, 1, (H, W)).astype(np.float32) * (rng.uniform(0, 1, (H, W)) > 0.2)
-    return img, w.astype(np.float32)
+def aligned_frames():
+    """Aligned RGBA frames: the oracle's remap of a small synthetic stack."""
+    poses = [oracle.synth_pose(5, oracle.SCENE_SMALL, 120, 90, k, F) for k in range(F)]
+    frames = [oracle.synth_frame(5, oracle.SCENE_SMALL, 120, 90, k, F) for k in range(F)]
+    return [oracle.remap(f, p, (10, 12, 10 + W, 12 + H)) for f, p in zip(frames, poses)]
 
 
-class FakeStack:
-    """Phase interface of PyramidContrastStack over CPU tensors: the weight
-    sum and union of its frames, acc = sum_k img_k * w_k / global weight sum
-    (1/N where it is 0), collapse = rounded acc."""
+class OracleShardStack:
+    """The phase interface of PyramidContrastStack (end_pass1, buffer, blend,
+    collapse) over the oracle's stages, for a shard of a stack's frames."""
 
     def __init__(self, frames):
         self.frames = frames
         self.out_width, self.out_height = W, H
-        self.norm = torch.zeros((H, P), dtype=torch.float32)
-        self.uni = torch.zeros((H, P), dtype=torch.uint8)
-        self.acc = [torch.zeros((3, H, P), dtype=torch.float32) for _ in range(fsb.sharded.level_count(W, H))]
         self.total = len(frames)
+        self.norm = torch.zeros((H, W), dtype=torch.float32)
+        self.uni = torch.zeros((H, W), dtype=torch.uint8)
+        self.acc = torch.zeros(oracle.pyramid_floats(W, H), dtype=torch.float32)
+        self.weights = []
+        self.levels = []
+        w, h, off = W, H, 0
+        for _ in range(fsb.sharded.level_count(W, H)):
+            self.levels.append(self.acc[off:off + w * h * 3])
+            off += w * h * 3
+            w, h = oracle.next_level_size(w), oracle.next_level_size(h)
 
     def set_frame_total(self, n):
         self.total = n
 
     def end_pass1(self):
-        for _, w in self.frames:
-            self.norm[:, :W] += torch.from_numpy(w)
-            self.uni[:, :W] = torch.maximum(self.uni[:, :W], torch.from_numpy((w > 0).astype(np.uint8)))
+        for f in self.frames:
+            w = oracle.weight_map(f)
+            self.weights.append(w)
+            self.norm += torch.from_numpy(w)
+            self.uni = torch.maximum(self.uni, torch.from_numpy((f[..., 3] > 0).astype(np.uint8)))
 
     def buffer(self, which, level=0):
-        return {fsb.BUFFER_WEIGHT_SUM: self.norm, fsb.BUFFER_UNION: self.uni}.get(which, self.acc[level])
+        if which == fsb.BUFFER_WEIGHT_SUM:
+            return self.norm
+        if which == fsb.BUFFER_UNION:
+            return self.uni
+        return self.levels[level]
 
     def blend(self):
-        nv = self.norm[:, :W]
-        for img, w in self.frames:
-            m = torch.where(nv > 1e-12, torch.from_numpy(w) / nv, torch.full_like(nv, 1.0 / self.total))
-            for c in range(3):
-                self.acc[0][c, :, :W] += torch.from_numpy(img) * m * self.uni[:, :W]
-        for lvl in range(1, len(self.acc)):
-            self.acc[lvl][:, 0, 0] += float(len(self.frames))  # frame count summed over shards
+        norm = self.norm.numpy()
+        uni = self.uni.numpy().astype(np.float32)
+        acc = self.acc.numpy()  # shares memory with the tensor the collectives use
+        for f, w in zip(self.frames, self.weights):
+            m = oracle.normalize_weights(w, norm, self.total)
+            oracle.pyramid_accumulate(f, m, uni, acc)
 
     def collapse(self):
-        return np.rint(self.acc[0][:, :, :W].numpy()), self.acc[-1][:, 0, 0].numpy().copy()
+        return oracle.pyramid_collapse(self.acc.numpy(), W, H)
 
 
 def _worker(rank, world, port, q):
@@ -68,7 +84,7 @@ def _worker(rank, world, port, q):
     os.environ["MASTER_PORT"] = str(port)
     dist.init_process_group("gloo", rank=rank, world_size=world)
     b, e = fsb.sharded.shard_range(F, world, rank)
-    st = FakeStack([frame(k) for k in range(b, e)])
+    st = OracleShardStack(aligned_frames()[b:e])
     out = fsb.sharded.fuse_sharded(st, F, dist, as_tensor=lambda x: x)
     q.put((rank, out))
     dist.barrier()
@@ -91,11 +107,19 @@ def test_shard_ranges_cover_the_stack():
             assert max(sizes) - min(sizes) <= 1
 
 
+def test_oracle_shard_stack_alone_is_the_oracle_fusion():
+    frames = aligned_frames()
+    st = OracleShardStack(frames)
+    st.end_pass1()
+    st.blend()
+    out, base = st.collapse()
+    ref, ref_base = oracle.fuse_aligned(frames, want_base=True)
+    assert np.array_equal(out, ref) and np.array_equal(base, ref_base)
+
+
 def test_two_ranks_match_one_stack():
-    single = FakeStack([frame(k) for k in range(F)])
-    single.end_pass1()
-    single.blend()
-    want, want_count = single.collapse()
+    frames = aligned_frames()
+    want, want_base = oracle.fuse_aligned(frames, want_base=True)
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     port = _free_port()
@@ -107,6 +131,6 @@ def test_two_ranks_match_one_stack():
         p.join(timeout=60)
         assert p.exitcode == 0
     assert got[1] is None
-    out, count = got[0]
-    assert np.abs(out - want).max() <= 1e-3
-    assert np.array_equal(count, want_count)  # every shard's contribution reached the root
+    out, base = got[0]
+    assert np.abs(base - want_base).max() <= 1e-3
+    assert np.abs(out.astype(np.int16) - want.astype(np.int16)).max() <= 1
