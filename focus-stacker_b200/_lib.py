@@ -32,6 +32,7 @@ EXPORTED = (
     "fs_batch_create", "fs_batch_run", "fs_batch_stack_count", "fs_batch_pass2_mode", "fs_batch_uses_graph",
     "fs_batch_destroy",
     "fs_fuse_aligned_device_static", "fs_synth_frame_device", "fs_synth_pose",
+    "fs_jpeg_info", "fs_decode_jpeg", "fs_stack_add_frame_jpeg",
 )
 
 
@@ -140,3 +141,6 @@ def _bind(L):
     L.fs_batch_destroy.argtypes = [vp]
     L.fs_synth_frame_device.argtypes = [ctx, u64, i32, u32, u32, u32, u32, vp, sz, P(FsPose)]
     L.fs_synth_pose.argtypes = [u64, i32, u32, u32, u32, u32, P(FsPose)]
+    L.fs_jpeg_info.argtypes = [vp, sz, P(u32), P(u32)]
+    L.fs_decode_jpeg.argtypes = [ctx, vp, sz, vp, sz, i32]
+    L.fs_stack_add_frame_jpeg.argtypes = [vp, vp, sz, P(FsPose)]

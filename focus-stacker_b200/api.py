@@ -280,6 +280,31 @@ def remap_rigid_image_device(ctx: Context, src, src_stride: int, width: int, hei
     _check(rc, ctx.handle)
 
 
+# ----------------------------------------------------------------------- JPEG
+def jpeg_info(data: bytes):
+    """(width, height) of a JPEG file the device decoder takes; raises
+    FocusCudaError(FS_ERR_UNSUPPORTED) for other files."""
+    w, h = ctypes.c_uint32(), ctypes.c_uint32()
+    buf = ctypes.create_string_buffer(bytes(data), len(data))
+    _check(L().fs_jpeg_info(buf, len(data), ctypes.byref(w), ctypes.byref(h)))
+    return w.value, h.value
+
+
+def decode_jpeg(ctx: Context, data: bytes) -> np.ndarray:
+    """Decode a JPEG file on the device (libjpeg's default output: islow IDCT,
+    fancy upsampling); returns HxWx3 uint8."""
+    w, h = jpeg_info(data)
+    out = np.zeros((h, w, 3), np.uint8)
+    buf = ctypes.create_string_buffer(bytes(data), len(data))
+    _check(L().fs_decode_jpeg(ctx.handle, buf, len(data), out.ctypes.data, out.strides[0], 0), ctx.handle)
+    return out
+
+
+def decode_jpeg_device(ctx: Context, data: bytes, dst, dst_stride: int):
+    buf = ctypes.create_string_buffer(bytes(data), len(data))
+    _check(L().fs_decode_jpeg(ctx.handle, buf, len(data), _ptr(dst), dst_stride, 1), ctx.handle)
+
+
 # --------------------------------------------------------------------- fusion
 PASS2_MODES = ("cache", "resident", "refetch", "laps")
 # fs_stack_set_method: the fusion methods the stack runs on the device, and
@@ -407,6 +432,14 @@ class PyramidContrastStack:
         p = _pose(pose).to_c() if pose is not None else None
         rc = L().fs_stack_add_frame_async(self.handle, pixels.ctypes.data, pixels.strides[0],
                                           ctypes.byref(p) if p is not None else None)
+        _check(rc, self.ctx.handle)
+
+    def add_frame_jpeg(self, data: bytes, pose=None):
+        """A frame given as a JPEG file, decoded on the device
+        (fs_stack_add_frame_jpeg)."""
+        p = _pose(pose).to_c() if pose is not None else None
+        buf = ctypes.create_string_buffer(bytes(data), len(data))
+        rc = L().fs_stack_add_frame_jpeg(self.handle, buf, len(data), ctypes.byref(p) if p is not None else None)
         _check(rc, self.ctx.handle)
 
     def add_frame_device(self, buf, row_stride: int, pose=None):

@@ -23,6 +23,7 @@
 #include "fs_common.h"
 #include "fs_host.h"
 #include "fusion_kernels.cuh"
+#include "jpeg.h"
 
 using namespace fs;
 
@@ -58,6 +59,21 @@ struct fs_ctx {
   // so that a later fs_stack_destroy of a stack that outlived its context
   // only frees the host record.
   std::set<fs_stack*> stacks;
+  // JPEG decoding workspace, grown to the largest file decoded so far: the
+  // parsed tables, the unstuffed entropy-coded bytes and interval bounds,
+  // coefficients, component planes and the decode status flag.
+  struct JpegWork {
+    void* tables = nullptr;
+    uint8_t* data = nullptr;
+    size_t data_cap = 0;
+    uint32_t* seg = nullptr;
+    size_t seg_cap = 0;
+    int16_t* coef = nullptr;
+    size_t coef_cap = 0;
+    uint8_t* planes = nullptr;
+    size_t planes_cap = 0;
+    int* status = nullptr;
+  } jpeg;
 };
 
 namespace {
@@ -456,6 +472,105 @@ int run_pending_pass1(fs_stack* s, bool flush) {
   return FS_OK;
 }
 
+// ------------------------------------------------------------------- JPEG
+void jpeg_release(fs_ctx* ctx) {
+  fs_ctx::JpegWork& j = ctx->jpeg;
+  dev_free(ctx, j.tables, sizeof(jpeg::Tables));
+  dev_free(ctx, j.data, j.data_cap);
+  dev_free(ctx, j.seg, j.seg_cap * 8);
+  dev_free(ctx, j.coef, j.coef_cap * 2);
+  dev_free(ctx, j.planes, j.planes_cap);
+  dev_free(ctx, j.status, 16);
+  j = fs_ctx::JpegWork();
+}
+
+// Grow a workspace buffer to `need` (elements of `esz` bytes), ordered on the
+// context's stream.
+template <typename T>
+int jpeg_grow(fs_ctx* ctx, T** buf, size_t* cap, size_t need, size_t esz) {
+  if (*buf && *cap >= need) return FS_OK;
+  dev_free(ctx, *buf, *cap * esz);
+  *buf = nullptr;
+  *cap = 0;
+  void* p;
+  const int rc = dev_alloc(ctx, need * esz, &p);
+  if (rc != FS_OK) return rc;
+  *buf = (T*)p;
+  *cap = need;
+  return FS_OK;
+}
+
+// Decode a JPEG file into device RGB u8 (row pitch in bytes), queued on the
+// context's stream.  expect_w / expect_h != 0: the file must have that size.
+// The host buffer may be reused once this returns.
+int jpeg_decode(fs_ctx* ctx, const void* data, size_t len, uint8_t* d_dst, int64_t dst_pitch, uint32_t expect_w,
+                uint32_t expect_h) {
+  jpeg::Parsed P;
+  std::string why;
+  if (!jpeg::parse((const uint8_t*)data, len, &P, &why)) return set_err(ctx, FS_ERR_UNSUPPORTED, "JPEG: " + why);
+  if (expect_w && (P.width != expect_w || P.height != expect_h))
+    return set_err(ctx, FS_ERR_MISMATCH, "JPEG frame size differs from the stack's");
+  fs_ctx::JpegWork& j = ctx->jpeg;
+  int rc;
+  if (!j.tables) {
+    if ((rc = dev_alloc(ctx, sizeof(jpeg::Tables), &j.tables)) != FS_OK) return rc;
+    void* p;
+    if ((rc = dev_alloc(ctx, 16, &p)) != FS_OK) return rc;
+    j.status = (int*)p;
+    if (cudaMemsetAsync(j.status, 0, sizeof(int), ctx->stream) != cudaSuccess)
+      return cuda_err(ctx, cudaGetLastError(), "JPEG status");
+  }
+  const size_t ncoef = jpeg::coef_count(P.t);
+  if ((rc = jpeg_grow(ctx, &j.coef, &j.coef_cap, ncoef, 2)) != FS_OK) return rc;
+  if ((rc = jpeg_grow(ctx, &j.planes, &j.planes_cap, ncoef, 1)) != FS_OK) return rc;  // one sample per coefficient
+  cudaStream_t st = ctx->stream;
+  cudaError_t e = cudaMemcpyAsync(j.tables, &P.t, sizeof(jpeg::Tables), cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(j.coef, 0, ncoef * 2, st);
+  if (e != cudaSuccess) return cuda_err(ctx, e, "JPEG upload");
+  const int nseg = (int)P.seg_begin.size();
+  if (nseg > 1) {
+    // restart intervals: entropy decoding on the GPU, one thread per interval
+    if ((rc = jpeg_grow(ctx, &j.data, &j.data_cap, std::max<size_t>(P.data.size(), 16), 1)) != FS_OK) return rc;
+    if ((rc = jpeg_grow(ctx, &j.seg, &j.seg_cap, (size_t)nseg, 8)) != FS_OK) return rc;
+    std::vector<uint32_t> seg(P.seg_begin);
+    seg.insert(seg.end(), P.seg_end.begin(), P.seg_end.end());
+    e = cudaMemcpyAsync(j.data, P.data.data(), P.data.size(), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(j.seg, seg.data(), seg.size() * 4, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess)
+      e = timed(ctx, "jpeg", [&] {
+        return jpeg::launch_entropy((const jpeg::Tables*)j.tables, j.data, j.seg, j.seg + nseg, nseg, j.coef, j.status,
+                                    st);
+      });
+    if (e != cudaSuccess) return cuda_err(ctx, e, "JPEG entropy decoding");
+  } else {
+    // one interval: a sequential bitstream, decoded on the host
+    std::vector<int16_t> coef(ncoef, 0);
+    if (!jpeg::decode_interval(P.t, P.data.data(), 0, (uint32_t)P.data.size(), 0,
+                               (int64_t)P.t.mcus_x * P.t.mcus_y, coef.data()))
+      return set_err(ctx, FS_ERR_INVALID, "JPEG: corrupt entropy-coded data");
+    e = cudaMemcpyAsync(j.coef, coef.data(), ncoef * 2, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);  // `coef` goes out of scope
+    if (e != cudaSuccess) return cuda_err(ctx, e, "JPEG coefficient upload");
+  }
+  e = timed(ctx, "jpeg", [&] {
+    return jpeg::launch_idct_color((const jpeg::Tables*)j.tables, P.t, j.coef, j.planes, P.width, P.height, d_dst,
+                                   dst_pitch, st);
+  });
+  if (e != cudaSuccess) return cuda_err(ctx, e, "JPEG inverse DCT / colour");
+  return FS_OK;
+}
+
+// Read and clear the JPEG status flag (waits for the stream).
+int jpeg_status(fs_ctx* ctx) {
+  if (!ctx->jpeg.status) return FS_OK;
+  int v = 0;
+  cudaError_t e = cudaMemcpyAsync(&v, ctx->jpeg.status, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(ctx->jpeg.status, 0, sizeof(int), ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  if (e != cudaSuccess) return cuda_err(ctx, e, "JPEG status");
+  return v ? set_err(ctx, FS_ERR_INVALID, "JPEG: corrupt entropy-coded data") : FS_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -520,6 +635,7 @@ void fs_destroy(fs_ctx* ctx) {
   cudaStreamSynchronize(ctx->copy);
   for (fs_stack* s : ctx->stacks) detach_stack(s);
   ctx->stacks.clear();
+  jpeg_release(ctx);
   pool_trim(ctx);
   for (auto& t : ctx->timings) {
     cudaEventDestroy(t.start);
@@ -1071,6 +1187,92 @@ static int add_frame_impl(fs_stack* s, const void* pixels, size_t row_stride, co
   return run_pending_pass1(s, s->frames.size() == s->d.frame_count);
 }
 
+int fs_jpeg_info(const void* data, size_t len, uint32_t* width, uint32_t* height) {
+  if (!data || !width || !height) return FS_ERR_INVALID;
+  jpeg::Parsed P;
+  std::string why;
+  if (!jpeg::parse((const uint8_t*)data, len, &P, &why)) return FS_ERR_UNSUPPORTED;
+  *width = P.width;
+  *height = P.height;
+  return FS_OK;
+}
+
+int fs_decode_jpeg(fs_ctx* ctx, const void* data, size_t len, void* dst, size_t dst_stride, int device_dst) {
+  if (!ctx || !data || !dst) return set_err(ctx, FS_ERR_INVALID, "null argument");
+  uint32_t w = 0, h = 0;
+  if (fs_jpeg_info(data, len, &w, &h) != FS_OK) {
+    jpeg::Parsed P;
+    std::string why;
+    jpeg::parse((const uint8_t*)data, len, &P, &why);
+    return set_err(ctx, FS_ERR_UNSUPPORTED, "JPEG: " + why);
+  }
+  if (dst_stride < (size_t)w * 3) return set_err(ctx, FS_ERR_INVALID, "output stride too small");
+  cudaSetDevice(ctx->device);
+  void* ddst = dst;
+  const size_t bytes = (size_t)w * 3 * h;
+  if (!device_dst) {
+    int rc = dev_alloc(ctx, bytes, &ddst);
+    if (rc != FS_OK) return rc;
+  }
+  int rc = jpeg_decode(ctx, data, len, (uint8_t*)ddst, device_dst ? (int64_t)dst_stride : (int64_t)w * 3, 0, 0);
+  if (rc == FS_OK && !device_dst) {
+    cudaError_t e = cudaMemcpy2DAsync(dst, dst_stride, ddst, (size_t)w * 3, (size_t)w * 3, h, cudaMemcpyDeviceToHost,
+                                      ctx->stream);
+    if (e != cudaSuccess) rc = cuda_err(ctx, e, "JPEG output copy");
+  }
+  const int st = jpeg_status(ctx);  // waits for the stream
+  if (!device_dst) dev_free(ctx, ddst, bytes);
+  return rc != FS_OK ? rc : st;
+}
+
+// A JPEG frame of the stack: decoded on the device into the frame's staging
+// (or resident) buffer, then pass 1 as for fs_stack_add_frame.
+int fs_stack_add_frame_jpeg(fs_stack* s, const void* data, size_t len, const fs_pose* pose) {
+  if (!s || !data) return FS_ERR_INVALID;
+  if (!s->ctx) return FS_ERR_STATE;
+  fs_ctx* ctx = s->ctx;
+  if (s->finished) return set_err(ctx, FS_ERR_STATE, "stack already finished");
+  if (s->frames.size() >= s->d.frame_count) return set_err(ctx, FS_ERR_STATE, "more frames than frame_count");
+  if (!s->aligned && !pose) return set_err(ctx, FS_ERR_INVALID, "pose required for source frames");
+  if (s->bps != 1 || s->d.channels != 3) return set_err(ctx, FS_ERR_MISMATCH, "JPEG frames are 8-bit RGB");
+  cudaSetDevice(ctx->device);
+  fs_stack::Frame fr;
+  if (pose) fr.pose = *pose; else fs_pose_default(&fr.pose);
+  uint8_t* buf = nullptr;
+  if (s->mode == P2_RESIDENT) {
+    void* p;
+    int rc = stack_alloc(s, s->frame_bytes, &p);
+    if (rc != FS_OK) return rc;
+    buf = (uint8_t*)p;
+    fr.owned = true;
+  } else {
+    const size_t nslots = 2 * (size_t)s->K;
+    const size_t slot = s->frames.size() % nslots;
+    while (s->staging.size() <= slot) {
+      void* p;
+      int rc = stack_alloc(s, s->frame_bytes, &p, ctx->copy);
+      if (rc != FS_OK) return rc;
+      s->staging.push_back((uint8_t*)p);
+      cudaEvent_t ev;
+      cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+      s->slot_done.push_back(ev);
+    }
+    // the buffer's allocation (and any raw upload into it) is ordered on the
+    // copy stream: the decode on the compute stream waits for it
+    cudaEventRecord(s->copy_done, ctx->copy);
+    cudaStreamWaitEvent(ctx->stream, s->copy_done, 0);
+    buf = s->staging[slot];
+    fr.resident = false;
+    fr.slot = (int)slot;
+  }
+  int rc = jpeg_decode(ctx, data, len, buf, s->frame_pitch, s->d.src_width, s->d.src_height);
+  if (rc != FS_OK) return rc;
+  fr.px = buf;
+  fr.pitch = s->frame_pitch;
+  s->frames.push_back(fr);
+  return run_pending_pass1(s, s->frames.size() == s->d.frame_count);
+}
+
 int fs_stack_add_frame(fs_stack* stack, const void* pixels, size_t row_stride, const fs_pose* pose) {
   return add_frame_impl(stack, pixels, row_stride, pose, false);
 }
@@ -1108,6 +1310,7 @@ static int finish_impl(fs_stack* s, fs_frame_fetch_cb refetch, void* user, void*
     s->phase = 2;
   }
   if ((rc = collapse_impl(s, out, out_stride, device_out, wait)) != FS_OK) return rc;
+  if (wait && (rc = jpeg_status(ctx)) != FS_OK) return rc;  // a corrupt JPEG frame of this stack
   if (mark_done) {
     cudaError_t e = s->done ? cudaSuccess : cudaEventCreateWithFlags(&s->done, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventRecord(s->done, ctx->stream);

@@ -152,6 +152,18 @@ int fs_remap_frame16_device(fs_ctx* ctx, const void* src, size_t src_stride, uin
                             uint32_t channels, const fs_pose* pose, const fs_rect* roi, void* dst,
                             size_t dst_stride);
 
+/* ---------------------------------------------------------------- JPEG */
+
+/* Size of a JPEG file the decoder takes (FS_ERR_UNSUPPORTED otherwise: a
+ * progressive, arithmetic-coded, 12-bit, grayscale or otherwise subsampled
+ * file).  Host only. */
+int fs_jpeg_info(const void* data, size_t len, uint32_t* width, uint32_t* height);
+
+/* Decode a JPEG file to interleaved RGB u8 (device_dst != 0: dst is device
+ * memory), the image libjpeg's default decompression gives (image_io.loadImage,
+ * src/image_io.zig:160-173).  Returns when the image is in dst. */
+int fs_decode_jpeg(fs_ctx* ctx, const void* data, size_t len, void* dst, size_t dst_stride, int device_dst);
+
 /* ------------------------------------------------------- fusion (stacks) */
 
 typedef struct fs_stack_desc {
@@ -184,6 +196,16 @@ int fs_stack_add_frame(fs_stack* stack, const void* pixels, size_t row_stride, c
  * buffer (best pinned) must stay valid and unchanged until fs_stack_finish
  * or fs_stack_wait has returned. */
 int fs_stack_add_frame_async(fs_stack* stack, const void* pixels, size_t row_stride, const fs_pose* pose);
+
+/* A frame given as a JPEG file (baseline sequential Huffman, 8-bit YCbCr at
+ * 4:4:4, 4:2:2 or 4:2:0): decoded on the device into the stack's frame buffer
+ * and run through pass 1.  Replaces image_io.loadImage of a JPEG frame
+ * (src/image_io.zig:160-173) before remapRigidImage: the pixels are those
+ * libjpeg gives with its default settings (islow IDCT, fancy upsampling).
+ * Files with restart markers are entropy-decoded on the GPU (one thread per
+ * restart interval), others on the host.  The file buffer may be reused when
+ * the call returns.  A corrupt stream is reported by fs_stack_finish. */
+int fs_stack_add_frame_jpeg(fs_stack* stack, const void* data, size_t len, const fs_pose* pose);
 
 /* Same with a device pointer; the buffer must stay valid and unchanged until
  * fs_stack_finish returns (pass 2 reads it again). */
