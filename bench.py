@@ -154,9 +154,10 @@ def algorithmic_bytes(roi_w, roi_h, frames, k, mode="cache", storage_bytes=4):
     the remapped frame (RGBA, 4 B) and its weight (4 B) for pass 2; "recompute":
     pass 2 remaps again into per-batch slots; "laps": pass 1 also builds the
     Gaussian/Laplacian pyramids ("image") and pass 2 only the masks and the
-    blend, with level 0 fused into pass 1 (remap, weights, level-1 REDUCE,
-    Laplacian x weight summed over frames; pass 2 divides that sum by the
-    weight sum).  Returns {kernel: bytes per step} and the pipeline total."""
+    blend; "fused": the same with level 0 fused into pass 1 (remap, weights,
+    level-1 REDUCE, Laplacian x weight summed over frames; pass 2 divides that
+    sum by the weight sum).  Returns {kernel: bytes per step} and the
+    pipeline total."""
     sz = level_sizes(roi_w, roi_h)
     A = [w * h for w, h in sz]
     L = len(sz)
@@ -168,7 +169,7 @@ def algorithmic_bytes(roi_w, roi_h, frames, k, mode="cache", storage_bytes=4):
     # read+write per batch (the first batch only writes)
     b["pass1"] = frames * (3 + keep) * A[0] + batches * 10 * A[0] - 5 * A[0]
     # pass-2 re-remap (recompute mode): frame 3 B/px read, planes 8 B/px written
-    b["remap_weights"] = 0 if mode in ("cache", "laps") else frames * 11 * A[0]
+    b["remap_weights"] = frames * 11 * A[0] if mode == "recompute" else 0
     # level 0: planes 8 B/px read; level-1 Gaussian/mask (4 s B) + support (1 B)
     # written at 1/4 area; weight sum 4 + union 1 read and accumulator 24
     # read+write per batch
@@ -191,24 +192,37 @@ def algorithmic_bytes(roi_w, roi_h, frames, k, mode="cache", storage_bytes=4):
     b["collapse"] = col
     b["image"] = 0
     b["blend0"] = 0
-    if mode == "laps":
-        # fused pass 1: frame 3 B/px read, weight (4 B) and level-1 Gaussian
-        # + support (3s + 1 B at 1/4 area) written per frame; weight sum f32,
-        # union u8 and the level-0 sum A_w (3 x f32) read + written per batch
-        # (the first batch only writes); A_u touches the window border only
-        b["pass1"] = frames * (3 * A[0] + 4 * A[0] + (3 * s + 1) * l1) + batches * 34 * A[0] - 17 * A[0]
+    if mode in ("laps", "fused"):
         # levels >= 1 of each frame's image pyramid: read G_l + support,
         # write the Laplacian (3s B) and G_{l+1} + support (the top one f32)
         img = 0
         for l in range(1, L - 1):
             nxt = (3 * s + 1) * A[l + 1] if l + 2 < L else 12 * A[l + 1]
             img += (3 * s + 1) * A[l] + 3 * s * A[l] + nxt
+        if mode == "laps":
+            # level 0 of the image pyramid: RGBA read, the f32 Laplacian
+            # (12 B) and the level-1 Gaussian + support written
+            img += 4 * A[0] + 12 * A[0] + (3 * s + 1) * l1
+            # blend0: Laplacian 12 B + weight 4 B read and mask 4 B written
+            # per frame; weight sum read, accumulator written once
+            b["blend0"] = frames * 20 * A[0] + 16 * A[0]
+            # level 0: mask REDUCE of every frame (mask 4 B read, level-1 mask
+            # written in the storage type) and the union support read once
+            b["level0"] = frames * (4 * A[0] + (s if L > 2 else 4) * l1) + A[0]
+        else:
+            # fused pass 1: frame 3 B/px read, weight (4 B) and level-1
+            # Gaussian + support (3s + 1 B at 1/4 area) written per frame;
+            # weight sum f32, union u8 and the level-0 sum A_w (3 x f32) read
+            # + written per batch (the first batch only writes); A_u touches
+            # the window border only
+            b["pass1"] = frames * (3 * A[0] + 4 * A[0] + (3 * s + 1) * l1) + batches * 34 * A[0] - 17 * A[0]
+            # finalize: A_w (12) and the weight sum (4) read, acc0 (12) written
+            b["blend0"] = 28 * A[0]
+            # level 0: mask REDUCE of every frame from its weight and the
+            # weight sum (w 4 B per frame, N and the union once), level-1
+            # mask written
+            b["level0"] = frames * (4 * A[0] + (s if L > 2 else 4) * l1) + 5 * A[0]
         b["image"] = frames * img
-        # finalize: A_w (12) and the weight sum (4) read, acc0 (12) written
-        b["blend0"] = 28 * A[0]
-        # level 0: mask REDUCE of every frame from its weight and the weight
-        # sum (w 4 B per frame, N and the union once), level-1 mask written
-        b["level0"] = frames * (4 * A[0] + (s if L > 2 else 4) * l1) + 5 * A[0]
         # levels >= 1: mask REDUCE (mask read, next mask written; the top one
         # in f32; support once) and the blend of each level over all frames
         # (Laplacian 3s B (the top Gaussian 12 B) and mask read per frame,
@@ -610,7 +624,7 @@ def main():
     k_default = 8 if args.batch == 0 else args.batch
     k_eff = max(1, min(k_default, 8, F))
     alg, alg_total = algorithmic_bytes(roi.width, roi.height, F, k_eff,
-                                       mode_used["mode"] if mode_used["mode"] in ("cache", "laps") else "recompute")
+                                       mode_used["mode"] if mode_used["mode"] in ("cache", "laps", "fused") else "recompute")
     dom = max(stats, key=lambda n: stats[n][1])
     n_dom, ms_dom = stats[dom]
     peak, peak_kind = measured_hbm_peak()

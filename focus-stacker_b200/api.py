@@ -306,7 +306,7 @@ def decode_jpeg_device(ctx: Context, data: bytes, dst, dst_stride: int):
 
 
 # --------------------------------------------------------------------- fusion
-PASS2_MODES = ("cache", "resident", "refetch", "laps")
+PASS2_MODES = ("cache", "resident", "refetch", "laps", "fused")
 # fs_stack_set_method: the fusion methods the stack runs on the device, and
 # the default weight of the hard image's levels (--hybrid-sharpness,
 # src/fuse/pyramid.zig:11)
@@ -379,7 +379,7 @@ class PyramidContrastStack:
                  level_storage: int = 0, pass2_mode: Optional[str] = None, sample_bits: int = 8,
                  method: str = "pyramid-contrast", hybrid_sharpness: float = HYBRID_SHARPNESS):
         """pass2_mode: None picks the mode from the context's budget; "cache",
-        "resident", "refetch" or "laps" imposes one.  sample_bits 16: uint16
+        "resident", "refetch", "laps" or "fused" imposes one.  sample_bits 16: uint16
         frames in and a uint16 image out (FP32 levels; resident / refetch)."""
         self.ctx = ctx
         d = stack_desc(src_width, src_height, frame_count, roi, channels, contrast_window, aligned, frames_per_batch,

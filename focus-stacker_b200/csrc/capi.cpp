@@ -188,15 +188,18 @@ int64_t round_up(int64_t v, int64_t m) { return (v + m - 1) / m * m; }
 //  REFETCH   frames are only staged; pass 2 asks the caller for them again
 //            and remaps them (src/stack/pipeline.zig:561-597).
 //  LAPS      pass 1 also builds each frame's Gaussian/Laplacian pyramid (it
-//            does not depend on the weight sum): one fused kernel remaps,
-//            weights, reduces to level 1 and blends level 0 as A_w += lap0 * w
-//            (divided by the weight sum once it is complete), and the levels
-//            above keep their Laplacians and the frame its weight; pass 2 is
-//            then only the mask pyramid and the blend of levels >= 1.  Level 0
-//            rounds in another order than the batch modes (within a few ulp of
-//            the accumulator); the levels above give the same bytes.  It moves
-//            most of pass 2 into pass 1, which overlaps the frame uploads.
-enum Pass2Mode { P2_CACHE = 0, P2_RESIDENT = 1, P2_REFETCH = 2, P2_LAPS = 3 };
+//            does not depend on the weight sum) and keeps its Laplacians and
+//            weight; pass 2 is then only the mask pyramid and the blend.  Same
+//            operations, so the same bytes as the other modes; it moves most
+//            of pass 2 into pass 1, which overlaps the frame uploads.
+//  FUSED     the split pyramid with level 0 fused into pass 1: one kernel
+//            remaps, weights, reduces to level 1 and sums lap0 * w over the
+//            frames (divided by the weight sum once it is complete), so no
+//            level-0 Laplacian or remapped frame is kept: 9-10 bytes per
+//            frame-pixel instead of LAPS's 21.  Level 0 rounds in another
+//            order (within a few ulp of the accumulator).  The mode for
+//            stacks whose LAPS planes do not fit.
+enum Pass2Mode { P2_CACHE = 0, P2_RESIDENT = 1, P2_REFETCH = 2, P2_LAPS = 3, P2_FUSED = 4 };
 
 struct fs_stack {
   fs_ctx* ctx = nullptr;
@@ -214,20 +217,21 @@ struct fs_stack {
   std::vector<float*> acc;     // per level, 3 planes
   std::vector<std::vector<LevelPlanes>> slot;  // [k][l], l = 1 .. L-2
   std::vector<FramePlanes> cache;              // CACHE: per frame
-  std::vector<FramePlanes> p2;                 // RESIDENT / REFETCH: per batch slot (K)
+  std::vector<FramePlanes> p2;                 // RESIDENT / REFETCH / LAPS: per batch slot (K)
   std::vector<LevelPlanes> slot0;              // 16-bit frames: level-0 planes per batch slot (K)
   uint32_t bps = 1;                            // bytes per sample (1: u8, 2: u16)
   int method = FS_METHOD_PYRAMID_CONTRAST;     // fs_stack_set_method
   float hybrid_mix = 0.35f;                    // hybrid: weight of the hard image's levels
   float* best = nullptr;                       // hybrid: per pixel the winning weight
   uint32_t* hard = nullptr;                    // hybrid: per pixel the winning frame's RGBA word
-  std::vector<float*> wplane;                  // LAPS: per frame, its weight (level 0)
-  std::vector<std::vector<void*>> lap;         // LAPS: per frame, Laplacian of levels 1 .. L-2 (storage; [0] unused)
-  float* au = nullptr;                         // LAPS: sum of level-0 Laplacians where the weight sum <= 1e-12
-  std::vector<float*> gtop;                    // LAPS: per frame, Gaussian of the top level
-  std::vector<std::vector<void*>> mplane;      // LAPS: per frame, mask of levels 1 .. L-2 (storage type)
-  std::vector<float*> mtop;                    // LAPS: per frame, mask of the top level (f32)
-  std::vector<const float*> tab_host;          // LAPS: per level, Laplacian then mask pointers of all frames
+  std::vector<float*> wplane;                  // LAPS / FUSED: per frame, its weight (level 0)
+  std::vector<std::vector<void*>> lap;         // LAPS / FUSED: per frame, Laplacian of levels 0 .. L-2 (level 0:
+                                               // f32, LAPS only; above: the storage type)
+  float* au = nullptr;                         // FUSED: sum of level-0 Laplacians where the weight sum <= 1e-12
+  std::vector<float*> gtop;                    // LAPS / FUSED: per frame, Gaussian of the top level
+  std::vector<std::vector<void*>> mplane;      // LAPS / FUSED: per frame, mask of levels 1 .. L-2 (storage type)
+  std::vector<float*> mtop;                    // LAPS / FUSED: per frame, mask of the top level (f32)
+  std::vector<const float*> tab_host;          // LAPS / FUSED: per level, Laplacian then mask pointers of all frames
   const float** tab = nullptr;                 // the same table on the device
   uint8_t* out_dev = nullptr;
   std::vector<Alloc> allocs;
@@ -323,6 +327,7 @@ int launch_remap_weights_batch(fs_stack* s, const std::vector<fs_stack::Frame>& 
     if (!build_frame_in(s, frames[k], &a.f[k - begin], &why)) return set_err(s->ctx, FS_ERR_INVALID, why);
     if (pass1) {
       if (s->mode == P2_CACHE) a.out[k - begin] = s->cache[k];
+      if (s->mode == P2_LAPS) a.out[k - begin] = FramePlanes{s->p2[k - begin].rgba, s->wplane[k]};
     } else {
       a.out[k - begin] = s->p2[k - begin];
     }
@@ -389,7 +394,7 @@ int launch_remap16_batch(fs_stack* s, const std::vector<fs_stack::Frame>& frames
   return FS_OK;
 }
 
-// LAPS pass 1, level 0 of frames [begin, end): remap, weights (weight sum
+// FUSED pass 1, level 0 of frames [begin, end): remap, weights (weight sum
 // and union), level-1 Gaussian into the batch slots, A_w += lap0 * w.
 int launch_lap0_batch(fs_stack* s, size_t begin, size_t end) {
   Lap0Args a;
@@ -423,17 +428,19 @@ int launch_lap0_batch(fs_stack* s, size_t begin, size_t end) {
   return FS_OK;
 }
 
-// LAPS pass 1: the Gaussian / Laplacian pyramid of levels >= 1 of frames
-// [begin, end) from their level-1 Gaussians in the batch slots.
+// LAPS / FUSED pass 1: the Gaussian / Laplacian pyramid of frames [begin,
+// end), one frame per CTA, from their remapped RGBA in the batch slots (LAPS,
+// from level 0) or their level-1 Gaussians (FUSED, from level 1).
 int launch_image_pyramid(fs_stack* s, size_t begin, size_t end) {
   LevelArgs a;
   std::memset(&a, 0, sizeof(a));
   a.levels = (int32_t)s->L;
   a.K = (int32_t)(end - begin);
-  for (uint32_t l = 1; l + 1 < s->L; ++l) {
+  for (uint32_t l = s->mode == P2_FUSED ? 1 : 0; l + 1 < s->L; ++l) {
     level_geometry(s, l, &a);
     for (size_t k = 0; k < (size_t)a.K; ++k) {
-      a.in[k] = s->slot[k][l];
+      if (l == 0) a.in0[k] = s->p2[k];
+      else a.in[k] = s->slot[k][l];
       a.out[k] = l + 1 < s->L - 1 ? s->slot[k][l + 1] : LevelPlanes{};
       a.lap[k] = s->lap[begin + k][l];
       a.gtop[k] = s->gtop[begin + k];
@@ -455,9 +462,9 @@ int run_pending_pass1(fs_stack* s, bool flush) {
     const size_t to_come = s->d.frame_count - s->frames.size();
     if (!(pending >= s->K || (pending > 0 && (flush || to_come <= kTailFrames)))) break;
     size_t begin = s->pass1_done, end = std::min(s->frames.size(), begin + s->K);
-    int rc = s->mode == P2_LAPS ? launch_lap0_batch(s, begin, end)
-             : s->bps == 2      ? launch_remap16_batch(s, s->frames, begin, end, true, 0.0f)
-                                : launch_remap_weights_batch(s, s->frames, begin, end, true);
+    int rc = s->mode == P2_FUSED ? launch_lap0_batch(s, begin, end)
+             : s->bps == 2       ? launch_remap16_batch(s, s->frames, begin, end, true, 0.0f)
+                                 : launch_remap_weights_batch(s, s->frames, begin, end, true);
     if (rc != FS_OK) return rc;
     // the staging buffers of these frames are free for reuse after this remap
     for (size_t f = begin; f < end; ++f) {
@@ -466,7 +473,18 @@ int run_pending_pass1(fs_stack* s, bool flush) {
       cudaError_t e = cudaEventRecord(s->slot_done[slot], s->ctx->stream);
       if (e != cudaSuccess) return cuda_err(s->ctx, e, "pass-1 event");
     }
-    if (s->mode == P2_LAPS && (rc = launch_image_pyramid(s, begin, end)) != FS_OK) return rc;
+    if (s->mode == P2_LAPS && s->best) {
+      // hybrid: the hardmask winners of the batch, from its pass-1 planes
+      FramePlanes pl[kMaxBatch];
+      for (size_t k = begin; k < end; ++k) pl[k - begin] = FramePlanes{s->p2[k - begin].rgba, s->wplane[k]};
+      cudaError_t e = timed(s->ctx, "winners", [&] {
+        return launch_winners(pl, (int)(end - begin), s->best, s->hard, begin == 0 ? 1 : 0, (int)s->W, (int)s->H,
+                              s->pitch[0], s->ctx->stream);
+      });
+      if (e != cudaSuccess) return cuda_err(s->ctx, e, "winners");
+    }
+    if ((s->mode == P2_LAPS || s->mode == P2_FUSED) && (rc = launch_image_pyramid(s, begin, end)) != FS_OK)
+      return rc;
     s->pass1_done = end;
   }
   return FS_OK;
@@ -882,7 +900,8 @@ struct StackPlan {
   uint32_t fp_level = 0;     // first level l >= 1 run one frame per CTA (L - 1: none)
   size_t contrib = 0, contrib_top = 0;  // bytes of the contribution buffers
   size_t laps_frame = 0;                // LAPS: weight, Laplacians, top Gaussian and masks of one frame
-  size_t laps_fixed = 0;                // LAPS: the level-0 Laplacian sum of the fallback pixels
+  size_t fused_frame = 0;               // FUSED: the same without the level-0 Laplacian
+  size_t fused_fixed = 0;               // FUSED: the level-0 Laplacian sum of the fallback pixels
 };
 
 // Levels with fewer 64x32 tiles than this run one frame per CTA (grid.z = K)
@@ -932,12 +951,13 @@ StackPlan plan_stack(const fs_stack_desc& d) {
     }
   }
   if (p.L >= 3 && bps == 1) {
-    p.laps_frame = n0 * 4;
-    for (uint32_t l = 1; l + 1 < p.L; ++l) p.laps_frame += (size_t)p.pitch[l] * p.lh[l] * 3 * esz;
-    p.laps_frame += (size_t)p.pitch[p.L - 1] * p.lh[p.L - 1] * 12;  // top Gaussian
-    for (uint32_t l = 1; l + 1 < p.L; ++l) p.laps_frame += (size_t)p.pitch[l] * p.lh[l] * esz;  // masks
-    p.laps_frame += (size_t)p.pitch[p.L - 1] * p.lh[p.L - 1] * 4;  // top mask
-    p.laps_fixed = n0 * 12;
+    p.fused_frame = n0 * 4;                                                                      // weight
+    for (uint32_t l = 1; l + 1 < p.L; ++l) p.fused_frame += (size_t)p.pitch[l] * p.lh[l] * 3 * esz;  // Laplacians
+    p.fused_frame += (size_t)p.pitch[p.L - 1] * p.lh[p.L - 1] * 12;  // top Gaussian
+    for (uint32_t l = 1; l + 1 < p.L; ++l) p.fused_frame += (size_t)p.pitch[l] * p.lh[l] * esz;  // masks
+    p.fused_frame += (size_t)p.pitch[p.L - 1] * p.lh[p.L - 1] * 4;  // top mask
+    p.fused_fixed = n0 * 12;
+    p.laps_frame = p.fused_frame + n0 * 12;  // and the level-0 Laplacian (f32)
   }
   if (p.fp_level + 1 < p.L) {
     p.contrib = (size_t)p.K * 3 * p.pitch[p.fp_level] * p.lh[p.fp_level] * 4;
@@ -953,7 +973,10 @@ uint64_t plan_bytes(const StackPlan& p, uint32_t frames, Pass2Mode mode, bool ho
   const uint64_t staging = host_frames ? (uint64_t)p.frame_bytes * p.staging_slots : 0;
   switch (mode) {
     case P2_LAPS:
-      return p.fixed + p.laps_fixed + ((uint64_t)p.laps_frame + 2 * p.L * sizeof(float*)) * frames + staging;
+      return p.fixed + (uint64_t)p.planes / 2 * p.K + ((uint64_t)p.laps_frame + 2 * p.L * sizeof(float*)) * frames +
+             staging;
+    case P2_FUSED:
+      return p.fixed + p.fused_fixed + ((uint64_t)p.fused_frame + 2 * p.L * sizeof(float*)) * frames + staging;
     case P2_CACHE: return p.fixed + (uint64_t)p.planes * frames + staging;
     case P2_RESIDENT: return p.fixed + (uint64_t)p.planes * p.K + (uint64_t)p.frame_bytes * frames;
     default: return p.fixed + (uint64_t)p.planes * p.K + staging;
@@ -964,6 +987,7 @@ uint64_t plan_bytes(const StackPlan& p, uint32_t frames, Pass2Mode mode, bool ho
 // fit, else keep the frames, else refetch them.
 Pass2Mode choose_mode(const StackPlan& p, uint32_t frames, uint64_t available, bool host_frames, bool wide) {
   if (p.laps_frame && plan_bytes(p, frames, P2_LAPS, host_frames) <= available) return P2_LAPS;
+  if (p.fused_frame && plan_bytes(p, frames, P2_FUSED, host_frames) <= available) return P2_FUSED;
   if (!wide && plan_bytes(p, frames, P2_CACHE, host_frames) <= available) return P2_CACHE;
   if (plan_bytes(p, frames, P2_RESIDENT, host_frames) <= available) return P2_RESIDENT;
   return P2_REFETCH;
@@ -1048,15 +1072,28 @@ static int begin_impl(fs_ctx* ctx, const fs_stack_desc* desc, fs_stack** out, in
   s->mode = forced_mode >= 0 ? (Pass2Mode)forced_mode
                              : choose_mode(plan, d.frame_count, available, true, d.sample_bits == 16);
   const size_t planes_bytes = plan.planes;
-  if (s->mode == P2_LAPS) {
-    if ((rc = stack_alloc(s, plan.laps_fixed, &p)) != FS_OK) return fail(rc);
-    s->au = (float*)p;
+  if (s->mode == P2_LAPS || s->mode == P2_FUSED) {
+    const bool laps = s->mode == P2_LAPS;
+    if (laps) {
+      // remapped RGBA of the batch's frames, read by the level-0 image step
+      for (uint32_t kk = 0; kk < s->K; ++kk) {
+        if ((rc = stack_alloc(s, n0 * 4, &p)) != FS_OK) return fail(rc);
+        s->p2.push_back(FramePlanes{(uint32_t*)p, nullptr});
+      }
+    } else {
+      if ((rc = stack_alloc(s, plan.fused_fixed, &p)) != FS_OK) return fail(rc);
+      s->au = (float*)p;
+    }
     for (uint32_t f = 0; f < d.frame_count; ++f) {
-      if ((rc = stack_alloc(s, plan.laps_frame, &p)) != FS_OK) return fail(rc);
+      if ((rc = stack_alloc(s, laps ? plan.laps_frame : plan.fused_frame, &p)) != FS_OK) return fail(rc);
       uint8_t* q = (uint8_t*)p;
       s->wplane.push_back((float*)q);
       q += n0 * 4;
-      std::vector<void*> lv(1, nullptr);  // level 0 is blended by the fused pass-1 kernel
+      std::vector<void*> lv(1, nullptr);  // FUSED: level 0 is blended by the fused pass-1 kernel
+      if (laps) {
+        lv[0] = q;  // level-0 Laplacian, f32
+        q += n0 * 12;
+      }
       for (uint32_t l = 1; l + 1 < s->L; ++l) {
         lv.push_back(q);
         q += (size_t)s->pitch[l] * s->lh[l] * 3 * esz;
@@ -1109,11 +1146,11 @@ static int begin_impl(fs_ctx* ctx, const fs_stack_desc* desc, fs_stack** out, in
 int fs_stack_begin(fs_ctx* ctx, const fs_stack_desc* desc, fs_stack** out) { return begin_impl(ctx, desc, out, -1); }
 
 int fs_stack_begin_mode(fs_ctx* ctx, const fs_stack_desc* desc, int pass2_mode, fs_stack** out) {
-  if (pass2_mode < -1 || pass2_mode > 3) return set_err(ctx, FS_ERR_INVALID, "unknown pass-2 mode");
-  if (desc && desc->sample_bits == 16 && (pass2_mode == P2_CACHE || pass2_mode == P2_LAPS))
+  if (pass2_mode < -1 || pass2_mode > P2_FUSED) return set_err(ctx, FS_ERR_INVALID, "unknown pass-2 mode");
+  if (desc && desc->sample_bits == 16 && (pass2_mode == P2_CACHE || pass2_mode >= P2_LAPS))
     return set_err(ctx, FS_ERR_UNSUPPORTED, "16-bit stacks run the resident or refetch mode");
-  if (desc && pass2_mode == P2_LAPS && plan_stack(*desc).laps_frame == 0)
-    return set_err(ctx, FS_ERR_UNSUPPORTED, "the laps mode needs at least 3 pyramid levels (8-bit samples)");
+  if (desc && pass2_mode >= P2_LAPS && plan_stack(*desc).laps_frame == 0)
+    return set_err(ctx, FS_ERR_UNSUPPORTED, "the laps and fused modes need at least 3 pyramid levels (8-bit samples)");
   return begin_impl(ctx, desc, out, pass2_mode);
 }
 
@@ -1334,8 +1371,8 @@ static int pass2_impl(fs_stack* s, fs_frame_fetch_cb refetch, void* user) {
     e = timed(ctx, "mask_support", [&] { return launch_mask_support(m, st); });
     if (e != cudaSuccess) return cuda_err(ctx, e, "mask support");
   }
-  // (the LAPS blends write every accumulator level whole)
-  for (uint32_t l = 0; l < s->L && s->mode != P2_LAPS; ++l) {
+  // (the split-pyramid blends write every accumulator level whole)
+  for (uint32_t l = 0; l < s->L && s->mode != P2_LAPS && s->mode != P2_FUSED; ++l) {
     e = cudaMemsetAsync(s->acc[l], 0, (size_t)s->pitch[l] * s->lh[l] * 3 * 4, st);
     if (e != cudaSuccess) return cuda_err(ctx, e, "accumulator clear");
   }
@@ -1343,14 +1380,23 @@ static int pass2_impl(fs_stack* s, fs_frame_fetch_cb refetch, void* user) {
   // of the stack, also those of other shards
   const size_t N = s->frames.size();
   const float inv_count = 1.0f / (float)(s->frame_total ? s->frame_total : N);
-  if (s->mode == P2_LAPS) {
-    // level 0: the weighted Laplacian sum of pass 1 divided by the complete
-    // weight sum (the 1/N fallback from the plain sum)
-    e = timed(ctx, "blend0", [&] {
-      return launch_finalize0(s->acc[0], s->au, s->norm, s->pitch[0] * s->lh[0], s->pitch[0], (int)s->W, (int)s->H,
-                              inv_count, st);
-    });
-    if (e != cudaSuccess) return cuda_err(ctx, e, "level-0 finalize");
+  if (s->mode == P2_LAPS || s->mode == P2_FUSED) {
+    if (s->mode == P2_LAPS) {
+      // level-0 blend of every frame at once, streaming over the Laplacians
+      // (it also turns each frame's weight into its normalised mask)
+      e = timed(ctx, "blend0", [&] {
+        return launch_blend0(s->acc[0], s->pitch[0] * s->lh[0], s->pitch[0], (int)s->W, (int)s->H, s->norm, s->tab,
+                             (float* const*)(s->tab + N), (int)N, inv_count, st);
+      });
+    } else {
+      // level 0: the weighted Laplacian sum of pass 1 divided by the complete
+      // weight sum (the 1/N fallback from the plain sum)
+      e = timed(ctx, "blend0", [&] {
+        return launch_finalize0(s->acc[0], s->au, s->norm, s->pitch[0] * s->lh[0], s->pitch[0], (int)s->W,
+                                (int)s->H, inv_count, st);
+      });
+    }
+    if (e != cudaSuccess) return cuda_err(ctx, e, "level-0 blend");
     // the mask pyramid of every frame, level by level (one frame per grid z)
     for (uint32_t l = 0; l + 1 < s->L; ++l) {
       MaskReduceArgs m;
@@ -1363,8 +1409,9 @@ static int pass2_impl(fs_stack* s, fs_frame_fetch_cb refetch, void* user) {
       m.hn = (int32_t)s->lh[l + 1];
       m.pitch_l = s->pitch[l];
       m.pitch_n = s->pitch[l + 1];
-      // level 0: each frame's raw weight, normalised by the weight sum on the fly
-      m.norm = l == 0 ? s->norm : nullptr;
+      // FUSED level 0: each frame's raw weight, normalised by the weight sum on
+      // the fly (LAPS: blend0 has already written the normalised masks)
+      m.norm = l == 0 && s->mode == P2_FUSED ? s->norm : nullptr;
       m.inv_count = inv_count;
       const int in_storage = l == 0 ? FS_STORAGE_F32 : s->storage;
       const int out_storage = l + 2 < s->L ? s->storage : FS_STORAGE_F32;
@@ -1649,12 +1696,12 @@ int fs_stack_set_method(fs_stack* s, int method, float hybrid_sharpness) {
 int fs_stack_pass2_mode(const fs_stack* s) { return s ? (int)s->mode : -1; }
 
 int fs_stack_mode_bytes(const fs_stack_desc* desc, int pass2_mode, int host_frames, uint64_t* bytes) {
-  if (!desc || !bytes || pass2_mode < 0 || pass2_mode > 3) return FS_ERR_INVALID;
+  if (!desc || !bytes || pass2_mode < 0 || pass2_mode > P2_FUSED) return FS_ERR_INVALID;
   int code = FS_OK;
   if (check_desc(*desc, &code)) return code;
   const StackPlan plan = plan_stack(*desc);
-  if (pass2_mode == P2_LAPS && plan.laps_frame == 0) return FS_ERR_UNSUPPORTED;
-  if (desc->sample_bits == 16 && pass2_mode == P2_CACHE) return FS_ERR_UNSUPPORTED;
+  if (pass2_mode >= P2_LAPS && plan.laps_frame == 0) return FS_ERR_UNSUPPORTED;
+  if (desc->sample_bits == 16 && (pass2_mode == P2_CACHE || pass2_mode >= P2_LAPS)) return FS_ERR_UNSUPPORTED;
   *bytes = plan_bytes(plan, desc->frame_count, (Pass2Mode)pass2_mode, host_frames != 0);
   return FS_OK;
 }

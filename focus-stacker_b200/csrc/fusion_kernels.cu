@@ -983,7 +983,7 @@ __device__ void store_next_image(const ImgSmem& S, const LevelArgs& a, int x0, i
 
 }  // namespace
 
-template <typename T>
+template <typename T, bool L0>
 __global__ void __launch_bounds__(NT) img_kernel(const __grid_constant__ LevelArgs a) {
   extern __shared__ __align__(16) uint8_t smem_raw[];
   ImgSmem& S = *reinterpret_cast<ImgSmem*>(smem_raw);
@@ -1000,22 +1000,78 @@ __global__ void __launch_bounds__(NT) img_kernel(const __grid_constant__ LevelAr
       v[j] = make_float4(0.f, 0.f, 0.f, 0.f);
       if (i < GH * GW && X >= 0 && Y >= 0 && X < a.wl && Y < a.hl) {
         const int64_t o = (int64_t)Y * a.pitch_l + X;
-        const LevelPlanes& in = a.in[k];
-        const T* g = (const T*)in.g;
-        v[j] = make_float4(ldv<T>(g, o), ldv<T>(g, in.plane + o), ldv<T>(g, 2 * in.plane + o), in.s[o] ? 1.0f : 0.0f);
+        if constexpr (L0) {
+          const uint32_t q = __ldg(a.in0[k].rgba + o);
+          v[j] = make_float4(__uint_as_float(q), 0.f, 0.f, 0.f);
+        } else {
+          const LevelPlanes& in = a.in[k];
+          const T* g = (const T*)in.g;
+          v[j] = make_float4(ldv<T>(g, o), ldv<T>(g, in.plane + o), ldv<T>(g, 2 * in.plane + o),
+                             in.s[o] ? 1.0f : 0.0f);
+        }
       }
     }
 #pragma unroll
     for (int j = 0; j < HALF; ++j) {
       const int i = threadIdx.x + (h * HALF + j) * NT;
-      if (i < GH * GW) S.gs[i] = v[j];
+      if (i >= GH * GW) continue;
+      if constexpr (L0) {
+        const uint32_t q = __float_as_uint(v[j].x);
+        S.gs[i] = make_float4(chf(q, 0), chf(q, 1), chf(q, 2), px_alpha(q) > 0 ? 1.0f : 0.0f);
+      } else {
+        S.gs[i] = v[j];
+      }
     }
   }
   __syncthreads();
   reduce_image_step(S, a, x0, y0);
   store_next_image<T>(S, a, x0, y0, k);
   float unused[PPT][3];
-  expand_blend_step<true, ImgSmem, T>(S, a, x0, y0, unused, (T*)a.lap[k]);
+  // the level-0 Laplacian stays FP32; the levels above are in the storage type
+  using TL = typename std::conditional<L0, float, T>::type;
+  expand_blend_step<true, ImgSmem, TL>(S, a, x0, y0, unused, (TL*)a.lap[k]);
+}
+
+
+// Level-0 blend of a whole stack in frame order, one pixel per thread:
+// acc = sum over frames of lap_k * (w_k / weight sum) (1 / N where the sum
+// is <= 1e-12), the same products and sums the per-batch kernels form.
+// The normalised mask replaces each frame's weight in place (the level-0
+// mask REDUCE then reads it without dividing again).
+__global__ void blend0_kernel(float* acc, int64_t plane, int64_t pitch, int w, int h, const float* norm,
+                              const float* const* lap, float* const* wgt, int frames, float inv_count) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (int64_t)w * h) return;
+  const int64_t o = (i / w) * pitch + i % w;
+  const float nv = norm[o];
+  float a0 = 0.0f, a1 = 0.0f, a2 = 0.0f;
+  constexpr int U = 4;  // frames whose loads are issued together
+  for (int k0 = 0; k0 < frames; k0 += U) {
+    float l0[U], l1[U], l2[U], wv[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      if (k0 + u < frames) {
+        const float* lk = lap[k0 + u];
+        l0[u] = __ldg(lk + o);
+        l1[u] = __ldg(lk + plane + o);
+        l2[u] = __ldg(lk + 2 * plane + o);
+        wv[u] = wgt[k0 + u][o];
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      if (k0 + u < frames) {
+        const float m = nv > 1e-12f ? __fdiv_rn(wv[u], nv) : inv_count;
+        wgt[k0 + u][o] = m;
+        a0 = __fadd_rn(a0, __fmul_rn(l0[u], m));
+        a1 = __fadd_rn(a1, __fmul_rn(l1[u], m));
+        a2 = __fadd_rn(a2, __fmul_rn(l2[u], m));
+      }
+    }
+  }
+  acc[o] = a0;
+  acc[plane + o] = a1;
+  acc[2 * plane + o] = a2;
 }
 
 // Blend of one level over all frames in order, one pixel per thread (the
@@ -1242,7 +1298,7 @@ cudaError_t launch_mask_reduce(const MaskReduceArgs& a, int frames, int in_stora
   const dim3 grid((unsigned)((a.wn + 63) / 64), (unsigned)((a.hn + kReduceWarps * kReduceRows - 1) /
                                                               (kReduceWarps * kReduceRows)),
                   (unsigned)frames);
-  if (a.norm) {  // level 0 of a LAPS stack: raw weights, normalised on the fly
+  if (a.norm) {  // level 0 of a FUSED stack: raw weights, normalised on the fly
     if (in_storage != FS_STORAGE_F32) return cudaErrorInvalidValue;
     return launch_mask_reduce_in<float, true>(a, grid, block, out_storage, s);
   }
@@ -1353,16 +1409,59 @@ __device__ __forceinline__ void sum_row_u8(const uint32_t (&wr)[7], int c, int w
   }
 }
 
-// One vertical REDUCE tap: v = fma(w, row, v) on value and weight sums.
+// The words of level-0 row y under the lane's taps (columns c - 2 .. c + 4);
+// only loads, so that the next rows can be fetched while this one is summed.
+__device__ __forceinline__ void load_row_u8(const LevelArgs& a, int k, int y, int c, bool live, uint32_t (&w)[7]) {
+#pragma unroll
+  for (int u = 0; u < 7; ++u) w[u] = 0u;
+  if (live && y >= 0 && y < a.hl) {
+    const uint32_t* row = a.in0[k].rgba + (int64_t)y * a.pitch_l;
+    const uint4 q4 = *reinterpret_cast<const uint4*>(row + c);  // inside the row's pitch
+    w[2] = q4.x;
+    w[3] = q4.y;
+    w[4] = q4.z;
+    w[5] = q4.w;
+    if (c > 0) {
+      const uint2 q2 = *reinterpret_cast<const uint2*>(row + c - 2);
+      w[0] = q2.x;
+      w[1] = q2.y;
+    }
+    if (c + 4 < a.wl) w[6] = row[c + 4];
+  }
+}
+
+__device__ __forceinline__ void img_row_u8(const LevelArgs& a, int k, int y, int c, bool live, int4 (&hs)[2]) {
+  uint32_t w[7];
+  load_row_u8(a, k, y, c, live, w);
+  sum_row_u8(w, c, a.wl, hs);
+}
+
+// One vertical REDUCE tap: v = fma(w, row, v) on value and weight sums
+// (integer sums at level 0).
 __device__ __forceinline__ float4 vtap(int w, float4 t, float4 v) {
   const float f = (float)w;
   return make_float4(fmaf(f, t.x, v.x), fmaf(f, t.y, v.y), fmaf(f, t.z, v.z), fmaf(f, t.w, v.w));
 }
+__device__ __forceinline__ int4 vtap(int w, int4 t, int4 v) {
+  return make_int4(v.x + w * t.x, v.y + w * t.y, v.z + w * t.z, v.w + w * t.w);
+}
+template <class A> __device__ __forceinline__ A acc_zero();
+template <> __device__ __forceinline__ float4 acc_zero<float4>() { return make_float4(0.f, 0.f, 0.f, 0.f); }
+template <> __device__ __forceinline__ int4 acc_zero<int4>() { return make_int4(0, 0, 0, 0); }
 // exact float of a non-negative integer below 2^23
 __device__ __forceinline__ float small_int_float(int v) { return __int_as_float(0x4B000000 | v) - 8388608.0f; }
+__device__ __forceinline__ float4 acc_float(float4 v) { return v; }
+__device__ __forceinline__ float4 acc_float(int4 v) {
+  return make_float4(small_int_float(v.x), small_int_float(v.y), small_int_float(v.z), small_int_float(v.w));
+}
+template <typename T, bool L0, class A>
+__device__ __forceinline__ void row_sums(const LevelArgs& a, int k, int y, int c, bool live, A (&hs)[2]) {
+  if constexpr (L0) img_row_u8(a, k, y, c, live, hs);
+  else img_row<T>(a, k, y, c, live, hs);
+}
 __device__ __forceinline__ int kwi(int i) { return (i == 0 || i == 4) ? 1 : ((i == 1 || i == 3) ? 4 : 6); }
 
-template <typename T>
+template <typename T, bool L0>
 __global__ void __launch_bounds__(32 * kImgWarps) img_stream_kernel(const __grid_constant__ LevelArgs a, int rows) {
   const int lane = (int)threadIdx.x, k = (int)blockIdx.z;
   const int first = ((int)blockIdx.x * kImgWarps + (int)threadIdx.y) * kImgPairs;  // pair of lane 1
@@ -1374,38 +1473,78 @@ __global__ void __launch_bounds__(32 * kImgWarps) img_stream_kernel(const __grid
   const bool j1in = J0 + 1 < a.wn, rin = J0 + 2 < a.wn;
   const int i0 = (int)blockIdx.y * rows;
   const int i1 = min(i0 + rows, a.hn);
-  const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
+  using Acc = typename std::conditional<L0, int4, float4>::type;
+  const Acc zero = acc_zero<Acc>();
   // vertical REDUCE sums in tap order (level-l rows 2r - 2 .. 2r + 2 for
   // level-(l+1) row r): cur = row r with taps 0 .. 2, nxt = row r + 1 with
   // tap 0; the level-l rows 2r + 1, 2r + 2 complete cur, advance nxt and
   // start row r + 2
-  float4 cur[2], nxt[2];
+  Acc cur[2], nxt[2];
   float Hm2[3][4], Hm1[3][4], Hc[3][4];
 #pragma unroll
   for (int ch = 0; ch < 3; ++ch)
 #pragma unroll
     for (int u = 0; u < 4; ++u) Hm2[ch][u] = Hm1[ch][u] = 0.0f;
   int r = i0 > 0 ? i0 - 1 : 0;
+  // level 0: the lane's four words of level-l rows 2r - 2, 2r - 1, 2r at the
+  // top of step r (the Laplacian rows emitted at step r are the first two)
+  uint4 ringR = make_uint4(0u, 0u, 0u, 0u), ringQ = ringR, ringP = ringR;
   {
-    float4 t0[2], t1[2], t2[2];
-    img_row<T>(a, k, 2 * r - 2, c, live, t0);
-    img_row<T>(a, k, 2 * r - 1, c, live, t1);
-    img_row<T>(a, k, 2 * r, c, live, t2);
+    Acc t0[2], t1[2], t2[2];
+    if constexpr (L0) {
+      uint32_t w0[7], w1[7], w2[7];
+      load_row_u8(a, k, 2 * r - 2, c, live, w0);
+      load_row_u8(a, k, 2 * r - 1, c, live, w1);
+      load_row_u8(a, k, 2 * r, c, live, w2);
+      sum_row_u8(w0, c, a.wl, t0);
+      sum_row_u8(w1, c, a.wl, t1);
+      sum_row_u8(w2, c, a.wl, t2);
+      ringR = make_uint4(w0[2], w0[3], w0[4], w0[5]);
+      ringQ = make_uint4(w1[2], w1[3], w1[4], w1[5]);
+      ringP = make_uint4(w2[2], w2[3], w2[4], w2[5]);
+    } else {
+      row_sums<T, L0>(a, k, 2 * r - 2, c, live, t0);
+      row_sums<T, L0>(a, k, 2 * r - 1, c, live, t1);
+      row_sums<T, L0>(a, k, 2 * r, c, live, t2);
+    }
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
       cur[h] = vtap(kwi(2), t2[h], vtap(kwi(1), t1[h], vtap(kwi(0), t0[h], zero)));
       nxt[h] = vtap(kwi(0), t2[h], zero);
     }
   }
+  uint32_t n3[7], n4[7];  // level 0: the words of the next two rows, fetched one step ahead
+  if constexpr (L0) {
+    load_row_u8(a, k, 2 * r + 1, c, live, n3);
+    load_row_u8(a, k, 2 * r + 2, c, live, n4);
+  }
   for (; r <= i1; ++r) {
     float4 fin[2];
+    uint4 c3 = make_uint4(0u, 0u, 0u, 0u), c4 = c3;  // level 0: words of rows 2r + 1, 2r + 2
     {
-      float4 t3[2], t4[2];
-      img_row<T>(a, k, 2 * r + 1, c, live, t3);
-      img_row<T>(a, k, 2 * r + 2, c, live, t4);
+      Acc t3[2], t4[2];
+      if constexpr (L0) {
+        uint32_t w3[7], w4[7];
+#pragma unroll
+        for (int u = 0; u < 7; ++u) {
+          w3[u] = n3[u];
+          w4[u] = n4[u];
+        }
+        if (r < i1) {
+          load_row_u8(a, k, 2 * r + 3, c, live, n3);
+          load_row_u8(a, k, 2 * r + 4, c, live, n4);
+        }
+        sum_row_u8(w3, c, a.wl, t3);
+        sum_row_u8(w4, c, a.wl, t4);
+        c3 = make_uint4(w3[2], w3[3], w3[4], w3[5]);
+        c4 = make_uint4(w4[2], w4[3], w4[4], w4[5]);
+      } else {
+        row_sums<T, L0>(a, k, 2 * r + 1, c, live, t3);
+        row_sums<T, L0>(a, k, 2 * r + 2, c, live, t4);
+      }
 #pragma unroll
       for (int h = 0; h < 2; ++h) {
-        fin[h] = vtap(kwi(4), t4[h], vtap(kwi(3), t3[h], cur[h]));
+        fin[h] = acc_float(vtap(kwi(4), t4[h], vtap(kwi(3), t3[h], cur[h])));
         cur[h] = vtap(kwi(2), t4[h], vtap(kwi(1), t3[h], nxt[h]));
         nxt[h] = vtap(kwi(0), t4[h], zero);
       }
@@ -1467,10 +1606,20 @@ __global__ void __launch_bounds__(32 * kImgWarps) img_stream_kernel(const __grid
         if (y >= a.hl) break;
         const int64_t ro = (int64_t)y * a.pitch_l;
         float gv[3][4];
-        const LevelPlanes& in = a.in[k];
+        if constexpr (L0) {
+          const uint4 q4 = yy == 0 ? ringR : ringQ;  // rows 2r - 2, 2r - 1
+          const uint32_t w[4] = {q4.x, q4.y, q4.z, q4.w};
 #pragma unroll
-        for (int ch = 0; ch < 3; ++ch) ld4<T>((const T*)in.g + ch * in.plane + ro + c, gv[ch]);
-        T* lp = (T*)a.lap[k] + ro + c;
+          for (int ch = 0; ch < 3; ++ch)
+#pragma unroll
+            for (int u = 0; u < 4; ++u) gv[ch][u] = chf(w[u], ch);
+        } else {
+          const LevelPlanes& in = a.in[k];
+#pragma unroll
+          for (int ch = 0; ch < 3; ++ch) ld4<T>((const T*)in.g + ch * in.plane + ro + c, gv[ch]);
+        }
+        using TL = typename std::conditional<L0, float, T>::type;  // level-0 Laplacians stay FP32
+        TL* lp = (TL*)a.lap[k] + ro + c;
 #pragma unroll
         for (int ch = 0; ch < 3; ++ch) {
           float lv[4];
@@ -1481,13 +1630,13 @@ __global__ void __launch_bounds__(32 * kImgWarps) img_stream_kernel(const __grid
                 : __fmul_rn(__fadd_rn(Hm1[ch][u], Hm1[ch][u]), 0.5f);
             lv[u] = __fsub_rn(gv[ch][u], e);
           }
-          T* lc = lp + ch * a.acc_plane_l;
+          TL* lc = lp + ch * a.acc_plane_l;
           if (c + 3 < a.wl) {
-            st4<T>(lc, lv);
+            st4<TL>(lc, lv);
           } else {
 #pragma unroll
             for (int u = 0; u < 4; ++u)
-              if (c + u < a.wl) stv<T>(lc, u, lv[u]);
+              if (c + u < a.wl) stv<TL>(lc, u, lv[u]);
           }
         }
       }
@@ -1499,12 +1648,17 @@ __global__ void __launch_bounds__(32 * kImgWarps) img_stream_kernel(const __grid
         Hm2[ch][u] = Hm1[ch][u];
         Hm1[ch][u] = Hc[ch][u];
       }
+    if constexpr (L0) {
+      ringR = ringP;
+      ringQ = c3;
+      ringP = c4;
+    }
   }
 }
 
 // Rows per strip: 32, halved (down to 8) while the grid would give fewer
 // than 8 CTAs per SM.
-template <typename T>
+template <typename T, bool L0>
 static cudaError_t launch_img_stream(const LevelArgs& a, cudaStream_t s) {
   const int pairs = (a.wn + 1) / 2;
   const int warps = (pairs + kImgPairs - 1) / kImgPairs;
@@ -1512,33 +1666,66 @@ static cudaError_t launch_img_stream(const LevelArgs& a, cudaStream_t s) {
   int rows = 32;
   while (rows > 8 && (int64_t)bx * ((a.hn + rows - 1) / rows) * a.K < 8 * 148) rows /= 2;
   const dim3 grid((unsigned)bx, (unsigned)((a.hn + rows - 1) / rows), (unsigned)a.K);
-  img_stream_kernel<T><<<grid, dim3(32, kImgWarps), 0, s>>>(a, rows);
+  img_stream_kernel<T, L0><<<grid, dim3(32, kImgWarps), 0, s>>>(a, rows);
   return cudaGetLastError();
 }
 
-template <typename T>
-static cudaError_t launch_img_tile(const LevelArgs& a, cudaStream_t s, DeviceOnce* cfg) {
+cudaError_t launch_blend0(float* acc, int64_t plane, int64_t pitch, int w, int h, const float* norm,
+                          const float* const* lap, float* const* wgt, int frames, float inv_count,
+                          cudaStream_t s) {
+  const int64_t n = (int64_t)w * h;
+  blend0_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(acc, plane, pitch, w, h, norm, lap, wgt, frames,
+                                                           inv_count);
+  return cudaGetLastError();
+}
+
+template <template <typename, bool> class KER, bool L0>
+static cudaError_t launch_split(const LevelArgs& a, int storage, cudaStream_t s, DeviceOnce* cfg) {
   dim3 grid((a.wl + TW - 1) / TW, (a.hl + TH - 1) / TH, a.K);
   const size_t sm = sizeof(ImgSmem);
-  cudaError_t e = configure(img_kernel<T>, sm, cfg);
-  if (e != cudaSuccess) return e;
-  img_kernel<T><<<grid, NT, sm, s>>>(a);
+  cudaError_t e;
+  switch (storage) {
+    case FS_STORAGE_F32:
+      if ((e = configure(KER<float, L0>::kernel, sm, &cfg[0])) != cudaSuccess) return e;
+      KER<float, L0>::kernel<<<grid, NT, sm, s>>>(a);
+      break;
+    case FS_STORAGE_F16:
+      if ((e = configure(KER<__half, L0>::kernel, sm, &cfg[1])) != cudaSuccess) return e;
+      KER<__half, L0>::kernel<<<grid, NT, sm, s>>>(a);
+      break;
+    case FS_STORAGE_BF16:
+      if ((e = configure(KER<__nv_bfloat16, L0>::kernel, sm, &cfg[2])) != cudaSuccess) return e;
+      KER<__nv_bfloat16, L0>::kernel<<<grid, NT, sm, s>>>(a);
+      break;
+    default:
+      return cudaErrorInvalidValue;
+  }
   return cudaGetLastError();
 }
+template <typename T, bool L0> struct ImgK {
+  static constexpr auto kernel = img_kernel<T, L0>;
+};
 
 cudaError_t launch_img_level(const LevelArgs& a, int storage, cudaStream_t s) {
-  static DeviceOnce cfg[3];
-  if (a.level < 1) return cudaErrorInvalidValue;  // level 0 is part of the fused pass-1 kernel
+  static DeviceOnce cfg0[3], cfg1[3];
   // clamped-EXPAND levels (never followed by the top level): streaming kernel
-  const bool stream = !a.exact_expand && a.level + 2 < a.levels;
-  switch (storage) {
-    case FS_STORAGE_F32: return stream ? launch_img_stream<float>(a, s) : launch_img_tile<float>(a, s, &cfg[0]);
-    case FS_STORAGE_F16: return stream ? launch_img_stream<__half>(a, s) : launch_img_tile<__half>(a, s, &cfg[1]);
-    case FS_STORAGE_BF16:
-      return stream ? launch_img_stream<__nv_bfloat16>(a, s) : launch_img_tile<__nv_bfloat16>(a, s, &cfg[2]);
-    default: return cudaErrorInvalidValue;
+  if (!a.exact_expand && a.level + 2 < a.levels) {
+    switch (storage) {
+      case FS_STORAGE_F32:
+        return a.level == 0 ? launch_img_stream<float, true>(a, s) : launch_img_stream<float, false>(a, s);
+      case FS_STORAGE_F16:
+        return a.level == 0 ? launch_img_stream<__half, true>(a, s) : launch_img_stream<__half, false>(a, s);
+      case FS_STORAGE_BF16:
+        return a.level == 0 ? launch_img_stream<__nv_bfloat16, true>(a, s)
+                            : launch_img_stream<__nv_bfloat16, false>(a, s);
+      default:
+        return cudaErrorInvalidValue;
+    }
   }
+  return a.level == 0 ? launch_split<ImgK, true>(a, storage, s, cfg0)
+                      : launch_split<ImgK, false>(a, storage, s, cfg1);
 }
+
 
 __global__ void sum_contrib_kernel(float* acc, int64_t plane, int64_t pitch, int w, int h, const float* contrib,
                                    int K) {

@@ -225,11 +225,19 @@ cudaError_t launch_finalize0(float* acc, const float* au, const float* norm, int
 cudaError_t launch_level0(const LevelArgs& a, int storage, cudaStream_t s);
 cudaError_t launch_level(const LevelArgs& a, int storage, cudaStream_t s);
 cudaError_t launch_collapse(const CollapseArgs& a, cudaStream_t s);
-// Split pyramid: the image half of a level step l >= 1 for the batch's
-// frames, one frame per CTA (grid.z = K): Gaussian REDUCE to level l + 1
-// (slots out[k], or gtop[k] at the top) and the Laplacian of level l into
-// lap[k] (level 0 is part of the fused pass-1 kernel, launch_lap0).
+// Split pyramid: the image half of a level step for the batch's frames, one
+// frame per CTA (grid.z = K): Gaussian REDUCE to level l + 1 (slots out[k],
+// or gtop[k] at the top) and the Laplacian of level l into lap[k] (FP32 at
+// level 0, the storage type above); level 0 reads the remapped RGBA planes
+// in0[k].rgba.
 cudaError_t launch_img_level(const LevelArgs& a, int storage, cudaStream_t s);
+// Level-0 blend of all frames of a stack (device tables of each frame's
+// level-0 Laplacian and weight planes), written over acc; each weight plane
+// is replaced by the frame's normalised mask, which launch_mask_reduce then
+// reads.
+cudaError_t launch_blend0(float* acc, int64_t plane, int64_t pitch, int w, int h, const float* norm,
+                          const float* const* lap, float* const* wgt, int frames, float inv_count,
+                          cudaStream_t s);
 // acc = sum over frames k, in order, of lap[k] (3 planes of `plane`) times
 // mask[k] (both in storage T: 0 f32, 1 f16, 2 bf16), written over acc.
 cudaError_t launch_blend(float* acc, int64_t plane, int64_t pitch, int w, int h, const void* const* lap,

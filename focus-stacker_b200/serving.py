@@ -7,10 +7,10 @@ Admission is the per-request form of the reference's memory budget
 (--memory-fraction, src/memory_budget.zig:3-53): a request is admitted when
 the device bytes its stack will hold (fs_stack_footprint, computed without
 allocating) fit in the budget left by the stacks in flight.  The stack's
-pass-2 mode is the first of `modes` (memory-lean first: keeping the pass-1
-planes, the reference's cached path, else keeping the frames) that fits both
-that remainder and a cap on one stack's share of the budget; requests wait
-in arrival order otherwise.  Each worker owns a context (its own streams),
+pass-2 mode is the first of `modes` (by default the fused split pyramid,
+then keeping the pass-1 planes, the reference's cached path, then keeping
+the frames) that fits both that remainder and a cap on one stack's share of
+the budget; requests wait in arrival order otherwise.  Each worker owns a context (its own streams),
 so stacks in flight overlap on the device; memory comes from the device's shared stream-ordered
 pool, and a worker's context budget is set to the reservation of the stack it
 runs.
@@ -117,7 +117,7 @@ class StackServer:
 
     def __init__(self, device: int = 0, hbm_budget_bytes: int = 120 * 10**9, workers: int = 4,
                  frames_per_batch: int = 0, context_factory=None, max_stack_fraction: float = 0.25,
-                 prewarm: bool = False, modes=("cache", "resident")):
+                 prewarm: bool = False, modes=("fused", "cache", "resident")):
         self.device = device
         self.budget = int(hbm_budget_bytes)
         self.frames_per_batch = frames_per_batch
@@ -157,8 +157,11 @@ class StackServer:
         busy = sum(o.reserved for o in self.workers if o.busy)
         avail = min(max(0, self.budget - busy), self.max_stack)
         mode, nbytes = None, 0
-        for m in self.modes:  # memory-lean modes first: more stacks in flight
-            b = api.stack_mode_bytes(desc, m, host_frames=True)
+        for m in self.modes:
+            try:
+                b = api.stack_mode_bytes(desc, m, host_frames=True)
+            except api.FocusCudaError:  # mode not available for this stack (fused needs 3 levels)
+                continue
             if b <= avail:
                 mode, nbytes = m, b
                 break

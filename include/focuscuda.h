@@ -253,7 +253,7 @@ int fs_stack_pass2_mode(const fs_stack* stack);
 
 /* Device bytes a stack of `desc` holds over its life when `available_bytes`
  * of budget are free, and the pass-2 mode it would pick there (0 cache, 1
- * resident, 2 refetch); host_frames != 0 counts the upload staging ring.
+ * resident, 2 refetch, 3 laps, 4 fused); host_frames != 0 counts the upload staging ring.
  * FS_ERR_BUDGET when not even the refetch mode fits.  Allocates nothing; the
  * admission test of a serving loop (the analogue of --memory-fraction,
  * src/memory_budget.zig:3-53, applied per request).  Not part of the
@@ -261,7 +261,9 @@ int fs_stack_pass2_mode(const fs_stack* stack);
 int fs_stack_footprint(const fs_stack_desc* desc, uint64_t available_bytes, int host_frames, uint64_t* bytes,
                        int* mode);
 /* Device bytes of a stack of `desc` in pass-2 mode pass2_mode (0 cache, 1
- * resident, 2 refetch, 3 laps), and fs_stack_begin with that mode imposed
+ * resident, 2 refetch, 3 laps: the split pyramid built in pass 1, 4 fused:
+ * the split pyramid with level 0 blended by the remap kernel itself, about
+ * half the bytes per frame-pixel of laps), and fs_stack_begin with that mode imposed
  * (-1: chosen from the budget as fs_stack_begin does); for a caller that
  * trades memory for speed itself (a serving loop keeps more stacks in flight
  * with the cache mode than with laps).  Not part of the reference. */

@@ -73,7 +73,7 @@ def test_level_sizes_halve_with_ceil_down_to_one():
     assert bench.level_sizes(1, 1) == [(1, 1)]
 
 
-@pytest.mark.parametrize("mode", ["laps", "cache", "recompute"])
+@pytest.mark.parametrize("mode", ["laps", "fused", "cache", "recompute"])
 def test_algorithmic_bytes_model(mode):
     w, h, f, k = 7872, 5243, 30, 8
     per_kernel, total = bench.algorithmic_bytes(w, h, f, k, mode, 4)
@@ -81,11 +81,15 @@ def test_algorithmic_bytes_model(mode):
                                "mask_support"}
     assert all(v >= 0 for v in per_kernel.values()) and total == sum(per_kernel.values())
     per_px = total / (f * w * h)
-    # pass 1 reads the 3 B frame; laps and cache also keep 8 B of planes
-    assert per_kernel["pass1"] / (f * w * h) > (11 if mode in ("laps", "cache") else 3)
+    # pass 1 reads the 3 B frame; laps and cache also keep 8 B of planes,
+    # fused writes the 4 B weight
+    assert per_kernel["pass1"] / (f * w * h) > {"laps": 11, "cache": 11, "fused": 7}.get(mode, 3)
     assert 25 < per_px < 100
-    if mode == "laps":
+    if mode in ("laps", "fused"):
         assert per_kernel["image"] > 0 and per_kernel["blend0"] > 0 and per_kernel["remap_weights"] == 0
+    if mode == "fused":
+        # no level-0 Laplacian or remapped frame through HBM
+        assert total < bench.algorithmic_bytes(w, h, f, k, "laps", 4)[1] - 20 * f * w * h
     if mode == "recompute":
         assert per_kernel["remap_weights"] > 0
     # FP16 storage moves fewer level bytes

@@ -276,10 +276,10 @@ def close_outputs(a, b):
 def test_pass2_modes_give_identical_results(torch, ctx):
     # cache (pass-1 planes kept), resident (frames kept, remapped again) and
     # refetch (frames fetched again) must produce the same bytes; laps (pass 1
-    # builds the pyramids and blends level 0 as sum(lap * w) / N) rounds level
-    # 0 in another order: within one u8 step of them, on a handful of pixels
-    # at most.  Each budget is the footprint of its mode, the largest the
-    # stack picks there
+    # builds the pyramids) and fused (pass 1 also blends level 0 as
+    # sum(lap * w) / N) round level 0 in another order: within one u8 step of
+    # them, on a handful of pixels at most.  Each budget is the footprint of
+    # its mode, the largest the stack picks there
     W, H, F = 240, 160, 8
     frames, poses = synth_stack(torch, ctx, W, H, F, seed=12)
     roi = fsb.compute_common_overlap_roi([True] * F, [W] * F, [H] * F, poses)
@@ -292,7 +292,7 @@ def test_pass2_modes_give_identical_results(torch, ctx):
             break
         budgets.setdefault(mode, b)
         avail = b - 1
-    assert set(budgets) == {"laps", "cache", "resident", "refetch"}
+    assert set(budgets) == {"laps", "fused", "cache", "resident", "refetch"}
     results = {}
     for want, budget in budgets.items():
         c = fsb.Context(0, hbm_budget_bytes=budget)
@@ -305,18 +305,23 @@ def test_pass2_modes_give_identical_results(torch, ctx):
         c.close()
     for m in ("resident", "refetch"):
         assert np.array_equal(results["cache"], results[m]), m
-    assert close_outputs(results["laps"], results["cache"])
+    for m in ("laps", "fused"):
+        assert close_outputs(results[m], results["cache"]), m
 
 @pytest.mark.parametrize("storage", [fsb.STORAGE_F32, fsb.STORAGE_F16, fsb.STORAGE_BF16])
 def test_laps_large_levels_match_cache(torch, ctx, storage):
-    # levels wider than 512 take the streaming pyramid kernel in laps mode;
-    # odd, non-multiple-of-4 level sizes exercise its edge columns and rows
+    # levels wider than 512 take the streaming pyramid kernel in the laps and
+    # fused modes;
+    # odd, non-multiple-of-4 level sizes exercise its edge columns and rows.
+    # FP32: laps and fused within one u8 step of cache on a handful of pixels;
+    # reduced storage (they also keep their Laplacians in it): each mode within the
+    # precision form's u8 bound of the oracle (1 for FP16, 2 for BF16)
     W, H, F = 1203, 917, 4
     frames, poses = synth_stack(torch, ctx, W, H, F, seed=21)
     roi = fsb.compute_common_overlap_roi([True] * F, [W] * F, [H] * F, poses)
     assert max(roi.width, roi.height) > 1024
     results = {}
-    for mode in ("laps", "cache"):
+    for mode in ("laps", "fused", "cache"):
         st = fsb.PyramidContrastStack(ctx, W, H, F, roi=roi, frames_per_batch=3, level_storage=storage,
                                       pass2_mode=mode)
         assert st.pass2_mode == mode
@@ -324,7 +329,14 @@ def test_laps_large_levels_match_cache(torch, ctx, storage):
             st.add_frame(f, p)
         results[mode] = st.finish()
         st.close()
-    assert close_outputs(results["laps"], results["cache"])
+    if storage == fsb.STORAGE_F32:
+        for m in ("laps", "fused"):
+            assert close_outputs(results[m], results["cache"]), m
+        return
+    ref = oracle.stack_fuse(frames, [p.as_dict() for p in poses], roi.as_tuple(), jobs=8)
+    bound = 1 if storage == fsb.STORAGE_F16 else 2
+    for mode, out in results.items():
+        assert np.abs(out.astype(np.int16) - ref.astype(np.int16)).max() <= bound, mode
 
 
 def test_stack_errors(torch, ctx):

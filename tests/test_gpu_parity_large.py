@@ -4,8 +4,8 @@ C ABI, against the CPU oracle.
 The reference expands with the clamped separable filter whenever a level
 side exceeds 512 (src/fuse/pyramid.zig:859-861, 1101-1149, 1748-1775); only
 stacks whose ROI is wider than 2048 take that path at levels 1 and 2 too.
-These tests fuse such stacks in every pass-2 mode (laps: the streaming image
-pyramid kernels; cache / resident / refetch: the tiled level kernels with
+These tests fuse such stacks in every pass-2 mode (laps and fused: the
+streaming image pyramid kernels; cache / resident / refetch: the tiled level kernels with
 exact_expand = 0; collapse in the clamped mode at each of those levels) and
 the full 30 x 7952 x 5304 production stack, and compare each with the
 oracle's FP32 evaluation: collapsed base within one 16-bit LSB (1/257 in
@@ -83,7 +83,7 @@ def wide_stack(torch, ctx):
     return frames, poses, roi, ref
 
 
-@pytest.mark.parametrize("mode", ["laps", "cache", "resident", "refetch"])
+@pytest.mark.parametrize("mode", ["laps", "fused", "cache", "resident", "refetch"])
 def test_clamped_expand_levels_match_oracle(torch, ctx, wide_stack, mode):
     frames, poses, roi, (ref_out, ref_base) = wide_stack
     out, base = fuse(torch, ctx, frames, poses, roi, mode, frames_per_batch=3)

@@ -204,8 +204,10 @@ def test_stack_footprint_modes_follow_the_budget():
     d = fsb.stack_desc(7952, 5304, 30, fsb.Rect(82, 63, 7872, 5243))
     laps, m_laps, ok = fsb.stack_footprint(d, 1 << 50)
     assert m_laps == "laps" and ok
-    cache, m_cache, ok = fsb.stack_footprint(d, laps - 1)
-    assert m_cache == "cache" and ok and cache < laps
+    fused, m_fused, ok = fsb.stack_footprint(d, laps - 1)
+    assert m_fused == "fused" and ok and fused < laps
+    cache, m_cache, ok = fsb.stack_footprint(d, fused - 1)
+    assert m_cache == "cache" and ok and cache < fused
     resident, m_res, ok = fsb.stack_footprint(d, cache - 1)
     assert m_res == "resident" and ok and resident < cache
     refetch, m_ref, ok = fsb.stack_footprint(d, resident - 1)
@@ -222,11 +224,15 @@ def test_stack_footprint_modes_follow_the_budget():
 
 def test_mode_bytes_order():
     d = fsb.stack_desc(7952, 5304, 30, fsb.Rect(82, 63, 7872, 5243))
-    b = {m: fsb.stack_mode_bytes(d, m) for m in ("laps", "cache", "resident", "refetch")}
-    assert b["laps"] > b["cache"] > b["resident"] > b["refetch"]
+    b = {m: fsb.stack_mode_bytes(d, m) for m in ("laps", "fused", "cache", "resident", "refetch")}
+    assert b["laps"] > b["fused"] > b["cache"] > b["resident"] > b["refetch"]
+    # per frame-pixel: laps keeps the f32 level-0 Laplacian (12 B) that fused does not
+    n0 = 7872 * 5243 * 30
+    assert 11.5 < (b["laps"] - b["fused"]) / n0 < 12.5
     assert fsb.stack_footprint(d, b["cache"])[:2] == (b["cache"], "cache")
-    with pytest.raises(fsb.FocusCudaError):  # two levels only: no laps mode
-        fsb.stack_mode_bytes(fsb.stack_desc(2, 1, 2), "laps")
+    for m in ("laps", "fused"):
+        with pytest.raises(fsb.FocusCudaError):  # two levels only: no split pyramid
+            fsb.stack_mode_bytes(fsb.stack_desc(2, 1, 2), m)
 
 
 def test_stack_footprint_rejects_bad_desc():
@@ -257,7 +263,8 @@ def test_server_admission_respects_the_budget():
                                   max_stack_fraction=1.0)
     big = fsb.serving.StackRequest(0, 0.0, 7952, 5304, 30)
     roi = fsb.Rect(0, 0, 7952, 5304)
-    need = fsb.stack_mode_bytes(fsb.stack_desc(7952, 5304, 30, roi), "cache")
+    # the server's first mode (the fused split pyramid) fits two stacks
+    need = fsb.stack_mode_bytes(fsb.stack_desc(7952, 5304, 30, roi), srv.modes[0])
     w1, b1 = srv._try_admit(big, roi)
     assert b1 == need and w1.busy and w1.ctx.budget == need
     w2, b2 = srv._try_admit(fsb.serving.StackRequest(1, 0.0, 7952, 5304, 30), roi)

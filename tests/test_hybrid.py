@@ -78,7 +78,7 @@ def stack(torch, ctx):
     return frames, poses, roi, ref_out, ref_base, ref_hard
 
 
-@pytest.mark.parametrize("mode", ["laps", "cache", "resident"])
+@pytest.mark.parametrize("mode", ["laps", "fused", "cache", "resident"])
 def test_hybrid_matches_oracle(torch, ctx, stack, mode):
     frames, poses, roi, ref_out, ref_base, ref_hard = stack
     soft, _, _ = run(torch, ctx, frames, poses, roi, "pyramid-contrast", mode)

@@ -43,12 +43,12 @@ def test_mixed_stream_same_alone_and_in_the_mix(torch):
     for r in rep.results:
         assert r.done_s >= r.admitted_s >= r.arrival_s
     # alone: the same frames through a fresh context, one stack at a time, in
-    # the cache mode (the server admits stacks in the cache / resident modes,
-    # which give the same bytes)
+    # the pass-2 mode the server ran the request in (cache and resident give
+    # the same bytes; laps rounds level 0 in its own order)
     alone_ctx = fsb.Context(0)
     for req, res in zip(sorted(reqs, key=lambda r: r.arrival_s), rep.results):
         roi = pool.roi(req)
-        st = fsb.PyramidContrastStack(alone_ctx, req.width, req.height, req.frames, roi=roi, pass2_mode="cache")
+        st = fsb.PyramidContrastStack(alone_ctx, req.width, req.height, req.frames, roi=roi, pass2_mode=res.pass2)
         for i in range(req.frames):
             buf, stride, pose = pool.frame(req, i)
             st.add_frame_device(buf, stride, pose)

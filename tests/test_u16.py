@@ -28,7 +28,7 @@ def test_desc_checks_for_16_bit_stacks():
     # argument checks only: no GPU needed
     d = fsb.stack_desc(640, 480, 20, sample_bits=16)
     assert fsb.stack_mode_bytes(d, "resident") > fsb.stack_mode_bytes(d, "refetch")
-    for mode in ("cache", "laps"):
+    for mode in ("cache", "laps", "fused"):
         with pytest.raises(fsb.FocusCudaError):
             fsb.stack_mode_bytes(d, mode)
     with pytest.raises(fsb.FocusCudaError) as e:
