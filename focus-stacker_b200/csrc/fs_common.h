@@ -33,7 +33,8 @@ struct Warp {
   int32_t kind;
   int32_t guard;          // 1: the denominator may reach <= 0 inside the ROI (every pixel takes the exact path)
   int32_t behind_is_void; // 1: D <= 0 gives an empty sample (basic chain); 0: |D| < eps gives empty (lens path)
-  int32_t pad0;
+  float tie_band;         // fast FP32 sampler: values within this of a .5 rounding boundary take the
+                          // exact path (from the map's error bound; kernels use at least 2.5e-4)
   double a, b, c, d, e, f, g, h;  // displacement-form homography coefficients
   // radial inverse (WARP_RADIAL): src = centre + undistort(radial point)
   double src_cx, src_cy;

@@ -89,15 +89,50 @@ __device__ __forceinline__ uint32_t px_alpha(uint32_t v) { return v >> 24; }
 __device__ __forceinline__ float chf(uint32_t v, int c) {
   return __uint_as_float(__byte_perm(v, 0x4B000000u, 0x7440u + (unsigned)c)) - 8388608.0f;
 }
-// contrast word: gray sum k = R + G + B (<= 765) in bits 0..19 and the
-// support flag at bit 20, zero for unsupported pixels, so that window sums
-// of these words add counts and gray sums in one integer add (a 15x15 window
-// stays below 2^20 for the gray sum and 2^12 for the count)
+// contrast word (16 bits): gray sum k = R + G + B (<= 765) in bits 0..14
+// and the support flag at bit 15, zero for unsupported pixels, so that the
+// sum of a window row of these words adds counts and gray sums in one
+// integer add (a row of at most 15 words keeps its gray sum below 2^15)
 __device__ __forceinline__ uint32_t contrast_word(uint32_t v) {
   if (px_alpha(v) == 0) return 0u;
   uint32_t k = (v & 255u) + ((v >> 8) & 255u) + ((v >> 16) & 255u);
-  return k | (1u << 20);
+  return k | kSupportFlag;
 }
+
+// A window-row sum of contrast words (count << 15 | gray sum) in the layout
+// of the window sums, count << 20 | gray sum (a 15 x 15 window stays below
+// 2^20 for the gray sum and 2^12 for the count)
+__device__ __forceinline__ uint32_t row_sum_word(uint32_t p) { return p + (p >> 15) * ((1u << 20) - kSupportFlag); }
+
+// Horizontal window sums of one region row for 8 consecutive output columns:
+// h1 = count << 20 | gray sum and h2 = sum of gray^2 over the window
+// columns [c, c + 2B], sliding from the first column
+template <int B>
+__device__ __forceinline__ void window_row8(const uint16_t* row, uint32_t* h1, uint32_t* h2) {
+  uint32_t p = 0, q = 0;
+#pragma unroll
+  for (int t = 0; t <= 2 * B; ++t) {
+    const uint32_t v = row[t];
+    const uint32_t g = v & 0x7FFFu;
+    p += v;
+    q += g * g;
+  }
+  h1[0] = row_sum_word(p);
+  h2[0] = q;
+#pragma unroll
+  for (int c = 1; c < 8; ++c) {
+    const uint32_t vin = row[c + 2 * B], vout = row[c - 1];
+    const uint32_t gin = vin & 0x7FFFu, gout = vout & 0x7FFFu;
+    p += vin - vout;
+    q += gin * gin - gout * gout;
+    h1[c] = row_sum_word(p);
+    h2[c] = q;
+  }
+}
+
+// Row stride (elements) of a region's 16-bit contrast words: an odd number of
+// 32-bit words, so that threads on consecutive rows hit distinct banks.
+constexpr int kv_stride(int rw) { return ((rw + 1) / 2) % 2 == 1 ? 2 * ((rw + 1) / 2) : 2 * ((rw + 1) / 2) + 2; }
 
 // f32(alpha) / 255 as the reference computes it (src/fuse/masks.zig:18).
 __device__ __forceinline__ float alpha_support(uint32_t al) {
@@ -135,26 +170,29 @@ constexpr int kExactQueue = 256;   // deferred exact samples per CTA and frame
 constexpr int kMaxAnchors = 120;   // 8x4 blocks of the largest region (contrast window 15)
 constexpr int32_t kNoAnchor = INT32_MIN;
 
-// Shared scratch of fill_region: the block anchors of the frame, and a queue
-// of samples the fast path could not decide, processed together after the
-// fast pass so that one lane's tie does not hold its whole warp on the
-// (long) exact path.
+// Shared scratch of fill_region: the block anchors of the frame (NB of the
+// region's 8x4 blocks), and a queue of samples the fast path could not
+// decide, processed together after the fast pass so that one lane's tie does
+// not hold its whole warp on the (long) exact path.
+template <int NB>
 struct __align__(16) ExactQueue {
-  Anchor anchor[kMaxAnchors];
+  Anchor anchor[NB];
   uint32_t count;
   uint32_t item[kExactQueue];  // ry << 16 | rx
 };
+template <int RW, int RH>
+using RegionQueue = ExactQueue<((RW + 7) / 8) * ((RH + 3) / 4)>;
 
 // The FP64 anchors of a region's 8x4 blocks into shared memory, one per
 // thread from thread `first` on, and the exact queue emptied.  The kernel
 // runs it for the next frame while the current one's window sums are formed
 // (the anchors are last read by the current frame's fast pass).
 template <int RW, int RH>
-__device__ __forceinline__ void region_anchors(const FrameIn& f, int rx0, int ry0, ExactQueue* q, int first) {
+__device__ __forceinline__ void region_anchors(const FrameIn& f, int rx0, int ry0, RegionQueue<RW, RH>* q, int first) {
   constexpr int NBX = (RW + 7) / 8, NBY = (RH + 3) / 4, NB = NBX * NBY;
   static_assert(NB <= kMaxAnchors && NB <= NT, "anchor table too small");
   if (f.warp.kind == WARP_ALIGNED) return;
-  const bool fast_ok = f.warp.kind == WARP_HOMOGRAPHY && !f.warp.guard;
+  const bool fast_ok = f.warp.kind == WARP_HOMOGRAPHY && !f.warp.guard && f.src.w >= 4 && f.src.h >= 4;
   if ((int)threadIdx.x == first) q->count = 0;
   const int b = (int)threadIdx.x - first;
   if (b >= 0 && b < NB) {
@@ -166,27 +204,46 @@ __device__ __forceinline__ void region_anchors(const FrameIn& f, int rx0, int ry
   }
 }
 
-// Remap of the region: the anchors (region_anchors) are in place.
-template <int RW, int RH, int KS = RW>
-__device__ void fill_region(const FrameIn& f, int W, int H, int rx0, int ry0, uint32_t* reg, uint32_t* kv,
-                            ExactQueue* q) {
+// Remap of the region: the anchors (region_anchors) are in place.  Writes
+// the packed samples of the region's window [RB, RW - RB) x [RB, RH - RB)
+// into `reg` (row stride RW - 2 RB; RB = 0: the whole region) and the 16-bit
+// contrast words of the whole region into `kv` (row stride KS).  CH = 3: RGB
+// sources (remap and aligned); CH = 0: the channel count read at run time
+// (gray remap sources, RGBA aligned frames).  The frame's source fields are
+// read into registers once per region.
+template <int RW, int RH, int KS, int CH = 0, int RB = 0>
+__device__ void fill_region(const FrameIn& f, int W, int H, int rx0, int ry0, uint32_t* reg, uint16_t* kv,
+                            RegionQueue<RW, RH>* q) {
+  constexpr int GW = RW - 2 * RB, GH = RH - 2 * RB;
+  auto put = [&](int i, int rx, int ry, uint32_t v, uint32_t w) {
+    if (RB == 0) {
+      reg[i] = v;
+    } else if ((unsigned)(rx - RB) < (unsigned)GW && (unsigned)(ry - RB) < (unsigned)GH) {
+      reg[(ry - RB) * GW + rx - RB] = v;
+    }
+    kv[i + ry * (KS - RW)] = (uint16_t)w;
+  };
+  // region fully inside the ROI: no per-pixel bounds test
+  const bool inside = rx0 >= 0 && ry0 >= 0 && rx0 + RW <= W && ry0 + RH <= H;
   if (f.warp.kind == WARP_ALIGNED) {
+    const uint8_t* px = f.src.px;
+    const int64_t pitch = f.src.pitch;
+    const int ch = CH ? CH : f.src.ch;
     for (int i = threadIdx.x; i < RW * RH; i += NT) {
-      const int rx = i % RW, ry = i / RW;
+      const int ry = i / RW, rx = i - ry * RW;
       const int X = rx0 + rx, Y = ry0 + ry;
       uint32_t v = 0;
-      if (X >= 0 && Y >= 0 && X < W && Y < H) {
-        const uint8_t* p = f.src.px + (int64_t)Y * f.src.pitch + (int64_t)X * f.src.ch;
-        const uint32_t al = f.src.ch == 4 ? (uint32_t)__ldg(p + 3) : 255u;
+      if (inside || ((unsigned)X < (unsigned)W && (unsigned)Y < (unsigned)H)) {
+        const uint8_t* p = px + (int64_t)Y * pitch + X * ch;
+        const uint32_t al = ch == 4 ? (uint32_t)__ldg(p + 3) : 255u;
         v = pack_rgba(__ldg(p), __ldg(p + 1), __ldg(p + 2), al);
       }
-      reg[i] = v;
-      if (kv) kv[ry * KS + rx] = contrast_word(v);
+      put(i, rx, ry, v, contrast_word(v));
     }
     return;
   }
-  constexpr int NBX = (RW + 7) / 8, NBY = (RH + 3) / 4, NB = NBX * NBY;
-  static_assert(NB <= kMaxAnchors, "anchor table too small");
+  constexpr int NBX = (RW + 7) / 8;
+  const TapSrc src = tap_src(f.src, f.warp.tie_band);
   // region pixels in row order over all threads (a warp's 32 pixels lie in
   // one or two rows: coalesced taps and stores, and no idle lanes in the
   // region's last block column); each reads its 8x4 block's anchor
@@ -194,105 +251,96 @@ __device__ void fill_region(const FrameIn& f, int W, int H, int rx0, int ry0, ui
     const int ry = i / RW, rx = i - ry * RW;
     const int du = rx & 7, dv = ry & 3;
     const Anchor an = q->anchor[(ry >> 2) * NBX + (rx >> 3)];
-    const int X = rx0 + rx, Y = ry0 + ry;
-    uint32_t v = 0;
-    if (X >= 0 && Y >= 0 && X < W && Y < H) {
+    uint32_t v = 0, w = 0;
+    if (inside || ((unsigned)(rx0 + rx) < (unsigned)W && (unsigned)(ry0 + ry) < (unsigned)H)) {
       if (an.ix == kNoAnchor) {
-        v = sample_exact(f.warp, f.src, X, Y);  // whole block without an anchor (guarded / lens poses)
-      } else if (!sample_try(f.src, an, du, dv, &v)) {
+        v = sample_exact(f.warp, f.src, rx0 + rx, ry0 + ry);  // whole block without an anchor (guarded / lens poses)
+        w = contrast_word(v);
+      } else if (!sample_try<CH>(src, an, (float)du, (float)dv, du, dv, &v, &w)) {
         const uint32_t slot = atomicAdd(&q->count, 1u);
         if (slot < (uint32_t)kExactQueue) {
           q->item[slot] = ((uint32_t)ry << 16) | (uint32_t)rx;
           continue;  // filled after the fast pass
         }
-        v = sample_exact(f.warp, f.src, X, Y);
+        v = sample_exact(f.warp, f.src, rx0 + rx, ry0 + ry);
+        w = contrast_word(v);
       }
     }
-    reg[ry * RW + rx] = v;
-    if (kv) kv[ry * KS + rx] = contrast_word(v);
+    put(i, rx, ry, v, w);
   }
   __syncthreads();
   const uint32_t n = min(q->count, (uint32_t)kExactQueue);
   for (uint32_t i = threadIdx.x; i < n; i += NT) {
     const int rx = (int)(q->item[i] & 0xFFFFu), ry = (int)(q->item[i] >> 16);
     const uint32_t v = sample_exact(f.warp, f.src, rx0 + rx, ry0 + ry);
-    reg[ry * RW + rx] = v;
-    if (kv) kv[ry * KS + rx] = contrast_word(v);
+    put(ry * RW + rx, rx, ry, v, contrast_word(v));
   }
 }
 
 }  // namespace
 
 // ======================================================== remap + weights
-// Shared memory: region of packed samples and contrast words ((TW + 2B) x
-// (TH + 2B)), horizontal window sums (TW x (TH + 2B)), 1/den table.
+// Shared memory: the tile's packed samples (TW x TH), the region's 16-bit
+// contrast words ((TW + 2B) x (TH + 2B)), horizontal window sums (TW x
+// (TH + 2B)), the tile's weight sums (TW x TH), 1/den table, anchors and the
+// exact queue: about 44 KB for the 5x5 window; four CTAs per SM (64 registers a thread).
 template <int B>
 struct RWLayout {
   static constexpr int RW = TW + 2 * B, RH = TH + 2 * B;
-  static constexpr int KS = RW + 1, HS = TW + 1;  // odd strides: lanes on consecutive rows hit distinct banks
+  static constexpr int KS = kv_stride(RW), HS = TW + 1;  // odd word strides: lanes on consecutive rows hit distinct banks
   static constexpr int NWIN = (2 * B + 1) * (2 * B + 1);
-  static constexpr size_t bytes =
-      (size_t)RW * RH * 4 + (size_t)KS * RH * 4 + (size_t)RH * HS * 4 * 2 + (NWIN + 1) * 4 + sizeof(ExactQueue) + 16;
+  static constexpr size_t bytes = (size_t)TW * TH * 4 + (size_t)KS * RH * 2 + (size_t)RH * HS * 4 * 2 +
+                                  (size_t)TW * TH * 4 + (NWIN + 1) * 4 + sizeof(RegionQueue<RW, RH>) + 16;
 };
 
-template <int B>
-__global__ void __launch_bounds__(NT, 5) remap_weights_kernel(const __grid_constant__ RemapWeightArgs a) {
+template <int B, int CH>
+__global__ void __launch_bounds__(NT, 4) remap_weights_kernel(const __grid_constant__ RemapWeightArgs a) {
   using Lay = RWLayout<B>;
   constexpr int RW = Lay::RW, RH = Lay::RH, KS = Lay::KS, HS = Lay::HS;
   extern __shared__ __align__(16) uint8_t smem[];
-  uint32_t* reg = (uint32_t*)smem;
-  uint32_t* kv = reg + RW * RH;
-  uint32_t* h1 = kv + KS * RH;   // packed count | gray sum, rows x TW (stride HS)
-  uint32_t* h2 = h1 + RH * HS;   // sum of k^2
-  float* inv_den = (float*)(h2 + RH * HS);
-  ExactQueue* queue = (ExactQueue*)(((uintptr_t)(inv_den + Lay::NWIN + 1) + 15) & ~(uintptr_t)15);
+  uint32_t* reg = (uint32_t*)smem;              // tile samples, TW x TH
+  uint16_t* kv = (uint16_t*)(reg + TW * TH);    // region contrast words, stride KS
+  uint32_t* h1 = (uint32_t*)(kv + KS * RH);     // packed count | gray sum, rows x TW (stride HS)
+  uint32_t* h2 = h1 + RH * HS;                  // sum of k^2
+  float* wsum = (float*)(h2 + RH * HS);         // the tile's weight sums over the batch so far
+  float* inv_den = wsum + TW * TH;
+  auto* queue = (RegionQueue<RW, RH>*)(((uintptr_t)(inv_den + Lay::NWIN + 1) + 15) & ~(uintptr_t)15);
   const int x0 = blockIdx.x * TW, y0 = blockIdx.y * TH;
   for (int n = threadIdx.x; n <= Lay::NWIN; n += NT)
     inv_den[n] = n > 1 ? 1.0f / ((float)(n * (n - 1)) * 585225.0f) : 0.0f;
-  // vertical stage ownership: column vc, rows vr0 .. vr0 + 7 (fixed for all frames)
+  // vertical stage ownership: column vc, rows vr0 .. vr0 + 7 (fixed for all
+  // frames); per own row whether it lies in the ROI (rows_in) and whether its
+  // whole contrast window does (win_rows)
   const int vc = threadIdx.x % TW, vr0 = (threadIdx.x / TW) * PPT;
-  float nacc[PPT];
-  uint32_t umask = 0;
+  float* const nacc = wsum + vr0 * TW + vc;  // row i at nacc[i * TW]
+  uint32_t umask = 0, rows_in = 0, win_rows = 0;
   const int X = x0 + vc;
+  const int64_t obase = (int64_t)(y0 + vr0) * a.pitch + X;
 #pragma unroll
   for (int i = 0; i < PPT; ++i) {
     const int Y = y0 + vr0 + i;
-    nacc[i] = 0.0f;
-    if (a.accumulate && !a.first && X < a.W && Y < a.H) {
-      nacc[i] = a.norm[(int64_t)Y * a.pitch + X];
-      if (a.uni[(int64_t)Y * a.pitch + X]) umask |= 1u << i;
+    float n0 = 0.0f;
+    if (X < a.W && Y < a.H) {
+      rows_in |= 1u << i;
+      if (a.window_ok && X >= B && Y >= B && X < a.W - B && Y < a.H - B) win_rows |= 1u << i;
+      if (a.accumulate && !a.first) {
+        n0 = a.norm[obase + (int64_t)i * a.pitch];
+        if (a.uni[obase + (int64_t)i * a.pitch]) umask |= 1u << i;
+      }
     }
+    nacc[i * TW] = n0;
   }
   constexpr int kAnchorThreads = ((RW + 7) / 8) * ((RH + 3) / 4);
   if (a.K > 0) region_anchors<RW, RH>(a.f[0], x0 - B, y0 - B, queue, 0);
   __syncthreads();
   for (int k = 0; k < a.K; ++k) {
-    fill_region<RW, RH, KS>(a.f[k], a.W, a.H, x0 - B, y0 - B, reg, kv, queue);
+    fill_region<RW, RH, KS, CH, B>(a.f[k], a.W, a.H, x0 - B, y0 - B, reg, kv, queue);
     __syncthreads();
     // horizontal sliding window sums: region row r, output columns c0 .. c0+7,
     // window = region columns [c, c + 2B]
     for (int it = threadIdx.x; it < RH * (TW / 8); it += NT) {
       const int r = it % RH, c0 = (it / RH) * 8;
-      const uint32_t* row = kv + r * KS + c0;
-      uint32_t p = 0, q = 0;
-#pragma unroll
-      for (int t = 0; t <= 2 * B; ++t) {
-        const uint32_t v = row[t];
-        const uint32_t g = v & 0xFFFFFu;
-        p += v;
-        q += g * g;
-      }
-      h1[r * HS + c0] = p;
-      h2[r * HS + c0] = q;
-#pragma unroll
-      for (int c = 1; c < 8; ++c) {
-        const uint32_t vin = row[c + 2 * B], vout = row[c - 1];
-        const uint32_t gin = vin & 0xFFFFFu, gout = vout & 0xFFFFFu;
-        p += vin - vout;
-        q += gin * gin - gout * gout;
-        h1[r * HS + c0 + c] = p;
-        h2[r * HS + c0 + c] = q;
-      }
+      window_row8<B>(kv + r * KS + c0, h1 + r * HS + c0, h2 + r * HS + c0);
     }
     // the next frame's anchors, on the threads with one row item (the last ones)
     if (k + 1 < a.K) region_anchors<RW, RH>(a.f[k + 1], x0 - B, y0 - B, queue, NT - kAnchorThreads);
@@ -305,27 +353,26 @@ __global__ void __launch_bounds__(NT, 5) remap_weights_kernel(const __grid_const
         p += h1[(vr0 + t) * HS + vc];
         q += h2[(vr0 + t) * HS + vc];
       }
-      const FramePlanes& out = a.out[k];
+      float* const wout = a.out[k].w;
+      uint32_t* const rout = a.out[k].rgba;
 #pragma unroll
       for (int i = 0; i < PPT; ++i) {
         if (i > 0) {
           p += h1[(vr0 + i + 2 * B) * HS + vc] - h1[(vr0 + i - 1) * HS + vc];
           q += h2[(vr0 + i + 2 * B) * HS + vc] - h2[(vr0 + i - 1) * HS + vc];
         }
-        const int Y = y0 + vr0 + i;
-        if (X >= a.W || Y >= a.H) continue;
-        const uint32_t own = reg[(vr0 + i + B) * RW + (vc + B)];
+        if (!((rows_in >> i) & 1u)) continue;
+        const uint32_t own = reg[(vr0 + i) * TW + vc];
         const uint32_t al = px_alpha(own);
         float w = 0.0f;
-        if (a.window_ok && al > 0 && X >= B && Y >= B && X < a.W - B && Y < a.H - B)
-          w = __fmul_rn(window_stddev<B>(p, q, inv_den), alpha_support(al));
+        if (((win_rows >> i) & 1u) && al > 0) w = __fmul_rn(window_stddev<B>(p, q, inv_den), alpha_support(al));
         if (a.accumulate) {
-          nacc[i] = __fadd_rn(nacc[i], w);
+          nacc[i * TW] = __fadd_rn(nacc[i * TW], w);
           if (al > 0) umask |= 1u << i;
         }
-        const int64_t o = (int64_t)Y * a.pitch + X;
-        if (out.w) out.w[o] = w;
-        if (out.rgba) out.rgba[o] = own;
+        const int64_t o = obase + (int64_t)i * a.pitch;
+        if (wout) wout[o] = w;
+        if (rout) rout[o] = own;
       }
     }
     __syncthreads();
@@ -333,26 +380,32 @@ __global__ void __launch_bounds__(NT, 5) remap_weights_kernel(const __grid_const
   if (a.accumulate) {
 #pragma unroll
     for (int i = 0; i < PPT; ++i) {
-      const int Y = y0 + vr0 + i;
-      if (X < a.W && Y < a.H) {
-        a.norm[(int64_t)Y * a.pitch + X] = nacc[i];
-        a.uni[(int64_t)Y * a.pitch + X] = (uint8_t)((umask >> i) & 1u);
+      if ((rows_in >> i) & 1u) {
+        a.norm[obase + (int64_t)i * a.pitch] = nacc[i * TW];
+        a.uni[obase + (int64_t)i * a.pitch] = (uint8_t)((umask >> i) & 1u);
       }
     }
   }
 }
 
-template <int B>
-static cudaError_t launch_rw(const RemapWeightArgs& a, cudaStream_t s) {
+template <int B, int CH>
+static cudaError_t launch_rw_ch(const RemapWeightArgs& a, cudaStream_t s) {
   static DeviceOnce configured;
   const size_t sm = RWLayout<B>::bytes;
   cudaError_t e = configured.run([&] {
-    return cudaFuncSetAttribute(remap_weights_kernel<B>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    return cudaFuncSetAttribute(remap_weights_kernel<B, CH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   });
   if (e != cudaSuccess) return e;
   dim3 grid((a.W + TW - 1) / TW, (a.H + TH - 1) / TH);
-  remap_weights_kernel<B><<<grid, NT, sm, s>>>(a);
+  remap_weights_kernel<B, CH><<<grid, NT, sm, s>>>(a);
   return cudaGetLastError();
+}
+
+// RGB frames (the frames of a batch share their channel count) take the
+// kernel with three channels compiled in
+template <int B>
+static cudaError_t launch_rw(const RemapWeightArgs& a, cudaStream_t s) {
+  return a.K > 0 && a.f[0].src.ch == 3 ? launch_rw_ch<B, 3>(a, s) : launch_rw_ch<B, 0>(a, s);
 }
 
 cudaError_t launch_remap_weights(const RemapWeightArgs& a, int border, cudaStream_t s) {
@@ -1817,7 +1870,7 @@ struct Lap0Layout {
   static constexpr int R0 = B > 4 ? B : 4;  // region halo left / top (REDUCE of the level-1 halo needs 4)
   static constexpr int R1 = B > 3 ? B : 3;  // right / bottom
   static constexpr int RW = TW + R0 + R1, RH = TH + R0 + R1;
-  static constexpr int KS = RW + 1;         // contrast-word row stride (odd: distinct banks per row)
+  static constexpr int KS = kv_stride(RW);  // contrast-word row stride (odd words: distinct banks per row)
   static constexpr int CH = TH + 2 * B;     // rows of the window sums
   static constexpr int HS = TW + 1;
   static constexpr int NWIN = (2 * B + 1) * (2 * B + 1);
@@ -1829,9 +1882,9 @@ struct Lap0Layout {
 template <int B>
 struct __align__(16) Lap0Smem {
   using Lay = Lap0Layout<B>;
-  ExactQueue queue;
+  RegionQueue<Lay::RW, Lay::RH> queue;
   uint32_t reg[Lay::RH * Lay::RW];   // remapped RGBA words of the region
-  uint32_t kv[Lay::RH * Lay::KS];    // contrast words of the region
+  uint16_t kv[Lay::RH * Lay::KS];    // contrast words of the region
   union {
     struct {
       uint32_t h1[Lay::CH * Lay::HS];  // horizontal window sums: count | gray sum
@@ -1910,26 +1963,7 @@ __global__ void __launch_bounds__(NT, 2) lap0_kernel(const __grid_constant__ Lap
     for (int it = threadIdx.x; it < kWinItems + kRedItems; it += NT) {
       if (it < kWinItems) {
         const int r = it % Lay::CH, c0 = (it / Lay::CH) * 8;
-        const uint32_t* row = S.kv + (r + R0 - B) * KS + c0 + R0 - B;
-        uint32_t p = 0, q = 0;
-#pragma unroll
-        for (int t = 0; t <= 2 * B; ++t) {
-          const uint32_t v = row[t];
-          const uint32_t g = v & 0xFFFFFu;
-          p += v;
-          q += g * g;
-        }
-        S.u.win.h1[r * HS + c0] = p;
-        S.u.win.h2[r * HS + c0] = q;
-#pragma unroll
-        for (int c = 1; c < 8; ++c) {
-          const uint32_t vin = row[c + 2 * B], vout = row[c - 1];
-          const uint32_t gin = vin & 0xFFFFFu, gout = vout & 0xFFFFFu;
-          p += vin - vout;
-          q += gin * gin - gout * gout;
-          S.u.win.h1[r * HS + c0 + c] = p;
-          S.u.win.h2[r * HS + c0 + c] = q;
-        }
+        window_row8<B>(S.kv + (r + R0 - B) * KS + c0 + R0 - B, S.u.win.h1 + r * HS + c0, S.u.win.h2 + r * HS + c0);
       } else {
         const int j = it - kWinItems;
         const int r = j % Lay::RRows, jj = 2 * (j / Lay::RRows);

@@ -8,11 +8,13 @@
 //    (fs_common.h, Warp);
 //  * FAST path: per 8x4 pixel block an FP64 anchor is formed once (split
 //    into two FP32 words), and each pixel's position offset from the anchor
-//    is a small FP32 rational (error < 1e-7 px).  The FP32 bilinear value is
-//    then within 1e-4 of the exact one; when every channel's value is farther
-//    than kTieBand from a .5 rounding boundary and the 4 taps lie at least
-//    one pixel inside the frame, the result is certain and equals the
-//    reference's;
+//    is a small FP32 rational (error < 1e-7 px for near-identity maps).  The
+//    FP32 bilinear value is then within 1e-4 of the exact one; when every
+//    channel's value is farther than the frame's tie band from a .5 rounding
+//    boundary and the 4 taps lie at least one pixel inside the frame, the
+//    result is certain and equals the reference's.  The band is kTieBand or
+//    more: the host widens it from the map's error bound (Warp::tie_band);
+//    maps far from the identity take wider bands and the exact path more often;
 //  * EXACT path (edge band, near-ties, guarded or lens poses): the
 //    reference's f64 sampler op for op (products and sums rounded one by one,
 //    no fused multiply-add), with its edge rules (soft support, alpha =
@@ -241,59 +243,109 @@ __device__ __forceinline__ uint32_t round_near_u8(float v, float* dist) {
   return (uint32_t)min(max(r, 0), 255);
 }
 
-// Fast path only: returns false (leaving *out untouched) when the exact
-// path must decide the sample.
-__device__ __forceinline__ bool sample_try(const SrcImage& s, const Anchor& a, int du, int dv, uint32_t* out) {
-  float fdu = (float)du, fdv = (float)dv;
-  float gd = fmaf(a.gam, fdu, a.eta * fdv);
-  float den = 1.0f + gd;
-  float nx = fmaf(a.am1x, fdu, a.bx * fdv) - fdu * gd;
-  float ny = fmaf(a.ay, fdu, a.bm1y * fdv) - fdv * gd;
-  float rd = __fdividef(1.0f, den);
-  float tx = a.fxh + fmaf(nx, rd, a.fxl);
-  float ty = a.fyh + fmaf(ny, rd, a.fyl);
+// A frame's source for the fast sampler, held in registers for the whole
+// region (CH = 3: RGB, 1: gray; 0: read at run time from `ch`).
+struct TapSrc {
+  const uint8_t* px;
+  uint32_t pitch;  // bytes per row
+  uint32_t xm, ym;  // fast taps need 1 <= x0 <= w - 3: (unsigned)(x0 - 1) <= w - 4 (w, h >= 4)
+  int32_t ch;
+  float lim;        // 0.5 - tie band
+};
+
+__device__ __forceinline__ TapSrc tap_src(const SrcImage& s, float tie_band) {
+  TapSrc t;
+  t.px = s.px;
+  t.pitch = (uint32_t)s.pitch;
+  t.xm = (uint32_t)(s.w - 4);
+  t.ym = (uint32_t)(s.h - 4);
+  t.ch = s.ch;
+  t.lim = 0.5f - fmaxf(tie_band, kTieBand);
+  return t;
+}
+
+// Support flag of a 16-bit contrast word (gray sum R + G + B in bits 0..14).
+static constexpr uint32_t kSupportFlag = 1u << 15;
+
+// Contrast word of a supported sample from its three channel floats
+// 1.5 * 2^23 + c: gray sum R + G + B with the support flag.
+__device__ __forceinline__ uint32_t biased_contrast_word(float r, float g, float b) {
+  return __float_as_uint(r) + __float_as_uint(g) + __float_as_uint(b) + (kSupportFlag - 3u * 0x4B400000u);
+}
+
+// Fast path only: returns false (leaving *out untouched) when the exact path
+// must decide the sample.  On success *out is the packed sample (alpha 255)
+// and *kw its contrast word.  The source fields sit in registers (TapSrc),
+// the tap addresses are one 32 x 32 -> 64-bit multiply-add per row and the
+// taps are byte loads at immediate offsets from the two row pointers.
+template <int CH>
+__device__ __forceinline__ bool sample_try(const TapSrc& s, const Anchor& a, float fdu, float fdv, int du, int dv,
+                                           uint32_t* out, uint32_t* kw) {
+  const float gd = fmaf(a.gam, fdu, a.eta * fdv);
+  const float rd = __fdividef(1.0f, 1.0f + gd);
+  const float nx = fmaf(a.am1x, fdu, a.bx * fdv) - fdu * gd;
+  const float ny = fmaf(a.ay, fdu, a.bm1y * fdv) - fdv * gd;
+  const float tx = a.fxh + fmaf(nx, rd, a.fxl);
+  const float ty = a.fyh + fmaf(ny, rd, a.fyl);
   int ixf, iyf;
   const float flx = floor_small(tx, &ixf), fly = floor_small(ty, &iyf);
-  int x0 = a.ix + du + ixf;
-  int y0 = a.iy + dv + iyf;
-  float fx = tx - flx, fy = ty - fly;
-  if (x0 < 1 || y0 < 1 || x0 > s.w - 3 || y0 > s.h - 3) return false;
-  float v00[3], v10[3], v01[3], v11[3];
-  load_rgb_biased(s, x0, y0, v00);
-  load_rgb_biased(s, x0 + 1, y0, v10);
-  load_rgb_biased(s, x0, y0 + 1, v01);
-  load_rgb_biased(s, x0 + 1, y0 + 1, v11);
+  const int x0 = a.ix + du + ixf;
+  const int y0 = a.iy + dv + iyf;
+  // taps at least one pixel inside on every side: the floor decision then
+  // cannot change which sampler the reference takes
+  if ((uint32_t)(x0 - 1) > s.xm || (uint32_t)(y0 - 1) > s.ym) return false;
+  const float fx = tx - flx, fy = ty - fly;
+  const int ch = CH ? CH : s.ch;
+  const uint8_t* r0 = s.px + ((uint64_t)(uint32_t)y0 * s.pitch + (uint32_t)(x0 * ch));
+  const uint8_t* r1 = r0 + s.pitch;
   const float fxy = fx * fy;
-  // red and green as FP32 pairs (each lane of a pair rounds exactly like the
-  // scalar operation: a - b is fma(b, -1, a)), blue alone; the same
-  // operations in the same order as sample_fast
   const float2 m1 = make_float2(-1.0f, -1.0f);
-  const float2 a00 = make_float2(v00[0], v00[1]), a10 = make_float2(v10[0], v10[1]);
-  const float2 a01 = make_float2(v01[0], v01[1]), a11 = make_float2(v11[0], v11[1]);
+  const float2 M = make_float2(12582912.0f, 12582912.0f);
+  auto bf = [](uint8_t v) { return __uint_as_float(0x4B000000u | (uint32_t)v); };
+  if (CH == 1 || (CH == 0 && ch == 1)) {
+    // gray: one channel, replicated
+    const float v00 = bf(__ldg(r0)), v10 = bf(__ldg(r0 + 1)), v01 = bf(__ldg(r1)), v11 = bf(__ldg(r1 + 1));
+    const float e10 = v10 - v00, e01 = v01 - v00, e11 = (v11 - v10) - e01;
+    float v = fmaf(fx, e10, v00 - 8388608.0f);
+    v = fmaf(fy, e01, v);
+    v = fmaf(fxy, e11, v);
+    const float t = __fadd_rn(v, 12582912.0f);
+    const float d = __fsub_rn(v, __fsub_rn(t, 12582912.0f));
+    if (fabsf(d) > s.lim) return false;
+    const uint32_t g = __float_as_uint(t) & 255u;
+    *out = g * 0x010101u | 0xFF000000u;
+    *kw = 3u * g | kSupportFlag;
+    return true;
+  }
+  const float2 a00 = make_float2(bf(__ldg(r0)), bf(__ldg(r0 + 1)));
+  const float2 a10 = make_float2(bf(__ldg(r0 + ch)), bf(__ldg(r0 + ch + 1)));
+  const float2 a01 = make_float2(bf(__ldg(r1)), bf(__ldg(r1 + 1)));
+  const float2 a11 = make_float2(bf(__ldg(r1 + ch)), bf(__ldg(r1 + ch + 1)));
+  const float b00 = bf(__ldg(r0 + 2)), b10 = bf(__ldg(r0 + ch + 2));
+  const float b01 = bf(__ldg(r1 + 2)), b11 = bf(__ldg(r1 + ch + 2));
+  // red and green as FP32 pairs (each lane of a pair rounds exactly like the
+  // scalar operation: a - b is fma(b, -1, a)), blue alone
   const float2 d10 = __ffma2_rn(a00, m1, a10), d01 = __ffma2_rn(a00, m1, a01);
   const float2 d11 = __ffma2_rn(d01, m1, __ffma2_rn(a10, m1, a11));
   float2 v = __fadd2_rn(a00, make_float2(-8388608.0f, -8388608.0f));
   v = __ffma2_rn(make_float2(fx, fx), d10, v);
   v = __ffma2_rn(make_float2(fy, fy), d01, v);
   v = __ffma2_rn(make_float2(fxy, fxy), d11, v);
-  float vb;
-  {
-    const float e10 = v10[2] - v00[2], e01 = v01[2] - v00[2], e11 = (v11[2] - v10[2]) - e01;
-    vb = fmaf(fx, e10, v00[2] - 8388608.0f);
-    vb = fmaf(fy, e01, vb);
-    vb = fmaf(fxy, e11, vb);
-  }
+  const float e10 = b10 - b00, e01 = b01 - b00, e11 = (b11 - b10) - e01;
+  float vb = fmaf(fx, e10, b00 - 8388608.0f);
+  vb = fmaf(fy, e01, vb);
+  vb = fmaf(fxy, e11, vb);
   // nearest integers by adding and removing 1.5 * 2^23: t's low byte is the
   // integer (a bilinear value of bytes lies in [0, 255] up to ~1e-4)
-  const float2 M = make_float2(12582912.0f, 12582912.0f);
   const float2 t = __fadd2_rn(v, M);
   const float2 dl = __ffma2_rn(__fadd2_rn(t, make_float2(-12582912.0f, -12582912.0f)), m1, v);
   const float tb = __fadd_rn(vb, 12582912.0f);
   const float db = __fsub_rn(vb, __fsub_rn(tb, 12582912.0f));
   const float dmax = fmaxf(fmaxf(fabsf(dl.x), fabsf(dl.y)), fabsf(db));
-  if (dmax > 0.5f - kTieBand) return false;
+  if (dmax > s.lim) return false;
   const uint32_t rg = __byte_perm(__float_as_uint(t.x), __float_as_uint(t.y), 0x0040u);
   *out = __byte_perm(rg, __float_as_uint(tb), 0x0410u) | 0xFF000000u;
+  *kw = biased_contrast_word(t.x, t.y, tb);
   return true;
 }
 
@@ -335,7 +387,7 @@ __device__ __forceinline__ uint32_t sample_fast(const Warp& w, const SrcImage& s
     o[c] = round_near_u8(v, &d);
     dmax = fmaxf(dmax, d);
   }
-  const bool tie = dmax > 0.5f - kTieBand;
+  const bool tie = dmax > 0.5f - fmaxf(w.tie_band, kTieBand);
   if (tie) return sample_exact(w, s, X, Y);
   return pack_rgba(o[0], o[1], o[2], 255u);
 }

@@ -143,6 +143,8 @@ void radial_inverse(const fs_pose& p, double inv_norm, double dx, double dy, dou
 
 }  // namespace
 
+static float fast_tie_band(const Warp& w, double ow, double oh);
+
 bool compose_warp(const fs_pose& pose, uint32_t src_w, uint32_t src_h, const fs_rect& roi, Warp* out,
                   const char** why) {
   Composed c = compose(pose, src_w, src_h, roi);
@@ -189,11 +191,49 @@ bool compose_warp(const fs_pose& pose, uint32_t src_w, uint32_t src_h, const fs_
       dmin = std::min(dmin, 1.0 + n[2][0] * X + n[2][1] * Y);
     }
   w.guard = dmin < 0.25 ? 1 : 0;
+  w.tie_band = fast_tie_band(w, ow, oh);
+  if (!(w.tie_band < 0.05f)) w.guard = 1;  // the fast sampler would decide too little: exact path only
   w.behind_is_void = c.basic ? 1 : 0;
   // the reference's |denominator| < 1e-12 is on -local_z; D is that scaled by 1/|h22|
   w.eps_den = 1e-12 / std::fabs(h22);
   *out = w;
   return true;
+}
+
+// Tie band of the device's fast FP32 sampler for this map.  Per 8x4 block
+// the sampler takes the block anchor's FP64 position (fraction as two FP32
+// words) and adds the offset of pixel (du, dv) from it, the FP32 rational
+// (am1x du + bx dv - du (gam du + eta dv)) / (1 + gam du + eta dv) with
+// coefficients rounded to FP32 (and likewise for y).  With T the sum of
+// the absolute terms of that numerator, the position carries at most
+// ~10 roundings of relative 2^-24 on T plus half an ulp of |position| <= 1 + T:
+//   e_pos <= 2^-24 (1 + 11 T).
+// The bilinear value moves by at most 255 per pixel of either coordinate
+// and its own three FMAs round below 2^-16 each, so
+//   e_val <= 510 e_pos + 6e-5,
+// and twice that is the band.  T is largest at a corner of the ROI (the
+// coefficients are ratios of affine functions of X and Y), evaluated there
+// and at the centre with a 25% margin.
+static float fast_tie_band(const Warp& w, double ow, double oh) {
+  double T = 0.0;
+  const double pts[5][2] = {{0, 0}, {ow, 0}, {0, oh}, {ow, oh}, {ow * 0.5, oh * 0.5}};
+  for (const auto& pt : pts) {
+    const double X = pt[0], Y = pt[1];
+    const double D = 1.0 + w.g * X + w.h * Y;
+    if (!(std::fabs(D) > 1e-3)) return 1.0f;
+    const double dx = (w.a * X + w.b * Y + w.c - X * (w.g * X + w.h * Y)) / D;
+    const double dy = (w.d * X + w.e * Y + w.f - Y * (w.g * X + w.h * Y)) / D;
+    const double xa = X + dx, ya = Y + dy, dDa = D - 1.0;
+    const double am1x = (w.a - xa * w.g - dDa) / D, bx = (w.b - xa * w.h) / D;
+    const double ay = (w.d - ya * w.g) / D, bm1y = (w.e - ya * w.h - dDa) / D;
+    const double gd = std::fabs(w.g / D) * 7.0 + std::fabs(w.h / D) * 3.0;
+    T = std::max(T, std::fabs(am1x) * 7.0 + std::fabs(bx) * 3.0 + 7.0 * gd);
+    T = std::max(T, std::fabs(ay) * 7.0 + std::fabs(bm1y) * 3.0 + 3.0 * gd);
+  }
+  T *= 1.25;
+  const double e_pos = std::ldexp(1.0 + 11.0 * T, -24);
+  const double band = 2.0 * (510.0 * e_pos + 6e-5);
+  return (float)std::min(band, 1.0);
 }
 
 void inverse_map_point_f64(const fs_pose& pose, uint32_t w, uint32_t h, double x, double y, double* sx, double* sy) {
