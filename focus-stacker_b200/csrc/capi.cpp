@@ -307,8 +307,8 @@ bool build_frame_in(fs_stack* s, const fs_stack::Frame& fr, FrameIn* fi, std::st
 }
 
 // remap + weights for frames [begin, end): pass 1 (accumulate, and keep
-// the planes in CACHE mode) or pass 2 of RESIDENT / REFETCH (planes into the
-// batch slots, no accumulation).
+// the planes in CACHE / LAPS mode) or pass 2 of RESIDENT / REFETCH (planes
+// into the batch slots, no accumulation).
 int launch_remap_weights_batch(fs_stack* s, const std::vector<fs_stack::Frame>& frames, size_t begin, size_t end,
                                bool pass1) {
   RemapWeightArgs a;
@@ -326,8 +326,11 @@ int launch_remap_weights_batch(fs_stack* s, const std::vector<fs_stack::Frame>& 
     std::string why;
     if (!build_frame_in(s, frames[k], &a.f[k - begin], &why)) return set_err(s->ctx, FS_ERR_INVALID, why);
     if (pass1) {
+      // the weights are formed from the remapped words: modes that keep no
+      // planes in pass 1 remap into the (still unused) pass-2 batch slots
       if (s->mode == P2_CACHE) a.out[k - begin] = s->cache[k];
-      if (s->mode == P2_LAPS) a.out[k - begin] = FramePlanes{s->p2[k - begin].rgba, s->wplane[k]};
+      else if (s->mode == P2_LAPS) a.out[k - begin] = FramePlanes{s->p2[k - begin].rgba, s->wplane[k]};
+      else a.out[k - begin] = FramePlanes{s->p2[k - begin].rgba, nullptr};
     } else {
       a.out[k - begin] = s->p2[k - begin];
     }

@@ -280,99 +280,207 @@ __device__ void fill_region(const FrameIn& f, int W, int H, int rx0, int ry0, ui
 }  // namespace
 
 // ======================================================== remap + weights
-// Shared memory: the tile's packed samples (TW x TH), the region's 16-bit
-// contrast words ((TW + 2B) x (TH + 2B)), horizontal window sums (TW x
-// (TH + 2B)), the tile's weight sums (TW x TH), 1/den table, anchors and the
-// exact queue: about 44 KB for the 5x5 window; four CTAs per SM (64 registers a thread).
-template <int B>
-struct RWLayout {
-  static constexpr int RW = TW + 2 * B, RH = TH + 2 * B;
-  static constexpr int KS = kv_stride(RW), HS = TW + 1;  // odd word strides: lanes on consecutive rows hit distinct banks
-  static constexpr int NWIN = (2 * B + 1) * (2 * B + 1);
-  static constexpr size_t bytes = (size_t)TW * TH * 4 + (size_t)KS * RH * 2 + (size_t)RH * HS * 4 * 2 +
-                                  (size_t)TW * TH * 4 + (NWIN + 1) * 4 + sizeof(RegionQueue<RW, RH>) + 16;
+// Pass 1 in two kernels per batch of K frames:
+//  remap_tile_kernel   one frame per grid z: each 64x32 tile's samples,
+//                      written as packed RGBA words (the kept plane, or the
+//                      batch slot when the mode keeps none); no halo, so
+//                      every sample is taken once;
+//  weights_kernel<B>   each tile with its window halo read back from those
+//                      planes (L2), contrast words, sliding window sums, the
+//                      alpha-weighted standard deviation; pass 1 adds it to
+//                      the weight sum (frame order) and union support.
+
+namespace {
+
+constexpr int kTileBlocks = (TW / 8) * (TH / 4);  // 8x4 anchor blocks of a tile
+constexpr int kRowsPerThread = TW * TH / NT;      // tile rows a thread samples (column fixed)
+static_assert(NT % TW == 0 && (NT / TW) == 4 && kRowsPerThread * 4 == TH, "one anchor row per pass");
+
+struct __align__(16) RemapTileSmem {
+  Anchor anchor[kTileBlocks];
+  uint32_t count;
+  uint32_t overflow;
+  uint32_t item[kExactQueue];  // ry << 16 | rx
 };
 
-template <int B, int CH>
-__global__ void __launch_bounds__(NT, 4) remap_weights_kernel(const __grid_constant__ RemapWeightArgs a) {
-  using Lay = RWLayout<B>;
-  constexpr int RW = Lay::RW, RH = Lay::RH, KS = Lay::KS, HS = Lay::HS;
-  extern __shared__ __align__(16) uint8_t smem[];
-  uint32_t* reg = (uint32_t*)smem;              // tile samples, TW x TH
-  uint16_t* kv = (uint16_t*)(reg + TW * TH);    // region contrast words, stride KS
-  uint32_t* h1 = (uint32_t*)(kv + KS * RH);     // packed count | gray sum, rows x TW (stride HS)
-  uint32_t* h2 = h1 + RH * HS;                  // sum of k^2
-  float* wsum = (float*)(h2 + RH * HS);         // the tile's weight sums over the batch so far
-  float* inv_den = wsum + TW * TH;
-  auto* queue = (RegionQueue<RW, RH>*)(((uintptr_t)(inv_den + Lay::NWIN + 1) + 15) & ~(uintptr_t)15);
+}  // namespace
+
+// Thread t samples column rx = t % 64 of the tile at rows t / 64 + 4 j, so
+// its offsets (du, dv) inside the 8x4 blocks are fixed and block row j is
+// pass j; samples the fast path cannot decide are queued and taken exactly
+// after the pass (and, should the queue overflow, on a second pass).
+template <int CH>
+__global__ void __launch_bounds__(NT, 6) remap_tile_kernel(const __grid_constant__ RemapWeightArgs a) {
+  __shared__ RemapTileSmem S;
+  const int k = blockIdx.z;
+  const FrameIn& f = a.f[k];
+  uint32_t* const out = a.out[k].rgba;
+  const int x0 = blockIdx.x * TW, y0 = blockIdx.y * TH;
+  const int rx = threadIdx.x % TW, ry0 = threadIdx.x / TW;
+  const int X = x0 + rx;
+  const int64_t pitch = a.pitch;
+  // rows of this thread's column inside the ROI
+  const int nrows = X < a.W ? min(kRowsPerThread, (a.H - y0 - ry0 + 3) / 4) : 0;
+  uint32_t* const col = out + (int64_t)(y0 + ry0) * pitch + X;
+  if (f.warp.kind == WARP_ALIGNED) {
+    const int ch = CH ? CH : f.src.ch;
+    const uint8_t* p = f.src.px + (int64_t)(y0 + ry0) * f.src.pitch + (int64_t)X * ch;
+    for (int j = 0; j < nrows; ++j, p += 4 * f.src.pitch) {
+      const uint32_t al = ch == 4 ? (uint32_t)__ldg(p + 3) : 255u;
+      col[4 * j * pitch] = pack_rgba(__ldg(p), __ldg(p + 1), __ldg(p + 2), al);
+    }
+    return;
+  }
+  if (threadIdx.x < kTileBlocks) {
+    const bool fast_ok = f.warp.kind == WARP_HOMOGRAPHY && !f.warp.guard && f.src.w >= 4 && f.src.h >= 4;
+    const int b = threadIdx.x;
+    bool ok = false;
+    Anchor an = {};
+    if (fast_ok) an = make_anchor(f.warp, x0 + (b % (TW / 8)) * 8, y0 + (b / (TW / 8)) * 4, &ok);
+    if (!ok) an.ix = kNoAnchor;
+    S.anchor[b] = an;
+  }
+  if (threadIdx.x == 0) {
+    S.count = 0;
+    S.overflow = 0;
+  }
+  __syncthreads();
+  const int du = rx & 7, dv = ry0;
+  const float fdu = (float)du, fdv = (float)dv;
+  const TapSrc src = tap_src(f.src, f.warp.tie_band);
+  const Anchor* an_col = S.anchor + (rx >> 3);
+#pragma unroll 2
+  for (int j = 0; j < nrows; ++j) {
+    const Anchor an = an_col[j * (TW / 8)];
+    uint32_t v, w;
+    if (an.ix != kNoAnchor && sample_try<CH>(src, an, fdu, fdv, du, dv, &v, &w)) {
+      col[4 * j * pitch] = v;
+    } else {
+      const uint32_t slot = atomicAdd(&S.count, 1u);
+      if (slot < (uint32_t)kExactQueue) S.item[slot] = ((uint32_t)(ry0 + 4 * j) << 16) | (uint32_t)rx;
+      else S.overflow = 1;
+    }
+  }
+  __syncthreads();
+  const uint32_t n = min(S.count, (uint32_t)kExactQueue);
+  for (uint32_t i = threadIdx.x; i < n; i += NT) {
+    const int qx = (int)(S.item[i] & 0xFFFFu), qy = (int)(S.item[i] >> 16);
+    out[(int64_t)(y0 + qy) * pitch + x0 + qx] = sample_exact(f.warp, f.src, x0 + qx, y0 + qy);
+  }
+  if (S.overflow) {  // block-uniform: more undecided samples than the queue holds
+    for (int j = 0; j < nrows; ++j) {
+      const Anchor an = an_col[j * (TW / 8)];
+      uint32_t v, w;
+      if (!(an.ix != kNoAnchor && sample_try<CH>(src, an, fdu, fdv, du, dv, &v, &w)))
+        col[4 * j * pitch] = sample_exact(f.warp, f.src, X, y0 + ry0 + 4 * j);
+    }
+  }
+}
+
+namespace {
+
+// Weights kernel geometry: the region is the tile with the window halo B
+// (RW x RH); its rows are read from the RGBA planes in 16-byte chunks of
+// four words starting at column x0 - CB (CB = B rounded up to 4).
+template <int B>
+struct WLayout {
+  static constexpr int RW = TW + 2 * B, RH = TH + 2 * B;
+  static constexpr int CB = (B + 3) / 4 * 4;
+  static constexpr int CHUNKS = (TW + 2 * CB) / 4;  // chunks per region row
+  static constexpr int KS = kv_stride(RW), HS = TW + 1;
+  static constexpr int NWIN = (2 * B + 1) * (2 * B + 1);
+};
+
+template <int B>
+struct __align__(16) WeightsSmem {
+  using Lay = WLayout<B>;
+  uint16_t kv[Lay::RH * Lay::KS];   // contrast words of the region
+  uint8_t alpha[TW * TH];           // alpha of the tile's samples
+  uint32_t h1[Lay::RH * Lay::HS];   // horizontal window sums: count << 20 | gray sum
+  uint32_t h2[Lay::RH * Lay::HS];   // sum of gray^2
+  float inv_den[Lay::NWIN + 1];
+};
+
+}  // namespace
+
+template <int B>
+__global__ void __launch_bounds__(NT, 6) weights_kernel(const __grid_constant__ RemapWeightArgs a) {
+  using Lay = WLayout<B>;
+  constexpr int RH = Lay::RH, KS = Lay::KS, HS = Lay::HS, CB = Lay::CB, CHUNKS = Lay::CHUNKS;
+  extern __shared__ __align__(16) uint8_t smem_w[];
+  WeightsSmem<B>& S = *reinterpret_cast<WeightsSmem<B>*>(smem_w);
   const int x0 = blockIdx.x * TW, y0 = blockIdx.y * TH;
   for (int n = threadIdx.x; n <= Lay::NWIN; n += NT)
-    inv_den[n] = n > 1 ? 1.0f / ((float)(n * (n - 1)) * 585225.0f) : 0.0f;
-  // vertical stage ownership: column vc, rows vr0 .. vr0 + 7 (fixed for all
-  // frames); per own row whether it lies in the ROI (rows_in) and whether its
-  // whole contrast window does (win_rows)
+    S.inv_den[n] = n > 1 ? 1.0f / ((float)(n * (n - 1)) * 585225.0f) : 0.0f;
+  // own pixels: column vc, rows vr0 .. vr0 + 7; rows_in / win_rows as in
+  // the reference's window rule (the whole window inside the ROI)
   const int vc = threadIdx.x % TW, vr0 = (threadIdx.x / TW) * PPT;
-  float* const nacc = wsum + vr0 * TW + vc;  // row i at nacc[i * TW]
-  uint32_t umask = 0, rows_in = 0, win_rows = 0;
   const int X = x0 + vc;
   const int64_t obase = (int64_t)(y0 + vr0) * a.pitch + X;
+  float nacc[PPT];
+  uint32_t umask = 0, rows_in = 0, win_rows = 0;
 #pragma unroll
   for (int i = 0; i < PPT; ++i) {
     const int Y = y0 + vr0 + i;
-    float n0 = 0.0f;
+    nacc[i] = 0.0f;
     if (X < a.W && Y < a.H) {
       rows_in |= 1u << i;
       if (a.window_ok && X >= B && Y >= B && X < a.W - B && Y < a.H - B) win_rows |= 1u << i;
       if (a.accumulate && !a.first) {
-        n0 = a.norm[obase + (int64_t)i * a.pitch];
+        nacc[i] = a.norm[obase + (int64_t)i * a.pitch];
         if (a.uni[obase + (int64_t)i * a.pitch]) umask |= 1u << i;
       }
     }
-    nacc[i * TW] = n0;
   }
-  constexpr int kAnchorThreads = ((RW + 7) / 8) * ((RH + 3) / 4);
-  if (a.K > 0) region_anchors<RW, RH>(a.f[0], x0 - B, y0 - B, queue, 0);
-  __syncthreads();
   for (int k = 0; k < a.K; ++k) {
-    fill_region<RW, RH, KS, CH, B>(a.f[k], a.W, a.H, x0 - B, y0 - B, reg, kv, queue);
+    const uint32_t* plane = a.out[k].rgba;
+    // region rows -> contrast words (0 outside the ROI) and the tile's alpha
+    for (int it = threadIdx.x; it < RH * CHUNKS; it += NT) {
+      const int r = it / CHUNKS, c = it - r * CHUNKS;
+      const int Y = y0 - B + r, Xc = x0 - CB + 4 * c;  // first column of the chunk
+      uint4 q = make_uint4(0u, 0u, 0u, 0u);
+      if ((unsigned)Y < (unsigned)a.H && Xc >= 0 && Xc < a.W)
+        q = __ldg(reinterpret_cast<const uint4*>(plane + (int64_t)Y * a.pitch + Xc));
+      const uint32_t wv[4] = {q.x, q.y, q.z, q.w};
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const int rc = Xc + e - (x0 - B);  // region column
+        if ((unsigned)rc >= (unsigned)Lay::RW) continue;
+        const uint32_t v = Xc + e < a.W ? wv[e] : 0u;
+        S.kv[r * KS + rc] = (uint16_t)contrast_word(v);
+        if ((unsigned)(rc - B) < (unsigned)TW && (unsigned)(r - B) < (unsigned)TH)
+          S.alpha[(r - B) * TW + rc - B] = (uint8_t)px_alpha(v);
+      }
+    }
     __syncthreads();
-    // horizontal sliding window sums: region row r, output columns c0 .. c0+7,
-    // window = region columns [c, c + 2B]
     for (int it = threadIdx.x; it < RH * (TW / 8); it += NT) {
       const int r = it % RH, c0 = (it / RH) * 8;
-      window_row8<B>(kv + r * KS + c0, h1 + r * HS + c0, h2 + r * HS + c0);
+      window_row8<B>(S.kv + r * KS + c0, S.h1 + r * HS + c0, S.h2 + r * HS + c0);
     }
-    // the next frame's anchors, on the threads with one row item (the last ones)
-    if (k + 1 < a.K) region_anchors<RW, RH>(a.f[k + 1], x0 - B, y0 - B, queue, NT - kAnchorThreads);
     __syncthreads();
-    // vertical sliding sums down column vc -> weights of rows vr0 .. vr0+7
     {
       uint32_t p = 0, q = 0;
 #pragma unroll
       for (int t = 0; t <= 2 * B; ++t) {
-        p += h1[(vr0 + t) * HS + vc];
-        q += h2[(vr0 + t) * HS + vc];
+        p += S.h1[(vr0 + t) * HS + vc];
+        q += S.h2[(vr0 + t) * HS + vc];
       }
       float* const wout = a.out[k].w;
-      uint32_t* const rout = a.out[k].rgba;
 #pragma unroll
       for (int i = 0; i < PPT; ++i) {
         if (i > 0) {
-          p += h1[(vr0 + i + 2 * B) * HS + vc] - h1[(vr0 + i - 1) * HS + vc];
-          q += h2[(vr0 + i + 2 * B) * HS + vc] - h2[(vr0 + i - 1) * HS + vc];
+          p += S.h1[(vr0 + i + 2 * B) * HS + vc] - S.h1[(vr0 + i - 1) * HS + vc];
+          q += S.h2[(vr0 + i + 2 * B) * HS + vc] - S.h2[(vr0 + i - 1) * HS + vc];
         }
         if (!((rows_in >> i) & 1u)) continue;
-        const uint32_t own = reg[(vr0 + i) * TW + vc];
-        const uint32_t al = px_alpha(own);
+        const uint32_t al = S.alpha[(vr0 + i) * TW + vc];
         float w = 0.0f;
-        if (((win_rows >> i) & 1u) && al > 0) w = __fmul_rn(window_stddev<B>(p, q, inv_den), alpha_support(al));
+        if (((win_rows >> i) & 1u) && al > 0) w = __fmul_rn(window_stddev<B>(p, q, S.inv_den), alpha_support(al));
         if (a.accumulate) {
-          nacc[i * TW] = __fadd_rn(nacc[i * TW], w);
+          nacc[i] = __fadd_rn(nacc[i], w);
           if (al > 0) umask |= 1u << i;
         }
-        const int64_t o = obase + (int64_t)i * a.pitch;
-        if (wout) wout[o] = w;
-        if (rout) rout[o] = own;
+        if (wout) wout[obase + (int64_t)i * a.pitch] = w;
       }
     }
     __syncthreads();
@@ -381,42 +489,44 @@ __global__ void __launch_bounds__(NT, 4) remap_weights_kernel(const __grid_const
 #pragma unroll
     for (int i = 0; i < PPT; ++i) {
       if ((rows_in >> i) & 1u) {
-        a.norm[obase + (int64_t)i * a.pitch] = nacc[i * TW];
+        a.norm[obase + (int64_t)i * a.pitch] = nacc[i];
         a.uni[obase + (int64_t)i * a.pitch] = (uint8_t)((umask >> i) & 1u);
       }
     }
   }
 }
 
-template <int B, int CH>
-static cudaError_t launch_rw_ch(const RemapWeightArgs& a, cudaStream_t s) {
+template <int B>
+static cudaError_t launch_weights(const RemapWeightArgs& a, cudaStream_t s) {
   static DeviceOnce configured;
-  const size_t sm = RWLayout<B>::bytes;
-  cudaError_t e = configured.run([&] {
-    return cudaFuncSetAttribute(remap_weights_kernel<B, CH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-  });
+  const size_t sm = sizeof(WeightsSmem<B>);
+  cudaError_t e = configure(weights_kernel<B>, sm, &configured);
   if (e != cudaSuccess) return e;
   dim3 grid((a.W + TW - 1) / TW, (a.H + TH - 1) / TH);
-  remap_weights_kernel<B, CH><<<grid, NT, sm, s>>>(a);
+  weights_kernel<B><<<grid, NT, sm, s>>>(a);
   return cudaGetLastError();
 }
 
-// RGB frames (the frames of a batch share their channel count) take the
-// kernel with three channels compiled in
-template <int B>
-static cudaError_t launch_rw(const RemapWeightArgs& a, cudaStream_t s) {
-  return a.K > 0 && a.f[0].src.ch == 3 ? launch_rw_ch<B, 3>(a, s) : launch_rw_ch<B, 0>(a, s);
-}
-
+// Every frame's plane must hold RGBA words (the weights read them back) on
+// 16-byte aligned rows.  RGB frames (the frames of a batch share their
+// channel count) take the remap kernel with three channels compiled in.
 cudaError_t launch_remap_weights(const RemapWeightArgs& a, int border, cudaStream_t s) {
+  if (a.K < 1 || a.K > kMaxBatch || a.W < 1 || a.H < 1 || (a.pitch & 3)) return cudaErrorInvalidValue;
+  for (int k = 0; k < a.K; ++k)
+    if (!a.out[k].rgba || ((uintptr_t)a.out[k].rgba & 15)) return cudaErrorInvalidValue;
+  const dim3 grid((a.W + TW - 1) / TW, (a.H + TH - 1) / TH, a.K);
+  if (a.f[0].src.ch == 3) remap_tile_kernel<3><<<grid, NT, 0, s>>>(a);
+  else remap_tile_kernel<0><<<grid, NT, 0, s>>>(a);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
   switch (border) {
-    case 1: return launch_rw<1>(a, s);
-    case 2: return launch_rw<2>(a, s);
-    case 3: return launch_rw<3>(a, s);
-    case 4: return launch_rw<4>(a, s);
-    case 5: return launch_rw<5>(a, s);
-    case 6: return launch_rw<6>(a, s);
-    case 7: return launch_rw<7>(a, s);
+    case 1: return launch_weights<1>(a, s);
+    case 2: return launch_weights<2>(a, s);
+    case 3: return launch_weights<3>(a, s);
+    case 4: return launch_weights<4>(a, s);
+    case 5: return launch_weights<5>(a, s);
+    case 6: return launch_weights<6>(a, s);
+    case 7: return launch_weights<7>(a, s);
     default: return cudaErrorInvalidValue;
   }
 }
