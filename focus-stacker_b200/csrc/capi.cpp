@@ -298,6 +298,11 @@ bool build_frame_in(fs_stack* s, const fs_stack::Frame& fr, FrameIn* fi, std::st
     fi->warp.kind = WARP_ALIGNED;
     return true;
   }
+  // the remap addresses its taps with 32-bit offsets
+  if (s->bps == 1 && (uint64_t)fr.pitch * s->d.src_height >= (1ull << 32)) {
+    *why = "source frames of 4 GiB or more (row stride x height) are not supported";
+    return false;
+  }
   const char* w = nullptr;
   if (!compose_warp(fr.pose, s->d.src_width, s->d.src_height, s->roi, &fi->warp, &w)) {
     *why = w ? w : "invalid pose";

@@ -142,20 +142,18 @@ __device__ __forceinline__ float alpha_support(uint32_t al) {
 // Sample standard deviation of gray = k / 765 over the supported pixels of
 // the window, from exact integer sums (src/fuse/contrast.zig:284-290):
 // var = (n S2 - S1^2) / (n (n - 1) 765^2); inv_den[n] = 1 / (n (n-1) 765^2).
+// Without branches: inv_den[0] = inv_den[1] = 0 and a nonpositive numerator
+// clamped to 0 give the 0 of a window with fewer than two samples or no
+// spread.
 template <int B>
 __device__ __forceinline__ float window_stddev(uint32_t packed, uint32_t s2, const float* inv_den) {
   const int n = (int)(packed >> 20);
-  if (n <= 1) return 0.0f;
   const int s1 = (int)(packed & 0xFFFFFu);
   float num;
   if (B <= 3) {
-    int v = n * (int)s2 - s1 * s1;  // < 2^31 for windows up to 7x7
-    if (v <= 0) return 0.0f;
-    num = (float)v;
+    num = (float)max(n * (int)s2 - s1 * s1, 0);  // < 2^31 for windows up to 7x7
   } else {
-    long long v = (long long)n * s2 - (long long)s1 * s1;
-    if (v <= 0) return 0.0f;
-    num = (float)v;
+    num = (float)max((long long)n * s2 - (long long)s1 * s1, 0ll);
   }
   return sqrtf(num * inv_den[n]);
 }
@@ -297,7 +295,7 @@ constexpr int kRowsPerThread = TW * TH / NT;      // tile rows a thread samples 
 static_assert(NT % TW == 0 && (NT / TW) == 4 && kRowsPerThread * 4 == TH, "one anchor row per pass");
 
 struct __align__(16) RemapTileSmem {
-  Anchor anchor[kTileBlocks];
+  TileAnchor anchor[kTileBlocks];
   uint32_t count;
   uint32_t overflow;
   uint32_t item[kExactQueue];  // ry << 16 | rx
@@ -308,7 +306,9 @@ struct __align__(16) RemapTileSmem {
 // Thread t samples column rx = t % 64 of the tile at rows t / 64 + 4 j, so
 // its offsets (du, dv) inside the 8x4 blocks are fixed and block row j is
 // pass j; samples the fast path cannot decide are queued and taken exactly
-// after the pass (and, should the queue overflow, on a second pass).
+// after the pass (and, should the queue overflow, on a second pass).  CH:
+// channels of remapped sources (3 or 1); aligned frames read theirs at run
+// time.
 template <int CH>
 __global__ void __launch_bounds__(NT, 6) remap_tile_kernel(const __grid_constant__ RemapWeightArgs a) {
   __shared__ RemapTileSmem S;
@@ -323,7 +323,7 @@ __global__ void __launch_bounds__(NT, 6) remap_tile_kernel(const __grid_constant
   const int nrows = X < a.W ? min(kRowsPerThread, (a.H - y0 - ry0 + 3) / 4) : 0;
   uint32_t* const col = out + (int64_t)(y0 + ry0) * pitch + X;
   if (f.warp.kind == WARP_ALIGNED) {
-    const int ch = CH ? CH : f.src.ch;
+    const int ch = f.src.ch;
     const uint8_t* p = f.src.px + (int64_t)(y0 + ry0) * f.src.pitch + (int64_t)X * ch;
     for (int j = 0; j < nrows; ++j, p += 4 * f.src.pitch) {
       const uint32_t al = ch == 4 ? (uint32_t)__ldg(p + 3) : 255u;
@@ -337,8 +337,9 @@ __global__ void __launch_bounds__(NT, 6) remap_tile_kernel(const __grid_constant
     bool ok = false;
     Anchor an = {};
     if (fast_ok) an = make_anchor(f.warp, x0 + (b % (TW / 8)) * 8, y0 + (b / (TW / 8)) * 4, &ok);
-    if (!ok) an.ix = kNoAnchor;
-    S.anchor[b] = an;
+    TileAnchor t = tile_anchor(an);
+    if (!ok) t.kx = kNoTileAnchor;
+    S.anchor[b] = t;
   }
   if (threadIdx.x == 0) {
     S.count = 0;
@@ -347,14 +348,19 @@ __global__ void __launch_bounds__(NT, 6) remap_tile_kernel(const __grid_constant
   __syncthreads();
   const int du = rx & 7, dv = ry0;
   const float fdu = (float)du, fdv = (float)dv;
-  const TapSrc src = tap_src(f.src, f.warp.tie_band);
-  const Anchor* an_col = S.anchor + (rx >> 3);
+  // the frame's pixel (1, 1): tap offsets are (x0 - 1, y0 - 1) from it
+  const uint32_t spitch = (uint32_t)f.src.pitch;
+  const uint8_t* const org = f.src.px + spitch + CH;
+  const uint32_t xm = (uint32_t)(f.src.w - 4), ym = (uint32_t)(f.src.h - 4);
+  const float lim = 0.5f - fmaxf(f.warp.tie_band, kTieBand);
+  const TileAnchor* an_col = S.anchor + (rx >> 3);
+  const int64_t step = 4 * pitch;
 #pragma unroll 2
   for (int j = 0; j < nrows; ++j) {
-    const Anchor an = an_col[j * (TW / 8)];
-    uint32_t v, w;
-    if (an.ix != kNoAnchor && sample_try<CH>(src, an, fdu, fdv, du, dv, &v, &w)) {
-      col[4 * j * pitch] = v;
+    const TileAnchor an = an_col[j * (TW / 8)];
+    uint32_t v;
+    if (an.kx != kNoTileAnchor && sample_tile<CH>(org, spitch, xm, ym, lim, an, fdu, fdv, du, dv, &v)) {
+      col[j * step] = v;
     } else {
       const uint32_t slot = atomicAdd(&S.count, 1u);
       if (slot < (uint32_t)kExactQueue) S.item[slot] = ((uint32_t)(ry0 + 4 * j) << 16) | (uint32_t)rx;
@@ -369,25 +375,27 @@ __global__ void __launch_bounds__(NT, 6) remap_tile_kernel(const __grid_constant
   }
   if (S.overflow) {  // block-uniform: more undecided samples than the queue holds
     for (int j = 0; j < nrows; ++j) {
-      const Anchor an = an_col[j * (TW / 8)];
-      uint32_t v, w;
-      if (!(an.ix != kNoAnchor && sample_try<CH>(src, an, fdu, fdv, du, dv, &v, &w)))
-        col[4 * j * pitch] = sample_exact(f.warp, f.src, X, y0 + ry0 + 4 * j);
+      const TileAnchor an = an_col[j * (TW / 8)];
+      uint32_t v;
+      if (!(an.kx != kNoTileAnchor && sample_tile<CH>(org, spitch, xm, ym, lim, an, fdu, fdv, du, dv, &v)))
+        col[j * step] = sample_exact(f.warp, f.src, X, y0 + ry0 + 4 * j);
     }
   }
 }
 
 namespace {
 
-// Weights kernel geometry: the region is the tile with the window halo B
-// (RW x RH); its rows are read from the RGBA planes in 16-byte chunks of
-// four words starting at column x0 - CB (CB = B rounded up to 4).
+// Weights kernel geometry: the region is the tile with the window halo B;
+// its rows are read from the RGBA planes in 16-byte chunks of four words,
+// and its contrast words kept from column x0 - CB on (CB = B rounded up to
+// 4), so that every chunk lands whole (RX columns per row).
 template <int B>
 struct WLayout {
-  static constexpr int RW = TW + 2 * B, RH = TH + 2 * B;
+  static constexpr int RH = TH + 2 * B;
   static constexpr int CB = (B + 3) / 4 * 4;
-  static constexpr int CHUNKS = (TW + 2 * CB) / 4;  // chunks per region row
-  static constexpr int KS = kv_stride(RW), HS = TW + 1;
+  static constexpr int RX = TW + 2 * CB;
+  static constexpr int CHUNKS = RX / 4;  // chunks per region row
+  static constexpr int KS = kv_stride(RX), HS = TW + 1;
   static constexpr int NWIN = (2 * B + 1) * (2 * B + 1);
 };
 
@@ -398,8 +406,22 @@ struct __align__(16) WeightsSmem {
   uint8_t alpha[TW * TH];           // alpha of the tile's samples
   uint32_t h1[Lay::RH * Lay::HS];   // horizontal window sums: count << 20 | gray sum
   uint32_t h2[Lay::RH * Lay::HS];   // sum of gray^2
+  float asup[256];                  // alpha support f32(a) / 255
   float inv_den[Lay::NWIN + 1];
 };
+
+// Contrast words of two packed samples as one 32-bit pair (first in the low
+// half), in 16-bit lanes: gray sums of the bytes, support flag where alpha
+// is nonzero, zero where it is zero.
+__device__ __forceinline__ uint32_t contrast_pair(uint32_t v0, uint32_t v1) {
+  const uint32_t r = __byte_perm(v0, v1, 0x7470u) & 0x00FF00FFu;  // R0, R1 in lanes
+  const uint32_t g = __byte_perm(v0, v1, 0x7571u) & 0x00FF00FFu;
+  const uint32_t b = __byte_perm(v0, v1, 0x7672u) & 0x00FF00FFu;
+  const uint32_t al = __byte_perm(v0, v1, 0x7773u) & 0x00FF00FFu;
+  const uint32_t flag = (al + 0x7FFF7FFFu) & 0x80008000u;  // bit 15 of a lane set iff its alpha >= 1
+  const uint32_t keep = (flag >> 15) * 0xFFFFu;            // the lane's mask
+  return ((r + g + b) & keep) | flag;
+}
 
 }  // namespace
 
@@ -407,13 +429,15 @@ template <int B>
 __global__ void __launch_bounds__(NT, 6) weights_kernel(const __grid_constant__ RemapWeightArgs a) {
   using Lay = WLayout<B>;
   constexpr int RH = Lay::RH, KS = Lay::KS, HS = Lay::HS, CB = Lay::CB, CHUNKS = Lay::CHUNKS;
+  static_assert(kSupportFlag == 0x8000u, "contrast_pair writes the flag at bit 15");
   extern __shared__ __align__(16) uint8_t smem_w[];
   WeightsSmem<B>& S = *reinterpret_cast<WeightsSmem<B>*>(smem_w);
   const int x0 = blockIdx.x * TW, y0 = blockIdx.y * TH;
   for (int n = threadIdx.x; n <= Lay::NWIN; n += NT)
     S.inv_den[n] = n > 1 ? 1.0f / ((float)(n * (n - 1)) * 585225.0f) : 0.0f;
-  // own pixels: column vc, rows vr0 .. vr0 + 7; rows_in / win_rows as in
-  // the reference's window rule (the whole window inside the ROI)
+  for (int n = threadIdx.x; n < 256; n += NT) S.asup[n] = alpha_support((uint32_t)n);
+  // own pixels: column vc, rows vr0 .. vr0 + 7; rows_in / win_rows: in the
+  // ROI / with the whole window inside it (the reference's window rule)
   const int vc = threadIdx.x % TW, vr0 = (threadIdx.x / TW) * PPT;
   const int X = x0 + vc;
   const int64_t obase = (int64_t)(y0 + vr0) * a.pitch + X;
@@ -432,6 +456,7 @@ __global__ void __launch_bounds__(NT, 6) weights_kernel(const __grid_constant__ 
       }
     }
   }
+  const bool right_edge = x0 + TW + CB > a.W;  // chunks reaching past the ROI's last column
   for (int k = 0; k < a.K; ++k) {
     const uint32_t* plane = a.out[k].rgba;
     // region rows -> contrast words (0 outside the ROI) and the tile's alpha
@@ -439,23 +464,26 @@ __global__ void __launch_bounds__(NT, 6) weights_kernel(const __grid_constant__ 
       const int r = it / CHUNKS, c = it - r * CHUNKS;
       const int Y = y0 - B + r, Xc = x0 - CB + 4 * c;  // first column of the chunk
       uint4 q = make_uint4(0u, 0u, 0u, 0u);
-      if ((unsigned)Y < (unsigned)a.H && Xc >= 0 && Xc < a.W)
+      if ((unsigned)Y < (unsigned)a.H && Xc >= 0 && Xc < a.W) {
         q = __ldg(reinterpret_cast<const uint4*>(plane + (int64_t)Y * a.pitch + Xc));
-      const uint32_t wv[4] = {q.x, q.y, q.z, q.w};
-#pragma unroll
-      for (int e = 0; e < 4; ++e) {
-        const int rc = Xc + e - (x0 - B);  // region column
-        if ((unsigned)rc >= (unsigned)Lay::RW) continue;
-        const uint32_t v = Xc + e < a.W ? wv[e] : 0u;
-        S.kv[r * KS + rc] = (uint16_t)contrast_word(v);
-        if ((unsigned)(rc - B) < (unsigned)TW && (unsigned)(r - B) < (unsigned)TH)
-          S.alpha[(r - B) * TW + rc - B] = (uint8_t)px_alpha(v);
+        if (right_edge) {  // words past the last column are not samples
+          if (Xc + 1 >= a.W) q.y = 0u;
+          if (Xc + 2 >= a.W) q.z = 0u;
+          if (Xc + 3 >= a.W) q.w = 0u;
+        }
       }
+      uint32_t* kw = reinterpret_cast<uint32_t*>(S.kv + r * KS + 4 * c);
+      kw[0] = contrast_pair(q.x, q.y);
+      kw[1] = contrast_pair(q.z, q.w);
+      const int ar = r - B, ac = 4 * c - CB;
+      if ((unsigned)ar < (unsigned)TH && (unsigned)ac < (unsigned)TW)
+        *reinterpret_cast<uint32_t*>(S.alpha + ar * TW + ac) =
+            __byte_perm(__byte_perm(q.x, q.y, 0x0073u), __byte_perm(q.z, q.w, 0x0073u), 0x5410u);
     }
     __syncthreads();
     for (int it = threadIdx.x; it < RH * (TW / 8); it += NT) {
       const int r = it % RH, c0 = (it / RH) * 8;
-      window_row8<B>(S.kv + r * KS + c0, S.h1 + r * HS + c0, S.h2 + r * HS + c0);
+      window_row8<B>(S.kv + r * KS + c0 + CB - B, S.h1 + r * HS + c0, S.h2 + r * HS + c0);
     }
     __syncthreads();
     {
@@ -472,15 +500,14 @@ __global__ void __launch_bounds__(NT, 6) weights_kernel(const __grid_constant__ 
           p += S.h1[(vr0 + i + 2 * B) * HS + vc] - S.h1[(vr0 + i - 1) * HS + vc];
           q += S.h2[(vr0 + i + 2 * B) * HS + vc] - S.h2[(vr0 + i - 1) * HS + vc];
         }
-        if (!((rows_in >> i) & 1u)) continue;
         const uint32_t al = S.alpha[(vr0 + i) * TW + vc];
-        float w = 0.0f;
-        if (((win_rows >> i) & 1u) && al > 0) w = __fmul_rn(window_stddev<B>(p, q, S.inv_den), alpha_support(al));
+        // alpha 0 has support 0: the weight is 0 without a test
+        const float w = ((win_rows >> i) & 1u) ? __fmul_rn(window_stddev<B>(p, q, S.inv_den), S.asup[al]) : 0.0f;
         if (a.accumulate) {
           nacc[i] = __fadd_rn(nacc[i], w);
-          if (al > 0) umask |= 1u << i;
+          umask |= (al > 0 ? 1u : 0u) << i;
         }
-        if (wout) wout[obase + (int64_t)i * a.pitch] = w;
+        if (wout && ((rows_in >> i) & 1u)) wout[obase + (int64_t)i * a.pitch] = w;
       }
     }
     __syncthreads();
@@ -508,15 +535,21 @@ static cudaError_t launch_weights(const RemapWeightArgs& a, cudaStream_t s) {
 }
 
 // Every frame's plane must hold RGBA words (the weights read them back) on
-// 16-byte aligned rows.  RGB frames (the frames of a batch share their
-// channel count) take the remap kernel with three channels compiled in.
+// 16-byte aligned rows; remapped frames stay below 4 GiB (32-bit tap
+// offsets).  The frames of a batch share their channel count: the remap
+// kernel has it compiled in (RGB or gray; aligned frames read it).
 cudaError_t launch_remap_weights(const RemapWeightArgs& a, int border, cudaStream_t s) {
   if (a.K < 1 || a.K > kMaxBatch || a.W < 1 || a.H < 1 || (a.pitch & 3)) return cudaErrorInvalidValue;
-  for (int k = 0; k < a.K; ++k)
+  for (int k = 0; k < a.K; ++k) {
     if (!a.out[k].rgba || ((uintptr_t)a.out[k].rgba & 15)) return cudaErrorInvalidValue;
+    const SrcImage& src = a.f[k].src;
+    if (a.f[k].warp.kind != WARP_ALIGNED && (src.ch != a.f[0].src.ch || (src.ch != 1 && src.ch != 3) ||
+                                             (uint64_t)src.pitch * (uint64_t)src.h >= (1ull << 32)))
+      return cudaErrorInvalidValue;
+  }
   const dim3 grid((a.W + TW - 1) / TW, (a.H + TH - 1) / TH, a.K);
-  if (a.f[0].src.ch == 3) remap_tile_kernel<3><<<grid, NT, 0, s>>>(a);
-  else remap_tile_kernel<0><<<grid, NT, 0, s>>>(a);
+  if (a.f[0].src.ch == 1) remap_tile_kernel<1><<<grid, NT, 0, s>>>(a);
+  else remap_tile_kernel<3><<<grid, NT, 0, s>>>(a);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   switch (border) {

@@ -349,6 +349,99 @@ __device__ __forceinline__ bool sample_try(const TapSrc& s, const Anchor& a, flo
   return true;
 }
 
+// Block anchor of the tile sampler: the integer position pre-biased so that
+// one three-input add of the rounded-down float's bits gives x0 - 1 (see
+// sample_tile), the rest as in Anchor.
+struct __align__(16) TileAnchor {
+  int32_t kx, ky;  // ix - 1 - 0x4B400000, iy - 1 - 0x4B400000; kx == kNoTileAnchor: none
+  float fxh, fxl, fyh, fyl;
+  float am1x, bx, ay, bm1y, gam, eta;
+};
+static constexpr int32_t kNoTileAnchor = INT32_MIN;  // |ix| < 1e8 keeps kx far from it
+
+__device__ __forceinline__ TileAnchor tile_anchor(const Anchor& a) {
+  TileAnchor t;
+  t.kx = (int32_t)((uint32_t)a.ix - 1u - 0x4B400000u);
+  t.ky = (int32_t)((uint32_t)a.iy - 1u - 0x4B400000u);
+  t.fxh = a.fxh;
+  t.fxl = a.fxl;
+  t.fyh = a.fyh;
+  t.fyl = a.fyl;
+  t.am1x = a.am1x;
+  t.bx = a.bx;
+  t.ay = a.ay;
+  t.bm1y = a.bm1y;
+  t.gam = a.gam;
+  t.eta = a.eta;
+  return t;
+}
+
+// The fast sampler of the tile kernel, the same decision as sample_try with
+// fewer operations: floor(t) from one round-down add of 1.5 * 2^23 (its bits
+// minus 0x4B400000 are the integer, |t| < 2^22), the taps' bounds as two
+// unsigned compares of x0 - 1 and y0 - 1 against w - 4 and h - 4, 32-bit tap
+// offsets from `org` (the frame's pixel (1, 1); frames below 4 GiB), taps
+// converted to floats directly.  `lim` is 0.5 - the frame's tie band.
+template <int CH>
+__device__ __forceinline__ bool sample_tile(const uint8_t* org, uint32_t pitch, uint32_t xm, uint32_t ym, float lim,
+                                            const TileAnchor& a, float fdu, float fdv, int du, int dv,
+                                            uint32_t* out) {
+  const float gd = fmaf(a.gam, fdu, a.eta * fdv);
+  const float rd = __fdividef(1.0f, 1.0f + gd);
+  const float nx = fmaf(a.am1x, fdu, a.bx * fdv) - fdu * gd;
+  const float ny = fmaf(a.ay, fdu, a.bm1y * fdv) - fdv * gd;
+  const float tx = a.fxh + fmaf(nx, rd, a.fxl);
+  const float ty = a.fyh + fmaf(ny, rd, a.fyl);
+  const float sx = __fadd_rd(tx, 12582912.0f), sy = __fadd_rd(ty, 12582912.0f);
+  const uint32_t xm1 = __float_as_uint(sx) + (uint32_t)a.kx + (uint32_t)du;  // x0 - 1
+  const uint32_t ym1 = __float_as_uint(sy) + (uint32_t)a.ky + (uint32_t)dv;  // y0 - 1
+  // taps at least one pixel inside on every side: the floor decision then
+  // cannot change which sampler the reference takes
+  if (xm1 > xm || ym1 > ym) return false;
+  const float fx = tx - (sx - 12582912.0f), fy = ty - (sy - 12582912.0f);
+  const uint32_t o0 = ym1 * pitch + xm1 * (uint32_t)CH;
+  const uint8_t* r0 = org + o0;
+  const uint8_t* r1 = org + (o0 + pitch);
+  const float fxy = fx * fy;
+  auto f8 = [](uint8_t v) { return (float)(uint32_t)v; };
+  if (CH == 1) {
+    const float v00 = f8(__ldg(r0)), v10 = f8(__ldg(r0 + 1)), v01 = f8(__ldg(r1)), v11 = f8(__ldg(r1 + 1));
+    const float e10 = v10 - v00, e01 = v01 - v00, e11 = (v11 - v10) - e01;
+    float v = fmaf(fx, e10, v00);
+    v = fmaf(fy, e01, v);
+    v = fmaf(fxy, e11, v);
+    const float t = __fadd_rn(v, 12582912.0f);
+    if (fabsf(__fsub_rn(v, __fsub_rn(t, 12582912.0f))) > lim) return false;
+    *out = (__float_as_uint(t) & 255u) * 0x010101u | 0xFF000000u;
+    return true;
+  }
+  const float2 m1 = make_float2(-1.0f, -1.0f);
+  const float2 a00 = make_float2(f8(__ldg(r0)), f8(__ldg(r0 + 1)));
+  const float2 a10 = make_float2(f8(__ldg(r0 + CH)), f8(__ldg(r0 + CH + 1)));
+  const float2 a01 = make_float2(f8(__ldg(r1)), f8(__ldg(r1 + 1)));
+  const float2 a11 = make_float2(f8(__ldg(r1 + CH)), f8(__ldg(r1 + CH + 1)));
+  const float b00 = f8(__ldg(r0 + 2)), b10 = f8(__ldg(r0 + CH + 2));
+  const float b01 = f8(__ldg(r1 + 2)), b11 = f8(__ldg(r1 + CH + 2));
+  const float2 d10 = __ffma2_rn(a00, m1, a10), d01 = __ffma2_rn(a00, m1, a01);
+  const float2 d11 = __ffma2_rn(d01, m1, __ffma2_rn(a10, m1, a11));
+  float2 v = __ffma2_rn(make_float2(fx, fx), d10, a00);
+  v = __ffma2_rn(make_float2(fy, fy), d01, v);
+  v = __ffma2_rn(make_float2(fxy, fxy), d11, v);
+  const float e10 = b10 - b00, e01 = b01 - b00, e11 = (b11 - b10) - e01;
+  float vb = fmaf(fx, e10, b00);
+  vb = fmaf(fy, e01, vb);
+  vb = fmaf(fxy, e11, vb);
+  const float2 M = make_float2(12582912.0f, 12582912.0f);
+  const float2 t = __fadd2_rn(v, M);
+  const float2 dl = __ffma2_rn(__fadd2_rn(t, make_float2(-12582912.0f, -12582912.0f)), m1, v);
+  const float tb = __fadd_rn(vb, 12582912.0f);
+  const float db = __fsub_rn(vb, __fsub_rn(tb, 12582912.0f));
+  if (fmaxf(fmaxf(fabsf(dl.x), fabsf(dl.y)), fabsf(db)) > lim) return false;
+  const uint32_t rg = __byte_perm(__float_as_uint(t.x), __float_as_uint(t.y), 0x0040u);
+  *out = __byte_perm(rg, __float_as_uint(tb), 0x0410u) | 0xFF000000u;
+  return true;
+}
+
 // Sample output pixel (X, Y) = anchor pixel + (du, dv).  Falls back to the
 // exact path when the fast path cannot certify the result.
 __device__ __forceinline__ uint32_t sample_fast(const Warp& w, const SrcImage& s, const Anchor& a, int du, int dv,
