@@ -60,6 +60,8 @@ def parse():
     ap.add_argument("--width", type=int, default=WIDTH)
     ap.add_argument("--height", type=int, default=HEIGHT)
     ap.add_argument("--batch", type=int, default=0, help="frames per pass over per-pixel state (0 = library default)")
+    ap.add_argument("--pass2-mode", default=None, choices=["cache", "resident", "refetch", "laps", "fused"],
+                    help="impose the stack's pass-2 mode (default: the library's choice for the HBM budget)")
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -578,7 +580,7 @@ def main():
     mode_used = {}
 
     def step():
-        st = fsb.PyramidContrastStack(ctx, W, H, F, roi=roi, frames_per_batch=args.batch)
+        st = fsb.PyramidContrastStack(ctx, W, H, F, roi=roi, frames_per_batch=args.batch, pass2_mode=args.pass2_mode)
         mode_used["mode"] = st.pass2_mode
         for f, p in zip(frames, poses):
             st.add_frame_device(f, W * 3, p)
@@ -654,7 +656,8 @@ def main():
                  for _ in range(2)]
 
         def new_stack(i):
-            st = fsb.PyramidContrastStack(ctx, W, H, F, roi=roi, frames_per_batch=args.batch)
+            st = fsb.PyramidContrastStack(ctx, W, H, F, roi=roi, frames_per_batch=args.batch,
+                                          pass2_mode=args.pass2_mode)
             for f, p in zip(hframes, poses):
                 st.add_frame_async(f, p)  # uploads queued back to back (pinned frames stay put)
             return st

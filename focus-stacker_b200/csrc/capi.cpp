@@ -425,13 +425,24 @@ int launch_lap0_batch(fs_stack* s, size_t begin, size_t end) {
   a.au = s->au;
   a.best = s->best;
   a.hard = s->hard;
+  // the remap of the batch into its RGBA slots, then the fused level 0 from them
+  RemapWeightArgs r;
+  std::memset(&r, 0, sizeof(r));
+  r.W = a.W;
+  r.H = a.H;
+  r.K = a.K;
+  r.pitch = s->pitch[0];
   for (size_t k = begin; k < end; ++k) {
     std::string why;
-    if (!build_frame_in(s, s->frames[k], &a.f[k - begin], &why)) return set_err(s->ctx, FS_ERR_INVALID, why);
+    if (!build_frame_in(s, s->frames[k], &r.f[k - begin], &why)) return set_err(s->ctx, FS_ERR_INVALID, why);
+    r.out[k - begin] = FramePlanes{s->p2[k - begin].rgba, nullptr};
+    a.rgba[k - begin] = s->p2[k - begin].rgba;
     a.w[k - begin] = s->wplane[k];
     a.g1[k - begin] = s->slot[k - begin][1];
   }
-  cudaError_t e = timed(s->ctx, "pass1", [&] { return launch_lap0(a, (int)s->border, s->ctx->stream); });
+  cudaError_t e = timed(s->ctx, "pass1", [&] { return launch_remap_tiles(r, s->ctx->stream); });
+  if (e != cudaSuccess) return cuda_err(s->ctx, e, "remap launch");
+  e = timed(s->ctx, "pass1", [&] { return launch_lap0(a, (int)s->border, s->ctx->stream); });
   if (e != cudaSuccess) return cuda_err(s->ctx, e, "fused pass-1 launch");
   return FS_OK;
 }
@@ -984,7 +995,8 @@ uint64_t plan_bytes(const StackPlan& p, uint32_t frames, Pass2Mode mode, bool ho
       return p.fixed + (uint64_t)p.planes / 2 * p.K + ((uint64_t)p.laps_frame + 2 * p.L * sizeof(float*)) * frames +
              staging;
     case P2_FUSED:
-      return p.fixed + p.fused_fixed + ((uint64_t)p.fused_frame + 2 * p.L * sizeof(float*)) * frames + staging;
+      return p.fixed + p.fused_fixed + (uint64_t)p.planes / 2 * p.K +
+             ((uint64_t)p.fused_frame + 2 * p.L * sizeof(float*)) * frames + staging;
     case P2_CACHE: return p.fixed + (uint64_t)p.planes * frames + staging;
     case P2_RESIDENT: return p.fixed + (uint64_t)p.planes * p.K + (uint64_t)p.frame_bytes * frames;
     default: return p.fixed + (uint64_t)p.planes * p.K + staging;
@@ -1082,13 +1094,13 @@ static int begin_impl(fs_ctx* ctx, const fs_stack_desc* desc, fs_stack** out, in
   const size_t planes_bytes = plan.planes;
   if (s->mode == P2_LAPS || s->mode == P2_FUSED) {
     const bool laps = s->mode == P2_LAPS;
-    if (laps) {
-      // remapped RGBA of the batch's frames, read by the level-0 image step
-      for (uint32_t kk = 0; kk < s->K; ++kk) {
-        if ((rc = stack_alloc(s, n0 * 4, &p)) != FS_OK) return fail(rc);
-        s->p2.push_back(FramePlanes{(uint32_t*)p, nullptr});
-      }
-    } else {
+    // remapped RGBA of the batch's frames, read by the level-0 image step
+    // (LAPS) or the fused level-0 kernel (FUSED)
+    for (uint32_t kk = 0; kk < s->K; ++kk) {
+      if ((rc = stack_alloc(s, n0 * 4, &p)) != FS_OK) return fail(rc);
+      s->p2.push_back(FramePlanes{(uint32_t*)p, nullptr});
+    }
+    if (!laps) {
       if ((rc = stack_alloc(s, plan.fused_fixed, &p)) != FS_OK) return fail(rc);
       s->au = (float*)p;
     }

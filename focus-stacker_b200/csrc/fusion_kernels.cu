@@ -158,120 +158,43 @@ __device__ __forceinline__ float window_stddev(uint32_t packed, uint32_t s2, con
   return sqrtf(num * inv_den[n]);
 }
 
-// --------------------------------------------------------- region remap
-// Fill a shared region of packed RGBA samples for output pixels
-// [rx0, rx0 + RW) x [ry0, ry0 + RH) (ROI coordinates); pixels outside the ROI
-// get 0 (no support).  Optionally also the contrast words.  Work unit: 8x4
-// pixel blocks, one warp each; the blocks' FP64 anchors are formed first, one
-// per thread, into shared memory.
-constexpr int kExactQueue = 256;   // deferred exact samples per CTA and frame
-constexpr int kMaxAnchors = 120;   // 8x4 blocks of the largest region (contrast window 15)
+// ------------------------------------------------- region of a tile
+constexpr int kExactQueue = 256;  // deferred exact samples per CTA and frame
 constexpr int32_t kNoAnchor = INT32_MIN;
 
-// Shared scratch of fill_region: the block anchors of the frame (NB of the
-// region's 8x4 blocks), and a queue of samples the fast path could not
-// decide, processed together after the fast pass so that one lane's tie does
-// not hold its whole warp on the (long) exact path.
-template <int NB>
-struct __align__(16) ExactQueue {
-  Anchor anchor[NB];
-  uint32_t count;
-  uint32_t item[kExactQueue];  // ry << 16 | rx
-};
-template <int RW, int RH>
-using RegionQueue = ExactQueue<((RW + 7) / 8) * ((RH + 3) / 4)>;
-
-// The FP64 anchors of a region's 8x4 blocks into shared memory, one per
-// thread from thread `first` on, and the exact queue emptied.  The kernel
-// runs it for the next frame while the current one's window sums are formed
-// (the anchors are last read by the current frame's fast pass).
-template <int RW, int RH>
-__device__ __forceinline__ void region_anchors(const FrameIn& f, int rx0, int ry0, RegionQueue<RW, RH>* q, int first) {
-  constexpr int NBX = (RW + 7) / 8, NBY = (RH + 3) / 4, NB = NBX * NBY;
-  static_assert(NB <= kMaxAnchors && NB <= NT, "anchor table too small");
-  if (f.warp.kind == WARP_ALIGNED) return;
-  const bool fast_ok = f.warp.kind == WARP_HOMOGRAPHY && !f.warp.guard && f.src.w >= 4 && f.src.h >= 4;
-  if ((int)threadIdx.x == first) q->count = 0;
-  const int b = (int)threadIdx.x - first;
-  if (b >= 0 && b < NB) {
-    bool ok = false;
-    Anchor an = {};
-    if (fast_ok) an = make_anchor(f.warp, rx0 + (b % NBX) * 8, ry0 + (b / NBX) * 4, &ok);
-    if (!ok) an.ix = kNoAnchor;
-    q->anchor[b] = an;
-  }
-}
-
-// Remap of the region: the anchors (region_anchors) are in place.  Writes
-// the packed samples of the region's window [RB, RW - RB) x [RB, RH - RB)
-// into `reg` (row stride RW - 2 RB; RB = 0: the whole region) and the 16-bit
-// contrast words of the whole region into `kv` (row stride KS).  CH = 3: RGB
-// sources (remap and aligned); CH = 0: the channel count read at run time
-// (gray remap sources, RGBA aligned frames).  The frame's source fields are
-// read into registers once per region.
-template <int RW, int RH, int KS, int CH = 0, int RB = 0>
-__device__ void fill_region(const FrameIn& f, int W, int H, int rx0, int ry0, uint32_t* reg, uint16_t* kv,
-                            RegionQueue<RW, RH>* q) {
-  constexpr int GW = RW - 2 * RB, GH = RH - 2 * RB;
-  auto put = [&](int i, int rx, int ry, uint32_t v, uint32_t w) {
-    if (RB == 0) {
-      reg[i] = v;
-    } else if ((unsigned)(rx - RB) < (unsigned)GW && (unsigned)(ry - RB) < (unsigned)GH) {
-      reg[(ry - RB) * GW + rx - RB] = v;
-    }
-    kv[i + ry * (KS - RW)] = (uint16_t)w;
-  };
-  // region fully inside the ROI: no per-pixel bounds test
-  const bool inside = rx0 >= 0 && ry0 >= 0 && rx0 + RW <= W && ry0 + RH <= H;
-  if (f.warp.kind == WARP_ALIGNED) {
-    const uint8_t* px = f.src.px;
-    const int64_t pitch = f.src.pitch;
-    const int ch = CH ? CH : f.src.ch;
-    for (int i = threadIdx.x; i < RW * RH; i += NT) {
-      const int ry = i / RW, rx = i - ry * RW;
-      const int X = rx0 + rx, Y = ry0 + ry;
-      uint32_t v = 0;
-      if (inside || ((unsigned)X < (unsigned)W && (unsigned)Y < (unsigned)H)) {
-        const uint8_t* p = px + (int64_t)Y * pitch + X * ch;
-        const uint32_t al = ch == 4 ? (uint32_t)__ldg(p + 3) : 255u;
-        v = pack_rgba(__ldg(p), __ldg(p + 1), __ldg(p + 2), al);
-      }
-      put(i, rx, ry, v, contrast_word(v));
-    }
-    return;
-  }
-  constexpr int NBX = (RW + 7) / 8;
-  const TapSrc src = tap_src(f.src, f.warp.tie_band);
-  // region pixels in row order over all threads (a warp's 32 pixels lie in
-  // one or two rows: coalesced taps and stores, and no idle lanes in the
-  // region's last block column); each reads its 8x4 block's anchor
-  for (int i = threadIdx.x; i < RW * RH; i += NT) {
-    const int ry = i / RW, rx = i - ry * RW;
-    const int du = rx & 7, dv = ry & 3;
-    const Anchor an = q->anchor[(ry >> 2) * NBX + (rx >> 3)];
-    uint32_t v = 0, w = 0;
-    if (inside || ((unsigned)(rx0 + rx) < (unsigned)W && (unsigned)(ry0 + ry) < (unsigned)H)) {
-      if (an.ix == kNoAnchor) {
-        v = sample_exact(f.warp, f.src, rx0 + rx, ry0 + ry);  // whole block without an anchor (guarded / lens poses)
-        w = contrast_word(v);
-      } else if (!sample_try<CH>(src, an, (float)du, (float)dv, du, dv, &v, &w)) {
-        const uint32_t slot = atomicAdd(&q->count, 1u);
-        if (slot < (uint32_t)kExactQueue) {
-          q->item[slot] = ((uint32_t)ry << 16) | (uint32_t)rx;
-          continue;  // filled after the fast pass
-        }
-        v = sample_exact(f.warp, f.src, rx0 + rx, ry0 + ry);
-        w = contrast_word(v);
+// Rows [y0 - R0, y0 - R0 + RH) x columns [x0 - R0, x0 - R0 + RW) of a frame's
+// RGBA plane (written by remap_tile_kernel; 16-byte aligned rows) into
+// shared memory: the packed words into `reg` (row stride RW) and their
+// 16-bit contrast words into `kv` (row stride KS), zero outside the ROI.
+// The rows are read in 16-byte chunks from column x0 - CB (R0 rounded up to
+// a multiple of 4).
+template <int RW, int RH, int KS, int R0>
+__device__ __forceinline__ void load_region(const uint32_t* plane, int64_t pitch, int W, int H, int x0, int y0,
+                                            uint32_t* reg, uint16_t* kv) {
+  constexpr int CB = (R0 + 3) / 4 * 4;
+  constexpr int SK = CB - R0;  // chunk columns before the region's first
+  constexpr int CHUNKS = (RW + SK + 3) / 4;
+  for (int it = threadIdx.x; it < RH * CHUNKS; it += NT) {
+    const int r = it / CHUNKS, c = it - r * CHUNKS;
+    const int Y = y0 - R0 + r, Xc = x0 - CB + 4 * c;
+    uint4 q = make_uint4(0u, 0u, 0u, 0u);
+    if ((unsigned)Y < (unsigned)H && Xc >= 0 && Xc < W) {
+      q = __ldg(reinterpret_cast<const uint4*>(plane + (int64_t)Y * pitch + Xc));
+      if (Xc + 3 >= W) {  // words past the last column are not samples
+        if (Xc + 1 >= W) q.y = 0u;
+        if (Xc + 2 >= W) q.z = 0u;
+        q.w = 0u;
       }
     }
-    put(i, rx, ry, v, w);
-  }
-  __syncthreads();
-  const uint32_t n = min(q->count, (uint32_t)kExactQueue);
-  for (uint32_t i = threadIdx.x; i < n; i += NT) {
-    const int rx = (int)(q->item[i] & 0xFFFFu), ry = (int)(q->item[i] >> 16);
-    const uint32_t v = sample_exact(f.warp, f.src, rx0 + rx, ry0 + ry);
-    put(ry * RW + rx, rx, ry, v, contrast_word(v));
+    const uint32_t wv[4] = {q.x, q.y, q.z, q.w};
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const int rc = 4 * c + e - SK;
+      if ((SK == 0 || rc >= 0) && rc < RW) {
+        reg[r * RW + rc] = wv[e];
+        kv[r * KS + rc] = (uint16_t)contrast_word(wv[e]);
+      }
+    }
   }
 }
 
@@ -355,16 +278,25 @@ __global__ void __launch_bounds__(NT, 6) remap_tile_kernel(const __grid_constant
   const float lim = 0.5f - fmaxf(f.warp.tie_band, kTieBand);
   const TileAnchor* an_col = S.anchor + (rx >> 3);
   const int64_t step = 4 * pitch;
-#pragma unroll 2
-  for (int j = 0; j < nrows; ++j) {
-    const TileAnchor an = an_col[j * (TW / 8)];
-    uint32_t v;
-    if (an.kx != kNoTileAnchor && sample_tile<CH>(org, spitch, xm, ym, lim, an, fdu, fdv, du, dv, &v)) {
-      col[j * step] = v;
-    } else {
-      const uint32_t slot = atomicAdd(&S.count, 1u);
-      if (slot < (uint32_t)kExactQueue) S.item[slot] = ((uint32_t)(ry0 + 4 * j) << 16) | (uint32_t)rx;
-      else S.overflow = 1;
+  auto undecided = [&](int j) {
+    const uint32_t slot = atomicAdd(&S.count, 1u);
+    if (slot < (uint32_t)kExactQueue) S.item[slot] = ((uint32_t)(ry0 + 4 * j) << 16) | (uint32_t)rx;
+    else S.overflow = 1;
+  };
+  // two rows per step, both samples taken before either is stored, so that
+  // their tap loads are in flight together
+  for (int j = 0; j < nrows; j += 2) {
+    const bool two = j + 1 < nrows;
+    const TileAnchor an0 = an_col[j * (TW / 8)];
+    const TileAnchor an1 = an_col[(two ? j + 1 : j) * (TW / 8)];
+    uint32_t v0, v1;
+    const bool ok0 = sample_tile<CH>(org, spitch, xm, ym, lim, an0, fdu, fdv, du, dv, &v0);
+    const bool ok1 = sample_tile<CH>(org, spitch, xm, ym, lim, an1, fdu, fdv, du, dv, &v1);
+    if (ok0) col[j * step] = v0;
+    else undecided(j);
+    if (two) {
+      if (ok1) col[(j + 1) * step] = v1;
+      else undecided(j + 1);
     }
   }
   __syncthreads();
@@ -377,7 +309,7 @@ __global__ void __launch_bounds__(NT, 6) remap_tile_kernel(const __grid_constant
     for (int j = 0; j < nrows; ++j) {
       const TileAnchor an = an_col[j * (TW / 8)];
       uint32_t v;
-      if (!(an.kx != kNoTileAnchor && sample_tile<CH>(org, spitch, xm, ym, lim, an, fdu, fdv, du, dv, &v)))
+      if (!sample_tile<CH>(org, spitch, xm, ym, lim, an, fdu, fdv, du, dv, &v))
         col[j * step] = sample_exact(f.warp, f.src, X, y0 + ry0 + 4 * j);
     }
   }
@@ -538,7 +470,7 @@ static cudaError_t launch_weights(const RemapWeightArgs& a, cudaStream_t s) {
 // 16-byte aligned rows; remapped frames stay below 4 GiB (32-bit tap
 // offsets).  The frames of a batch share their channel count: the remap
 // kernel has it compiled in (RGB or gray; aligned frames read it).
-cudaError_t launch_remap_weights(const RemapWeightArgs& a, int border, cudaStream_t s) {
+cudaError_t launch_remap_tiles(const RemapWeightArgs& a, cudaStream_t s) {
   if (a.K < 1 || a.K > kMaxBatch || a.W < 1 || a.H < 1 || (a.pitch & 3)) return cudaErrorInvalidValue;
   for (int k = 0; k < a.K; ++k) {
     if (!a.out[k].rgba || ((uintptr_t)a.out[k].rgba & 15)) return cudaErrorInvalidValue;
@@ -550,7 +482,11 @@ cudaError_t launch_remap_weights(const RemapWeightArgs& a, int border, cudaStrea
   const dim3 grid((a.W + TW - 1) / TW, (a.H + TH - 1) / TH, a.K);
   if (a.f[0].src.ch == 1) remap_tile_kernel<1><<<grid, NT, 0, s>>>(a);
   else remap_tile_kernel<3><<<grid, NT, 0, s>>>(a);
-  cudaError_t e = cudaGetLastError();
+  return cudaGetLastError();
+}
+
+cudaError_t launch_remap_weights(const RemapWeightArgs& a, int border, cudaStream_t s) {
+  cudaError_t e = launch_remap_tiles(a, s);
   if (e != cudaSuccess) return e;
   switch (border) {
     case 1: return launch_weights<1>(a, s);
@@ -2025,7 +1961,6 @@ struct Lap0Layout {
 template <int B>
 struct __align__(16) Lap0Smem {
   using Lay = Lap0Layout<B>;
-  RegionQueue<Lay::RW, Lay::RH> queue;
   uint32_t reg[Lay::RH * Lay::RW];   // remapped RGBA words of the region
   uint16_t kv[Lay::RH * Lay::KS];    // contrast words of the region
   union {
@@ -2090,13 +2025,11 @@ __global__ void __launch_bounds__(NT, 2) lap0_kernel(const __grid_constant__ Lap
       }
     }
   }
-  constexpr int kAnchorThreads = ((RW + 7) / 8) * ((RH + 3) / 4);
-  if (a.K > 0) region_anchors<RW, RH>(a.f[0], x0 - R0, y0 - R0, &S.queue, 0);
   __syncthreads();
   const bool exact = a.exact_expand != 0;
   for (int k = 0; k < a.K; ++k) {
     // A: the region's remapped words and contrast words
-    fill_region<RW, RH, KS>(a.f[k], a.W, a.H, x0 - R0, y0 - R0, S.reg, S.kv, &S.queue);
+    load_region<RW, RH, KS, R0>(a.rgba[k], a.pitch, a.W, a.H, x0, y0, S.reg, S.kv);
     __syncthreads();
     // B: horizontal window sums (rows R0 - B .. R0 + TH + B - 1 of the
     // region, output columns c0 .. c0 + 7) and horizontal REDUCE sums (region
@@ -2122,7 +2055,6 @@ __global__ void __launch_bounds__(NT, 2) lap0_kernel(const __grid_constant__ Lap
                                              (uint32_t)hs[h].z | ((uint32_t)hs[h].w << 16));
       }
     }
-    if (k + 1 < a.K) region_anchors<RW, RH>(a.f[k + 1], x0 - R0, y0 - R0, &S.queue, NT - kAnchorThreads);
     __syncthreads();
     // C1: vertical window sums -> this frame's weights of the own pixels
     {

@@ -104,7 +104,7 @@ struct Lap0Args {
   uint8_t* uni;            // union support
   float* aw;               // A_w = sum of lap0 * w, 3 planes
   float* au;               // A_u = sum of lap0 while N <= 1e-12, 3 planes
-  FrameIn f[kMaxBatch];
+  const uint32_t* rgba[kMaxBatch];  // per frame: its remapped RGBA plane (remap_tile_kernel)
   float* w[kMaxBatch];         // per frame: its level-0 weight plane
   LevelPlanes g1[kMaxBatch];   // per frame: level-1 Gaussian (storage) and support
   // hybrid method only (null otherwise): per pixel the largest weight so far
@@ -165,6 +165,8 @@ struct RemapArgs {
 };
 
 cudaError_t launch_remap_weights(const RemapWeightArgs& a, int border, cudaStream_t s);
+// The remap alone (the RGBA planes; norm, uni and the weight planes untouched).
+cudaError_t launch_remap_tiles(const RemapWeightArgs& a, cudaStream_t s);
 
 // 16-bit frames (fusion16.cu): pass 1 (accumulate = 1: weight sum and union)
 // or pass 2 (out[k]: the frame's level-0 Gaussian as 3 f32 planes, its

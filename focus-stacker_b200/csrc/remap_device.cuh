@@ -377,11 +377,13 @@ __device__ __forceinline__ TileAnchor tile_anchor(const Anchor& a) {
 }
 
 // The fast sampler of the tile kernel, the same decision as sample_try with
-// fewer operations: floor(t) from one round-down add of 1.5 * 2^23 (its bits
+// fewer operations and no branches (so that the loads of neighbouring
+// samples overlap): floor(t) from one round-down add of 1.5 * 2^23 (its bits
 // minus 0x4B400000 are the integer, |t| < 2^22), the taps' bounds as two
 // unsigned compares of x0 - 1 and y0 - 1 against w - 4 and h - 4, 32-bit tap
-// offsets from `org` (the frame's pixel (1, 1); frames below 4 GiB), taps
-// converted to floats directly.  `lim` is 0.5 - the frame's tie band.
+// offsets from `org` (the frame's pixel (1, 1); frames below 4 GiB; a sample
+// that fails the bounds reads the taps at `org` and is discarded).  `lim` is
+// 0.5 - the frame's tie band.  Returns whether *out is decided.
 template <int CH>
 __device__ __forceinline__ bool sample_tile(const uint8_t* org, uint32_t pitch, uint32_t xm, uint32_t ym, float lim,
                                             const TileAnchor& a, float fdu, float fdv, int du, int dv,
@@ -397,38 +399,41 @@ __device__ __forceinline__ bool sample_tile(const uint8_t* org, uint32_t pitch, 
   const uint32_t ym1 = __float_as_uint(sy) + (uint32_t)a.ky + (uint32_t)dv;  // y0 - 1
   // taps at least one pixel inside on every side: the floor decision then
   // cannot change which sampler the reference takes
-  if (xm1 > xm || ym1 > ym) return false;
+  bool ok = a.kx != kNoTileAnchor && xm1 <= xm && ym1 <= ym;
   const float fx = tx - (sx - 12582912.0f), fy = ty - (sy - 12582912.0f);
-  const uint32_t o0 = ym1 * pitch + xm1 * (uint32_t)CH;
+  const uint32_t o0 = ok ? ym1 * pitch + xm1 * (uint32_t)CH : 0u;
   const uint8_t* r0 = org + o0;
   const uint8_t* r1 = org + (o0 + pitch);
   const float fxy = fx * fy;
-  auto f8 = [](uint8_t v) { return (float)(uint32_t)v; };
+  // taps as biased floats 2^23 + v (one OR each): differences are exact
+  // without removing the bias, which only the first tap's value drops
+  auto bf = [](uint8_t v) { return __uint_as_float(0x4B000000u | (uint32_t)v); };
   if (CH == 1) {
-    const float v00 = f8(__ldg(r0)), v10 = f8(__ldg(r0 + 1)), v01 = f8(__ldg(r1)), v11 = f8(__ldg(r1 + 1));
+    const float v00 = bf(__ldg(r0)), v10 = bf(__ldg(r0 + 1)), v01 = bf(__ldg(r1)), v11 = bf(__ldg(r1 + 1));
     const float e10 = v10 - v00, e01 = v01 - v00, e11 = (v11 - v10) - e01;
-    float v = fmaf(fx, e10, v00);
+    float v = fmaf(fx, e10, v00 - 8388608.0f);
     v = fmaf(fy, e01, v);
     v = fmaf(fxy, e11, v);
     const float t = __fadd_rn(v, 12582912.0f);
-    if (fabsf(__fsub_rn(v, __fsub_rn(t, 12582912.0f))) > lim) return false;
+    ok = ok && fabsf(__fsub_rn(v, __fsub_rn(t, 12582912.0f))) <= lim;
     *out = (__float_as_uint(t) & 255u) * 0x010101u | 0xFF000000u;
-    return true;
+    return ok;
   }
   const float2 m1 = make_float2(-1.0f, -1.0f);
-  const float2 a00 = make_float2(f8(__ldg(r0)), f8(__ldg(r0 + 1)));
-  const float2 a10 = make_float2(f8(__ldg(r0 + CH)), f8(__ldg(r0 + CH + 1)));
-  const float2 a01 = make_float2(f8(__ldg(r1)), f8(__ldg(r1 + 1)));
-  const float2 a11 = make_float2(f8(__ldg(r1 + CH)), f8(__ldg(r1 + CH + 1)));
-  const float b00 = f8(__ldg(r0 + 2)), b10 = f8(__ldg(r0 + CH + 2));
-  const float b01 = f8(__ldg(r1 + 2)), b11 = f8(__ldg(r1 + CH + 2));
+  const float2 a00 = make_float2(bf(__ldg(r0)), bf(__ldg(r0 + 1)));
+  const float2 a10 = make_float2(bf(__ldg(r0 + CH)), bf(__ldg(r0 + CH + 1)));
+  const float2 a01 = make_float2(bf(__ldg(r1)), bf(__ldg(r1 + 1)));
+  const float2 a11 = make_float2(bf(__ldg(r1 + CH)), bf(__ldg(r1 + CH + 1)));
+  const float b00 = bf(__ldg(r0 + 2)), b10 = bf(__ldg(r0 + CH + 2));
+  const float b01 = bf(__ldg(r1 + 2)), b11 = bf(__ldg(r1 + CH + 2));
   const float2 d10 = __ffma2_rn(a00, m1, a10), d01 = __ffma2_rn(a00, m1, a01);
   const float2 d11 = __ffma2_rn(d01, m1, __ffma2_rn(a10, m1, a11));
-  float2 v = __ffma2_rn(make_float2(fx, fx), d10, a00);
+  float2 v = __fadd2_rn(a00, make_float2(-8388608.0f, -8388608.0f));
+  v = __ffma2_rn(make_float2(fx, fx), d10, v);
   v = __ffma2_rn(make_float2(fy, fy), d01, v);
   v = __ffma2_rn(make_float2(fxy, fxy), d11, v);
   const float e10 = b10 - b00, e01 = b01 - b00, e11 = (b11 - b10) - e01;
-  float vb = fmaf(fx, e10, b00);
+  float vb = fmaf(fx, e10, b00 - 8388608.0f);
   vb = fmaf(fy, e01, vb);
   vb = fmaf(fxy, e11, vb);
   const float2 M = make_float2(12582912.0f, 12582912.0f);
@@ -436,10 +441,10 @@ __device__ __forceinline__ bool sample_tile(const uint8_t* org, uint32_t pitch, 
   const float2 dl = __ffma2_rn(__fadd2_rn(t, make_float2(-12582912.0f, -12582912.0f)), m1, v);
   const float tb = __fadd_rn(vb, 12582912.0f);
   const float db = __fsub_rn(vb, __fsub_rn(tb, 12582912.0f));
-  if (fmaxf(fmaxf(fabsf(dl.x), fabsf(dl.y)), fabsf(db)) > lim) return false;
+  ok = ok && fmaxf(fmaxf(fabsf(dl.x), fabsf(dl.y)), fabsf(db)) <= lim;
   const uint32_t rg = __byte_perm(__float_as_uint(t.x), __float_as_uint(t.y), 0x0040u);
   *out = __byte_perm(rg, __float_as_uint(tb), 0x0410u) | 0xFF000000u;
-  return true;
+  return ok;
 }
 
 // Sample output pixel (X, Y) = anchor pixel + (du, dv).  Falls back to the

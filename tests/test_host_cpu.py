@@ -228,7 +228,7 @@ def test_mode_bytes_order():
     assert b["laps"] > b["fused"] > b["cache"] > b["resident"] > b["refetch"]
     # per frame-pixel: laps keeps the f32 level-0 Laplacian (12 B) that fused does not
     n0 = 7872 * 5243 * 30
-    assert 11.5 < (b["laps"] - b["fused"]) / n0 < 12.5
+    assert 11.0 < (b["laps"] - b["fused"]) / n0 < 12.5
     assert fsb.stack_footprint(d, b["cache"])[:2] == (b["cache"], "cache")
     for m in ("laps", "fused"):
         with pytest.raises(fsb.FocusCudaError):  # two levels only: no split pyramid
