@@ -69,7 +69,9 @@ def parse():
     ap.add_argument("--precision-frames", type=int, default=143,
                     help="frames of the precision-form stack (7952x5304 each)")
     ap.add_argument("--serving-requests", type=int, default=500, help="requests per arrival rate (serving form)")
-    ap.add_argument("--serving-rates", default="20,40", help="swept Poisson arrival rates, requests/s")
+    ap.add_argument("--serving-rates", default="20,40,60", help="swept Poisson arrival rates, requests/s")
+    ap.add_argument("--serving-repeats", type=int, default=2,
+                    help="runs per rate (independent arrival streams), so that the spread of p99 is on record")
     ap.add_argument("--serving-budget-gb", type=float, default=120.0)
     ap.add_argument("--batched-stacks", type=int, default=64, help="stacks of the batched form (0: skip)")
     ap.add_argument("--batched-budget-gb", type=float, default=130.0)
@@ -325,13 +327,58 @@ def precision_form(fsb, torch, dev, seed, frames_n, W=7952, H=5304, steps=2, war
             "psnr_db": float("inf") if mse == 0 else 10.0 * math.log10(255.0 ** 2 / mse)}
         res[fsb.STORAGE_NAMES[storage]]["speedup_vs_f32"] = round(
             res[fsb.STORAGE_NAMES[storage]]["value"] / res["f32"]["value"], 3)
-    del frames, bases, ref
+    del bases, ref
+    res["vs_fp64_oracle"] = precision_error_band(fsb, torch, ctx, dev, frames, poses, W, H, roi)
+    del frames
     ctx.close()
     torch.cuda.empty_cache()
     return res
 
 
-def serving_form(fsb, torch, dev, seed, n_requests, rates, budget_gb, workers=8):
+def precision_error_band(fsb, torch, ctx, dev, frames, poses, W, H, roi, rows=256):
+    """Error of each level storage against the FP64 oracle on a band of the
+    stack: the band (full ROI width, `rows` ROI rows in the middle) is fused
+    as its own ROI by the library and by the oracle evaluated in FP64 from
+    the same source rows (copied back from the device frames); max-abs of
+    the collapsed base in 16-bit LSBs, PSNR and the u8 difference."""
+    oracle = _oracle()
+    top = roi.top + (roi.height - rows) // 2
+    band = fsb.Rect(roi.left, top, roi.right, top + rows)
+    F = len(frames)
+    host = []
+    for f, p in zip(frames, poses):
+        pts = [(float(x), float(y)) for x in (band.left, (band.left + band.right) / 2, band.right)
+               for y in (band.top, band.bottom)]
+        ys = fsb.api.inverse_map_points(p, W, H, np.array(pts))[:, 1]
+        y0 = max(0, int(math.floor(min(ys))) - 4)
+        y1 = min(H, int(math.ceil(max(ys))) + 5)
+        img = np.zeros((H, W, 3), np.uint8)  # rows outside [y0, y1) stay untouched pages
+        img[y0:y1] = f[y0:y1].cpu().numpy()
+        host.append(img)
+    t0 = time.perf_counter()
+    ref_out, ref_base = oracle.stack_fuse(host, [p.as_dict() for p in poses], band.as_tuple(),
+                                          jobs=os.cpu_count() or 1, precision=64, want_base=True, native=True)
+    t_oracle = time.perf_counter() - t0
+    out = {"band": f"{band.width}x{band.height} ROI rows {band.top}..{band.bottom} of the {F}-frame stack, "
+                   f"{len(level_sizes(band.width, band.height))} levels; FP64 oracle {t_oracle:.1f} s on "
+                   f"{os.cpu_count()} threads"}
+    for storage in (fsb.STORAGE_F32, fsb.STORAGE_F16, fsb.STORAGE_BF16):
+        st = fsb.PyramidContrastStack(ctx, W, H, F, roi=band, level_storage=storage)
+        mode = st.pass2_mode
+        base = torch.zeros((band.height, band.width, 3), dtype=torch.float32, device=f"cuda:{dev}")
+        st.set_base_output(base, band.width * 3)
+        for f, p in zip(frames, poses):
+            st.add_frame_device(f, W * 3, p)
+        fused = st.finish()
+        st.close()
+        err = fsb.error_vs_reference(base.cpu().numpy(), ref_base, fused, ref_out)
+        out[fsb.STORAGE_NAMES[storage]] = dict({k: (round(v, 6) if isinstance(v, float) else v)
+                                                for k, v in err.items()}, pass2=mode)
+    del host
+    return out
+
+
+def serving_form(fsb, torch, dev, seed, n_requests, rates, budget_gb, workers=8, repeats=1):
     """Serving form: Poisson request streams (sizes 640x480 .. 6000x4000 with
     4-40 frames, 5 % 7952x5304 stacks of up to 143 frames) admitted against an
     HBM budget; frames are device-resident (a synthetic pool per size, as a
@@ -351,9 +398,17 @@ def serving_form(fsb, torch, dev, seed, n_requests, rates, budget_gb, workers=8)
         warm = [sv.StackRequest(i, 0.0, w, h, 4) for i, (w, h) in enumerate(sizes)]
         srv.serve(warm, pool.roi, pool.frame, torch)
         for rate in rates:
-            reqs = sv.poisson_stream(n_requests, rate, seed=seed * 1000 + int(rate))
-            rep = srv.serve(reqs, pool.roi, pool.frame, torch)
-            out["rates"][f"{rate:g}"] = rep.summary()
+            runs = []
+            for r in range(repeats):
+                reqs = sv.poisson_stream(n_requests, rate, seed=seed * 1000 + int(rate) + 7919 * r)
+                runs.append(srv.serve(reqs, pool.roi, pool.frame, torch).summary())
+            res = dict(runs[0])
+            if repeats > 1:
+                res["runs"] = [{k: x[k] for k in ("p50_latency_ms", "p99_latency_ms", "throughput_mpix_frames_s",
+                                                   "makespan_s")} for x in runs]
+                for key in ("p50_latency_ms", "p99_latency_ms", "throughput_mpix_frames_s"):
+                    res[key + "_range"] = [min(x[key] for x in runs), max(x[key] for x in runs)]
+            out["rates"][f"{rate:g}"] = res
     del pool
     ctx.close()
     torch.cuda.empty_cache()
@@ -715,7 +770,7 @@ def main():
         if args.serving_requests > 0:
             rates = [float(x) for x in args.serving_rates.split(",") if x]
             forms["serving"] = serving_form(fsb, torch, dev, args.seed + rank, args.serving_requests, rates,
-                                            args.serving_budget_gb)
+                                            args.serving_budget_gb, repeats=args.serving_repeats)
         if args.batched_stacks > 0:
             forms["batched"] = batched_form(fsb, torch, dev, args.seed + rank, args.batched_stacks,
                                             args.batched_budget_gb)

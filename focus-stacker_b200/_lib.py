@@ -23,6 +23,7 @@ STATUS_NAMES = {
 # Every function the header declares (checked by the CPU tests).
 EXPORTED = (
     "fs_create", "fs_destroy", "fs_last_error", "fs_status_string", "fs_api_version", "fs_ctx_device_bytes",
+    "fs_ctx_budget",
     "fs_ctx_synchronize", "fs_ctx_trim", "fs_ctx_reserve", "fs_ctx_set_budget", "fs_ctx_stream", "fs_ctx_launch_count", "fs_ctx_set_kernel_timing", "fs_ctx_kernel_stats",
     "fs_pose_default", "fs_compute_roi", "fs_inverse_map_points", "fs_forward_map_points", "fs_exact_expand_divisor",
     "fs_remap_frame", "fs_remap_frame_device", "fs_remap_frame16", "fs_remap_frame16_device",
@@ -90,6 +91,8 @@ def _bind(L):
     L.fs_api_version.argtypes = []
     L.fs_ctx_device_bytes.argtypes = [ctx]
     L.fs_ctx_device_bytes.restype = u64
+    L.fs_ctx_budget.argtypes = [ctx]
+    L.fs_ctx_budget.restype = u64
     L.fs_ctx_synchronize.argtypes = [ctx]
     L.fs_ctx_trim.argtypes = [ctx]
     L.fs_ctx_reserve.argtypes = [ctx, u64]

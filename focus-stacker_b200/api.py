@@ -183,6 +183,10 @@ class Context:
     def device_bytes(self) -> int:
         return int(L().fs_ctx_device_bytes(self.handle))
 
+    def budget(self) -> int:
+        """The context's HBM budget in bytes."""
+        return int(L().fs_ctx_budget(self.handle))
+
     def trim(self):
         _check(L().fs_ctx_trim(self.handle), self.handle)
 

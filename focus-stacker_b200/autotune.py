@@ -1,33 +1,50 @@
 """Autotuner of the batched form: picks, for a given set of stacks, the
 schedule knobs the library exposes by timing them on the device:
 
-  lanes             concurrent streams (graph branches) the stacks are spread over;
-  frames_per_batch  frames per pass over the per-pixel state (K, 1..8): larger
-                    K reads the accumulators and weight sums fewer times but
-                    holds K level slots;
-  pass2_mode        0: keep the pass-1 planes for pass 2 (8 B per frame-pixel
-                    of memory), 1: keep only the frames and remap them again,
-                    -1: per stack, the planes while the budget allows.
+  lanes             concurrent streams (graph branches) the stacks are spread
+                    over; the stacks of a lane run one after another in one
+                    arena, so more lanes overlap more stacks but hold more
+                    device memory (one arena of the lane's largest stack each);
+  frames_per_batch  frames per pass-1 launch (K, 1..8): larger K reads the
+                    weight sums fewer times and gives the level launches more
+                    frames (grid z) but holds K batch slots;
+  pass2_mode        3: split pyramid (each frame's Laplacian pyramid kept from
+                    pass 1), 4: split pyramid with level 0 blended inside
+                    pass 1 (12 B per frame-pixel less to keep), 0: pass-1 planes
+                    kept, 1: frames kept and remapped again, -1: the first of
+                    3, 4, 0, 1 that fits the budget.
 
 Every candidate is built as a StackBatch, run twice (direct, then captured),
 and timed over `reps` graph replays; the fastest wins.  Candidates that do not
-fit the context's budget are skipped.  Results are plain dicts, so a caller can
-store them per workload signature and skip the search next time.
+fit the context's budget are skipped.  With `cache_path`, the winner is kept
+in a JSON file under the workload's signature (the stacks' sizes, frame
+counts, storage and budget), and a later call with the same signature returns
+it without timing.
 """
 from __future__ import annotations
 
 import itertools
+import json
+import os
 import time
 from typing import Callable, Dict, Iterable, List, Sequence
 
 from . import api
 
-DEFAULT_SPACE = {"lanes": (4, 8, 16), "frames_per_batch": (8,), "pass2_mode": (-1, 1)}
+DEFAULT_SPACE = {"lanes": (2, 4, 8), "frames_per_batch": (4, 8), "pass2_mode": (3, 4, 0)}
 
 
 def candidates(space: Dict[str, Iterable]) -> List[dict]:
     keys = ("lanes", "frames_per_batch", "pass2_mode")
     return [dict(zip(keys, v)) for v in itertools.product(*(tuple(space[k]) for k in keys))]
+
+
+def signature(ctx: api.Context, stacks: Sequence[api.BatchStack], level_storage: int = 0) -> str:
+    """Key of a workload: sorted (width, height, frames) of its stacks, the
+    level storage and the context's budget in GB."""
+    shapes = sorted((st.width, st.height, len(st.frames)) for st in stacks)
+    return json.dumps({"stacks": shapes, "storage": level_storage, "budget_gb": round(ctx.budget() / 1e9, 1)},
+                      separators=(",", ":"))
 
 
 def time_batch(ctx: api.Context, stacks: Sequence[api.BatchStack], reps: int = 3, level_storage: int = 0,
@@ -48,9 +65,23 @@ def time_batch(ctx: api.Context, stacks: Sequence[api.BatchStack], reps: int = 3
             "pass2": {m: modes.count(m) for m in set(modes)}}
 
 
+def _load(path: str) -> dict:
+    try:
+        with open(path) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return {}
+
+
 def tune(ctx: api.Context, stacks: Sequence[api.BatchStack], space: Dict[str, Iterable] = None, reps: int = 3,
-         level_storage: int = 0, log: Callable[[str], None] = None) -> dict:
-    """Time every candidate of `space` and return {"best": knobs, "trials": [...]}."""
+         level_storage: int = 0, log: Callable[[str], None] = None, cache_path: str = None) -> dict:
+    """Time every candidate of `space` and return {"best": knobs, "trials": [...]}
+    (from `cache_path` without timing when it holds this workload)."""
+    key = signature(ctx, stacks, level_storage)
+    if cache_path:
+        hit = _load(cache_path).get(key)
+        if hit is not None:
+            return dict(hit, cached=True)
     trials = []
     for knobs in candidates(space or DEFAULT_SPACE):
         try:
@@ -64,4 +95,12 @@ def tune(ctx: api.Context, stacks: Sequence[api.BatchStack], space: Dict[str, It
     if not ok:
         raise api.FocusCudaError(3, "no candidate fits the budget")
     best = min(ok, key=lambda t: t["s_per_run"])
-    return {"best": best["knobs"], "s_per_run": best["s_per_run"], "trials": trials}
+    res = {"best": best["knobs"], "s_per_run": best["s_per_run"], "trials": trials}
+    if cache_path:
+        table = _load(cache_path)
+        table[key] = {"best": res["best"], "s_per_run": res["s_per_run"]}
+        tmp = cache_path + ".tmp"
+        with open(tmp, "w") as f:
+            json.dump(table, f, indent=1)
+        os.replace(tmp, cache_path)
+    return dict(res, cached=False)

@@ -259,6 +259,15 @@ struct fs_stack {
   float* contrib = nullptr;       // per-frame blend contributions of those levels
   float* contrib_top = nullptr;   // and of the top level
   int64_t base_pitch = 0;         // elements
+  // Batches: the stack's buffers are carved from its lane's arena (shared by
+  // the lane's stacks, which run one after another) instead of the pool.
+  uint8_t* arena = nullptr;
+  size_t arena_size = 0, arena_used = 0;
+  // LAPS / FUSED: first level of the small-level tail (0: none) and the
+  // blend-tail launch's ticket (zero between launches)
+  uint32_t tail = 0;
+  uint32_t* tail_counter = nullptr;
+  bool tail_folded = false;  // pass 2 has added the tail levels' EXPANDs into acc[tail]
 };
 
 namespace {
@@ -281,7 +290,23 @@ void detach_stack(fs_stack* s) {
   s->ctx = nullptr;
 }
 
-int stack_alloc(fs_stack* s, size_t bytes, void** out, cudaStream_t on = nullptr) {
+// Arena pieces start on 256-byte boundaries, as pool allocations do.
+constexpr size_t kArenaAlign = 256;
+
+// pooled: from the context's pool even for an arena stack (buffers whose
+// contents are written once, at begin, and must survive the lane's other
+// stacks).
+int stack_alloc(fs_stack* s, size_t bytes, void** out, cudaStream_t on = nullptr, bool pooled = false) {
+  if (s->arena && !pooled) {
+    const size_t at = round_up((int64_t)s->arena_used, (int64_t)kArenaAlign);
+    const size_t n = bytes == 0 ? 16 : bytes;
+    if (at + n > s->arena_size)
+      return set_err(s->ctx, FS_ERR_BUDGET, "stack needs more than its lane arena (" + std::to_string(at + n) +
+                                                " > " + std::to_string(s->arena_size) + " bytes)");
+    *out = s->arena + at;
+    s->arena_used = at + n;
+    return FS_OK;
+  }
   int rc = dev_alloc(s->ctx, bytes, out, on);
   if (rc == FS_OK) s->allocs.push_back({*out, bytes == 0 ? 16 : bytes});
   return rc;
@@ -455,6 +480,10 @@ int launch_image_pyramid(fs_stack* s, size_t begin, size_t end) {
   std::memset(&a, 0, sizeof(a));
   a.levels = (int32_t)s->L;
   a.K = (int32_t)(end - begin);
+  const uint32_t tail = s->tail ? s->tail : s->L;  // levels from here on: one tail launch
+  ImgTailArgs t;
+  t.steps = 0;
+  t.pad = 0;
   for (uint32_t l = s->mode == P2_FUSED ? 1 : 0; l + 1 < s->L; ++l) {
     level_geometry(s, l, &a);
     for (size_t k = 0; k < (size_t)a.K; ++k) {
@@ -464,8 +493,16 @@ int launch_image_pyramid(fs_stack* s, size_t begin, size_t end) {
       a.lap[k] = s->lap[begin + k][l];
       a.gtop[k] = s->gtop[begin + k];
     }
+    if (l >= tail) {
+      t.lv[t.steps++] = a;
+      continue;
+    }
     cudaError_t e = timed(s->ctx, "image", [&] { return launch_img_level(a, s->storage, s->ctx->stream); });
     if (e != cudaSuccess) return cuda_err(s->ctx, e, "image pyramid launch");
+  }
+  if (t.steps > 0) {
+    cudaError_t e = timed(s->ctx, "image", [&] { return launch_img_tail(t, a.K, s->storage, s->ctx->stream); });
+    if (e != cudaSuccess) return cuda_err(s->ctx, e, "image pyramid tail launch");
   }
   return FS_OK;
 }
@@ -690,6 +727,8 @@ const char* fs_last_error(const fs_ctx* ctx) {
 }
 
 uint64_t fs_ctx_device_bytes(const fs_ctx* ctx) { return ctx ? ctx->held : 0; }
+
+uint64_t fs_ctx_budget(const fs_ctx* ctx) { return ctx ? ctx->budget : 0; }
 
 int fs_ctx_set_budget(fs_ctx* ctx, uint64_t hbm_budget_bytes) {
   if (!ctx || hbm_budget_bytes == 0) return FS_ERR_INVALID;
@@ -1015,8 +1054,10 @@ Pass2Mode choose_mode(const StackPlan& p, uint32_t frames, uint64_t available, b
 
 }  // namespace
 
-// forced_mode >= 0: pass-2 mode chosen by the caller (batches plan it)
-static int begin_impl(fs_ctx* ctx, const fs_stack_desc* desc, fs_stack** out, int forced_mode) {
+// forced_mode >= 0: pass-2 mode chosen by the caller (batches plan it);
+// arena: device memory the stack's buffers are carved from (batches).
+static int begin_impl(fs_ctx* ctx, const fs_stack_desc* desc, fs_stack** out, int forced_mode,
+                      uint8_t* arena = nullptr, size_t arena_size = 0) {
   if (!ctx || !desc || !out) return set_err(ctx, FS_ERR_INVALID, "null argument");
   *out = nullptr;
   const fs_stack_desc& d = *desc;
@@ -1040,6 +1081,8 @@ static int begin_impl(fs_ctx* ctx, const fs_stack_desc* desc, fs_stack** out, in
   s->lw = plan.lw;
   s->lh = plan.lh;
   s->pitch = plan.pitch;
+  s->arena = arena;
+  s->arena_size = arena ? arena_size : 0;
   auto fail = [&](int rc) {
     fs_stack_destroy(s);
     return rc;
@@ -1136,10 +1179,21 @@ static int begin_impl(fs_ctx* ctx, const fs_stack_desc* desc, fs_stack** out, in
       for (uint32_t f = 0; f < d.frame_count; ++f)
         s->tab_host.push_back(l == 0 ? s->wplane[f] : l + 1 < s->L ? (const float*)s->mplane[f][l] : s->mtop[f]);
     }
-    if ((rc = stack_alloc(s, s->tab_host.size() * sizeof(float*), &p)) != FS_OK) return fail(rc);
+    // the small-level tail: levels T >= 1 whose sides are at most kTailSide,
+    // when they make two level steps or more
+    for (uint32_t l = 1; l < s->L; ++l) {
+      if (std::max(s->lw[l], s->lh[l]) <= (uint32_t)kTailSide) {
+        if (s->L - 1 - l >= 2 && s->L - 1 - l <= (uint32_t)kMaxTail) s->tail = l;
+        break;
+      }
+    }
+    const size_t tab_bytes = round_up((int64_t)(s->tab_host.size() * sizeof(float*)), 16);
+    if ((rc = stack_alloc(s, tab_bytes + 16, &p, nullptr, true)) != FS_OK) return fail(rc);
     s->tab = (const float**)p;
+    s->tail_counter = (uint32_t*)((uint8_t*)p + tab_bytes);
     if (cudaMemcpyAsync(p, s->tab_host.data(), s->tab_host.size() * sizeof(float*), cudaMemcpyHostToDevice,
-                        ctx->stream) != cudaSuccess)
+                        ctx->stream) != cudaSuccess ||
+        cudaMemsetAsync(s->tail_counter, 0, 16, ctx->stream) != cudaSuccess)
       return fail(cuda_err(ctx, cudaGetLastError(), "frame table upload"));
   } else if (s->mode == P2_CACHE) {
     for (uint32_t f = 0; f < d.frame_count; ++f) {
@@ -1342,7 +1396,7 @@ int fs_stack_add_frame_device(fs_stack* stack, const void* dev_pixels, size_t ro
   return add_frame_impl(stack, dev_pixels, row_stride, pose, true);
 }
 
-static int pass2_impl(fs_stack* s, fs_frame_fetch_cb refetch, void* user);
+static int pass2_impl(fs_stack* s, fs_frame_fetch_cb refetch, void* user, bool fold_tail);
 static int collapse_impl(fs_stack* s, void* out, size_t out_stride, bool device_out, bool wait);
 
 // wait: block until the output is written; mark_done: record the stack's
@@ -1363,7 +1417,7 @@ static int finish_impl(fs_stack* s, fs_frame_fetch_cb refetch, void* user, void*
     s->phase = 1;
   }
   if (s->phase < 2) {
-    if ((rc = pass2_impl(s, refetch, user)) != FS_OK) return rc;
+    if ((rc = pass2_impl(s, refetch, user, true)) != FS_OK) return rc;
     s->phase = 2;
   }
   if ((rc = collapse_impl(s, out, out_stride, device_out, wait)) != FS_OK) return rc;
@@ -1378,14 +1432,20 @@ static int finish_impl(fs_stack* s, fs_frame_fetch_cb refetch, void* user, void*
 }
 
 // Pass 2: mask-support pyramid, accumulators cleared, the blend of every
-// frame into them (in the stack's pass-2 mode).
-static int pass2_impl(fs_stack* s, fs_frame_fetch_cb refetch, void* user) {
+// frame into them (in the stack's pass-2 mode).  fold_tail: a LAPS / FUSED
+// stack with a small-level tail blends its tail levels and collapses them
+// into acc[tail] in the same launches (the accumulators above it are then
+// spent: the frame-shard phases, which exchange accumulators, pass false).
+static int pass2_impl(fs_stack* s, fs_frame_fetch_cb refetch, void* user, bool fold_tail) {
   fs_ctx* ctx = s->ctx;
   int rc;
   cudaStream_t st = ctx->stream;
   cudaError_t e;
-  // mask-support pyramid (frame independent)
-  for (uint32_t l = 0; l + 1 < s->L; ++l) {
+  const bool split = s->mode == P2_LAPS || s->mode == P2_FUSED;
+  const uint32_t tail = split && fold_tail && s->tail && !s->frame_total ? s->tail : s->L;
+  s->tail_folded = false;
+  // mask-support pyramid (frame independent; the tail forms its own levels)
+  for (uint32_t l = 0; l + 1 < s->L && l < tail; ++l) {
     MaskSupportArgs m = {s->sm[l], (int32_t)s->lw[l], (int32_t)s->lh[l], s->pitch[l],
                          s->sm[l + 1], (int32_t)s->lw[l + 1], (int32_t)s->lh[l + 1], s->pitch[l + 1]};
     e = timed(ctx, "mask_support", [&] { return launch_mask_support(m, st); });
@@ -1418,7 +1478,7 @@ static int pass2_impl(fs_stack* s, fs_frame_fetch_cb refetch, void* user) {
     }
     if (e != cudaSuccess) return cuda_err(ctx, e, "level-0 blend");
     // the mask pyramid of every frame, level by level (one frame per grid z)
-    for (uint32_t l = 0; l + 1 < s->L; ++l) {
+    for (uint32_t l = 0; l + 1 < s->L && l < tail; ++l) {
       MaskReduceArgs m;
       m.in = (const void* const*)(s->tab + (size_t)l * 2 * N + N);
       m.out = (void* const*)(s->tab + (size_t)(l + 1) * 2 * N + N);
@@ -1440,7 +1500,7 @@ static int pass2_impl(fs_stack* s, fs_frame_fetch_cb refetch, void* user) {
       if (e != cudaSuccess) return cuda_err(ctx, e, "mask reduce");
     }
     // the blend of levels 1 .. L-1 over every frame (top: Gaussian x mask)
-    for (uint32_t l = 1; l < s->L; ++l) {
+    for (uint32_t l = 1; l < s->L && l < tail; ++l) {
       const void* const* lap = (const void* const*)(s->tab + (size_t)l * 2 * N);
       const void* const* msk = (const void* const*)(s->tab + (size_t)l * 2 * N + N);
       const int storage = l + 1 < s->L ? s->storage : FS_STORAGE_F32;
@@ -1449,6 +1509,25 @@ static int pass2_impl(fs_stack* s, fs_frame_fetch_cb refetch, void* user) {
                             (int)N, storage, st);
       });
       if (e != cudaSuccess) return cuda_err(ctx, e, "level blend");
+    }
+    if (tail < s->L) {
+      // levels tail .. L-1: masks, blends and their collapse in two launches
+      BlendTailArgs b;
+      std::memset(&b, 0, sizeof(b));
+      b.first = (int32_t)tail;
+      b.levels = (int32_t)s->L;
+      b.frames = (int32_t)N;
+      b.storage = s->storage;
+      b.tab = (const void* const*)s->tab;
+      b.sm_first = s->sm[tail];
+      b.counter = s->tail_counter;
+      for (uint32_t l = tail; l < s->L; ++l)
+        b.lv[l - tail] = TailLevel{(int32_t)s->lw[l], (int32_t)s->lh[l], s->pitch[l], s->acc[l],
+                                   s->pitch[l] * s->lh[l]};
+      e = timed(ctx, "level", [&] { return launch_mask_tail(b, st); });
+      if (e == cudaSuccess) e = timed(ctx, "level", [&] { return launch_blend_tail(b, st); });
+      if (e != cudaSuccess) return cuda_err(ctx, e, "small-level tail");
+      s->tail_folded = true;
     }
     return FS_OK;
   }
@@ -1551,8 +1630,9 @@ static int pass2_impl(fs_stack* s, fs_frame_fetch_cb refetch, void* user) {
 }
 
 // Collapse kernels of the accumulator pyramid into the quantised output
-// out_dev, with the collapsed base into `base` when given.
-static int collapse_kernels(fs_stack* s, float* base) {
+// out_dev, with the collapsed base into `base` when given, from level `top`
+// down (levels above it already added into it).
+static int collapse_kernels(fs_stack* s, float* base, uint32_t top) {
   fs_ctx* ctx = s->ctx;
   cudaStream_t st = ctx->stream;
   cudaError_t e;
@@ -1563,7 +1643,7 @@ static int collapse_kernels(fs_stack* s, float* base) {
     });
     if (e != cudaSuccess) return cuda_err(ctx, e, "quantise");
   }
-  for (uint32_t l = s->L - 1; l >= 1 && s->L > 1; --l) {
+  for (uint32_t l = std::min(top, s->L - 1); l >= 1 && s->L > 1; --l) {
     CollapseArgs c;
     std::memset(&c, 0, sizeof(c));
     c.wp = (int32_t)s->lw[l - 1];
@@ -1670,10 +1750,12 @@ static int collapse_impl(fs_stack* s, void* out, size_t out_stride, bool device_
   cudaError_t e;
   int rc;
   if (s->best) {
-    if ((rc = collapse_kernels(s, nullptr)) != FS_OK) return rc;
+    // the soft image, then the merged pyramid (written whole by the merge)
+    if ((rc = collapse_kernels(s, nullptr, s->tail_folded ? s->tail : s->L - 1)) != FS_OK) return rc;
     if ((rc = hybrid_merge(s)) != FS_OK) return rc;
+    s->tail_folded = false;
   }
-  if ((rc = collapse_kernels(s, s->base_out)) != FS_OK) return rc;
+  if ((rc = collapse_kernels(s, s->base_out, s->tail_folded ? s->tail : s->L - 1)) != FS_OK) return rc;
   const cudaMemcpyKind kind = device_out ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
   const size_t row = (size_t)s->W * 3 * s->bps;
   if (out_stride == row)
@@ -1771,7 +1853,7 @@ int fs_stack_end_pass1(fs_stack* s) {
 int fs_stack_blend(fs_stack* s, fs_frame_fetch_cb refetch, void* user) {
   int rc = phase_check(s, 1);
   if (rc != FS_OK) return rc;
-  if ((rc = pass2_impl(s, refetch, user)) != FS_OK) return rc;
+  if ((rc = pass2_impl(s, refetch, user, false)) != FS_OK) return rc;
   cudaError_t e = cudaStreamSynchronize(s->ctx->stream);
   if (e != cudaSuccess) return cuda_err(s->ctx, e, "pass 2");
   s->phase = 2;
@@ -1920,10 +2002,16 @@ int fs_synth_frame_device(fs_ctx* ctx, uint64_t seed, int scene, uint32_t width,
 // over `lanes` contexts (streams) and run as one CUDA graph: the first
 // fs_batch_run executes the work directly (and configures the kernels), the
 // second captures the same launch sequence, every later run replays it with
-// one graph launch.  Every stack's state is re-initialised by the kernels of
-// the run itself (pass 1 writes the weight sum and union of the first batch,
-// pass 2 clears the accumulators), so a replay recomputes every stack from
-// the frames at the same device addresses.
+// one graph launch.  The stacks of a lane run one after another on its
+// stream, so they share one device arena, sized for the lane's largest
+// stack: a batch holds (lanes x its largest stacks) bytes instead of the sum
+// over all its stacks, which lets every stack take the split-pyramid modes.
+// Every stack's state is re-initialised by the kernels of the run itself
+// (pass 1 writes the weight sum, union and per-frame planes of the first
+// batch, pass 2 clears or writes the accumulators whole), so a replay
+// recomputes every stack from the frames at the same device addresses; only
+// the split-pyramid frame tables, written once at create, live outside the
+// arenas.
 struct fs_batch {
   fs_ctx* parent = nullptr;
   std::vector<fs_ctx*> lanes;
@@ -1937,6 +2025,8 @@ struct fs_batch {
     size_t out_stride = 0;
   };
   std::vector<Item> items;
+  std::vector<void*> arenas;         // per lane
+  std::vector<uint64_t> arena_bytes;
   std::vector<cudaEvent_t> join;
   std::vector<int> planned;  // pass-2 mode of each stack
   uint64_t charged = 0;      // device bytes counted against the parent's budget
@@ -1949,19 +2039,23 @@ struct fs_batch {
 namespace {
 
 int batch_enqueue(fs_batch* b) {
-  for (auto& it : b->items) {
-    fs_stack* s = it.stack;
-    s->frames.clear();
-    s->pass1_done = 0;
-    s->finished = false;
-    s->phase = 0;
-    for (size_t k = 0; k < it.frames.size(); ++k) {
-      const fs_pose* pose = s->aligned ? nullptr : &it.poses[k];
-      int rc = add_frame_impl(s, it.frames[k], it.stride, pose, true);
+  // lane by lane, each lane's stacks in order (they share its arena)
+  for (size_t l = 0; l < b->lanes.size(); ++l) {
+    for (auto& it : b->items) {
+      if (it.lane != (int)l) continue;
+      fs_stack* s = it.stack;
+      s->frames.clear();
+      s->pass1_done = 0;
+      s->finished = false;
+      s->phase = 0;
+      for (size_t k = 0; k < it.frames.size(); ++k) {
+        const fs_pose* pose = s->aligned ? nullptr : &it.poses[k];
+        int rc = add_frame_impl(s, it.frames[k], it.stride, pose, true);
+        if (rc != FS_OK) return rc;
+      }
+      int rc = finish_impl(s, nullptr, nullptr, it.out, it.out_stride, true, false);
       if (rc != FS_OK) return rc;
     }
-    int rc = finish_impl(s, nullptr, nullptr, it.out, it.out_stride, true, false);
-    if (rc != FS_OK) return rc;
   }
   return FS_OK;
 }
@@ -1979,6 +2073,27 @@ int batch_enqueue_forked(fs_batch* b) {
   return rc;
 }
 
+// Arena bytes of one stack in mode m: its plan plus the 256-byte rounding of
+// every piece (at most this many pieces: fixed state, level slots, batch
+// slots, per-frame planes).
+uint64_t arena_need(const StackPlan& p, uint32_t frames, Pass2Mode m) {
+  const uint64_t pieces = 8 + 3ull * p.L + (uint64_t)p.K * (p.L + 1) + frames;
+  return plan_bytes(p, frames, m, false) + pieces * kArenaAlign;
+}
+
+// The split-pyramid frame table of a stack (allocated from the lane's pool).
+uint64_t table_bytes(const StackPlan& p, uint32_t frames, Pass2Mode m) {
+  return (m == P2_LAPS || m == P2_FUSED) ? 2ull * p.L * frames * sizeof(float*) : 0;
+}
+
+// The stack's mode when the batch asks for `want`: the split-pyramid modes
+// need three levels or more (smaller stacks cache their planes).
+Pass2Mode stack_mode(const StackPlan& p, Pass2Mode want) {
+  if (want == P2_LAPS && !p.laps_frame) return P2_CACHE;
+  if (want == P2_FUSED && !p.fused_frame) return P2_CACHE;
+  return want;
+}
+
 }  // namespace
 
 int fs_batch_create(fs_ctx* ctx, uint32_t n, const fs_stack_desc* descs, const void* const* const* frames,
@@ -1986,7 +2101,8 @@ int fs_batch_create(fs_ctx* ctx, uint32_t n, const fs_stack_desc* descs, const v
                     const size_t* out_strides, uint32_t lanes, int pass2_mode, fs_batch** out) {
   if (!ctx || !descs || !frames || !row_strides || !dev_out || !out_strides || !out || n == 0)
     return set_err(ctx, FS_ERR_INVALID, "null argument");
-  if (pass2_mode < -1 || pass2_mode > 1) return set_err(ctx, FS_ERR_INVALID, "pass2_mode must be -1, 0 or 1");
+  if (pass2_mode < -1 || pass2_mode > P2_FUSED || pass2_mode == P2_REFETCH)
+    return set_err(ctx, FS_ERR_INVALID, "pass2_mode must be -1, 0 (cache), 1 (resident), 3 (laps) or 4 (fused)");
   *out = nullptr;
   lanes = std::max(1u, std::min(lanes, n));
   cudaSetDevice(ctx->device);
@@ -1996,59 +2112,80 @@ int fs_batch_create(fs_ctx* ctx, uint32_t n, const fs_stack_desc* descs, const v
     fs_batch_destroy(b);
     return rc;
   };
-  // plan: footprints in the requested (or best affordable) mode, stacks to
-  // the least-loaded lane by frame-pixels, largest first
-  std::vector<uint64_t> bytes(n);
+  std::vector<StackPlan> plans;
   std::vector<double> work(n);
-  uint64_t total = 0;
   for (uint32_t i = 0; i < n; ++i) {
     int code = FS_OK;
     if (const char* why = check_desc(descs[i], &code)) return fail(set_err(ctx, code, why));
     if (descs[i].sample_bits != 8) return fail(set_err(ctx, FS_ERR_UNSUPPORTED, "batches take 8-bit stacks"));
     if (!frames[i]) return fail(set_err(ctx, FS_ERR_INVALID, "null frame list"));
     if (!descs[i].input_is_aligned && !poses) return fail(set_err(ctx, FS_ERR_INVALID, "poses required"));
-    const StackPlan plan = plan_stack(descs[i]);
-    const uint64_t left = ctx->budget > ctx->held + total ? ctx->budget - ctx->held - total : 0;
-    Pass2Mode m = pass2_mode == 0 ? P2_CACHE
-                  : pass2_mode == 1 ? P2_RESIDENT
-                                    : choose_mode(plan, descs[i].frame_count, left, true, descs[i].sample_bits == 16);
-    if (m == P2_REFETCH) m = P2_RESIDENT;
-    b->planned.push_back((int)m);
-    bytes[i] = plan_bytes(plan, descs[i].frame_count, m, true);
-    total += bytes[i];
-    work[i] = (double)descs[i].frame_count * plan.W * plan.H;
+    plans.push_back(plan_stack(descs[i]));
+    work[i] = (double)descs[i].frame_count * plans[i].W * plans[i].H;
   }
-  if (ctx->held + total > ctx->budget)
-    return fail(set_err(ctx, FS_ERR_BUDGET, "batch needs " + std::to_string(total) + " device bytes, budget leaves " +
-                                               std::to_string(ctx->budget > ctx->held ? ctx->budget - ctx->held : 0)));
+  // lanes: largest stack first to the least-loaded lane (frame-pixels)
   std::vector<uint32_t> order(n);
   for (uint32_t i = 0; i < n; ++i) order[i] = i;
   std::sort(order.begin(), order.end(), [&](uint32_t a, uint32_t c) { return work[a] > work[c]; });
   std::vector<double> load(lanes, 0.0);
-  std::vector<uint64_t> lane_bytes(lanes, 0);
   b->items.resize(n);
   for (uint32_t i : order) {
     const int l = (int)(std::min_element(load.begin(), load.end()) - load.begin());
     load[l] += work[i];
-    lane_bytes[l] += bytes[i];
     b->items[i].lane = l;
   }
+  // mode: the one asked for, or the fastest whose lane arenas fit the budget
+  // (split pyramid, then fused, then cached planes, then frames kept)
+  const uint64_t left = ctx->budget > ctx->held ? ctx->budget - ctx->held : 0;
+  std::vector<uint64_t> arena(lanes), tables(lanes);
+  auto size_lanes = [&](Pass2Mode want) {
+    std::fill(arena.begin(), arena.end(), 0);
+    std::fill(tables.begin(), tables.end(), 0);
+    uint64_t total = 0;
+    for (uint32_t i = 0; i < n; ++i) {
+      const Pass2Mode m = stack_mode(plans[i], want);
+      const int l = b->items[i].lane;
+      arena[l] = std::max(arena[l], arena_need(plans[i], descs[i].frame_count, m));
+      tables[l] += table_bytes(plans[i], descs[i].frame_count, m) + kArenaAlign;
+    }
+    for (uint32_t l = 0; l < lanes; ++l) total += arena[l] + tables[l];
+    return total;
+  };
+  Pass2Mode want = P2_CACHE;
+  uint64_t total = 0;
+  if (pass2_mode >= 0) {
+    want = (Pass2Mode)pass2_mode;
+    total = size_lanes(want);
+  } else {
+    for (Pass2Mode m : {P2_LAPS, P2_FUSED, P2_CACHE, P2_RESIDENT}) {
+      want = m;
+      if ((total = size_lanes(m)) <= left) break;
+    }
+  }
+  if (total > left)
+    return fail(set_err(ctx, FS_ERR_BUDGET, "batch needs " + std::to_string(total) + " device bytes, budget leaves " +
+                                                std::to_string(left)));
+  for (uint32_t i = 0; i < n; ++i) b->planned.push_back((int)stack_mode(plans[i], want));
   for (uint32_t l = 0; l < lanes; ++l) {
     fs_ctx* c = nullptr;
-    int rc = fs_create(ctx->device, std::max<uint64_t>(lane_bytes[l], 1), &c);
+    int rc = fs_create(ctx->device, std::max<uint64_t>(arena[l] + tables[l], 1), &c);
     if (rc != FS_OK) return fail(rc);
     b->lanes.push_back(c);
     cudaEvent_t ev;
     cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
     b->join.push_back(ev);
+    void* p = nullptr;
+    if (arena[l] && (rc = dev_alloc(c, arena[l], &p)) != FS_OK)
+      return fail(set_err(ctx, rc, std::string("lane arena: ") + fs_last_error(c)));
+    b->arenas.push_back(p);
+    b->arena_bytes.push_back(arena[l]);
   }
   cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming);
-  // stacks in lane order; each sees its lane's remaining budget, so it picks
-  // the mode its footprint was planned for
   for (uint32_t i = 0; i < n; ++i) {
     auto& it = b->items[i];
     fs_ctx* lc = b->lanes[it.lane];
-    int rc = begin_impl(lc, &descs[i], &it.stack, b->planned[i]);
+    int rc = begin_impl(lc, &descs[i], &it.stack, b->planned[i], (uint8_t*)b->arenas[it.lane],
+                        b->arena_bytes[it.lane]);
     if (rc != FS_OK) return fail(set_err(ctx, rc, std::string("stack begin: ") + fs_last_error(lc)));
     it.frames.assign(frames[i], frames[i] + descs[i].frame_count);
     it.stride = row_strides[i];
@@ -2057,6 +2194,8 @@ int fs_batch_create(fs_ctx* ctx, uint32_t n, const fs_stack_desc* descs, const v
     it.out_stride = out_strides[i];
     if (!it.out || it.out_stride < (size_t)it.stack->W * 3) return fail(set_err(ctx, FS_ERR_INVALID, "bad output"));
   }
+  // the frame tables' uploads are done before the lanes' streams read them
+  for (fs_ctx* c : b->lanes) cudaStreamSynchronize(c->stream);
   ctx->held += total;  // the lanes' memory counts against the parent's budget
   b->charged = total;
   b->runs = 0;
@@ -2112,6 +2251,7 @@ int fs_batch_destroy(fs_batch* b) {
   if (b->graph) cudaGraphDestroy(b->graph);
   for (auto& it : b->items)
     if (it.stack) fs_stack_destroy(it.stack);
+  for (size_t l = 0; l < b->arenas.size(); ++l) dev_free(b->lanes[l], b->arenas[l], b->arena_bytes[l]);
   for (fs_ctx* c : b->lanes) fs_destroy(c);
   for (cudaEvent_t ev : b->join) cudaEventDestroy(ev);
   if (b->fork) cudaEventDestroy(b->fork);

@@ -22,6 +22,11 @@
 // mask_reduce_kernel       each frame's mask pyramid, one level per launch
 //                          (level 0 normalises the weights on the fly)
 // blend_kernel<T>          the blend of one level l >= 1 over every frame
+// img_tail_kernel<T>       pass 1, the image pyramid of the small levels
+//                          (sides <= 64) of a batch, one frame per CTA
+// mask_tail_kernel<T>      pass 2, each frame's masks of the small levels
+// blend_tail_kernel<T>     pass 2, the small levels' blends, then (last CTA)
+//                          their collapse down to the first small level
 // Both:
 // collapse_kernel          parent += EXPAND(child); quantise at level 0
 //
@@ -1115,11 +1120,10 @@ __device__ void store_next_image(const ImgSmem& S, const LevelArgs& a, int x0, i
 
 }  // namespace
 
+// One 64x32 tile of frame k's level step l -> l + 1 (the split pyramid's
+// image half): Gaussian REDUCE, its store, and the tile's Laplacian.
 template <typename T, bool L0>
-__global__ void __launch_bounds__(NT) img_kernel(const __grid_constant__ LevelArgs a) {
-  extern __shared__ __align__(16) uint8_t smem_raw[];
-  ImgSmem& S = *reinterpret_cast<ImgSmem*>(smem_raw);
-  const int x0 = blockIdx.x * TW, y0 = blockIdx.y * TH, k = blockIdx.z;
+__device__ __forceinline__ void img_tile(ImgSmem& S, const LevelArgs& a, int x0, int y0, int k) {
   // region loads issued together (all in flight before the first store)
   constexpr int NI = (GH * GW + NT - 1) / NT, HALF = (NI + 1) / 2;
 #pragma unroll
@@ -1162,6 +1166,13 @@ __global__ void __launch_bounds__(NT) img_kernel(const __grid_constant__ LevelAr
   // the level-0 Laplacian stays FP32; the levels above are in the storage type
   using TL = typename std::conditional<L0, float, T>::type;
   expand_blend_step<true, ImgSmem, TL>(S, a, x0, y0, unused, (TL*)a.lap[k]);
+}
+
+template <typename T, bool L0>
+__global__ void __launch_bounds__(NT) img_kernel(const __grid_constant__ LevelArgs a) {
+  extern __shared__ __align__(16) uint8_t smem_raw[];
+  ImgSmem& S = *reinterpret_cast<ImgSmem*>(smem_raw);
+  img_tile<T, L0>(S, a, blockIdx.x * TW, blockIdx.y * TH, blockIdx.z);
 }
 
 
@@ -1858,6 +1869,239 @@ cudaError_t launch_img_level(const LevelArgs& a, int storage, cudaStream_t s) {
                       : launch_split<ImgK, false>(a, storage, s, cfg1);
 }
 
+
+// ====================================================== small-level tail
+// The split pyramid's levels whose sides are at most kTailSide (a handful of
+// 64x32 tiles each, too small to fill the GPU) go through three launches per
+// stack instead of four per level: every operation and its order are those
+// of the per-level kernels (img_tile, mask_reduce_kernel's rows, blend_kernel,
+// collapse_kernel's no-wrap EXPAND), so the bytes are the same.
+
+// Pass 1: one frame per CTA walks the tail's level steps in order; a level's
+// Gaussian written by this CTA is read back by it at the next level (after
+// the barrier that ends img_tile).
+template <typename T>
+__global__ void __launch_bounds__(NT) img_tail_kernel(const __grid_constant__ ImgTailArgs t) {
+  extern __shared__ __align__(16) uint8_t smem_raw[];
+  ImgSmem& S = *reinterpret_cast<ImgSmem*>(smem_raw);
+  const int k = blockIdx.x;
+  for (int i = 0; i < t.steps; ++i) {
+    const LevelArgs& a = t.lv[i];
+    for (int y0 = 0; y0 < a.hl; y0 += TH)
+      for (int x0 = 0; x0 < a.wl; x0 += TW) img_tile<T, false>(S, a, x0, y0, k);
+  }
+}
+
+cudaError_t launch_img_tail(const ImgTailArgs& a, int frames, int storage, cudaStream_t s) {
+  static DeviceOnce cfg[3];
+  if (a.steps < 1 || a.steps > kMaxTail || frames < 1) return cudaErrorInvalidValue;
+  const size_t sm = sizeof(ImgSmem);
+  cudaError_t e;
+  switch (storage) {
+    case FS_STORAGE_F32:
+      if ((e = configure(img_tail_kernel<float>, sm, &cfg[0])) != cudaSuccess) return e;
+      img_tail_kernel<float><<<frames, NT, sm, s>>>(a);
+      break;
+    case FS_STORAGE_F16:
+      if ((e = configure(img_tail_kernel<__half>, sm, &cfg[1])) != cudaSuccess) return e;
+      img_tail_kernel<__half><<<frames, NT, sm, s>>>(a);
+      break;
+    case FS_STORAGE_BF16:
+      if ((e = configure(img_tail_kernel<__nv_bfloat16>, sm, &cfg[2])) != cudaSuccess) return e;
+      img_tail_kernel<__nv_bfloat16><<<frames, NT, sm, s>>>(a);
+      break;
+    default:
+      return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
+// Bytes of the tail's mask-support levels T+1 .. L-1 in shared memory (each
+// at most 32 x 32 at its 32-element pitch, every later one at most half as
+// tall).
+constexpr int kTailSupportBytes = 4096;
+
+// Pass 2, masks: frame blockIdx.x, levels T+1 .. L-1.  The support of level
+// l + 1 is any supported in-range tap of the 5x5 window below it
+// (mask_support_kernel); the mask REDUCE of each output pair is
+// mask_reduce_kernel's: the five rows' horizontal sums (reduce_row), then the
+// vertical taps in order.
+template <typename TS>
+__global__ void __launch_bounds__(NT) mask_tail_kernel(const __grid_constant__ BlendTailArgs a) {
+  __shared__ __align__(16) uint8_t sms[kTailSupportBytes];
+  const int k = blockIdx.x, N = a.frames, nlev = a.levels - a.first;
+  const uint8_t* sup[kMaxTail + 1];
+  sup[0] = a.sm_first;
+  int off = 0;
+  for (int i = 1; i < nlev; ++i) {
+    const TailLevel& P = a.lv[i - 1];
+    const TailLevel& C = a.lv[i];
+    uint8_t* dst = sms + off;
+    off += (int)(C.pitch * C.h + 15) & ~15;
+    for (int p = threadIdx.x; p < C.w * C.h; p += NT) {
+      const int x = p % C.w, y = p / C.w;
+      uint8_t any = 0;
+      for (int ky = 0; ky < 5 && !any; ++ky) {
+        const int sy = 2 * y - 2 + ky;
+        if (sy < 0 || sy >= P.h) continue;
+        for (int kx = 0; kx < 5; ++kx) {
+          const int sx = 2 * x - 2 + kx;
+          if (sx < 0 || sx >= P.w) continue;
+          if (sup[i - 1][(int64_t)sy * P.pitch + sx]) {
+            any = 1;
+            break;
+          }
+        }
+      }
+      dst[(int64_t)y * C.pitch + x] = any;
+    }
+    sup[i] = dst;
+    __syncthreads();
+  }
+  for (int i = 0; i + 1 < nlev; ++i) {
+    const int l = a.first + i;
+    const TailLevel& P = a.lv[i];
+    const TailLevel& C = a.lv[i + 1];
+    const TS* in = (const TS*)a.tab[(size_t)l * 2 * N + N + k];
+    void* out = const_cast<void*>(a.tab[(size_t)(l + 1) * 2 * N + N + k]);
+    const bool top = l + 2 == a.levels;  // the top mask is f32
+    const int pairs = (C.w + 1) / 2;
+    for (int t = threadIdx.x; t < pairs * C.h; t += NT) {
+      const int j0 = 2 * (t % pairs), r = t / pairs;
+      float hv[5][2], hw[5][2];
+#pragma unroll
+      for (int u = 0; u < 5; ++u) reduce_row<TS>(in, sup[i], P.pitch, P.w, P.h, 2 * r - 2 + u, j0, hv[u], hw[u]);
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        float v = 0.f, ws = 0.f;
+#pragma unroll
+        for (int ky = 0; ky < 5; ++ky) {
+          v = fmaf(kw(ky), hv[ky][h], v);
+          ws = fmaf(kw(ky), hw[ky][h], ws);
+        }
+        if (j0 + h < C.w) {
+          const float m = ws > 0.f ? v * __fdividef(1.0f, ws) : 0.f;
+          const int64_t o = (int64_t)r * C.pitch + j0 + h;
+          if (top) stv<float>((float*)out, o, m);
+          else stv<TS>((TS*)out, o, m);
+        }
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// Horizontal no-wrap EXPAND of child row `row` at parent column x (zero
+// outside the child), expand_h1's operations.
+__device__ __forceinline__ float tail_expand_h(const float* row, int x, int wc) {
+  const int j = x >> 1;
+  auto g = [&](int i) { return (i < 0 || i >= wc) ? 0.0f : __ldcg(row + i); };
+  if (x & 1) return __fmul_rn(4.0f, __fadd_rn(g(j), g(j + 1)));
+  return __fadd_rn(__fadd_rn(g(j - 1), __fmul_rn(6.0f, g(j))), g(j + 1));
+}
+
+// Pass 2, blend + collapse: one thread per pixel of the tail levels forms
+// acc_l = sum over frames in order of lap * mask (blend_kernel); the last
+// CTA to finish (a ticket on a.counter, no waiting) adds EXPAND(acc_l) into
+// acc_{l-1} from the top down to level T with collapse_kernel's no-wrap
+// operations (every tail parent is at most kTailSide <= 512 wide), and
+// resets the ticket.
+template <typename TS>
+__global__ void __launch_bounds__(256) blend_tail_kernel(const __grid_constant__ BlendTailArgs a) {
+  __shared__ bool last;
+  const int N = a.frames, nlev = a.levels - a.first;
+  int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  int i = 0;
+  while (i < nlev && g >= (int64_t)a.lv[i].w * a.lv[i].h) {
+    g -= (int64_t)a.lv[i].w * a.lv[i].h;
+    ++i;
+  }
+  if (i < nlev) {
+    const TailLevel& V = a.lv[i];
+    const int l = a.first + i;
+    const int64_t o = (g / V.w) * V.pitch + g % V.w;
+    const void* const* lap = a.tab + (size_t)l * 2 * N;
+    const void* const* msk = lap + N;
+    float a0 = 0.0f, a1 = 0.0f, a2 = 0.0f;
+    if (l + 1 == a.levels) {
+      for (int f = 0; f < N; ++f) {
+        const float* lk = (const float*)lap[f];
+        const float m = ((const float*)msk[f])[o];
+        a0 = __fadd_rn(a0, __fmul_rn(lk[o], m));
+        a1 = __fadd_rn(a1, __fmul_rn(lk[V.plane + o], m));
+        a2 = __fadd_rn(a2, __fmul_rn(lk[2 * V.plane + o], m));
+      }
+    } else {
+      for (int f = 0; f < N; ++f) {
+        const TS* lk = (const TS*)lap[f];
+        const float m = ldv<TS>((const TS*)msk[f], o);
+        a0 = __fadd_rn(a0, __fmul_rn(ldv<TS>(lk, o), m));
+        a1 = __fadd_rn(a1, __fmul_rn(ldv<TS>(lk, V.plane + o), m));
+        a2 = __fadd_rn(a2, __fmul_rn(ldv<TS>(lk, 2 * V.plane + o), m));
+      }
+    }
+    V.acc[o] = a0;
+    V.acc[V.plane + o] = a1;
+    V.acc[2 * V.plane + o] = a2;
+  }
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = atomicAdd(a.counter, 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  for (int c_i = nlev - 1; c_i >= 1; --c_i) {
+    const TailLevel& C = a.lv[c_i];
+    const TailLevel& P = a.lv[c_i - 1];
+    for (int p = threadIdx.x; p < P.w * P.h; p += blockDim.x) {
+      const int x = p % P.w, y = p / P.w, q = y >> 1;
+      const float div = exact_expand_divisor(x, y, C.w, C.h);
+      auto hrow = [&](int c, int row) -> float {  // zero rows outside the child
+        return (row < 0 || row >= C.h) ? 0.0f : tail_expand_h(C.acc + c * C.plane + (int64_t)row * C.pitch, x, C.w);
+      };
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        float v;
+        if (y & 1) v = __fadd_rn(hrow(c, q), hrow(c, q + 1));
+        else v = __fadd_rn(__fadd_rn(hrow(c, q - 1), __fmul_rn(6.0f, hrow(c, q))), hrow(c, q + 1));
+        float* dst = P.acc + c * P.plane + (int64_t)y * P.pitch + x;
+        *dst = __fadd_rn(__ldcg(dst), __fdiv_rn(v, div));
+      }
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *a.counter = 0u;
+}
+
+cudaError_t launch_mask_tail(const BlendTailArgs& a, cudaStream_t s) {
+  const int nlev = a.levels - a.first;
+  if (a.first < 1 || nlev < 2 || nlev > kMaxTail + 1 || a.frames < 1) return cudaErrorInvalidValue;
+  int bytes = 0;
+  for (int i = 1; i < nlev; ++i) bytes += (int)(a.lv[i].pitch * a.lv[i].h + 15) & ~15;
+  if (bytes > kTailSupportBytes) return cudaErrorInvalidValue;
+  switch (a.storage) {
+    case FS_STORAGE_F32: mask_tail_kernel<float><<<a.frames, NT, 0, s>>>(a); break;
+    case FS_STORAGE_F16: mask_tail_kernel<__half><<<a.frames, NT, 0, s>>>(a); break;
+    case FS_STORAGE_BF16: mask_tail_kernel<__nv_bfloat16><<<a.frames, NT, 0, s>>>(a); break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_blend_tail(const BlendTailArgs& a, cudaStream_t s) {
+  const int nlev = a.levels - a.first;
+  if (a.first < 1 || nlev < 2 || nlev > kMaxTail + 1 || a.frames < 1 || !a.counter) return cudaErrorInvalidValue;
+  int64_t px = 0;
+  for (int i = 0; i < nlev; ++i) px += (int64_t)a.lv[i].w * a.lv[i].h;
+  const unsigned blocks = (unsigned)((px + 255) / 256);
+  switch (a.storage) {
+    case FS_STORAGE_F32: blend_tail_kernel<float><<<blocks, 256, 0, s>>>(a); break;
+    case FS_STORAGE_F16: blend_tail_kernel<__half><<<blocks, 256, 0, s>>>(a); break;
+    case FS_STORAGE_BF16: blend_tail_kernel<__nv_bfloat16><<<blocks, 256, 0, s>>>(a); break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
 
 __global__ void sum_contrib_kernel(float* acc, int64_t plane, int64_t pitch, int w, int h, const float* contrib,
                                    int K) {

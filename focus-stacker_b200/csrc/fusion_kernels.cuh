@@ -252,6 +252,48 @@ cudaError_t launch_remap(const RemapArgs& a, cudaStream_t s);
 cudaError_t launch_quantize(const float* acc, int64_t plane, int64_t pitch, int w, int h, uint8_t* out,
                             int64_t out_pitch, float* base, int64_t base_pitch, int out16, cudaStream_t s);
 
+// Small-level tail of the split pyramid: the levels whose sides are both at
+// most kTailSide, from level T >= 1 up to the top (at most kMaxTail steps),
+// in three launches instead of four per level.
+static constexpr int kTailSide = 64;
+static constexpr int kMaxTail = 8;
+
+// Pass 1: the image half of the level steps T .. T + steps - 1 of a batch
+// (lv[i] as launch_img_level takes it for level T + i), one frame per CTA,
+// the levels one after another inside the CTA.
+struct ImgTailArgs {
+  int32_t steps;
+  int32_t pad;
+  LevelArgs lv[kMaxTail];
+};
+cudaError_t launch_img_tail(const ImgTailArgs& a, int frames, int storage, cudaStream_t s);
+
+struct TailLevel {
+  int32_t w, h;
+  int64_t pitch;   // elements (bytes for u8 planes)
+  float* acc;      // accumulator, 3 planes
+  int64_t plane;   // elements per accumulator plane
+};
+// Pass 2 over levels T .. L-1 of a LAPS / FUSED stack.  tab: the stack's
+// frame table (per level l: N Laplacian pointers, the top level's Gaussians,
+// then N mask pointers; level-l masks in the level storage, the top's f32).
+struct BlendTailArgs {
+  int32_t first;             // T (>= 1)
+  int32_t levels;            // L
+  int32_t frames;            // N
+  int32_t storage;           // level storage of levels T .. L-2
+  const void* const* tab;
+  const uint8_t* sm_first;   // union mask support of level T
+  uint32_t* counter;         // zero before the blend launch; the launch leaves it zero
+  TailLevel lv[kMaxTail + 1];  // levels T .. L-1
+};
+// Each frame's masks of levels T+1 .. L-1 (one frame per CTA; the mask
+// support of those levels is formed in shared memory).
+cudaError_t launch_mask_tail(const BlendTailArgs& a, cudaStream_t s);
+// The blend of levels T .. L-1 over every frame in order, then (last CTA to
+// finish) the collapse of those levels down to level T.
+cudaError_t launch_blend_tail(const BlendTailArgs& a, cudaStream_t s);
+
 // Synthetic stacks (synth.cu).
 void synth_pose(uint64_t seed, int scene, uint32_t width, uint32_t height, uint32_t frame, uint32_t frame_count,
                 fs_pose* p);

@@ -70,6 +70,9 @@ int fs_api_version(void);
 /* Bytes of device memory in the context's live buffers (what its budget
  * counts). */
 uint64_t fs_ctx_device_bytes(const fs_ctx* ctx);
+/* The context's HBM budget in bytes (0 for a null context).  Not part of the
+ * reference. */
+uint64_t fs_ctx_budget(const fs_ctx* ctx);
 /* Wait for all work queued on the context's stream. */
 int fs_ctx_synchronize(fs_ctx* ctx);
 /* Buffers come from a stream-ordered memory pool shared by the contexts of
@@ -351,10 +354,14 @@ int fs_fuse_aligned_device_static(const void* const* dev_frames, const size_t* r
  * frames[i][0 .. frame_count-1] (device pointers, row stride row_strides[i]),
  * poses[i] (NULL list for aligned input) and a device RGB u8 output
  * dev_out[i] (row stride out_strides[i]).  The stacks are spread over `lanes`
- * streams, largest first to the least-loaded lane, and each keeps its device
- * state for the life of the batch (counted against ctx's budget; pass2_mode
- * -1 picks per stack what the budget allows, 0 caches the pass-1 planes, 1
- * keeps only the frames and remaps them again).  The first fs_batch_run
+ * streams, largest first to the least-loaded lane; the stacks of a lane run
+ * one after another and share one device arena the size of the lane's
+ * largest stack, held for the life of the batch and counted against ctx's
+ * budget.  pass2_mode: 3 split pyramid (LAPS), 4 split pyramid with level 0
+ * fused into pass 1, 0 cached pass-1 planes, 1 frames kept and remapped
+ * again (stacks of fewer than three levels take 0 in modes 3 and 4); -1
+ * takes the first of 3, 4, 0, 1 whose arenas fit the budget.  The first
+ * fs_batch_run
  * executes the work directly; the second captures the same launches into a
  * CUDA graph, which every later run replays with one graph launch, reading
  * the frames at the same addresses (refill them in place between runs).
@@ -365,7 +372,7 @@ int fs_batch_create(fs_ctx* ctx, uint32_t n, const fs_stack_desc* descs, const v
                     const size_t* out_strides, uint32_t lanes, int pass2_mode, fs_batch** out);
 int fs_batch_run(fs_batch* batch);
 int fs_batch_stack_count(const fs_batch* batch);
-/* Pass-2 mode of stack i (0 cache, 1 resident). */
+/* Pass-2 mode of stack i (0 cache, 1 resident, 3 laps, 4 fused). */
 int fs_batch_pass2_mode(const fs_batch* batch, uint32_t i);
 /* 1 once runs replay a captured graph. */
 int fs_batch_uses_graph(const fs_batch* batch);

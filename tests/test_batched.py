@@ -33,11 +33,11 @@ def make_stacks(torch, ctx, specs, seed):
     return stacks
 
 
-def alone(torch, ctx, st, storage, k=0):
-    # the batch runs the cache / resident modes (the same kernels, the same
-    # bytes); the laps mode blends level 0 in another rounding order
+def alone(torch, ctx, st, storage, k=0, mode="cache"):
+    # the cache / resident / laps modes give the same bytes; the fused mode
+    # blends level 0 in another rounding order, so it is compared with itself
     s = fsb.PyramidContrastStack(ctx, st.width, st.height, len(st.frames), roi=st.roi, level_storage=storage,
-                                 frames_per_batch=k, pass2_mode="cache")
+                                 frames_per_batch=k, pass2_mode=mode)
     for f, p in zip(st.frames, st.poses):
         s.add_frame_device(f, st.width * 3, p)
     out = s.finish()
@@ -46,14 +46,18 @@ def alone(torch, ctx, st, storage, k=0):
 
 
 @pytest.mark.parametrize("storage", [fsb.STORAGE_F32, fsb.STORAGE_F16])
-@pytest.mark.parametrize("pass2_mode", [0, 1])
+@pytest.mark.parametrize("pass2_mode", [0, 1, 3, 4])
 def test_batch_matches_stacks_alone(torch, storage, pass2_mode):
+    """Every stack of the batch gives the bytes of the same stack fused alone
+    in the same pass-2 mode, on the direct run and on graph replays, with
+    the stacks of a lane sharing one arena."""
     ctx = fsb.Context(0)
     specs = [(320, 240, 5), (640, 480, 9), (200, 150, 3), (512, 384, 12), (320, 240, 4)]
     stacks = make_stacks(torch, ctx, specs, seed=40)
-    want = [alone(torch, ctx, st, storage) for st in stacks]
+    name = fsb.api.PASS2_MODES[pass2_mode]
+    want = [alone(torch, ctx, st, storage, mode=name) for st in stacks]
     with fsb.StackBatch(ctx, stacks, lanes=3, pass2_mode=pass2_mode, level_storage=storage) as b:
-        assert b.pass2_modes() == [("cache", "resident")[pass2_mode]] * len(stacks)
+        assert b.pass2_modes() == [name] * len(stacks)
         for run in range(3):
             for st in stacks:
                 st.out.zero_()
@@ -91,4 +95,24 @@ def test_autotuner_picks_a_fitting_candidate(torch):
                             reps=2)
     assert res["best"] in [t["knobs"] for t in res["trials"]]
     assert all(t.get("graph", True) for t in res["trials"])
+    ctx.close()
+
+
+def test_lanes_share_their_arena(torch):
+    """A batch holds about one arena per lane (its largest stack), not the sum
+    over its stacks: four equal stacks on two lanes hold about half of what
+    four stacks alone would, and the default mode takes the split pyramid."""
+    ctx = fsb.Context(0)
+    stacks = make_stacks(torch, ctx, [(640, 480, 6)] * 4, seed=80)
+    one = fsb.api.stack_mode_bytes(fsb.api.stack_desc(640, 480, 6, stacks[0].roi), "laps", host_frames=False)
+    before = ctx.device_bytes()
+    with fsb.StackBatch(ctx, stacks, lanes=2) as b:
+        assert b.pass2_modes() == ["laps"] * 4
+        held = ctx.device_bytes() - before
+        assert 2 * one <= held < 3 * one, (held, one)
+        b.run()
+        b.run()
+        for st in stacks:
+            assert np.array_equal(st.out.cpu().numpy(), alone(torch, ctx, st, fsb.STORAGE_F32, mode="laps"))
+    assert ctx.device_bytes() == before
     ctx.close()

@@ -308,6 +308,36 @@ def test_pass2_modes_give_identical_results(torch, ctx):
     for m in ("laps", "fused"):
         assert close_outputs(results[m], results["cache"]), m
 
+@pytest.mark.parametrize("mode", ["laps", "fused"])
+@pytest.mark.parametrize("storage", [fsb.STORAGE_F32, fsb.STORAGE_F16])
+@pytest.mark.parametrize("W,H,F", [(320, 240, 5), (130, 70, 9), (1100, 700, 3)])
+def test_small_level_tail_matches_per_level_launches(torch, ctx, mode, storage, W, H, F):
+    """finish() blends the split pyramid's small levels (sides <= 64) and
+    collapses them in the tail launches; the phase entry points (end_pass1,
+    blend, collapse) launch those levels one by one.  Same operations in the
+    same order: the same output bytes and collapsed base."""
+    frames, poses = synth_stack(torch, ctx, W, H, F, seed=W + F)
+    roi = fsb.compute_common_overlap_roi([True] * F, [W] * F, [H] * F, poses)
+    outs = []
+    for phases in (False, True):
+        st = fsb.PyramidContrastStack(ctx, W, H, F, roi=roi, frames_per_batch=3, pass2_mode=mode,
+                                      level_storage=storage)
+        base = torch.zeros((roi.height, roi.width, 3), dtype=torch.float32, device="cuda:0")
+        st.set_base_output(base, roi.width * 3)
+        for f, p in zip(frames, poses):
+            st.add_frame(f, p)
+        if phases:
+            st.end_pass1()
+            st.blend()
+            out = st.collapse()
+        else:
+            out = st.finish()
+        st.close()
+        outs.append((out, base.cpu().numpy()))
+    assert np.array_equal(outs[0][0], outs[1][0])
+    assert np.array_equal(outs[0][1], outs[1][1])
+
+
 @pytest.mark.parametrize("storage", [fsb.STORAGE_F32, fsb.STORAGE_F16, fsb.STORAGE_BF16])
 def test_laps_large_levels_match_cache(torch, ctx, storage):
     # levels wider than 512 take the streaming pyramid kernel in the laps and

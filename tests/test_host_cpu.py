@@ -316,3 +316,35 @@ def test_oracle_synthetic_frame_rows_and_statistics():
     assert np.array_equal(part[100:120], full[100:120])
     assert not part[:100].any() and not part[120:].any()
     assert 90 < full.mean() < 160 and 15 < full.std() < 60
+
+
+def test_autotuner_caches_the_winner_per_workload(tmp_path, monkeypatch):
+    """The batched-form tuner times every candidate once per workload
+    signature and answers later calls from its JSON cache (no device work:
+    the timing call is replaced by a fake)."""
+    from types import SimpleNamespace
+
+    at = fsb.autotune
+    calls = []
+
+    def fake_time(ctx, stacks, reps=3, level_storage=0, **knobs):
+        calls.append(knobs)
+        if knobs["pass2_mode"] == 0:
+            raise fsb.FocusCudaError(3, "does not fit")
+        return {"knobs": dict(knobs), "s_per_run": 1.0 / knobs["lanes"] + 0.01 * knobs["frames_per_batch"]}
+
+    monkeypatch.setattr(at, "time_batch", fake_time)
+    ctx = SimpleNamespace(budget=lambda: 120e9)
+    stacks = [SimpleNamespace(width=640, height=480, frames=[0] * 5), SimpleNamespace(width=320, height=240,
+                                                                                       frames=[0] * 3)]
+    path = str(tmp_path / "tune.json")
+    space = {"lanes": (2, 4), "frames_per_batch": (4, 8), "pass2_mode": (3, 0)}
+    r1 = at.tune(ctx, stacks, space=space, cache_path=path)
+    assert not r1["cached"] and len(calls) == 8
+    assert r1["best"] == {"lanes": 4, "frames_per_batch": 4, "pass2_mode": 3}
+    assert sum("skipped" in t for t in r1["trials"]) == 4
+    r2 = at.tune(ctx, list(reversed(stacks)), space=space, cache_path=path)
+    assert r2["cached"] and r2["best"] == r1["best"] and len(calls) == 8
+    # another workload is timed again
+    at.tune(ctx, stacks[:1], space=space, cache_path=path)
+    assert len(calls) == 16
