@@ -1029,13 +1029,15 @@ StackPlan plan_stack(const fs_stack_desc& d) {
 // staging ring counts when frames come from host memory.
 uint64_t plan_bytes(const StackPlan& p, uint32_t frames, Pass2Mode mode, bool host_frames) {
   const uint64_t staging = host_frames ? (uint64_t)p.frame_bytes * p.staging_slots : 0;
+  // split pyramid: the frame table and, after it, the small-level tail's counter
+  const uint64_t table = 16;
   switch (mode) {
     case P2_LAPS:
       return p.fixed + (uint64_t)p.planes / 2 * p.K + ((uint64_t)p.laps_frame + 2 * p.L * sizeof(float*)) * frames +
-             staging;
+             table + staging;
     case P2_FUSED:
       return p.fixed + p.fused_fixed + (uint64_t)p.planes / 2 * p.K +
-             ((uint64_t)p.fused_frame + 2 * p.L * sizeof(float*)) * frames + staging;
+             ((uint64_t)p.fused_frame + 2 * p.L * sizeof(float*)) * frames + table + staging;
     case P2_CACHE: return p.fixed + (uint64_t)p.planes * frames + staging;
     case P2_RESIDENT: return p.fixed + (uint64_t)p.planes * p.K + (uint64_t)p.frame_bytes * frames;
     default: return p.fixed + (uint64_t)p.planes * p.K + staging;
@@ -2081,9 +2083,10 @@ uint64_t arena_need(const StackPlan& p, uint32_t frames, Pass2Mode m) {
   return plan_bytes(p, frames, m, false) + pieces * kArenaAlign;
 }
 
-// The split-pyramid frame table of a stack (allocated from the lane's pool).
+// The split-pyramid frame table of a stack and the tail counter after it
+// (allocated from the lane's pool).
 uint64_t table_bytes(const StackPlan& p, uint32_t frames, Pass2Mode m) {
-  return (m == P2_LAPS || m == P2_FUSED) ? 2ull * p.L * frames * sizeof(float*) : 0;
+  return (m == P2_LAPS || m == P2_FUSED) ? 2ull * p.L * frames * sizeof(float*) + 16 : 0;
 }
 
 // The stack's mode when the batch asks for `want`: the split-pyramid modes
