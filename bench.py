@@ -378,7 +378,7 @@ def precision_error_band(fsb, torch, ctx, dev, frames, poses, W, H, roi, rows=25
     return out
 
 
-def serving_form(fsb, torch, dev, seed, n_requests, rates, budget_gb, workers=8, repeats=1):
+def serving_form(fsb, torch, dev, seed, n_requests, rates, budget_gb, workers=16, repeats=1):
     """Serving form: Poisson request streams (sizes 640x480 .. 6000x4000 with
     4-40 frames, 5 % 7952x5304 stacks of up to 143 frames) admitted against an
     HBM budget; frames are device-resident (a synthetic pool per size, as a

@@ -139,6 +139,13 @@ int dev_alloc(fs_ctx* ctx, size_t bytes, void** out, cudaStream_t on = nullptr) 
     return set_err(ctx, FS_ERR_BUDGET, "device memory budget exceeded (" + std::to_string(ctx->held + bytes) +
                                            " > " + std::to_string(ctx->budget) + " bytes)");
   cudaError_t e = cudaMallocFromPoolAsync(out, bytes, ctx->mempool, on ? on : ctx->stream);
+  if (e == cudaErrorMemoryAllocation && ctx->mempool) {
+    // the pool keeps freed memory for reuse; when a request finds none that
+    // fits, give back what it holds unused (completed frees only) and retry
+    cudaGetLastError();
+    cudaMemPoolTrimTo(ctx->mempool, 0);
+    e = cudaMallocFromPoolAsync(out, bytes, ctx->mempool, on ? on : ctx->stream);
+  }
   if (e != cudaSuccess) {
     cudaGetLastError();
     return set_err(ctx, FS_ERR_OOM, std::string("device allocation failed: ") + cudaGetErrorString(e));
@@ -1465,10 +1472,9 @@ static int pass2_impl(fs_stack* s, fs_frame_fetch_cb refetch, void* user, bool f
   if (s->mode == P2_LAPS || s->mode == P2_FUSED) {
     if (s->mode == P2_LAPS) {
       // level-0 blend of every frame at once, streaming over the Laplacians
-      // (it also turns each frame's weight into its normalised mask)
       e = timed(ctx, "blend0", [&] {
         return launch_blend0(s->acc[0], s->pitch[0] * s->lh[0], s->pitch[0], (int)s->W, (int)s->H, s->norm, s->tab,
-                             (float* const*)(s->tab + N), (int)N, inv_count, st);
+                             s->tab + N, (int)N, inv_count, st);
       });
     } else {
       // level 0: the weighted Laplacian sum of pass 1 divided by the complete
@@ -1491,9 +1497,8 @@ static int pass2_impl(fs_stack* s, fs_frame_fetch_cb refetch, void* user, bool f
       m.hn = (int32_t)s->lh[l + 1];
       m.pitch_l = s->pitch[l];
       m.pitch_n = s->pitch[l + 1];
-      // FUSED level 0: each frame's raw weight, normalised by the weight sum on
-      // the fly (LAPS: blend0 has already written the normalised masks)
-      m.norm = l == 0 && s->mode == P2_FUSED ? s->norm : nullptr;
+      // level 0: each frame's raw weight, normalised by the weight sum on the fly
+      m.norm = l == 0 ? s->norm : nullptr;
       m.inv_count = inv_count;
       const int in_storage = l == 0 ? FS_STORAGE_F32 : s->storage;
       const int out_storage = l + 2 < s->L ? s->storage : FS_STORAGE_F32;

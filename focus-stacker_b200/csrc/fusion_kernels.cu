@@ -1179,10 +1179,10 @@ __global__ void __launch_bounds__(NT) img_kernel(const __grid_constant__ LevelAr
 // Level-0 blend of a whole stack in frame order, one pixel per thread:
 // acc = sum over frames of lap_k * (w_k / weight sum) (1 / N where the sum
 // is <= 1e-12), the same products and sums the per-batch kernels form.
-// The normalised mask replaces each frame's weight in place (the level-0
-// mask REDUCE then reads it without dividing again).
+// The weights stay as they are: the level-0 mask REDUCE forms the same
+// quotients again as it reads them.
 __global__ void blend0_kernel(float* acc, int64_t plane, int64_t pitch, int w, int h, const float* norm,
-                              const float* const* lap, float* const* wgt, int frames, float inv_count) {
+                              const float* const* lap, const float* const* wgt, int frames, float inv_count) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= (int64_t)w * h) return;
   const int64_t o = (i / w) * pitch + i % w;
@@ -1198,14 +1198,13 @@ __global__ void blend0_kernel(float* acc, int64_t plane, int64_t pitch, int w, i
         l0[u] = __ldg(lk + o);
         l1[u] = __ldg(lk + plane + o);
         l2[u] = __ldg(lk + 2 * plane + o);
-        wv[u] = wgt[k0 + u][o];
+        wv[u] = __ldg(wgt[k0 + u] + o);
       }
     }
 #pragma unroll
     for (int u = 0; u < U; ++u) {
       if (k0 + u < frames) {
         const float m = nv > 1e-12f ? __fdiv_rn(wv[u], nv) : inv_count;
-        wgt[k0 + u][o] = m;
         a0 = __fadd_rn(a0, __fmul_rn(l0[u], m));
         a1 = __fadd_rn(a1, __fmul_rn(l1[u], m));
         a2 = __fadd_rn(a2, __fmul_rn(l2[u], m));
@@ -1385,14 +1384,17 @@ __device__ __forceinline__ void reduce_row(const T* in, const uint8_t* sm, int64
   }
 }
 
+// Grid: frames fastest (blockIdx.x), then column and row blocks, so that the
+// CTAs resident together read the same region's support (and, at level 0,
+// weight sum) through L2 instead of fetching it again for every frame.
 template <typename TI, typename TO, bool N0 = false>
 __global__ void __launch_bounds__(32 * kReduceWarps) mask_reduce_kernel(const __grid_constant__ MaskReduceArgs a) {
-  const int j0 = 2 * (int)(blockIdx.x * 32 + threadIdx.x);
-  const int i0 = (int)(blockIdx.y * kReduceWarps + threadIdx.y) * kReduceRows;
+  const int j0 = 2 * (int)(blockIdx.y * 32 + threadIdx.x);
+  const int i0 = (int)(blockIdx.z * kReduceWarps + threadIdx.y) * kReduceRows;
   if (j0 >= a.wn || i0 >= a.hn) return;  // no barriers below
   const int i1 = min(i0 + kReduceRows, a.hn);
-  const TI* in = (const TI*)a.in[blockIdx.z];
-  TO* out = (TO*)a.out[blockIdx.z];
+  const TI* in = (const TI*)a.in[blockIdx.x];
+  TO* out = (TO*)a.out[blockIdx.x];
   // window of horizontal sums: rows 2i - 2 .. 2i + 2 for output row i
   float hv[5][2], hw[5][2];
 #pragma unroll
@@ -1436,11 +1438,11 @@ static cudaError_t launch_mask_reduce_in(const MaskReduceArgs& a, dim3 grid, dim
 
 cudaError_t launch_mask_reduce(const MaskReduceArgs& a, int frames, int in_storage, int out_storage,
                                cudaStream_t s) {
-  if (frames <= 0 || frames > 65535) return cudaErrorInvalidValue;
   const dim3 block(32, kReduceWarps);
-  const dim3 grid((unsigned)((a.wn + 63) / 64), (unsigned)((a.hn + kReduceWarps * kReduceRows - 1) /
-                                                              (kReduceWarps * kReduceRows)),
-                  (unsigned)frames);
+  const unsigned gx = (unsigned)((a.wn + 63) / 64);
+  const unsigned gy = (unsigned)((a.hn + kReduceWarps * kReduceRows - 1) / (kReduceWarps * kReduceRows));
+  if (frames <= 0 || gx > 65535u || gy > 65535u) return cudaErrorInvalidValue;
+  const dim3 grid((unsigned)frames, gx, gy);
   if (a.norm) {  // level 0 of a FUSED stack: raw weights, normalised on the fly
     if (in_storage != FS_STORAGE_F32) return cudaErrorInvalidValue;
     return launch_mask_reduce_in<float, true>(a, grid, block, out_storage, s);
@@ -1814,7 +1816,7 @@ static cudaError_t launch_img_stream(const LevelArgs& a, cudaStream_t s) {
 }
 
 cudaError_t launch_blend0(float* acc, int64_t plane, int64_t pitch, int w, int h, const float* norm,
-                          const float* const* lap, float* const* wgt, int frames, float inv_count,
+                          const float* const* lap, const float* const* wgt, int frames, float inv_count,
                           cudaStream_t s) {
   const int64_t n = (int64_t)w * h;
   blend0_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(acc, plane, pitch, w, h, norm, lap, wgt, frames,
@@ -1995,19 +1997,29 @@ __global__ void __launch_bounds__(NT) mask_tail_kernel(const __grid_constant__ B
 // outside the child), expand_h1's operations.
 __device__ __forceinline__ float tail_expand_h(const float* row, int x, int wc) {
   const int j = x >> 1;
-  auto g = [&](int i) { return (i < 0 || i >= wc) ? 0.0f : __ldcg(row + i); };
+  auto g = [&](int i) { return (i < 0 || i >= wc) ? 0.0f : row[i]; };
   if (x & 1) return __fmul_rn(4.0f, __fadd_rn(g(j), g(j + 1)));
   return __fadd_rn(__fadd_rn(g(j - 1), __fmul_rn(6.0f, g(j))), g(j + 1));
 }
 
+// Shared-memory bytes of the tail's accumulators (3 planes per level, rows
+// of the level's width).
+__host__ __device__ inline int tail_acc_floats(const BlendTailArgs& a) {
+  int n = 0;
+  for (int i = 0; i < a.levels - a.first; ++i) n += 3 * a.lv[i].w * a.lv[i].h;
+  return n;
+}
+
 // Pass 2, blend + collapse: one thread per pixel of the tail levels forms
-// acc_l = sum over frames in order of lap * mask (blend_kernel); the last
-// CTA to finish (a ticket on a.counter, no waiting) adds EXPAND(acc_l) into
-// acc_{l-1} from the top down to level T with collapse_kernel's no-wrap
-// operations (every tail parent is at most kTailSide <= 512 wide), and
-// resets the ticket.
+// acc_l = sum over frames in order of lap * mask (blend_kernel, its loads
+// issued four frames at a time); the last CTA to finish (a ticket on
+// a.counter, no waiting) brings every tail level's accumulator into shared
+// memory, adds EXPAND(acc_l) into acc_{l-1} from the top down to level T with
+// collapse_kernel's no-wrap operations (every tail parent is at most
+// kTailSide <= 512 wide), writes level T back and resets the ticket.
 template <typename TS>
 __global__ void __launch_bounds__(256) blend_tail_kernel(const __grid_constant__ BlendTailArgs a) {
+  extern __shared__ float tsm[];
   __shared__ bool last;
   const int N = a.frames, nlev = a.levels - a.first;
   int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -2022,22 +2034,36 @@ __global__ void __launch_bounds__(256) blend_tail_kernel(const __grid_constant__
     const int64_t o = (g / V.w) * V.pitch + g % V.w;
     const void* const* lap = a.tab + (size_t)l * 2 * N;
     const void* const* msk = lap + N;
+    const bool top = l + 1 == a.levels;  // the top level's Gaussians and masks are f32
     float a0 = 0.0f, a1 = 0.0f, a2 = 0.0f;
-    if (l + 1 == a.levels) {
-      for (int f = 0; f < N; ++f) {
-        const float* lk = (const float*)lap[f];
-        const float m = ((const float*)msk[f])[o];
-        a0 = __fadd_rn(a0, __fmul_rn(lk[o], m));
-        a1 = __fadd_rn(a1, __fmul_rn(lk[V.plane + o], m));
-        a2 = __fadd_rn(a2, __fmul_rn(lk[2 * V.plane + o], m));
+    constexpr int U = 4;
+    for (int f0 = 0; f0 < N; f0 += U) {
+      float l0[U], l1[U], l2[U], mv[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        if (f0 + u < N) {
+          if (top) {
+            const float* lk = (const float*)lap[f0 + u];
+            l0[u] = lk[o];
+            l1[u] = lk[V.plane + o];
+            l2[u] = lk[2 * V.plane + o];
+            mv[u] = ((const float*)msk[f0 + u])[o];
+          } else {
+            const TS* lk = (const TS*)lap[f0 + u];
+            l0[u] = ldv<TS>(lk, o);
+            l1[u] = ldv<TS>(lk, V.plane + o);
+            l2[u] = ldv<TS>(lk, 2 * V.plane + o);
+            mv[u] = ldv<TS>((const TS*)msk[f0 + u], o);
+          }
+        }
       }
-    } else {
-      for (int f = 0; f < N; ++f) {
-        const TS* lk = (const TS*)lap[f];
-        const float m = ldv<TS>((const TS*)msk[f], o);
-        a0 = __fadd_rn(a0, __fmul_rn(ldv<TS>(lk, o), m));
-        a1 = __fadd_rn(a1, __fmul_rn(ldv<TS>(lk, V.plane + o), m));
-        a2 = __fadd_rn(a2, __fmul_rn(ldv<TS>(lk, 2 * V.plane + o), m));
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        if (f0 + u < N) {
+          a0 = __fadd_rn(a0, __fmul_rn(l0[u], mv[u]));
+          a1 = __fadd_rn(a1, __fmul_rn(l1[u], mv[u]));
+          a2 = __fadd_rn(a2, __fmul_rn(l2[u], mv[u]));
+        }
       }
     }
     V.acc[o] = a0;
@@ -2050,25 +2076,51 @@ __global__ void __launch_bounds__(256) blend_tail_kernel(const __grid_constant__
   __syncthreads();
   if (!last) return;
   __threadfence();
+  // the tail accumulators into shared memory: level i at off[i], plane c at
+  // + c * w * h, rows of w floats
+  int off[kMaxTail + 1];
+  {
+    int n = 0;
+    for (int k = 0; k < nlev; ++k) {
+      off[k] = n;
+      const TailLevel& V = a.lv[k];
+      for (int e = threadIdx.x; e < 3 * V.w * V.h; e += blockDim.x) {
+        const int c = e / (V.w * V.h), r = e % (V.w * V.h);
+        tsm[n + e] = __ldcg(V.acc + c * V.plane + (int64_t)(r / V.w) * V.pitch + r % V.w);
+      }
+      n += 3 * V.w * V.h;
+    }
+  }
+  __syncthreads();
   for (int c_i = nlev - 1; c_i >= 1; --c_i) {
     const TailLevel& C = a.lv[c_i];
     const TailLevel& P = a.lv[c_i - 1];
+    const float* cs = tsm + off[c_i];
+    float* ps = tsm + off[c_i - 1];
     for (int p = threadIdx.x; p < P.w * P.h; p += blockDim.x) {
       const int x = p % P.w, y = p / P.w, q = y >> 1;
       const float div = exact_expand_divisor(x, y, C.w, C.h);
-      auto hrow = [&](int c, int row) -> float {  // zero rows outside the child
-        return (row < 0 || row >= C.h) ? 0.0f : tail_expand_h(C.acc + c * C.plane + (int64_t)row * C.pitch, x, C.w);
-      };
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
+        const float* cp = cs + c * C.w * C.h;
+        auto hrow = [&](int row) -> float {  // zero rows outside the child
+          return (row < 0 || row >= C.h) ? 0.0f : tail_expand_h(cp + row * C.w, x, C.w);
+        };
         float v;
-        if (y & 1) v = __fadd_rn(hrow(c, q), hrow(c, q + 1));
-        else v = __fadd_rn(__fadd_rn(hrow(c, q - 1), __fmul_rn(6.0f, hrow(c, q))), hrow(c, q + 1));
-        float* dst = P.acc + c * P.plane + (int64_t)y * P.pitch + x;
-        *dst = __fadd_rn(__ldcg(dst), __fdiv_rn(v, div));
+        if (y & 1) v = __fadd_rn(hrow(q), hrow(q + 1));
+        else v = __fadd_rn(__fadd_rn(hrow(q - 1), __fmul_rn(6.0f, hrow(q))), hrow(q + 1));
+        float* dst = ps + c * P.w * P.h + p;
+        *dst = __fadd_rn(*dst, __fdiv_rn(v, div));
       }
     }
     __syncthreads();
+  }
+  {
+    const TailLevel& V = a.lv[0];
+    for (int e = threadIdx.x; e < 3 * V.w * V.h; e += blockDim.x) {
+      const int c = e / (V.w * V.h), r = e % (V.w * V.h);
+      V.acc[c * V.plane + (int64_t)(r / V.w) * V.pitch + r % V.w] = tsm[e];
+    }
   }
   if (threadIdx.x == 0) *a.counter = 0u;
 }
@@ -2088,17 +2140,38 @@ cudaError_t launch_mask_tail(const BlendTailArgs& a, cudaStream_t s) {
   return cudaGetLastError();
 }
 
+// Largest shared memory of the blend tail: every level's side is at most
+// kTailSide, so its accumulators take at most 3 x 4 x (64^2 + 32^2 + ...) B.
+constexpr size_t kTailAccBytes = 3 * 4 * (kTailSide * kTailSide * 4 / 3 + 64);
+
 cudaError_t launch_blend_tail(const BlendTailArgs& a, cudaStream_t s) {
+  static DeviceOnce cfg[3];
   const int nlev = a.levels - a.first;
   if (a.first < 1 || nlev < 2 || nlev > kMaxTail + 1 || a.frames < 1 || !a.counter) return cudaErrorInvalidValue;
   int64_t px = 0;
-  for (int i = 0; i < nlev; ++i) px += (int64_t)a.lv[i].w * a.lv[i].h;
+  for (int i = 0; i < nlev; ++i) {
+    if (a.lv[i].w > kTailSide || a.lv[i].h > kTailSide) return cudaErrorInvalidValue;
+    px += (int64_t)a.lv[i].w * a.lv[i].h;
+  }
+  const size_t sm = (size_t)tail_acc_floats(a) * sizeof(float);
+  if (sm > kTailAccBytes) return cudaErrorInvalidValue;
   const unsigned blocks = (unsigned)((px + 255) / 256);
+  cudaError_t e;
   switch (a.storage) {
-    case FS_STORAGE_F32: blend_tail_kernel<float><<<blocks, 256, 0, s>>>(a); break;
-    case FS_STORAGE_F16: blend_tail_kernel<__half><<<blocks, 256, 0, s>>>(a); break;
-    case FS_STORAGE_BF16: blend_tail_kernel<__nv_bfloat16><<<blocks, 256, 0, s>>>(a); break;
-    default: return cudaErrorInvalidValue;
+    case FS_STORAGE_F32:
+      if ((e = configure(blend_tail_kernel<float>, kTailAccBytes, &cfg[0])) != cudaSuccess) return e;
+      blend_tail_kernel<float><<<blocks, 256, sm, s>>>(a);
+      break;
+    case FS_STORAGE_F16:
+      if ((e = configure(blend_tail_kernel<__half>, kTailAccBytes, &cfg[1])) != cudaSuccess) return e;
+      blend_tail_kernel<__half><<<blocks, 256, sm, s>>>(a);
+      break;
+    case FS_STORAGE_BF16:
+      if ((e = configure(blend_tail_kernel<__nv_bfloat16>, kTailAccBytes, &cfg[2])) != cudaSuccess) return e;
+      blend_tail_kernel<__nv_bfloat16><<<blocks, 256, sm, s>>>(a);
+      break;
+    default:
+      return cudaErrorInvalidValue;
   }
   return cudaGetLastError();
 }

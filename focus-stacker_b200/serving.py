@@ -106,7 +106,6 @@ class _Worker:
         self.busy = False
         self.reserved = 0  # footprint of the stack in flight
         self.mode = None   # its pass-2 mode
-        self.cached = 0    # upper bound of the memory its last stack left cached in the pool
 
 
 class StackServer:
@@ -140,10 +139,6 @@ class StackServer:
         self.close()
 
     # -------------------------------------------------------------- admission
-    def _in_use(self, exclude: Optional[_Worker]) -> int:
-        """Bytes reserved by busy workers and cached by idle ones."""
-        return sum((w.reserved if w.busy else w.cached) for w in self.workers if w is not exclude)
-
     def _try_admit(self, req: StackRequest, roi: api.Rect):
         idle = [w for w in self.workers if not w.busy]
         if not idle:
@@ -151,9 +146,9 @@ class StackServer:
         w = idle[0]
         desc = api.stack_desc(req.width, req.height, req.frames, roi, level_storage=req.level_storage,
                               frames_per_batch=self.frames_per_batch)
-        # the first mode that fits once idle workers' cached memory is
-        # released (bytes with the upload staging ring; the stack is begun in
-        # exactly that mode)
+        # the first mode that fits what the busy workers leave of the budget
+        # (bytes with the upload staging ring; the stack is begun in exactly
+        # that mode)
         busy = sum(o.reserved for o in self.workers if o.busy)
         avail = min(max(0, self.budget - busy), self.max_stack)
         mode, nbytes = None, 0
@@ -167,11 +162,10 @@ class StackServer:
                 break
         if mode is None:
             return None
-        if nbytes > self.budget - self._in_use(w):
-            for o in self.workers:
-                if o is not w and not o.busy and o.cached > 0:
-                    o.ctx.trim()
-                    o.cached = 0
+        # the stacks' memory comes from the device's shared pool, which keeps
+        # freed blocks for the next stacks (trimmed by the library only when
+        # an allocation finds nothing that fits): no trim here, which would
+        # hand the pool's memory back and make the next stacks map it again
         w.busy = True
         w.reserved = nbytes
         w.mode = mode
@@ -227,7 +221,6 @@ class StackServer:
                 if res is not None:
                     results[req.rid] = res
                 w.busy = False
-                w.cached = max(w.cached, w.reserved)
                 w.reserved = 0
                 lock.notify_all()
 
