@@ -67,7 +67,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-forms", action="store_true", help="skip the precision / serving / batched legs")
     ap.add_argument("--precision-frames", type=int, default=143,
-                    help="frames of the precision-form stack (7952x5304 each)")
+                    help="frames of the precision-form stack (7952x5304 each; 0: skip)")
     ap.add_argument("--serving-requests", type=int, default=500, help="requests per arrival rate (serving form)")
     ap.add_argument("--serving-rates", default="20,40,60", help="swept Poisson arrival rates, requests/s")
     ap.add_argument("--serving-repeats", type=int, default=2,
@@ -766,7 +766,9 @@ def main():
         del frames
         ctx.trim()
         torch.cuda.empty_cache()
-        forms = {"precision": precision_form(fsb, torch, dev, args.seed + rank, args.precision_frames)}
+        forms = {}
+        if args.precision_frames > 0:
+            forms["precision"] = precision_form(fsb, torch, dev, args.seed + rank, args.precision_frames)
         if args.serving_requests > 0:
             rates = [float(x) for x in args.serving_rates.split(",") if x]
             forms["serving"] = serving_form(fsb, torch, dev, args.seed + rank, args.serving_requests, rates,

@@ -1472,9 +1472,10 @@ static int pass2_impl(fs_stack* s, fs_frame_fetch_cb refetch, void* user, bool f
   if (s->mode == P2_LAPS || s->mode == P2_FUSED) {
     if (s->mode == P2_LAPS) {
       // level-0 blend of every frame at once, streaming over the Laplacians
+      // (it also turns each frame's weight into its normalised mask)
       e = timed(ctx, "blend0", [&] {
         return launch_blend0(s->acc[0], s->pitch[0] * s->lh[0], s->pitch[0], (int)s->W, (int)s->H, s->norm, s->tab,
-                             s->tab + N, (int)N, inv_count, st);
+                             (float* const*)(s->tab + N), (int)N, inv_count, st);
       });
     } else {
       // level 0: the weighted Laplacian sum of pass 1 divided by the complete
@@ -1497,8 +1498,9 @@ static int pass2_impl(fs_stack* s, fs_frame_fetch_cb refetch, void* user, bool f
       m.hn = (int32_t)s->lh[l + 1];
       m.pitch_l = s->pitch[l];
       m.pitch_n = s->pitch[l + 1];
-      // level 0: each frame's raw weight, normalised by the weight sum on the fly
-      m.norm = l == 0 ? s->norm : nullptr;
+      // FUSED level 0: each frame's raw weight, normalised by the weight sum on
+      // the fly (LAPS: blend0 has already written the normalised masks)
+      m.norm = l == 0 && s->mode == P2_FUSED ? s->norm : nullptr;
       m.inv_count = inv_count;
       const int in_storage = l == 0 ? FS_STORAGE_F32 : s->storage;
       const int out_storage = l + 2 < s->L ? s->storage : FS_STORAGE_F32;

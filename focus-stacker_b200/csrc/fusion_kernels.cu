@@ -1179,10 +1179,11 @@ __global__ void __launch_bounds__(NT) img_kernel(const __grid_constant__ LevelAr
 // Level-0 blend of a whole stack in frame order, one pixel per thread:
 // acc = sum over frames of lap_k * (w_k / weight sum) (1 / N where the sum
 // is <= 1e-12), the same products and sums the per-batch kernels form.
-// The weights stay as they are: the level-0 mask REDUCE forms the same
-// quotients again as it reads them.
+// The normalised mask replaces each frame's weight in place (the level-0
+// mask REDUCE then reads it without dividing again: forming the quotients
+// there, seven per tap row, costs more than this write).
 __global__ void blend0_kernel(float* acc, int64_t plane, int64_t pitch, int w, int h, const float* norm,
-                              const float* const* lap, const float* const* wgt, int frames, float inv_count) {
+                              const float* const* lap, float* const* wgt, int frames, float inv_count) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= (int64_t)w * h) return;
   const int64_t o = (i / w) * pitch + i % w;
@@ -1198,13 +1199,14 @@ __global__ void blend0_kernel(float* acc, int64_t plane, int64_t pitch, int w, i
         l0[u] = __ldg(lk + o);
         l1[u] = __ldg(lk + plane + o);
         l2[u] = __ldg(lk + 2 * plane + o);
-        wv[u] = __ldg(wgt[k0 + u] + o);
+        wv[u] = wgt[k0 + u][o];
       }
     }
 #pragma unroll
     for (int u = 0; u < U; ++u) {
       if (k0 + u < frames) {
         const float m = nv > 1e-12f ? __fdiv_rn(wv[u], nv) : inv_count;
+        wgt[k0 + u][o] = m;
         a0 = __fadd_rn(a0, __fmul_rn(l0[u], m));
         a1 = __fadd_rn(a1, __fmul_rn(l1[u], m));
         a2 = __fadd_rn(a2, __fmul_rn(l2[u], m));
@@ -1816,7 +1818,7 @@ static cudaError_t launch_img_stream(const LevelArgs& a, cudaStream_t s) {
 }
 
 cudaError_t launch_blend0(float* acc, int64_t plane, int64_t pitch, int w, int h, const float* norm,
-                          const float* const* lap, const float* const* wgt, int frames, float inv_count,
+                          const float* const* lap, float* const* wgt, int frames, float inv_count,
                           cudaStream_t s) {
   const int64_t n = (int64_t)w * h;
   blend0_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(acc, plane, pitch, w, h, norm, lap, wgt, frames,

@@ -234,10 +234,11 @@ cudaError_t launch_collapse(const CollapseArgs& a, cudaStream_t s);
 // in0[k].rgba.
 cudaError_t launch_img_level(const LevelArgs& a, int storage, cudaStream_t s);
 // Level-0 blend of all frames of a stack (device tables of each frame's
-// level-0 Laplacian and weight planes), written over acc; the weights are
-// left as they are (launch_mask_reduce normalises them again at level 0).
+// level-0 Laplacian and weight planes), written over acc; each weight plane
+// is replaced by the frame's normalised mask, which launch_mask_reduce then
+// reads.
 cudaError_t launch_blend0(float* acc, int64_t plane, int64_t pitch, int w, int h, const float* norm,
-                          const float* const* lap, const float* const* wgt, int frames, float inv_count,
+                          const float* const* lap, float* const* wgt, int frames, float inv_count,
                           cudaStream_t s);
 // acc = sum over frames k, in order, of lap[k] (3 planes of `plane`) times
 // mask[k] (both in storage T: 0 f32, 1 f16, 2 bf16), written over acc.
