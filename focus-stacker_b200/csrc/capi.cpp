@@ -375,6 +375,7 @@ int launch_remap_weights_batch(fs_stack* s, const std::vector<fs_stack::Frame>& 
   cudaError_t e = timed(s->ctx, pass1 ? "pass1" : "remap_weights",
                         [&] { return launch_remap_weights(a, (int)s->border, s->ctx->stream); });
   if (e != cudaSuccess) return cuda_err(s->ctx, e, "remap/weights launch");
+  s->ctx->launches += 1;  // two kernels: the remap of the tiles, then the weights
   return FS_OK;
 }
 
