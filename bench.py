@@ -69,7 +69,7 @@ def parse():
     ap.add_argument("--precision-frames", type=int, default=143,
                     help="frames of the precision-form stack (7952x5304 each; 0: skip)")
     ap.add_argument("--serving-requests", type=int, default=500, help="requests per arrival rate (serving form)")
-    ap.add_argument("--serving-rates", default="20,40,60", help="swept Poisson arrival rates, requests/s")
+    ap.add_argument("--serving-rates", default="20,40,60,100", help="swept Poisson arrival rates, requests/s")
     ap.add_argument("--serving-repeats", type=int, default=2,
                     help="runs per rate (independent arrival streams), so that the spread of p99 is on record")
     ap.add_argument("--serving-budget-gb", type=float, default=120.0)

@@ -418,8 +418,19 @@ __global__ void __launch_bounds__(NT, 6) weights_kernel(const __grid_constant__ 
             __byte_perm(__byte_perm(q.x, q.y, 0x0073u), __byte_perm(q.z, q.w, 0x0073u), 0x5410u);
     }
     __syncthreads();
+    // rows 0..31 first, a warp per column block, then the RH - 32 halo rows:
+    // the lanes of a warp never wrap to a second column block, whose rows
+    // would fall on the same shared-memory banks
+    static_assert(NT == 32 * (TW / 8), "one pass covers rows 0..31 of every column block");
     for (int it = threadIdx.x; it < RH * (TW / 8); it += NT) {
-      const int r = it % RH, c0 = (it / RH) * 8;
+      int r, c0;
+      if (it < NT) {
+        r = it % 32;
+        c0 = (it / 32) * 8;
+      } else {
+        r = 32 + (it - NT) % (RH - 32);
+        c0 = ((it - NT) / (RH - 32)) * 8;
+      }
       window_row8<B>(S.kv + r * KS + c0 + CB - B, S.h1 + r * HS + c0, S.h2 + r * HS + c0);
     }
     __syncthreads();
