@@ -1814,15 +1814,48 @@ __global__ void __launch_bounds__(32 * kImgWarps) img_stream_kernel(const __grid
   }
 }
 
-// Rows per strip: 32, halved (down to 8) while the grid would give fewer
-// than 8 CTAs per SM.
+// Resident CTAs of a kernel per SM on this device's SMs (queried once per
+// kernel and device ordinal below 64).
+template <class K>
+static int resident_ctas(K kernel, int threads, int* sms) {
+  static std::atomic<int> cache[64][2];
+  int dev = 0;
+  cudaGetDevice(&dev);
+  const int d = dev >= 0 && dev < 64 ? dev : 0;
+  int per = cache[d][0].load(std::memory_order_relaxed), n = cache[d][1].load(std::memory_order_relaxed);
+  if (per <= 0 || n <= 0 || dev >= 64) {
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, threads, 0) != cudaSuccess || per < 1) per = 1;
+    if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n < 1) n = 148;
+    cudaGetLastError();
+    cache[d][0].store(per, std::memory_order_relaxed);
+    cache[d][1].store(n, std::memory_order_relaxed);
+  }
+  *sms = n;
+  return per;
+}
+
+// Rows per strip: the candidate with the least estimated time, counted as
+// whole waves of resident CTAs times the level-l rows a strip reads
+// (2 rows + 3 of its REDUCE window): short strips fill the last wave of a
+// small level, long ones read fewer window rows twice.
 template <typename T, bool L0>
 static cudaError_t launch_img_stream(const LevelArgs& a, cudaStream_t s) {
   const int pairs = (a.wn + 1) / 2;
   const int warps = (pairs + kImgPairs - 1) / kImgPairs;
   const int bx = (warps + kImgWarps - 1) / kImgWarps;
+  int sms = 148;
+  const int per_sm = resident_ctas(img_stream_kernel<T, L0>, 32 * kImgWarps, &sms);
+  const int64_t slots = (int64_t)per_sm * sms;
   int rows = 32;
-  while (rows > 8 && (int64_t)bx * ((a.hn + rows - 1) / rows) * a.K < 8 * 148) rows /= 2;
+  int64_t best = INT64_MAX;
+  for (int r : {32, 28, 24, 20, 16, 12, 8}) {
+    const int64_t ctas = (int64_t)bx * ((a.hn + r - 1) / r) * a.K;
+    const int64_t cost = ((ctas + slots - 1) / slots) * (2 * r + 3);
+    if (cost < best) {
+      best = cost;
+      rows = r;
+    }
+  }
   const dim3 grid((unsigned)bx, (unsigned)((a.hn + rows - 1) / rows), (unsigned)a.K);
   img_stream_kernel<T, L0><<<grid, dim3(32, kImgWarps), 0, s>>>(a, rows);
   return cudaGetLastError();
@@ -2661,7 +2694,104 @@ __global__ void __launch_bounds__(NT) collapse_kernel(const __grid_constant__ Co
   }
 }
 
+// The clamped-EXPAND collapse step (parent side > 512), streaming: each
+// thread owns parent columns 2j, 2j + 1 (child columns j - 1 .. j + 1,
+// clamped) and walks a strip of parent rows, keeping the horizontal EXPAND of
+// child rows q - 1, q, q + 1 in registers; parent row 2q takes all three,
+// row 2q + 1 row q twice.  Every operation is collapse_kernel's clamped one
+// (expand_h1, expand_v1), in its order.
+constexpr int kCollapseRows = 32;  // parent rows per strip (even)
+
+__device__ __forceinline__ void collapse_hrow(const CollapseArgs& a, int q, int jl, int jc, int jr,
+                                              float (&h)[3][2]) {
+  const int r = clampi(q, 0, a.hc - 1);
+  const float* row = a.acc_c + (int64_t)r * a.pitch_c;
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    const float* g = row + c * a.plane_c;
+    const float g0 = g[jl], g1 = g[jc], g2 = g[jr];
+    h[c][0] = __fmul_rn(__fadd_rn(__fadd_rn(g0, __fmul_rn(6.0f, g1)), g2), 0.125f);
+    h[c][1] = __fmul_rn(__fadd_rn(g1, g2), 0.5f);
+  }
+}
+
+__global__ void __launch_bounds__(128) collapse_stream_kernel(const __grid_constant__ CollapseArgs a) {
+  const int j = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  const int x = 2 * j;
+  if (x >= a.wp) return;  // no barriers below
+  const bool two = x + 1 < a.wp;
+  const int jl = max(j - 1, 0), jc = min(j, a.wc - 1), jr = min(j + 1, a.wc - 1);
+  const int y0 = (int)blockIdx.y * kCollapseRows;
+  const int y1 = min(y0 + kCollapseRows, a.hp);
+  float hm[3][2], hc[3][2], hn[3][2];
+  int q = y0 >> 1;
+  collapse_hrow(a, q - 1, jl, jc, jr, hm);
+  collapse_hrow(a, q, jl, jc, jr, hc);
+  collapse_hrow(a, q + 1, jl, jc, jr, hn);
+  for (int y = y0; y < y1; y += 2, ++q) {
+#pragma unroll
+    for (int yy = 0; yy < 2; ++yy) {
+      const int yr = y + yy;
+      if (yr >= y1) break;
+      float v[3][2];
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+#pragma unroll
+        for (int u = 0; u < 2; ++u)
+          v[c][u] = yy == 0 ? __fmul_rn(__fadd_rn(__fadd_rn(hm[c][u], __fmul_rn(6.0f, hc[c][u])), hn[c][u]), 0.125f)
+                            : __fmul_rn(__fadd_rn(hc[c][u], hc[c][u]), 0.5f);
+      const int64_t o = (int64_t)yr * a.pitch_p + x;
+      float nv[3][2];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        float* p = a.acc_p + c * a.plane_p + o;
+        if (two) {
+          const float2 pv = *reinterpret_cast<const float2*>(p);  // x even, pitch a multiple of 32
+          nv[c][0] = __fadd_rn(pv.x, v[c][0]);
+          nv[c][1] = __fadd_rn(pv.y, v[c][1]);
+          if (!a.out) *reinterpret_cast<float2*>(p) = make_float2(nv[c][0], nv[c][1]);
+        } else {
+          nv[c][0] = __fadd_rn(p[0], v[c][0]);
+          nv[c][1] = 0.0f;
+          if (!a.out) p[0] = nv[c][0];
+        }
+      }
+      if (a.out) {
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+          if (u == 1 && !two) break;
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            const int64_t ob = (int64_t)(x + u) * 3 + c;
+            if (a.out16) {
+              const float q16 = fminf(fmaxf(__fadd_rn(nv[c][u], 0.5f), 0.0f), 65535.0f);
+              reinterpret_cast<uint16_t*>(a.out + (int64_t)yr * a.out_pitch)[ob] = (uint16_t)q16;
+            } else {
+              const float q8 = fminf(fmaxf(__fadd_rn(nv[c][u], 0.5f), 0.0f), 255.0f);
+              a.out[(int64_t)yr * a.out_pitch + ob] = (uint8_t)q8;
+            }
+            if (a.base) a.base[(int64_t)yr * a.base_pitch + ob] = nv[c][u];
+          }
+        }
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+      for (int u = 0; u < 2; ++u) {
+        hm[c][u] = hc[c][u];
+        hc[c][u] = hn[c][u];
+      }
+    if (y + 2 < y1) collapse_hrow(a, q + 2, jl, jc, jr, hn);
+  }
+}
+
 cudaError_t launch_collapse(const CollapseArgs& a, cudaStream_t s) {
+  if (!a.exact_expand) {
+    const dim3 grid((unsigned)((a.wp + 255) / 256), (unsigned)((a.hp + kCollapseRows - 1) / kCollapseRows));
+    collapse_stream_kernel<<<grid, 128, 0, s>>>(a);
+    return cudaGetLastError();
+  }
   dim3 grid((a.wp + TW - 1) / TW, (a.hp + TH - 1) / TH);
   collapse_kernel<<<grid, NT, 0, s>>>(a);
   return cudaGetLastError();
