@@ -207,12 +207,11 @@ def algorithmic_bytes(roi_w, roi_h, frames, k, mode="cache", storage_bytes=4):
             # level 0 of the image pyramid: RGBA read, the f32 Laplacian
             # (12 B) and the level-1 Gaussian + support written
             img += 4 * A[0] + 12 * A[0] + (3 * s + 1) * l1
-            # blend0: Laplacian 12 B + weight 4 B read and mask 4 B written
-            # per frame; weight sum read, accumulator written once
-            b["blend0"] = frames * 20 * A[0] + 16 * A[0]
-            # level 0: mask REDUCE of every frame (mask 4 B read, level-1 mask
-            # written in the storage type) and the union support read once
-            b["level0"] = frames * (4 * A[0] + (s if L > 2 else 4) * l1) + A[0]
+            # blend0 with the level-0 mask REDUCE: Laplacian 12 B + weight
+            # 4 B read and the level-1 mask written (storage type) per frame;
+            # weight sum and union support read, accumulator written once
+            b["blend0"] = frames * (16 * A[0] + (s if L > 2 else 4) * l1) + 17 * A[0]
+            b["level0"] = 0
         else:
             # fused pass 1: frame 3 B/px read, weight (4 B) and level-1
             # Gaussian + support (3s + 1 B at 1/4 area) written per frame;

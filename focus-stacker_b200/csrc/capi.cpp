@@ -1472,11 +1472,13 @@ static int pass2_impl(fs_stack* s, fs_frame_fetch_cb refetch, void* user, bool f
   const float inv_count = 1.0f / (float)(s->frame_total ? s->frame_total : N);
   if (s->mode == P2_LAPS || s->mode == P2_FUSED) {
     if (s->mode == P2_LAPS) {
-      // level-0 blend of every frame at once, streaming over the Laplacians
-      // (it also turns each frame's weight into its normalised mask)
+      // level-0 blend of every frame at once, with each frame's level-0 mask
+      // REDUCE to level 1 in the same pass (LAPS needs three levels or more)
+      const int out_storage = 2 < s->L ? s->storage : FS_STORAGE_F32;
       e = timed(ctx, "blend0", [&] {
-        return launch_blend0(s->acc[0], s->pitch[0] * s->lh[0], s->pitch[0], (int)s->W, (int)s->H, s->norm, s->tab,
-                             (float* const*)(s->tab + N), (int)N, inv_count, st);
+        return launch_blend0_reduce(s->acc[0], s->pitch[0] * s->lh[0], s->pitch[0], (int)s->W, (int)s->H, s->norm,
+                                    s->sm[0], s->tab, s->tab + N, (void* const*)(s->tab + 3 * N), s->pitch[1],
+                                    (int)s->lw[1], (int)s->lh[1], (int)N, inv_count, out_storage, st);
       });
     } else {
       // level 0: the weighted Laplacian sum of pass 1 divided by the complete
@@ -1488,7 +1490,7 @@ static int pass2_impl(fs_stack* s, fs_frame_fetch_cb refetch, void* user, bool f
     }
     if (e != cudaSuccess) return cuda_err(ctx, e, "level-0 blend");
     // the mask pyramid of every frame, level by level (one frame per grid z)
-    for (uint32_t l = 0; l + 1 < s->L && l < tail; ++l) {
+    for (uint32_t l = s->mode == P2_LAPS ? 1 : 0; l + 1 < s->L && l < tail; ++l) {
       MaskReduceArgs m;
       m.in = (const void* const*)(s->tab + (size_t)l * 2 * N + N);
       m.out = (void* const*)(s->tab + (size_t)(l + 1) * 2 * N + N);
@@ -1500,7 +1502,7 @@ static int pass2_impl(fs_stack* s, fs_frame_fetch_cb refetch, void* user, bool f
       m.pitch_l = s->pitch[l];
       m.pitch_n = s->pitch[l + 1];
       // FUSED level 0: each frame's raw weight, normalised by the weight sum on
-      // the fly (LAPS: blend0 has already written the normalised masks)
+      // the fly (LAPS: the level-0 blend has REDUCEd its masks already)
       m.norm = l == 0 && s->mode == P2_FUSED ? s->norm : nullptr;
       m.inv_count = inv_count;
       const int in_storage = l == 0 ? FS_STORAGE_F32 : s->storage;

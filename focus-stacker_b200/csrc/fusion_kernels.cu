@@ -1229,6 +1229,231 @@ __global__ void blend0_kernel(float* acc, int64_t plane, int64_t pitch, int w, i
   acc[2 * plane + o] = a2;
 }
 
+// Level-0 blend and level-0 mask REDUCE of a split-pyramid stack in one pass
+// over each frame's weight and Laplacian.  A CTA owns a 64 x 32 level-0 tile
+// (the 32 x 16 level-1 masks it REDUCEs to) and walks the frames in order.
+// Per frame, each thread forms the normalised masks m = w / N (inv_count
+// where N <= 1e-12) of its two 4-pixel chunks, adds lap x m into its
+// accumulators (blend0_kernel's products and sums, frame order) and stores
+// m, zero where the union support is 0 or outside the level, into a shared
+// region that adds the REDUCE halo (level-0 rows y0 - 2 .. y0 + 32, columns
+// x0 - 4 .. x0 + 67 in 16-byte chunks; the halo's chunks are formed by the
+// first threads).  After one barrier each thread REDUCEs two level-1 masks
+// from the region with mask_reduce_kernel's five-tap sums in its order; the
+// weight sums depend on the support alone and are formed once.  The region
+// is double-buffered (one barrier per frame).  Each thread stages its own
+// chunks of the next frame (weights, Laplacians, its halo weight) into shared
+// memory with cp.async while the current frame is processed: only the thread
+// that copies a chunk reads it, so the staging needs no barrier of its own,
+// and a frame's loads have a whole frame's work to land in.  (Loads held in
+// registers would cover only the REDUCE and leave 2 CTAs per SM waiting on
+// HBM: 0.6 of the copy bandwidth against 0.77.)  No level-0 mask goes
+// through HBM: per frame
+// the weight (4 B) and the Laplacian (12 B) are read once and the level-1
+// mask is written.
+namespace {
+constexpr int kB0Rows = kTileH + 3;                   // region rows: level-0 rows y0 - 2 .. y0 + 32
+constexpr int kB0Chunks = kTileW / 4 + 2;             // 16-byte chunks per region row (x0 - 4 .. x0 + 67)
+constexpr int kB0Stride = 4 * kB0Chunks;              // floats per region row
+constexpr int kB0Halo = 3 * kB0Chunks + 2 * kTileH;   // rows 0, 1 and 34 whole, chunks 0 and 17 of the rest
+static_assert(kThreads == 16 * (kTileH / 2) && kB0Halo <= kThreads, "two own chunks and at most one halo chunk per thread");
+
+struct B0Chunk {
+  int64_t off;      // element offset of the chunk in the level-0 planes
+  float n[4];       // weight sums
+  uint32_t keep;    // bit e: column e of the chunk is inside the level with union support
+  int32_t so;       // offset of the chunk in the region (floats)
+  bool in;          // the chunk's first column is inside the level (the chunk is read)
+};
+
+__device__ __forceinline__ B0Chunk b0_chunk(const float* norm, const uint8_t* sm, int64_t pitch, int wl, int hl,
+                                            int x0, int y0, int rr, int cc, bool live = true) {
+  B0Chunk c;
+  const int Y = y0 - 2 + rr, X = x0 - 4 + 4 * cc;
+  c.so = rr * kB0Stride + 4 * cc;
+  c.keep = 0u;
+  c.off = 0;
+  c.in = false;
+#pragma unroll
+  for (int e = 0; e < 4; ++e) c.n[e] = 1.0f;
+  if (live && Y >= 0 && Y < hl && X >= 0 && X < wl) {  // the chunk lies inside the row's pitch
+    const int64_t o = (int64_t)Y * pitch + X;
+    c.off = o;
+    c.in = true;
+    const float4 q = __ldg(reinterpret_cast<const float4*>(norm + o));
+    c.n[0] = q.x; c.n[1] = q.y; c.n[2] = q.z; c.n[3] = q.w;
+    const uint32_t s = __ldg(reinterpret_cast<const uint32_t*>(sm + o));
+#pragma unroll
+    for (int e = 0; e < 4; ++e)
+      if (X + e < wl && ((s >> (8 * e)) & 255u)) c.keep |= 1u << e;
+  }
+  return c;
+}
+
+__device__ __forceinline__ float4 b0_mask(const B0Chunk& c, float4 w, float inv_count) {
+  float4 m;
+  m.x = c.n[0] > 1e-12f ? __fdiv_rn(w.x, c.n[0]) : inv_count;
+  m.y = c.n[1] > 1e-12f ? __fdiv_rn(w.y, c.n[1]) : inv_count;
+  m.z = c.n[2] > 1e-12f ? __fdiv_rn(w.z, c.n[2]) : inv_count;
+  m.w = c.n[3] > 1e-12f ? __fdiv_rn(w.w, c.n[3]) : inv_count;
+  return m;
+}
+
+__device__ __forceinline__ float4 b0_keep(const B0Chunk& c, float4 m) {
+  return make_float4((c.keep & 1u) ? m.x : 0.0f, (c.keep & 2u) ? m.y : 0.0f, (c.keep & 4u) ? m.z : 0.0f,
+                     (c.keep & 8u) ? m.w : 0.0f);
+}
+}  // namespace
+
+// cp.async.wait_group 1: all but the most recent group of this thread's
+// asynchronous copies have landed.
+__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+
+// Dynamic shared memory: the double-buffered mask region, then the staged
+// chunks of two frames, [stage][slot][thread] (slots: weight of the two own
+// chunks, their Laplacian planes, the halo weight).
+constexpr int kB0Slots = 9;
+constexpr size_t kB0Smem = 2 * kB0Rows * kB0Stride * sizeof(float) + 2 * kB0Slots * kThreads * sizeof(float4);
+
+template <typename TO>
+__global__ void __launch_bounds__(kThreads, 2)
+    blend0_reduce_kernel(float* acc, int64_t plane, int64_t pitch, int wl, int hl, const float* norm,
+           const uint8_t* sm, const float* const* lap, const float* const* wgt, void* const* mask1,
+           int64_t pitch_n, int wn, int hn, int frames, float inv_count) {
+  extern __shared__ __align__(16) float b0_smem[];
+  float* const reg0 = b0_smem;  // [2][kB0Rows * kB0Stride]
+  float4* const stage = reinterpret_cast<float4*>(b0_smem + 2 * kB0Rows * kB0Stride);
+  const int tid = threadIdx.x;
+  const int x0 = blockIdx.x * kTileW, y0 = blockIdx.y * kTileH;
+  const int g = tid % 16, r = tid / 16;
+  const B0Chunk c0 = b0_chunk(norm, sm, pitch, wl, hl, x0, y0, 2 + r, 1 + g);
+  const B0Chunk c1 = b0_chunk(norm, sm, pitch, wl, hl, x0, y0, 18 + r, 1 + g);
+  int hr = 0, hc = 0;
+  if (tid < 3 * kB0Chunks) {
+    hr = tid < 2 * kB0Chunks ? tid / kB0Chunks : kB0Rows - 1;
+    hc = tid % kB0Chunks;
+  } else {
+    const int q = tid - 3 * kB0Chunks;
+    hr = 2 + q / 2;
+    hc = (q & 1) ? kB0Chunks - 1 : 0;
+  }
+  const bool has_halo = tid < kB0Halo;
+  const B0Chunk ch = b0_chunk(norm, sm, pitch, wl, hl, x0, y0, hr, hc, has_halo);
+  const int ri = tid / 16, jp = tid % 16;
+  const int I = y0 / 2 + ri, J = x0 / 2 + 2 * jp;
+  const int tap0 = 2 * ri * kB0Stride + 4 * jp + 2;
+  int ws0 = 0, ws1 = 0;
+#pragma unroll
+  for (int ky = 0; ky < 5; ++ky) {
+    const int Y = 2 * I - 2 + ky;
+    int h0 = 0, h1 = 0;
+    if (Y >= 0 && Y < hl) {
+      const uint8_t* srow = sm + (int64_t)Y * pitch;
+#pragma unroll
+      for (int u = 0; u < 7; ++u) {
+        const int X = 2 * J - 2 + u;
+        const int s = (X >= 0 && X < wl && __ldg(srow + X)) ? 1 : 0;
+        if (u < 5) h0 += s * (int)kw(u);
+        if (u >= 2) h1 += s * (int)kw(u - 2);
+      }
+    }
+    ws0 += (int)kw(ky) * h0;
+    ws1 += (int)kw(ky) * h1;
+  }
+  const float rws0 = ws0 > 0 ? __fdividef(1.0f, (float)ws0) : 0.0f;
+  const float rws1 = ws1 > 0 ? __fdividef(1.0f, (float)ws1) : 0.0f;
+  const bool out_row = I < hn;
+  float a[2][3][4];
+#pragma unroll
+  for (int u = 0; u < 2; ++u)
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+      for (int e = 0; e < 4; ++e) a[u][c][e] = 0.0f;
+  auto slot = [&](int s, int i) { return stage + (s * kB0Slots + i) * kThreads + tid; };
+  auto issue = [&](int k) {
+    const int s = k & 1;
+    const float* wk = wgt[k];
+    const float* lk = lap[k];
+    cp_async16(slot(s, 0), wk + c0.off, c0.in ? 16 : 0);
+    cp_async16(slot(s, 1), wk + c1.off, c1.in ? 16 : 0);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      cp_async16(slot(s, 2 + c), lk + c * plane + c0.off, c0.in ? 16 : 0);
+      cp_async16(slot(s, 5 + c), lk + c * plane + c1.off, c1.in ? 16 : 0);
+    }
+    if (has_halo) cp_async16(slot(s, 8), wk + ch.off, ch.in ? 16 : 0);
+  };
+  auto blend = [&](float (&av)[3][4], int s, int i0, float4 m) {
+    const float mv[4] = {m.x, m.y, m.z, m.w};
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const float4 l = *slot(s, i0 + c);
+      const float lv[4] = {l.x, l.y, l.z, l.w};
+#pragma unroll
+      for (int e = 0; e < 4; ++e) av[c][e] = __fadd_rn(av[c][e], __fmul_rn(lv[e], mv[e]));
+    }
+  };
+  issue(0);
+  cp_async_commit();
+  for (int k = 0; k < frames; ++k) {
+    const int s = k & 1;
+    float* const buf = reg0 + s * kB0Rows * kB0Stride;
+    if (k + 1 < frames) issue(k + 1);
+    cp_async_commit();
+    cp_async_wait1();
+    {
+      const float4 m0 = b0_mask(c0, *slot(s, 0), inv_count), m1 = b0_mask(c1, *slot(s, 1), inv_count);
+      blend(a[0], s, 2, m0);
+      blend(a[1], s, 5, m1);
+      *reinterpret_cast<float4*>(buf + c0.so) = b0_keep(c0, m0);
+      *reinterpret_cast<float4*>(buf + c1.so) = b0_keep(c1, m1);
+      if (has_halo) *reinterpret_cast<float4*>(buf + ch.so) = b0_keep(ch, b0_mask(ch, *slot(s, 8), inv_count));
+    }
+    __syncthreads();
+    float v0 = 0.f, v1 = 0.f;
+#pragma unroll
+    for (int ky = 0; ky < 5; ++ky) {
+      const float* row = buf + tap0 + ky * kB0Stride;
+      const float2 p = *reinterpret_cast<const float2*>(row);
+      const float4 q = *reinterpret_cast<const float4*>(row + 2);
+      const float t[7] = {p.x, p.y, q.x, q.y, q.z, q.w, row[6]};
+      float h0 = 0.f, h1 = 0.f;
+#pragma unroll
+      for (int kx = 0; kx < 5; ++kx) {
+        h0 = fmaf(kw(kx), t[kx], h0);
+        h1 = fmaf(kw(kx), t[2 + kx], h1);
+      }
+      v0 = fmaf(kw(ky), h0, v0);
+      v1 = fmaf(kw(ky), h1, v1);
+    }
+    if (out_row) {
+      TO* orow = (TO*)mask1[k] + (int64_t)I * pitch_n;
+      if (J < wn) stv<TO>(orow, J, ws0 > 0 ? v0 * rws0 : 0.f);
+      if (J + 1 < wn) stv<TO>(orow, J + 1, ws1 > 0 ? v1 * rws1 : 0.f);
+    }
+  }
+  cp_async_wait_all();
+  auto store = [&](const B0Chunk& c, const float (&av)[3][4]) {
+    if (!c.in) return;
+    const int64_t o = c.off;
+    const int X = x0 - 4 + (c.so % kB0Stride);
+    if (X + 3 < wl) {
+#pragma unroll
+      for (int ci = 0; ci < 3; ++ci)
+        *reinterpret_cast<float4*>(acc + ci * plane + o) = make_float4(av[ci][0], av[ci][1], av[ci][2], av[ci][3]);
+    } else {
+#pragma unroll
+      for (int e = 0; e < 4; ++e)
+        if (X + e < wl)
+#pragma unroll
+          for (int ci = 0; ci < 3; ++ci) acc[ci * plane + o + e] = av[ci][e];
+    }
+  };
+  store(c0, a[0]);
+  store(c1, a[1]);
+}
+
 // Blend of one level over all frames in order, one pixel per thread (the
 // products and sums of the per-batch kernels, from acc = 0).
 template <typename T>
@@ -1867,6 +2092,36 @@ cudaError_t launch_blend0(float* acc, int64_t plane, int64_t pitch, int w, int h
   const int64_t n = (int64_t)w * h;
   blend0_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(acc, plane, pitch, w, h, norm, lap, wgt, frames,
                                                            inv_count);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_blend0_reduce(float* acc, int64_t plane, int64_t pitch, int w, int h, const float* norm,
+                                 const uint8_t* sm, const float* const* lap, const float* const* wgt,
+                                 void* const* mask1, int64_t pitch_n, int wn, int hn, int frames, float inv_count,
+                                 int out_storage, cudaStream_t s) {
+  const dim3 grid((unsigned)((w + kTileW - 1) / kTileW), (unsigned)((h + kTileH - 1) / kTileH));
+  if (frames <= 0 || grid.y > 65535u) return cudaErrorInvalidValue;
+  static DeviceOnce cfg_f32, cfg_f16, cfg_bf16;
+  cudaError_t e;
+  switch (out_storage) {
+    case FS_STORAGE_F32:
+      if ((e = configure(blend0_reduce_kernel<float>, kB0Smem, &cfg_f32)) != cudaSuccess) return e;
+      blend0_reduce_kernel<float><<<grid, kThreads, kB0Smem, s>>>(acc, plane, pitch, w, h, norm, sm, lap, wgt,
+                                                                  mask1, pitch_n, wn, hn, frames, inv_count);
+      break;
+    case FS_STORAGE_F16:
+      if ((e = configure(blend0_reduce_kernel<__half>, kB0Smem, &cfg_f16)) != cudaSuccess) return e;
+      blend0_reduce_kernel<__half><<<grid, kThreads, kB0Smem, s>>>(acc, plane, pitch, w, h, norm, sm, lap, wgt,
+                                                                   mask1, pitch_n, wn, hn, frames, inv_count);
+      break;
+    case FS_STORAGE_BF16:
+      if ((e = configure(blend0_reduce_kernel<__nv_bfloat16>, kB0Smem, &cfg_bf16)) != cudaSuccess) return e;
+      blend0_reduce_kernel<__nv_bfloat16><<<grid, kThreads, kB0Smem, s>>>(acc, plane, pitch, w, h, norm, sm, lap,
+                                                                           wgt, mask1, pitch_n, wn, hn, frames,
+                                                                           inv_count);
+      break;
+    default: return cudaErrorInvalidValue;
+  }
   return cudaGetLastError();
 }
 

@@ -240,6 +240,15 @@ cudaError_t launch_img_level(const LevelArgs& a, int storage, cudaStream_t s);
 cudaError_t launch_blend0(float* acc, int64_t plane, int64_t pitch, int w, int h, const float* norm,
                           const float* const* lap, float* const* wgt, int frames, float inv_count,
                           cudaStream_t s);
+// The same level-0 blend fused with the level-0 mask REDUCE of every frame:
+// acc as launch_blend0 gives it, and mask1[k] (level-1 size wn x hn, row
+// pitch pitch_n, in out_storage) as launch_mask_reduce gives it from the
+// normalised masks; the weight planes are only read.  sm: level-0 union
+// support (row pitch `pitch`).
+cudaError_t launch_blend0_reduce(float* acc, int64_t plane, int64_t pitch, int w, int h, const float* norm,
+                                 const uint8_t* sm, const float* const* lap, const float* const* wgt,
+                                 void* const* mask1, int64_t pitch_n, int wn, int hn, int frames, float inv_count,
+                                 int out_storage, cudaStream_t s);
 // acc = sum over frames k, in order, of lap[k] (3 planes of `plane`) times
 // mask[k] (both in storage T: 0 f32, 1 f16, 2 bf16), written over acc.
 cudaError_t launch_blend(float* acc, int64_t plane, int64_t pitch, int w, int h, const void* const* lap,
