@@ -1186,55 +1186,13 @@ __global__ void __launch_bounds__(NT) img_kernel(const __grid_constant__ LevelAr
   img_tile<T, L0>(S, a, blockIdx.x * TW, blockIdx.y * TH, blockIdx.z);
 }
 
-
-// Level-0 blend of a whole stack in frame order, one pixel per thread:
-// acc = sum over frames of lap_k * (w_k / weight sum) (1 / N where the sum
-// is <= 1e-12), the same products and sums the per-batch kernels form.
-// The normalised mask replaces each frame's weight in place (the level-0
-// mask REDUCE then reads it without dividing again: forming the quotients
-// there, seven per tap row, costs more than this write).
-__global__ void blend0_kernel(float* acc, int64_t plane, int64_t pitch, int w, int h, const float* norm,
-                              const float* const* lap, float* const* wgt, int frames, float inv_count) {
-  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= (int64_t)w * h) return;
-  const int64_t o = (i / w) * pitch + i % w;
-  const float nv = norm[o];
-  float a0 = 0.0f, a1 = 0.0f, a2 = 0.0f;
-  constexpr int U = 4;  // frames whose loads are issued together
-  for (int k0 = 0; k0 < frames; k0 += U) {
-    float l0[U], l1[U], l2[U], wv[U];
-#pragma unroll
-    for (int u = 0; u < U; ++u) {
-      if (k0 + u < frames) {
-        const float* lk = lap[k0 + u];
-        l0[u] = __ldg(lk + o);
-        l1[u] = __ldg(lk + plane + o);
-        l2[u] = __ldg(lk + 2 * plane + o);
-        wv[u] = wgt[k0 + u][o];
-      }
-    }
-#pragma unroll
-    for (int u = 0; u < U; ++u) {
-      if (k0 + u < frames) {
-        const float m = nv > 1e-12f ? __fdiv_rn(wv[u], nv) : inv_count;
-        wgt[k0 + u][o] = m;
-        a0 = __fadd_rn(a0, __fmul_rn(l0[u], m));
-        a1 = __fadd_rn(a1, __fmul_rn(l1[u], m));
-        a2 = __fadd_rn(a2, __fmul_rn(l2[u], m));
-      }
-    }
-  }
-  acc[o] = a0;
-  acc[plane + o] = a1;
-  acc[2 * plane + o] = a2;
-}
-
 // Level-0 blend and level-0 mask REDUCE of a split-pyramid stack in one pass
 // over each frame's weight and Laplacian.  A CTA owns a 64 x 32 level-0 tile
 // (the 32 x 16 level-1 masks it REDUCEs to) and walks the frames in order.
 // Per frame, each thread forms the normalised masks m = w / N (inv_count
-// where N <= 1e-12) of its two 4-pixel chunks, adds lap x m into its
-// accumulators (blend0_kernel's products and sums, frame order) and stores
+// where N <= 1e-12; normalizeWeightsInto, src/fuse/pyramid.zig:303-316) of
+// its two 4-pixel chunks, adds lap x m into its accumulators (the products
+// and sums of the per-batch level-0 kernel, frame order) and stores
 // m, zero where the union support is 0 or outside the level, into a shared
 // region that adds the REDUCE halo (level-0 rows y0 - 2 .. y0 + 32, columns
 // x0 - 4 .. x0 + 67 in 16-byte chunks; the halo's chunks are formed by the
@@ -2083,15 +2041,6 @@ static cudaError_t launch_img_stream(const LevelArgs& a, cudaStream_t s) {
   }
   const dim3 grid((unsigned)bx, (unsigned)((a.hn + rows - 1) / rows), (unsigned)a.K);
   img_stream_kernel<T, L0><<<grid, dim3(32, kImgWarps), 0, s>>>(a, rows);
-  return cudaGetLastError();
-}
-
-cudaError_t launch_blend0(float* acc, int64_t plane, int64_t pitch, int w, int h, const float* norm,
-                          const float* const* lap, float* const* wgt, int frames, float inv_count,
-                          cudaStream_t s) {
-  const int64_t n = (int64_t)w * h;
-  blend0_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(acc, plane, pitch, w, h, norm, lap, wgt, frames,
-                                                           inv_count);
   return cudaGetLastError();
 }
 

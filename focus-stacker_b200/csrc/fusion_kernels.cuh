@@ -233,18 +233,13 @@ cudaError_t launch_collapse(const CollapseArgs& a, cudaStream_t s);
 // level 0, the storage type above); level 0 reads the remapped RGBA planes
 // in0[k].rgba.
 cudaError_t launch_img_level(const LevelArgs& a, int storage, cudaStream_t s);
-// Level-0 blend of all frames of a stack (device tables of each frame's
-// level-0 Laplacian and weight planes), written over acc; each weight plane
-// is replaced by the frame's normalised mask, which launch_mask_reduce then
-// reads.
-cudaError_t launch_blend0(float* acc, int64_t plane, int64_t pitch, int w, int h, const float* norm,
-                          const float* const* lap, float* const* wgt, int frames, float inv_count,
-                          cudaStream_t s);
-// The same level-0 blend fused with the level-0 mask REDUCE of every frame:
-// acc as launch_blend0 gives it, and mask1[k] (level-1 size wn x hn, row
-// pitch pitch_n, in out_storage) as launch_mask_reduce gives it from the
-// normalised masks; the weight planes are only read.  sm: level-0 union
-// support (row pitch `pitch`).
+// Level-0 blend of all frames of a split-pyramid stack (device tables of
+// each frame's level-0 Laplacian and weight planes) fused with every frame's
+// level-0 mask REDUCE: acc = sum over frames, in order, of lap[k] x (w_k /
+// weight sum) (1 / N where the sum is <= 1e-12), written over acc, and
+// mask1[k] (level-1 size wn x hn, row pitch pitch_n, in out_storage) the
+// REDUCE of those normalised masks with the union support sm (row pitch
+// `pitch`), as launch_mask_reduce forms it; the weight planes are only read.
 cudaError_t launch_blend0_reduce(float* acc, int64_t plane, int64_t pitch, int w, int h, const float* norm,
                                  const uint8_t* sm, const float* const* lap, const float* const* wgt,
                                  void* const* mask1, int64_t pitch_n, int wn, int hn, int frames, float inv_count,
