@@ -1997,17 +1997,265 @@ __global__ void __launch_bounds__(32 * kImgWarps) img_stream_kernel(const __grid
   }
 }
 
+// The same image step for l >= 1 with each warp's level-l rows staged in
+// shared memory: a ring of kStageRows rows per warp, filled by cp.async one
+// step (two rows) ahead of the REDUCE and kept for the Laplacian of the rows
+// two and three steps back, so that a step's loads land while the previous
+// step computes and the Laplacian reads no row from HBM again (the streaming
+// kernel above reads each row's taps when it needs them and waits on HBM).
+// Lane L copies its own four columns of each plane and of the support, lane
+// 0 also the four before them (its REDUCE taps c - 2, c - 1), lane 31 the
+// four after; the taps of a row are read from the ring after the lane's
+// copies have landed (cp.async.wait_group) and the warp has met
+// (__syncwarp), and a slot is refilled only after the warp has met again.
+// Products, sums and their order are those of img_stream_kernel<T, false>.
+constexpr int kStageRows = 7;       // level-l rows 2r - 2 .. 2r + 4 at step r
+constexpr int kStageCols = 4 * 34;  // chunk 0: before lane 0; 1 + L: lane L; 33: after lane 31
+
+template <typename T>
+struct __align__(16) StageRow {
+  T g[3][kStageCols];
+  uint8_t s[kStageCols];
+};
+
+template <int N>
+__device__ __forceinline__ void cp_async_ca(void* dst, const void* src, bool full) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  if constexpr (N == 16)
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(d), "l"(src), "r"(full ? 16 : 0) : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;\n" ::"r"(d), "l"(src), "n"(N), "r"(full ? N : 0)
+                 : "memory");
+}
+
+template <typename T>
+__device__ __forceinline__ void stage_row(StageRow<T>& R, const LevelPlanes& in, int64_t pitch, int wl, int hl,
+                                          int y, int c, int lane) {
+  const bool rin = y >= 0 && y < hl;
+  const int64_t ro = rin ? (int64_t)y * pitch : 0;
+  const T* g = (const T*)in.g;
+  auto chunk = [&](int dst, int col) {  // columns col .. col + 3, inside the row's pitch when col < wl
+    const bool ok = rin && col >= 0 && col < wl;
+    const int64_t o = ok ? ro + col : 0;
+#pragma unroll
+    for (int ch = 0; ch < 3; ++ch) cp_async_ca<4 * sizeof(T)>(&R.g[ch][dst], g + ch * in.plane + o, ok);
+    cp_async_ca<4>(&R.s[dst], in.s + o, ok);
+  };
+  chunk(4 + 4 * lane, c);
+  if (lane == 0) chunk(0, c - 4);
+  if (lane == 31) chunk(4 * 33, c + 4);
+}
+
+// img_row from a staged row: taps c - 2 .. c + 4 at ring columns 4L + 2 .. 4L + 8.
+template <typename T>
+__device__ __forceinline__ void staged_row_sums(const StageRow<T>& R, int lane, int c, int wl, float4 (&hs)[2]) {
+  float v[3][7];
+  const int b = 4 * lane + 2;
+#pragma unroll
+  for (int ch = 0; ch < 3; ++ch) {
+    ld2<T>(&R.g[ch][b], v[ch]);
+    ld4<T>(&R.g[ch][b + 2], v[ch] + 2);
+    v[ch][6] = ldv<T>(&R.g[ch][b + 6], 0);
+  }
+  const uint32_t s2 = *reinterpret_cast<const uint16_t*>(&R.s[b]);
+  uint32_t s4 = *reinterpret_cast<const uint32_t*>(&R.s[b + 2]);
+  const uint32_t s6 = c + 4 < wl ? R.s[b + 6] : 0u;
+  if (c + 3 >= wl) s4 &= c < wl ? (1u << (8 * (wl - c))) - 1u : 0u;  // columns past the level
+  const uint32_t nz0 = __vcmpne4(__byte_perm(s2, s4, 0x5410u), 0u);  // taps 0..3
+  const uint32_t nz1 = __vcmpne4(s4, 0u);                            // taps 2..5
+  bool sup[7];
+  sup[0] = (nz0 & 0x000000ffu) != 0u;
+  sup[1] = (nz0 & 0x0000ff00u) != 0u;
+#pragma unroll
+  for (int u = 0; u < 4; ++u) sup[2 + u] = (nz1 & (0xffu << (8 * u))) != 0u;
+  sup[6] = s6 != 0u;
+  constexpr uint32_t kW = 0x04060401u;
+  const int wsum[2] = {(int)__dp4a(nz0 & kW, 0x01010101u, (nz1 >> 16) & 1u),
+                       (int)__dp4a(nz1 & kW, 0x01010101u, s6 ? 1u : 0u)};
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    float acc[3];
+#pragma unroll
+    for (int ch = 0; ch < 3; ++ch) {
+      float sum = 0.f;
+#pragma unroll
+      for (int kx = 0; kx < 5; ++kx) sum = fmaf(kw(kx), sup[2 * h + kx] ? v[ch][2 * h + kx] : 0.0f, sum);
+      acc[ch] = sum;
+    }
+    hs[h] = make_float4(acc[0], acc[1], acc[2], __int_as_float(0x4B000000 | wsum[h]) - 8388608.0f);
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(32 * kImgWarps) img_stage_kernel(const __grid_constant__ LevelArgs a, int rows) {
+  extern __shared__ __align__(16) uint8_t stage_smem[];
+  StageRow<T>* const ring = reinterpret_cast<StageRow<T>*>(stage_smem) + threadIdx.y * kStageRows;
+  const int lane = (int)threadIdx.x, k = (int)blockIdx.z;
+  const int first = ((int)blockIdx.x * kImgWarps + (int)threadIdx.y) * kImgPairs;  // pair of lane 1
+  if (2 * first >= a.wn) return;  // the whole warp: none of its pairs is in the level
+  const int p = first + lane - 1;
+  const int J0 = 2 * p, c = 4 * p;
+  const bool live = p >= 0 && J0 < a.wn;
+  const bool emit = live && lane >= 1 && lane <= kImgPairs;
+  const bool j1in = J0 + 1 < a.wn, rin = J0 + 2 < a.wn;
+  const int i0 = (int)blockIdx.y * rows;
+  const int i1 = min(i0 + rows, a.hn);
+  const LevelPlanes& in = a.in[k];
+  auto slot = [&](int y) -> StageRow<T>& { return ring[(y + 2 * kStageRows) % kStageRows]; };
+  auto sums = [&](int y, float4 (&hs)[2]) {
+    if (live) {
+      staged_row_sums<T>(slot(y), lane, c, a.wl, hs);
+    } else {
+      hs[0] = hs[1] = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+  };
+  const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
+  float4 cur[2], nxt[2];
+  float Hm2[3][4], Hm1[3][4], Hc[3][4];
+#pragma unroll
+  for (int ch = 0; ch < 3; ++ch)
+#pragma unroll
+    for (int u = 0; u < 4; ++u) Hm2[ch][u] = Hm1[ch][u] = 0.0f;
+  int r = i0 > 0 ? i0 - 1 : 0;
+  for (int y = 2 * r - 2; y <= 2 * r + 2; ++y) stage_row<T>(slot(y), in, a.pitch_l, a.wl, a.hl, y, c, lane);
+  cp_async_commit();
+  cp_async_wait_all();
+  __syncwarp();
+  {
+    float4 t0[2], t1[2], t2[2];
+    sums(2 * r - 2, t0);
+    sums(2 * r - 1, t1);
+    sums(2 * r, t2);
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      cur[h] = vtap(kwi(2), t2[h], vtap(kwi(1), t1[h], vtap(kwi(0), t0[h], zero)));
+      nxt[h] = vtap(kwi(0), t2[h], zero);
+    }
+  }
+  for (; r <= i1; ++r) {
+    __syncwarp();  // every lane is done with the rows whose slots are refilled now
+    if (r < i1) {
+      stage_row<T>(slot(2 * r + 3), in, a.pitch_l, a.wl, a.hl, 2 * r + 3, c, lane);
+      stage_row<T>(slot(2 * r + 4), in, a.pitch_l, a.wl, a.hl, 2 * r + 4, c, lane);
+    }
+    cp_async_commit();
+    cp_async_wait1();  // rows 2r + 1, 2r + 2
+    __syncwarp();
+    float4 fin[2];
+    {
+      float4 t3[2], t4[2];
+      sums(2 * r + 1, t3);
+      sums(2 * r + 2, t4);
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        fin[h] = vtap(kwi(4), t4[h], vtap(kwi(3), t3[h], cur[h]));
+        cur[h] = vtap(kwi(2), t4[h], vtap(kwi(1), t3[h], nxt[h]));
+        nxt[h] = vtap(kwi(0), t4[h], zero);
+      }
+    }
+    if (r < a.hn) {  // warp-uniform
+      float g[2][3];
+      bool sp[2];
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const float ws = fin[h].w;
+        sp[h] = live && J0 + h < a.wn && ws > 0.f;
+        const float rc = sp[h] ? __fdividef(1.0f, ws) : 0.0f;
+        g[h][0] = fin[h].x * rc;
+        g[h][1] = fin[h].y * rc;
+        g[h][2] = fin[h].z * rc;
+      }
+      if (emit && r >= i0 && r < i1) {
+        const LevelPlanes& out = a.out[k];
+        const int64_t o = (int64_t)r * a.pitch_n + J0;
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          if (J0 + h >= a.wn) continue;
+#pragma unroll
+          for (int ch = 0; ch < 3; ++ch) stv<T>((T*)out.g, ch * out.plane + o + h, g[h][ch]);
+          out.s[o + h] = sp[h] ? 1 : 0;
+        }
+      }
+#pragma unroll
+      for (int ch = 0; ch < 3; ++ch) {
+        const float gA = g[0][ch], gB = j1in ? g[1][ch] : gA;
+        float gL = __shfl_up_sync(0xffffffffu, gB, 1);
+        const float gRn = __shfl_down_sync(0xffffffffu, gA, 1);
+        if (p == 0) gL = gA;
+        const float gR = rin ? gRn : gB;
+        Hc[ch][0] = __fmul_rn(__fadd_rn(__fadd_rn(gL, __fmul_rn(6.0f, gA)), gB), 0.125f);
+        Hc[ch][1] = __fmul_rn(__fadd_rn(gA, gB), 0.5f);
+        Hc[ch][2] = __fmul_rn(__fadd_rn(__fadd_rn(gA, __fmul_rn(6.0f, gB)), gR), 0.125f);
+        Hc[ch][3] = __fmul_rn(__fadd_rn(gB, gR), 0.5f);
+      }
+      if (r == 0) {  // row -1 clamps to row 0
+#pragma unroll
+        for (int ch = 0; ch < 3; ++ch)
+#pragma unroll
+          for (int u = 0; u < 4; ++u) Hm1[ch][u] = Hc[ch][u];
+      }
+    } else {  // row hn clamps to row hn - 1
+#pragma unroll
+      for (int ch = 0; ch < 3; ++ch)
+#pragma unroll
+        for (int u = 0; u < 4; ++u) Hc[ch][u] = Hm1[ch][u];
+    }
+    // Laplacian of level-l rows 2q, 2q + 1, q = r - 1 (both still in the ring)
+    if (emit && r >= i0 + 1) {
+#pragma unroll
+      for (int yy = 0; yy < 2; ++yy) {
+        const int y = 2 * (r - 1) + yy;
+        if (y >= a.hl) break;
+        const int64_t ro = (int64_t)y * a.pitch_l;
+        const StageRow<T>& R = slot(y);
+        float gv[3][4];
+#pragma unroll
+        for (int ch = 0; ch < 3; ++ch) ld4<T>(&R.g[ch][4 + 4 * lane], gv[ch]);
+        T* lp = (T*)a.lap[k] + ro + c;
+#pragma unroll
+        for (int ch = 0; ch < 3; ++ch) {
+          float lv[4];
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            const float e = yy == 0
+                ? __fmul_rn(__fadd_rn(__fadd_rn(Hm2[ch][u], __fmul_rn(6.0f, Hm1[ch][u])), Hc[ch][u]), 0.125f)
+                : __fmul_rn(__fadd_rn(Hm1[ch][u], Hm1[ch][u]), 0.5f);
+            lv[u] = __fsub_rn(gv[ch][u], e);
+          }
+          T* lc = lp + ch * a.acc_plane_l;
+          if (c + 3 < a.wl) {
+            st4<T>(lc, lv);
+          } else {
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+              if (c + u < a.wl) stv<T>(lc, u, lv[u]);
+          }
+        }
+      }
+    }
+#pragma unroll
+    for (int ch = 0; ch < 3; ++ch)
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        Hm2[ch][u] = Hm1[ch][u];
+        Hm1[ch][u] = Hc[ch][u];
+      }
+  }
+  cp_async_wait_all();
+}
+
 // Resident CTAs of a kernel per SM on this device's SMs (queried once per
-// kernel and device ordinal below 64).
+// device ordinal below 64 into the caller's cache, one cache per kernel:
+// kernels of one signature share their pointer type).
+using ResidentCache = std::atomic<int>[64][2];
 template <class K>
-static int resident_ctas(K kernel, int threads, int* sms) {
-  static std::atomic<int> cache[64][2];
+static int resident_ctas(K kernel, int threads, size_t smem, ResidentCache& cache, int* sms) {
   int dev = 0;
   cudaGetDevice(&dev);
   const int d = dev >= 0 && dev < 64 ? dev : 0;
   int per = cache[d][0].load(std::memory_order_relaxed), n = cache[d][1].load(std::memory_order_relaxed);
   if (per <= 0 || n <= 0 || dev >= 64) {
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, threads, 0) != cudaSuccess || per < 1) per = 1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, threads, smem) != cudaSuccess || per < 1) per = 1;
     if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n < 1) n = 148;
     cudaGetLastError();
     cache[d][0].store(per, std::memory_order_relaxed);
@@ -2027,7 +2275,8 @@ static cudaError_t launch_img_stream(const LevelArgs& a, cudaStream_t s) {
   const int warps = (pairs + kImgPairs - 1) / kImgPairs;
   const int bx = (warps + kImgWarps - 1) / kImgWarps;
   int sms = 148;
-  const int per_sm = resident_ctas(img_stream_kernel<T, L0>, 32 * kImgWarps, &sms);
+  static ResidentCache cache;
+  const int per_sm = resident_ctas(img_stream_kernel<T, L0>, 32 * kImgWarps, 0, cache, &sms);
   const int64_t slots = (int64_t)per_sm * sms;
   int rows = 32;
   int64_t best = INT64_MAX;
@@ -2041,6 +2290,34 @@ static cudaError_t launch_img_stream(const LevelArgs& a, cudaStream_t s) {
   }
   const dim3 grid((unsigned)bx, (unsigned)((a.hn + rows - 1) / rows), (unsigned)a.K);
   img_stream_kernel<T, L0><<<grid, dim3(32, kImgWarps), 0, s>>>(a, rows);
+  return cudaGetLastError();
+}
+
+template <typename T>
+static cudaError_t launch_img_stage(const LevelArgs& a, cudaStream_t s) {
+  constexpr size_t smem = sizeof(StageRow<T>) * kStageRows * kImgWarps;
+  static DeviceOnce configured;
+  cudaError_t e = configure(img_stage_kernel<T>, smem, &configured);
+  if (e != cudaSuccess) return e;
+  const int pairs = (a.wn + 1) / 2;
+  const int warps = (pairs + kImgPairs - 1) / kImgPairs;
+  const int bx = (warps + kImgWarps - 1) / kImgWarps;
+  int sms = 148;
+  static ResidentCache cache;
+  const int per_sm = resident_ctas(img_stage_kernel<T>, 32 * kImgWarps, smem, cache, &sms);
+  const int64_t slots = (int64_t)per_sm * sms;
+  int rows = 32;
+  int64_t best = INT64_MAX;
+  for (int r : {32, 28, 24, 20, 16, 12, 8}) {
+    const int64_t ctas = (int64_t)bx * ((a.hn + r - 1) / r) * a.K;
+    const int64_t cost = ((ctas + slots - 1) / slots) * (2 * r + 3);
+    if (cost < best) {
+      best = cost;
+      rows = r;
+    }
+  }
+  const dim3 grid((unsigned)bx, (unsigned)((a.hn + rows - 1) / rows), (unsigned)a.K);
+  img_stage_kernel<T><<<grid, dim3(32, kImgWarps), smem, s>>>(a, rows);
   return cudaGetLastError();
 }
 
@@ -2107,12 +2384,11 @@ cudaError_t launch_img_level(const LevelArgs& a, int storage, cudaStream_t s) {
   if (!a.exact_expand && a.level + 2 < a.levels) {
     switch (storage) {
       case FS_STORAGE_F32:
-        return a.level == 0 ? launch_img_stream<float, true>(a, s) : launch_img_stream<float, false>(a, s);
+        return a.level == 0 ? launch_img_stream<float, true>(a, s) : launch_img_stage<float>(a, s);
       case FS_STORAGE_F16:
-        return a.level == 0 ? launch_img_stream<__half, true>(a, s) : launch_img_stream<__half, false>(a, s);
+        return a.level == 0 ? launch_img_stream<__half, true>(a, s) : launch_img_stage<__half>(a, s);
       case FS_STORAGE_BF16:
-        return a.level == 0 ? launch_img_stream<__nv_bfloat16, true>(a, s)
-                            : launch_img_stream<__nv_bfloat16, false>(a, s);
+        return a.level == 0 ? launch_img_stream<__nv_bfloat16, true>(a, s) : launch_img_stage<__nv_bfloat16>(a, s);
       default:
         return cudaErrorInvalidValue;
     }
