@@ -229,12 +229,16 @@ def algorithmic_bytes(roi_w, roi_h, frames, k, mode="cache", storage_bytes=4):
         # levels >= 1: mask REDUCE (mask read, next mask written; the top one
         # in f32; support once) and the blend of each level over all frames
         # (Laplacian 3s B (the top Gaussian 12 B) and mask read per frame,
-        # accumulator 12 B written)
+        # accumulator 12 B written); levels 1 .. lf-1, those of at least 1184
+        # 64x32 tiles, blend and REDUCE in one pass (the mask read once)
+        lf = 1
+        while lf + 1 < L and -(-sz[lf][0] // 64) * -(-sz[lf][1] // 32) >= 1184:
+            lf += 1
         lv = 0
         for l in range(1, L):
             ms = s if l + 1 < L else 4
             if l + 1 < L:
-                lv += frames * (ms * A[l] + (s if l + 2 < L else 4) * A[l + 1]) + A[l]
+                lv += frames * ((ms * A[l] if l >= lf else 0) + (s if l + 2 < L else 4) * A[l + 1]) + A[l]
             lv += frames * ((3 * ms) + ms) * A[l] + 12 * A[l]
         b["level"] = lv
     return b, sum(b.values())

@@ -1489,8 +1489,9 @@ static int pass2_impl(fs_stack* s, fs_frame_fetch_cb refetch, void* user, bool f
       });
     }
     if (e != cudaSuccess) return cuda_err(ctx, e, "level-0 blend");
-    // the mask pyramid of every frame, level by level (one frame per grid z)
-    for (uint32_t l = s->mode == P2_LAPS ? 1 : 0; l + 1 < s->L && l < tail; ++l) {
+    // the mask pyramid of every frame, level by level (one frame per grid z),
+    // from level `from` (LAPS: the level-0 blend has REDUCEd its masks)
+    auto mask_reduce = [&](uint32_t l) {
       MaskReduceArgs m;
       m.in = (const void* const*)(s->tab + (size_t)l * 2 * N + N);
       m.out = (void* const*)(s->tab + (size_t)(l + 1) * 2 * N + N);
@@ -1502,17 +1503,37 @@ static int pass2_impl(fs_stack* s, fs_frame_fetch_cb refetch, void* user, bool f
       m.pitch_l = s->pitch[l];
       m.pitch_n = s->pitch[l + 1];
       // FUSED level 0: each frame's raw weight, normalised by the weight sum on
-      // the fly (LAPS: the level-0 blend has REDUCEd its masks already)
+      // the fly
       m.norm = l == 0 && s->mode == P2_FUSED ? s->norm : nullptr;
       m.inv_count = inv_count;
       const int in_storage = l == 0 ? FS_STORAGE_F32 : s->storage;
       const int out_storage = l + 2 < s->L ? s->storage : FS_STORAGE_F32;
-      e = timed(ctx, l == 0 ? "level0" : "level",
-                [&] { return launch_mask_reduce(m, (int)N, in_storage, out_storage, st); });
-      if (e != cudaSuccess) return cuda_err(ctx, e, "mask reduce");
+      return timed(ctx, l == 0 ? "level0" : "level",
+                   [&] { return launch_mask_reduce(m, (int)N, in_storage, out_storage, st); });
+    };
+    if (s->mode == P2_FUSED && 1 < s->L && 0 < tail && (e = mask_reduce(0)) != cudaSuccess)
+      return cuda_err(ctx, e, "mask reduce");
+    // levels l >= 1 with enough tiles to fill the GPU: the blend of the level
+    // and its mask REDUCE to l + 1 in one pass over every frame
+    uint32_t lf = 1;
+    for (; lf + 1 < s->L && lf < tail; ++lf) {
+      const int64_t tiles = (int64_t)((s->lw[lf] + kTileW - 1) / kTileW) * ((s->lh[lf] + kTileH - 1) / kTileH);
+      if (tiles < kBlendReduceMinTiles) break;
+      const void* const* lap = (const void* const*)(s->tab + (size_t)lf * 2 * N);
+      const void* const* msk = (const void* const*)(s->tab + (size_t)lf * 2 * N + N);
+      void* const* nxt = (void* const*)(s->tab + (size_t)(lf + 1) * 2 * N + N);
+      const int out_storage = lf + 2 < s->L ? s->storage : FS_STORAGE_F32;
+      e = timed(ctx, "level", [&] {
+        return launch_blend_reduce(s->acc[lf], s->pitch[lf] * s->lh[lf], s->pitch[lf], (int)s->lw[lf], (int)s->lh[lf],
+                                   s->sm[lf], lap, msk, nxt, s->pitch[lf + 1], (int)s->lw[lf + 1],
+                                   (int)s->lh[lf + 1], (int)N, s->storage, out_storage, st);
+      });
+      if (e != cudaSuccess) return cuda_err(ctx, e, "level blend + mask reduce");
     }
-    // the blend of levels 1 .. L-1 over every frame (top: Gaussian x mask)
-    for (uint32_t l = 1; l < s->L && l < tail; ++l) {
+    for (uint32_t l = lf; l + 1 < s->L && l < tail; ++l)
+      if ((e = mask_reduce(l)) != cudaSuccess) return cuda_err(ctx, e, "mask reduce");
+    // the blend of the other levels up to L-1 over every frame (top: Gaussian x mask)
+    for (uint32_t l = lf; l < s->L && l < tail; ++l) {
       const void* const* lap = (const void* const*)(s->tab + (size_t)l * 2 * N);
       const void* const* msk = (const void* const*)(s->tab + (size_t)l * 2 * N + N);
       const int storage = l + 1 < s->L ? s->storage : FS_STORAGE_F32;

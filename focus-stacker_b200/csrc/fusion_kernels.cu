@@ -1238,8 +1238,10 @@ __device__ __forceinline__ B0Chunk b0_chunk(const float* norm, const uint8_t* sm
     const int64_t o = (int64_t)Y * pitch + X;
     c.off = o;
     c.in = true;
-    const float4 q = __ldg(reinterpret_cast<const float4*>(norm + o));
-    c.n[0] = q.x; c.n[1] = q.y; c.n[2] = q.z; c.n[3] = q.w;
+    if (norm) {
+      const float4 q = __ldg(reinterpret_cast<const float4*>(norm + o));
+      c.n[0] = q.x; c.n[1] = q.y; c.n[2] = q.z; c.n[3] = q.w;
+    }
     const uint32_t s = __ldg(reinterpret_cast<const uint32_t*>(sm + o));
 #pragma unroll
     for (int e = 0; e < 4; ++e)
@@ -1261,6 +1263,28 @@ __device__ __forceinline__ float4 b0_keep(const B0Chunk& c, float4 m) {
   return make_float4((c.keep & 1u) ? m.x : 0.0f, (c.keep & 2u) ? m.y : 0.0f, (c.keep & 4u) ? m.z : 0.0f,
                      (c.keep & 8u) ? m.w : 0.0f);
 }
+
+// A chunk of four samples in storage TS into a 16-byte staging slot (16-bit
+// samples fill its first 8 bytes), and back as four floats.
+template <typename TS>
+__device__ __forceinline__ void b0_copy(float4* dst, const TS* src, bool ok) {
+  if constexpr (sizeof(TS) == 4) {
+    cp_async16(dst, src, ok ? 16 : 0);
+  } else {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d), "l"(src), "r"(ok ? 8 : 0) : "memory");
+  }
+}
+template <typename TS>
+__device__ __forceinline__ float4 b0_load(const float4* p) {
+  if constexpr (sizeof(TS) == 4) {
+    return *p;
+  } else {
+    const uint2 q = *reinterpret_cast<const uint2*>(p);
+    const TS* h = reinterpret_cast<const TS*>(&q);
+    return make_float4(ldv<TS>(h, 0), ldv<TS>(h, 1), ldv<TS>(h, 2), ldv<TS>(h, 3));
+  }
+}
 }  // namespace
 
 // cp.async.wait_group 1: all but the most recent group of this thread's
@@ -1273,10 +1297,12 @@ __device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_g
 constexpr int kB0Slots = 9;
 constexpr size_t kB0Smem = 2 * kB0Rows * kB0Stride * sizeof(float) + 2 * kB0Slots * kThreads * sizeof(float4);
 
-template <typename TO>
+// TS: storage of the level's Laplacians and masks; NORM: level 0, the
+// masks formed from the weights (w / N) rather than read.
+template <typename TS, typename TO, bool NORM>
 __global__ void __launch_bounds__(kThreads, 2)
     blend0_reduce_kernel(float* acc, int64_t plane, int64_t pitch, int wl, int hl, const float* norm,
-           const uint8_t* sm, const float* const* lap, const float* const* wgt, void* const* mask1,
+           const uint8_t* sm, const void* const* lap, const void* const* wgt, void* const* mask1,
            int64_t pitch_n, int wn, int hn, int frames, float inv_count) {
   extern __shared__ __align__(16) float b0_smem[];
   float* const reg0 = b0_smem;  // [2][kB0Rows * kB0Stride]
@@ -1284,6 +1310,7 @@ __global__ void __launch_bounds__(kThreads, 2)
   const int tid = threadIdx.x;
   const int x0 = blockIdx.x * kTileW, y0 = blockIdx.y * kTileH;
   const int g = tid % 16, r = tid / 16;
+  if (!NORM) norm = nullptr;
   const B0Chunk c0 = b0_chunk(norm, sm, pitch, wl, hl, x0, y0, 2 + r, 1 + g);
   const B0Chunk c1 = b0_chunk(norm, sm, pitch, wl, hl, x0, y0, 18 + r, 1 + g);
   int hr = 0, hc = 0;
@@ -1331,22 +1358,27 @@ __global__ void __launch_bounds__(kThreads, 2)
   auto slot = [&](int s, int i) { return stage + (s * kB0Slots + i) * kThreads + tid; };
   auto issue = [&](int k) {
     const int s = k & 1;
-    const float* wk = wgt[k];
-    const float* lk = lap[k];
-    cp_async16(slot(s, 0), wk + c0.off, c0.in ? 16 : 0);
-    cp_async16(slot(s, 1), wk + c1.off, c1.in ? 16 : 0);
+    const TS* wk = (const TS*)wgt[k];
+    const TS* lk = (const TS*)lap[k];
+    b0_copy<TS>(slot(s, 0), wk + c0.off, c0.in);
+    b0_copy<TS>(slot(s, 1), wk + c1.off, c1.in);
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      cp_async16(slot(s, 2 + c), lk + c * plane + c0.off, c0.in ? 16 : 0);
-      cp_async16(slot(s, 5 + c), lk + c * plane + c1.off, c1.in ? 16 : 0);
+      b0_copy<TS>(slot(s, 2 + c), lk + c * plane + c0.off, c0.in);
+      b0_copy<TS>(slot(s, 5 + c), lk + c * plane + c1.off, c1.in);
     }
-    if (has_halo) cp_async16(slot(s, 8), wk + ch.off, ch.in ? 16 : 0);
+    if (has_halo) b0_copy<TS>(slot(s, 8), wk + ch.off, ch.in);
+  };
+  // level 0: the normalised mask; above: the stored mask
+  auto mask = [&](const B0Chunk& c, const float4* p) {
+    const float4 v = b0_load<TS>(p);
+    return NORM ? b0_mask(c, v, inv_count) : v;
   };
   auto blend = [&](float (&av)[3][4], int s, int i0, float4 m) {
     const float mv[4] = {m.x, m.y, m.z, m.w};
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      const float4 l = *slot(s, i0 + c);
+      const float4 l = b0_load<TS>(slot(s, i0 + c));
       const float lv[4] = {l.x, l.y, l.z, l.w};
 #pragma unroll
       for (int e = 0; e < 4; ++e) av[c][e] = __fadd_rn(av[c][e], __fmul_rn(lv[e], mv[e]));
@@ -1361,12 +1393,12 @@ __global__ void __launch_bounds__(kThreads, 2)
     cp_async_commit();
     cp_async_wait1();
     {
-      const float4 m0 = b0_mask(c0, *slot(s, 0), inv_count), m1 = b0_mask(c1, *slot(s, 1), inv_count);
+      const float4 m0 = mask(c0, slot(s, 0)), m1 = mask(c1, slot(s, 1));
       blend(a[0], s, 2, m0);
       blend(a[1], s, 5, m1);
       *reinterpret_cast<float4*>(buf + c0.so) = b0_keep(c0, m0);
       *reinterpret_cast<float4*>(buf + c1.so) = b0_keep(c1, m1);
-      if (has_halo) *reinterpret_cast<float4*>(buf + ch.so) = b0_keep(ch, b0_mask(ch, *slot(s, 8), inv_count));
+      if (has_halo) *reinterpret_cast<float4*>(buf + ch.so) = b0_keep(ch, mask(ch, slot(s, 8)));
     }
     __syncthreads();
     float v0 = 0.f, v1 = 0.f;
@@ -2321,34 +2353,66 @@ static cudaError_t launch_img_stage(const LevelArgs& a, cudaStream_t s) {
   return cudaGetLastError();
 }
 
+template <typename TS, typename TO, bool NORM>
+static cudaError_t launch_blend_reduce_t(float* acc, int64_t plane, int64_t pitch, int w, int h, const float* norm,
+                                         const uint8_t* sm, const void* const* lap, const void* const* mask,
+                                         void* const* mask_next, int64_t pitch_n, int wn, int hn, int frames,
+                                         float inv_count, cudaStream_t s) {
+  static DeviceOnce cfg;
+  cudaError_t e = configure(blend0_reduce_kernel<TS, TO, NORM>, kB0Smem, &cfg);
+  if (e != cudaSuccess) return e;
+  const dim3 grid((unsigned)((w + kTileW - 1) / kTileW), (unsigned)((h + kTileH - 1) / kTileH));
+  blend0_reduce_kernel<TS, TO, NORM><<<grid, kThreads, kB0Smem, s>>>(acc, plane, pitch, w, h, norm, sm, lap, mask,
+                                                                      mask_next, pitch_n, wn, hn, frames, inv_count);
+  return cudaGetLastError();
+}
+
+template <typename TS, bool NORM>
+static cudaError_t launch_blend_reduce_o(int out_storage, float* acc, int64_t plane, int64_t pitch, int w, int h,
+                                         const float* norm, const uint8_t* sm, const void* const* lap,
+                                         const void* const* mask, void* const* mask_next, int64_t pitch_n, int wn,
+                                         int hn, int frames, float inv_count, cudaStream_t s) {
+  switch (out_storage) {
+    case FS_STORAGE_F32:
+      return launch_blend_reduce_t<TS, float, NORM>(acc, plane, pitch, w, h, norm, sm, lap, mask, mask_next, pitch_n,
+                                                    wn, hn, frames, inv_count, s);
+    case FS_STORAGE_F16:
+      return launch_blend_reduce_t<TS, __half, NORM>(acc, plane, pitch, w, h, norm, sm, lap, mask, mask_next, pitch_n,
+                                                     wn, hn, frames, inv_count, s);
+    case FS_STORAGE_BF16:
+      return launch_blend_reduce_t<TS, __nv_bfloat16, NORM>(acc, plane, pitch, w, h, norm, sm, lap, mask, mask_next,
+                                                            pitch_n, wn, hn, frames, inv_count, s);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
 cudaError_t launch_blend0_reduce(float* acc, int64_t plane, int64_t pitch, int w, int h, const float* norm,
                                  const uint8_t* sm, const float* const* lap, const float* const* wgt,
                                  void* const* mask1, int64_t pitch_n, int wn, int hn, int frames, float inv_count,
                                  int out_storage, cudaStream_t s) {
-  const dim3 grid((unsigned)((w + kTileW - 1) / kTileW), (unsigned)((h + kTileH - 1) / kTileH));
-  if (frames <= 0 || grid.y > 65535u) return cudaErrorInvalidValue;
-  static DeviceOnce cfg_f32, cfg_f16, cfg_bf16;
-  cudaError_t e;
-  switch (out_storage) {
+  if (frames <= 0 || (h + kTileH - 1) / kTileH > 65535) return cudaErrorInvalidValue;
+  return launch_blend_reduce_o<float, true>(out_storage, acc, plane, pitch, w, h, norm, sm,
+                                            (const void* const*)lap, (const void* const*)wgt, mask1, pitch_n, wn, hn,
+                                            frames, inv_count, s);
+}
+
+cudaError_t launch_blend_reduce(float* acc, int64_t plane, int64_t pitch, int w, int h, const uint8_t* sm,
+                                const void* const* lap, const void* const* mask, void* const* mask_next,
+                                int64_t pitch_n, int wn, int hn, int frames, int storage, int out_storage,
+                                cudaStream_t s) {
+  if (frames <= 0 || (h + kTileH - 1) / kTileH > 65535) return cudaErrorInvalidValue;
+  switch (storage) {
     case FS_STORAGE_F32:
-      if ((e = configure(blend0_reduce_kernel<float>, kB0Smem, &cfg_f32)) != cudaSuccess) return e;
-      blend0_reduce_kernel<float><<<grid, kThreads, kB0Smem, s>>>(acc, plane, pitch, w, h, norm, sm, lap, wgt,
-                                                                  mask1, pitch_n, wn, hn, frames, inv_count);
-      break;
+      return launch_blend_reduce_o<float, false>(out_storage, acc, plane, pitch, w, h, nullptr, sm, lap, mask,
+                                                 mask_next, pitch_n, wn, hn, frames, 0.0f, s);
     case FS_STORAGE_F16:
-      if ((e = configure(blend0_reduce_kernel<__half>, kB0Smem, &cfg_f16)) != cudaSuccess) return e;
-      blend0_reduce_kernel<__half><<<grid, kThreads, kB0Smem, s>>>(acc, plane, pitch, w, h, norm, sm, lap, wgt,
-                                                                   mask1, pitch_n, wn, hn, frames, inv_count);
-      break;
+      return launch_blend_reduce_o<__half, false>(out_storage, acc, plane, pitch, w, h, nullptr, sm, lap, mask,
+                                                  mask_next, pitch_n, wn, hn, frames, 0.0f, s);
     case FS_STORAGE_BF16:
-      if ((e = configure(blend0_reduce_kernel<__nv_bfloat16>, kB0Smem, &cfg_bf16)) != cudaSuccess) return e;
-      blend0_reduce_kernel<__nv_bfloat16><<<grid, kThreads, kB0Smem, s>>>(acc, plane, pitch, w, h, norm, sm, lap,
-                                                                           wgt, mask1, pitch_n, wn, hn, frames,
-                                                                           inv_count);
-      break;
+      return launch_blend_reduce_o<__nv_bfloat16, false>(out_storage, acc, plane, pitch, w, h, nullptr, sm, lap, mask,
+                                                         mask_next, pitch_n, wn, hn, frames, 0.0f, s);
     default: return cudaErrorInvalidValue;
   }
-  return cudaGetLastError();
 }
 
 template <template <typename, bool> class KER, bool L0>

@@ -244,6 +244,19 @@ cudaError_t launch_blend0_reduce(float* acc, int64_t plane, int64_t pitch, int w
                                  const uint8_t* sm, const float* const* lap, const float* const* wgt,
                                  void* const* mask1, int64_t pitch_n, int wn, int hn, int frames, float inv_count,
                                  int out_storage, cudaStream_t s);
+// The same for a level l >= 1 of a split-pyramid stack: acc = sum over
+// frames, in order, of lap[k] x mask[k] (both in `storage`; 3 Laplacian
+// planes of `plane` samples), and mask_next[k] the REDUCE of mask[k] with
+// the level's mask support sm, as launch_blend and launch_mask_reduce give
+// them (level l + 1: wn x hn, row pitch pitch_n, in out_storage).
+cudaError_t launch_blend_reduce(float* acc, int64_t plane, int64_t pitch, int w, int h, const uint8_t* sm,
+                                const void* const* lap, const void* const* mask, void* const* mask_next,
+                                int64_t pitch_n, int wn, int hn, int frames, int storage, int out_storage,
+                                cudaStream_t s);
+// Tiles a level needs (64 x 32 each) for launch_blend_reduce to fill the GPU
+// better than the per-frame launches: below it the mask REDUCE and the blend
+// of the level run apart, with every frame in the grid.
+static constexpr int64_t kBlendReduceMinTiles = 1184;
 // acc = sum over frames k, in order, of lap[k] (3 planes of `plane`) times
 // mask[k] (both in storage T: 0 f32, 1 f16, 2 bf16), written over acc.
 cudaError_t launch_blend(float* acc, int64_t plane, int64_t pitch, int w, int h, const void* const* lap,
