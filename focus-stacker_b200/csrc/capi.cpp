@@ -258,6 +258,10 @@ struct fs_stack {
   bool finished = false;
   cudaEvent_t copy_done = nullptr;
   cudaEvent_t done = nullptr;     // recorded after the output copy of fs_stack_finish_async
+  // the exact-sample queue of a pass-1 / pass-2 remap batch (8-bit frames)
+  uint32_t* exact_n = nullptr;
+  uint64_t* exact_q = nullptr;
+  uint32_t exact_cap = 0;
   std::vector<cudaEvent_t> slot_done;  // per staging buffer: the remap that last read it
   float* base_out = nullptr;      // optional device buffer for the collapsed base (RGB f32)
   uint32_t fp_level = 0;          // first level run one frame per CTA (none: >= L - 1)
@@ -359,6 +363,9 @@ int launch_remap_weights_batch(fs_stack* s, const std::vector<fs_stack::Frame>& 
   a.norm = s->norm;
   a.uni = s->uni;
   a.pitch = s->pitch[0];
+  a.exact_q = s->exact_q;
+  a.exact_n = s->exact_n;
+  a.exact_cap = s->exact_cap;
   for (size_t k = begin; k < end; ++k) {
     std::string why;
     if (!build_frame_in(s, frames[k], &a.f[k - begin], &why)) return set_err(s->ctx, FS_ERR_INVALID, why);
@@ -375,7 +382,8 @@ int launch_remap_weights_batch(fs_stack* s, const std::vector<fs_stack::Frame>& 
   cudaError_t e = timed(s->ctx, pass1 ? "pass1" : "remap_weights",
                         [&] { return launch_remap_weights(a, (int)s->border, s->ctx->stream); });
   if (e != cudaSuccess) return cuda_err(s->ctx, e, "remap/weights launch");
-  s->ctx->launches += 1;  // two kernels: the remap of the tiles, then the weights
+  // the remap of the tiles, its exact samples, then the weights
+  s->ctx->launches += a.exact_q ? 2 : 1;
   return FS_OK;
 }
 
@@ -465,6 +473,9 @@ int launch_lap0_batch(fs_stack* s, size_t begin, size_t end) {
   r.H = a.H;
   r.K = a.K;
   r.pitch = s->pitch[0];
+  r.exact_q = s->exact_q;
+  r.exact_n = s->exact_n;
+  r.exact_cap = s->exact_cap;
   for (size_t k = begin; k < end; ++k) {
     std::string why;
     if (!build_frame_in(s, s->frames[k], &r.f[k - begin], &why)) return set_err(s->ctx, FS_ERR_INVALID, why);
@@ -475,6 +486,7 @@ int launch_lap0_batch(fs_stack* s, size_t begin, size_t end) {
   }
   cudaError_t e = timed(s->ctx, "pass1", [&] { return launch_remap_tiles(r, s->ctx->stream); });
   if (e != cudaSuccess) return cuda_err(s->ctx, e, "remap launch");
+  if (r.exact_q) s->ctx->launches += 1;  // and its exact samples
   e = timed(s->ctx, "pass1", [&] { return launch_lap0(a, (int)s->border, s->ctx->stream); });
   if (e != cudaSuccess) return cuda_err(s->ctx, e, "fused pass-1 launch");
   return FS_OK;
@@ -968,7 +980,19 @@ struct StackPlan {
   size_t laps_frame = 0;                // LAPS: weight, Laplacians, top Gaussian and masks of one frame
   size_t fused_frame = 0;               // FUSED: the same without the level-0 Laplacian
   size_t fused_fixed = 0;               // FUSED: the level-0 Laplacian sum of the fallback pixels
+  uint32_t exact_cap = 0;               // entries of the exact-sample queue (0: none)
 };
+
+// The exact-sample queue of a remap batch: kExactPerTile entries per tile and
+// frame of a batch (8-bit remapped frames only: aligned frames are not
+// sampled, 16-bit frames take the exact path in their own kernels), after a
+// 16-byte counter.
+uint32_t exact_queue_cap(const StackPlan& p, const fs_stack_desc& d) {
+  if (d.input_is_aligned || d.sample_bits == 16) return 0;
+  const uint64_t tiles = (uint64_t)((p.W + kTileW - 1) / kTileW) * ((p.H + kTileH - 1) / kTileH);
+  return (uint32_t)std::min<uint64_t>(tiles * p.K * kExactPerTile, 1u << 30);
+}
+size_t exact_queue_bytes(uint32_t cap) { return cap ? 16 + (size_t)cap * 8 : 0; }
 
 // Levels with fewer 64x32 tiles than this run one frame per CTA (grid.z = K)
 // and add the frames' contributions in order afterwards: a small level has
@@ -1000,6 +1024,8 @@ StackPlan plan_stack(const fs_stack_desc& d) {
   for (uint32_t l = 0; l < p.L; ++l) p.fixed += (size_t)p.pitch[l] * p.lh[l] * 12;  // accumulators
   for (uint32_t l = 1; l + 1 < p.L; ++l) p.fixed += p.K * ((size_t)p.pitch[l] * p.lh[l] * (esz * 4 + 1));
   p.fixed += (size_t)p.W * p.H * 3 * bps;  // output
+  p.exact_cap = exact_queue_cap(p, d);
+  p.fixed += exact_queue_bytes(p.exact_cap);
   // per frame (cache) or batch slot: remapped RGBA + weight; 16-bit frames:
   // level-0 Gaussian (3 f32 planes), normalised mask (f32) and support (u8)
   p.planes = bps == 2 ? n0 * 17 : n0 * 8;
@@ -1104,6 +1130,12 @@ static int begin_impl(fs_ctx* ctx, const fs_stack_desc* desc, fs_stack** out, in
   s->norm = (float*)p;
   if ((rc = stack_alloc(s, n0, &p)) != FS_OK) return fail(rc);
   s->uni = (uint8_t*)p;
+  if (plan.exact_cap) {
+    if ((rc = stack_alloc(s, exact_queue_bytes(plan.exact_cap), &p)) != FS_OK) return fail(rc);
+    s->exact_n = (uint32_t*)p;
+    s->exact_q = (uint64_t*)((uint8_t*)p + 16);
+    s->exact_cap = plan.exact_cap;
+  }
   s->sm.push_back(s->uni);
   for (uint32_t l = 1; l < s->L; ++l) {
     if ((rc = stack_alloc(s, (size_t)s->pitch[l] * s->lh[l], &p)) != FS_OK) return fail(rc);
@@ -2110,7 +2142,7 @@ int batch_enqueue_forked(fs_batch* b) {
 // every piece (at most this many pieces: fixed state, level slots, batch
 // slots, per-frame planes).
 uint64_t arena_need(const StackPlan& p, uint32_t frames, Pass2Mode m) {
-  const uint64_t pieces = 8 + 3ull * p.L + (uint64_t)p.K * (p.L + 1) + frames;
+  const uint64_t pieces = 9 + 3ull * p.L + (uint64_t)p.K * (p.L + 1) + frames;
   return plan_bytes(p, frames, m, false) + pieces * kArenaAlign;
 }
 

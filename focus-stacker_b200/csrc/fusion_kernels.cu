@@ -226,8 +226,12 @@ struct __align__(16) RemapTileSmem {
   TileAnchor anchor[kTileBlocks];
   uint32_t count;
   uint32_t overflow;
+  uint32_t base;               // the CTA's first entry in the batch's exact-sample queue (kNoQueue: no room)
+  uint32_t reserved;           // the first entry reserved when there was no room
   uint32_t item[kExactQueue];  // ry << 16 | rx
 };
+constexpr uint32_t kNoQueue = 0xFFFFFFFFu;
+constexpr uint64_t kEmptyEntry = ~0ull;
 
 }  // namespace
 
@@ -306,6 +310,28 @@ __global__ void __launch_bounds__(NT, 6) remap_tile_kernel(const __grid_constant
   }
   __syncthreads();
   const uint32_t n = min(S.count, (uint32_t)kExactQueue);
+  if (a.exact_q && !S.overflow && n > 0) {  // block-uniform
+    // hand the undecided samples to the batch's queue: the exact FP64 sampler
+    // then runs on full warps in remap_exact_kernel instead of on a few lanes
+    // of this CTA while its other warps have finished
+    if (threadIdx.x == 0) {
+      const uint32_t base = atomicAdd(a.exact_n, n);
+      S.base = base + n <= a.exact_cap ? base : kNoQueue;
+      S.reserved = base;
+    }
+    __syncthreads();
+    if (S.base != kNoQueue) {
+      for (uint32_t i = threadIdx.x; i < n; i += NT) {
+        const uint32_t qx = S.item[i] & 0xFFFFu, qy = S.item[i] >> 16;
+        a.exact_q[S.base + i] = ((uint64_t)k << 48) | ((uint64_t)(y0 + qy) << 24) | (uint64_t)(x0 + qx);
+      }
+      return;
+    }
+    // no room: the entries reserved below the capacity stay empty and the
+    // CTA takes its samples itself
+    for (uint32_t i = threadIdx.x; i < n && S.reserved + i < a.exact_cap; i += NT)
+      a.exact_q[S.reserved + i] = kEmptyEntry;
+  }
   for (uint32_t i = threadIdx.x; i < n; i += NT) {
     const int qx = (int)(S.item[i] & 0xFFFFu), qy = (int)(S.item[i] >> 16);
     out[(int64_t)(y0 + qy) * pitch + x0 + qx] = sample_exact(f.warp, f.src, x0 + qx, y0 + qy);
@@ -317,6 +343,18 @@ __global__ void __launch_bounds__(NT, 6) remap_tile_kernel(const __grid_constant
       if (!sample_tile<CH>(org, spitch, xm, ym, lim, an, fdu, fdv, du, dv, &v))
         col[j * step] = sample_exact(f.warp, f.src, X, y0 + ry0 + 4 * j);
     }
+  }
+}
+
+// The batch's queued samples, one per thread, by the reference's FP64
+// sampler (the same call the tile kernel makes for the samples it keeps).
+__global__ void __launch_bounds__(NT) remap_exact_kernel(const __grid_constant__ RemapWeightArgs a) {
+  const uint32_t n = min(*a.exact_n, a.exact_cap);
+  for (uint32_t i = blockIdx.x * NT + threadIdx.x; i < n; i += gridDim.x * NT) {
+    const uint64_t e = a.exact_q[i];
+    if (e == kEmptyEntry) continue;
+    const int k = (int)(e >> 48), Y = (int)((e >> 24) & 0xFFFFFFu), X = (int)(e & 0xFFFFFFu);
+    a.out[k].rgba[(int64_t)Y * a.pitch + X] = sample_exact(a.f[k].warp, a.f[k].src, X, Y);
   }
 }
 
@@ -495,9 +533,20 @@ cudaError_t launch_remap_tiles(const RemapWeightArgs& a, cudaStream_t s) {
                                              (uint64_t)src.pitch * (uint64_t)src.h >= (1ull << 32)))
       return cudaErrorInvalidValue;
   }
+  if (a.exact_q && (!a.exact_n || ((uintptr_t)a.exact_q & 7))) return cudaErrorInvalidValue;
+  if (a.exact_q) {
+    cudaError_t e = cudaMemsetAsync(a.exact_n, 0, sizeof(uint32_t), s);
+    if (e != cudaSuccess) return e;
+  }
   const dim3 grid((a.W + TW - 1) / TW, (a.H + TH - 1) / TH, a.K);
   if (a.f[0].src.ch == 1) remap_tile_kernel<1><<<grid, NT, 0, s>>>(a);
   else remap_tile_kernel<3><<<grid, NT, 0, s>>>(a);
+  if (a.exact_q) {
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    remap_exact_kernel<<<(unsigned)(8 * sms), NT, 0, s>>>(a);
+  }
   return cudaGetLastError();
 }
 

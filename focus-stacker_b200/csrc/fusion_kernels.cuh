@@ -50,7 +50,18 @@ struct RemapWeightArgs {
   int64_t pitch;         // level-0 row pitch (elements; bytes for u8 planes)
   FrameIn f[kMaxBatch];
   FramePlanes out[kMaxBatch];  // null members: do not store
+  // the batch's exact-sample queue (remap_tile_kernel hands the samples its
+  // fast path cannot decide to remap_exact_kernel): frame << 48 | Y << 24 |
+  // X per entry, exact_n entries reserved of exact_cap; null: each CTA takes
+  // its own undecided samples exactly
+  uint64_t* exact_q;
+  uint32_t* exact_n;
+  uint32_t exact_cap;
 };
+// Entries of the exact-sample queue per 64x32 tile and frame of a batch
+// (about 3 are used under the synthetic stacks' warps; a CTA whose samples
+// do not fit takes them itself).
+static constexpr uint32_t kExactPerTile = 16;
 
 struct LevelArgs {
   int32_t level;         // l: this launch reads level l, writes level l + 1
