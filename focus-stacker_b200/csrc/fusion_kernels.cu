@@ -1581,6 +1581,19 @@ __device__ __forceinline__ void ld2(const T* p, float* v) {
   }
 }
 
+// Two consecutive samples, one vector store (8 bytes of f32, 4 of f16/bf16).
+template <typename T>
+__device__ __forceinline__ void st2(T* p, float v0, float v1) {
+  if constexpr (std::is_same<T, float>::value) {
+    *reinterpret_cast<float2*>(p) = make_float2(v0, v1);
+  } else {
+    T h[2];
+    stv<T>(h, 0, v0);
+    stv<T>(h, 1, v1);
+    *reinterpret_cast<uint32_t*>(p) = *reinterpret_cast<const uint32_t*>(h);
+  }
+}
+
 // Four consecutive samples, one vector store (16 bytes of f32, 8 of f16/bf16).
 template <typename T>
 __device__ __forceinline__ void st4(T* p, const float* v) {
@@ -1986,13 +1999,15 @@ __global__ void __launch_bounds__(32 * kImgWarps) img_stream_kernel(const __grid
       }
       if (emit && r >= i0 && r < i1) {
         const LevelPlanes& out = a.out[k];
-        const int64_t o = (int64_t)r * a.pitch_n + J0;
+        const int64_t o = (int64_t)r * a.pitch_n + J0;  // J0 even: the pair is one aligned vector
+        if (j1in) {
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {
-          if (J0 + h >= a.wn) continue;
+          for (int ch = 0; ch < 3; ++ch) st2<T>((T*)out.g + ch * out.plane + o, g[0][ch], g[1][ch]);
+          *reinterpret_cast<uint16_t*>(out.s + o) = (uint16_t)((sp[0] ? 1u : 0u) | (sp[1] ? 0x100u : 0u));
+        } else {
 #pragma unroll
-          for (int ch = 0; ch < 3; ++ch) stv<T>((T*)out.g, ch * out.plane + o + h, g[h][ch]);
-          out.s[o + h] = sp[h] ? 1 : 0;
+          for (int ch = 0; ch < 3; ++ch) stv<T>((T*)out.g, ch * out.plane + o, g[0][ch]);
+          out.s[o] = sp[0] ? 1 : 0;
         }
       }
       // horizontal EXPAND of row r onto columns c .. c + 3 (clamped)
@@ -2047,9 +2062,10 @@ __global__ void __launch_bounds__(32 * kImgWarps) img_stream_kernel(const __grid
           float lv[4];
 #pragma unroll
           for (int u = 0; u < 4; ++u) {
+            // odd rows: the reference's (H + H) * 0.5, which is H exactly
             const float e = yy == 0
                 ? __fmul_rn(__fadd_rn(__fadd_rn(Hm2[ch][u], __fmul_rn(6.0f, Hm1[ch][u])), Hc[ch][u]), 0.125f)
-                : __fmul_rn(__fadd_rn(Hm1[ch][u], Hm1[ch][u]), 0.5f);
+                : Hm1[ch][u];
             lv[u] = __fsub_rn(gv[ch][u], e);
           }
           TL* lc = lp + ch * a.acc_plane_l;
@@ -2248,13 +2264,15 @@ __global__ void __launch_bounds__(32 * kImgWarps) img_stage_kernel(const __grid_
       }
       if (emit && r >= i0 && r < i1) {
         const LevelPlanes& out = a.out[k];
-        const int64_t o = (int64_t)r * a.pitch_n + J0;
+        const int64_t o = (int64_t)r * a.pitch_n + J0;  // J0 even: the pair is one aligned vector
+        if (j1in) {
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {
-          if (J0 + h >= a.wn) continue;
+          for (int ch = 0; ch < 3; ++ch) st2<T>((T*)out.g + ch * out.plane + o, g[0][ch], g[1][ch]);
+          *reinterpret_cast<uint16_t*>(out.s + o) = (uint16_t)((sp[0] ? 1u : 0u) | (sp[1] ? 0x100u : 0u));
+        } else {
 #pragma unroll
-          for (int ch = 0; ch < 3; ++ch) stv<T>((T*)out.g, ch * out.plane + o + h, g[h][ch]);
-          out.s[o + h] = sp[h] ? 1 : 0;
+          for (int ch = 0; ch < 3; ++ch) stv<T>((T*)out.g, ch * out.plane + o, g[0][ch]);
+          out.s[o] = sp[0] ? 1 : 0;
         }
       }
 #pragma unroll
@@ -2298,9 +2316,10 @@ __global__ void __launch_bounds__(32 * kImgWarps) img_stage_kernel(const __grid_
           float lv[4];
 #pragma unroll
           for (int u = 0; u < 4; ++u) {
+            // odd rows: the reference's (H + H) * 0.5, which is H exactly
             const float e = yy == 0
                 ? __fmul_rn(__fadd_rn(__fadd_rn(Hm2[ch][u], __fmul_rn(6.0f, Hm1[ch][u])), Hc[ch][u]), 0.125f)
-                : __fmul_rn(__fadd_rn(Hm1[ch][u], Hm1[ch][u]), 0.5f);
+                : Hm1[ch][u];
             lv[u] = __fsub_rn(gv[ch][u], e);
           }
           T* lc = lp + ch * a.acc_plane_l;
