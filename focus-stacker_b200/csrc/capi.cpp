@@ -1543,8 +1543,17 @@ static int pass2_impl(fs_stack* s, fs_frame_fetch_cb refetch, void* user, bool f
       return timed(ctx, l == 0 ? "level0" : "level",
                    [&] { return launch_mask_reduce(m, (int)N, in_storage, out_storage, st); });
     };
-    if (s->mode == P2_FUSED && 1 < s->L && 0 < tail && (e = mask_reduce(0)) != cudaSuccess)
-      return cuda_err(ctx, e, "mask reduce");
+    if (s->mode == P2_FUSED && 1 < s->L && 0 < tail) {
+      // FUSED level 0: every frame's normalised masks REDUCEd to level 1 (the
+      // blend of level 0 happened in pass 1)
+      const int out_storage = 2 < s->L ? s->storage : FS_STORAGE_F32;
+      e = timed(ctx, "level0", [&] {
+        return launch_blend0_reduce(nullptr, s->pitch[0] * s->lh[0], s->pitch[0], (int)s->W, (int)s->H, s->norm,
+                                    s->sm[0], nullptr, s->tab + N, (void* const*)(s->tab + 3 * N), s->pitch[1],
+                                    (int)s->lw[1], (int)s->lh[1], (int)N, inv_count, out_storage, st);
+      });
+      if (e != cudaSuccess) return cuda_err(ctx, e, "level-0 mask reduce");
+    }
     // levels l >= 1 with enough tiles to fill the GPU: the blend of the level
     // and its mask REDUCE to l + 1 in one pass over every frame
     uint32_t lf = 1;

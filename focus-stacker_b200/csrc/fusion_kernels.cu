@@ -1430,16 +1430,19 @@ __global__ void __launch_bounds__(kThreads, 2)
 #pragma unroll
       for (int e = 0; e < 4; ++e) a[u][c][e] = 0.0f;
   auto slot = [&](int s, int i) { return stage + (s * kB0Slots + i) * kThreads + tid; };
+  const bool blending = lap != nullptr;  // null: the masks alone (FUSED level 0)
   auto issue = [&](int k) {
     const int s = k & 1;
     const TS* wk = (const TS*)wgt[k];
-    const TS* lk = (const TS*)lap[k];
     b0_copy<TS>(slot(s, 0), wk + c0.off, c0.in);
     b0_copy<TS>(slot(s, 1), wk + c1.off, c1.in);
+    if (blending) {
+      const TS* lk = (const TS*)lap[k];
 #pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      b0_copy<TS>(slot(s, 2 + c), lk + c * plane + c0.off, c0.in);
-      b0_copy<TS>(slot(s, 5 + c), lk + c * plane + c1.off, c1.in);
+      for (int c = 0; c < 3; ++c) {
+        b0_copy<TS>(slot(s, 2 + c), lk + c * plane + c0.off, c0.in);
+        b0_copy<TS>(slot(s, 5 + c), lk + c * plane + c1.off, c1.in);
+      }
     }
     if (has_halo) b0_copy<TS>(slot(s, 8), wk + ch.off, ch.in);
   };
@@ -1468,8 +1471,10 @@ __global__ void __launch_bounds__(kThreads, 2)
     cp_async_wait1();
     {
       const float4 m0 = mask(c0, slot(s, 0), 0), m1 = mask(c1, slot(s, 1), 1);
-      blend(a[0], s, 2, m0);
-      blend(a[1], s, 5, m1);
+      if (blending) {
+        blend(a[0], s, 2, m0);
+        blend(a[1], s, 5, m1);
+      }
       *reinterpret_cast<float4*>(buf + c0.so) = b0_keep(c0, m0);
       *reinterpret_cast<float4*>(buf + c1.so) = b0_keep(c1, m1);
       if (has_halo) *reinterpret_cast<float4*>(buf + ch.so) = b0_keep(ch, mask(ch, slot(s, 8), 2));
@@ -1514,8 +1519,10 @@ __global__ void __launch_bounds__(kThreads, 2)
           for (int ci = 0; ci < 3; ++ci) acc[ci * plane + o + e] = av[ci][e];
     }
   };
-  store(c0, a[0]);
-  store(c1, a[1]);
+  if (blending) {
+    store(c0, a[0]);
+    store(c1, a[1]);
+  }
 }
 
 // Blend of one level over all frames in order, one pixel per thread (the

@@ -251,6 +251,8 @@ cudaError_t launch_img_level(const LevelArgs& a, int storage, cudaStream_t s);
 // mask1[k] (level-1 size wn x hn, row pitch pitch_n, in out_storage) the
 // REDUCE of those normalised masks with the union support sm (row pitch
 // `pitch`), as launch_mask_reduce forms it; the weight planes are only read.
+// lap null: the masks alone (acc untouched), the level-0 mask pyramid step
+// of a FUSED stack.
 cudaError_t launch_blend0_reduce(float* acc, int64_t plane, int64_t pitch, int w, int h, const float* norm,
                                  const uint8_t* sm, const float* const* lap, const float* const* wgt,
                                  void* const* mask1, int64_t pitch_n, int wn, int hn, int frames, float inv_count,
