@@ -1521,8 +1521,8 @@ static int pass2_impl(fs_stack* s, fs_frame_fetch_cb refetch, void* user, bool f
       });
     }
     if (e != cudaSuccess) return cuda_err(ctx, e, "level-0 blend");
-    // the mask pyramid of every frame, level by level (one frame per grid z),
-    // from level `from` (LAPS: the level-0 blend has REDUCEd its masks)
+    // the mask pyramid of every frame from level 1 on, level by level (one
+    // frame per grid z; level 0's masks come from the level-0 tile kernel)
     auto mask_reduce = [&](uint32_t l) {
       MaskReduceArgs m;
       m.in = (const void* const*)(s->tab + (size_t)l * 2 * N + N);
@@ -1534,14 +1534,8 @@ static int pass2_impl(fs_stack* s, fs_frame_fetch_cb refetch, void* user, bool f
       m.hn = (int32_t)s->lh[l + 1];
       m.pitch_l = s->pitch[l];
       m.pitch_n = s->pitch[l + 1];
-      // FUSED level 0: each frame's raw weight, normalised by the weight sum on
-      // the fly
-      m.norm = l == 0 && s->mode == P2_FUSED ? s->norm : nullptr;
-      m.inv_count = inv_count;
-      const int in_storage = l == 0 ? FS_STORAGE_F32 : s->storage;
       const int out_storage = l + 2 < s->L ? s->storage : FS_STORAGE_F32;
-      return timed(ctx, l == 0 ? "level0" : "level",
-                   [&] { return launch_mask_reduce(m, (int)N, in_storage, out_storage, st); });
+      return timed(ctx, "level", [&] { return launch_mask_reduce(m, (int)N, s->storage, out_storage, st); });
     };
     if (s->mode == P2_FUSED && 1 < s->L && 0 < tail) {
       // FUSED level 0: every frame's normalised masks REDUCEd to level 1 (the

@@ -1639,14 +1639,10 @@ __device__ __forceinline__ void st4(T* p, const float* v) {
   }
 }
 
-// Horizontal sums of level-l row r for output columns j0, j0 + 1.  N0: the
-// level-0 row of a LAPS stack, `in` holding a frame's raw weights, each tap
-// normalised on the fly (w / N where N > 1e-12, else inv_count; the division
-// blend0 of the reference's normalizeWeightsInto, src/fuse/pyramid.zig:303-316).
-template <typename T, bool N0 = false>
+// Horizontal sums of level-l row r for output columns j0, j0 + 1.
+template <typename T>
 __device__ __forceinline__ void reduce_row(const T* in, const uint8_t* sm, int64_t pitch, int wl, int hl, int r,
-                                           int j0, float* v, float* ws, const float* norm = nullptr,
-                                           float inv_count = 0.0f) {
+                                           int j0, float* v, float* ws) {
   float m[7];
   uint32_t s4 = 0u, s2 = 0u, s6 = 0u;  // support bytes of taps 2..5, 0..1 and 6
 #pragma unroll
@@ -1665,19 +1661,6 @@ __device__ __forceinline__ void reduce_row(const T* in, const uint8_t* sm, int64
     if (c + 4 < wl) {
       m[6] = ldv<T>(row, c + 4);
       s6 = srow[c + 4];
-    }
-    if constexpr (N0) {
-      // taps past the level or without support are masked out below, whatever
-      // their quotient
-      const float* nrow = norm + (int64_t)r * pitch;
-      float nv[7];
-#pragma unroll
-      for (int u = 0; u < 7; ++u) nv[u] = 1.0f;
-      ld4<float>(nrow + c, nv + 2);
-      if (c > 0) ld2<float>(nrow + c - 2, nv);
-      if (c + 4 < wl) nv[6] = nrow[c + 4];
-#pragma unroll
-      for (int u = 0; u < 7; ++u) m[u] = nv[u] > 1e-12f ? __fdiv_rn(m[u], nv[u]) : inv_count;
     }
   }
   if (c + 3 >= wl) s4 &= (1u << (8 * (wl - c))) - 1u;  // columns past the level: no support (wl - c in 1..3)
@@ -1709,7 +1692,7 @@ __device__ __forceinline__ void reduce_row(const T* in, const uint8_t* sm, int64
 // Grid: frames fastest (blockIdx.x), then column and row blocks, so that the
 // CTAs resident together read the same region's support (and, at level 0,
 // weight sum) through L2 instead of fetching it again for every frame.
-template <typename TI, typename TO, bool N0 = false>
+template <typename TI, typename TO>
 __global__ void __launch_bounds__(32 * kReduceWarps) mask_reduce_kernel(const __grid_constant__ MaskReduceArgs a) {
   const int j0 = 2 * (int)(blockIdx.y * 32 + threadIdx.x);
   const int i0 = (int)(blockIdx.z * kReduceWarps + threadIdx.y) * kReduceRows;
@@ -1721,10 +1704,10 @@ __global__ void __launch_bounds__(32 * kReduceWarps) mask_reduce_kernel(const __
   float hv[5][2], hw[5][2];
 #pragma unroll
   for (int u = 0; u < 3; ++u)
-    reduce_row<TI, N0>(in, a.sm, a.pitch_l, a.wl, a.hl, 2 * i0 - 2 + u, j0, hv[u], hw[u], a.norm, a.inv_count);
+    reduce_row<TI>(in, a.sm, a.pitch_l, a.wl, a.hl, 2 * i0 - 2 + u, j0, hv[u], hw[u]);
   for (int i = i0; i < i1; ++i) {
-    reduce_row<TI, N0>(in, a.sm, a.pitch_l, a.wl, a.hl, 2 * i + 1, j0, hv[3], hw[3], a.norm, a.inv_count);
-    reduce_row<TI, N0>(in, a.sm, a.pitch_l, a.wl, a.hl, 2 * i + 2, j0, hv[4], hw[4], a.norm, a.inv_count);
+    reduce_row<TI>(in, a.sm, a.pitch_l, a.wl, a.hl, 2 * i + 1, j0, hv[3], hw[3]);
+    reduce_row<TI>(in, a.sm, a.pitch_l, a.wl, a.hl, 2 * i + 2, j0, hv[4], hw[4]);
     TO* orow = out + (int64_t)i * a.pitch_n;
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
@@ -1746,13 +1729,13 @@ __global__ void __launch_bounds__(32 * kReduceWarps) mask_reduce_kernel(const __
   }
 }
 
-template <typename TI, bool N0 = false>
+template <typename TI>
 static cudaError_t launch_mask_reduce_in(const MaskReduceArgs& a, dim3 grid, dim3 block, int out_storage,
                                          cudaStream_t s) {
   switch (out_storage) {
-    case FS_STORAGE_F32: mask_reduce_kernel<TI, float, N0><<<grid, block, 0, s>>>(a); break;
-    case FS_STORAGE_F16: mask_reduce_kernel<TI, __half, N0><<<grid, block, 0, s>>>(a); break;
-    case FS_STORAGE_BF16: mask_reduce_kernel<TI, __nv_bfloat16, N0><<<grid, block, 0, s>>>(a); break;
+    case FS_STORAGE_F32: mask_reduce_kernel<TI, float><<<grid, block, 0, s>>>(a); break;
+    case FS_STORAGE_F16: mask_reduce_kernel<TI, __half><<<grid, block, 0, s>>>(a); break;
+    case FS_STORAGE_BF16: mask_reduce_kernel<TI, __nv_bfloat16><<<grid, block, 0, s>>>(a); break;
     default: return cudaErrorInvalidValue;
   }
   return cudaGetLastError();
@@ -1765,10 +1748,6 @@ cudaError_t launch_mask_reduce(const MaskReduceArgs& a, int frames, int in_stora
   const unsigned gy = (unsigned)((a.hn + kReduceWarps * kReduceRows - 1) / (kReduceWarps * kReduceRows));
   if (frames <= 0 || gx > 65535u || gy > 65535u) return cudaErrorInvalidValue;
   const dim3 grid((unsigned)frames, gx, gy);
-  if (a.norm) {  // level 0 of a FUSED stack: raw weights, normalised on the fly
-    if (in_storage != FS_STORAGE_F32) return cudaErrorInvalidValue;
-    return launch_mask_reduce_in<float, true>(a, grid, block, out_storage, s);
-  }
   switch (in_storage) {
     case FS_STORAGE_F32: return launch_mask_reduce_in<float>(a, grid, block, out_storage, s);
     case FS_STORAGE_F16: return launch_mask_reduce_in<__half>(a, grid, block, out_storage, s);

@@ -144,16 +144,11 @@ struct CollapseArgs {
 // level-l union support (src/fuse/pyramid.zig:997-1043), the products and
 // sums of the level kernels' mask REDUCE in the same order.
 struct MaskReduceArgs {
-  const void* const* in;  // per frame: level-l mask (level 0: the frame's weight plane, see norm)
+  const void* const* in;  // per frame: level-l mask (l >= 1)
   void* const* out;       // per frame: level-(l+1) mask
   const uint8_t* sm;      // level-l union support
   int32_t wl, hl, wn, hn;
   int64_t pitch_l, pitch_n;
-  // level 0 of a LAPS stack: `in` holds each frame's raw weight w and the
-  // mask is formed on the fly, w / N where N > 1e-12 else inv_count
-  // (src/fuse/pyramid.zig:303-316); null at levels >= 1
-  const float* norm;
-  float inv_count;
 };
 // Storage of in / out masks: 0 f32, 1 f16, 2 bf16.
 cudaError_t launch_mask_reduce(const MaskReduceArgs& a, int frames, int in_storage, int out_storage, cudaStream_t s);
