@@ -198,6 +198,13 @@ class Context:
         """Change the HBM budget later allocations and pass-2 mode choices use."""
         _check(L().fs_ctx_set_budget(self.handle, int(hbm_budget_bytes)), self.handle)
 
+    def set_level_schedule(self, fuse_min_tiles: int = 0, tail_side: int = 0):
+        """Level schedule of the split-pyramid stacks begun from now on: levels
+        of at least fuse_min_tiles 64x32 tiles blend and REDUCE their masks in
+        one pass (0: the default 1184), levels with both sides at most
+        tail_side (0: 64) run as the small-level tail.  Same bytes either way."""
+        _check(L().fs_ctx_set_level_schedule(self.handle, int(fuse_min_tiles), int(tail_side)), self.handle)
+
     def stream_handle(self) -> int:
         """cudaStream_t of the context (e.g. for torch.cuda.ExternalStream)."""
         v = ctypes.c_void_p()
@@ -606,8 +613,11 @@ class StackBatch:
     second run on.  Frames are read at the same addresses on every run."""
 
     def __init__(self, ctx: Context, stacks: Sequence[BatchStack], lanes: int = 4, pass2_mode: int = -1,
-                 contrast_window: int = 5, frames_per_batch: int = 0, level_storage: int = 0):
+                 contrast_window: int = 5, frames_per_batch: int = 0, level_storage: int = 0,
+                 fuse_min_tiles: int = 0, tail_side: int = 0):
         self.ctx = ctx
+        # the lanes' stacks take the context's level schedule at creation
+        ctx.set_level_schedule(fuse_min_tiles, tail_side)
         n = len(stacks)
         descs = (_lib.FsStackDesc * n)()
         frame_lists, pose_lists = [], []

@@ -12,7 +12,17 @@ schedule knobs the library exposes by timing them on the device:
                     pass 1), 4: split pyramid with level 0 blended inside
                     pass 1 (12 B per frame-pixel less to keep), 0: pass-1 planes
                     kept, 1: frames kept and remapped again, -1: the first of
-                    3, 4, 0, 1 that fits the budget.
+                    3, 4, 0, 1 that fits the budget;
+  fuse_min_tiles    level schedule: levels of at least this many 64x32 tiles
+                    blend and REDUCE their masks in one pass over every frame
+                    (0: the library's 1184), the smaller ones in two launches
+                    with every frame in the grid;
+  tail_side         level schedule: levels with both sides at most this (0:
+                    64) run as the small-level tail, three launches for all of
+                    them.
+
+lanes x frames_per_batch x pass2_mode are searched first; the level schedule
+(SCHEDULE_SPACE) is then searched with the best of them.
 
 Every candidate is built as a StackBatch, run twice (direct, then captured),
 and timed over `reps` graph replays; the fastest wins.  Candidates that do not
@@ -32,6 +42,7 @@ from typing import Callable, Dict, Iterable, List, Sequence
 from . import api
 
 DEFAULT_SPACE = {"lanes": (2, 4, 8), "frames_per_batch": (4, 8), "pass2_mode": (3, 4, 0)}
+SCHEDULE_SPACE = {"fuse_min_tiles": (0, 296, 4294967295), "tail_side": (0, 32)}
 
 
 def candidates(space: Dict[str, Iterable]) -> List[dict]:
@@ -74,9 +85,12 @@ def _load(path: str) -> dict:
 
 
 def tune(ctx: api.Context, stacks: Sequence[api.BatchStack], space: Dict[str, Iterable] = None, reps: int = 3,
-         level_storage: int = 0, log: Callable[[str], None] = None, cache_path: str = None) -> dict:
-    """Time every candidate of `space` and return {"best": knobs, "trials": [...]}
-    (from `cache_path` without timing when it holds this workload)."""
+         level_storage: int = 0, log: Callable[[str], None] = None, cache_path: str = None,
+         schedule_space: Dict[str, Iterable] = None) -> dict:
+    """Time every candidate of `space`, then every level schedule of
+    `schedule_space` with the best of them, and return {"best": knobs,
+    "trials": [...]} (from `cache_path` without timing when it holds this
+    workload)."""
     key = signature(ctx, stacks, level_storage)
     if cache_path:
         hit = _load(cache_path).get(key)
@@ -95,6 +109,21 @@ def tune(ctx: api.Context, stacks: Sequence[api.BatchStack], space: Dict[str, It
     if not ok:
         raise api.FocusCudaError(3, "no candidate fits the budget")
     best = min(ok, key=lambda t: t["s_per_run"])
+    sched = schedule_space if schedule_space is not None else SCHEDULE_SPACE
+    keys = ("fuse_min_tiles", "tail_side")
+    for values in itertools.product(*(tuple(sched.get(k, (0,))) for k in keys)):
+        if all(v == 0 for v in values):
+            continue  # the library's schedule: timed above
+        knobs = dict(best["knobs"], **dict(zip(keys, values)))
+        try:
+            r = time_batch(ctx, stacks, reps=reps, level_storage=level_storage, **knobs)
+        except api.FocusCudaError as e:
+            r = {"knobs": knobs, "skipped": str(e)}
+        trials.append(r)
+        if log:
+            log(str(r))
+        if "s_per_run" in r and r["s_per_run"] < best["s_per_run"]:
+            best = r
     res = {"best": best["knobs"], "s_per_run": best["s_per_run"], "trials": trials}
     if cache_path:
         table = _load(cache_path)

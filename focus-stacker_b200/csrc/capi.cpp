@@ -43,6 +43,9 @@ struct fs_ctx {
   cudaStream_t stream = nullptr;
   cudaStream_t copy = nullptr;
   cudaStream_t idle = nullptr;  // given no work: frees of finished stacks take effect at once
+  // level schedule of the split-pyramid stacks begun from now on (0: defaults)
+  uint32_t fuse_min_tiles = 0;  // levels l >= 1 of at least this many tiles blend and REDUCE in one pass
+  uint32_t tail_side = 0;       // levels with both sides at most this go to the small-level tail
   std::string err;
   mutable std::mutex mu;
   bool timing = false;
@@ -278,6 +281,7 @@ struct fs_stack {
   // blend-tail launch's ticket (zero between launches)
   uint32_t tail = 0;
   uint32_t* tail_counter = nullptr;
+  int64_t fuse_min_tiles = kBlendReduceMinTiles;  // the context's schedule at begin
   bool tail_folded = false;  // pass 2 has added the tail levels' EXPANDs into acc[tail]
 };
 
@@ -756,6 +760,14 @@ int fs_ctx_set_budget(fs_ctx* ctx, uint64_t hbm_budget_bytes) {
   return FS_OK;
 }
 
+int fs_ctx_set_level_schedule(fs_ctx* ctx, uint32_t fuse_min_tiles, uint32_t tail_side) {
+  if (!ctx) return FS_ERR_INVALID;
+  if (tail_side > (uint32_t)kTailSide) return set_err(ctx, FS_ERR_INVALID, "tail side above the tail kernels' 64");
+  ctx->fuse_min_tiles = fuse_min_tiles;
+  ctx->tail_side = tail_side;
+  return FS_OK;
+}
+
 int fs_ctx_reserve(fs_ctx* ctx, uint64_t bytes) {
   if (!ctx) return FS_ERR_INVALID;
   if (bytes == 0) return FS_OK;
@@ -1119,6 +1131,7 @@ static int begin_impl(fs_ctx* ctx, const fs_stack_desc* desc, fs_stack** out, in
   s->pitch = plan.pitch;
   s->arena = arena;
   s->arena_size = arena ? arena_size : 0;
+  if (ctx->fuse_min_tiles) s->fuse_min_tiles = ctx->fuse_min_tiles;
   auto fail = [&](int rc) {
     fs_stack_destroy(s);
     return rc;
@@ -1221,10 +1234,11 @@ static int begin_impl(fs_ctx* ctx, const fs_stack_desc* desc, fs_stack** out, in
       for (uint32_t f = 0; f < d.frame_count; ++f)
         s->tab_host.push_back(l == 0 ? s->wplane[f] : l + 1 < s->L ? (const float*)s->mplane[f][l] : s->mtop[f]);
     }
-    // the small-level tail: levels T >= 1 whose sides are at most kTailSide,
-    // when they make two level steps or more
+    // the small-level tail: levels T >= 1 whose sides are at most kTailSide
+    // (or the context's smaller side), when they make two level steps or more
+    const uint32_t tail_side = ctx->tail_side ? ctx->tail_side : (uint32_t)kTailSide;
     for (uint32_t l = 1; l < s->L; ++l) {
-      if (std::max(s->lw[l], s->lh[l]) <= (uint32_t)kTailSide) {
+      if (std::max(s->lw[l], s->lh[l]) <= tail_side) {
         if (s->L - 1 - l >= 2 && s->L - 1 - l <= (uint32_t)kMaxTail) s->tail = l;
         break;
       }
@@ -1553,7 +1567,7 @@ static int pass2_impl(fs_stack* s, fs_frame_fetch_cb refetch, void* user, bool f
     uint32_t lf = 1;
     for (; lf + 1 < s->L && lf < tail; ++lf) {
       const int64_t tiles = (int64_t)((s->lw[lf] + kTileW - 1) / kTileW) * ((s->lh[lf] + kTileH - 1) / kTileH);
-      if (tiles < kBlendReduceMinTiles) break;
+      if (tiles < s->fuse_min_tiles) break;
       const void* const* lap = (const void* const*)(s->tab + (size_t)lf * 2 * N);
       const void* const* msk = (const void* const*)(s->tab + (size_t)lf * 2 * N + N);
       void* const* nxt = (void* const*)(s->tab + (size_t)(lf + 1) * 2 * N + N);
@@ -2239,6 +2253,8 @@ int fs_batch_create(fs_ctx* ctx, uint32_t n, const fs_stack_desc* descs, const v
     fs_ctx* c = nullptr;
     int rc = fs_create(ctx->device, std::max<uint64_t>(arena[l] + tables[l], 1), &c);
     if (rc != FS_OK) return fail(rc);
+    c->fuse_min_tiles = ctx->fuse_min_tiles;  // the lanes' stacks take the parent's level schedule
+    c->tail_side = ctx->tail_side;
     b->lanes.push_back(c);
     cudaEvent_t ev;
     cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);

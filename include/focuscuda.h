@@ -89,6 +89,14 @@ int fs_ctx_reserve(fs_ctx* ctx, uint64_t bytes);
  * use it; memory already held is not released).  Used by a serving loop that
  * hands each admitted stack its reservation.  Not part of the reference. */
 int fs_ctx_set_budget(fs_ctx* ctx, uint64_t hbm_budget_bytes);
+/* Level schedule of the split-pyramid stacks begun on the context from now
+ * on (and of the stacks of batches created from it): levels l >= 1 of at
+ * least fuse_min_tiles 64x32 tiles blend and REDUCE their masks in one pass
+ * (0: 1184; UINT32_MAX: none), and the levels whose sides are both at most
+ * tail_side (0: 64, at most 64) run as the small-level tail.  Every schedule
+ * gives the same bytes; the batched form's autotuner picks among them.  Not
+ * part of the reference. */
+int fs_ctx_set_level_schedule(fs_ctx* ctx, uint32_t fuse_min_tiles, uint32_t tail_side);
 /* The CUDA stream (cudaStream_t) all of the context's kernels run on, for
  * callers that order their own work or record events against it. */
 int fs_ctx_stream(const fs_ctx* ctx, void** stream);

@@ -341,12 +341,36 @@ def test_autotuner_caches_the_winner_per_workload(tmp_path, monkeypatch):
                                                                                        frames=[0] * 3)]
     path = str(tmp_path / "tune.json")
     space = {"lanes": (2, 4), "frames_per_batch": (4, 8), "pass2_mode": (3, 0)}
-    r1 = at.tune(ctx, stacks, space=space, cache_path=path)
+    r1 = at.tune(ctx, stacks, space=space, cache_path=path, schedule_space={})
     assert not r1["cached"] and len(calls) == 8
     assert r1["best"] == {"lanes": 4, "frames_per_batch": 4, "pass2_mode": 3}
     assert sum("skipped" in t for t in r1["trials"]) == 4
     r2 = at.tune(ctx, list(reversed(stacks)), space=space, cache_path=path)
     assert r2["cached"] and r2["best"] == r1["best"] and len(calls) == 8
     # another workload is timed again
-    at.tune(ctx, stacks[:1], space=space, cache_path=path)
+    at.tune(ctx, stacks[:1], space=space, cache_path=path, schedule_space={})
     assert len(calls) == 16
+
+
+def test_autotuner_searches_the_level_schedule_with_the_best_knobs(monkeypatch):
+    """After lanes x K x pass-2 mode, the level schedule is timed with the best
+    of them (the library's own schedule, all zeros, is not timed twice) and a
+    faster schedule becomes part of the winner."""
+    from types import SimpleNamespace
+
+    at = fsb.autotune
+    calls = []
+
+    def fake_time(ctx, stacks, reps=3, level_storage=0, **knobs):
+        calls.append(knobs)
+        t = 1.0 / knobs["lanes"] - 0.05 * (knobs.get("fuse_min_tiles", 0) == 296) - 0.01 * (knobs.get("tail_side", 0) == 32)
+        return {"knobs": dict(knobs), "s_per_run": t}
+
+    monkeypatch.setattr(at, "time_batch", fake_time)
+    ctx = SimpleNamespace(budget=lambda: 120e9)
+    stacks = [SimpleNamespace(width=640, height=480, frames=[0] * 5)]
+    r = at.tune(ctx, stacks, space={"lanes": (2, 4), "frames_per_batch": (8,), "pass2_mode": (3,)},
+                schedule_space={"fuse_min_tiles": (0, 296), "tail_side": (0, 32)})
+    assert len(calls) == 2 + 3
+    assert all(c["lanes"] == 4 for c in calls[2:])
+    assert r["best"] == {"lanes": 4, "frames_per_batch": 8, "pass2_mode": 3, "fuse_min_tiles": 296, "tail_side": 32}
