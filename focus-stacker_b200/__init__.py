@@ -16,5 +16,5 @@ from .api import (  # noqa: F401
     decode_jpeg, decode_jpeg_device, jpeg_info, DeviceBuffer, StackBatch, stack_desc,
     stack_footprint, stack_mode_bytes, exact_expand_divisor, forward_map_points, fuse_aligned_images, fuse_remapped_images,
     inverse_map_points, parse_method, parse_window_size, remap_rigid_image, remap_rigid_image_device,
-    synth_frame_device, synth_pose,
+    synth_frame_device, synth_pose, check_normalise,
 )

@@ -24,7 +24,7 @@ STATUS_NAMES = {
 EXPORTED = (
     "fs_create", "fs_destroy", "fs_last_error", "fs_status_string", "fs_api_version", "fs_ctx_device_bytes",
     "fs_ctx_budget",
-    "fs_ctx_synchronize", "fs_ctx_trim", "fs_ctx_reserve", "fs_ctx_set_budget", "fs_ctx_set_level_schedule", "fs_ctx_stream", "fs_ctx_launch_count", "fs_ctx_set_kernel_timing", "fs_ctx_kernel_stats",
+    "fs_ctx_synchronize", "fs_ctx_trim", "fs_ctx_reserve", "fs_ctx_set_budget", "fs_ctx_set_level_schedule", "fs_check_normalise", "fs_ctx_stream", "fs_ctx_launch_count", "fs_ctx_set_kernel_timing", "fs_ctx_kernel_stats",
     "fs_pose_default", "fs_compute_roi", "fs_inverse_map_points", "fs_forward_map_points", "fs_exact_expand_divisor",
     "fs_remap_frame", "fs_remap_frame_device", "fs_remap_frame16", "fs_remap_frame16_device",
     "fs_stack_begin", "fs_stack_add_frame", "fs_stack_add_frame_async", "fs_stack_add_frame_device", "fs_stack_finish",
@@ -98,6 +98,7 @@ def _bind(L):
     L.fs_ctx_reserve.argtypes = [ctx, u64]
     L.fs_ctx_set_budget.argtypes = [ctx, u64]
     L.fs_ctx_set_level_schedule.argtypes = [ctx, ctypes.c_uint32, ctypes.c_uint32]
+    L.fs_check_normalise.argtypes = [ctx, vp, vp, vp, sz]
     L.fs_ctx_stream.argtypes = [ctx, P(vp)]
     L.fs_ctx_launch_count.argtypes = [ctx]
     L.fs_ctx_launch_count.restype = u64

@@ -713,6 +713,16 @@ def synth_pose(seed: int, scene: int, width: int, height: int, frame: int, frame
     return ImagePose.from_c(p)
 
 
+def check_normalise(ctx: Context, w, n, out):
+    """out = w / n elementwise (device float32 buffers of one length) as the
+    split pyramid's level-0 blend divides: Markstein's refinement from n's
+    correctly rounded reciprocal; for tests against the IEEE division."""
+    count = int(w.numel())
+    if int(n.numel()) != count or int(out.numel()) != count:
+        raise FocusCudaError(2, "check_normalise: buffers of different lengths")
+    _check(L().fs_check_normalise(ctx.handle, _ptr(w), _ptr(n), _ptr(out), count), ctx.handle)
+
+
 def synth_frame_device(ctx: Context, seed: int, scene: int, width: int, height: int, frame: int, frame_count: int,
                        dst, dst_stride: int) -> ImagePose:
     p = _lib.FsPose()

@@ -791,6 +791,14 @@ int fs_ctx_trim(fs_ctx* ctx) {
   return FS_OK;
 }
 
+int fs_check_normalise(fs_ctx* ctx, const float* w, const float* n, float* out, size_t count) {
+  if (!ctx || (count && (!w || !n || !out))) return FS_ERR_INVALID;
+  cudaSetDevice(ctx->device);
+  cudaError_t e = launch_normalise_check(w, n, out, count, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  return e == cudaSuccess ? FS_OK : cuda_err(ctx, e, "normalise check");
+}
+
 int fs_ctx_stream(const fs_ctx* ctx, void** stream) {
   if (!ctx || !stream) return FS_ERR_INVALID;
   *stream = (void*)ctx->stream;

@@ -1315,6 +1315,12 @@ __device__ __forceinline__ float div_by_rcp(float a, float b, float y) {
   return __fmaf_rn(__fmaf_rn(-b, q1, a), y, q1);
 }
 
+// out[i] = w[i] / n[i] by div_by_rcp, for the check of its rounding.
+__global__ void normalise_check_kernel(const float* w, const float* n, float* out, size_t count) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < count; i += (size_t)gridDim.x * blockDim.x)
+    out[i] = div_by_rcp(w[i], n[i], __frcp_rn(n[i]));
+}
+
 // w / N (inv_count where N <= 1e-12), N's reciprocals in ry.
 __device__ __forceinline__ float4 b0_mask(const B0Chunk& c, const float (&ry)[4], float4 w, float inv_count) {
   float4 m;
@@ -2463,6 +2469,15 @@ static cudaError_t launch_blend_reduce_o(int out_storage, float* acc, int64_t pl
                                                             pitch_n, wn, hn, frames, inv_count, s);
     default: return cudaErrorInvalidValue;
   }
+}
+
+cudaError_t launch_normalise_check(const float* w, const float* n, float* out, size_t count, cudaStream_t s) {
+  if (count == 0) return cudaSuccess;
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  normalise_check_kernel<<<(unsigned)(8 * sms), 256, 0, s>>>(w, n, out, count);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_blend0_reduce(float* acc, int64_t plane, int64_t pitch, int w, int h, const float* norm,

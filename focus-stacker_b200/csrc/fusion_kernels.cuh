@@ -252,6 +252,9 @@ cudaError_t launch_blend0_reduce(float* acc, int64_t plane, int64_t pitch, int w
                                  const uint8_t* sm, const float* const* lap, const float* const* wgt,
                                  void* const* mask1, int64_t pitch_n, int wn, int hn, int frames, float inv_count,
                                  int out_storage, cudaStream_t s);
+// out[i] = w[i] / n[i] as the level-0 blend divides (the refinement from
+// the correctly rounded reciprocal), on device arrays of `count` floats.
+cudaError_t launch_normalise_check(const float* w, const float* n, float* out, size_t count, cudaStream_t s);
 // The same for a level l >= 1 of a split-pyramid stack: acc = sum over
 // frames, in order, of lap[k] x mask[k] (both in `storage`; 3 Laplacian
 // planes of `plane` samples), and mask_next[k] the REDUCE of mask[k] with

@@ -97,6 +97,13 @@ int fs_ctx_set_budget(fs_ctx* ctx, uint64_t hbm_budget_bytes);
  * gives the same bytes; the batched form's autotuner picks among them.  Not
  * part of the reference. */
 int fs_ctx_set_level_schedule(fs_ctx* ctx, uint32_t fuse_min_tiles, uint32_t tail_side);
+/* out[i] = w[i] / n[i] (device arrays of `count` floats) as the level-0
+ * blend of the split pyramid divides each frame's weight by the weight sum:
+ * Markstein's refinement from n's correctly rounded reciprocal, which the
+ * blend forms once per pixel for all frames.  For tests that compare it bit
+ * for bit with the IEEE division.  No counterpart in the reference (which
+ * divides, src/fuse/pyramid.zig:303-316). */
+int fs_check_normalise(fs_ctx* ctx, const float* w, const float* n, float* out, size_t count);
 /* The CUDA stream (cudaStream_t) all of the context's kernels run on, for
  * callers that order their own work or record events against it. */
 int fs_ctx_stream(const fs_ctx* ctx, void** stream);
