@@ -41,6 +41,8 @@ def test_stack_entry_points_reject_null_handles():
     cb = ctypes.cast(None, fsb._lib.FETCH_CB)
     assert L.fs_stack_finish_async(None, cb, None, out.ctypes.data, 16) == invalid
     assert L.fs_stack_finish(None, cb, None, out.ctypes.data, 16) == invalid
+    assert L.fs_ctx_set_level_schedule(None, 0, 0) == invalid
+    assert L.fs_check_normalise(None, None, None, None, 0) == invalid
 
 
 def test_context_without_gpu_reports_no_device():
