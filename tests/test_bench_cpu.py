@@ -94,3 +94,27 @@ def test_algorithmic_bytes_model(mode):
         assert per_kernel["remap_weights"] > 0
     # FP16 storage moves fewer level bytes
     assert bench.algorithmic_bytes(w, h, f, k, mode, 2)[1] < total
+
+
+def test_split_pyramid_byte_model_follows_the_fused_kernels():
+    """laps: the level-0 blend reads each frame's Laplacian (12 B) and weight
+    (4 B) once and writes its level-1 mask, with no level-0 mask through
+    HBM; levels of at least 1184 64x32 tiles (1 and 2 of the bench stack)
+    read each frame's mask once for the blend and the REDUCE together."""
+    w, h, f, k = 7872, 5243, 30, 8
+    per_kernel, _ = bench.algorithmic_bytes(w, h, f, k, "laps", 4)
+    sizes = bench.level_sizes(w, h)
+    a0, a1, a2 = (sizes[0][0] * sizes[0][1], sizes[1][0] * sizes[1][1], sizes[2][0] * sizes[2][1])
+    assert per_kernel["level0"] == 0
+    assert per_kernel["blend0"] == f * (16 * a0 + 4 * a1) + 17 * a0
+    # the unfused model of the same levels reads every mask of levels 1 and 2 once more
+    tiles = [-(-x // 64) * -(-y // 32) for x, y in sizes]
+    assert tiles[1] >= 1184 and tiles[2] >= 1184 and tiles[3] < 1184
+    L = len(sizes)
+    unfused = 0
+    for l in range(1, L):  # FP32 storage: 4 B per mask sample, 12 + 4 B per Laplacian + mask
+        al = sizes[l][0] * sizes[l][1]
+        if l + 1 < L:
+            unfused += f * (4 * al + 4 * sizes[l + 1][0] * sizes[l + 1][1]) + al
+        unfused += f * 16 * al + 12 * al
+    assert unfused - per_kernel["level"] == f * 4 * (a1 + a2)
